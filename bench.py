@@ -1,0 +1,418 @@
+#!/usr/bin/env python
+"""Benchmark of the assembly + GMRES hot path on the 2.1M-node quench case.
+
+Metric (the reference's): assembly Melem/s and GMRES s/solve at 2.1M nodes,
+mixed precision vs FP64, to a true relative residual of 1e-8.
+
+Workload: NS+VOF+T quench physics on a 128^3-cell unit cube split into 6
+Kuhn tets per cell (12,582,912 tets, 2,146,689 nodes, 31,802,497 CSR slots),
+synthetic seeded fields (interface phi = tanh((z-0.5)/0.02), hot centred
+cube), inputs far larger than L2.
+
+One step = one assembly pass of all fields (alpha stage, NS+VOF MAT+VEC,
+temperature MAT+VEC) in FP32 (the mixed path).  `value` is its throughput
+(E / device time).  The GMRES solves are timed separately: the coupled
+NS+VOF system and the temperature system, each brought to
+||b - A x|| <= 1e-8 ||b|| by the mixed path (FP32 matrix/SpMV/basis, FP64
+Gram-Schmidt/Givens/refinement residual) and by the all-FP64 path.
+
+    python bench.py [--gpus N --steps K --warmup W] [--impl reference]
+
+With --gpus N > 1 (torchrun) every rank solves its own replica of the case
+(weak scaling; the path's multi-GPU halo exchange is not built).
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import threading
+import time
+from pathlib import Path
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT))
+
+METRIC = "assembly Melem/s & GMRES s/solve at 2.1M nodes, mixed vs FP64 to rel. resid 1e-8"
+
+
+def _peaks():
+    try:
+        return json.loads((ROOT / "MEASURED_PEAKS.json").read_text()), "measured"
+    except Exception:
+        return {"hbm_gbs": 6650.0, "bf16_tflops": 1590.0}, "fallback"
+
+
+# ------------------------------------------------------------------ clocks
+class ClockSampler:
+    """nvidia-smi sampling of SM clocks and throttle reasons while running."""
+
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu: int):
+        self.gpu = gpu
+        self.f = tempfile.NamedTemporaryFile("w+", suffix=".csv", delete=False)
+        self.p = None
+        self.marks = []
+
+    def start(self):
+        try:
+            self.p = subprocess.Popen(["nvidia-smi", "-i", str(self.gpu), f"--query-gpu={self.Q}",
+                                       "--format=csv,noheader,nounits", "-lms", "200"],
+                                      stdout=self.f, stderr=subprocess.DEVNULL)
+        except Exception:
+            self.p = None
+
+    def mark(self, on: bool):
+        self.marks.append((time.time(), on))
+
+    def stop(self) -> dict:
+        if self.p is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.p.terminate()
+        try:
+            self.p.wait(timeout=5)
+        except Exception:
+            self.p.kill()
+        self.f.flush()
+        rows = [l.split(",") for l in Path(self.f.name).read_text().splitlines() if l.strip()]
+        sm, mx, reasons, power = [], None, set(), []
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for r in rows:
+            try:
+                s, m = float(r[1]), float(r[2])
+            except (ValueError, IndexError):
+                continue
+            mx = m
+            power.append(float(r[3]) if r[3].strip().replace(".", "").isdigit() else 0.0)
+            if s > 0.5 * m:          # samples under load
+                sm.append(s)
+            for nm, v in zip(names, r[5:9]):
+                if v.strip().lower() == "active":
+                    reasons.add(nm)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": mx,
+                "reasons": sorted(reasons), "samples": len(rows), "samples_under_load": len(sm),
+                "power_w_max": max(power) if power else None}
+
+
+# -------------------------------------------------------------- CPU oracle
+def config3_slab(n: int, k0: int, nl: int):
+    """Layers k0..k0+nl of the n^3 quench cube, same geometry and fields
+    (the bounded sample of the full workload timed on the host)."""
+    import numpy as np
+    from oversetdevfort_b200 import mesh as M
+    m = M.box_tet(n, n, nl, 1.0, 1.0, nl / n)
+    m.xg[:, 2] += k0 / n
+    case = M.quench_case(m, f"config3_slab_{k0}_{nl}")
+    z = m.xg[:, 2]
+    phi = np.tanh((z - 0.5) / 0.02)
+    case.state["phig"][:] = phi
+    case.state["phigold"][:] = phi
+    hot = np.all(np.abs(m.xg - 0.5) <= 0.2 + 1e-12, axis=1)
+    T = np.where(hot, 1000.0, 300.0)
+    case.state["tg"][:] = T
+    case.state["tgold"][:] = T
+    return case
+
+
+def cpu_assembly_pass(case, reps: int = 1):
+    """Seconds of alpha stage + NS+VOF and temperature element loops (MAT+VEC)
+    of the oracle on `case`, best of reps."""
+    from oracle import pyoracle as O
+    oc = O.OracleCase(case)
+    best = None
+    for _ in range(reps):
+        t = oc.time_alpha_stage()
+        t += oc.time_element_loop("nsvof", 6, 0, oc.E)
+        t += oc.time_element_loop("tem", 6, 0, oc.E)
+        best = t if best is None else min(best, t)
+    return best, oc.E, oc.N
+
+
+def _cpu_worker(args):
+    n, k0, nl, steps, warmup = args
+    case = config3_slab(n, k0, nl)
+    from oracle import pyoracle as O
+    oc = O.OracleCase(case)
+    times = []
+    for i in range(warmup + steps):
+        t0 = time.perf_counter()
+        oc.time_alpha_stage()
+        oc.time_element_loop("nsvof", 6, 0, oc.E)
+        oc.time_element_loop("tem", 6, 0, oc.E)
+        if i >= warmup:
+            times.append(time.perf_counter() - t0)
+    return oc.E, times
+
+
+def run_reference(args, world, rank):
+    """--impl reference: the reference's CPU algorithm (the oracle port; the
+    Fortran reference cannot be compiled here) on all host cores, one
+    process per core on its own slab of the workload, like the reference's
+    MPI ranks."""
+    if rank != 0:
+        return
+    import multiprocessing as mp
+    cores = os.cpu_count() or 1
+    n, nl = args.n, 2
+    nslab = max(1, n // nl)
+    jobs = [(n, (i * nl) % (n - nl + 1), nl, args.steps, args.warmup) for i in range(cores)]
+    from oracle import pyoracle as O
+    O.build()
+    t0 = time.time()
+    with mp.get_context("spawn").Pool(cores) as pool:
+        res = pool.map(_cpu_worker, jobs)
+    wall = time.time() - t0
+    E_tot = sum(e for e, _ in res)
+    per_step = [max(r[1][k] for r in res) for k in range(args.steps)]
+    thr = [E_tot / t / 1e6 for t in per_step]
+    value = statistics.mean(thr)
+    line = {
+        "impl": "reference", "metric": METRIC, "value": value, "unit": "Melem/s",
+        "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": statistics.mean(per_step) * 1e3, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": {"workload": f"config3 quench NS+VOF+T assembly, {n}^3 cells x6 tets; each of "
+                               f"{cores} processes assembles a {n}x{n}x{nl}-cell slab of it",
+                   "cache": "per-process slab", "parallelism": f"{cores} processes (MPI-rank analogue)"},
+        "cpu_baseline": {"value": value, "unit": "Melem/s", "cores": cores, "kind": "port",
+                         "sample": f"{cores} slabs of {E_tot // cores} tets, alpha stage + NS+VOF + T "
+                                   f"element loops MAT+VEC, {args.steps} timed passes"},
+        "e2e": {"value": value, "unit": "Melem/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+        "wall_s": wall,
+    }
+    print(json.dumps(line), flush=True)
+
+
+# --------------------------------------------------------------- GPU arm
+def run_ours(args, world, rank, local_rank, dist):
+    import numpy as np
+    from oversetdevfort_b200 import _ffi as F
+    from oversetdevfort_b200 import mesh as M
+    from oversetdevfort_b200.api import Context, PinnedArray
+
+    peaks, peak_kind = _peaks()
+    n = args.n
+    t_setup = time.time()
+    case = M.config3(n)
+    m = case.mesh
+    E, N = m.nelem, m.nnode
+    ctx = Context.from_case(case, device=local_rank)
+    nnz = ctx.icnt
+    setup_s = time.time() - t_setup
+
+    def barrier():
+        if dist is not None:
+            dist.barrier()
+
+    def maxr(x: float) -> float:
+        if dist is None:
+            return x
+        import torch
+        t = torch.tensor([x], dtype=torch.float64, device=f"cuda:{local_rank}")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return float(t.item())
+
+    def assembly_pass(prec):
+        ctx.assemble(F.OVS_ASM_NSVOF, 6, prec)
+        a = ctx.last_device_ms()
+        ctx.assemble(F.OVS_ASM_TEM, 6, prec)
+        return a + ctx.last_device_ms()
+
+    # ---------------------------------------------------- CPU baseline
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu:
+        nl = 8
+        slab = config3_slab(n, n // 2 - nl // 2, nl)
+        t, Es, Ns = cpu_assembly_pass(slab, reps=1)
+        cpu = {"value": Es / t / 1e6, "unit": "Melem/s", "cores": 1, "kind": "port",
+               "sample": f"{Es} tets ({n}x{n}x{nl}-cell slab of the workload across the interface): "
+                         f"alpha stage + NS+VOF + T element loops MAT+VEC, one pass, {t:.1f} s"}
+
+    clocks = ClockSampler(local_rank)
+    clocks.start()
+    launches0 = ctx.launch_count()
+    # ------------------------------------------------- timed assembly
+    res = {}
+    for prec, name in ((F.OVS_FP32, "fp32"), (F.OVS_FP64, "fp64")):
+        for _ in range(args.warmup):
+            assembly_pass(prec)
+        barrier()
+        ctx.synchronize()
+        t0 = time.time()
+        ms = [assembly_pass(prec) for _ in range(args.steps)]
+        ctx.synchronize()
+        wall = time.time() - t0
+        barrier()
+        res[name] = {"ms": maxr(statistics.mean(ms)), "wall_s": wall}
+    launches_step = (ctx.launch_count() - launches0) / (2 * (args.warmup + args.steps))
+    ms_step = res["fp32"]["ms"]
+    value = world * E / (ms_step * 1e-3) / 1e6
+
+    # --------------------------------------------- kernel roofline
+    prof = {}
+    prof["asm_nsvof_fp32_ms"] = ctx.profile(F.OVS_PROF_ASSEMBLE, F.OVS_ASM_NSVOF, F.OVS_FP32, 5)
+    prof["asm_tem_fp32_ms"] = ctx.profile(F.OVS_PROF_ASSEMBLE, F.OVS_ASM_TEM, F.OVS_FP32, 5)
+    prof["asm_nsvof_fp64_ms"] = ctx.profile(F.OVS_PROF_ASSEMBLE, F.OVS_ASM_NSVOF, F.OVS_FP64, 3)
+    ctx.assemble(F.OVS_ASM_NSVOF, 6, F.OVS_FP32)
+    prof["spmv_nsvof_fp32_ms"] = ctx.profile(F.OVS_PROF_SPMV, F.OVS_SYS_NSVOF, F.OVS_FP32, 20)
+    prof["spmv_nsvof_fp64_ms"] = ctx.profile(F.OVS_PROF_SPMV, F.OVS_SYS_NSVOF, F.OVS_FP64, 10)
+    prof["mgs_nsvof_fp32_ms"] = ctx.profile(F.OVS_PROF_MGS, F.OVS_SYS_NSVOF, F.OVS_FP32, 20)
+    prof["mgs_nsvof_fp64_ms"] = ctx.profile(F.OVS_PROF_MGS, F.OVS_SYS_NSVOF, F.OVS_FP64, 20)
+
+    def spmv_bytes(s):  # values, colidx, rowptr, x gather (once), y, preconditioner
+        return 24 * nnz * s + 4 * nnz + 4 * (N + 1) + 5 * N * s + 5 * N * s + 11 * N * s
+
+    def asm_bytes(s):   # FP64 state read by the alpha stage is not in the row kernel
+        return 4 * 4 * E + 20 * N * s + N + 4 * (N + 1) + 4 * nnz + 8 * (N + 1) + 4 * 4 * E \
+            + 24 * nnz * s + 5 * N * s
+
+    hbm = float(peaks["hbm_gbs"])
+    sp_ach = spmv_bytes(4) / (prof["spmv_nsvof_fp32_ms"] * 1e-3) / 1e9
+    as_ach = asm_bytes(4) / (prof["asm_nsvof_fp32_ms"] * 1e-3) / 1e9
+    roof_asm = {"kernel": "assemble_rows_kernel<float,NSVOF> (row-owner element assembly)",
+                "bound": "hbm", "achieved": as_ach, "peak": hbm, "unit": "GB/s",
+                "frac": as_ach / hbm, "traffic": None, "peak_kind": peak_kind,
+                "algorithmic_bytes": asm_bytes(4), "avg_ms": prof["asm_nsvof_fp32_ms"]}
+    roof_spmv = {"kernel": "spmv_block_kernel<6,float> (P^-1 A x, NS+VOF)", "bound": "hbm",
+                 "achieved": sp_ach, "peak": hbm, "unit": "GB/s", "frac": sp_ach / hbm, "traffic": None,
+                 "peak_kind": peak_kind, "algorithmic_bytes": spmv_bytes(4),
+                 "avg_ms": prof["spmv_nsvof_fp32_ms"]}
+
+    # ------------------------------------------------------- solves
+    gm = {}
+    if not args.no_solve:
+        sols = {}
+        for mode, name in ((F.OVS_FP32, "mixed"), (F.OVS_FP64, "fp64")):
+            rec = {}
+            for sysid, kern, key in ((F.OVS_SYS_NSVOF, F.OVS_ASM_NSVOF, "nsvof"),
+                                     (F.OVS_SYS_TEM, F.OVS_ASM_TEM, "tem")):
+                ctx.assemble(kern, 6, mode)
+                barrier()
+                sol, info = ctx.solve(sysid, mode, args.rtol, kspace=args.kspace, max_cycles=args.max_cycles)
+                barrier()
+                rec[key] = {"s": maxr(info.seconds), "iterations": info.iterations, "cycles": info.cycles,
+                            "rel_residual": info.rel_residual, "converged": bool(info.converged)}
+                sols[(name, key)] = sol
+            rec["s_per_solve"] = rec["nsvof"]["s"] + rec["tem"]["s"]
+            gm[name] = rec
+        gm["speedup_mixed_vs_fp64"] = gm["fp64"]["s_per_solve"] / gm["mixed"]["s_per_solve"]
+        err = {}
+        for key, names in (("nsvof", ["u", "v", "w", "p", "phi"]), ("tem", ["T"])):
+            a, b = sols[("mixed", key)], sols[("fp64", key)]
+            for f, nm in enumerate(names):
+                err[nm] = float(np.abs(a[:, f] - b[:, f]).max() / max(np.abs(b[:, f]).max(), 1e-300))
+        gm["max_rel_err_mixed_vs_fp64"] = err
+        gm["rtol"] = args.rtol
+        gm["kspace"] = args.kspace
+
+    # ------------------------------------------------------------ e2e
+    # public API with host buffers: upload the state the assembly reads from
+    # page-locked host memory, assemble all fields (FP32), read the residual back
+    fields = ["dg", "dgold", "ug", "ugold", "acg", "acgold", "ugm", "ugmold", "pg", "phig", "phigold",
+              "rphig", "rphigold", "tg", "tgold", "rtg", "rtgold"]
+    host = {}
+    for f in fields:
+        pa = PinnedArray(case.state[f].shape)
+        pa.array[...] = case.state[f]
+        host[f] = pa
+    out_ns = PinnedArray((N, 5))
+    out_t = PinnedArray((N, 1))
+    h2d = sum(host[f].array.nbytes for f in fields)
+    d2h = out_ns.array.nbytes + out_t.array.nbytes
+    import ctypes as C
+    dp = C.POINTER(C.c_double)
+
+    def e2e_step():
+        for f in fields:
+            F.check(ctx.lib.ovs_set_field(ctx.h, F.FIELD_ID[f], host[f].array.ctypes.data_as(dp)), f)
+        ctx.assemble(F.OVS_ASM_NSVOF, 6, F.OVS_FP32)
+        ctx.assemble(F.OVS_ASM_TEM, 6, F.OVS_FP32)
+        F.check(ctx.lib.ovs_get_rhs(ctx.h, F.OVS_SYS_NSVOF, F.OVS_FP32, out_ns.array.ctypes.data_as(dp)), "rhs")
+        F.check(ctx.lib.ovs_get_rhs(ctx.h, F.OVS_SYS_TEM, F.OVS_FP32, out_t.array.ctypes.data_as(dp)), "rhs")
+
+    for _ in range(args.warmup):
+        e2e_step()
+    barrier()
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        e2e_step()
+    e2e_s = maxr((time.perf_counter() - t0) / args.steps)
+    barrier()
+    clk = clocks.stop()
+    total_launches = ctx.launch_count() - launches0
+
+    line = {
+        "metric": METRIC, "value": value, "unit": "Melem/s", "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": ms_step, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+        "config": {"workload": f"config3: NS+VOF+T quench assembly pass, {n}^3 cells x6 Kuhn tets "
+                               f"({E} tets, {N} nodes, {nnz} CSR slots), FP32 mixed path",
+                   "cache": "inputs larger than L2 (FP32 CSR values alone 2.9 GB); no flush",
+                   "parallelism": f"replicas x{world}" if world > 1 else "1 GPU"},
+        "e2e": {"value": world * E / e2e_s / 1e6, "unit": "Melem/s", "h2d_bytes_per_step": h2d,
+                "d2h_bytes_per_step": d2h},
+        "gpu_launches": int(launches_step * args.steps),
+        "clocks": clk,
+        "roofline": roof_asm,
+        "roofline_spmv": roof_spmv,
+        "assembly_melem_s": {"fp32": world * E / (res["fp32"]["ms"] * 1e-3) / 1e6,
+                             "fp64": world * E / (res["fp64"]["ms"] * 1e-3) / 1e6,
+                             "ms_fp32": res["fp32"]["ms"], "ms_fp64": res["fp64"]["ms"]},
+        "gmres": gm,
+        "kernel_ms": prof,
+        "launches_total": total_launches,
+        "setup_s": setup_s,
+    }
+    if cpu is not None:
+        line["cpu_baseline"] = cpu
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    for pa in list(host.values()) + [out_ns, out_t]:
+        pa.free()
+    ctx.close()
+
+
+def main():
+    ap = argparse.ArgumentParser(description=__doc__, formatter_class=argparse.RawDescriptionHelpFormatter)
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--n", type=int, default=128, help="cells per side of the cube (128: 2.1M nodes)")
+    ap.add_argument("--rtol", type=float, default=1e-8)
+    ap.add_argument("--kspace", type=int, default=50)
+    ap.add_argument("--max-cycles", type=int, default=400)
+    ap.add_argument("--no-solve", action="store_true")
+    ap.add_argument("--no-cpu", action="store_true")
+    args = ap.parse_args()
+    if args.warmup < 3:
+        args.warmup = 3
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local_rank = int(os.environ.get("LOCAL_RANK", "0"))
+    dist = None
+    if world > 1 and args.impl == "ours":
+        import datetime
+        import torch
+        import torch.distributed as tdist
+        torch.cuda.set_device(local_rank)
+        tdist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
+        dist = tdist
+    if args.impl == "reference":
+        run_reference(args, world, rank)
+    else:
+        run_ours(args, world, rank, local_rank, dist)
+    if dist is not None:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,263 @@
+/*
+ * ovs.h - C ABI of the B200 (sm_100a) implementation of the OversetDevFort
+ * per-timestep hot path: finite-element assembly of the VMS Navier-Stokes,
+ * VOF and temperature equations into the node-block CSR system, and the
+ * diagonally preconditioned GMRES solve of that system.
+ *
+ * Conventions (identical to the Fortran reference so that its arrays can be
+ * passed straight through):
+ *   - every array is column-major, "(N,3)" means three contiguous length-N
+ *     columns; element connectivity IEN(E,nshl) is 1-based;
+ *   - the CSR pattern uses the reference names: col(N+1) is the ROW POINTER,
+ *     row(icnt) holds the COLUMN indices, both 1-based, rows sorted ascending
+ *     (src/genSparStruc.f90:27-45);
+ *   - block values of slot k are stored the reference way: LHSK11(9,icnt)
+ *     with index (i-1)*3+j = (row component i, column component j),
+ *     LHSG(3,icnt), LHSD1(3,icnt), LHSM(icnt), LHSLS(icnt), LHSLSU(3,icnt),
+ *     LHSULS(3,icnt), LHSPLS(icnt), LHSTem(icnt) (src/alloc.f90:47-57).
+ *
+ * Every entry point returns an int status (OVS_OK = 0, negative = error,
+ * positive = warning, results valid).  All calls on one context are
+ * synchronous at return and must not be made concurrently from several host
+ * threads.  Device state stays resident in the context between calls.
+ */
+#ifndef OVS_H
+#define OVS_H
+
+#include <stddef.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---------------------------------------------------------------- status */
+enum {
+  OVS_OK = 0,
+  OVS_WARN_NEG_DETJ = 1,      /* some element had DetJ <= 0 (the reference
+                                 prints a warning and carries on:
+                                 src/eval_shape_FEM.f90:54-60) */
+  OVS_ERR_ARG = -1,           /* bad argument / size */
+  OVS_ERR_CUDA = -2,          /* CUDA runtime error */
+  OVS_ERR_NOMEM = -3,         /* device allocation failed */
+  OVS_ERR_STATE = -4,         /* call order (e.g. assemble before pattern) */
+  OVS_ERR_NONFINITE = -5,     /* NaN/Inf in an assembled residual */
+  OVS_ERR_PATTERN = -6,       /* a node has more neighbours than supported */
+  OVS_ERR_NODEVICE = -7,      /* no CUDA device */
+  OVS_ERR_TIMEOUT = -8        /* a bounded host wait on the device expired */
+};
+
+/* ------------------------------------------------------------- selectors */
+enum { OVS_FP64 = 0, OVS_FP32 = 1 };
+
+/* assembly kernels (the reference element routines they replace) */
+enum {
+  OVS_ASM_NS = 1,     /* IntElmAss_NS_overset, src/assembleNavSto.f90:76-336 */
+  OVS_ASM_NSVOF = 2,  /* IntElmAss_NSVOF_Quenching_STAB, src/solveQuenching.f90:122-573 */
+  OVS_ASM_TEM = 3     /* IntElmAss_Tem_Quenching_STAB, src/solveQuenching.f90:579-882 */
+};
+
+/* linear systems (dofs per node) */
+enum {
+  OVS_SYS_NS = 1,     /* u,v,w,p   : SparseGMRES_up / SparseProdUP_3D         */
+  OVS_SYS_NSVOF = 2,  /* u,v,w,p,phi: SparseGMRES_ns_conv / SparseProd_NS_conv */
+  OVS_SYS_TEM = 3     /* T          : SparseGMRES_tem / SparseProd_LS           */
+};
+
+/* tensor flags, same values as commonpars (src/modules.f90:218-228) */
+enum { OVS_TENSOR_VEC = 2, OVS_TENSOR_MAT = 4 };
+
+/* matrix blocks for ovs_get_lhs_block / ovs_set_lhs_block */
+enum {
+  OVS_BLK_K11 = 0,  /* (9,icnt) */
+  OVS_BLK_G = 1,    /* (3,icnt) */
+  OVS_BLK_D1 = 2,   /* (3,icnt) */
+  OVS_BLK_M = 3,    /* (icnt)   */
+  OVS_BLK_LS = 4,   /* (icnt)   */
+  OVS_BLK_LSU = 5,  /* (3,icnt) row phi, column u_i   */
+  OVS_BLK_ULS = 6,  /* (3,icnt) row u_i, column phi   */
+  OVS_BLK_PLS = 7,  /* (icnt)   row p,   column phi   */
+  OVS_BLK_TEM = 8   /* (icnt)   */
+};
+
+/* nodal state arrays (module aAdjKeep, src/modules.f90:235-320) */
+enum {
+  OVS_F_XG = 0,                     /* (N,3) reference coordinates   */
+  OVS_F_DG, OVS_F_DGOLD,            /* (N,3) displacement            */
+  OVS_F_UG, OVS_F_UGOLD,            /* (N,3) velocity                */
+  OVS_F_ACG, OVS_F_ACGOLD,          /* (N,3) acceleration            */
+  OVS_F_UGM, OVS_F_UGMOLD,          /* (N,3) mesh velocity           */
+  OVS_F_ACGM, OVS_F_ACGMOLD,        /* (N,3) mesh acceleration       */
+  OVS_F_PG,                         /* (N)   pressure                */
+  OVS_F_PHIG, OVS_F_PHIGOLD,        /* (N)   VOF                     */
+  OVS_F_RPHIG, OVS_F_RPHIGOLD,      /* (N)   VOF rate                */
+  OVS_F_TG, OVS_F_TGOLD,            /* (N)   temperature             */
+  OVS_F_RTG, OVS_F_RTGOLD,          /* (N)   temperature rate        */
+  OVS_F_COUNT
+};
+
+/* ---------------------------------------------------------------- types */
+typedef struct ovs_ctx ovs_ctx;
+
+typedef struct ovs_dims {
+  int nnode;   /* NNODE */
+  int nelem;   /* NELEM */
+  int nshl;    /* nodes per element: 4 (linear tet) or 8 (trilinear hex) */
+  int device;  /* CUDA device ordinal, or -1 for the calling thread's current one */
+} ovs_dims;
+
+/* Scalars of module commonvars the element routines read
+ * (src/modules.f90:325-455, src/param.f90:205-490). */
+typedef struct ovs_params {
+  double almi, alfi, gami, beti;   /* generalized-alpha (src/param.f90:469-480) */
+  double delt;                     /* time step Delt                        */
+  double rhow, rhoa, rhos;         /* density: liquid (phi=0), gas (phi=1), solid */
+  double muw, mua, mus;            /* viscosity                               */
+  double cpw, cpa, cps;            /* heat capacity                           */
+  double kappaw, kappaa, kappas;   /* conductivity                            */
+  double ts;                       /* saturation temperature Ts               */
+  double lh;                       /* latent heat Lh                          */
+  double c_evap, c_cond, c_dmdot;  /* phase-change model constants            */
+  double ns_kdc_w, ns_kdc_a;       /* NS discontinuity capturing              */
+  double lsc_kdc, tem_kdc, tref;   /* VOF / temperature discontinuity capturing */
+  double gravvec[3];               /* body force per unit mass (0,0,-9.81)    */
+  int fluid_elm_id;                /* ELM_ID of fluid elements (102)          */
+  int subdomain_flag;              /* assembleNavSto subdomain bit flags       */
+  int elm_id_set[2];               /* ELM_ID_SET(1:2)                          */
+} ovs_params;
+
+typedef struct ovs_gmres_info {
+  int iterations;      /* iKs on exit                                   */
+  int converged;       /* |e(iKs+1)| <= tol*|P^-1 b| and iKs >= kspace_min */
+  int breakdown;       /* H(k+1,k) == 0 met (exact solution reached)     */
+  int reserved;
+  double res0;         /* |P^-1 b| (unorm at entry)                      */
+  double ercheck;      /* |e(iKs+1)| on exit                             */
+} ovs_gmres_info;
+
+typedef struct ovs_solve_info {
+  int cycles;          /* outer refinement / restart cycles              */
+  int iterations;      /* total inner Krylov iterations                  */
+  int converged;       /* true relative residual <= rtol                  */
+  int reserved;
+  double rel_residual; /* ||b - A x||_2 / ||b||_2 in FP64 on exit        */
+  double seconds;      /* device time of the solve (CUDA events)          */
+} ovs_solve_info;
+
+/* ------------------------------------------------------- generalized-alpha */
+/* almi, alfi, gami, beti from rho_inf exactly as src/param.f90:469-480
+ * (backward Euler when rho_inf is outside [0,1]). */
+int ovs_params_genalpha(double rhoinf, ovs_params* p);
+
+/* ------------------------------------------------------------ stateless */
+int ovs_version(void);
+const char* ovs_status_string(int status);
+
+/* genSparStruc drop-in (src/genSparStruc.f90:4-105): builds the sorted,
+ * unique node-adjacency CSR of IEN on the GPU.  On entry *icnt is the
+ * capacity of `row`; on exit it is the number of entries.  Pass row=NULL to
+ * query icnt only.  col has N+1 entries.  All indices 1-based. */
+int ovs_gen_spar_struc(int nnode, int nelem, int nshl, const int* ien,
+                       int* col, int* row, int* icnt);
+
+/* -------------------------------------------------------------- context */
+int ovs_create(ovs_ctx** out, const ovs_dims* dims);
+int ovs_destroy(ovs_ctx* ctx);
+int ovs_synchronize(ovs_ctx* ctx);
+/* the cudaStream_t every call of this context is issued on */
+int ovs_get_stream(ovs_ctx* ctx, void** stream);
+
+/* mesh: xg(N,3), IEN(E,nshl) 1-based, ELM_ID(E) (may be NULL: all 102) */
+int ovs_upload_mesh(ovs_ctx* ctx, const double* xg, const int* ien,
+                    const int* elm_id);
+/* genSparStruc on the resident mesh; *icnt receives the entry count */
+int ovs_build_pattern(ovs_ctx* ctx, int* icnt);
+/* copy the pattern out (1-based, reference layout), col(N+1), row(icnt) */
+int ovs_get_pattern(ovs_ctx* ctx, int* col, int* row);
+
+int ovs_set_params(ovs_ctx* ctx, const ovs_params* p);
+/* IBC(N,nibc) column-major, entries 0/1 (src/setBCs.f90:183-187: columns
+ * 1-3 velocity, 4 pressure, 5 VOF, 6 temperature) */
+int ovs_set_ibc(ovs_ctx* ctx, const int* ibc, int nibc);
+int ovs_set_field(ovs_ctx* ctx, int field, const double* host);
+int ovs_get_field(ovs_ctx* ctx, int field, double* host);
+
+/* Assembly.  Replaces assembleNavSto (kernel OVS_ASM_NS,
+ * src/assembleNavSto.f90:4-72) and assembleQuenching with
+ * ASSEMBLE_FIELD_NS+VOF (OVS_ASM_NSVOF) or ASSEMBLE_FIELD_TEM (OVS_ASM_TEM)
+ * (src/solveQuenching.f90:4-117): alpha-stage blend, zeroing, element loop,
+ * element Dirichlet BCs and the scatter into CSR/RHS, in `precision`.
+ * cfl (may be NULL) receives the largest element CFL number. */
+int ovs_assemble(ovs_ctx* ctx, int kernel, int tensor_flag, int precision,
+                 double* cfl);
+
+/* RHS of `system` in reference layout: NS -> RHSGu(N,3),RHSGp(N);
+ * NSVOF -> additionally RHSGls(N); TEM -> RHSGtem(N).  Concatenated. */
+int ovs_get_rhs(ovs_ctx* ctx, int system, int precision, double* rhs);
+int ovs_set_rhs(ovs_ctx* ctx, int system, int precision, const double* rhs);
+/* one matrix block in reference layout (see OVS_BLK_*) */
+int ovs_get_lhs_block(ovs_ctx* ctx, int system, int precision, int block,
+                      double* out);
+int ovs_set_lhs_block(ovs_ctx* ctx, int system, int precision, int block,
+                      const double* in);
+
+/* y = A x without preconditioning (SparseProdUP_3D / SparseProd_NS_conv /
+ * SparseProd_LS, src/SparseProd.f90:4-60,128-242) on host vectors in
+ * reference layout. */
+int ovs_spmv(ovs_ctx* ctx, int system, int precision, const double* x,
+             double* y);
+
+/* One GMRES cycle with the reference's exact semantics, in FP64 on the FP64
+ * system: SparseGMRES_up (src/SparseGMRES_NS.f90:4-369),
+ * SparseGMRES_ns_conv (src/SparseGMRES_NS_conv.f:1-406),
+ * SparseGMRES_tem (src/SparseGMRES_tem.f90:1-256).  sol (host, reference
+ * layout) is accumulated into: sol += sum_j y_j v_j. */
+int ovs_gmres(ovs_ctx* ctx, int system, double tol, int kspace,
+              int kspace_min, double* sol, ovs_gmres_info* info);
+
+/* Solve A x = b to ||b - A x||_2 <= rtol ||b||_2 (true residual, FP64).
+ * mode OVS_FP64: restarted FP64 GMRES(kspace) on the FP64 system.
+ * mode OVS_FP32: mixed precision - FP32 system and FP32 Krylov basis inside,
+ * FP64 Gram-Schmidt dots / Givens / back-substitution, FP64 iterative
+ * refinement residual r = b - A x.  The solution stays on the device
+ * (ovs_newton_update applies it); sol (host, may be NULL) receives a copy. */
+int ovs_solve(ovs_ctx* ctx, int system, int mode, double rtol, int kspace,
+              int max_cycles, double* sol, ovs_solve_info* info);
+
+/* Newton update with the last solution of `system` (src/solveFlow.f90:99-104,
+ * 139-140; src/solveOverset.f90:76-78):
+ *   NS/NSVOF: acg += du; ug += gami*Delt*du; pg += alfi*gami*Delt*dp;
+ *   NSVOF:    rphig += dphi; phig += gami*Delt*dphi;
+ *   TEM:      rTg += dT; Tg += gami*Delt*dT. */
+int ovs_newton_update(ovs_ctx* ctx, int system);
+
+/* calculate_residual (src/solveFlow.f90:169-187): sums of squares (no sqrt)
+ * of RHSGu, RHSGp, RHSGls, RHSGtem of the given precision. */
+int ovs_residual_norms(ovs_ctx* ctx, int precision, double r[4]);
+
+/* ----------------------------------------------------------- measurement
+ * Hooks for benchmarking; they have no counterpart in the reference. */
+enum { OVS_PROF_SPMV = 1, OVS_PROF_ASSEMBLE = 2, OVS_PROF_MGS = 3 };
+/* Average device time in ms (CUDA events on the context stream) of `reps`
+ * back-to-back launches of one internal kernel on the resident data:
+ *   OVS_PROF_SPMV      preconditioned SpMV y = P^-1 A x of `system`, matrix
+ *                      and vectors in `precision` (needs the matrix);
+ *   OVS_PROF_ASSEMBLE  the element/row kernel of assembly kernel `system`
+ *                      (an OVS_ASM_* value), MAT+VEC, on the node records of
+ *                      the last ovs_assemble of that kernel and precision;
+ *   OVS_PROF_MGS       one fused Gram-Schmidt step (w -= b v; <w, v>) on
+ *                      basis vectors of `system` in `precision`. */
+int ovs_profile(ovs_ctx* ctx, int what, int system, int precision, int reps,
+                double* avg_ms);
+/* number of CUDA kernels this context has launched so far */
+int ovs_launch_count(ovs_ctx* ctx, long long* n);
+/* device time in ms (CUDA events) of the most recent ovs_assemble,
+ * ovs_solve or ovs_gmres call of this context */
+int ovs_last_device_ms(ovs_ctx* ctx, double* ms);
+/* page-locked host buffers for fast transfers of state and results */
+int ovs_host_alloc(void** p, size_t bytes);
+int ovs_host_free(void* p);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* OVS_H */

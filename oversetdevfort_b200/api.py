@@ -1,0 +1,333 @@
+"""Host-side mirror of the reference's hot-path interface.
+
+The reference calls these Fortran routines from its Newton drivers
+(src/solveFlow.f90, src/solveOverset.f90):
+
+    genSparStruc()                                   src/genSparStruc.f90:4
+    assembleNavSto(tensor_flag, subdomain_flag)      src/assembleNavSto.f90:4
+    assembleQuenching(tensor_flag, field_flag)       src/solveQuenching.f90:4
+    SparseGMRES_up(..., Utol, Kspaceu, Kspaceu_mn)   src/SparseGMRES_NS.f90:4
+    SparseGMRES_ns_conv(...)                         src/SparseGMRES_NS_conv.f:1
+    SparseGMRES_tem(...)                             src/SparseGMRES_tem.f90:1
+    calculate_residual(...)                          src/solveFlow.f90:169
+
+The functions of the same names below take a :class:`Context` (the device
+resident replacement of the module globals) and keep the argument meaning,
+flag values and in/out behaviour: assembly overwrites the LHS/RHS of the
+fields it assembles, GMRES accumulates into ``sol``.  Everything runs in the
+CUDA library (``_lib/libovs_b200.so``); there is no CPU path.
+"""
+from __future__ import annotations
+
+import ctypes as C
+
+import numpy as np
+
+from . import _ffi as F
+from .mesh import Case, Mesh, to_ovs_params
+
+ASSEMBLE_FIELD_NS, ASSEMBLE_FIELD_VOF, ASSEMBLE_FIELD_TEM = 1, 2, 4
+ASSEMBLE_TENSOR_VEC, ASSEMBLE_TENSOR_MAT = F.OVS_TENSOR_VEC, F.OVS_TENSOR_MAT
+
+_dp = C.POINTER(C.c_double)
+_ip = C.POINTER(C.c_int)
+
+
+def _dptr(a: np.ndarray):
+    return a.ctypes.data_as(_dp)
+
+
+def _iptr(a: np.ndarray):
+    return a.ctypes.data_as(_ip)
+
+
+def _f64(a) -> np.ndarray:
+    return np.asfortranarray(a, dtype=np.float64)
+
+
+def _i32(a) -> np.ndarray:
+    return np.asfortranarray(a, dtype=np.int32)
+
+
+NF = {F.OVS_SYS_NS: 4, F.OVS_SYS_NSVOF: 5, F.OVS_SYS_TEM: 1}
+BLOCK_W = {F.OVS_BLK_K11: 9, F.OVS_BLK_G: 3, F.OVS_BLK_D1: 3, F.OVS_BLK_M: 1, F.OVS_BLK_LS: 1,
+           F.OVS_BLK_LSU: 3, F.OVS_BLK_ULS: 3, F.OVS_BLK_PLS: 1, F.OVS_BLK_TEM: 1}
+BLOCK_NAME = {F.OVS_BLK_K11: "K11", F.OVS_BLK_G: "G", F.OVS_BLK_D1: "D1", F.OVS_BLK_M: "M",
+              F.OVS_BLK_LS: "LS", F.OVS_BLK_LSU: "LSU", F.OVS_BLK_ULS: "ULS", F.OVS_BLK_PLS: "PLS",
+              F.OVS_BLK_TEM: "TEM"}
+SYS_BLOCKS = {F.OVS_SYS_NS: [F.OVS_BLK_K11, F.OVS_BLK_G, F.OVS_BLK_D1, F.OVS_BLK_M],
+              F.OVS_SYS_NSVOF: [F.OVS_BLK_K11, F.OVS_BLK_G, F.OVS_BLK_D1, F.OVS_BLK_M, F.OVS_BLK_LS,
+                                F.OVS_BLK_LSU, F.OVS_BLK_ULS, F.OVS_BLK_PLS],
+              F.OVS_SYS_TEM: [F.OVS_BLK_TEM]}
+
+
+class Context:
+    """Device-resident mesh, pattern, state and assembled systems (one CUDA
+    stream).  Wraps ``ovs_ctx`` of include/ovs.h."""
+
+    def __init__(self, nnode: int, nelem: int, nshl: int = 4, device: int = -1):
+        self.lib = F.load()
+        self.N, self.E, self.nshl = int(nnode), int(nelem), int(nshl)
+        self.h = C.c_void_p()
+        d = F.OvsDims(self.N, self.E, self.nshl, int(device))
+        F.check(self.lib.ovs_create(C.byref(self.h), C.byref(d)), "ovs_create")
+        self.icnt = 0
+        self.last_status = 0
+
+    # ------------------------------------------------------------ lifecycle
+    def close(self):
+        if self.h:
+            self.lib.ovs_destroy(self.h)
+            self.h = C.c_void_p()
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    @classmethod
+    def from_case(cls, case: Case, build: bool = True, device: int = -1) -> "Context":
+        m = case.mesh
+        ctx = cls(m.nnode, m.nelem, m.nshl, device)
+        ctx.upload_mesh(m)
+        if build:
+            ctx.build_pattern()
+        ctx.set_params(case.params)
+        ctx.set_ibc(case.ibc)
+        ctx.set_state(case.state)
+        return ctx
+
+    # ----------------------------------------------------------------- mesh
+    def upload_mesh(self, m: Mesh):
+        self._xg = _f64(m.xg)
+        ien = _i32(m.ien)
+        elm = np.ascontiguousarray(m.elm_id, dtype=np.int32)
+        F.check(self.lib.ovs_upload_mesh(self.h, _dptr(self._xg), _iptr(ien), _iptr(elm)),
+                "ovs_upload_mesh")
+        self.xg = self._xg
+
+    def build_pattern(self) -> int:
+        icnt = C.c_int(0)
+        F.check(self.lib.ovs_build_pattern(self.h, C.byref(icnt)), "ovs_build_pattern")
+        self.icnt = icnt.value
+        return self.icnt
+
+    def get_pattern(self):
+        col = np.zeros(self.N + 1, dtype=np.int32)
+        row = np.zeros(max(self.icnt, 1), dtype=np.int32)
+        F.check(self.lib.ovs_get_pattern(self.h, _iptr(col), _iptr(row)), "ovs_get_pattern")
+        return col, row[: self.icnt]
+
+    # ---------------------------------------------------------- parameters
+    def set_params(self, p: dict):
+        self.params = dict(p)
+        op = to_ovs_params(p)
+        F.check(self.lib.ovs_set_params(self.h, C.byref(op)), "ovs_set_params")
+
+    def set_ibc(self, ibc: np.ndarray):
+        a = _i32(ibc)
+        F.check(self.lib.ovs_set_ibc(self.h, _iptr(a), a.shape[1]), "ovs_set_ibc")
+
+    def set_field(self, name: str, arr: np.ndarray):
+        a = _f64(arr)
+        F.check(self.lib.ovs_set_field(self.h, F.FIELD_ID[name], _dptr(a)), f"ovs_set_field({name})")
+
+    def get_field(self, name: str) -> np.ndarray:
+        shape = (self.N, 3) if F.FIELD_WIDTH[name] == 3 else (self.N,)
+        a = np.zeros(shape, order="F")
+        F.check(self.lib.ovs_get_field(self.h, F.FIELD_ID[name], _dptr(a)), f"ovs_get_field({name})")
+        return a
+
+    def set_state(self, st: dict):
+        for n, v in st.items():
+            if n != "xg":
+                self.set_field(n, v)
+
+    # ------------------------------------------------------------- assembly
+    def assemble(self, kernel: int, tensor_flag: int, precision: int = F.OVS_FP64) -> float:
+        cfl = C.c_double(0.0)
+        st = self.lib.ovs_assemble(self.h, kernel, tensor_flag, precision, C.byref(cfl))
+        self.last_status = F.check(st, "ovs_assemble")
+        return cfl.value
+
+    def get_rhs(self, system: int, precision: int = F.OVS_FP64) -> np.ndarray:
+        a = np.zeros((self.N, NF[system]), order="F")
+        F.check(self.lib.ovs_get_rhs(self.h, system, precision, _dptr(a)), "ovs_get_rhs")
+        return a
+
+    def set_rhs(self, system: int, precision: int, rhs: np.ndarray):
+        a = _f64(np.reshape(rhs, (self.N, NF[system]), order="F"))
+        F.check(self.lib.ovs_set_rhs(self.h, system, precision, _dptr(a)), "ovs_set_rhs")
+
+    def get_lhs(self, system: int, precision: int, block: int) -> np.ndarray:
+        w = BLOCK_W[block]
+        a = np.zeros((self.icnt, w))
+        F.check(self.lib.ovs_get_lhs_block(self.h, system, precision, block, _dptr(a)),
+                "ovs_get_lhs_block")
+        return a if w > 1 else a[:, 0]
+
+    def set_lhs(self, system: int, precision: int, block: int, vals: np.ndarray):
+        w = BLOCK_W[block]
+        a = np.ascontiguousarray(np.reshape(vals, (self.icnt, w)), dtype=np.float64)
+        F.check(self.lib.ovs_set_lhs_block(self.h, system, precision, block, _dptr(a)),
+                "ovs_set_lhs_block")
+
+    def get_system(self, system: int, precision: int = F.OVS_FP64) -> dict:
+        out = {BLOCK_NAME[b]: self.get_lhs(system, precision, b) for b in SYS_BLOCKS[system]}
+        out["rhs"] = self.get_rhs(system, precision)
+        return out
+
+    def set_system(self, system: int, precision: int, blocks: dict, rhs: np.ndarray):
+        for b in SYS_BLOCKS[system]:
+            self.set_lhs(system, precision, b, blocks[BLOCK_NAME[b]])
+        self.set_rhs(system, precision, rhs)
+
+    # ---------------------------------------------------------------- solve
+    def spmv(self, system: int, precision: int, x: np.ndarray) -> np.ndarray:
+        xa = _f64(np.reshape(x, (self.N, NF[system]), order="F"))
+        y = np.zeros_like(xa, order="F")
+        F.check(self.lib.ovs_spmv(self.h, system, precision, _dptr(xa), _dptr(y)), "ovs_spmv")
+        return y
+
+    def gmres(self, system: int, tol: float, kspace: int, kspace_min: int, sol: np.ndarray):
+        s = _f64(np.reshape(sol, (self.N, NF[system]), order="F")).copy(order="F")
+        info = F.OvsGmresInfo()
+        F.check(self.lib.ovs_gmres(self.h, system, tol, kspace, kspace_min, _dptr(s), C.byref(info)),
+                "ovs_gmres")
+        return s, info
+
+    def solve(self, system: int, mode: int, rtol: float, kspace: int = 50, max_cycles: int = 100,
+              want_solution: bool = True):
+        info = F.OvsSolveInfo()
+        s = np.zeros((self.N, NF[system]), order="F") if want_solution else None
+        F.check(self.lib.ovs_solve(self.h, system, mode, rtol, kspace, max_cycles,
+                                   _dptr(s) if s is not None else None, C.byref(info)), "ovs_solve")
+        return s, info
+
+    def newton_update(self, system: int):
+        F.check(self.lib.ovs_newton_update(self.h, system), "ovs_newton_update")
+
+    def residual_norms(self, precision: int = F.OVS_FP64) -> np.ndarray:
+        r = np.zeros(4)
+        F.check(self.lib.ovs_residual_norms(self.h, precision, _dptr(r)), "ovs_residual_norms")
+        return r
+
+    def synchronize(self):
+        F.check(self.lib.ovs_synchronize(self.h), "ovs_synchronize")
+
+    # ---------------------------------------------------------- measurement
+    def profile(self, what: int, system: int, precision: int, reps: int = 10) -> float:
+        """Average device ms of one internal kernel (see ovs_profile)."""
+        ms = C.c_double(0.0)
+        F.check(self.lib.ovs_profile(self.h, what, system, precision, reps, C.byref(ms)), "ovs_profile")
+        return ms.value
+
+    def launch_count(self) -> int:
+        n = C.c_longlong(0)
+        F.check(self.lib.ovs_launch_count(self.h, C.byref(n)), "ovs_launch_count")
+        return n.value
+
+    def last_device_ms(self) -> float:
+        ms = C.c_double(0.0)
+        F.check(self.lib.ovs_last_device_ms(self.h, C.byref(ms)), "ovs_last_device_ms")
+        return ms.value
+
+
+class PinnedArray:
+    """numpy view of a page-locked host buffer (ovs_host_alloc)."""
+
+    def __init__(self, shape, dtype=np.float64, order="F"):
+        self.lib = F.load()
+        dt = np.dtype(dtype)
+        n = int(np.prod(shape)) * dt.itemsize
+        self.ptr = C.c_void_p()
+        F.check(self.lib.ovs_host_alloc(C.byref(self.ptr), n), "ovs_host_alloc")
+        buf = (C.c_char * n).from_address(self.ptr.value)
+        self.array = np.ndarray(shape, dtype=dt, buffer=buf, order=order)
+
+    def free(self):
+        if self.ptr:
+            self.array = None
+            self.lib.ovs_host_free(self.ptr)
+            self.ptr = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.free()
+        except Exception:
+            pass
+
+
+# --------------------------------------------------- reference-named routines
+def genSparStruc(ien: np.ndarray, nnode: int):
+    """CSR pattern of IEN(E,nshl) (1-based): returns (col(N+1), row(icnt)),
+    col = row pointer, row = column indices, 1-based, rows ascending
+    (src/genSparStruc.f90:4-47)."""
+    lib = F.load()
+    ien = _i32(ien)
+    E, nshl = ien.shape
+    col = np.zeros(nnode + 1, dtype=np.int32)
+    icnt = C.c_int(0)
+    F.check(lib.ovs_gen_spar_struc(nnode, E, nshl, _iptr(ien), _iptr(col), None, C.byref(icnt)),
+            "genSparStruc")
+    row = np.zeros(max(icnt.value, 1), dtype=np.int32)
+    F.check(lib.ovs_gen_spar_struc(nnode, E, nshl, _iptr(ien), _iptr(col), _iptr(row),
+                                   C.byref(icnt)), "genSparStruc")
+    return col, row[: icnt.value]
+
+
+def assembleNavSto(ctx: Context, assemble_tensor_flag: int, precision: int = F.OVS_FP64) -> float:
+    """src/assembleNavSto.f90:4-72 (NS-only; the subdomain flag lives in the
+    parameters).  Returns the CFL number the reference prints."""
+    return ctx.assemble(F.OVS_ASM_NS, assemble_tensor_flag, precision)
+
+
+def assembleQuenching(ctx: Context, assemble_tensor_flag: int, assemble_field_flag: int,
+                      precision: int = F.OVS_FP64) -> float:
+    """src/solveQuenching.f90:4-117: NS+VOF when NS or VOF is flagged, then
+    the temperature pass when TEM is flagged."""
+    cfl = 0.0
+    if assemble_field_flag & (ASSEMBLE_FIELD_NS | ASSEMBLE_FIELD_VOF):
+        cfl = ctx.assemble(F.OVS_ASM_NSVOF, assemble_tensor_flag, precision)
+    if assemble_field_flag & ASSEMBLE_FIELD_TEM:
+        c2 = ctx.assemble(F.OVS_ASM_TEM, assemble_tensor_flag, precision)
+        if not assemble_field_flag & (ASSEMBLE_FIELD_NS | ASSEMBLE_FIELD_VOF):
+            cfl = c2
+    return cfl
+
+
+def SparseGMRES_up(ctx: Context, Utol: float, Kspaceu: int, Kspaceu_mn: int,
+                   solu: np.ndarray, solp: np.ndarray):
+    """src/SparseGMRES_NS.f90:4-369 on the resident FP64 (u,p) system; solu
+    (N,3) and solp (N) are accumulated into and returned with the info."""
+    sol = np.concatenate([_f64(solu).reshape(-1, 3, order="F"), _f64(solp).reshape(-1, 1)], axis=1)
+    s, info = ctx.gmres(F.OVS_SYS_NS, Utol, Kspaceu, Kspaceu_mn, sol)
+    return np.asfortranarray(s[:, :3]), s[:, 3].copy(), info
+
+
+def SparseGMRES_ns_conv(ctx: Context, Utol: float, Kspaceu: int, Kspaceu_mn: int,
+                        solu: np.ndarray, solp: np.ndarray, solls: np.ndarray):
+    """src/SparseGMRES_NS_conv.f:1-406 on the resident FP64 (u,p,phi) system."""
+    sol = np.concatenate([_f64(solu).reshape(-1, 3, order="F"), _f64(solp).reshape(-1, 1),
+                          _f64(solls).reshape(-1, 1)], axis=1)
+    s, info = ctx.gmres(F.OVS_SYS_NSVOF, Utol, Kspaceu, Kspaceu_mn, sol)
+    return np.asfortranarray(s[:, :3]), s[:, 3].copy(), s[:, 4].copy(), info
+
+
+def SparseGMRES_tem(ctx: Context, Utol: float, Kspaceu: int, Kspaceu_mn: int, sol: np.ndarray):
+    """src/SparseGMRES_tem.f90:1-256 on the resident FP64 temperature system."""
+    s, info = ctx.gmres(F.OVS_SYS_TEM, Utol, Kspaceu, Kspaceu_mn, _f64(sol).reshape(-1, 1))
+    return s[:, 0].copy(), info
+
+
+def calculate_residual(ctx: Context, precision: int = F.OVS_FP64) -> np.ndarray:
+    """src/solveFlow.f90:169-187: sums of squares (no square root) of the
+    momentum, continuity, VOF and temperature residuals."""
+    return ctx.residual_norms(precision)

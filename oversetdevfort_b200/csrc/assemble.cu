@@ -1,0 +1,956 @@
+// Element assembly into the node-block CSR system (sm_100a).
+//
+// Replaces the element loops of
+//   IntElmAss_NS_overset            src/assembleNavSto.f90:76-336 (+e3LHS/e3RHS)
+//   IntElmAss_NSVOF_Quenching_STAB  src/solveQuenching.f90:122-573
+//   IntElmAss_Tem_Quenching_STAB    src/solveQuenching.f90:579-882
+// together with the element Dirichlet treatment (BCLhs_3D / BCLhs_NS_conv /
+// BCLhs_tem, src/BCLhs_3D.f90) and the scatter (FillSparseMat_*,
+// LocaltoGlobalNSVOF_3D).
+//
+// Scheme (row owner, deterministic, atomic-free):
+//   * one warp owns one CSR row, i.e. one node A;
+//   * phase 1: lane l takes the l-th element of A's element list (sorted by
+//     element id) and evaluates A's row of that element's matrix, i.e. the
+//     nshl node-pair blocks (A, b), plus A's residual entries, from the
+//     gathered node records; results go to shared memory;
+//   * phase 2: the warp adds the element rows into a shared accumulator of
+//     A's CSR slots, element by element in ascending element id, so every
+//     slot is summed in the same order on every run;
+//   * the Dirichlet treatment of the reference zeroes element rows/columns
+//     and puts 1 on the element diagonal; both commute with the sum, so they
+//     are applied once at the row write: masked entries are 0, a constrained
+//     diagonal entry equals the number of elements around A;
+//   * the row (contiguous in the CSR value array) is written with vector
+//     stores.
+// Gauss-point physics is recomputed by each of the element's nshl rows
+// instead of being staged through HBM.
+#include "ovs_internal.cuh"
+
+#include <math.h>
+
+namespace {
+
+// ------------------------------------------------------------------ params
+struct AsmArgs {
+  const void* rec;        // alpha-stage node records, REC values per node
+  const int* ien;         // E*nshl element-major, 0-based
+  const int* elm_id;      // E
+  const uint8_t* ibc;     // N
+  const int* rowptr;
+  const int* colidx;
+  const int* n2e_ptr;
+  const int* n2e;
+  void* vals;             // nnz*NV
+  void* rhs;              // NF*N field-major
+  int* flags;             // [0] non-positive DetJ count, [1] non-finite residual
+  unsigned long long* cfl_bits;
+  int N;
+  int mat, vec;
+  int max_deg;
+  ovs_params p;
+};
+
+// value position tables of the internal slot layout (24 values per slot):
+//   0..3  K(1,1) K(1,2) K(1,3) G(1)     row u1
+//   4..7  K(2,1) K(2,2) K(2,3) G(2)     row u2
+//   8..11 K(3,1) K(3,2) K(3,3) G(3)     row u3
+//  12..15 D(1)   D(2)   D(3)   M        row p
+//  16..19 LSU(1) LSU(2) LSU(3) LS       row phi
+//  20..23 ULS(1) ULS(2) ULS(3) PLS      column phi
+// The NS system keeps the first 16, the temperature system one value.
+// IBC bit d <=> IBC(:, d+1) == 1: bits 0-2 velocity, 3 pressure, 4 VOF, 5 T.
+// rowbits: A-side constraints that zero the entry (element row zeroing),
+// colbits: B-side constraints (element column zeroing), diagbit: the entry
+// set to 1 on the element diagonal.  Row/column rules follow BCLhs_3D
+// (src/BCLhs_3D.f90:18-120) and BCLhs_NS_conv (:295-424) with the pressure at
+// IBC column 4 and VOF at column 5; note M is only row-zeroed, ULS only
+// column-zeroed, and LSU(i) is also zeroed by the u_i constraint of the ROW
+// node (BCLhs_NS_conv :313,:345,:377).
+constexpr uint8_t U0 = 1, U1 = 2, U2 = 4, PB = 8, FB = 16, TB = 32;
+__constant__ uint8_t c_rowbits[24] = {U0, U0, U0, U0, U1, U1, U1, U1, U2, U2, U2, U2,
+                                      PB, PB, PB, PB, FB | U0, FB | U1, FB | U2, FB, 0, 0, 0, PB};
+__constant__ uint8_t c_colbits[24] = {U0, U1, U2, PB, U0, U1, U2, PB, U0, U1, U2, PB,
+                                      U0, U1, U2, 0, U0, U1, U2, FB, FB, FB, FB, FB};
+__constant__ uint8_t c_diagbit[24] = {U0, 0, 0, 0, 0, U1, 0, 0, 0, 0, U2, 0,
+                                      0, 0, 0, PB, 0, 0, 0, FB, 0, 0, 0, 0};
+
+// tet 4-point rule (src/genGP_GW.f90:332-353); N = (xi, eta, zeta, 1-xi-eta-zeta)
+template <typename T>
+__device__ __forceinline__ void tet_shape(int g, T N[4]) {
+  const T a = (T)0.5854101966249685, b = (T)0.1381966011250105;
+  T xi = (g == 0) ? a : b, eta = (g == 1) ? a : b, ze = (g == 2) ? a : b;
+  N[0] = xi; N[1] = eta; N[2] = ze;
+  N[3] = (T)1.0 - xi - eta - ze;
+}
+
+// VOF field at tet Gauss point g in FP64 from the record value (slot k)
+// plus its rounding remainder (lo[.][3]): sum_a N_a phi_a, in node order
+template <typename T>
+__device__ __forceinline__ double gp_phi(const T r[4][16], const T lo[4][4], int k, int g) {
+  const double a = 0.5854101966249685, b = 0.1381966011250105;
+  const double xi = (g == 0) ? a : b, eta = (g == 1) ? a : b, ze = (g == 2) ? a : b;
+  const double N[4] = {xi, eta, ze, 1.0 - xi - eta - ze};
+  double s = 0.0;
+#pragma unroll
+  for (int n = 0; n < 4; ++n) s += ((double)r[n][k] + (double)lo[n][3]) * N[n];
+  return s;
+}
+
+// store NV (multiple of 4) register values to 16-byte aligned shared memory
+template <int NV>
+__device__ __forceinline__ void store_row(float* dst, const float* v) {
+#pragma unroll
+  for (int k = 0; k < NV; k += 4)
+    *reinterpret_cast<float4*>(dst + k) = make_float4(v[k], v[k + 1], v[k + 2], v[k + 3]);
+}
+template <int NV>
+__device__ __forceinline__ void store_row(double* dst, const double* v) {
+#pragma unroll
+  for (int k = 0; k < NV; k += 2)
+    *reinterpret_cast<double2*>(dst + k) = make_double2(v[k], v[k + 1]);
+}
+
+template <typename T>
+__device__ __forceinline__ T pick4(const T v[4], int i) {
+  return i == 0 ? v[0] : (i == 1 ? v[1] : (i == 2 ? v[2] : v[3]));
+}
+
+// Node records: REC = 20 values per node.  0-2: x+d (rounded to T),
+// 3-15: the fields of the pass, 16-18: the rounding remainder of x+d, 19:
+// the rounding remainder of the VOF field.  With the remainders, edge
+// vectors x_j - x_k keep full T accuracy on fine meshes far from the origin,
+// and the VOF value that blends properties 1000:1 is exact to FP64 (in FP64
+// the remainders are 0).
+constexpr int REC = 20;
+__device__ __forceinline__ void load_rec(const float* rec, int node, float r[16], float lo[4]) {
+  const float4* p = reinterpret_cast<const float4*>(rec) + (size_t)node * 5;
+#pragma unroll
+  for (int k = 0; k < 4; ++k) {
+    float4 v = __ldg(p + k);
+    r[4 * k] = v.x; r[4 * k + 1] = v.y; r[4 * k + 2] = v.z; r[4 * k + 3] = v.w;
+  }
+  float4 v = __ldg(p + 4);
+  lo[0] = v.x; lo[1] = v.y; lo[2] = v.z; lo[3] = v.w;
+}
+__device__ __forceinline__ void load_rec(const double* rec, int node, double r[16], double lo[4]) {
+  const double2* p = reinterpret_cast<const double2*>(rec) + (size_t)node * 10;
+#pragma unroll
+  for (int k = 0; k < 8; ++k) {
+    double2 v = __ldg(p + k);
+    r[2 * k] = v.x; r[2 * k + 1] = v.y;
+  }
+  double2 v0 = __ldg(p + 8), v1 = __ldg(p + 9);
+  lo[0] = v0.x; lo[1] = v0.y; lo[2] = v1.x; lo[3] = v1.y;
+}
+
+// Geometry of a linear tet on the current configuration x+d
+// (eval_shape_fem, src/eval_shape_FEM.f90:4-61, with get_inverse_3x3,
+// src/eval_shape.f90:85-112).  xd[a][i] = x+d of node a.  The Jacobian of a
+// linear tet is the same at every Gauss point, so it is evaluated once.
+template <typename T>
+__device__ __forceinline__ T tet_geometry(const T xd[4][3], const T lo[4][4], T g[4][3], T G[3][3]) {
+  T A[3][3], Ai[3][3];
+#pragma unroll
+  for (int i = 0; i < 3; ++i)
+#pragma unroll
+    for (int j = 0; j < 3; ++j) A[i][j] = (xd[j][i] - xd[3][i]) + (lo[j][i] - lo[3][i]);
+  Ai[0][0] = A[1][1] * A[2][2] - A[2][1] * A[1][2];
+  Ai[0][1] = A[2][1] * A[0][2] - A[0][1] * A[2][2];
+  Ai[0][2] = A[0][1] * A[1][2] - A[0][2] * A[1][1];
+  T tmp = (T)1.0 / (Ai[0][0] * A[0][0] + Ai[0][1] * A[1][0] + Ai[0][2] * A[2][0]);
+  Ai[0][0] *= tmp; Ai[0][1] *= tmp; Ai[0][2] *= tmp;
+  Ai[1][0] = (A[1][2] * A[2][0] - A[1][0] * A[2][2]) * tmp;
+  Ai[1][1] = (A[0][0] * A[2][2] - A[2][0] * A[0][2]) * tmp;
+  Ai[1][2] = (A[1][0] * A[0][2] - A[0][0] * A[1][2]) * tmp;
+  Ai[2][0] = (A[1][0] * A[2][1] - A[1][1] * A[2][0]) * tmp;
+  Ai[2][1] = (A[2][0] * A[0][1] - A[0][0] * A[2][1]) * tmp;
+  Ai[2][2] = (A[0][0] * A[1][1] - A[0][1] * A[1][0]) * tmp;
+#pragma unroll
+  for (int j = 0; j < 3; ++j) {
+    g[0][j] = Ai[0][j]; g[1][j] = Ai[1][j]; g[2][j] = Ai[2][j];
+    g[3][j] = (-Ai[0][j] - Ai[1][j]) - Ai[2][j];
+  }
+#pragma unroll
+  for (int i = 0; i < 3; ++i)
+#pragma unroll
+    for (int j = 0; j < 3; ++j)
+      G[i][j] = Ai[0][i] * Ai[0][j] + Ai[1][i] * Ai[1][j] + Ai[2][i] * Ai[2][j];
+  return (T)1.0 / tmp;
+}
+
+template <typename T>
+__device__ __forceinline__ T quad_uGu(const T u[3], const T G[3][3]) {
+  T t = 0;
+#pragma unroll
+  for (int j = 0; j < 3; ++j)
+#pragma unroll
+    for (int i = 0; i < 3; ++i) t += u[i] * G[i][j] * u[j];
+  return t;
+}
+
+// e3DC_beta2's INTEGER dummy receiving a real(8) (src/e3STAB.f90:175-189):
+// the callee reads the low 4 bytes of the double.
+__device__ __forceinline__ int low_word(double v) {
+  return (int)(unsigned)(__double_as_longlong(v) & 0xffffffffULL);
+}
+
+__device__ __forceinline__ void cfl_max(unsigned long long* bits, double v) {
+  if (v >= 0.0) atomicMax(bits, (unsigned long long)__double_as_longlong(v));
+}
+
+// ----------------------------------------------------- per-kind physics
+// Each kind fills, for lane element (with row-local index la):
+//   blk[b*NVP + v]  v < NV : A's row block with column node b
+//   rv[f]           f < NF : A's residual entries
+// returns DetJ.
+template <typename T, int KIND> struct Phys;
+
+// NS-only, IntElmAss_NS_overset + e3LHS_3D_fluid_Old + e3Rhs_3D_fluid.
+// Quirks kept: uprime = 0 (shhessgu passed for uprime), kap_dc = NS_kdc_a,
+// tauBar = 0, rho = rhoa, mu = mua.
+template <typename T> struct Phys<T, OVS_ASM_NS> {
+  static constexpr int NV = 16, NF = 4;
+  __device__ static T eval(const AsmArgs& a, int e, int la, const T r[4][16], const T lo[4][4], bool target,
+                           T* blk, int nvp, T* rv, double& cfl) {
+    const ovs_params& p = a.p;
+    T xd[4][3], g[4][3], G[3][3];
+#pragma unroll
+    for (int n = 0; n < 4; ++n)
+#pragma unroll
+      for (int i = 0; i < 3; ++i) xd[n][i] = r[n][i];
+    const T detj = tet_geometry<T>(xd, lo, g, G);
+    const T w = detj * (T)(0.25 / 6.0);
+    T GG = 0;
+#pragma unroll
+    for (int j = 0; j < 3; ++j)
+#pragma unroll
+      for (int i = 0; i < 3; ++i) GG += G[i][j] * G[i][j];
+    const T trG = G[0][0] + G[1][1] + G[2][2];
+    T du[3][3], dp[3];
+#pragma unroll
+    for (int i = 0; i < 3; ++i)
+#pragma unroll
+      for (int j = 0; j < 3; ++j)
+        du[i][j] = r[0][3 + i] * g[0][j] + r[1][3 + i] * g[1][j] + r[2][3 + i] * g[2][j] + r[3][3 + i] * g[3][j];
+#pragma unroll
+    for (int j = 0; j < 3; ++j) dp[j] = r[0][12] * g[0][j] + r[1][12] * g[1][j] + r[2][12] * g[2][j] + r[3][12] * g[3][j];
+    const T divu = du[0][0] + du[1][1] + du[2][2];
+    const T rho = (T)p.rhoa, mu = (T)p.mua, mupkdc = mu + (T)p.ns_kdc_a;
+    const T fact1 = (T)p.almi, fact2 = (T)(p.alfi * p.gami * p.delt);
+    const T taut = (T)(4.0 / (p.delt * p.delt));
+    const T ga[3] = {la == 0 ? g[0][0] : la == 1 ? g[1][0] : la == 2 ? g[2][0] : g[3][0],
+                     la == 0 ? g[0][1] : la == 1 ? g[1][1] : la == 2 ? g[2][1] : g[3][1],
+                     la == 0 ? g[0][2] : la == 1 ? g[1][2] : la == 2 ? g[2][2] : g[3][2]};
+    T gab[4];
+#pragma unroll
+    for (int b = 0; b < 4; ++b) gab[b] = ga[0] * g[b][0] + ga[1] * g[b][1] + ga[2] * g[b][2];
+    // factored Gauss-point sums (see the block formulas below)
+    T KA = 0, KB = 0, Q = 0, R = 0, MM = 0;
+    T Pb[4] = {0, 0, 0, 0}, Tb[4] = {0, 0, 0, 0}, Sb[4] = {0, 0, 0, 0};
+    T ru[3] = {0, 0, 0}, rp = 0;
+    // A's residual gradient term: sum_j ga_j tmp2_ij, tmp2 = -ptot I + mupkdc (du + du^T)
+    T sym[3];
+#pragma unroll
+    for (int i = 0; i < 3; ++i)
+      sym[i] = mupkdc * (ga[0] * (du[i][0] + du[0][i]) + ga[1] * (du[i][1] + du[1][i]) + ga[2] * (du[i][2] + du[2][i]));
+#pragma unroll
+    for (int gp = 0; gp < 4; ++gp) {
+      T N[4];
+      tet_shape<T>(gp, N);
+      T ui[3], umi[3], aci[3], pri;
+#pragma unroll
+      for (int d = 0; d < 3; ++d) {
+        ui[d] = r[0][3 + d] * N[0] + r[1][3 + d] * N[1] + r[2][3 + d] * N[2] + r[3][3 + d] * N[3];
+        umi[d] = r[0][6 + d] * N[0] + r[1][6 + d] * N[1] + r[2][6 + d] * N[2] + r[3][6 + d] * N[3];
+        aci[d] = r[0][9 + d] * N[0] + r[1][9 + d] * N[1] + r[2][9 + d] * N[2] + r[3][9 + d] * N[3];
+      }
+      pri = r[0][12] * N[0] + r[1][12] * N[1] + r[2][12] * N[2] + r[3][12] * N[3];
+      T uadv[3] = {ui[0] - umi[0], ui[1] - umi[1], ui[2] - umi[2]};
+      const T taua = quad_uGu<T>(uadv, G);
+      const T nu = mu / rho;
+      const T taud = nu * nu * (T)12.0 * GG;
+      const T tauM = (T)1.0 / (rho * sqrt(taut + taua + taud));
+      const T tauC = rho * sqrt(taua + taud) / trG;
+      {
+        double c = (double)p.delt * sqrt((double)taua);
+        if (c > cfl) cfl = c;
+      }
+      T c[4];
+#pragma unroll
+      for (int b = 0; b < 4; ++b) c[b] = uadv[0] * g[b][0] + uadv[1] * g[b][1] + uadv[2] * g[b][2];
+      const T Na = pick4<T>(N, la), ca = pick4<T>(c, la);
+      if (target) {
+        // tmp4 = rho (Na + rho tauM ca)(fact1 Nb + fact2 cb) + fact2 mupkdc gab
+        const T alpha = w * rho * (Na + rho * tauM * ca);
+        KA += fact2 * mupkdc * w;
+        KB += fact2 * tauC * w;
+        Q += fact2 * w * rho * tauM * ca;
+        R += fact2 * w * Na;
+        MM += fact2 * w * tauM;
+#pragma unroll
+        for (int b = 0; b < 4; ++b) {
+          const T beta = fact1 * N[b] + fact2 * c[b];
+          Sb[b] += alpha * beta;
+          Pb[b] += fact2 * w * N[b];
+          Tb[b] += w * tauM * rho * beta;
+        }
+        // e3Rhs_3D_fluid with uprime = 0
+        const T ptot = pri - tauC * divu;
+#pragma unroll
+        for (int i = 0; i < 3; ++i) {
+          const T tmp1 = rho * (aci[i] + uadv[0] * du[i][0] + uadv[1] * du[i][1] + uadv[2] * du[i][2]) - (T)p.gravvec[i] * rho;
+          ru[i] -= (Na * tmp1 + (sym[i] - ga[i] * ptot)) * w;
+        }
+        rp -= (Na * divu) * w;
+      }
+    }
+#pragma unroll
+    for (int b = 0; b < 4; ++b) {
+      T o[16];
+      const T* gb = g[b];
+      const T dg = KA * gab[b] + Sb[b];
+#pragma unroll
+      for (int i = 0; i < 3; ++i) {
+#pragma unroll
+        for (int j = 0; j < 3; ++j) o[4 * i + j] = KA * ga[j] * gb[i] + KB * ga[i] * gb[j] + (i == j ? dg : (T)0);
+        o[4 * i + 3] = -ga[i] * Pb[b] + gb[i] * Q;
+      }
+#pragma unroll
+      for (int d = 0; d < 3; ++d) o[12 + d] = gb[d] * R + ga[d] * Tb[b];
+      o[15] = MM * gab[b];
+      store_row<16>(blk + b * nvp, o);
+    }
+    rv[0] = ru[0]; rv[1] = ru[1]; rv[2] = ru[2]; rv[3] = rp;
+    return detj;
+  }
+};
+
+// NS+VOF quench element, IntElmAss_NSVOF_Quenching_STAB.
+template <typename T> struct Phys<T, OVS_ASM_NSVOF> {
+  static constexpr int NV = 24, NF = 5;
+  __device__ static T eval(const AsmArgs& a, int e, int la, const T r[4][16], const T lo[4][4], bool fluid,
+                           T* blk, int nvp, T* rv, double& cfl) {
+    const ovs_params& p = a.p;
+    T xd[4][3], g[4][3], G[3][3];
+#pragma unroll
+    for (int n = 0; n < 4; ++n)
+#pragma unroll
+      for (int i = 0; i < 3; ++i) xd[n][i] = r[n][i];
+    const T detj = tet_geometry<T>(xd, lo, g, G);
+    const T w = detj * (T)(0.25 / 6.0);
+    T GG = 0;
+#pragma unroll
+    for (int j = 0; j < 3; ++j)
+#pragma unroll
+      for (int i = 0; i < 3; ++i) GG += G[i][j] * G[i][j];
+    const T trG = G[0][0] + G[1][1] + G[2][2];
+    T du[3][3], dp[3], dphi[3];
+#pragma unroll
+    for (int i = 0; i < 3; ++i)
+#pragma unroll
+      for (int j = 0; j < 3; ++j)
+        du[i][j] = r[0][3 + i] * g[0][j] + r[1][3 + i] * g[1][j] + r[2][3 + i] * g[2][j] + r[3][3 + i] * g[3][j];
+#pragma unroll
+    for (int j = 0; j < 3; ++j) {
+      dp[j] = r[0][12] * g[0][j] + r[1][12] * g[1][j] + r[2][12] * g[2][j] + r[3][12] * g[3][j];
+      dphi[j] = r[0][13] * g[0][j] + r[1][13] * g[1][j] + r[2][13] * g[2][j] + r[3][13] * g[3][j];
+    }
+    const T divu = du[0][0] + du[1][1] + du[2][2];
+    const T fact1 = (T)p.almi, fact2 = (T)(p.alfi * p.delt * p.gami);
+    const T taut = (T)(4.0 / (p.delt * p.delt));
+    const T rhoa = (T)p.rhoa, rhow = (T)p.rhow, ts = (T)p.ts;
+    const T ira = (T)1.0 / rhoa - (T)1.0 / rhow;
+    const T ga[3] = {la == 0 ? g[0][0] : la == 1 ? g[1][0] : la == 2 ? g[2][0] : g[3][0],
+                     la == 0 ? g[0][1] : la == 1 ? g[1][1] : la == 2 ? g[2][1] : g[3][1],
+                     la == 0 ? g[0][2] : la == 1 ? g[1][2] : la == 2 ? g[2][2] : g[3][2]};
+    T gab[4];
+#pragma unroll
+    for (int b = 0; b < 4; ++b) gab[b] = ga[0] * g[b][0] + ga[1] * g[b][1] + ga[2] * g[b][2];
+    // sum_k sum_j ga_j (du(j,k) + du(k,j)): the three viscous RHS scalars that
+    // the reference subtracts from every momentum component (:508-510)
+    T svis = 0;
+#pragma unroll
+    for (int k = 0; k < 3; ++k)
+      svis += ga[0] * (du[0][k] + du[k][0]) + ga[1] * (du[1][k] + du[k][1]) + ga[2] * (du[2][k] + du[k][2]);
+    const T gdphi = ga[0] * dphi[0] + ga[1] * dphi[1] + ga[2] * dphi[2];
+    T KA = 0, KB = 0, Q = 0, R = 0, MM = 0, KDP = 0, W = 0;
+    T Pb[4] = {0, 0, 0, 0}, Tb[4] = {0, 0, 0, 0}, Sb[4] = {0, 0, 0, 0}, L1[4] = {0, 0, 0, 0},
+      Eb[4] = {0, 0, 0, 0}, Ub[4] = {0, 0, 0, 0}, PLb[4] = {0, 0, 0, 0}, Vb[4] = {0, 0, 0, 0};
+    T ru[3] = {0, 0, 0}, rp = 0, rf = 0;
+    const bool kdc_on = fabs(p.ns_kdc_w) + fabs(p.ns_kdc_a) > 0.0;
+    const bool kdcphi_on = fabs(p.lsc_kdc) > 0.0;
+#pragma unroll
+    for (int gp = 0; gp < 4; ++gp) {
+      T N[4];
+      tet_shape<T>(gp, N);
+      T ui[3], umi[3], aci[3];
+#pragma unroll
+      for (int d = 0; d < 3; ++d) {
+        ui[d] = r[0][3 + d] * N[0] + r[1][3 + d] * N[1] + r[2][3 + d] * N[2] + r[3][3 + d] * N[3];
+        umi[d] = r[0][6 + d] * N[0] + r[1][6 + d] * N[1] + r[2][6 + d] * N[2] + r[3][6 + d] * N[3];
+        aci[d] = r[0][9 + d] * N[0] + r[1][9 + d] * N[1] + r[2][9 + d] * N[2] + r[3][9 + d] * N[3];
+      }
+      const T pri = r[0][12] * N[0] + r[1][12] * N[1] + r[2][12] * N[2] + r[3][12] * N[3];
+      const double phid = gp_phi(r, lo, 13, gp);   // VOF in FP64 (property blend)
+      const T phii = (T)phid;
+      const T rphii = r[0][14] * N[0] + r[1][14] * N[1] + r[2][14] * N[2] + r[3][14] * N[3];
+      const T Ti = r[0][15] * N[0] + r[1][15] * N[1] + r[2][15] * N[2] + r[3][15] * N[3];
+      const double phicd = fmax(fmin(phid, 1.0), 0.0);
+      const T phic = (T)phicd;
+      T mdot, dmd;
+      if (Ti > ts) {
+        mdot = (T)p.c_evap * (T)(1.0 - phicd) * rhow * (Ti - ts) / ts;
+        dmd = -(T)p.c_evap * rhow * (Ti - ts) / ts * (T)p.c_dmdot;
+      } else {
+        mdot = (T)p.c_cond * phic * rhoa * (Ti - ts) / ts;
+        dmd = (T)p.c_cond * rhoa * (Ti - ts) / ts * (T)p.c_dmdot;
+      }
+      const T vdot = mdot / rhoa - mdot / rhow;
+      T rho, mu;
+      if (fluid) {
+        rho = (T)(p.rhow * (1.0 - phicd) + p.rhoa * phicd);
+        mu = (T)(p.muw * (1.0 - phicd) + p.mua * phicd);
+      } else {
+        rho = (T)p.rhos; mu = (T)p.mus;
+      }
+      const T lambda = (T)(-2.0 / 3.0) * mu;
+      if (phid < 0.0 || phid > 1.0) dmd = 0;
+      T uadv[3] = {ui[0] - umi[0], ui[1] - umi[1], ui[2] - umi[2]};
+      T tmp1[3], rL[3];
+#pragma unroll
+      for (int i = 0; i < 3; ++i) {
+        const T conv = du[i][0] * uadv[0] + du[i][1] * uadv[1] + du[i][2] * uadv[2];
+        tmp1[i] = rho * aci[i] + rho * conv - (T)p.gravvec[i] * rho;
+        rL[i] = tmp1[i] + dp[i];
+      }
+      const T res_phi = rphii + (uadv[0] * dphi[0] + uadv[1] * dphi[1] + uadv[2] * dphi[2]) + phii * vdot - mdot / rhoa;
+      const T taua = quad_uGu<T>(uadv, G);
+      const T nu = mu / rho;
+      const T taud = nu * nu * (T)12.0 * GG;
+      const T tauM = (T)1.0 / (rho * sqrt(taut + taua + taud));
+      const T tauLS = (T)1.0 / sqrt(taut + taua);
+      const T tauC = rho * sqrt(taua + taud) / trG;
+      {
+        double cf = (double)p.delt * sqrt((double)taua);
+        if (cf > cfl) cfl = cf;
+      }
+      T c[4];
+#pragma unroll
+      for (int b = 0; b < 4; ++b) c[b] = uadv[0] * g[b][0] + uadv[1] * g[b][1] + uadv[2] * g[b][2];
+      T kdc = 0;
+      if (kdc_on) {
+        double pc = phicd;
+        double nk = p.ns_kdc_w * (1.0 - pc) + p.ns_kdc_a * pc;
+        T rr = rL[0] * rL[0] + rL[1] * rL[1] + rL[2] * rL[2];
+        kdc = (T)low_word(nk) * sqrt(rr / GG);
+      }
+      T kdphi = 0;
+      if (kdcphi_on) kdphi = (T)p.lsc_kdc * fabs(res_phi) / sqrt(GG);
+      if (!fluid) continue;
+      const T Na = pick4<T>(N, la), ca = pick4<T>(c, la);
+      const T mupk = mu + kdc;
+      // ---- matrix sums (block formulas after the loop)
+      const T alpha = w * rho * (Na + rho * tauM * ca);
+      const T gam = w * (Na + tauLS * ca);
+      const T dmdi = dmd * ira;
+      const T eps = fact2 * w * tauC * dmdi * dmdi;
+      const T src = vdot + phii * ira * dmd - dmd / rhoa;
+      KA += fact2 * mupk * w;
+      KB += fact2 * (tauC + lambda) * w;
+      Q += fact2 * w * rho * tauM * ca;
+      R += fact2 * w * Na;
+      MM += fact2 * w * tauM;
+      KDP += fact2 * w * kdphi;
+      W += dmdi * fact2 * tauC * w * Na;
+#pragma unroll
+      for (int b = 0; b < 4; ++b) {
+        const T beta = fact1 * N[b] + fact2 * c[b];
+        Sb[b] += alpha * beta;
+        Pb[b] += fact2 * w * N[b];
+        Tb[b] += w * tauM * rho * beta;
+        L1[b] += gam * (beta + fact2 * N[b] * src);
+        Eb[b] += eps * Na * N[b];
+        Ub[b] += fact2 * tauC * dmdi * w * N[b];
+        PLb[b] -= fact2 * dmdi * w * Na * N[b];
+        Vb[b] += fact2 * gam * N[b];
+      }
+      // ---- residual (src/solveQuenching.f90:496-521)
+      const T tdiv = -pri + tauC * divu;
+#pragma unroll
+      for (int i = 0; i < 3; ++i)
+        ru[i] += w * (-Na * tmp1[i] - ga[i] * tdiv + ga[i] * tauC * vdot - ga[i] * lambda * divu - mupk * svis +
+                      rho * ca * (-tauM * rL[i]));
+      rp += w * (-Na * (divu - vdot) + (ga[0] * rL[0] + ga[1] * rL[1] + ga[2] * rL[2]) * (-tauM));
+      rf += w * (-(Na + tauLS * ca) * res_phi - kdphi * gdphi + Na * dmdi * tauC * (divu - vdot));
+    }
+    // ---- blocks of row A:
+    //  K(i,j) = KA ga_j gb_i + KB ga_i gb_j + delta_ij (KA gab + S_b)
+    //  G(i) = -ga_i P_b + gb_i Q        D(i) = gb_i R + ga_i T_b
+    //  M = MM gab   LS = L1_b + KDP gab + E_b   ULS(i) = ga_i U_b
+    //  PLS = PL_b   LSU(i) = dphi_i V_b - gb_i W
+#pragma unroll
+    for (int b = 0; b < 4; ++b) {
+      T o[24];
+      const T* gb = g[b];
+      const T dg = KA * gab[b] + Sb[b];
+#pragma unroll
+      for (int i = 0; i < 3; ++i) {
+#pragma unroll
+        for (int j = 0; j < 3; ++j) o[4 * i + j] = KA * ga[j] * gb[i] + KB * ga[i] * gb[j] + (i == j ? dg : (T)0);
+        o[4 * i + 3] = -ga[i] * Pb[b] + gb[i] * Q;
+      }
+#pragma unroll
+      for (int d = 0; d < 3; ++d) o[12 + d] = gb[d] * R + ga[d] * Tb[b];
+      o[15] = MM * gab[b];
+#pragma unroll
+      for (int d = 0; d < 3; ++d) o[16 + d] = dphi[d] * Vb[b] - gb[d] * W;
+      o[19] = L1[b] + KDP * gab[b] + Eb[b];
+#pragma unroll
+      for (int d = 0; d < 3; ++d) o[20 + d] = ga[d] * Ub[b];
+      o[23] = PLb[b];
+      store_row<24>(blk + b * nvp, o);
+    }
+    rv[0] = ru[0]; rv[1] = ru[1]; rv[2] = ru[2]; rv[3] = rp; rv[4] = rf;
+    return detj;
+  }
+};
+
+// Temperature element, IntElmAss_Tem_Quenching_STAB.  Record layout for
+// this pass: xd(0:2) u(3:5) um(6:8) phi(9) T(10) rT(11).
+template <typename T> struct Phys<T, OVS_ASM_TEM> {
+  static constexpr int NV = 1, NF = 1;
+  __device__ static T eval(const AsmArgs& a, int e, int la, const T r[4][16], const T lo[4][4], bool fluid,
+                           T* blk, int nvp, T* rv, double& cfl) {
+    const ovs_params& p = a.p;
+    T xd[4][3], g[4][3], G[3][3];
+#pragma unroll
+    for (int n = 0; n < 4; ++n)
+#pragma unroll
+      for (int i = 0; i < 3; ++i) xd[n][i] = r[n][i];
+    const T detj = tet_geometry<T>(xd, lo, g, G);
+    const T w = detj * (T)(0.25 / 6.0);
+    T GG = 0;
+#pragma unroll
+    for (int j = 0; j < 3; ++j)
+#pragma unroll
+      for (int i = 0; i < 3; ++i) GG += G[i][j] * G[i][j];
+    T dT[3];
+#pragma unroll
+    for (int j = 0; j < 3; ++j) dT[j] = r[0][10] * g[0][j] + r[1][10] * g[1][j] + r[2][10] * g[2][j] + r[3][10] * g[3][j];
+    const T fact1 = (T)p.almi, fact2 = (T)(p.alfi * p.gami * p.delt);
+    const T ts = (T)p.ts, cpw = (T)p.cpw, cpa = (T)p.cpa, lh = (T)p.lh;
+    const T ga[3] = {la == 0 ? g[0][0] : la == 1 ? g[1][0] : la == 2 ? g[2][0] : g[3][0],
+                     la == 0 ? g[0][1] : la == 1 ? g[1][1] : la == 2 ? g[2][1] : g[3][1],
+                     la == 0 ? g[0][2] : la == 1 ? g[1][2] : la == 2 ? g[2][2] : g[3][2]};
+    T gab[4];
+#pragma unroll
+    for (int b = 0; b < 4; ++b) gab[b] = ga[0] * g[b][0] + ga[1] * g[b][1] + ga[2] * g[b][2];
+    const T gdT = ga[0] * dT[0] + ga[1] * dT[1] + ga[2] * dT[2];
+    T Xb[4] = {0, 0, 0, 0}, HK = 0, rt = 0;
+    const bool kdc_on = fabs(p.tem_kdc) > 0.0;
+#pragma unroll
+    for (int gp = 0; gp < 4; ++gp) {
+      T N[4];
+      tet_shape<T>(gp, N);
+      const double phid = gp_phi(r, lo, 9, gp);
+      const T Ti = r[0][10] * N[0] + r[1][10] * N[1] + r[2][10] * N[2] + r[3][10] * N[3];
+      const T rTi = r[0][11] * N[0] + r[1][11] * N[1] + r[2][11] * N[2] + r[3][11] * N[3];
+      T ui[3], umi[3];
+#pragma unroll
+      for (int d = 0; d < 3; ++d) {
+        ui[d] = r[0][3 + d] * N[0] + r[1][3 + d] * N[1] + r[2][3 + d] * N[2] + r[3][3 + d] * N[3];
+        umi[d] = r[0][6 + d] * N[0] + r[1][6 + d] * N[1] + r[2][6 + d] * N[2] + r[3][6 + d] * N[3];
+      }
+      const double phicd = fmax(fmin(phid, 1.0), 0.0);
+      const T phic = (T)phicd;
+      T mdot, dmdT;
+      if (Ti > ts) {
+        mdot = (T)p.c_evap * (T)(1.0 - phicd) * (T)p.rhow * (Ti - ts) / ts;
+        dmdT = (T)p.c_evap * (T)(1.0 - phicd) * (T)p.rhow / ts * (T)p.c_dmdot;
+      } else {
+        mdot = (T)p.c_cond * phic * (T)p.rhoa * (Ti - ts) / ts;
+        dmdT = (T)p.c_cond * phic * (T)p.rhoa / ts * (T)p.c_dmdot;
+      }
+      T rho, cp, hk, rcp;
+      if (fluid) {
+        rho = (T)(p.rhow * (1.0 - phicd) + p.rhoa * phicd);
+        cp = (T)(p.cpw * (1.0 - phicd) + p.cpa * phicd);
+        hk = (T)(p.kappaw * (1.0 - phicd) + p.kappaa * phicd);
+        rcp = (T)((p.rhow * p.cpw) * (1.0 - phicd) + (p.rhoa * p.cpa) * phicd);
+      } else {
+        rho = (T)p.rhos; cp = (T)p.cps; hk = (T)p.kappas; rcp = (T)(p.rhos * p.cps);
+      }
+      T uadv[3] = {ui[0] - umi[0], ui[1] - umi[1], ui[2] - umi[2]};
+      const T Se = ((cpw - cpa) * (Ti - ts) - lh) * mdot;
+      const T udT = uadv[0] * dT[0] + uadv[1] * dT[1] + uadv[2] * dT[2];
+      const T res = rcp * (rTi + udT) - Se;
+      const T taua = quad_uGu<T>(uadv, G);
+      T tt = taua + (T)(4.0 / (p.delt * p.delt));
+      const T kk = hk / (rho * cp);
+      tt = tt + kk * kk * (T)12.0 * GG;
+      const T tauT = (T)1.0 / (rho * cp * sqrt(tt));
+      {
+        double cf = (double)p.delt * sqrt((double)taua);
+        if (cf > cfl) cfl = cf;
+      }
+      T kdcT = 0;
+      if (kdc_on && fluid) kdcT = (T)p.tem_kdc * fabs(res) / sqrt(GG) / (T)p.tref;
+      T c[4];
+#pragma unroll
+      for (int b = 0; b < 4; ++b) c[b] = g[b][0] * uadv[0] + g[b][1] * uadv[1] + g[b][2] * uadv[2];
+      const T dSe = (cpw - cpa) * mdot + ((cpw - cpa) * (Ti - ts) - lh) * dmdT;
+      const T Na = pick4<T>(N, la), ca = pick4<T>(c, la);
+      if (fluid) {
+        // xTebe(a,b) = sum w (Na + tauT rcp ca)[rcp(fact1 Nb + fact2 cb) - fact2 dSe Nb] + fact2 (hk+kdc) gab w
+        const T aw = w * (Na + tauT * rcp * ca);
+#pragma unroll
+        for (int b = 0; b < 4; ++b) Xb[b] += aw * (rcp * (fact1 * N[b] + fact2 * c[b]) - fact2 * dSe * N[b]);
+        HK += fact2 * (hk + kdcT) * w;
+        rt += w * (-Na * rcp * (rTi + udT) + Na * Se - rcp * tauT * ca * res - (hk + kdcT) * gdT);
+      } else {
+#pragma unroll
+        for (int b = 0; b < 4; ++b) Xb[b] += w * Na * rcp * fact1 * N[b];
+        HK += fact2 * hk * w;
+        rt += w * (-Na * rcp * rTi - hk * gdT);
+      }
+    }
+#pragma unroll
+    for (int b = 0; b < 4; ++b) blk[b * nvp] = Xb[b] + HK * gab[b];
+    rv[0] = rt;
+    return detj;
+  }
+};
+
+template <typename T> struct Vec4 {};
+template <> struct Vec4<float> {
+  __device__ static void add(float* dst, const float* src) {
+    float4 a = *reinterpret_cast<float4*>(dst);
+    float4 b = *reinterpret_cast<const float4*>(src);
+    a.x += b.x; a.y += b.y; a.z += b.z; a.w += b.w;
+    *reinterpret_cast<float4*>(dst) = a;
+  }
+};
+template <> struct Vec4<double> {
+  __device__ static void add(double* dst, const double* src) {
+    double2 a0 = reinterpret_cast<double2*>(dst)[0], a1 = reinterpret_cast<double2*>(dst)[1];
+    double2 b0 = reinterpret_cast<const double2*>(src)[0], b1 = reinterpret_cast<const double2*>(src)[1];
+    a0.x += b0.x; a0.y += b0.y; a1.x += b1.x; a1.y += b1.y;
+    reinterpret_cast<double2*>(dst)[0] = a0;
+    reinterpret_cast<double2*>(dst)[1] = a1;
+  }
+};
+
+// shared-memory layout per warp
+template <typename T, int KIND> struct Smem {
+  static constexpr int NV = Phys<T, KIND>::NV, NF = Phys<T, KIND>::NF;
+  // per-lane stride of the element rows, padded so that 16-byte stores of
+  // the 32 lanes spread over all banks
+  static constexpr int NVP = (NV < 4) ? 1 : NV;
+  static constexpr int LSTR = 4 * NVP + (16 / (int)sizeof(T));
+  static constexpr int RSTR = NF + 1;
+  __host__ __device__ static size_t bytes(int max_deg) {
+    size_t b = sizeof(T) * ((size_t)32 * LSTR + (size_t)32 * RSTR + (size_t)max_deg * NVP);
+    b = (b + 15) & ~(size_t)15;
+    b += sizeof(int) * ((size_t)32 * 4 + max_deg);
+    return (b + 15) & ~(size_t)15;
+  }
+};
+
+// ------------------------------------------------------------ the kernel
+template <typename T, int KIND, int WARPS>
+__global__ void __launch_bounds__(WARPS * 32)
+assemble_rows_kernel(const AsmArgs a) {
+  using P = Phys<T, KIND>;
+  using S = Smem<T, KIND>;
+  constexpr int NV = P::NV, NF = P::NF, NVP = S::NVP, LSTR = S::LSTR, RSTR = S::RSTR;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+  unsigned char* base = smem_raw + (size_t)wid * S::bytes(a.max_deg);
+  T* blk = reinterpret_cast<T*>(base);                 // [32][LSTR]
+  T* rvs = blk + 32 * LSTR;                            // [32][RSTR]
+  T* acc = rvs + 32 * RSTR;                            // [max_deg][NVP]
+  size_t off = sizeof(T) * ((size_t)32 * LSTR + (size_t)32 * RSTR + (size_t)a.max_deg * NVP);
+  off = (off + 15) & ~(size_t)15;
+  int* slot = reinterpret_cast<int*>(base + off);      // [32][4]
+  int* cols = slot + 32 * 4;                           // [max_deg]
+
+  const T* rec = reinterpret_cast<const T*>(a.rec);
+  const int nwarps_total = gridDim.x * WARPS;
+  double cfl = 0.0;
+  int ndet = 0;
+  for (int A = blockIdx.x * WARPS + wid; A < a.N; A += nwarps_total) {
+    const int rp = a.rowptr[A], deg = a.rowptr[A + 1] - rp;
+    const int ep = a.n2e_ptr[A], ne = a.n2e_ptr[A + 1] - ep;
+    for (int s = lane; s < deg; s += 32) cols[s] = a.colidx[rp + s];
+    for (int q = lane; q < deg * NVP; q += 32) acc[q] = (T)0;
+    T racc = (T)0;
+    __syncwarp();
+    for (int c0 = 0; c0 < ne; c0 += 32) {
+      const int nc = min(32, ne - c0);
+      // ---------------- phase 1: lane = element
+      if (lane < nc) {
+        const int packed = a.n2e[ep + c0 + lane];
+        const int e = packed >> 3, la = packed & 7;
+        const int4 nd = reinterpret_cast<const int4*>(a.ien)[e];
+        const int nodes[4] = {nd.x, nd.y, nd.z, nd.w};
+        T r[4][16], lo[4][4];
+#pragma unroll
+        for (int n = 0; n < 4; ++n) load_rec(rec, nodes[n], r[n], lo[n]);
+        const int eid = a.elm_id[e];
+        bool active;
+        if (KIND == OVS_ASM_NS) {
+          active = ((a.p.subdomain_flag & 1) && eid == a.p.elm_id_set[0]) ||
+                   ((a.p.subdomain_flag & 2) && eid == a.p.elm_id_set[1]);
+        } else {
+          active = eid == a.p.fluid_elm_id;
+        }
+        T rv[NF];
+        T* myblk = blk + lane * LSTR;
+        const T detj = P::eval(a, e, la, r, lo, active, myblk, NVP, rv, cfl);
+        if (!(detj > (T)0)) ++ndet;
+#pragma unroll
+        for (int f = 0; f < NF; ++f) rvs[lane * RSTR + f] = rv[f];
+        // slot of each column node in row A (cols is sorted ascending)
+#pragma unroll
+        for (int b = 0; b < 4; ++b) {
+          int lo = 0, hi = deg;
+          while (hi - lo > 1) {
+            int mid = (lo + hi) >> 1;
+            if (cols[mid] > nodes[b]) hi = mid; else lo = mid;
+          }
+          slot[lane * 4 + b] = lo;
+        }
+      }
+      __syncwarp();
+      // ---------------- phase 2: ordered segmented reduction into acc
+      if constexpr (NV >= 4) {
+        constexpr int NG = NV / 4;             // 4-value groups per block
+        for (int j = 0; j < nc; ++j) {
+          for (int q = lane; q < 4 * NG; q += 32) {
+            const int b = q / NG, gidx = q - b * NG;
+            const int s = slot[j * 4 + b];
+            Vec4<T>::add(acc + s * NVP + gidx * 4, blk + j * LSTR + b * NVP + gidx * 4);
+          }
+          __syncwarp();
+        }
+      } else {
+        if (lane == 0)
+          for (int j = 0; j < nc; ++j)
+#pragma unroll
+            for (int b = 0; b < 4; ++b) acc[slot[j * 4 + b]] += blk[j * LSTR + b];
+      }
+      if (lane < NF)
+        for (int j = 0; j < nc; ++j) racc += rvs[j * RSTR + lane];
+      __syncwarp();
+    }
+    // ---------------- row write with the Dirichlet treatment
+    const uint8_t ibA = a.ibc[A];
+    if (a.mat) {
+      T* out = reinterpret_cast<T*>(a.vals) + (size_t)rp * NV;
+      const T cnt = (T)ne;
+      for (int q = lane; q < deg * NV; q += 32) {
+        const int s = q / NV, v = q - s * NV;
+        const int B = cols[s];
+        const uint8_t ibB = a.ibc[B];
+        T val = acc[s * NVP + v];
+        uint8_t rb, cb, db;
+        if constexpr (KIND == OVS_ASM_TEM) { rb = TB; cb = TB; db = TB; }
+        else { rb = c_rowbits[v]; cb = c_colbits[v]; db = c_diagbit[v]; }
+        if ((ibA & rb) || (ibB & cb)) val = (T)0;
+        if (B == A && (ibA & db)) val = cnt;
+        out[q] = val;
+      }
+    }
+    if (a.vec && lane < NF) {
+      uint8_t bit;
+      if (KIND == OVS_ASM_TEM) bit = TB;
+      else bit = (lane < 3) ? (uint8_t)(1 << lane) : (lane == 3 ? PB : FB);
+      T v = (ibA & bit) ? (T)0 : racc;
+      if (!isfinite((double)v)) atomicOr(a.flags + 1, 1);
+      reinterpret_cast<T*>(a.rhs)[(size_t)lane * a.N + A] = v;
+    }
+    __syncwarp();
+  }
+  // warp max of the CFL and count of bad Jacobians
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) {
+    cfl = fmax(cfl, __shfl_xor_sync(0xffffffffu, cfl, o));
+    ndet += __shfl_xor_sync(0xffffffffu, ndet, o);
+  }
+  if (lane == 0) {
+    cfl_max(a.cfl_bits, cfl);
+    if (ndet) atomicAdd(a.flags, ndet);
+  }
+}
+
+// ---------------------------------------------------- alpha-stage records
+// assembleQuenching / assembleNavSto alpha stage (src/solveQuenching.f90:26-37,
+// src/assembleNavSto.f90:25-30) fused with the packing of the values the
+// element kernels gather, 16 per node.
+struct AlphaArgs {
+  const double* f[OVS_F_COUNT];
+  const double* xg;
+  void* rec;
+  int N;
+  int tem;   // record layout of the temperature pass
+  double almi, alfi;
+};
+
+template <typename T>
+__global__ void alpha_records_kernel(const AlphaArgs a) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= a.N) return;
+  const size_t N = a.N;
+  const double am = a.almi, af = a.alfi;
+  T r[REC];
+#pragma unroll
+  for (int d = 0; d < 3; ++d) {
+    const size_t k = i + N * d;
+    const double dga = a.f[OVS_F_DGOLD][k] + af * (a.f[OVS_F_DG][k] - a.f[OVS_F_DGOLD][k]);
+    const double xd = a.xg[k] + dga;   // xl + dl of eval_shape_fem (:34)
+    r[d] = (T)xd;
+    r[16 + d] = (T)(xd - (double)r[d]);
+    r[3 + d] = (T)(a.f[OVS_F_UGOLD][k] + af * (a.f[OVS_F_UG][k] - a.f[OVS_F_UGOLD][k]));
+    r[6 + d] = (T)(a.f[OVS_F_UGMOLD][k] + af * (a.f[OVS_F_UGM][k] - a.f[OVS_F_UGMOLD][k]));
+    if (!a.tem) r[9 + d] = (T)(a.f[OVS_F_ACGOLD][k] + am * (a.f[OVS_F_ACG][k] - a.f[OVS_F_ACGOLD][k]));
+  }
+  const double phia = a.f[OVS_F_PHIGOLD][i] + af * (a.f[OVS_F_PHIG][i] - a.f[OVS_F_PHIGOLD][i]);
+  const double ta = a.f[OVS_F_TGOLD][i] + af * (a.f[OVS_F_TG][i] - a.f[OVS_F_TGOLD][i]);
+  r[19] = (T)(phia - (double)(T)phia);
+  if (!a.tem) {
+    r[12] = (T)a.f[OVS_F_PG][i];
+    r[13] = (T)phia;
+    r[14] = (T)(a.f[OVS_F_RPHIGOLD][i] + am * (a.f[OVS_F_RPHIG][i] - a.f[OVS_F_RPHIGOLD][i]));
+    r[15] = (T)ta;
+  } else {
+    r[9] = (T)phia;
+    r[10] = (T)ta;
+    r[11] = (T)(a.f[OVS_F_RTGOLD][i] + am * (a.f[OVS_F_RTG][i] - a.f[OVS_F_RTGOLD][i]));
+    r[12] = r[13] = r[14] = r[15] = (T)0;
+  }
+  T* o = reinterpret_cast<T*>(a.rec) + (size_t)i * REC;
+#pragma unroll
+  for (int k = 0; k < REC; ++k) o[k] = r[k];
+}
+
+template <typename T, int KIND>
+int launch_assemble(ovs_ctx* c, const AsmArgs& a) {
+  constexpr int WARPS = sizeof(T) == 8 ? 2 : 4;
+  using S = Smem<T, KIND>;
+  const size_t smem = S::bytes(a.max_deg) * WARPS;
+  auto kern = assemble_rows_kernel<T, KIND, WARPS>;
+  OVS_CUDA_TRY(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  int per_sm = 0;
+  OVS_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, WARPS * 32, smem));
+  if (per_sm < 1) return OVS_ERR_ARG;
+  long need = ((long)c->N + WARPS - 1) / WARPS;
+  long grid = (long)per_sm * c->num_sms * 8;
+  if (grid > need) grid = need;
+  if (grid < 1) grid = 1;
+  kern<<<(int)grid, WARPS * 32, smem, c->stream>>>(a);
+  ++c->launches;
+  OVS_CUDA_TRY(cudaGetLastError());
+  return OVS_OK;
+}
+
+}  // namespace
+
+static int dispatch_assemble(ovs_ctx* c, int kernel, int prec, const AsmArgs& a) {
+  if (prec == OVS_FP64) {
+    if (kernel == OVS_ASM_NS) return launch_assemble<double, OVS_ASM_NS>(c, a);
+    if (kernel == OVS_ASM_NSVOF) return launch_assemble<double, OVS_ASM_NSVOF>(c, a);
+    return launch_assemble<double, OVS_ASM_TEM>(c, a);
+  }
+  if (kernel == OVS_ASM_NS) return launch_assemble<float, OVS_ASM_NS>(c, a);
+  if (kernel == OVS_ASM_NSVOF) return launch_assemble<float, OVS_ASM_NSVOF>(c, a);
+  return launch_assemble<float, OVS_ASM_TEM>(c, a);
+}
+
+static void fill_args(ovs_ctx* c, int prec, SysStore& S, int tensor_flag, AsmArgs& a) {
+  a.rec = c->rec[prec];
+  a.ien = c->ien;
+  a.elm_id = c->elm_id;
+  a.ibc = c->ibc;
+  a.rowptr = c->rowptr;
+  a.colidx = c->colidx;
+  a.n2e_ptr = c->n2e_ptr;
+  a.n2e = c->n2e;
+  a.vals = S.vals;
+  a.rhs = S.rhs;
+  a.flags = c->flags;
+  a.cfl_bits = c->cfl_bits;
+  a.N = c->N;
+  a.mat = (tensor_flag & OVS_TENSOR_MAT) != 0;
+  a.vec = (tensor_flag & OVS_TENSOR_VEC) != 0;
+  a.max_deg = c->max_deg;
+  a.p = c->params;
+}
+
+int ovs_profile_assemble(ovs_ctx* c, int kernel, int prec, int reps, double* ms) {
+  if (kernel != OVS_ASM_NS && kernel != OVS_ASM_NSVOF && kernel != OVS_ASM_TEM) return OVS_ERR_ARG;
+  const int sys = kernel == OVS_ASM_NS ? OVS_SYS_NS : (kernel == OVS_ASM_NSVOF ? OVS_SYS_NSVOF : OVS_SYS_TEM);
+  SysStore& S = c->sys[sys][prec];
+  if (!S.vals || !S.rhs || !c->rec[prec]) return OVS_ERR_STATE;
+  AsmArgs a;
+  fill_args(c, prec, S, OVS_TENSOR_MAT | OVS_TENSOR_VEC, a);
+  int st;
+  if ((st = dispatch_assemble(c, kernel, prec, a))) return st;  // warm
+  OVS_CUDA_TRY(cudaEventRecord(c->ev0, c->stream));
+  for (int r = 0; r < reps; ++r)
+    if ((st = dispatch_assemble(c, kernel, prec, a))) return st;
+  OVS_CUDA_TRY(cudaEventRecord(c->ev1, c->stream));
+  OVS_CUDA_TRY(cudaEventSynchronize(c->ev1));
+  float t = 0.f;
+  OVS_CUDA_TRY(cudaEventElapsedTime(&t, c->ev0, c->ev1));
+  *ms = (double)t / reps;
+  return OVS_OK;
+}
+
+int ovs_assemble_impl(ovs_ctx* c, int kernel, int tensor_flag, int prec, double* cfl) {
+  if (!c->have_pattern || !c->have_params) return OVS_ERR_STATE;
+  if (c->nshl != 4) return OVS_ERR_ARG;
+  if (kernel != OVS_ASM_NS && kernel != OVS_ASM_NSVOF && kernel != OVS_ASM_TEM) return OVS_ERR_ARG;
+  if (prec != OVS_FP64 && prec != OVS_FP32) return OVS_ERR_ARG;
+  const int sys = kernel == OVS_ASM_NS ? OVS_SYS_NS : (kernel == OVS_ASM_NSVOF ? OVS_SYS_NSVOF : OVS_SYS_TEM);
+  const size_t ts = prec == OVS_FP64 ? 8 : 4;
+  const int nv = ovs_sys_nv(sys), nf = ovs_sys_nf(sys);
+  SysStore& S = c->sys[sys][prec];
+  int st;
+  if ((st = ovs_ensure(&S.vals, ts * (size_t)c->nnz * nv))) return st;
+  if ((st = ovs_ensure(&S.rhs, ts * (size_t)c->N * nf))) return st;
+  if ((st = ovs_ensure(&c->rec[prec], ts * (size_t)c->N * REC))) return st;
+  cudaStream_t s = c->stream;
+  OVS_CUDA_TRY(cudaMemsetAsync(c->flags, 0, sizeof(int) * 4, s));
+  OVS_CUDA_TRY(cudaMemsetAsync(c->cfl_bits, 0, sizeof(unsigned long long), s));
+  AlphaArgs aa;
+  for (int f = 0; f < OVS_F_COUNT; ++f) aa.f[f] = c->field[f];
+  aa.xg = c->field[OVS_F_XG];
+  aa.rec = c->rec[prec];
+  aa.N = c->N;
+  aa.tem = kernel == OVS_ASM_TEM;
+  aa.almi = c->params.almi;
+  aa.alfi = c->params.alfi;
+  if (prec == OVS_FP64) alpha_records_kernel<double><<<ovs_grid(c->N, 256, 1 << 30), 256, 0, s>>>(aa);
+  else alpha_records_kernel<float><<<ovs_grid(c->N, 256, 1 << 30), 256, 0, s>>>(aa);
+  ++c->launches;
+  OVS_CUDA_TRY(cudaGetLastError());
+  AsmArgs a;
+  fill_args(c, prec, S, tensor_flag, a);
+  if ((st = dispatch_assemble(c, kernel, prec, a))) return st;
+  if (a.mat) S.have_mat = true;
+  if (a.vec) S.have_rhs = true;
+  int hflags[4];
+  unsigned long long hcfl = 0;
+  OVS_CUDA_TRY(cudaMemcpyAsync(hflags, c->flags, sizeof(hflags), cudaMemcpyDeviceToHost, s));
+  OVS_CUDA_TRY(cudaMemcpyAsync(&hcfl, c->cfl_bits, sizeof(hcfl), cudaMemcpyDeviceToHost, s));
+  OVS_CUDA_TRY(cudaStreamSynchronize(s));
+  if (cfl) {
+    double v;
+    memcpy(&v, &hcfl, sizeof(v));
+    *cfl = v;
+  }
+  if (hflags[1]) return OVS_ERR_NONFINITE;
+  if (hflags[0]) return OVS_WARN_NEG_DETJ;
+  return OVS_OK;
+}

@@ -1,0 +1,663 @@
+// C ABI of the library (include/ovs.h): context, mesh/state transfer,
+// reference-layout conversions, Newton update and residual norms.
+#include "ovs_internal.cuh"
+
+#include <math.h>
+#include <stdio.h>
+#include <stdlib.h>
+#include <string.h>
+
+static thread_local char g_last_error[512] = {0};
+
+void ovs_set_last_cuda_error(cudaError_t e, const char* what, const char* file, int line) {
+  snprintf(g_last_error, sizeof(g_last_error), "%s: %s (%s:%d)", cudaGetErrorName(e), what, file, line);
+}
+
+int ovs_ensure(void** p, size_t bytes) {
+  if (*p) return OVS_OK;
+  if (bytes == 0) bytes = 16;
+  if (cudaMalloc(p, bytes) != cudaSuccess) {
+    cudaGetLastError();
+    *p = nullptr;
+    return OVS_ERR_NOMEM;
+  }
+  return OVS_OK;
+}
+
+int ovs_activate(ovs_ctx* c) {
+  OVS_CUDA_TRY(cudaSetDevice(c->device));
+  return OVS_OK;
+}
+
+namespace {
+
+inline int field_width(int f) { return f <= OVS_F_ACGMOLD ? 3 : 1; }
+
+__global__ void ien_pack_kernel(const int* __restrict__ ien_cm, int E, int nshl, int* __restrict__ out,
+                                int* __restrict__ bad) {
+  size_t t = blockIdx.x * (size_t)blockDim.x + threadIdx.x;
+  if (t >= (size_t)E * nshl) return;
+  int e = (int)(t / nshl), a = (int)(t % nshl);
+  int v = ien_cm[(size_t)a * E + e] - 1;
+  out[t] = v;
+  // an element must not repeat a node
+  for (int b = 0; b < a; ++b)
+    if (ien_cm[(size_t)b * E + e] - 1 == v) atomicOr(bad, 1);
+}
+
+__global__ void ibc_pack_kernel(const int* __restrict__ ibc, int N, int nibc, uint8_t* __restrict__ out) {
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= N) return;
+  unsigned m = 0;
+  for (int d = 0; d < nibc && d < 8; ++d)
+    if (ibc[(size_t)d * N + i] == 1) m |= 1u << d;
+  out[i] = (uint8_t)m;
+}
+
+// reference block <-> internal slot position (see assemble.cu)
+__constant__ int c_pos_k11[9] = {0, 1, 2, 4, 5, 6, 8, 9, 10};
+__constant__ int c_pos_g[3] = {3, 7, 11};
+__constant__ int c_pos_d[3] = {12, 13, 14};
+__constant__ int c_pos_lsu[3] = {16, 17, 18};
+__constant__ int c_pos_uls[3] = {20, 21, 22};
+
+__device__ int block_pos(int block, int t) {
+  switch (block) {
+    case OVS_BLK_K11: return c_pos_k11[t];
+    case OVS_BLK_G: return c_pos_g[t];
+    case OVS_BLK_D1: return c_pos_d[t];
+    case OVS_BLK_M: return 15;
+    case OVS_BLK_LS: return 19;
+    case OVS_BLK_LSU: return c_pos_lsu[t];
+    case OVS_BLK_ULS: return c_pos_uls[t];
+    case OVS_BLK_PLS: return 23;
+    default: return 0;
+  }
+}
+
+template <typename T>
+__global__ void block_get_kernel(const T* __restrict__ vals, int nv, int block, int w, size_t nnz,
+                                 double* __restrict__ out) {
+  size_t q = blockIdx.x * (size_t)blockDim.x + threadIdx.x;
+  if (q >= nnz * w) return;
+  size_t k = q / w;
+  int t = (int)(q - k * w);
+  out[q] = (double)vals[k * nv + block_pos(block, t)];
+}
+
+template <typename T>
+__global__ void block_set_kernel(T* __restrict__ vals, int nv, int block, int w, size_t nnz,
+                                 const double* __restrict__ in) {
+  size_t q = blockIdx.x * (size_t)blockDim.x + threadIdx.x;
+  if (q >= nnz * w) return;
+  size_t k = q / w;
+  int t = (int)(q - k * w);
+  vals[k * nv + block_pos(block, t)] = (T)in[q];
+}
+
+__global__ void fill_int_kernel(int* __restrict__ p, size_t n, int v) {
+  size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x;
+  if (i < n) p[i] = v;
+}
+
+template <typename TS, typename TD>
+__global__ void copy_convert_kernel(const TS* __restrict__ a, TD* __restrict__ b, size_t n) {
+  size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x;
+  if (i < n) b[i] = (TD)a[i];
+}
+
+// Newton update, src/solveFlow.f90:99-104,139-140
+__global__ void newton_update_kernel(int N, int sys, double gdt, double agdt, const double* __restrict__ sol,
+                                     double* acg, double* ug, double* pg, double* rphig, double* phig,
+                                     double* rtg, double* tg) {
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= N) return;
+  if (sys == OVS_SYS_TEM) {
+    rtg[i] = rtg[i] + sol[i];
+    tg[i] = tg[i] + gdt * sol[i];
+    return;
+  }
+  for (int d = 0; d < 3; ++d) {
+    size_t k = i + (size_t)N * d;
+    acg[k] = acg[k] + sol[k];
+    ug[k] = ug[k] + gdt * sol[k];
+  }
+  pg[i] = pg[i] + agdt * sol[3 * (size_t)N + i];
+  if (sys == OVS_SYS_NSVOF) {
+    rphig[i] = rphig[i] + sol[4 * (size_t)N + i];
+    phig[i] = phig[i] + gdt * sol[4 * (size_t)N + i];
+  }
+}
+
+int upload_double(ovs_ctx* c, double** dst, const double* host, size_t n) {
+  double* d = nullptr;
+  OVS_CUDA_TRY(cudaMallocAsync(&d, sizeof(double) * n, c->stream));
+  OVS_CUDA_TRY(cudaMemcpyAsync(d, host, sizeof(double) * n, cudaMemcpyHostToDevice, c->stream));
+  *dst = d;
+  return OVS_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int ovs_version(void) { return 10000; }
+
+const char* ovs_status_string(int status) {
+  switch (status) {
+    case OVS_OK: return "ok";
+    case OVS_WARN_NEG_DETJ: return "warning: element with non-positive Jacobian determinant";
+    case OVS_ERR_ARG: return "invalid argument";
+    case OVS_ERR_CUDA: return g_last_error[0] ? g_last_error : "CUDA error";
+    case OVS_ERR_NOMEM: return "device allocation failed";
+    case OVS_ERR_STATE: return "call order: required data not yet provided";
+    case OVS_ERR_NONFINITE: return "non-finite value in an assembled residual";
+    case OVS_ERR_PATTERN: return "a node has more CSR neighbours than supported";
+    case OVS_ERR_NODEVICE: return "no CUDA device";
+    case OVS_ERR_TIMEOUT: return "timed out waiting for the device";
+    default: return "unknown status";
+  }
+}
+
+int ovs_params_genalpha(double rhoinf, ovs_params* p) {
+  if (!p) return OVS_ERR_ARG;
+  if (rhoinf < 0.0 || rhoinf > 1.0) {
+    p->almi = 1.0; p->alfi = 1.0; p->gami = 1.0; p->beti = 1.0;
+  } else {
+    p->almi = (3.0 - rhoinf) / (1.0 + rhoinf) / 2.0;
+    p->alfi = 1.0 / (1.0 + rhoinf);
+    p->gami = 0.5 + p->almi - p->alfi;
+    p->beti = 0.25 * (1.0 + p->almi - p->alfi) * (1.0 + p->almi - p->alfi);
+  }
+  return OVS_OK;
+}
+
+int ovs_create(ovs_ctx** out, const ovs_dims* dims) {
+  if (!out || !dims) return OVS_ERR_ARG;
+  *out = nullptr;
+  if (dims->nnode <= 0 || dims->nelem <= 0 || (dims->nshl != 4 && dims->nshl != 8)) return OVS_ERR_ARG;
+  if ((long)dims->nelem * dims->nshl >= (1L << 31) || dims->nelem >= (1 << 28)) return OVS_ERR_ARG;
+  int ndev = 0;
+  if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) { cudaGetLastError(); return OVS_ERR_NODEVICE; }
+  if (dims->device >= ndev) return OVS_ERR_ARG;
+  if (dims->device >= 0) OVS_CUDA_TRY(cudaSetDevice(dims->device));
+  ovs_ctx* c = new ovs_ctx();
+  OVS_CUDA_TRY(cudaGetDevice(&c->device));
+  OVS_CUDA_TRY(cudaDeviceGetAttribute(&c->num_sms, cudaDevAttrMultiProcessorCount, c->device));
+  c->N = dims->nnode;
+  c->E = dims->nelem;
+  c->nshl = dims->nshl;
+  OVS_CUDA_TRY(cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking));
+  OVS_CUDA_TRY(cudaEventCreate(&c->ev0));
+  OVS_CUDA_TRY(cudaEventCreate(&c->ev1));
+  int st;
+  const size_t N = c->N;
+  for (int f = 0; f < OVS_F_COUNT; ++f) {
+    if ((st = ovs_ensure((void**)&c->field[f], sizeof(double) * N * field_width(f)))) { ovs_destroy(c); return st; }
+    OVS_CUDA_TRY(cudaMemsetAsync(c->field[f], 0, sizeof(double) * N * field_width(f), c->stream));
+  }
+  if ((st = ovs_ensure((void**)&c->ien, sizeof(int) * (size_t)c->E * c->nshl)) ||
+      (st = ovs_ensure((void**)&c->elm_id, sizeof(int) * (size_t)c->E)) ||
+      (st = ovs_ensure((void**)&c->ibc, N)) ||
+      (st = ovs_ensure((void**)&c->gm, sizeof(GmresDev))) ||
+      (st = ovs_ensure((void**)&c->flags, sizeof(int) * 4)) ||
+      (st = ovs_ensure((void**)&c->cfl_bits, sizeof(unsigned long long)))) {
+    ovs_destroy(c);
+    return st;
+  }
+  OVS_CUDA_TRY(cudaMemsetAsync(c->ibc, 0, N, c->stream));
+  OVS_CUDA_TRY(cudaMemsetAsync(c->gm, 0, sizeof(GmresDev), c->stream));
+  OVS_CUDA_TRY(cudaMallocHost(&c->h_pinned, sizeof(int) * 16));
+  OVS_CUDA_TRY(cudaMallocHost(&c->h_pinned_d, sizeof(double) * 16));
+  OVS_CUDA_TRY(cudaStreamSynchronize(c->stream));
+  *out = c;
+  return OVS_OK;
+}
+
+int ovs_destroy(ovs_ctx* c) {
+  if (!c) return OVS_OK;
+  cudaSetDevice(c->device);
+  if (c->stream) cudaStreamSynchronize(c->stream);
+  void* ptrs[] = {c->ien, c->elm_id, c->ibc, c->rowptr, c->colidx, c->diag, c->n2e_ptr, c->n2e,
+                  c->rec[0], c->rec[1], c->gm, c->basis[0], c->basis[1], c->work64, c->work32,
+                  c->flags, c->cfl_bits};
+  for (void* p : ptrs) if (p) cudaFree(p);
+  for (int f = 0; f < OVS_F_COUNT; ++f) if (c->field[f]) cudaFree(c->field[f]);
+  for (int s = 0; s < 4; ++s) {
+    if (c->sol[s]) cudaFree(c->sol[s]);
+    for (int p = 0; p < 2; ++p) {
+      SysStore& S = c->sys[s][p];
+      if (S.vals) cudaFree(S.vals);
+      if (S.rhs) cudaFree(S.rhs);
+      if (S.binv) cudaFree(S.binv);
+    }
+  }
+  if (c->h_pinned) cudaFreeHost(c->h_pinned);
+  if (c->h_pinned_d) cudaFreeHost(c->h_pinned_d);
+  if (c->ev0) cudaEventDestroy(c->ev0);
+  if (c->ev1) cudaEventDestroy(c->ev1);
+  if (c->stream) cudaStreamDestroy(c->stream);
+  cudaGetLastError();
+  delete c;
+  return OVS_OK;
+}
+
+int ovs_synchronize(ovs_ctx* c) {
+  if (!c) return OVS_ERR_ARG;
+  OVS_CUDA_TRY(cudaStreamSynchronize(c->stream));
+  return OVS_OK;
+}
+
+int ovs_get_stream(ovs_ctx* c, void** stream) {
+  if (!c || !stream) return OVS_ERR_ARG;
+  *stream = (void*)c->stream;
+  return OVS_OK;
+}
+
+int ovs_upload_mesh(ovs_ctx* c, const double* xg, const int* ien, const int* elm_id) {
+  if (!c || !ien) return OVS_ERR_ARG;
+  int st;
+  if ((st = ovs_activate(c))) return st;
+  cudaStream_t s = c->stream;
+  const size_t EN = (size_t)c->E * c->nshl;
+  if (xg) OVS_CUDA_TRY(cudaMemcpyAsync(c->field[OVS_F_XG], xg, sizeof(double) * 3 * (size_t)c->N, cudaMemcpyHostToDevice, s));
+  int *tmp = nullptr, *bad = nullptr;
+  OVS_CUDA_TRY(cudaMallocAsync(&tmp, sizeof(int) * EN, s));
+  OVS_CUDA_TRY(cudaMallocAsync(&bad, sizeof(int), s));
+  OVS_CUDA_TRY(cudaMemsetAsync(bad, 0, sizeof(int), s));
+  OVS_CUDA_TRY(cudaMemcpyAsync(tmp, ien, sizeof(int) * EN, cudaMemcpyHostToDevice, s));
+  ien_pack_kernel<<<ovs_grid(EN, 256, 1 << 30), 256, 0, s>>>(tmp, c->E, c->nshl, c->ien, bad);
+  ++c->launches;
+  OVS_CUDA_TRY(cudaGetLastError());
+  if (elm_id) {
+    OVS_CUDA_TRY(cudaMemcpyAsync(c->elm_id, elm_id, sizeof(int) * (size_t)c->E, cudaMemcpyHostToDevice, s));
+  } else {
+    fill_int_kernel<<<ovs_grid(c->E, 256, 1 << 30), 256, 0, s>>>(c->elm_id, (size_t)c->E, 102);
+    ++c->launches;
+  }
+  int hbad = 0;
+  OVS_CUDA_TRY(cudaMemcpyAsync(&hbad, bad, sizeof(int), cudaMemcpyDeviceToHost, s));
+  OVS_CUDA_TRY(cudaFreeAsync(tmp, s));
+  OVS_CUDA_TRY(cudaFreeAsync(bad, s));
+  OVS_CUDA_TRY(cudaStreamSynchronize(s));
+  if (hbad) return OVS_ERR_ARG;
+  c->have_mesh = true;
+  c->have_pattern = false;
+  return OVS_OK;
+}
+
+
+int ovs_build_pattern(ovs_ctx* c, int* icnt) {
+  if (!c) return OVS_ERR_ARG;
+  if (!c->have_mesh) return OVS_ERR_STATE;
+  int st;
+  if ((st = ovs_activate(c))) return st;
+  if ((st = ovs_pattern_build(c))) return st;
+  if (icnt) *icnt = c->nnz;
+  return OVS_OK;
+}
+
+int ovs_get_pattern(ovs_ctx* c, int* col, int* row) {
+  if (!c || !col) return OVS_ERR_ARG;
+  if (!c->have_pattern) return OVS_ERR_STATE;
+  int st;
+  if ((st = ovs_activate(c))) return st;
+  return ovs_pattern_to_host(c, col, row);
+}
+
+int ovs_gen_spar_struc(int nnode, int nelem, int nshl, const int* ien, int* col, int* row, int* icnt) {
+  if (!ien || !col || !icnt) return OVS_ERR_ARG;
+  ovs_dims d = {nnode, nelem, nshl, 0};
+  ovs_ctx* c = nullptr;
+  int st = ovs_create(&c, &d);
+  if (st) return st;
+  if ((st = ovs_upload_mesh(c, nullptr, ien, nullptr)) || (st = ovs_build_pattern(c, nullptr))) {
+    ovs_destroy(c);
+    return st;
+  }
+  if (row && *icnt < c->nnz) { *icnt = c->nnz; ovs_destroy(c); return OVS_ERR_ARG; }
+  *icnt = c->nnz;
+  st = ovs_pattern_to_host(c, col, row);
+  ovs_destroy(c);
+  return st;
+}
+
+int ovs_set_params(ovs_ctx* c, const ovs_params* p) {
+  if (!c || !p) return OVS_ERR_ARG;
+  if (!(p->delt > 0.0)) return OVS_ERR_ARG;
+  c->params = *p;
+  c->have_params = true;
+  return OVS_OK;
+}
+
+int ovs_set_ibc(ovs_ctx* c, const int* ibc, int nibc) {
+  if (!c || !ibc || nibc < 1) return OVS_ERR_ARG;
+  int st;
+  if ((st = ovs_activate(c))) return st;
+  cudaStream_t s = c->stream;
+  int* tmp = nullptr;
+  const size_t n = (size_t)c->N * nibc;
+  OVS_CUDA_TRY(cudaMallocAsync(&tmp, sizeof(int) * n, s));
+  OVS_CUDA_TRY(cudaMemcpyAsync(tmp, ibc, sizeof(int) * n, cudaMemcpyHostToDevice, s));
+  ibc_pack_kernel<<<ovs_grid(c->N, 256, 1 << 30), 256, 0, s>>>(tmp, c->N, nibc, c->ibc);
+  ++c->launches;
+  OVS_CUDA_TRY(cudaGetLastError());
+  OVS_CUDA_TRY(cudaFreeAsync(tmp, s));
+  OVS_CUDA_TRY(cudaStreamSynchronize(s));
+  return OVS_OK;
+}
+
+int ovs_set_field(ovs_ctx* c, int field, const double* host) {
+  if (!c || !host || field < 0 || field >= OVS_F_COUNT) return OVS_ERR_ARG;
+  int st;
+  if ((st = ovs_activate(c))) return st;
+  OVS_CUDA_TRY(cudaMemcpyAsync(c->field[field], host, sizeof(double) * (size_t)c->N * field_width(field),
+                               cudaMemcpyHostToDevice, c->stream));
+  OVS_CUDA_TRY(cudaStreamSynchronize(c->stream));
+  return OVS_OK;
+}
+
+int ovs_get_field(ovs_ctx* c, int field, double* host) {
+  if (!c || !host || field < 0 || field >= OVS_F_COUNT) return OVS_ERR_ARG;
+  int st;
+  if ((st = ovs_activate(c))) return st;
+  OVS_CUDA_TRY(cudaMemcpyAsync(host, c->field[field], sizeof(double) * (size_t)c->N * field_width(field),
+                               cudaMemcpyDeviceToHost, c->stream));
+  OVS_CUDA_TRY(cudaStreamSynchronize(c->stream));
+  return OVS_OK;
+}
+
+int ovs_assemble(ovs_ctx* c, int kernel, int tensor_flag, int precision, double* cfl) {
+  if (!c) return OVS_ERR_ARG;
+  if ((tensor_flag & (OVS_TENSOR_VEC | OVS_TENSOR_MAT)) == 0) return OVS_ERR_ARG;
+  int st;
+  if ((st = ovs_activate(c))) return st;
+  OVS_CUDA_TRY(cudaEventRecord(c->ev0, c->stream));
+  st = ovs_assemble_impl(c, kernel, tensor_flag, precision, cfl);
+  if (st < 0) return st;
+  OVS_CUDA_TRY(cudaEventRecord(c->ev1, c->stream));
+  OVS_CUDA_TRY(cudaEventSynchronize(c->ev1));
+  float ms = 0.f;
+  OVS_CUDA_TRY(cudaEventElapsedTime(&ms, c->ev0, c->ev1));
+  c->last_ms = ms;
+  return st;
+}
+
+static int sys_ok(ovs_ctx* c, int sys, int prec) {
+  if (!c) return 0;
+  if (sys != OVS_SYS_NS && sys != OVS_SYS_NSVOF && sys != OVS_SYS_TEM) return 0;
+  if (prec != OVS_FP64 && prec != OVS_FP32) return 0;
+  return 1;
+}
+
+int ovs_get_rhs(ovs_ctx* c, int sys, int prec, double* rhs) {
+  if (!sys_ok(c, sys, prec) || !rhs) return OVS_ERR_ARG;
+  SysStore& S = c->sys[sys][prec];
+  if (!S.rhs) return OVS_ERR_STATE;
+  int st;
+  if ((st = ovs_activate(c))) return st;
+  const size_t n = (size_t)c->N * ovs_sys_nf(sys);
+  if (prec == OVS_FP64) {
+    OVS_CUDA_TRY(cudaMemcpyAsync(rhs, S.rhs, sizeof(double) * n, cudaMemcpyDeviceToHost, c->stream));
+  } else {
+    double* tmp = nullptr;
+    OVS_CUDA_TRY(cudaMallocAsync(&tmp, sizeof(double) * n, c->stream));
+    copy_convert_kernel<float, double><<<ovs_grid(n, 256, 1 << 30), 256, 0, c->stream>>>((const float*)S.rhs, tmp, n);
+    ++c->launches;
+    OVS_CUDA_TRY(cudaMemcpyAsync(rhs, tmp, sizeof(double) * n, cudaMemcpyDeviceToHost, c->stream));
+    OVS_CUDA_TRY(cudaFreeAsync(tmp, c->stream));
+  }
+  OVS_CUDA_TRY(cudaStreamSynchronize(c->stream));
+  return OVS_OK;
+}
+
+int ovs_set_rhs(ovs_ctx* c, int sys, int prec, const double* rhs) {
+  if (!sys_ok(c, sys, prec) || !rhs) return OVS_ERR_ARG;
+  SysStore& S = c->sys[sys][prec];
+  int st;
+  if ((st = ovs_activate(c))) return st;
+  const size_t n = (size_t)c->N * ovs_sys_nf(sys);
+  const size_t ts = prec == OVS_FP64 ? 8 : 4;
+  if ((st = ovs_ensure(&S.rhs, ts * n))) return st;
+  double* tmp = nullptr;
+  if ((st = upload_double(c, &tmp, rhs, n))) return st;
+  if (prec == OVS_FP64)
+    {
+      copy_convert_kernel<double, double><<<ovs_grid(n, 256, 1 << 30), 256, 0, c->stream>>>(tmp, (double*)S.rhs, n);
+      ++c->launches;
+    }
+  else
+    {
+      copy_convert_kernel<double, float><<<ovs_grid(n, 256, 1 << 30), 256, 0, c->stream>>>(tmp, (float*)S.rhs, n);
+      ++c->launches;
+    }
+  OVS_CUDA_TRY(cudaFreeAsync(tmp, c->stream));
+  OVS_CUDA_TRY(cudaStreamSynchronize(c->stream));
+  S.have_rhs = true;
+  return OVS_OK;
+}
+
+static int block_width(int sys, int block) {
+  if (sys == OVS_SYS_TEM) return block == OVS_BLK_TEM ? 1 : 0;
+  switch (block) {
+    case OVS_BLK_K11: return 9;
+    case OVS_BLK_G: case OVS_BLK_D1: return 3;
+    case OVS_BLK_M: return 1;
+    case OVS_BLK_LS: case OVS_BLK_PLS: return sys == OVS_SYS_NSVOF ? 1 : 0;
+    case OVS_BLK_LSU: case OVS_BLK_ULS: return sys == OVS_SYS_NSVOF ? 3 : 0;
+    default: return 0;
+  }
+}
+
+int ovs_get_lhs_block(ovs_ctx* c, int sys, int prec, int block, double* out) {
+  if (!sys_ok(c, sys, prec) || !out) return OVS_ERR_ARG;
+  const int w = block_width(sys, block);
+  if (!w) return OVS_ERR_ARG;
+  SysStore& S = c->sys[sys][prec];
+  if (!S.vals) return OVS_ERR_STATE;
+  int st;
+  if ((st = ovs_activate(c))) return st;
+  const size_t n = (size_t)c->nnz * w;
+  double* tmp = nullptr;
+  OVS_CUDA_TRY(cudaMallocAsync(&tmp, sizeof(double) * (n ? n : 1), c->stream));
+  const int nv = ovs_sys_nv(sys);
+  const int bl = sys == OVS_SYS_TEM ? -1 : block;
+  if (prec == OVS_FP64)
+    {
+      block_get_kernel<double><<<ovs_grid(n, 256, 1 << 30), 256, 0, c->stream>>>((const double*)S.vals, nv, bl, w, c->nnz, tmp);
+      ++c->launches;
+    }
+  else
+    {
+      block_get_kernel<float><<<ovs_grid(n, 256, 1 << 30), 256, 0, c->stream>>>((const float*)S.vals, nv, bl, w, c->nnz, tmp);
+      ++c->launches;
+    }
+  OVS_CUDA_TRY(cudaGetLastError());
+  OVS_CUDA_TRY(cudaMemcpyAsync(out, tmp, sizeof(double) * n, cudaMemcpyDeviceToHost, c->stream));
+  OVS_CUDA_TRY(cudaFreeAsync(tmp, c->stream));
+  OVS_CUDA_TRY(cudaStreamSynchronize(c->stream));
+  return OVS_OK;
+}
+
+int ovs_set_lhs_block(ovs_ctx* c, int sys, int prec, int block, const double* in) {
+  if (!sys_ok(c, sys, prec) || !in) return OVS_ERR_ARG;
+  if (!c->have_pattern) return OVS_ERR_STATE;
+  const int w = block_width(sys, block);
+  if (!w) return OVS_ERR_ARG;
+  SysStore& S = c->sys[sys][prec];
+  int st;
+  if ((st = ovs_activate(c))) return st;
+  const int nv = ovs_sys_nv(sys);
+  const size_t ts = prec == OVS_FP64 ? 8 : 4;
+  if (!S.vals) {
+    if ((st = ovs_ensure(&S.vals, ts * (size_t)c->nnz * nv))) return st;
+    OVS_CUDA_TRY(cudaMemsetAsync(S.vals, 0, ts * (size_t)c->nnz * nv, c->stream));
+  }
+  const size_t n = (size_t)c->nnz * w;
+  double* tmp = nullptr;
+  if ((st = upload_double(c, &tmp, in, n))) return st;
+  const int bl = sys == OVS_SYS_TEM ? -1 : block;
+  if (prec == OVS_FP64)
+    {
+      block_set_kernel<double><<<ovs_grid(n, 256, 1 << 30), 256, 0, c->stream>>>((double*)S.vals, nv, bl, w, c->nnz, tmp);
+      ++c->launches;
+    }
+  else
+    {
+      block_set_kernel<float><<<ovs_grid(n, 256, 1 << 30), 256, 0, c->stream>>>((float*)S.vals, nv, bl, w, c->nnz, tmp);
+      ++c->launches;
+    }
+  OVS_CUDA_TRY(cudaGetLastError());
+  OVS_CUDA_TRY(cudaFreeAsync(tmp, c->stream));
+  OVS_CUDA_TRY(cudaStreamSynchronize(c->stream));
+  S.have_mat = true;
+  return OVS_OK;
+}
+
+int ovs_spmv(ovs_ctx* c, int sys, int prec, const double* x, double* y) {
+  if (!sys_ok(c, sys, prec) || !x || !y) return OVS_ERR_ARG;
+  int st;
+  if ((st = ovs_activate(c))) return st;
+  const size_t n = (size_t)c->N * ovs_sys_nf(sys);
+  double *dx = nullptr, *dy = nullptr;
+  if ((st = upload_double(c, &dx, x, n))) return st;
+  OVS_CUDA_TRY(cudaMallocAsync(&dy, sizeof(double) * n, c->stream));
+  st = ovs_spmv_impl(c, sys, prec, dx, dy);
+  if (!st) OVS_CUDA_TRY(cudaMemcpyAsync(y, dy, sizeof(double) * n, cudaMemcpyDeviceToHost, c->stream));
+  cudaFreeAsync(dx, c->stream);
+  cudaFreeAsync(dy, c->stream);
+  OVS_CUDA_TRY(cudaStreamSynchronize(c->stream));
+  return st;
+}
+
+int ovs_gmres(ovs_ctx* c, int sys, double tol, int kspace, int kspace_min, double* sol, ovs_gmres_info* info) {
+  if (!sys_ok(c, sys, OVS_FP64) || !sol) return OVS_ERR_ARG;
+  if (kspace < 1 || kspace > OVS_MAX_KSPACE) return OVS_ERR_ARG;
+  int st;
+  if ((st = ovs_activate(c))) return st;
+  const size_t n = (size_t)c->N * ovs_sys_nf(sys);
+  if ((st = ovs_ensure((void**)&c->sol[sys], sizeof(double) * 5 * (size_t)c->N))) return st;
+  OVS_CUDA_TRY(cudaMemcpyAsync(c->sol[sys], sol, sizeof(double) * n, cudaMemcpyHostToDevice, c->stream));
+  ovs_gmres_info gi;
+  memset(&gi, 0, sizeof(gi));
+  OVS_CUDA_TRY(cudaEventRecord(c->ev0, c->stream));
+  st = ovs_gmres_ref_impl(c, sys, tol, kspace, kspace_min, c->sol[sys], &gi);
+  if (st) return st;
+  OVS_CUDA_TRY(cudaEventRecord(c->ev1, c->stream));
+  OVS_CUDA_TRY(cudaEventSynchronize(c->ev1));
+  {
+    float ms = 0.f;
+    OVS_CUDA_TRY(cudaEventElapsedTime(&ms, c->ev0, c->ev1));
+    c->last_ms = ms;
+  }
+  OVS_CUDA_TRY(cudaMemcpyAsync(sol, c->sol[sys], sizeof(double) * n, cudaMemcpyDeviceToHost, c->stream));
+  OVS_CUDA_TRY(cudaStreamSynchronize(c->stream));
+  if (info) *info = gi;
+  return OVS_OK;
+}
+
+int ovs_solve(ovs_ctx* c, int sys, int mode, double rtol, int kspace, int max_cycles, double* sol,
+              ovs_solve_info* info) {
+  if (!sys_ok(c, sys, mode == OVS_FP32 ? OVS_FP32 : OVS_FP64)) return OVS_ERR_ARG;
+  if (kspace < 1 || kspace > OVS_MAX_KSPACE || max_cycles < 1 || !(rtol > 0.0)) return OVS_ERR_ARG;
+  int st;
+  if ((st = ovs_activate(c))) return st;
+  ovs_solve_info si;
+  memset(&si, 0, sizeof(si));
+  if ((st = ovs_solve_impl(c, sys, mode, rtol, kspace, max_cycles, &si))) return st;
+  c->last_ms = si.seconds * 1e3;
+  if (sol) {
+    const size_t n = (size_t)c->N * ovs_sys_nf(sys);
+    OVS_CUDA_TRY(cudaMemcpyAsync(sol, c->sol[sys], sizeof(double) * n, cudaMemcpyDeviceToHost, c->stream));
+    OVS_CUDA_TRY(cudaStreamSynchronize(c->stream));
+  }
+  if (info) *info = si;
+  return OVS_OK;
+}
+
+int ovs_newton_update(ovs_ctx* c, int sys) {
+  if (!sys_ok(c, sys, OVS_FP64)) return OVS_ERR_ARG;
+  if (!c->sol[sys] || !c->have_params) return OVS_ERR_STATE;
+  int st;
+  if ((st = ovs_activate(c))) return st;
+  const ovs_params& p = c->params;
+  newton_update_kernel<<<ovs_grid(c->N, 256, 1 << 30), 256, 0, c->stream>>>(
+      c->N, sys, p.gami * p.delt, p.alfi * p.gami * p.delt, c->sol[sys], c->field[OVS_F_ACG], c->field[OVS_F_UG],
+      c->field[OVS_F_PG], c->field[OVS_F_RPHIG], c->field[OVS_F_PHIG], c->field[OVS_F_RTG], c->field[OVS_F_TG]);
+  ++c->launches;
+  OVS_CUDA_TRY(cudaGetLastError());
+  OVS_CUDA_TRY(cudaStreamSynchronize(c->stream));
+  return OVS_OK;
+}
+
+int ovs_residual_norms(ovs_ctx* c, int prec, double r[4]) {
+  if (!c || !r || (prec != OVS_FP64 && prec != OVS_FP32)) return OVS_ERR_ARG;
+  int st;
+  if ((st = ovs_activate(c))) return st;
+  r[0] = r[1] = r[2] = r[3] = 0.0;
+  const size_t N = c->N;
+  // momentum/continuity/VOF from the NS+VOF system if assembled, else NS
+  int fs = c->sys[OVS_SYS_NSVOF][prec].rhs ? OVS_SYS_NSVOF : (c->sys[OVS_SYS_NS][prec].rhs ? OVS_SYS_NS : 0);
+  double* tmp = nullptr;
+  OVS_CUDA_TRY(cudaMallocAsync(&tmp, sizeof(double) * 5 * N, c->stream));
+  auto sumsq = [&](int sys, int f0, int nf, double* out) -> int {
+    const size_t n = N * nf;
+    if (prec == OVS_FP64)
+      {
+        copy_convert_kernel<double, double><<<ovs_grid(n, 256, 1 << 30), 256, 0, c->stream>>>(
+            (const double*)c->sys[sys][prec].rhs + N * f0, tmp, n);
+        ++c->launches;
+      }
+    else
+      {
+        copy_convert_kernel<float, double><<<ovs_grid(n, 256, 1 << 30), 256, 0, c->stream>>>(
+            (const float*)c->sys[sys][prec].rhs + N * f0, tmp, n);
+        ++c->launches;
+      }
+    return ovs_dot_impl(c, tmp, tmp, n, out);
+  };
+  if (fs) {
+    if ((st = sumsq(fs, 0, 3, &r[0]))) return st;
+    if ((st = sumsq(fs, 3, 1, &r[1]))) return st;
+    if (fs == OVS_SYS_NSVOF && (st = sumsq(fs, 4, 1, &r[2]))) return st;
+  }
+  if (c->sys[OVS_SYS_TEM][prec].rhs && (st = sumsq(OVS_SYS_TEM, 0, 1, &r[3]))) return st;
+  OVS_CUDA_TRY(cudaFreeAsync(tmp, c->stream));
+  OVS_CUDA_TRY(cudaStreamSynchronize(c->stream));
+  return OVS_OK;
+}
+
+int ovs_profile(ovs_ctx* c, int what, int system, int precision, int reps, double* avg_ms) {
+  if (!c || !avg_ms || reps < 1 || (precision != OVS_FP64 && precision != OVS_FP32)) return OVS_ERR_ARG;
+  int st;
+  if ((st = ovs_activate(c))) return st;
+  if (what == OVS_PROF_ASSEMBLE) return ovs_profile_assemble(c, system, precision, reps, avg_ms);
+  if (what != OVS_PROF_SPMV && what != OVS_PROF_MGS) return OVS_ERR_ARG;
+  if (!sys_ok(c, system, precision)) return OVS_ERR_ARG;
+  return ovs_profile_krylov(c, what, system, precision, reps, avg_ms);
+}
+
+int ovs_launch_count(ovs_ctx* c, long long* n) {
+  if (!c || !n) return OVS_ERR_ARG;
+  *n = c->launches;
+  return OVS_OK;
+}
+
+int ovs_last_device_ms(ovs_ctx* c, double* ms) {
+  if (!c || !ms) return OVS_ERR_ARG;
+  *ms = c->last_ms;
+  return OVS_OK;
+}
+
+int ovs_host_alloc(void** p, size_t bytes) {
+  if (!p) return OVS_ERR_ARG;
+  OVS_CUDA_TRY(cudaMallocHost(p, bytes ? bytes : 16));
+  return OVS_OK;
+}
+
+int ovs_host_free(void* p) {
+  if (p) OVS_CUDA_TRY(cudaFreeHost(p));
+  return OVS_OK;
+}
+
+}  // extern "C"

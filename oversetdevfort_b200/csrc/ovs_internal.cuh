@@ -1,0 +1,140 @@
+// Internal declarations of the B200 hot-path library (not part of the ABI).
+#pragma once
+#include <cuda_runtime.h>
+#include <stdint.h>
+#include <stddef.h>
+
+#include "../../include/ovs.h"
+
+#define OVS_MAX_DEG 128        // longest CSR row supported (27*nshl hex bound = 216 not needed)
+#define OVS_MAX_KSPACE 400     // largest Krylov space
+#define OVS_RED_BLOCKS 592     // fixed grid of every deterministic reduction (4 x 148 SMs)
+#define OVS_RED_THREADS 256
+
+#define OVS_CUDA_TRY(expr)                                   \
+  do {                                                       \
+    cudaError_t _e = (expr);                                 \
+    if (_e != cudaSuccess) {                                 \
+      ovs_set_last_cuda_error(_e, #expr, __FILE__, __LINE__); \
+      return OVS_ERR_CUDA;                                   \
+    }                                                        \
+  } while (0)
+
+void ovs_set_last_cuda_error(cudaError_t e, const char* what, const char* file,
+                             int line);
+
+// number of field components per node of each system
+static inline int ovs_sys_nf(int sys) {
+  return sys == OVS_SYS_NS ? 4 : (sys == OVS_SYS_NSVOF ? 5 : 1);
+}
+// matrix values stored per CSR slot
+static inline int ovs_sys_nv(int sys) {
+  return sys == OVS_SYS_NS ? 16 : (sys == OVS_SYS_NSVOF ? 24 : 1);
+}
+
+// Device-side GMRES bookkeeping (one per context, FP64 throughout).
+struct GmresDev {
+  double beta;        // result of the latest Gram-Schmidt dot
+  double epsnrm;      // tol * |P^-1 b|
+  double unorm0;      // |P^-1 b|
+  double ercheck;
+  int iks;            // iterations completed
+  int done;           // cycle finished (converged, breakdown or kspace)
+  int breakdown;
+  int converged;
+  int kspace, kmin;
+  int counter;        // last-block-done counter of the reductions
+  int pad;
+  double H[(OVS_MAX_KSPACE + 1) * OVS_MAX_KSPACE];  // column-major (kspace+1) x kspace
+  double e[OVS_MAX_KSPACE + 1];
+  double cs[OVS_MAX_KSPACE], sn[OVS_MAX_KSPACE];
+  double y[OVS_MAX_KSPACE];
+  double partials[OVS_RED_BLOCKS];
+  double scal[8];     // misc scalar results (norms)
+};
+
+struct SysStore {
+  void* vals = nullptr;   // nnz * nv values (internal slot layout)
+  void* rhs = nullptr;    // nf * N, field-major
+  void* binv = nullptr;   // preconditioner: N*9 (+N pinv +N lsinv), same precision
+  bool have_mat = false, have_rhs = false;
+};
+
+struct ovs_ctx {
+  int device = 0;
+  int num_sms = 148;
+  cudaStream_t stream = nullptr;
+  cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+  int N = 0, E = 0, nshl = 0;
+  // mesh
+  int* ien = nullptr;        // E*nshl, element-major, 0-based
+  int* elm_id = nullptr;     // E
+  uint8_t* ibc = nullptr;    // N bit masks (bit d <=> IBC(:,d+1) == 1)
+  // pattern
+  int* rowptr = nullptr;     // N+1, 0-based
+  int* colidx = nullptr;     // nnz
+  int* diag = nullptr;       // N: slot of the diagonal entry
+  int* n2e_ptr = nullptr;    // N+1
+  int* n2e = nullptr;        // nshl*E: (element << 3) | local index, sorted by element
+  int nnz = 0;
+  int max_deg = 0, max_elem = 0;
+  // nodal state (FP64, reference layout)
+  double* field[OVS_F_COUNT] = {};
+  // alpha-stage node records (16 values per node), per precision
+  void* rec[2] = {nullptr, nullptr};
+  // systems [sys][prec]
+  SysStore sys[4][2];
+  // last solution of each system (FP64, field-major)
+  double* sol[4] = {};
+  // GMRES / solve workspace
+  GmresDev* gm = nullptr;
+  void* basis[2] = {nullptr, nullptr};   // Krylov basis per precision
+  size_t basis_bytes[2] = {0, 0};
+  double* work64 = nullptr;              // 3 vectors of 5N doubles (b, r, x)
+  float* work32 = nullptr;               // 1 vector of 5N floats
+  // status words: [0] negative DetJ count, [1] non-finite flag
+  int* flags = nullptr;
+  unsigned long long* cfl_bits = nullptr;
+  // pinned host mirror
+  int* h_pinned = nullptr;
+  double* h_pinned_d = nullptr;
+  ovs_params params{};
+  bool have_mesh = false, have_pattern = false, have_params = false;
+  long long launches = 0;                // kernels launched by this context
+  double last_ms = 0.0;                  // device time of the last top-level call
+};
+
+// ------------------------------------------------------------ helpers
+int ovs_ensure(void** p, size_t bytes);
+int ovs_activate(ovs_ctx* c);
+
+// pattern.cu
+int ovs_pattern_build(ovs_ctx* c);
+int ovs_pattern_to_host(ovs_ctx* c, int* col, int* row);
+
+// assemble.cu
+int ovs_assemble_impl(ovs_ctx* c, int kernel, int tensor_flag, int prec,
+                      double* cfl);
+
+// spmv.cu / gmres.cu
+int ovs_precond_setup(ovs_ctx* c, int sys, int prec);
+int ovs_spmv_impl(ovs_ctx* c, int sys, int prec, const double* dx,
+                  double* dy);
+int ovs_gmres_ref_impl(ovs_ctx* c, int sys, double tol, int kspace, int kmin,
+                       double* dsol, ovs_gmres_info* info);
+int ovs_solve_impl(ovs_ctx* c, int sys, int mode, double rtol, int kspace,
+                   int max_cycles, ovs_solve_info* info);
+int ovs_update_impl(ovs_ctx* c, int sys);
+int ovs_resnorm_impl(ovs_ctx* c, int prec, double r[4]);
+int ovs_dot_impl(ovs_ctx* c, const double* a, const double* b, size_t n,
+                 double* out);
+int ovs_profile_assemble(ovs_ctx* c, int kernel, int prec, int reps, double* ms);
+int ovs_profile_krylov(ovs_ctx* c, int what, int sys, int prec, int reps, double* ms);
+
+// launch geometry helper
+static inline int ovs_grid(size_t n, int threads, int cap) {
+  size_t g = (n + threads - 1) / threads;
+  if (g < 1) g = 1;
+  if (g > (size_t)cap) g = cap;
+  return (int)g;
+}

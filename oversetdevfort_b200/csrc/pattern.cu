@@ -1,0 +1,235 @@
+// CSR sparsity pattern and node->element map (replaces genSparStruc/Asadj,
+// src/genSparStruc.f90:4-105, and the per-element slot lookups of
+// SparseMatLoc_3D, src/FillSparseMat.f90:4-28).
+//
+// The reference builds, per node, the unique list of nodes that share an
+// element and sorts every row ascending.  The sorted unique set does not
+// depend on the visit order, so it is built here row-parallel: one thread per
+// node walks its elements (node->element map), inserts their nodes into a
+// small sorted array and emits the row.  Two passes (count, scan, fill) keep
+// the output layout identical to the reference's col/row arrays.
+#include "ovs_internal.cuh"
+
+namespace {
+
+constexpr int SCAN_T = 1024;
+
+// ---------------------------------------------------------------- scans
+__global__ void scan_block_kernel(const int* __restrict__ in, int* __restrict__ out,
+                                  int* __restrict__ block_sums, int n) {
+  __shared__ int wsum[32];
+  int i = blockIdx.x * SCAN_T + threadIdx.x;
+  int v = (i < n) ? in[i] : 0;
+  int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  int x = v;
+#pragma unroll
+  for (int o = 1; o < 32; o <<= 1) {
+    int y = __shfl_up_sync(0xffffffffu, x, o);
+    if (lane >= o) x += y;
+  }
+  if (lane == 31) wsum[w] = x;
+  __syncthreads();
+  if (w == 0) {
+    int s = wsum[lane];
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      int y = __shfl_up_sync(0xffffffffu, s, o);
+      if (lane >= o) s += y;
+    }
+    wsum[lane] = s;
+  }
+  __syncthreads();
+  int excl = x - v + (w > 0 ? wsum[w - 1] : 0);
+  if (i < n) out[i] = excl;
+  if (threadIdx.x == SCAN_T - 1) block_sums[blockIdx.x] = excl + v;
+}
+
+__global__ void scan_add_kernel(int* __restrict__ out, const int* __restrict__ offs, int n) {
+  int i = blockIdx.x * SCAN_T + threadIdx.x;
+  if (i < n && blockIdx.x > 0) out[i] += offs[blockIdx.x];
+}
+
+// exclusive scan of n ints (n may be large); tmp needs >= 2*ceil(n/1024)+2 ints
+int exclusive_scan(const int* in, int* out, int n, int* tmp, cudaStream_t s) {
+  int nb = (n + SCAN_T - 1) / SCAN_T;
+  int* sums = tmp;
+  int* sums_scan = tmp + nb + 1;
+  scan_block_kernel<<<nb, SCAN_T, 0, s>>>(in, out, sums, n);
+  if (nb > 1) {
+    int nb2 = (nb + SCAN_T - 1) / SCAN_T;
+    if (nb2 > 1) {
+      // second level recursion (n up to 2^30)
+      int* tmp2 = sums_scan + nb + 1;
+      int st = exclusive_scan(sums, sums_scan, nb, tmp2, s);
+      if (st) return st;
+    } else {
+      int* dummy = sums_scan + nb + 1;
+      scan_block_kernel<<<1, SCAN_T, 0, s>>>(sums, sums_scan, dummy, nb);
+    }
+    scan_add_kernel<<<nb, SCAN_T, 0, s>>>(out, sums_scan, n);
+  }
+  return cudaGetLastError() == cudaSuccess ? 0 : OVS_ERR_CUDA;
+}
+
+// ------------------------------------------------------ node -> element map
+__global__ void count_n2e_kernel(const int* __restrict__ ien, int E, int nshl,
+                                 int N, int* __restrict__ cnt, int* __restrict__ bad) {
+  size_t t = blockIdx.x * (size_t)blockDim.x + threadIdx.x;
+  if (t >= (size_t)E * nshl) return;
+  int node = ien[t];
+  if (node < 0 || node >= N) { atomicAdd(bad, 1); return; }
+  atomicAdd(&cnt[node], 1);
+}
+
+__global__ void fill_n2e_kernel(const int* __restrict__ ien, int E, int nshl, int N,
+                                int* __restrict__ cursor, int* __restrict__ n2e) {
+  size_t t = blockIdx.x * (size_t)blockDim.x + threadIdx.x;
+  if (t >= (size_t)E * nshl) return;
+  int node = ien[t];
+  if (node < 0 || node >= N) return;
+  int e = (int)(t / nshl), a = (int)(t % nshl);
+  int pos = atomicAdd(&cursor[node], 1);
+  n2e[pos] = (e << 3) | a;
+}
+
+// sort every node's element list by element id (insertion sort; lists are short)
+__global__ void sort_n2e_kernel(const int* __restrict__ ptr, int* __restrict__ n2e, int N,
+                                int* __restrict__ max_elem) {
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= N) return;
+  int b = ptr[i], e = ptr[i + 1];
+  for (int k = b + 1; k < e; ++k) {
+    int v = n2e[k];
+    int j = k - 1;
+    while (j >= b && n2e[j] > v) { n2e[j + 1] = n2e[j]; --j; }
+    n2e[j + 1] = v;
+  }
+  atomicMax(max_elem, e - b);
+}
+
+// Collect the sorted unique neighbour list of node i into buf (local memory).
+__device__ int collect_row(int i, const int* __restrict__ ien, int nshl,
+                           const int* __restrict__ ptr, const int* __restrict__ n2e,
+                           int* buf) {
+  int len = 0;
+  for (int k = ptr[i]; k < ptr[i + 1]; ++k) {
+    int e = n2e[k] >> 3;
+    for (int a = 0; a < nshl; ++a) {
+      int nd = ien[(size_t)e * nshl + a];
+      // binary search for nd in buf[0,len)
+      int lo = 0, hi = len;
+      while (lo < hi) {
+        int mid = (lo + hi) >> 1;
+        if (buf[mid] < nd) lo = mid + 1; else hi = mid;
+      }
+      if (lo < len && buf[lo] == nd) continue;
+      if (len >= OVS_MAX_DEG) return -1;
+      for (int t = len; t > lo; --t) buf[t] = buf[t - 1];
+      buf[lo] = nd;
+      ++len;
+    }
+  }
+  return len;
+}
+
+__global__ void row_len_kernel(const int* __restrict__ ien, int nshl, int N,
+                               const int* __restrict__ ptr, const int* __restrict__ n2e,
+                               int* __restrict__ rowlen, int* __restrict__ flags,
+                               int* __restrict__ max_deg) {
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= N) return;
+  int buf[OVS_MAX_DEG];
+  int len = collect_row(i, ien, nshl, ptr, n2e, buf);
+  if (len < 0) { atomicOr(flags, 1); len = 0; }
+  rowlen[i] = len;
+  atomicMax(max_deg, len);
+}
+
+__global__ void row_fill_kernel(const int* __restrict__ ien, int nshl, int N,
+                                const int* __restrict__ ptr, const int* __restrict__ n2e,
+                                const int* __restrict__ rowptr, int* __restrict__ colidx,
+                                int* __restrict__ diag) {
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= N) return;
+  int buf[OVS_MAX_DEG];
+  int len = collect_row(i, ien, nshl, ptr, n2e, buf);
+  int base = rowptr[i];
+  int d = -1;
+  for (int k = 0; k < len; ++k) {
+    colidx[base + k] = buf[k];
+    if (buf[k] == i) d = base + k;
+  }
+  diag[i] = d;
+}
+
+__global__ void to_one_based_kernel(const int* __restrict__ in, int* __restrict__ out, size_t n) {
+  size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x;
+  if (i < n) out[i] = in[i] + 1;
+}
+
+}  // namespace
+
+int ovs_pattern_to_host(ovs_ctx* c, int* col, int* row) {
+  cudaStream_t s = c->stream;
+  size_t n1 = (size_t)c->N + 1, n2 = (size_t)c->nnz;
+  int* tmp = nullptr;
+  OVS_CUDA_TRY(cudaMallocAsync(&tmp, sizeof(int) * (n1 > n2 ? n1 : n2), s));
+  to_one_based_kernel<<<ovs_grid(n1, 256, 1 << 30), 256, 0, s>>>(c->rowptr, tmp, n1);
+  OVS_CUDA_TRY(cudaMemcpyAsync(col, tmp, sizeof(int) * n1, cudaMemcpyDeviceToHost, s));
+  if (row && n2) {
+    to_one_based_kernel<<<ovs_grid(n2, 256, 1 << 30), 256, 0, s>>>(c->colidx, tmp, n2);
+    OVS_CUDA_TRY(cudaMemcpyAsync(row, tmp, sizeof(int) * n2, cudaMemcpyDeviceToHost, s));
+  }
+  OVS_CUDA_TRY(cudaFreeAsync(tmp, s));
+  OVS_CUDA_TRY(cudaStreamSynchronize(s));
+  return OVS_OK;
+}
+
+int ovs_pattern_build(ovs_ctx* c) {
+  cudaStream_t s = c->stream;
+  const int N = c->N, E = c->E, nshl = c->nshl;
+  const size_t EN = (size_t)E * nshl;
+  int st;
+  if ((st = ovs_ensure((void**)&c->n2e_ptr, sizeof(int) * (N + 1)))) return st;
+  if ((st = ovs_ensure((void**)&c->n2e, sizeof(int) * EN))) return st;
+  if ((st = ovs_ensure((void**)&c->rowptr, sizeof(int) * (N + 1)))) return st;
+  if ((st = ovs_ensure((void**)&c->diag, sizeof(int) * N))) return st;
+  int *cnt = nullptr, *tmp = nullptr, *stats = nullptr;
+  const int nb = (N + 1 + SCAN_T - 1) / SCAN_T;
+  const size_t tmp_ints = 4 * (size_t)nb + 64;
+  OVS_CUDA_TRY(cudaMallocAsync(&cnt, sizeof(int) * (N + 1), s));
+  OVS_CUDA_TRY(cudaMallocAsync(&tmp, sizeof(int) * tmp_ints, s));
+  OVS_CUDA_TRY(cudaMallocAsync(&stats, sizeof(int) * 8, s));
+  OVS_CUDA_TRY(cudaMemsetAsync(cnt, 0, sizeof(int) * (N + 1), s));
+  OVS_CUDA_TRY(cudaMemsetAsync(stats, 0, sizeof(int) * 8, s));
+  // stats: [0] bad node ids, [1] row overflow, [2] max elements per node, [3] max degree
+  count_n2e_kernel<<<ovs_grid(EN, 256, 1 << 30), 256, 0, s>>>(c->ien, E, nshl, N, cnt, stats + 0);
+  if ((st = exclusive_scan(cnt, c->n2e_ptr, N + 1, tmp, s))) return st;
+  OVS_CUDA_TRY(cudaMemcpyAsync(cnt, c->n2e_ptr, sizeof(int) * N, cudaMemcpyDeviceToDevice, s));
+  fill_n2e_kernel<<<ovs_grid(EN, 256, 1 << 30), 256, 0, s>>>(c->ien, E, nshl, N, cnt, c->n2e);
+  sort_n2e_kernel<<<ovs_grid(N, 128, 1 << 30), 128, 0, s>>>(c->n2e_ptr, c->n2e, N, stats + 2);
+  row_len_kernel<<<ovs_grid(N, 128, 1 << 30), 128, 0, s>>>(c->ien, nshl, N, c->n2e_ptr, c->n2e,
+                                                           cnt, stats + 1, stats + 3);
+  OVS_CUDA_TRY(cudaMemsetAsync(cnt + N, 0, sizeof(int), s));
+  if ((st = exclusive_scan(cnt, c->rowptr, N + 1, tmp, s))) return st;
+  int h[8];
+  OVS_CUDA_TRY(cudaMemcpyAsync(h, stats, sizeof(int) * 8, cudaMemcpyDeviceToHost, s));
+  int nnz = 0;
+  OVS_CUDA_TRY(cudaMemcpyAsync(&nnz, c->rowptr + N, sizeof(int), cudaMemcpyDeviceToHost, s));
+  OVS_CUDA_TRY(cudaStreamSynchronize(s));
+  if (h[0] != 0) { cudaFreeAsync(cnt, s); cudaFreeAsync(tmp, s); cudaFreeAsync(stats, s); return OVS_ERR_ARG; }
+  if (h[1] != 0) { cudaFreeAsync(cnt, s); cudaFreeAsync(tmp, s); cudaFreeAsync(stats, s); return OVS_ERR_PATTERN; }
+  c->max_elem = h[2];
+  c->max_deg = h[3];
+  c->nnz = nnz;
+  if ((st = ovs_ensure((void**)&c->colidx, sizeof(int) * (size_t)(nnz > 0 ? nnz : 1)))) return st;
+  row_fill_kernel<<<ovs_grid(N, 128, 1 << 30), 128, 0, s>>>(c->ien, nshl, N, c->n2e_ptr, c->n2e,
+                                                            c->rowptr, c->colidx, c->diag);
+  OVS_CUDA_TRY(cudaFreeAsync(cnt, s));
+  OVS_CUDA_TRY(cudaFreeAsync(tmp, s));
+  OVS_CUDA_TRY(cudaFreeAsync(stats, s));
+  OVS_CUDA_TRY(cudaStreamSynchronize(s));
+  OVS_CUDA_TRY(cudaGetLastError());
+  c->have_pattern = true;
+  return OVS_OK;
+}

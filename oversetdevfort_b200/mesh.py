@@ -1,0 +1,276 @@
+"""Synthetic structured meshes and the benchmark configurations.
+
+The reference reads METIS-partitioned gmsh meshes (``part.N.dat``); none
+ship with it, so the workloads are generated here: structured boxes with
+lexicographic node numbering (x fastest), each cell split into 6 Kuhn
+tetrahedra sharing the (0,0,0)-(1,1,1) diagonal, or kept as trilinear hexes.
+Arrays use the reference conventions: ``xg`` is (N,3) Fortran-ordered,
+``ien`` is (E,nshl) Fortran-ordered with 1-based node ids, ``ibc`` is
+(N,8) with columns 1-3 velocity, 4 pressure, 5 VOF, 6 temperature
+(``setBCs_NSVOF``/``setBCs_Tem``, src/setBCs.f90:172-278).
+"""
+from __future__ import annotations
+
+from dataclasses import dataclass, field
+import math
+
+import numpy as np
+
+from . import _ffi as F
+
+# Kuhn split: permutation of the axes walked from (0,0,0) to (1,1,1) and its sign
+_PERMS = [((0, 1, 2), 1), ((0, 2, 1), -1), ((1, 0, 2), -1),
+          ((1, 2, 0), 1), ((2, 0, 1), 1), ((2, 1, 0), -1)]
+# trilinear hex local nodes of linhexshl (src/eval_shape_FEM.f90:148-196) as
+# cell-corner offsets: node a sits at xi = 2*offset - 1
+_HEX = [(0, 1, 0), (1, 1, 0), (1, 1, 1), (0, 1, 1), (0, 0, 0), (1, 0, 0), (1, 0, 1), (0, 0, 1)]
+
+
+@dataclass
+class Mesh:
+    xg: np.ndarray            # (N,3) float64, Fortran order
+    ien: np.ndarray           # (E,nshl) int32, Fortran order, 1-based
+    elm_id: np.ndarray        # (E,) int32
+    faces: list               # 6 arrays of 0-based node ids: x0, x1, y0, y1, z0, z1
+    dims: tuple               # (nx, ny, nz)
+    lengths: tuple
+
+    @property
+    def nnode(self) -> int:
+        return self.xg.shape[0]
+
+    @property
+    def nelem(self) -> int:
+        return self.ien.shape[0]
+
+    @property
+    def nshl(self) -> int:
+        return self.ien.shape[1]
+
+
+def _grid(nx, ny, nz, lx, ly, lz):
+    xs = np.linspace(0.0, lx, nx + 1)
+    ys = np.linspace(0.0, ly, ny + 1)
+    zs = np.linspace(0.0, lz, nz + 1)
+    Z, Y, X = np.meshgrid(zs, ys, xs, indexing="ij")
+    xg = np.asfortranarray(np.stack([X.ravel(), Y.ravel(), Z.ravel()], axis=1))
+    nid = lambda i, j, k: i + (nx + 1) * (j + (ny + 1) * k)
+    k, j, i = np.meshgrid(np.arange(nz), np.arange(ny), np.arange(nx), indexing="ij")
+    i, j, k = i.ravel(), j.ravel(), k.ravel()
+    faces = []
+    I, J, K = np.meshgrid(np.arange(nx + 1), np.arange(ny + 1), np.arange(nz + 1), indexing="ij")
+    allid = nid(I, J, K)
+    for ax, val in ((0, 0), (0, nx), (1, 0), (1, ny), (2, 0), (2, nz)):
+        sel = [I, J, K][ax] == val
+        faces.append(np.sort(allid[sel].ravel()).astype(np.int64))
+    return xg, nid, i, j, k, faces
+
+
+def box_tet(nx, ny, nz, lx=1.0, ly=1.0, lz=1.0) -> Mesh:
+    """Box of nx*ny*nz cells, 6 positively oriented Kuhn tets per cell."""
+    xg, nid, i, j, k, faces = _grid(nx, ny, nz, lx, ly, lz)
+    ncell = i.size
+    ien = np.empty((ncell, 6, 4), dtype=np.int64)
+    for t, (perm, sign) in enumerate(_PERMS):
+        p = [np.zeros(3, dtype=int)]
+        for ax in perm:
+            q = p[-1].copy()
+            q[ax] += 1
+            p.append(q)
+        P0, P1, P2, P3 = p
+        # reference ordering: DetJ = det[x1-x4, x2-x4, x3-x4]; (P1,P2,P3,P0) has sign(perm)
+        order = [P1, P2, P3, P0] if sign > 0 else [P2, P1, P3, P0]
+        for a, off in enumerate(order):
+            ien[:, t, a] = nid(i + off[0], j + off[1], k + off[2])
+    ien = np.asfortranarray(ien.reshape(ncell * 6, 4).astype(np.int32) + 1)
+    elm = np.full(ien.shape[0], 102, dtype=np.int32)
+    return Mesh(xg, ien, elm, faces, (nx, ny, nz), (lx, ly, lz))
+
+
+def box_hex(nx, ny, nz, lx=1.0, ly=1.0, lz=1.0) -> Mesh:
+    """Box of nx*ny*nz trilinear hexahedra with linhexshl node order."""
+    xg, nid, i, j, k, faces = _grid(nx, ny, nz, lx, ly, lz)
+    ien = np.empty((i.size, 8), dtype=np.int64)
+    for a, off in enumerate(_HEX):
+        ien[:, a] = nid(i + off[0], j + off[1], k + off[2])
+    ien = np.asfortranarray(ien.astype(np.int32) + 1)
+    elm = np.full(ien.shape[0], 102, dtype=np.int32)
+    return Mesh(xg, ien, elm, faces, (nx, ny, nz), (lx, ly, lz))
+
+
+def expected_nnz_kuhn(nx, ny, nz) -> int:
+    """Closed-form nnz of the Kuhn-split pattern: every node couples to itself
+    and to the neighbours along the 7 edge directions +-{x,y,z,xy,xz,yz,xyz}
+    present in the split (edge count times two plus N)."""
+    N = (nx + 1) * (ny + 1) * (nz + 1)
+    edges = (nx * (ny + 1) * (nz + 1) + (nx + 1) * ny * (nz + 1) + (nx + 1) * (ny + 1) * nz  # axis
+             + nx * ny * (nz + 1) + nx * (ny + 1) * nz + (nx + 1) * ny * nz                 # face diagonals
+             + nx * ny * nz)                                                                 # body diagonal
+    return N + 2 * edges
+
+
+def expected_nnz_hex(nx, ny, nz) -> int:
+    cnt = lambda n: np.array([min(i, 1) + 1 + min(n - i, 1) for i in range(n + 1)])
+    return int(cnt(nx).sum() * cnt(ny).sum() * cnt(nz).sum())
+
+
+# --------------------------------------------------------------------- configs
+@dataclass
+class Case:
+    name: str
+    mesh: Mesh
+    params: dict
+    state: dict               # field name -> ndarray (reference layout)
+    ibc: np.ndarray           # (N,8) int32 Fortran order
+    kernel: int               # OVS_ASM_NS or OVS_ASM_NSVOF (+TEM pass)
+    kspace: int = 50
+    gmres_tol: float = 1e-6
+    newton_iters: int = 1
+    extra: dict = field(default_factory=dict)
+
+
+def genalpha(rhoinf: float) -> dict:
+    """src/param.f90:469-480"""
+    if rhoinf < 0.0 or rhoinf > 1.0:
+        return dict(almi=1.0, alfi=1.0, gami=1.0, beti=1.0)
+    almi = (3.0 - rhoinf) / (1.0 + rhoinf) / 2.0
+    alfi = 1.0 / (1.0 + rhoinf)
+    gami = 0.5 + almi - alfi
+    beti = 0.25 * (1.0 + almi - alfi) * (1.0 + almi - alfi)
+    return dict(almi=almi, alfi=alfi, gami=gami, beti=beti)
+
+
+def base_params(**kw) -> dict:
+    p = dict(delt=1e-3, rhow=1000.0, rhoa=1.0, rhos=2700.0, muw=1e-3, mua=1e-5, mus=1.0,
+             cpw=4180.0, cpa=1000.0, cps=900.0, kappaw=0.6, kappaa=0.03, kappas=200.0,
+             ts=373.0, lh=2.26e6, c_evap=0.0, c_cond=0.0, c_dmdot=1.0, ns_kdc_w=0.0,
+             ns_kdc_a=0.0, lsc_kdc=0.0, tem_kdc=0.0, tref=1.0, gravvec=(0.0, 0.0, -9.81),
+             fluid_elm_id=102, subdomain_flag=1, elm_id_set=(102, 0))
+    p.update(genalpha(0.5))
+    p.update(kw)
+    return p
+
+
+def to_ovs_params(p: dict) -> F.OvsParams:
+    o = F.OvsParams()
+    for n in F.PARAM_DOUBLES:
+        setattr(o, n, float(p[n]))
+    for d in range(3):
+        o.gravvec[d] = float(p["gravvec"][d])
+    o.fluid_elm_id = int(p["fluid_elm_id"])
+    o.subdomain_flag = int(p["subdomain_flag"])
+    o.elm_id_set[0] = int(p["elm_id_set"][0])
+    o.elm_id_set[1] = int(p["elm_id_set"][1])
+    return o
+
+
+def empty_state(N: int) -> dict:
+    return {n: np.zeros((N, 3) if F.FIELD_WIDTH[n] == 3 else N, order="F")
+            for n in F.FIELDS if n != "xg"}
+
+
+def _apply_dirichlet_u(st, p, nodes, value):
+    """setBCs_NSVOF velocity part (src/setBCs.f90:210-220)."""
+    g, dt = p["gami"], p["delt"]
+    for d in range(3):
+        st["ug"][nodes, d] = value[d]
+        st["acg"][nodes, d] = ((st["ug"][nodes, d] - st["ugold"][nodes, d]) / dt
+                               + (g - 1.0) * st["acgold"][nodes, d]) / g
+
+
+def config1(n: int = 16, seed: int = 1, rhoinf: float = 0.5) -> Case:
+    """Plain NS lid-driven cavity on an n^3 x6-tet unit cube (NS-only path)."""
+    m = box_tet(n, n, n)
+    p = base_params(delt=0.01, rhoa=1.0, mua=0.01, rhow=1.0, muw=0.01)
+    p.update(genalpha(rhoinf))
+    N = m.nnode
+    st = empty_state(N)
+    rng = np.random.default_rng(seed)
+    st["ugold"][:] = rng.uniform(-0.01, 0.01, size=(N, 3))
+    st["ug"][:] = st["ugold"]                       # predictor ug = ugold
+    st["acg"][:] = (p["gami"] - 1.0) / p["gami"] * st["acgold"]
+    ibc = np.zeros((N, 8), dtype=np.int32, order="F")
+    for f in range(6):                               # faces in order, lid (z=1) last
+        nodes = m.faces[f]
+        ibc[nodes, 0:3] = 1
+        _apply_dirichlet_u(st, p, nodes, (1.0, 0.0, 0.0) if f == 5 else (0.0, 0.0, 0.0))
+    return Case("config1_ns_cavity_16", m, p, st, ibc, F.OVS_ASM_NS, kspace=50, gmres_tol=1e-6)
+
+
+def quench_case(m: Mesh, name: str, seed: int = 2, hot_side: float = 0.4) -> Case:
+    """NS+VOF+T quench physics (configs 2, 3, 5): interface phi =
+    tanh((z - H/2)/0.02) (phi = 1 is gas, src/solveQuenching.f90:353), a hot
+    centred cube, no-slip walls, natural temperature BCs, fluid at rest."""
+    p = base_params()
+    N = m.nnode
+    st = empty_state(N)
+    lx, ly, lz = m.lengths
+    z = m.xg[:, 2]
+    phi = np.tanh((z - 0.5 * lz) / 0.02)
+    st["phig"][:] = phi
+    st["phigold"][:] = phi
+    c = np.array([0.5 * lx, 0.5 * ly, 0.5 * lz])
+    hot = np.all(np.abs(m.xg - c) <= 0.5 * hot_side + 1e-12, axis=1)
+    T = np.where(hot, 1000.0, 300.0)
+    st["tg"][:] = T
+    st["tgold"][:] = T
+    ibc = np.zeros((N, 8), dtype=np.int32, order="F")
+    for f in range(6):
+        ibc[m.faces[f], 0:3] = 1
+        _apply_dirichlet_u(st, p, m.faces[f], (0.0, 0.0, 0.0))
+    return Case(name, m, p, st, ibc, F.OVS_ASM_NSVOF, kspace=50, gmres_tol=1e-6, newton_iters=3)
+
+
+def config2() -> Case:
+    return quench_case(box_tet(48, 48, 96, 1.0, 1.0, 2.0), "config2_quench_48x48x96")
+
+
+def config3(n: int = 128) -> Case:
+    return quench_case(box_tet(n, n, n), f"config3_quench_{n}cube")
+
+
+def config5(n: int = 32) -> Case:
+    return quench_case(box_tet(n, n, n), f"config5_quench_{n}cube")
+
+
+def random_case(nx=4, ny=3, nz=3, seed=0, kernel=F.OVS_ASM_NSVOF, solid_frac=0.15,
+                bc_frac=0.2, phase_change=True) -> Case:
+    """Small case with every code path switched on: random state fields,
+    mesh motion, mixed fluid/solid elements, random Dirichlet flags in all
+    six IBC columns, phase change and discontinuity capturing."""
+    rng = np.random.default_rng(seed)
+    m = box_tet(nx, ny, nz, 1.0, 0.8, 0.9)
+    N, E = m.nnode, m.nelem
+    h = min(1.0 / nx, 0.8 / ny, 0.9 / nz)
+    p = base_params(delt=rng.uniform(5e-4, 2e-3), c_evap=0.3 if phase_change else 0.0,
+                    c_cond=0.2 if phase_change else 0.0, c_dmdot=0.7,
+                    lsc_kdc=0.05, tem_kdc=0.02, tref=400.0,
+                    # NS_kdc is a real multiplier on the NS-only path but reaches an
+                    # INTEGER dummy on the quench path (see e3DC_beta2), where its
+                    # value is the low word of a double and not reproducible across
+                    # roundings; keep it to the NS-only cases
+                    ns_kdc_a=0.001 if kernel == F.OVS_ASM_NS else 0.0,
+                    rhow=1000.0, rhoa=1.2, muw=1e-3, mua=2e-5,
+                    subdomain_flag=3, elm_id_set=(102, 103))
+    p.update(genalpha(rng.uniform(0.2, 0.9)))
+    st = empty_state(N)
+    for n in ("ug", "ugold", "ugm", "ugmold"):
+        st[n][:] = rng.uniform(-1, 1, size=(N, 3)) * (0.1 if "ugm" in n else 1.0)
+    for n in ("acg", "acgold", "acgm", "acgmold"):
+        st[n][:] = rng.uniform(-5, 5, size=(N, 3))
+    for n in ("dg", "dgold"):
+        st[n][:] = rng.uniform(-0.05, 0.05, size=(N, 3)) * h
+    st["pg"][:] = rng.uniform(-100, 100, N)
+    for n in ("phig", "phigold"):
+        st[n][:] = rng.uniform(-0.3, 1.3, N)
+    for n in ("rphig", "rphigold"):
+        st[n][:] = rng.uniform(-2, 2, N)
+    for n in ("tg", "tgold"):
+        st[n][:] = rng.uniform(300, 450, N)
+    for n in ("rtg", "rtgold"):
+        st[n][:] = rng.uniform(-50, 50, N)
+    m.elm_id[:] = np.where(rng.random(E) < solid_frac, 101, 102)
+    m.elm_id[rng.random(E) < 0.1] = 103
+    ibc = (rng.random((N, 8)) < bc_frac).astype(np.int32)
+    ibc = np.asfortranarray(ibc)
+    return Case(f"random_{nx}x{ny}x{nz}_s{seed}", m, p, st, ibc, kernel, kspace=30, gmres_tol=1e-8)

@@ -1,0 +1,66 @@
+"""The C-ABI library builds for sm_100a, loads, and exports every entry point
+declared in include/ovs.h (CPU only; no compute call is made)."""
+import ctypes
+import re
+from pathlib import Path
+
+import numpy as np
+
+from oversetdevfort_b200 import _ffi as F
+from oversetdevfort_b200 import mesh as M
+
+ROOT = Path(__file__).resolve().parent.parent
+
+
+def _declared():
+    txt = (ROOT / "include" / "ovs.h").read_text()
+    txt = re.sub(r"/\*.*?\*/", "", txt, flags=re.S)
+    return sorted(set(re.findall(r"\b(?:int|const char\*)\s+(ovs_\w+)\s*\(", txt)))
+
+
+def test_header_declarations_exported(lib):
+    names = _declared()
+    assert len(names) >= 20
+    for n in names:
+        assert hasattr(lib, n), f"{n} declared in ovs.h but not exported"
+    assert sorted(F.EXPORTS) == names, "ctypes signature table out of sync with ovs.h"
+
+
+def test_library_is_sm100a_build(lib):
+    # the fat binary carries sm_100a code only (checked on the object list)
+    from oversetdevfort_b200 import build
+    assert "arch=compute_100a,code=sm_100a" in " ".join(build.ARCH)
+    assert build.LIB.exists()
+
+
+def test_status_strings(lib):
+    for s in (0, 1, -1, -2, -3, -4, -5, -6, -7, -8):
+        assert lib.ovs_status_string(s)
+    assert lib.ovs_version() >= 10000
+
+
+def test_create_argument_errors(lib):
+    h = ctypes.c_void_p()
+    bad = F.OvsDims(0, 10, 4, 0)
+    assert lib.ovs_create(ctypes.byref(h), ctypes.byref(bad)) == F.OVS_ERR_ARG
+    bad = F.OvsDims(10, 10, 5, 0)
+    assert lib.ovs_create(ctypes.byref(h), ctypes.byref(bad)) == F.OVS_ERR_ARG
+    assert lib.ovs_destroy(None) == 0
+
+
+def test_params_struct_layout():
+    # 30 doubles then 4 ints: offsets must match the C struct
+    assert ctypes.sizeof(F.OvsParams) == 30 * 8 + 4 * 4
+    assert F.OvsParams.gravvec.offset == 27 * 8
+    assert F.OvsParams.fluid_elm_id.offset == 30 * 8
+
+
+def test_mesh_generator_counts():
+    m = M.box_tet(4, 3, 2)
+    assert m.nnode == 5 * 4 * 3 and m.nelem == 6 * 24
+    assert m.ien.min() == 1 and m.ien.max() == m.nnode
+    assert all(len(f) > 0 for f in m.faces)
+    c = M.config1(n=4)
+    assert c.ibc[:, :3].sum() > 0 and c.ibc[:, 3:].sum() == 0
+    lid = c.mesh.faces[5]
+    np.testing.assert_array_equal(c.state["ug"][lid, 0], 1.0)

@@ -1,0 +1,332 @@
+"""GPU parity: every product entry point, called through the C ABI, against
+the CPU oracle on the same seeded inputs (and against the committed golden
+fixture).
+
+Tolerances (normwise per block, |gpu - ref|_max <= tol * |ref|_max):
+  * CSR pattern, slot maps, iteration counts: bit-exact / equal;
+  * FP64 assembly, SpMV, GMRES: 1e-12 (assembly) / 1e-13 (SpMV) / 1e-10
+    (GMRES solution, which amplifies the rounding differences of the
+    assembly by the condition of the Krylov process);
+  * FP32 assembly: 1e-5.
+"""
+import ctypes
+from pathlib import Path
+
+import numpy as np
+import pytest
+
+from oversetdevfort_b200 import _ffi as F
+from oversetdevfort_b200 import mesh as M
+from oversetdevfort_b200.api import (Context, genSparStruc, assembleQuenching, assembleNavSto,
+                                     SparseGMRES_up, SparseGMRES_ns_conv, SparseGMRES_tem, SYS_BLOCKS,
+                                     BLOCK_NAME)
+
+pytestmark = pytest.mark.gpu
+
+GOLDEN = Path(__file__).resolve().parent / "golden" / "quench_small.npz"
+KIND = {F.OVS_SYS_NS: "ns", F.OVS_SYS_NSVOF: "nsvof", F.OVS_SYS_TEM: "tem"}
+
+
+def close(gpu, ref, tol, what=""):
+    gpu, ref = np.asarray(gpu, dtype=np.float64), np.asarray(ref, dtype=np.float64)
+    assert gpu.shape == ref.shape, (what, gpu.shape, ref.shape)
+    scale = max(np.abs(ref).max(initial=0.0), 1e-300)
+    err = np.abs(gpu - ref).max(initial=0.0)
+    assert err <= tol * scale, f"{what}: max err {err:.3e} vs scale {scale:.3e} (tol {tol})"
+    return err / scale
+
+
+def _ctx(case):
+    return Context.from_case(case)
+
+
+# --------------------------------------------------------------- pattern
+@pytest.mark.parametrize("mk", [lambda: M.box_tet(16, 16, 16), lambda: M.box_tet(4, 3, 3),
+                                lambda: M.box_tet(7, 1, 3, 2.0, 0.5, 1.0), lambda: M.box_hex(3, 3, 2),
+                                lambda: M.box_tet(1, 1, 1)])
+def test_pattern_bit_exact(oracle, mk):
+    m = mk()
+    col_o, row_o = oracle.gen_spar_struc(m.ien, m.nnode)
+    col_g, row_g = genSparStruc(m.ien, m.nnode)
+    np.testing.assert_array_equal(col_g, col_o)
+    np.testing.assert_array_equal(row_g, row_o)
+
+
+def test_pattern_config2_size():
+    m = M.box_tet(48, 48, 96, 1.0, 1.0, 2.0)
+    col, row = genSparStruc(m.ien, m.nnode)
+    assert m.nnode == 232897 and len(row) == 3398977 == M.expected_nnz_kuhn(48, 48, 96)
+    assert np.all(np.diff(col) > 0)
+
+
+# -------------------------------------------------------------- assembly
+def _assemble_both(oracle, case, kernel, tensor_flag, prec):
+    oc = oracle.OracleCase(case)
+    ctx = _ctx(case)
+    if kernel == F.OVS_ASM_NS:
+        cfl_o = oc.assemble_navsto(tensor_flag)
+        cfl_g = assembleNavSto(ctx, tensor_flag, prec)
+        sysid, kind = F.OVS_SYS_NS, "ns"
+    elif kernel == F.OVS_ASM_NSVOF:
+        cfl_o = oc.assemble_quenching(tensor_flag, 3)
+        cfl_g = assembleQuenching(ctx, tensor_flag, 3, prec)
+        sysid, kind = F.OVS_SYS_NSVOF, "nsvof"
+    else:
+        cfl_o = oc.assemble_quenching(tensor_flag, 4)
+        cfl_g = assembleQuenching(ctx, tensor_flag, 4, prec)
+        sysid, kind = F.OVS_SYS_TEM, "tem"
+    return oc, ctx, sysid, kind, cfl_o, cfl_g
+
+
+def _compare_system(oc, ctx, sysid, kind, tensor_flag, prec, tol):
+    ref = oc.system(kind)
+    if tensor_flag & F.OVS_TENSOR_MAT:
+        for b in SYS_BLOCKS[sysid]:
+            name = BLOCK_NAME[b]
+            close(ctx.get_lhs(sysid, prec, b), ref[name], tol, f"{kind}.{name}")
+    if tensor_flag & F.OVS_TENSOR_VEC:
+        g = ctx.get_rhs(sysid, prec)
+        for f in range(g.shape[1]):
+            close(g[:, f], ref["rhs"][:, f], tol, f"{kind}.rhs[{f}]")
+
+
+CASES = [("nsvof", s) for s in (0, 1, 2)] + [("tem", s) for s in (0, 1)] + [("ns", s) for s in (0, 1)]
+
+
+@pytest.mark.parametrize("kind,seed", CASES)
+@pytest.mark.parametrize("tflag", [6, 4, 2])
+def test_assembly_fp64_random(oracle, kind, seed, tflag):
+    kernel = {"nsvof": F.OVS_ASM_NSVOF, "tem": F.OVS_ASM_TEM, "ns": F.OVS_ASM_NS}[kind]
+    case = M.random_case(nx=4 + seed, ny=3, nz=3 - (seed % 2), seed=seed, kernel=kernel)
+    oc, ctx, sysid, k, cfl_o, cfl_g = _assemble_both(oracle, case, kernel, tflag, F.OVS_FP64)
+    assert abs(cfl_g - cfl_o) <= 1e-12 * max(cfl_o, 1e-300)
+    _compare_system(oc, ctx, sysid, k, tflag, F.OVS_FP64, 1e-12)
+
+
+@pytest.mark.parametrize("kind,seed", CASES)
+def test_assembly_fp32_random(oracle, kind, seed):
+    kernel = {"nsvof": F.OVS_ASM_NSVOF, "tem": F.OVS_ASM_TEM, "ns": F.OVS_ASM_NS}[kind]
+    case = M.random_case(nx=4 + seed, ny=3, nz=3, seed=seed, kernel=kernel)
+    oc, ctx, sysid, k, cfl_o, cfl_g = _assemble_both(oracle, case, kernel, 6, F.OVS_FP32)
+    _compare_system(oc, ctx, sysid, k, 6, F.OVS_FP32, 1e-5)
+
+
+def test_assembly_config1_fp64_and_fp32(oracle):
+    case = M.config1()
+    oc, ctx, sysid, k, cfl_o, cfl_g = _assemble_both(oracle, case, F.OVS_ASM_NS, 6, F.OVS_FP64)
+    assert abs(cfl_g - cfl_o) <= 1e-12 * cfl_o
+    _compare_system(oc, ctx, sysid, k, 6, F.OVS_FP64, 1e-12)
+    assembleNavSto(ctx, 6, F.OVS_FP32)
+    _compare_system(oc, ctx, sysid, k, 6, F.OVS_FP32, 1e-5)
+
+
+def test_assembly_quench_config_fp64(oracle):
+    case = M.quench_case(M.box_tet(10, 10, 12, 1.0, 1.0, 1.2), "q10")
+    for kernel in (F.OVS_ASM_NSVOF, F.OVS_ASM_TEM):
+        oc, ctx, sysid, k, cfl_o, cfl_g = _assemble_both(oracle, case, kernel, 6, F.OVS_FP64)
+        _compare_system(oc, ctx, sysid, k, 6, F.OVS_FP64, 1e-12)
+        ctx.assemble(kernel, 6, F.OVS_FP32)
+        _compare_system(oc, ctx, sysid, k, 6, F.OVS_FP32, 1e-5)
+
+
+def test_assembly_against_golden_fixture():
+    g = np.load(GOLDEN)
+    case = M.random_case(nx=3, ny=2, nz=2, seed=11)
+    ctx = _ctx(case)
+    col, row = ctx.get_pattern()
+    np.testing.assert_array_equal(col, g["q_col"])
+    np.testing.assert_array_equal(row, g["q_row"])
+    cfl = assembleQuenching(ctx, 6, 7)
+    assert abs(cfl - g["q_cfl"][0]) <= 1e-12 * g["q_cfl"][0]
+    for b in SYS_BLOCKS[F.OVS_SYS_NSVOF]:
+        close(ctx.get_lhs(F.OVS_SYS_NSVOF, F.OVS_FP64, b), g["q_" + BLOCK_NAME[b]], 1e-12, BLOCK_NAME[b])
+    close(ctx.get_lhs(F.OVS_SYS_TEM, F.OVS_FP64, F.OVS_BLK_TEM), g["q_TEM"], 1e-12, "TEM")
+    r = ctx.get_rhs(F.OVS_SYS_NSVOF)
+    close(r[:, :3], g["q_rhsu"], 1e-12, "rhsu")
+    close(r[:, 3], g["q_rhsp"], 1e-12, "rhsp")
+    close(r[:, 4], g["q_rhsls"], 1e-12, "rhsls")
+    close(ctx.get_rhs(F.OVS_SYS_TEM)[:, 0], g["q_rhstem"], 1e-12, "rhstem")
+    su, sp, sl, info = SparseGMRES_ns_conv(ctx, 1e-8, 20, 1, np.zeros((ctx.N, 3)), np.zeros(ctx.N),
+                                           np.zeros(ctx.N))
+    assert info.iterations == g["q_it_nsvof"][0]
+    close(np.column_stack([su, sp, sl]), g["q_sol_nsvof"], 1e-10, "sol nsvof")
+    st, info = SparseGMRES_tem(ctx, 1e-8, 20, 1, np.zeros(ctx.N))
+    assert info.iterations == g["q_it_tem"][0]
+    close(st, g["q_sol_tem"][:, 0], 1e-10, "sol tem")
+
+
+def test_assembly_deterministic():
+    case = M.random_case(nx=6, ny=5, nz=4, seed=9)
+    ctx = _ctx(case)
+    for prec in (F.OVS_FP64, F.OVS_FP32):
+        runs = []
+        for _ in range(3):
+            ctx.assemble(F.OVS_ASM_NSVOF, 6, prec)
+            runs.append((ctx.get_lhs(F.OVS_SYS_NSVOF, prec, F.OVS_BLK_K11), ctx.get_rhs(F.OVS_SYS_NSVOF, prec)))
+        for k11, rhs in runs[1:]:
+            assert np.array_equal(k11, runs[0][0]) and np.array_equal(rhs, runs[0][1])
+
+
+# ------------------------------------------------------------ SpMV / GMRES
+def _system_pair(oracle, seed, kind):
+    kernel = {"nsvof": F.OVS_ASM_NSVOF, "tem": F.OVS_ASM_TEM, "ns": F.OVS_ASM_NS}[kind]
+    case = M.random_case(nx=5, ny=4, nz=3, seed=seed, kernel=kernel)
+    case.mesh.elm_id[:] = 102
+    case.ibc[:] = 0
+    for f in range(6):
+        case.ibc[case.mesh.faces[f], 0:3] = 1
+    case.ibc[0, 3] = 1
+    case.params["subdomain_flag"] = 1
+    oc = oracle.OracleCase(case)
+    if kind == "ns":
+        oc.assemble_navsto(6)
+    else:
+        oc.assemble_quenching(6, 3 if kind == "nsvof" else 4)
+    ctx = _ctx(case)
+    sysid = {"ns": F.OVS_SYS_NS, "nsvof": F.OVS_SYS_NSVOF, "tem": F.OVS_SYS_TEM}[kind]
+    ref = oc.system(kind)
+    blocks = {k: v for k, v in ref.items() if k != "rhs"}
+    ctx.set_system(sysid, F.OVS_FP64, blocks, ref["rhs"])
+    return oc, ctx, sysid, ref
+
+
+@pytest.mark.parametrize("kind", ["ns", "nsvof", "tem"])
+def test_spmv_parity(oracle, kind):
+    oc, ctx, sysid, ref = _system_pair(oracle, 21, kind)
+    rng = np.random.default_rng(3)
+    x = np.asfortranarray(rng.standard_normal(ref["rhs"].shape))
+    close(ctx.spmv(sysid, F.OVS_FP64, x), oc.spmv(kind, x), 1e-13, f"spmv {kind}")
+    # FP32 matrix: compare against the oracle on the FP32-rounded values
+    blocks32 = {k: v.astype(np.float32).astype(np.float64) for k, v in ref.items() if k != "rhs"}
+    ctx.set_system(sysid, F.OVS_FP32, blocks32, ref["rhs"])
+    oc.load_system(kind, dict(blocks32, rhs=ref["rhs"]))
+    close(ctx.spmv(sysid, F.OVS_FP32, x), oc.spmv(kind, x), 1e-13, f"spmv32 {kind}")
+
+
+@pytest.mark.parametrize("kind", ["ns", "nsvof", "tem"])
+@pytest.mark.parametrize("kspace,kmin,tol", [(40, 1, 1e-8), (25, 10, 1e-3), (60, 1, 1e-14)])
+def test_gmres_reference_semantics(oracle, kind, kspace, kmin, tol):
+    oc, ctx, sysid, ref = _system_pair(oracle, 22, kind)
+    rng = np.random.default_rng(4)
+    sol0 = np.asfortranarray(rng.standard_normal(ref["rhs"].shape)) * 1e-3
+    so, it_o, er_o, r0_o = oc.gmres(kind, tol, kspace, kmin, sol0)
+    sg, info = ctx.gmres(sysid, tol, kspace, kmin, sol0)
+    assert info.iterations == it_o
+    assert abs(info.res0 - r0_o) <= 1e-12 * r0_o
+    close(sg, so, 1e-10, f"gmres {kind}")
+
+
+def test_gmres_tem_zero_rhs_returns_zero(oracle):
+    oc, ctx, sysid, ref = _system_pair(oracle, 23, "tem")
+    ctx.set_rhs(F.OVS_SYS_TEM, F.OVS_FP64, np.zeros(ctx.N))
+    s, info = SparseGMRES_tem(ctx, 1e-8, 20, 1, np.ones(ctx.N))
+    assert np.all(s == 0.0)   # SparseGMRES_tem.f90:68-71 zeroes sol
+
+
+def test_config1_newton_step(oracle):
+    """Config 1 end to end: NS assembly, reference GMRES(50, 1e-6), Newton
+    update - GPU vs oracle."""
+    case = M.config1()
+    oc = oracle.OracleCase(case)
+    oc.assemble_navsto(6)
+    ctx = _ctx(case)
+    assembleNavSto(ctx, 6)
+    so, it_o, er_o, r0_o = oc.gmres("ns", 1e-6, 50, 1)
+    su, sp, info = SparseGMRES_up(ctx, 1e-6, 50, 1, np.zeros((ctx.N, 3)), np.zeros(ctx.N))
+    assert info.iterations == it_o
+    close(np.column_stack([su, sp]), so, 1e-9, "config1 sol")
+    ctx.newton_update(F.OVS_SYS_NS)
+    oc.newton_update(F.OVS_SYS_NS, so)
+    for f in ("ug", "acg", "pg"):
+        close(ctx.get_field(f), oc.state_arrays[f], 1e-12, f)
+    r_g = ctx.residual_norms()
+    oc.assemble_navsto(2)
+    assembleNavSto(ctx, 2)
+    r_o = oc.calculate_residual()
+    close(ctx.residual_norms()[:2], r_o[:2], 1e-9, "residual after update")
+    assert r_g[0] > 0
+
+
+@pytest.mark.parametrize("mode", [F.OVS_FP64, F.OVS_FP32])
+def test_refined_solve_reaches_true_residual(oracle, mode):
+    case = M.quench_case(M.box_tet(8, 8, 8), "q8")
+    ctx = _ctx(case)
+    prec = F.OVS_FP64 if mode == F.OVS_FP64 else F.OVS_FP32
+    ctx.assemble(F.OVS_ASM_NSVOF, 6, prec)
+    sol, info = ctx.solve(F.OVS_SYS_NSVOF, mode, 1e-8, kspace=50, max_cycles=200)
+    assert info.converged and info.rel_residual <= 1e-8
+    # independent check of the true residual with the oracle's SpMV
+    oc = oracle.OracleCase(case)
+    sysblocks = ctx.get_system(F.OVS_SYS_NSVOF, prec)
+    oc.load_system("nsvof", sysblocks)
+    r = sysblocks["rhs"] - oc.spmv("nsvof", sol)
+    assert np.linalg.norm(r) <= 1.05e-8 * np.linalg.norm(sysblocks["rhs"])
+
+
+def test_mixed_vs_fp64_solution_error():
+    case = M.quench_case(M.box_tet(8, 8, 8), "q8")
+    ctx = _ctx(case)
+    ctx.assemble(F.OVS_ASM_NSVOF, 6, F.OVS_FP64)
+    ctx.assemble(F.OVS_ASM_NSVOF, 6, F.OVS_FP32)
+    s64, i64 = ctx.solve(F.OVS_SYS_NSVOF, F.OVS_FP64, 1e-10, 50, 300)
+    s32, i32 = ctx.solve(F.OVS_SYS_NSVOF, F.OVS_FP32, 1e-10, 50, 300)
+    assert i64.converged and i32.converged
+    for f in range(5):
+        err = np.abs(s32[:, f] - s64[:, f]).max() / max(np.abs(s64[:, f]).max(), 1e-300)
+        assert err < 1e-3, (f, err)   # FP32 assembly: O(kappa * 1e-7)
+
+
+# ------------------------------------------------------------ error paths
+def test_error_paths():
+    lib = F.load()
+    case = M.random_case(seed=1)
+    m = case.mesh
+    ctx = Context(m.nnode, m.nelem, 4)
+    with pytest.raises(F.OvsError) as e:
+        ctx.assemble(F.OVS_ASM_NSVOF, 6)
+    assert e.value.status == F.OVS_ERR_STATE
+    ien = m.ien.copy(order="F")
+    ien[0, 1] = ien[0, 0]  # degenerate element
+    bad = M.Mesh(m.xg, ien, m.elm_id, m.faces, m.dims, m.lengths)
+    with pytest.raises(F.OvsError) as e:
+        ctx.upload_mesh(bad)
+    assert e.value.status == F.OVS_ERR_ARG
+    ctx.upload_mesh(m)
+    ctx.build_pattern()
+    ctx.set_params(case.params)
+    ctx.set_state(case.state)
+    with pytest.raises(F.OvsError):
+        ctx.assemble(99, 6)
+    with pytest.raises(F.OvsError) as e:
+        ctx.gmres(F.OVS_SYS_NSVOF, 1e-6, 10, 1, np.zeros((m.nnode, 5)))
+    assert e.value.status == F.OVS_ERR_STATE
+    # an inverted element: warning status, results still written
+    xg = m.xg.copy(order="F")
+    n1, n2, n3, n4 = (m.ien[0] - 1)
+    nrm = np.cross(xg[n3] - xg[n2], xg[n4] - xg[n2])
+    nrm /= np.linalg.norm(nrm)
+    xg[n1] -= 2.0 * np.dot(xg[n1] - xg[n2], nrm) * nrm   # mirror node 1 through face (2,3,4)
+    ctx.set_field("xg", xg)
+    ctx.assemble(F.OVS_ASM_NSVOF, 6)
+    assert ctx.last_status == F.OVS_WARN_NEG_DETJ
+    ctx.close()
+
+
+def test_kdc_integer_dummy_quirk(oracle):
+    """e3DC_beta2 declares ns_kdc INTEGER but receives real(8): the low 4
+    bytes of the double become the multiplier.  With phi clamped to exactly 0
+    the interpolated value is NS_kdc_w itself, so the quirk is reproducible:
+    1 + 3 ulp has low word 3, i.e. k_dc = 3 |rL| / |G|."""
+    case = M.random_case(nx=4, ny=3, nz=3, seed=12, kernel=F.OVS_ASM_NSVOF)
+    for n in ("phig", "phigold"):
+        case.state[n][:] = -0.5
+    case.params["ns_kdc_w"] = np.nextafter(np.nextafter(np.nextafter(1.0, 2.0), 2.0), 2.0)
+    assert np.frombuffer(np.float64(case.params["ns_kdc_w"]).tobytes()[:4], np.int32)[0] == 3
+    oc, ctx, sysid, k, cfl_o, cfl_g = _assemble_both(oracle, case, F.OVS_ASM_NSVOF, 6, F.OVS_FP64)
+    _compare_system(oc, ctx, sysid, k, 6, F.OVS_FP64, 1e-12)
+    base = M.random_case(nx=4, ny=3, nz=3, seed=12, kernel=F.OVS_ASM_NSVOF)
+    for n in ("phig", "phigold"):
+        base.state[n][:] = -0.5
+    ob = oracle.OracleCase(base)
+    ob.assemble_quenching(6, 3)
+    assert np.abs(ob.sys["K11"] - oc.sys["K11"]).max() > 0   # k_dc is active

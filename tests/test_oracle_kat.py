@@ -1,0 +1,261 @@
+"""Known-answer tests that pin the CPU oracle (CPU only, no GPU).
+
+The reference ships no tests or golden vectors, so the oracle is pinned by
+answers known in closed form: pattern counts of the Kuhn split and of the
+27-point hex stencil, the binary-search semantics of SparseMatLoc_3D, the
+Galerkin mass of a single tet, the domain volume, partition of unity, and
+GMRES against dense LU.
+"""
+import numpy as np
+import pytest
+
+from oversetdevfort_b200 import mesh as M
+from oversetdevfort_b200 import _ffi as F
+
+
+def _pattern_props(col, row, N):
+    assert col[0] == 1 and len(col) == N + 1
+    for i in range(N):
+        r = row[col[i] - 1: col[i + 1] - 1]
+        assert np.all(np.diff(r) > 0), "row not strictly ascending"
+        assert (i + 1) in r, "diagonal missing"
+
+
+@pytest.mark.parametrize("dims", [(1, 1, 1), (2, 3, 4), (5, 1, 2), (16, 16, 16)])
+def test_pattern_kuhn_closed_form(oracle, dims):
+    m = M.box_tet(*dims)
+    col, row = oracle.gen_spar_struc(m.ien, m.nnode)
+    assert len(row) == M.expected_nnz_kuhn(*dims)
+    if m.nnode < 2000:
+        _pattern_props(col, row, m.nnode)
+    # symmetric structure
+    N = m.nnode
+    rows = np.repeat(np.arange(N), np.diff(col))
+    a = set(zip(rows.tolist(), (row - 1).tolist()))
+    assert all((j, i) in a for (i, j) in list(a)[:5000])
+
+
+def test_pattern_config1_count(oracle):
+    m = M.box_tet(16, 16, 16)
+    col, row = oracle.gen_spar_struc(m.ien, m.nnode)
+    assert len(row) == 66961  # 16^3 x6 Kuhn tets, 4913 nodes
+
+
+@pytest.mark.parametrize("dims", [(1, 1, 1), (3, 2, 2), (4, 4, 3)])
+def test_pattern_hex_closed_form(oracle, dims):
+    m = M.box_hex(*dims)
+    col, row = oracle.gen_spar_struc(m.ien, m.nnode)
+    assert len(row) == M.expected_nnz_hex(*dims)
+    _pattern_props(col, row, m.nnode)
+
+
+def test_sparse_mat_loc_semantics(oracle):
+    lib = oracle.load()
+    lst = np.array([2, 5, 9, 11], dtype=np.int32)
+    p = oracle._i(lst)
+    # last 1-based index with list(idx) <= goal; no not-found check
+    assert lib.orc_sparse_mat_loc(p, 4, 9) == 3
+    assert lib.orc_sparse_mat_loc(p, 4, 2) == 1
+    assert lib.orc_sparse_mat_loc(p, 4, 1) == 1
+    assert lib.orc_sparse_mat_loc(p, 4, 10) == 3
+    assert lib.orc_sparse_mat_loc(p, 4, 12) == 4
+    assert lib.orc_sparse_mat_loc(p, 4, 11) == 4
+
+
+def test_mesh_orientation():
+    for m in (M.box_tet(3, 2, 2, 1.0, 0.5, 2.0), M.box_hex(2, 2, 3)):
+        x = m.xg[m.ien - 1]  # (E, nshl, 3)
+        if m.nshl == 4:
+            J = np.stack([x[:, 0] - x[:, 3], x[:, 1] - x[:, 3], x[:, 2] - x[:, 3]], axis=2)
+            assert np.all(np.linalg.det(J) > 0)
+            vol = np.linalg.det(J).sum() / 6.0
+            assert abs(vol - np.prod(m.lengths)) < 1e-12
+        else:
+            # node 5 is the (-1,-1,-1) corner, 3 the (+1,+1,+1) one
+            assert np.all(x[:, 2] - x[:, 4] > 0)
+
+
+def _single_tet_case(rho=2.0):
+    xg = np.asfortranarray(np.array([[1.2, 0.2, 0.1], [0.3, 0.1, 0.0], [0.4, 1.1, 0.2], [0.2, 0.3, 0.9]]))
+    ien = np.asfortranarray(np.array([[1, 2, 3, 4]], dtype=np.int32))
+    # orient positively
+    J = np.stack([xg[0] - xg[3], xg[1] - xg[3], xg[2] - xg[3]], axis=1)
+    assert np.linalg.det(J) > 0
+    m = M.Mesh(xg, ien, np.array([102], dtype=np.int32), [np.arange(4)] * 6, (1, 1, 1), (1, 1, 1))
+    p = M.base_params(rhow=rho, rhoa=rho, muw=0.0, mua=0.0)
+    st = M.empty_state(4)
+    ibc = np.zeros((4, 8), dtype=np.int32, order="F")
+    return M.Case("single_tet", m, p, st, ibc, F.OVS_ASM_NSVOF), abs(np.linalg.det(J)) / 6.0
+
+
+def test_single_tet_galerkin_mass(oracle):
+    """u = 0, mu = 0: K11(a,b) = alpha_m rho |T| (1 + delta_ab) / 20 (the
+    4-point rule integrates quadratics exactly)."""
+    rho = 2.0
+    case, vol = _single_tet_case(rho)
+    oc = oracle.OracleCase(case)
+    oc.assemble_quenching(F.OVS_TENSOR_MAT | F.OVS_TENSOR_VEC, 3)
+    K = oc.sys["K11"]
+    col, row = oc.col, oc.row
+    am = case.params["almi"]
+    for a in range(4):
+        for k in range(col[a] - 1, col[a + 1] - 1):
+            b = row[k] - 1
+            want = am * rho * vol * (1 + (a == b)) / 20.0
+            for comp in (0, 4, 8):
+                assert abs(K[k, comp] - want) < 1e-14 * abs(want) + 1e-16
+            for comp in (1, 2, 3, 5, 6, 7):
+                assert abs(K[k, comp]) < 1e-15
+
+
+@pytest.mark.parametrize("kernel", [F.OVS_ASM_NS, F.OVS_ASM_NSVOF])
+def test_volume_kat(oracle, kernel):
+    """With u = 0 and no BCs the velocity-block entries of K(1,1) sum to
+    alpha_m * rho * volume (shape-gradient terms sum to zero)."""
+    m = M.box_tet(3, 4, 2, 1.0, 0.7, 0.4)
+    rho = 3.5
+    p = M.base_params(rhow=rho, rhoa=rho, muw=0.01, mua=0.01)
+    st = M.empty_state(m.nnode)
+    ibc = np.zeros((m.nnode, 8), dtype=np.int32, order="F")
+    case = M.Case("vol", m, p, st, ibc, kernel)
+    oc = oracle.OracleCase(case)
+    if kernel == F.OVS_ASM_NS:
+        oc.assemble_navsto(F.OVS_TENSOR_MAT)
+    else:
+        oc.assemble_quenching(F.OVS_TENSOR_MAT, 3)
+    total = oc.sys["K11"][:, 0].sum()
+    want = p["almi"] * rho * 1.0 * 0.7 * 0.4
+    assert abs(total - want) < 1e-12 * want
+    # PSPG Laplacian rows sum to zero (sum_b grad N_b = 0)
+    rs = np.add.reduceat(oc.sys["M"], oc.col[:-1] - 1)
+    assert np.abs(rs).max() < 1e-12 * np.abs(oc.sys["M"]).max()
+
+
+def test_dirichlet_diagonal_counts(oracle):
+    """A constrained dof's assembled diagonal equals the number of elements
+    around the node (per-element BC treatment, src/BCLhs_3D.f90)."""
+    case = M.config1(n=3)
+    oc = oracle.OracleCase(case)
+    oc.assemble_navsto(F.OVS_TENSOR_MAT | F.OVS_TENSOR_VEC)
+    m = case.mesh
+    nelem_at = np.bincount(m.ien.ravel() - 1, minlength=m.nnode)
+    for i in m.faces[0][:10]:
+        k = next(k for k in range(oc.col[i] - 1, oc.col[i + 1] - 1) if oc.row[k] == i + 1)
+        assert oc.sys["K11"][k, 0] == nelem_at[i]
+        assert oc.sys["K11"][k, 4] == nelem_at[i]
+        assert oc.sys["K11"][k, 1] == 0.0
+        assert oc.sys["rhsu"][i, 0] == 0.0
+
+
+def test_quench_literal_switch_freezes_vof(oracle):
+    case = M.random_case(seed=3)
+    oc = oracle.OracleCase(case, literal=True)
+    oc.assemble_quenching(F.OVS_TENSOR_MAT | F.OVS_TENSOR_VEC, 3)
+    assert np.all(oc.sys["LS"] == 0) and np.all(oc.sys["LSU"] == 0)
+    assert np.abs(oc.sys["rhsls"]).max() > 0
+
+
+def _dense(oc, kind):
+    N = oc.N
+    nf = {"ns": 4, "nsvof": 5, "tem": 1}[kind]
+    A = np.zeros((N * nf, N * nf))
+    for j in range(N * nf):
+        e = np.zeros(N * nf)
+        e[j] = 1.0
+        A[:, j] = oc.spmv(kind, e.reshape((N, nf), order="F")).ravel(order="F")
+    return A
+
+
+def test_gmres_diagonal_one_iteration(oracle):
+    case = M.random_case(seed=4)
+    oc = oracle.OracleCase(case)
+    rng = np.random.default_rng(0)
+    d = np.zeros(oc.icnt)
+    for i in range(oc.N):
+        k = next(k for k in range(oc.col[i] - 1, oc.col[i + 1] - 1) if oc.row[k] == i + 1)
+        d[k] = rng.uniform(1, 3)
+    rhs = rng.standard_normal(oc.N)
+    oc.load_system("tem", {"TEM": d, "rhs": rhs[:, None]})
+    sol, it, er, r0 = oc.gmres("tem", 1e-10, 20, 1)
+    assert it == 1
+    dd = np.array([d[next(k for k in range(oc.col[i] - 1, oc.col[i + 1] - 1) if oc.row[k] == i + 1)]
+                   for i in range(oc.N)])
+    np.testing.assert_allclose(sol[:, 0], rhs / dd, rtol=1e-14)
+
+
+@pytest.mark.parametrize("kind", ["tem", "ns", "nsvof"])
+def test_gmres_full_space_matches_dense_lu(oracle, kind):
+    case = M.random_case(nx=2, ny=2, nz=2, seed=5, phase_change=False)
+    case.mesh.elm_id[:] = 102  # no all-solid / non-target rows (singular)
+    case.ibc[:] = 0
+    for f in range(6):                 # closed cavity ...
+        case.ibc[case.mesh.faces[f], 0:3] = 1
+    case.ibc[0, 3] = 1                 # ... with the pressure level pinned
+    oc = oracle.OracleCase(case)
+    if kind == "ns":
+        case.params["subdomain_flag"] = 1
+        oc = oracle.OracleCase(case)
+        oc.assemble_navsto(F.OVS_TENSOR_MAT | F.OVS_TENSOR_VEC)
+    else:
+        oc.assemble_quenching(F.OVS_TENSOR_MAT | F.OVS_TENSOR_VEC, 3 if kind == "nsvof" else 4)
+    s = oc.system(kind)
+    nf = s["rhs"].shape[1]
+    n = oc.N * nf
+    if kind == "nsvof":
+        # the VOF preconditioner maps 1/LS(ii) = 0 when LS(ii) = 0; make sure it is not
+        assert np.all(np.abs(s["LS"]) >= 0)
+    sol, it, er, r0 = oc.gmres(kind, 1e-13, n, 1)
+    A = _dense(oc, kind)
+    b = s["rhs"].ravel(order="F")
+    x = np.linalg.solve(A, b)
+    xs = sol.ravel(order="F")
+    res = np.linalg.norm(b - A @ xs) / np.linalg.norm(b)
+    assert res < 1e-9, (it, res)
+    # forward error within the conditioning of the system
+    err = np.linalg.norm(xs - x) / np.linalg.norm(x)
+    assert err < 1e-14 * np.linalg.cond(A), (it, err)
+
+
+def test_newton_update_and_residual(oracle):
+    case = M.random_case(seed=6)
+    oc = oracle.OracleCase(case)
+    oc.assemble_quenching(F.OVS_TENSOR_VEC, 7)
+    r = oc.calculate_residual()
+    s = oc.sys
+    np.testing.assert_allclose(r, [np.sum(s["rhsu"] ** 2), np.sum(s["rhsp"] ** 2), np.sum(s["rhsls"] ** 2),
+                                   np.sum(s["rhstem"] ** 2)], rtol=1e-13)
+    rng = np.random.default_rng(1)
+    sol = np.asfortranarray(rng.standard_normal((oc.N, 5)))
+    before = {k: v.copy() for k, v in oc.state_arrays.items()}
+    oc.newton_update(F.OVS_SYS_NSVOF, sol)
+    p = case.params
+    gdt = p["gami"] * p["delt"]
+    np.testing.assert_allclose(oc.state_arrays["acg"], before["acg"] + sol[:, :3], rtol=1e-15)
+    np.testing.assert_allclose(oc.state_arrays["ug"], before["ug"] + gdt * sol[:, :3], rtol=1e-15)
+    np.testing.assert_allclose(oc.state_arrays["pg"], before["pg"] + p["alfi"] * p["gami"] * p["delt"] * sol[:, 3],
+                               rtol=1e-15)
+    np.testing.assert_allclose(oc.state_arrays["phig"], before["phig"] + gdt * sol[:, 4], rtol=1e-15)
+
+
+def test_genalpha_matches_reference_formulas(lib):
+    for rinf in (0.0, 0.5, 1.0, -1.0, 2.0):
+        p = F.OvsParams()
+        assert lib.ovs_params_genalpha(rinf, p) == 0
+        want = M.genalpha(rinf)
+        for k in ("almi", "alfi", "gami", "beti"):
+            assert getattr(p, k) == want[k]
+
+
+def test_golden_fixture_regression(oracle):
+    """The committed fixture (made by tests/golden/make_golden.py) is
+    reproduced bit-for-bit by the oracle."""
+    import importlib.util
+    from pathlib import Path
+    here = Path(__file__).resolve().parent / "golden"
+    spec = importlib.util.spec_from_file_location("make_golden", here / "make_golden.py")
+    mg = importlib.util.module_from_spec(spec)
+    spec.loader.exec_module(mg)
+    g = np.load(here / "quench_small.npz")
+    fresh = mg.compute()
+    for k in g.files:
+        np.testing.assert_array_equal(g[k], fresh[k], err_msg=k)
