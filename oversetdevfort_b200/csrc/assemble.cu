@@ -199,299 +199,502 @@ __device__ __forceinline__ void cfl_max(unsigned long long* bits, double v) {
   if (v >= 0.0) atomicMax(bits, (unsigned long long)__double_as_longlong(v));
 }
 
-// ----------------------------------------------------- per-kind physics
-// Each kind fills, for lane element (with row-local index la):
-//   blk[b*NVP + v]  v < NV : A's row block with column node b
-//   rv[f]           f < NF : A's residual entries
-// returns DetJ.
-template <typename T, int KIND> struct Phys;
-
-// NS-only, IntElmAss_NS_overset + e3LHS_3D_fluid_Old + e3Rhs_3D_fluid.
-// Quirks kept: uprime = 0 (shhessgu passed for uprime), kap_dc = NS_kdc_a,
-// tauBar = 0, rho = rhoa, mu = mua.
-template <typename T> struct Phys<T, OVS_ASM_NS> {
-  static constexpr int NV = 16, NF = 4;
-  __device__ static T eval(const AsmArgs& a, int e, int la, const T r[4][16], const T lo[4][4], bool target,
-                           T* blk, int nvp, T* rv, double& cfl) {
-    const ovs_params& p = a.p;
-    T xd[4][3], g[4][3], G[3][3];
-#pragma unroll
-    for (int n = 0; n < 4; ++n)
-#pragma unroll
-      for (int i = 0; i < 3; ++i) xd[n][i] = r[n][i];
-    const T detj = tet_geometry<T>(xd, lo, g, G);
-    const T w = detj * (T)(0.25 / 6.0);
-    T GG = 0;
-#pragma unroll
-    for (int j = 0; j < 3; ++j)
-#pragma unroll
-      for (int i = 0; i < 3; ++i) GG += G[i][j] * G[i][j];
-    const T trG = G[0][0] + G[1][1] + G[2][2];
-    T du[3][3], dp[3];
-#pragma unroll
-    for (int i = 0; i < 3; ++i)
-#pragma unroll
-      for (int j = 0; j < 3; ++j)
-        du[i][j] = r[0][3 + i] * g[0][j] + r[1][3 + i] * g[1][j] + r[2][3 + i] * g[2][j] + r[3][3 + i] * g[3][j];
-#pragma unroll
-    for (int j = 0; j < 3; ++j) dp[j] = r[0][12] * g[0][j] + r[1][12] * g[1][j] + r[2][12] * g[2][j] + r[3][12] * g[3][j];
-    const T divu = du[0][0] + du[1][1] + du[2][2];
-    const T rho = (T)p.rhoa, mu = (T)p.mua, mupkdc = mu + (T)p.ns_kdc_a;
-    const T fact1 = (T)p.almi, fact2 = (T)(p.alfi * p.gami * p.delt);
-    const T taut = (T)(4.0 / (p.delt * p.delt));
-    const T ga[3] = {la == 0 ? g[0][0] : la == 1 ? g[1][0] : la == 2 ? g[2][0] : g[3][0],
-                     la == 0 ? g[0][1] : la == 1 ? g[1][1] : la == 2 ? g[2][1] : g[3][1],
-                     la == 0 ? g[0][2] : la == 1 ? g[1][2] : la == 2 ? g[2][2] : g[3][2]};
-    T gab[4];
-#pragma unroll
-    for (int b = 0; b < 4; ++b) gab[b] = ga[0] * g[b][0] + ga[1] * g[b][1] + ga[2] * g[b][2];
-    // factored Gauss-point sums (see the block formulas below)
-    T KA = 0, KB = 0, Q = 0, R = 0, MM = 0;
-    T Pb[4] = {0, 0, 0, 0}, Tb[4] = {0, 0, 0, 0}, Sb[4] = {0, 0, 0, 0};
-    T ru[3] = {0, 0, 0}, rp = 0;
-    // A's residual gradient term: sum_j ga_j tmp2_ij, tmp2 = -ptot I + mupkdc (du + du^T)
-    T sym[3];
-#pragma unroll
-    for (int i = 0; i < 3; ++i)
-      sym[i] = mupkdc * (ga[0] * (du[i][0] + du[0][i]) + ga[1] * (du[i][1] + du[1][i]) + ga[2] * (du[i][2] + du[2][i]));
-#pragma unroll
-    for (int gp = 0; gp < 4; ++gp) {
-      T N[4];
-      tet_shape<T>(gp, N);
-      T ui[3], umi[3], aci[3], pri;
-#pragma unroll
-      for (int d = 0; d < 3; ++d) {
-        ui[d] = r[0][3 + d] * N[0] + r[1][3 + d] * N[1] + r[2][3 + d] * N[2] + r[3][3 + d] * N[3];
-        umi[d] = r[0][6 + d] * N[0] + r[1][6 + d] * N[1] + r[2][6 + d] * N[2] + r[3][6 + d] * N[3];
-        aci[d] = r[0][9 + d] * N[0] + r[1][9 + d] * N[1] + r[2][9 + d] * N[2] + r[3][9 + d] * N[3];
-      }
-      pri = r[0][12] * N[0] + r[1][12] * N[1] + r[2][12] * N[2] + r[3][12] * N[3];
-      T uadv[3] = {ui[0] - umi[0], ui[1] - umi[1], ui[2] - umi[2]};
-      const T taua = quad_uGu<T>(uadv, G);
-      const T nu = mu / rho;
-      const T taud = nu * nu * (T)12.0 * GG;
-      const T tauM = (T)1.0 / (rho * sqrt(taut + taua + taud));
-      const T tauC = rho * sqrt(taua + taud) / trG;
-      {
-        double c = (double)p.delt * sqrt((double)taua);
-        if (c > cfl) cfl = c;
-      }
-      T c[4];
-#pragma unroll
-      for (int b = 0; b < 4; ++b) c[b] = uadv[0] * g[b][0] + uadv[1] * g[b][1] + uadv[2] * g[b][2];
-      const T Na = pick4<T>(N, la), ca = pick4<T>(c, la);
-      if (target) {
-        // tmp4 = rho (Na + rho tauM ca)(fact1 Nb + fact2 cb) + fact2 mupkdc gab
-        const T alpha = w * rho * (Na + rho * tauM * ca);
-        KA += fact2 * mupkdc * w;
-        KB += fact2 * tauC * w;
-        Q += fact2 * w * rho * tauM * ca;
-        R += fact2 * w * Na;
-        MM += fact2 * w * tauM;
-#pragma unroll
-        for (int b = 0; b < 4; ++b) {
-          const T beta = fact1 * N[b] + fact2 * c[b];
-          Sb[b] += alpha * beta;
-          Pb[b] += fact2 * w * N[b];
-          Tb[b] += w * tauM * rho * beta;
-        }
-        // e3Rhs_3D_fluid with uprime = 0
-        const T ptot = pri - tauC * divu;
-#pragma unroll
-        for (int i = 0; i < 3; ++i) {
-          const T tmp1 = rho * (aci[i] + uadv[0] * du[i][0] + uadv[1] * du[i][1] + uadv[2] * du[i][2]) - (T)p.gravvec[i] * rho;
-          ru[i] -= (Na * tmp1 + (sym[i] - ga[i] * ptot)) * w;
-        }
-        rp -= (Na * divu) * w;
-      }
-    }
-#pragma unroll
-    for (int b = 0; b < 4; ++b) {
-      T o[16];
-      const T* gb = g[b];
-      const T dg = KA * gab[b] + Sb[b];
-#pragma unroll
-      for (int i = 0; i < 3; ++i) {
-#pragma unroll
-        for (int j = 0; j < 3; ++j) o[4 * i + j] = KA * ga[j] * gb[i] + KB * ga[i] * gb[j] + (i == j ? dg : (T)0);
-        o[4 * i + 3] = -ga[i] * Pb[b] + gb[i] * Q;
-      }
-#pragma unroll
-      for (int d = 0; d < 3; ++d) o[12 + d] = gb[d] * R + ga[d] * Tb[b];
-      o[15] = MM * gab[b];
-      store_row<16>(blk + b * nvp, o);
-    }
-    rv[0] = ru[0]; rv[1] = ru[1]; rv[2] = ru[2]; rv[3] = rp;
-    return detj;
-  }
+// ----------------------------------------------------- element summaries
+// Pass 1 (one thread per element) evaluates everything the element matrix
+// needs from its Gauss points, once, plus the element's residual rows, and
+// stores it as a compact summary of SW values.  Pass 2 (one warp per CSR
+// row) expands A's row of each element matrix from the summaries.  Inactive
+// elements (solid on the NS+VOF pass, non-target on the NS pass) store w = 0
+// and zero residuals, which makes every expanded block exactly zero.
+//   NS   : g(12) w KA KB MM | GP x4: uadv(3) rt        | residual 4x4 = 48
+//   NSVOF: g(12) w KA KB MM KDP dphi(3) | GP x4: uadv(3) rho rt tauLS src
+//          eps ufac plfac                              | residual 4x5 = 80
+//   TEM  : g(12) w HK | GP x4: uadv(3) rcp dSe trc     | residual 4 +pad = 44
+// with rt = rho tauM, trc = tauT rho cp and the factors of the block sums
+// below (src, eps, ufac, plfac of the phase-change terms).
+template <int KIND> struct Lay;
+template <> struct Lay<OVS_ASM_NS> {
+  static constexpr int SW = 48, GP0 = 16, GPW = 4, RHS0 = 32, NF = 4, NV = 16;
+};
+template <> struct Lay<OVS_ASM_NSVOF> {
+  static constexpr int SW = 80, GP0 = 20, GPW = 10, RHS0 = 60, NF = 5, NV = 24;
+};
+template <> struct Lay<OVS_ASM_TEM> {
+  static constexpr int SW = 44, GP0 = 14, GPW = 6, RHS0 = 38, NF = 1, NV = 1;
 };
 
-// NS+VOF quench element, IntElmAss_NSVOF_Quenching_STAB.
-template <typename T> struct Phys<T, OVS_ASM_NSVOF> {
-  static constexpr int NV = 24, NF = 5;
-  __device__ static T eval(const AsmArgs& a, int e, int la, const T r[4][16], const T lo[4][4], bool fluid,
-                           T* blk, int nvp, T* rv, double& cfl) {
-    const ovs_params& p = a.p;
-    T xd[4][3], g[4][3], G[3][3];
+struct SumArgs {
+  const void* rec;
+  const int* ien;
+  const int* elm_id;
+  void* sum;
+  int* flags;
+  unsigned long long* cfl_bits;
+  int E;
+  ovs_params p;
+};
+
+template <typename T>
+__device__ __forceinline__ void element_geometry(const T r[4][16], const T lo[4][4], T g[4][3], T G[3][3],
+                                                 T& detj, T& GG, T& trG) {
+  T xd[4][3];
 #pragma unroll
-    for (int n = 0; n < 4; ++n)
+  for (int n = 0; n < 4; ++n)
 #pragma unroll
-      for (int i = 0; i < 3; ++i) xd[n][i] = r[n][i];
-    const T detj = tet_geometry<T>(xd, lo, g, G);
-    const T w = detj * (T)(0.25 / 6.0);
-    T GG = 0;
+    for (int i = 0; i < 3; ++i) xd[n][i] = r[n][i];
+  detj = tet_geometry<T>(xd, lo, g, G);
+  GG = 0;
+#pragma unroll
+  for (int j = 0; j < 3; ++j)
+#pragma unroll
+    for (int i = 0; i < 3; ++i) GG += G[i][j] * G[i][j];
+  trG = G[0][0] + G[1][1] + G[2][2];
+}
+
+// pass 1, NS-only: IntElmAss_NS_overset's Gauss loop with e3LHS_3D_fluid_Old /
+// e3Rhs_3D_fluid (quirks: uprime = 0, kap_dc = NS_kdc_a, tauBar = 0)
+template <typename T>
+__device__ void summarize_ns(const SumArgs& a, const T r[4][16], const T lo[4][4], bool target, T* o,
+                             double& cfl, T& detj_out) {
+  const ovs_params& p = a.p;
+  T g[4][3], G[3][3], detj, GG, trG;
+  element_geometry<T>(r, lo, g, G, detj, GG, trG);
+  detj_out = detj;
+  const T w = detj * (T)(0.25 / 6.0);
+  T du[3][3];
+#pragma unroll
+  for (int i = 0; i < 3; ++i)
 #pragma unroll
     for (int j = 0; j < 3; ++j)
+      du[i][j] = r[0][3 + i] * g[0][j] + r[1][3 + i] * g[1][j] + r[2][3 + i] * g[2][j] + r[3][3 + i] * g[3][j];
+  const T divu = du[0][0] + du[1][1] + du[2][2];
+  const T rho = (T)p.rhoa, mu = (T)p.mua, mupkdc = mu + (T)p.ns_kdc_a;
+  const T fact2 = (T)(p.alfi * p.gami * p.delt);
+  const T taut = (T)(4.0 / (p.delt * p.delt));
+  T KA = 0, KB = 0, MM = 0;
+  T ru[4][3], rp[4];
 #pragma unroll
-      for (int i = 0; i < 3; ++i) GG += G[i][j] * G[i][j];
-    const T trG = G[0][0] + G[1][1] + G[2][2];
-    T du[3][3], dp[3], dphi[3];
+  for (int n = 0; n < 4; ++n) { ru[n][0] = ru[n][1] = ru[n][2] = 0; rp[n] = 0; }
 #pragma unroll
-    for (int i = 0; i < 3; ++i)
+  for (int gp = 0; gp < 4; ++gp) {
+    T N[4];
+    tet_shape<T>(gp, N);
+    T ui[3], umi[3], aci[3];
 #pragma unroll
-      for (int j = 0; j < 3; ++j)
-        du[i][j] = r[0][3 + i] * g[0][j] + r[1][3 + i] * g[1][j] + r[2][3 + i] * g[2][j] + r[3][3 + i] * g[3][j];
-#pragma unroll
-    for (int j = 0; j < 3; ++j) {
-      dp[j] = r[0][12] * g[0][j] + r[1][12] * g[1][j] + r[2][12] * g[2][j] + r[3][12] * g[3][j];
-      dphi[j] = r[0][13] * g[0][j] + r[1][13] * g[1][j] + r[2][13] * g[2][j] + r[3][13] * g[3][j];
+    for (int d = 0; d < 3; ++d) {
+      ui[d] = r[0][3 + d] * N[0] + r[1][3 + d] * N[1] + r[2][3 + d] * N[2] + r[3][3 + d] * N[3];
+      umi[d] = r[0][6 + d] * N[0] + r[1][6 + d] * N[1] + r[2][6 + d] * N[2] + r[3][6 + d] * N[3];
+      aci[d] = r[0][9 + d] * N[0] + r[1][9 + d] * N[1] + r[2][9 + d] * N[2] + r[3][9 + d] * N[3];
     }
-    const T divu = du[0][0] + du[1][1] + du[2][2];
-    const T fact1 = (T)p.almi, fact2 = (T)(p.alfi * p.delt * p.gami);
-    const T taut = (T)(4.0 / (p.delt * p.delt));
-    const T rhoa = (T)p.rhoa, rhow = (T)p.rhow, ts = (T)p.ts;
-    const T ira = (T)1.0 / rhoa - (T)1.0 / rhow;
-    const T ga[3] = {la == 0 ? g[0][0] : la == 1 ? g[1][0] : la == 2 ? g[2][0] : g[3][0],
-                     la == 0 ? g[0][1] : la == 1 ? g[1][1] : la == 2 ? g[2][1] : g[3][1],
-                     la == 0 ? g[0][2] : la == 1 ? g[1][2] : la == 2 ? g[2][2] : g[3][2]};
-    T gab[4];
+    const T pri = r[0][12] * N[0] + r[1][12] * N[1] + r[2][12] * N[2] + r[3][12] * N[3];
+    const T uadv[3] = {ui[0] - umi[0], ui[1] - umi[1], ui[2] - umi[2]};
+    const T taua = quad_uGu<T>(uadv, G);
+    const T nu = mu / rho;
+    const T taud = nu * nu * (T)12.0 * GG;
+    const T tauM = (T)1.0 / (rho * sqrt(taut + taua + taud));
+    const T tauC = rho * sqrt(taua + taud) / trG;
+    {
+      const double c = (double)p.delt * sqrt((double)taua);
+      if (c > cfl) cfl = c;
+    }
+    T* og = o + Lay<OVS_ASM_NS>::GP0 + gp * Lay<OVS_ASM_NS>::GPW;
+    og[0] = uadv[0]; og[1] = uadv[1]; og[2] = uadv[2]; og[3] = rho * tauM;
+    if (target) {
+      KA += fact2 * mupkdc * w;
+      KB += fact2 * tauC * w;
+      MM += fact2 * w * tauM;
+      const T ptot = pri - tauC * divu;
 #pragma unroll
-    for (int b = 0; b < 4; ++b) gab[b] = ga[0] * g[b][0] + ga[1] * g[b][1] + ga[2] * g[b][2];
-    // sum_k sum_j ga_j (du(j,k) + du(k,j)): the three viscous RHS scalars that
-    // the reference subtracts from every momentum component (:508-510)
-    T svis = 0;
+      for (int i = 0; i < 3; ++i) {
+        const T tmp1 = rho * (aci[i] + uadv[0] * du[i][0] + uadv[1] * du[i][1] + uadv[2] * du[i][2]) - (T)p.gravvec[i] * rho;
+#pragma unroll
+        for (int n = 0; n < 4; ++n) {
+          const T sym = mupkdc * (g[n][0] * (du[i][0] + du[0][i]) + g[n][1] * (du[i][1] + du[1][i]) +
+                                  g[n][2] * (du[i][2] + du[2][i]));
+          ru[n][i] -= (N[n] * tmp1 + (sym - g[n][i] * ptot)) * w;
+        }
+      }
+#pragma unroll
+      for (int n = 0; n < 4; ++n) rp[n] -= (N[n] * divu) * w;
+    }
+  }
+#pragma unroll
+  for (int n = 0; n < 4; ++n)
+#pragma unroll
+    for (int d = 0; d < 3; ++d) o[3 * n + d] = g[n][d];
+  o[12] = target ? w : (T)0; o[13] = KA; o[14] = KB; o[15] = MM;
+#pragma unroll
+  for (int n = 0; n < 4; ++n) {
+    T* orh = o + Lay<OVS_ASM_NS>::RHS0 + 4 * n;
+    orh[0] = ru[n][0]; orh[1] = ru[n][1]; orh[2] = ru[n][2]; orh[3] = rp[n];
+  }
+}
+
+// pass 1, NS+VOF quench (src/solveQuenching.f90:295-523); the viscous RHS
+// broadcast (:508-510) is kept: the three scalars sum_j gN_a,j (du(j,k) +
+// du(k,j)), k = 1..3, are subtracted from every momentum component
+template <typename T>
+__device__ void summarize_nsvof(const SumArgs& a, const T r[4][16], const T lo[4][4], bool fluid, T* o,
+                                double& cfl, T& detj_out) {
+  const ovs_params& p = a.p;
+  T g[4][3], G[3][3], detj, GG, trG;
+  element_geometry<T>(r, lo, g, G, detj, GG, trG);
+  detj_out = detj;
+  const T w = detj * (T)(0.25 / 6.0);
+  T du[3][3], dp[3], dphi[3];
+#pragma unroll
+  for (int i = 0; i < 3; ++i)
+#pragma unroll
+    for (int j = 0; j < 3; ++j)
+      du[i][j] = r[0][3 + i] * g[0][j] + r[1][3 + i] * g[1][j] + r[2][3 + i] * g[2][j] + r[3][3 + i] * g[3][j];
+#pragma unroll
+  for (int j = 0; j < 3; ++j) {
+    dp[j] = r[0][12] * g[0][j] + r[1][12] * g[1][j] + r[2][12] * g[2][j] + r[3][12] * g[3][j];
+    dphi[j] = r[0][13] * g[0][j] + r[1][13] * g[1][j] + r[2][13] * g[2][j] + r[3][13] * g[3][j];
+  }
+  const T divu = du[0][0] + du[1][1] + du[2][2];
+  const T fact2 = (T)(p.alfi * p.delt * p.gami);
+  const T taut = (T)(4.0 / (p.delt * p.delt));
+  const T rhoa = (T)p.rhoa, rhow = (T)p.rhow, ts = (T)p.ts;
+  const T ira = (T)1.0 / rhoa - (T)1.0 / rhow;
+  const bool kdc_on = fabs(p.ns_kdc_w) + fabs(p.ns_kdc_a) > 0.0;
+  const bool kdcphi_on = fabs(p.lsc_kdc) > 0.0;
+  T svis[4], gdphi[4];
+#pragma unroll
+  for (int n = 0; n < 4; ++n) {
+    T sv = 0;
 #pragma unroll
     for (int k = 0; k < 3; ++k)
-      svis += ga[0] * (du[0][k] + du[k][0]) + ga[1] * (du[1][k] + du[k][1]) + ga[2] * (du[2][k] + du[k][2]);
-    const T gdphi = ga[0] * dphi[0] + ga[1] * dphi[1] + ga[2] * dphi[2];
-    T KA = 0, KB = 0, Q = 0, R = 0, MM = 0, KDP = 0, W = 0;
-    T Pb[4] = {0, 0, 0, 0}, Tb[4] = {0, 0, 0, 0}, Sb[4] = {0, 0, 0, 0}, L1[4] = {0, 0, 0, 0},
-      Eb[4] = {0, 0, 0, 0}, Ub[4] = {0, 0, 0, 0}, PLb[4] = {0, 0, 0, 0}, Vb[4] = {0, 0, 0, 0};
-    T ru[3] = {0, 0, 0}, rp = 0, rf = 0;
-    const bool kdc_on = fabs(p.ns_kdc_w) + fabs(p.ns_kdc_a) > 0.0;
-    const bool kdcphi_on = fabs(p.lsc_kdc) > 0.0;
+      sv += g[n][0] * (du[0][k] + du[k][0]) + g[n][1] * (du[1][k] + du[k][1]) + g[n][2] * (du[2][k] + du[k][2]);
+    svis[n] = sv;
+    gdphi[n] = g[n][0] * dphi[0] + g[n][1] * dphi[1] + g[n][2] * dphi[2];
+  }
+  T KA = 0, KB = 0, MM = 0, KDP = 0;
+  T ru[4][3], rp[4], rf[4];
+#pragma unroll
+  for (int n = 0; n < 4; ++n) { ru[n][0] = ru[n][1] = ru[n][2] = 0; rp[n] = 0; rf[n] = 0; }
+#pragma unroll
+  for (int gp = 0; gp < 4; ++gp) {
+    T N[4];
+    tet_shape<T>(gp, N);
+    T ui[3], umi[3], aci[3];
+#pragma unroll
+    for (int d = 0; d < 3; ++d) {
+      ui[d] = r[0][3 + d] * N[0] + r[1][3 + d] * N[1] + r[2][3 + d] * N[2] + r[3][3 + d] * N[3];
+      umi[d] = r[0][6 + d] * N[0] + r[1][6 + d] * N[1] + r[2][6 + d] * N[2] + r[3][6 + d] * N[3];
+      aci[d] = r[0][9 + d] * N[0] + r[1][9 + d] * N[1] + r[2][9 + d] * N[2] + r[3][9 + d] * N[3];
+    }
+    const T pri = r[0][12] * N[0] + r[1][12] * N[1] + r[2][12] * N[2] + r[3][12] * N[3];
+    const double phid = gp_phi(r, lo, 13, gp);   // VOF in FP64 for the 1000:1 property blend
+    const T phii = (T)phid;
+    const T rphii = r[0][14] * N[0] + r[1][14] * N[1] + r[2][14] * N[2] + r[3][14] * N[3];
+    const T Ti = r[0][15] * N[0] + r[1][15] * N[1] + r[2][15] * N[2] + r[3][15] * N[3];
+    const double phicd = fmax(fmin(phid, 1.0), 0.0);
+    const T phic = (T)phicd;
+    T mdot, dmd;
+    if (Ti > ts) {
+      mdot = (T)p.c_evap * (T)(1.0 - phicd) * rhow * (Ti - ts) / ts;
+      dmd = -(T)p.c_evap * rhow * (Ti - ts) / ts * (T)p.c_dmdot;
+    } else {
+      mdot = (T)p.c_cond * phic * rhoa * (Ti - ts) / ts;
+      dmd = (T)p.c_cond * rhoa * (Ti - ts) / ts * (T)p.c_dmdot;
+    }
+    const T vdot = mdot / rhoa - mdot / rhow;
+    T rho, mu;
+    if (fluid) {
+      rho = (T)(p.rhow * (1.0 - phicd) + p.rhoa * phicd);
+      mu = (T)(p.muw * (1.0 - phicd) + p.mua * phicd);
+    } else {
+      rho = (T)p.rhos; mu = (T)p.mus;
+    }
+    const T lambda = (T)(-2.0 / 3.0) * mu;
+    if (phid < 0.0 || phid > 1.0) dmd = 0;
+    const T uadv[3] = {ui[0] - umi[0], ui[1] - umi[1], ui[2] - umi[2]};
+    T tmp1[3], rL[3];
+#pragma unroll
+    for (int i = 0; i < 3; ++i) {
+      const T conv = du[i][0] * uadv[0] + du[i][1] * uadv[1] + du[i][2] * uadv[2];
+      tmp1[i] = rho * aci[i] + rho * conv - (T)p.gravvec[i] * rho;
+      rL[i] = tmp1[i] + dp[i];
+    }
+    const T res_phi = rphii + (uadv[0] * dphi[0] + uadv[1] * dphi[1] + uadv[2] * dphi[2]) + phii * vdot - mdot / rhoa;
+    const T taua = quad_uGu<T>(uadv, G);
+    const T nu = mu / rho;
+    const T taud = nu * nu * (T)12.0 * GG;
+    const T tauM = (T)1.0 / (rho * sqrt(taut + taua + taud));
+    const T tauLS = (T)1.0 / sqrt(taut + taua);
+    const T tauC = rho * sqrt(taua + taud) / trG;
+    {
+      const double cf = (double)p.delt * sqrt((double)taua);
+      if (cf > cfl) cfl = cf;
+    }
+    T kdc = 0;
+    if (kdc_on) {
+      const double nk = p.ns_kdc_w * (1.0 - phicd) + p.ns_kdc_a * phicd;
+      const T rr = rL[0] * rL[0] + rL[1] * rL[1] + rL[2] * rL[2];
+      kdc = (T)low_word(nk) * sqrt(rr / GG);
+    }
+    T kdphi = 0;
+    if (kdcphi_on) kdphi = (T)p.lsc_kdc * fabs(res_phi) / sqrt(GG);
+    const T mupk = mu + kdc;
+    const T dmdi = dmd * ira;
+    T* og = o + Lay<OVS_ASM_NSVOF>::GP0 + gp * Lay<OVS_ASM_NSVOF>::GPW;
+    og[0] = uadv[0]; og[1] = uadv[1]; og[2] = uadv[2];
+    og[3] = rho; og[4] = rho * tauM; og[5] = tauLS;
+    og[6] = vdot + phii * ira * dmd - dmd / rhoa;
+    const T wf = fluid ? w : (T)0;   // solid elements contribute nothing
+    og[7] = fact2 * wf * tauC * dmdi * dmdi;
+    og[8] = fact2 * tauC * dmdi * wf;
+    og[9] = fact2 * dmdi * wf;
+    if (!fluid) continue;
+    KA += fact2 * mupk * w;
+    KB += fact2 * (tauC + lambda) * w;
+    MM += fact2 * w * tauM;
+    KDP += fact2 * w * kdphi;
+    T c[4];
+#pragma unroll
+    for (int n = 0; n < 4; ++n) c[n] = uadv[0] * g[n][0] + uadv[1] * g[n][1] + uadv[2] * g[n][2];
+    const T tdiv = -pri + tauC * divu;
+#pragma unroll
+    for (int n = 0; n < 4; ++n) {
+#pragma unroll
+      for (int i = 0; i < 3; ++i)
+        ru[n][i] += w * (-N[n] * tmp1[i] - g[n][i] * tdiv + g[n][i] * tauC * vdot - g[n][i] * lambda * divu -
+                         mupk * svis[n] + rho * c[n] * (-tauM * rL[i]));
+      rp[n] += w * (-N[n] * (divu - vdot) + (g[n][0] * rL[0] + g[n][1] * rL[1] + g[n][2] * rL[2]) * (-tauM));
+      rf[n] += w * (-(N[n] + tauLS * c[n]) * res_phi - kdphi * gdphi[n] + N[n] * dmdi * tauC * (divu - vdot));
+    }
+  }
+#pragma unroll
+  for (int n = 0; n < 4; ++n)
+#pragma unroll
+    for (int d = 0; d < 3; ++d) o[3 * n + d] = g[n][d];
+  o[12] = fluid ? w : (T)0; o[13] = KA; o[14] = KB; o[15] = MM; o[16] = KDP;
+  o[17] = dphi[0]; o[18] = dphi[1]; o[19] = dphi[2];
+#pragma unroll
+  for (int n = 0; n < 4; ++n) {
+    T* orh = o + Lay<OVS_ASM_NSVOF>::RHS0 + 5 * n;
+    orh[0] = ru[n][0]; orh[1] = ru[n][1]; orh[2] = ru[n][2]; orh[3] = rp[n]; orh[4] = rf[n];
+  }
+}
+
+// pass 1, temperature (src/solveQuenching.f90:712-856).  Record layout of
+// this pass: xd(0:2) u(3:5) um(6:8) phi(9) T(10) rT(11).  Solid elements store
+// uadv = dSe = trc = 0, which turns the fluid block formula into the solid one.
+template <typename T>
+__device__ void summarize_tem(const SumArgs& a, const T r[4][16], const T lo[4][4], bool fluid, T* o,
+                              double& cfl, T& detj_out) {
+  const ovs_params& p = a.p;
+  T g[4][3], G[3][3], detj, GG, trG;
+  element_geometry<T>(r, lo, g, G, detj, GG, trG);
+  detj_out = detj;
+  const T w = detj * (T)(0.25 / 6.0);
+  T dT[3];
+#pragma unroll
+  for (int j = 0; j < 3; ++j) dT[j] = r[0][10] * g[0][j] + r[1][10] * g[1][j] + r[2][10] * g[2][j] + r[3][10] * g[3][j];
+  const T fact2 = (T)(p.alfi * p.gami * p.delt);
+  const T ts = (T)p.ts, cpw = (T)p.cpw, cpa = (T)p.cpa, lh = (T)p.lh;
+  T gdT[4];
+#pragma unroll
+  for (int n = 0; n < 4; ++n) gdT[n] = g[n][0] * dT[0] + g[n][1] * dT[1] + g[n][2] * dT[2];
+  T HK = 0, rt[4] = {0, 0, 0, 0};
+  const bool kdc_on = fabs(p.tem_kdc) > 0.0;
+#pragma unroll
+  for (int gp = 0; gp < 4; ++gp) {
+    T N[4];
+    tet_shape<T>(gp, N);
+    const double phid = gp_phi(r, lo, 9, gp);
+    const T Ti = r[0][10] * N[0] + r[1][10] * N[1] + r[2][10] * N[2] + r[3][10] * N[3];
+    const T rTi = r[0][11] * N[0] + r[1][11] * N[1] + r[2][11] * N[2] + r[3][11] * N[3];
+    T ui[3], umi[3];
+#pragma unroll
+    for (int d = 0; d < 3; ++d) {
+      ui[d] = r[0][3 + d] * N[0] + r[1][3 + d] * N[1] + r[2][3 + d] * N[2] + r[3][3 + d] * N[3];
+      umi[d] = r[0][6 + d] * N[0] + r[1][6 + d] * N[1] + r[2][6 + d] * N[2] + r[3][6 + d] * N[3];
+    }
+    const double phicd = fmax(fmin(phid, 1.0), 0.0);
+    const T phic = (T)phicd;
+    T mdot, dmdT;
+    if (Ti > ts) {
+      mdot = (T)p.c_evap * (T)(1.0 - phicd) * (T)p.rhow * (Ti - ts) / ts;
+      dmdT = (T)p.c_evap * (T)(1.0 - phicd) * (T)p.rhow / ts * (T)p.c_dmdot;
+    } else {
+      mdot = (T)p.c_cond * phic * (T)p.rhoa * (Ti - ts) / ts;
+      dmdT = (T)p.c_cond * phic * (T)p.rhoa / ts * (T)p.c_dmdot;
+    }
+    T rho, cp, hk, rcp;
+    if (fluid) {
+      rho = (T)(p.rhow * (1.0 - phicd) + p.rhoa * phicd);
+      cp = (T)(p.cpw * (1.0 - phicd) + p.cpa * phicd);
+      hk = (T)(p.kappaw * (1.0 - phicd) + p.kappaa * phicd);
+      rcp = (T)((p.rhow * p.cpw) * (1.0 - phicd) + (p.rhoa * p.cpa) * phicd);
+    } else {
+      rho = (T)p.rhos; cp = (T)p.cps; hk = (T)p.kappas; rcp = (T)(p.rhos * p.cps);
+    }
+    const T uadv[3] = {ui[0] - umi[0], ui[1] - umi[1], ui[2] - umi[2]};
+    const T Se = ((cpw - cpa) * (Ti - ts) - lh) * mdot;
+    const T udT = uadv[0] * dT[0] + uadv[1] * dT[1] + uadv[2] * dT[2];
+    const T res = rcp * (rTi + udT) - Se;
+    const T taua = quad_uGu<T>(uadv, G);
+    T tt = taua + (T)(4.0 / (p.delt * p.delt));
+    const T kk = hk / (rho * cp);
+    tt = tt + kk * kk * (T)12.0 * GG;
+    const T tauT = (T)1.0 / (rho * cp * sqrt(tt));
+    {
+      const double cf = (double)p.delt * sqrt((double)taua);
+      if (cf > cfl) cfl = cf;
+    }
+    T kdcT = 0;
+    if (kdc_on && fluid) kdcT = (T)p.tem_kdc * fabs(res) / sqrt(GG) / (T)p.tref;
+    const T dSe = (cpw - cpa) * mdot + ((cpw - cpa) * (Ti - ts) - lh) * dmdT;
+    T* og = o + Lay<OVS_ASM_TEM>::GP0 + gp * Lay<OVS_ASM_TEM>::GPW;
+    og[3] = rcp;
+    if (fluid) {
+      og[0] = uadv[0]; og[1] = uadv[1]; og[2] = uadv[2];
+      og[4] = dSe; og[5] = tauT * rcp;
+      HK += fact2 * (hk + kdcT) * w;
+#pragma unroll
+      for (int n = 0; n < 4; ++n) {
+        const T cn = uadv[0] * g[n][0] + uadv[1] * g[n][1] + uadv[2] * g[n][2];
+        rt[n] += w * (-N[n] * rcp * (rTi + udT) + N[n] * Se - rcp * tauT * cn * res - (hk + kdcT) * gdT[n]);
+      }
+    } else {
+      og[0] = og[1] = og[2] = 0; og[4] = 0; og[5] = 0;
+      HK += fact2 * hk * w;
+#pragma unroll
+      for (int n = 0; n < 4; ++n) rt[n] += w * (-N[n] * rcp * rTi - hk * gdT[n]);
+    }
+  }
+#pragma unroll
+  for (int n = 0; n < 4; ++n)
+#pragma unroll
+    for (int d = 0; d < 3; ++d) o[3 * n + d] = g[n][d];
+  o[12] = w; o[13] = HK;
+#pragma unroll
+  for (int n = 0; n < 4; ++n) o[Lay<OVS_ASM_TEM>::RHS0 + n] = rt[n];
+  o[42] = 0; o[43] = 0;
+}
+
+// -------------------------------------------------- pass 2: block expansion
+// Blocks of row A (local node la) of one element from its summary, for the
+// column nodes b = 0..3 (formulas factored from the reference's per Gauss
+// point sums; see the notes at each kind):
+//   K(i,j) = KA ga_j gb_i + KB ga_i gb_j + delta_ij (KA gab + S_b)
+//   G(i) = -ga_i P_b + gb_i Q        D(i) = gb_i R + ga_i T_b     M = MM gab
+//   LS = L1_b + KDP gab + E_b   ULS(i) = ga_i U_b   PLS = PL_b
+//   LSU(i) = dphi_i V_b - gb_i W
+// with the Gauss-point sums S_b = sum w rho (Na + rt ca)(fact1 Nb + fact2 cb),
+// P_b = sum fact2 w Nb, Q = sum fact2 w rt ca, R = sum fact2 w Na,
+// T_b = sum w rt (fact1 Nb + fact2 cb), L1_b = sum w (Na + tauLS ca)
+// (fact1 Nb + fact2 cb + fact2 Nb src), E_b = sum eps Na Nb,
+// U_b = sum ufac Nb, PL_b = -sum plfac Na Nb, V_b = sum fact2 w (Na +
+// tauLS ca) Nb, W = sum ufac Na, where c_n = uadv . grad N_n.
+template <typename T>
+__device__ __forceinline__ void ldv4(const T* p, T* d) {
+  if constexpr (sizeof(T) == 4) {
+    const float4 v = __ldg(reinterpret_cast<const float4*>(p));
+    d[0] = v.x; d[1] = v.y; d[2] = v.z; d[3] = v.w;
+  } else {
+    const double2 a = __ldg(reinterpret_cast<const double2*>(p)), b = __ldg(reinterpret_cast<const double2*>(p) + 1);
+    d[0] = a.x; d[1] = a.y; d[2] = b.x; d[3] = b.y;
+  }
+}
+
+template <typename T, int KIND>
+__device__ __forceinline__ void expand_row(const ovs_params& p, const T* sm, int la, T* blk, int nvp, T* rv) {
+  using L = Lay<KIND>;
+  T hd[16];
+#pragma unroll
+  for (int k = 0; k < 16; k += 4) ldv4(sm + k, hd + k);
+  T g[4][3];
+#pragma unroll
+  for (int n = 0; n < 4; ++n)
+#pragma unroll
+    for (int d = 0; d < 3; ++d) g[n][d] = hd[3 * n + d];
+  const T w = hd[12];
+  const T ga[3] = {la == 0 ? g[0][0] : la == 1 ? g[1][0] : la == 2 ? g[2][0] : g[3][0],
+                   la == 0 ? g[0][1] : la == 1 ? g[1][1] : la == 2 ? g[2][1] : g[3][1],
+                   la == 0 ? g[0][2] : la == 1 ? g[1][2] : la == 2 ? g[2][2] : g[3][2]};
+  T gab[4];
+#pragma unroll
+  for (int b = 0; b < 4; ++b) gab[b] = ga[0] * g[b][0] + ga[1] * g[b][1] + ga[2] * g[b][2];
+  if constexpr (KIND == OVS_ASM_TEM) {
+    const T fact1 = (T)p.almi, fact2 = (T)(p.alfi * p.gami * p.delt);
+    const T HK = hd[13];
+    T Xb[4] = {0, 0, 0, 0};
 #pragma unroll
     for (int gp = 0; gp < 4; ++gp) {
       T N[4];
       tet_shape<T>(gp, N);
-      T ui[3], umi[3], aci[3];
+      const T* q = sm + L::GP0 + gp * L::GPW;
+      const T uadv[3] = {q[0], q[1], q[2]}, rcp = q[3], dSe = q[4], trc = q[5];
+      T c[4];
 #pragma unroll
-      for (int d = 0; d < 3; ++d) {
-        ui[d] = r[0][3 + d] * N[0] + r[1][3 + d] * N[1] + r[2][3 + d] * N[2] + r[3][3 + d] * N[3];
-        umi[d] = r[0][6 + d] * N[0] + r[1][6 + d] * N[1] + r[2][6 + d] * N[2] + r[3][6 + d] * N[3];
-        aci[d] = r[0][9 + d] * N[0] + r[1][9 + d] * N[1] + r[2][9 + d] * N[2] + r[3][9 + d] * N[3];
-      }
-      const T pri = r[0][12] * N[0] + r[1][12] * N[1] + r[2][12] * N[2] + r[3][12] * N[3];
-      const double phid = gp_phi(r, lo, 13, gp);   // VOF in FP64 (property blend)
-      const T phii = (T)phid;
-      const T rphii = r[0][14] * N[0] + r[1][14] * N[1] + r[2][14] * N[2] + r[3][14] * N[3];
-      const T Ti = r[0][15] * N[0] + r[1][15] * N[1] + r[2][15] * N[2] + r[3][15] * N[3];
-      const double phicd = fmax(fmin(phid, 1.0), 0.0);
-      const T phic = (T)phicd;
-      T mdot, dmd;
-      if (Ti > ts) {
-        mdot = (T)p.c_evap * (T)(1.0 - phicd) * rhow * (Ti - ts) / ts;
-        dmd = -(T)p.c_evap * rhow * (Ti - ts) / ts * (T)p.c_dmdot;
-      } else {
-        mdot = (T)p.c_cond * phic * rhoa * (Ti - ts) / ts;
-        dmd = (T)p.c_cond * rhoa * (Ti - ts) / ts * (T)p.c_dmdot;
-      }
-      const T vdot = mdot / rhoa - mdot / rhow;
-      T rho, mu;
-      if (fluid) {
-        rho = (T)(p.rhow * (1.0 - phicd) + p.rhoa * phicd);
-        mu = (T)(p.muw * (1.0 - phicd) + p.mua * phicd);
-      } else {
-        rho = (T)p.rhos; mu = (T)p.mus;
-      }
-      const T lambda = (T)(-2.0 / 3.0) * mu;
-      if (phid < 0.0 || phid > 1.0) dmd = 0;
-      T uadv[3] = {ui[0] - umi[0], ui[1] - umi[1], ui[2] - umi[2]};
-      T tmp1[3], rL[3];
+      for (int b = 0; b < 4; ++b) c[b] = g[b][0] * uadv[0] + g[b][1] * uadv[1] + g[b][2] * uadv[2];
+      const T aw = w * (pick4<T>(N, la) + trc * pick4<T>(c, la));
 #pragma unroll
-      for (int i = 0; i < 3; ++i) {
-        const T conv = du[i][0] * uadv[0] + du[i][1] * uadv[1] + du[i][2] * uadv[2];
-        tmp1[i] = rho * aci[i] + rho * conv - (T)p.gravvec[i] * rho;
-        rL[i] = tmp1[i] + dp[i];
-      }
-      const T res_phi = rphii + (uadv[0] * dphi[0] + uadv[1] * dphi[1] + uadv[2] * dphi[2]) + phii * vdot - mdot / rhoa;
-      const T taua = quad_uGu<T>(uadv, G);
-      const T nu = mu / rho;
-      const T taud = nu * nu * (T)12.0 * GG;
-      const T tauM = (T)1.0 / (rho * sqrt(taut + taua + taud));
-      const T tauLS = (T)1.0 / sqrt(taut + taua);
-      const T tauC = rho * sqrt(taua + taud) / trG;
-      {
-        double cf = (double)p.delt * sqrt((double)taua);
-        if (cf > cfl) cfl = cf;
+      for (int b = 0; b < 4; ++b) Xb[b] += aw * (rcp * (fact1 * N[b] + fact2 * c[b]) - fact2 * dSe * N[b]);
+    }
+#pragma unroll
+    for (int b = 0; b < 4; ++b) blk[b * nvp] = Xb[b] + HK * gab[b];
+    rv[0] = sm[L::RHS0 + la];
+  } else {
+    constexpr bool vof = KIND == OVS_ASM_NSVOF;
+    const T fact1 = (T)p.almi;
+    const T fact2 = vof ? (T)(p.alfi * p.delt * p.gami) : (T)(p.alfi * p.gami * p.delt);
+    const T KA = hd[13], KB = hd[14], MM = hd[15];
+    T KDP = 0, dphi[3] = {0, 0, 0};
+    if constexpr (vof) {
+      T t4[4];
+      ldv4(sm + 16, t4);
+      KDP = t4[0]; dphi[0] = t4[1]; dphi[1] = t4[2]; dphi[2] = t4[3];
+    }
+    T Q = 0, R = 0, W = 0;
+    T Sb[4] = {0, 0, 0, 0}, Pb[4] = {0, 0, 0, 0}, Tb[4] = {0, 0, 0, 0};
+    T L1[4] = {0, 0, 0, 0}, Eb[4] = {0, 0, 0, 0}, Ub[4] = {0, 0, 0, 0}, PLb[4] = {0, 0, 0, 0}, Vb[4] = {0, 0, 0, 0};
+#pragma unroll
+    for (int gp = 0; gp < 4; ++gp) {
+      T N[4];
+      tet_shape<T>(gp, N);
+      const T* q = sm + L::GP0 + gp * L::GPW;
+      T uadv[3], rho, rt;
+      if constexpr (vof) {
+        uadv[0] = q[0]; uadv[1] = q[1]; uadv[2] = q[2]; rho = q[3]; rt = q[4];
+      } else {
+        uadv[0] = q[0]; uadv[1] = q[1]; uadv[2] = q[2]; rho = (T)p.rhoa; rt = q[3];
       }
       T c[4];
 #pragma unroll
       for (int b = 0; b < 4; ++b) c[b] = uadv[0] * g[b][0] + uadv[1] * g[b][1] + uadv[2] * g[b][2];
-      T kdc = 0;
-      if (kdc_on) {
-        double pc = phicd;
-        double nk = p.ns_kdc_w * (1.0 - pc) + p.ns_kdc_a * pc;
-        T rr = rL[0] * rL[0] + rL[1] * rL[1] + rL[2] * rL[2];
-        kdc = (T)low_word(nk) * sqrt(rr / GG);
-      }
-      T kdphi = 0;
-      if (kdcphi_on) kdphi = (T)p.lsc_kdc * fabs(res_phi) / sqrt(GG);
-      if (!fluid) continue;
       const T Na = pick4<T>(N, la), ca = pick4<T>(c, la);
-      const T mupk = mu + kdc;
-      // ---- matrix sums (block formulas after the loop)
-      const T alpha = w * rho * (Na + rho * tauM * ca);
-      const T gam = w * (Na + tauLS * ca);
-      const T dmdi = dmd * ira;
-      const T eps = fact2 * w * tauC * dmdi * dmdi;
-      const T src = vdot + phii * ira * dmd - dmd / rhoa;
-      KA += fact2 * mupk * w;
-      KB += fact2 * (tauC + lambda) * w;
-      Q += fact2 * w * rho * tauM * ca;
+      const T alpha = w * rho * (Na + rt * ca);
+      Q += fact2 * w * rt * ca;
       R += fact2 * w * Na;
-      MM += fact2 * w * tauM;
-      KDP += fact2 * w * kdphi;
-      W += dmdi * fact2 * tauC * w * Na;
 #pragma unroll
       for (int b = 0; b < 4; ++b) {
         const T beta = fact1 * N[b] + fact2 * c[b];
         Sb[b] += alpha * beta;
         Pb[b] += fact2 * w * N[b];
-        Tb[b] += w * tauM * rho * beta;
-        L1[b] += gam * (beta + fact2 * N[b] * src);
-        Eb[b] += eps * Na * N[b];
-        Ub[b] += fact2 * tauC * dmdi * w * N[b];
-        PLb[b] -= fact2 * dmdi * w * Na * N[b];
-        Vb[b] += fact2 * gam * N[b];
+        Tb[b] += w * rt * beta;
       }
-      // ---- residual (src/solveQuenching.f90:496-521)
-      const T tdiv = -pri + tauC * divu;
+      if constexpr (vof) {
+        const T tls = q[5], src = q[6], eps = q[7], ufac = q[8], plfac = q[9];
+        const T gam = w * (Na + tls * ca);
+        W += ufac * Na;
 #pragma unroll
-      for (int i = 0; i < 3; ++i)
-        ru[i] += w * (-Na * tmp1[i] - ga[i] * tdiv + ga[i] * tauC * vdot - ga[i] * lambda * divu - mupk * svis +
-                      rho * ca * (-tauM * rL[i]));
-      rp += w * (-Na * (divu - vdot) + (ga[0] * rL[0] + ga[1] * rL[1] + ga[2] * rL[2]) * (-tauM));
-      rf += w * (-(Na + tauLS * ca) * res_phi - kdphi * gdphi + Na * dmdi * tauC * (divu - vdot));
+        for (int b = 0; b < 4; ++b) {
+          const T beta = fact1 * N[b] + fact2 * c[b];
+          L1[b] += gam * (beta + fact2 * N[b] * src);
+          Eb[b] += eps * Na * N[b];
+          Ub[b] += ufac * N[b];
+          PLb[b] -= plfac * Na * N[b];
+          Vb[b] += fact2 * gam * N[b];
+        }
+      }
     }
-    // ---- blocks of row A:
-    //  K(i,j) = KA ga_j gb_i + KB ga_i gb_j + delta_ij (KA gab + S_b)
-    //  G(i) = -ga_i P_b + gb_i Q        D(i) = gb_i R + ga_i T_b
-    //  M = MM gab   LS = L1_b + KDP gab + E_b   ULS(i) = ga_i U_b
-    //  PLS = PL_b   LSU(i) = dphi_i V_b - gb_i W
 #pragma unroll
     for (int b = 0; b < 4; ++b) {
-      T o[24];
+      T o[L::NV];
       const T* gb = g[b];
       const T dg = KA * gab[b] + Sb[b];
 #pragma unroll
@@ -503,124 +706,20 @@ template <typename T> struct Phys<T, OVS_ASM_NSVOF> {
 #pragma unroll
       for (int d = 0; d < 3; ++d) o[12 + d] = gb[d] * R + ga[d] * Tb[b];
       o[15] = MM * gab[b];
+      if constexpr (vof) {
 #pragma unroll
-      for (int d = 0; d < 3; ++d) o[16 + d] = dphi[d] * Vb[b] - gb[d] * W;
-      o[19] = L1[b] + KDP * gab[b] + Eb[b];
+        for (int d = 0; d < 3; ++d) o[16 + d] = dphi[d] * Vb[b] - gb[d] * W;
+        o[19] = L1[b] + KDP * gab[b] + Eb[b];
 #pragma unroll
-      for (int d = 0; d < 3; ++d) o[20 + d] = ga[d] * Ub[b];
-      o[23] = PLb[b];
-      store_row<24>(blk + b * nvp, o);
-    }
-    rv[0] = ru[0]; rv[1] = ru[1]; rv[2] = ru[2]; rv[3] = rp; rv[4] = rf;
-    return detj;
-  }
-};
-
-// Temperature element, IntElmAss_Tem_Quenching_STAB.  Record layout for
-// this pass: xd(0:2) u(3:5) um(6:8) phi(9) T(10) rT(11).
-template <typename T> struct Phys<T, OVS_ASM_TEM> {
-  static constexpr int NV = 1, NF = 1;
-  __device__ static T eval(const AsmArgs& a, int e, int la, const T r[4][16], const T lo[4][4], bool fluid,
-                           T* blk, int nvp, T* rv, double& cfl) {
-    const ovs_params& p = a.p;
-    T xd[4][3], g[4][3], G[3][3];
-#pragma unroll
-    for (int n = 0; n < 4; ++n)
-#pragma unroll
-      for (int i = 0; i < 3; ++i) xd[n][i] = r[n][i];
-    const T detj = tet_geometry<T>(xd, lo, g, G);
-    const T w = detj * (T)(0.25 / 6.0);
-    T GG = 0;
-#pragma unroll
-    for (int j = 0; j < 3; ++j)
-#pragma unroll
-      for (int i = 0; i < 3; ++i) GG += G[i][j] * G[i][j];
-    T dT[3];
-#pragma unroll
-    for (int j = 0; j < 3; ++j) dT[j] = r[0][10] * g[0][j] + r[1][10] * g[1][j] + r[2][10] * g[2][j] + r[3][10] * g[3][j];
-    const T fact1 = (T)p.almi, fact2 = (T)(p.alfi * p.gami * p.delt);
-    const T ts = (T)p.ts, cpw = (T)p.cpw, cpa = (T)p.cpa, lh = (T)p.lh;
-    const T ga[3] = {la == 0 ? g[0][0] : la == 1 ? g[1][0] : la == 2 ? g[2][0] : g[3][0],
-                     la == 0 ? g[0][1] : la == 1 ? g[1][1] : la == 2 ? g[2][1] : g[3][1],
-                     la == 0 ? g[0][2] : la == 1 ? g[1][2] : la == 2 ? g[2][2] : g[3][2]};
-    T gab[4];
-#pragma unroll
-    for (int b = 0; b < 4; ++b) gab[b] = ga[0] * g[b][0] + ga[1] * g[b][1] + ga[2] * g[b][2];
-    const T gdT = ga[0] * dT[0] + ga[1] * dT[1] + ga[2] * dT[2];
-    T Xb[4] = {0, 0, 0, 0}, HK = 0, rt = 0;
-    const bool kdc_on = fabs(p.tem_kdc) > 0.0;
-#pragma unroll
-    for (int gp = 0; gp < 4; ++gp) {
-      T N[4];
-      tet_shape<T>(gp, N);
-      const double phid = gp_phi(r, lo, 9, gp);
-      const T Ti = r[0][10] * N[0] + r[1][10] * N[1] + r[2][10] * N[2] + r[3][10] * N[3];
-      const T rTi = r[0][11] * N[0] + r[1][11] * N[1] + r[2][11] * N[2] + r[3][11] * N[3];
-      T ui[3], umi[3];
-#pragma unroll
-      for (int d = 0; d < 3; ++d) {
-        ui[d] = r[0][3 + d] * N[0] + r[1][3 + d] * N[1] + r[2][3 + d] * N[2] + r[3][3 + d] * N[3];
-        umi[d] = r[0][6 + d] * N[0] + r[1][6 + d] * N[1] + r[2][6 + d] * N[2] + r[3][6 + d] * N[3];
+        for (int d = 0; d < 3; ++d) o[20 + d] = ga[d] * Ub[b];
+        o[23] = PLb[b];
       }
-      const double phicd = fmax(fmin(phid, 1.0), 0.0);
-      const T phic = (T)phicd;
-      T mdot, dmdT;
-      if (Ti > ts) {
-        mdot = (T)p.c_evap * (T)(1.0 - phicd) * (T)p.rhow * (Ti - ts) / ts;
-        dmdT = (T)p.c_evap * (T)(1.0 - phicd) * (T)p.rhow / ts * (T)p.c_dmdot;
-      } else {
-        mdot = (T)p.c_cond * phic * (T)p.rhoa * (Ti - ts) / ts;
-        dmdT = (T)p.c_cond * phic * (T)p.rhoa / ts * (T)p.c_dmdot;
-      }
-      T rho, cp, hk, rcp;
-      if (fluid) {
-        rho = (T)(p.rhow * (1.0 - phicd) + p.rhoa * phicd);
-        cp = (T)(p.cpw * (1.0 - phicd) + p.cpa * phicd);
-        hk = (T)(p.kappaw * (1.0 - phicd) + p.kappaa * phicd);
-        rcp = (T)((p.rhow * p.cpw) * (1.0 - phicd) + (p.rhoa * p.cpa) * phicd);
-      } else {
-        rho = (T)p.rhos; cp = (T)p.cps; hk = (T)p.kappas; rcp = (T)(p.rhos * p.cps);
-      }
-      T uadv[3] = {ui[0] - umi[0], ui[1] - umi[1], ui[2] - umi[2]};
-      const T Se = ((cpw - cpa) * (Ti - ts) - lh) * mdot;
-      const T udT = uadv[0] * dT[0] + uadv[1] * dT[1] + uadv[2] * dT[2];
-      const T res = rcp * (rTi + udT) - Se;
-      const T taua = quad_uGu<T>(uadv, G);
-      T tt = taua + (T)(4.0 / (p.delt * p.delt));
-      const T kk = hk / (rho * cp);
-      tt = tt + kk * kk * (T)12.0 * GG;
-      const T tauT = (T)1.0 / (rho * cp * sqrt(tt));
-      {
-        double cf = (double)p.delt * sqrt((double)taua);
-        if (cf > cfl) cfl = cf;
-      }
-      T kdcT = 0;
-      if (kdc_on && fluid) kdcT = (T)p.tem_kdc * fabs(res) / sqrt(GG) / (T)p.tref;
-      T c[4];
-#pragma unroll
-      for (int b = 0; b < 4; ++b) c[b] = g[b][0] * uadv[0] + g[b][1] * uadv[1] + g[b][2] * uadv[2];
-      const T dSe = (cpw - cpa) * mdot + ((cpw - cpa) * (Ti - ts) - lh) * dmdT;
-      const T Na = pick4<T>(N, la), ca = pick4<T>(c, la);
-      if (fluid) {
-        // xTebe(a,b) = sum w (Na + tauT rcp ca)[rcp(fact1 Nb + fact2 cb) - fact2 dSe Nb] + fact2 (hk+kdc) gab w
-        const T aw = w * (Na + tauT * rcp * ca);
-#pragma unroll
-        for (int b = 0; b < 4; ++b) Xb[b] += aw * (rcp * (fact1 * N[b] + fact2 * c[b]) - fact2 * dSe * N[b]);
-        HK += fact2 * (hk + kdcT) * w;
-        rt += w * (-Na * rcp * (rTi + udT) + Na * Se - rcp * tauT * ca * res - (hk + kdcT) * gdT);
-      } else {
-#pragma unroll
-        for (int b = 0; b < 4; ++b) Xb[b] += w * Na * rcp * fact1 * N[b];
-        HK += fact2 * hk * w;
-        rt += w * (-Na * rcp * rTi - hk * gdT);
-      }
+      store_row<L::NV>(blk + b * nvp, o);
     }
 #pragma unroll
-    for (int b = 0; b < 4; ++b) blk[b * nvp] = Xb[b] + HK * gab[b];
-    rv[0] = rt;
-    return detj;
+    for (int f = 0; f < L::NF; ++f) rv[f] = sm[L::RHS0 + L::NF * la + f];
   }
-};
+}
 
 template <typename T> struct Vec4 {};
 template <> struct Vec4<float> {
@@ -643,7 +742,7 @@ template <> struct Vec4<double> {
 
 // shared-memory layout per warp
 template <typename T, int KIND> struct Smem {
-  static constexpr int NV = Phys<T, KIND>::NV, NF = Phys<T, KIND>::NF;
+  static constexpr int NV = Lay<KIND>::NV, NF = Lay<KIND>::NF;
   // per-lane stride of the element rows, padded so that 16-byte stores of
   // the 32 lanes spread over all banks
   static constexpr int NVP = (NV < 4) ? 1 : NV;
@@ -657,14 +756,65 @@ template <typename T, int KIND> struct Smem {
   }
 };
 
-// ------------------------------------------------------------ the kernel
+// ---------------------------------------------------------- pass 1 kernel
+template <typename T, int KIND>
+__global__ void __launch_bounds__(128)
+element_summary_kernel(const SumArgs a) {
+  using L = Lay<KIND>;
+  const int e = blockIdx.x * blockDim.x + threadIdx.x;
+  double cfl = 0.0;
+  int nbad = 0;
+  if (e < a.E) {
+    const int4 nd = __ldg(reinterpret_cast<const int4*>(a.ien) + e);
+    const int nodes[4] = {nd.x, nd.y, nd.z, nd.w};
+    T r[4][16], lo[4][4];
+    const T* rec = reinterpret_cast<const T*>(a.rec);
+#pragma unroll
+    for (int n = 0; n < 4; ++n) load_rec(rec, nodes[n], r[n], lo[n]);
+    const int eid = __ldg(a.elm_id + e);
+    T o[L::SW];
+    T detj;
+    if constexpr (KIND == OVS_ASM_NS) {
+      const bool target = ((a.p.subdomain_flag & 1) && eid == a.p.elm_id_set[0]) ||
+                          ((a.p.subdomain_flag & 2) && eid == a.p.elm_id_set[1]);
+      summarize_ns<T>(a, r, lo, target, o, cfl, detj);
+    } else if constexpr (KIND == OVS_ASM_NSVOF) {
+      summarize_nsvof<T>(a, r, lo, eid == a.p.fluid_elm_id, o, cfl, detj);
+    } else {
+      summarize_tem<T>(a, r, lo, eid == a.p.fluid_elm_id, o, cfl, detj);
+    }
+    if (!(detj > (T)0)) nbad = 1;
+    store_row<L::SW>(reinterpret_cast<T*>(a.sum) + (size_t)e * L::SW, o);
+  }
+#pragma unroll
+  for (int off = 16; off > 0; off >>= 1) {
+    cfl = fmax(cfl, __shfl_xor_sync(0xffffffffu, cfl, off));
+    nbad += __shfl_xor_sync(0xffffffffu, nbad, off);
+  }
+  if ((threadIdx.x & 31) == 0) {
+    cfl_max(a.cfl_bits, cfl);
+    if (nbad) atomicAdd(a.flags, nbad);
+  }
+}
+
+// ---------------------------------------------------------- pass 2 kernel
+// The masks of the Dirichlet treatment, per value position v:
+// bits 0-7 row (A) constraints, 8-15 column (B) constraints, 16-23 the
+// diagonal entry set to 1 per element.
+__device__ __forceinline__ unsigned mask_of(int v) {
+  return (unsigned)c_rowbits[v] | ((unsigned)c_colbits[v] << 8) | ((unsigned)c_diagbit[v] << 16);
+}
+
 template <typename T, int KIND, int WARPS>
 __global__ void __launch_bounds__(WARPS * 32)
 assemble_rows_kernel(const AsmArgs a) {
-  using P = Phys<T, KIND>;
   using S = Smem<T, KIND>;
-  constexpr int NV = P::NV, NF = P::NF, NVP = S::NVP, LSTR = S::LSTR, RSTR = S::RSTR;
+  using L = Lay<KIND>;
+  constexpr int NV = S::NV, NF = S::NF, NVP = S::NVP, LSTR = S::LSTR, RSTR = S::RSTR;
   extern __shared__ __align__(16) unsigned char smem_raw[];
+  __shared__ unsigned masks[24];
+  if (threadIdx.x < 24) masks[threadIdx.x] = (KIND == OVS_ASM_TEM) ? (TB | (TB << 8) | (TB << 16)) : mask_of(threadIdx.x);
+  __syncthreads();
   const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
   unsigned char* base = smem_raw + (size_t)wid * S::bytes(a.max_deg);
   T* blk = reinterpret_cast<T*>(base);                 // [32][LSTR]
@@ -675,10 +825,8 @@ assemble_rows_kernel(const AsmArgs a) {
   int* slot = reinterpret_cast<int*>(base + off);      // [32][4]
   int* cols = slot + 32 * 4;                           // [max_deg]
 
-  const T* rec = reinterpret_cast<const T*>(a.rec);
+  const T* sum = reinterpret_cast<const T*>(a.rec);
   const int nwarps_total = gridDim.x * WARPS;
-  double cfl = 0.0;
-  int ndet = 0;
   for (int A = blockIdx.x * WARPS + wid; A < a.N; A += nwarps_total) {
     const int rp = a.rowptr[A], deg = a.rowptr[A + 1] - rp;
     const int ep = a.n2e_ptr[A], ne = a.n2e_ptr[A + 1] - ep;
@@ -688,27 +836,14 @@ assemble_rows_kernel(const AsmArgs a) {
     __syncwarp();
     for (int c0 = 0; c0 < ne; c0 += 32) {
       const int nc = min(32, ne - c0);
-      // ---------------- phase 1: lane = element
+      // ---------------- phase 1: lane = element: A's row of its matrix
       if (lane < nc) {
-        const int packed = a.n2e[ep + c0 + lane];
+        const int packed = __ldg(a.n2e + ep + c0 + lane);
         const int e = packed >> 3, la = packed & 7;
-        const int4 nd = reinterpret_cast<const int4*>(a.ien)[e];
+        const int4 nd = __ldg(reinterpret_cast<const int4*>(a.ien) + e);
         const int nodes[4] = {nd.x, nd.y, nd.z, nd.w};
-        T r[4][16], lo[4][4];
-#pragma unroll
-        for (int n = 0; n < 4; ++n) load_rec(rec, nodes[n], r[n], lo[n]);
-        const int eid = a.elm_id[e];
-        bool active;
-        if (KIND == OVS_ASM_NS) {
-          active = ((a.p.subdomain_flag & 1) && eid == a.p.elm_id_set[0]) ||
-                   ((a.p.subdomain_flag & 2) && eid == a.p.elm_id_set[1]);
-        } else {
-          active = eid == a.p.fluid_elm_id;
-        }
         T rv[NF];
-        T* myblk = blk + lane * LSTR;
-        const T detj = P::eval(a, e, la, r, lo, active, myblk, NVP, rv, cfl);
-        if (!(detj > (T)0)) ++ndet;
+        expand_row<T, KIND>(a.p, sum + (size_t)e * L::SW, la, blk + lane * LSTR, NVP, rv);
 #pragma unroll
         for (int f = 0; f < NF; ++f) rvs[lane * RSTR + f] = rv[f];
         // slot of each column node in row A (cols is sorted ascending)
@@ -716,7 +851,7 @@ assemble_rows_kernel(const AsmArgs a) {
         for (int b = 0; b < 4; ++b) {
           int lo = 0, hi = deg;
           while (hi - lo > 1) {
-            int mid = (lo + hi) >> 1;
+            const int mid = (lo + hi) >> 1;
             if (cols[mid] > nodes[b]) hi = mid; else lo = mid;
           }
           slot[lane * 4 + b] = lo;
@@ -724,63 +859,73 @@ assemble_rows_kernel(const AsmArgs a) {
       }
       __syncwarp();
       // ---------------- phase 2: ordered segmented reduction into acc
+      // elements are added one after another in ascending element id; the
+      // nshl blocks of one element go to distinct slots (elements with a
+      // repeated node are rejected at upload)
       if constexpr (NV >= 4) {
-        constexpr int NG = NV / 4;             // 4-value groups per block
+        constexpr int NG = NV / 4;
         for (int j = 0; j < nc; ++j) {
-          for (int q = lane; q < 4 * NG; q += 32) {
-            const int b = q / NG, gidx = q - b * NG;
+          if (lane < 4 * NG) {
+            const int b = lane / NG, gidx = lane - b * NG;
             const int s = slot[j * 4 + b];
             Vec4<T>::add(acc + s * NVP + gidx * 4, blk + j * LSTR + b * NVP + gidx * 4);
           }
           __syncwarp();
         }
       } else {
-        if (lane == 0)
-          for (int j = 0; j < nc; ++j)
-#pragma unroll
-            for (int b = 0; b < 4; ++b) acc[slot[j * 4 + b]] += blk[j * LSTR + b];
+        for (int j = 0; j < nc; ++j) {
+          if (lane < 4) acc[slot[j * 4 + lane]] += blk[j * LSTR + lane];
+          __syncwarp();
+        }
       }
       if (lane < NF)
         for (int j = 0; j < nc; ++j) racc += rvs[j * RSTR + lane];
       __syncwarp();
     }
     // ---------------- row write with the Dirichlet treatment
-    const uint8_t ibA = a.ibc[A];
+    const unsigned ibA = a.ibc[A];
     if (a.mat) {
       T* out = reinterpret_cast<T*>(a.vals) + (size_t)rp * NV;
       const T cnt = (T)ne;
-      for (int q = lane; q < deg * NV; q += 32) {
-        const int s = q / NV, v = q - s * NV;
-        const int B = cols[s];
-        const uint8_t ibB = a.ibc[B];
-        T val = acc[s * NVP + v];
-        uint8_t rb, cb, db;
-        if constexpr (KIND == OVS_ASM_TEM) { rb = TB; cb = TB; db = TB; }
-        else { rb = c_rowbits[v]; cb = c_colbits[v]; db = c_diagbit[v]; }
-        if ((ibA & rb) || (ibB & cb)) val = (T)0;
-        if (B == A && (ibA & db)) val = cnt;
-        out[q] = val;
+      if constexpr (NV >= 4) {
+        // one 4-value group per lane and step, 16-byte aligned (NV % 4 == 0)
+        constexpr int NG = NV / 4;
+        for (int q = lane; q < deg * NG; q += 32) {
+          const int s = q / NG, gidx = q - s * NG;
+          const int B = cols[s];
+          const unsigned ibB = __ldg(a.ibc + B);
+          const bool dg = B == A;
+          T v4[4];
+#pragma unroll
+          for (int t = 0; t < 4; ++t) {
+            const unsigned m = masks[4 * gidx + t];
+            T val = acc[s * NVP + 4 * gidx + t];
+            if ((ibA & m & 0xffu) || ((ibB << 8) & m & 0xff00u)) val = (T)0;
+            if (dg && ((ibA << 16) & m & 0xff0000u)) val = cnt;
+            v4[t] = val;
+          }
+          store_row<4>(out + (size_t)s * NV + 4 * gidx, v4);
+        }
+      } else {
+        for (int q = lane; q < deg; q += 32) {
+          const int B = cols[q];
+          const unsigned ibB = __ldg(a.ibc + B);
+          T val = acc[q];
+          if ((ibA & TB) || (ibB & TB)) val = (T)0;
+          if (B == A && (ibA & TB)) val = cnt;
+          out[q] = val;
+        }
       }
     }
     if (a.vec && lane < NF) {
-      uint8_t bit;
+      unsigned bit;
       if (KIND == OVS_ASM_TEM) bit = TB;
-      else bit = (lane < 3) ? (uint8_t)(1 << lane) : (lane == 3 ? PB : FB);
+      else bit = (lane < 3) ? (1u << lane) : (lane == 3 ? PB : FB);
       T v = (ibA & bit) ? (T)0 : racc;
       if (!isfinite((double)v)) atomicOr(a.flags + 1, 1);
       reinterpret_cast<T*>(a.rhs)[(size_t)lane * a.N + A] = v;
     }
     __syncwarp();
-  }
-  // warp max of the CFL and count of bad Jacobians
-#pragma unroll
-  for (int o = 16; o > 0; o >>= 1) {
-    cfl = fmax(cfl, __shfl_xor_sync(0xffffffffu, cfl, o));
-    ndet += __shfl_xor_sync(0xffffffffu, ndet, o);
-  }
-  if (lane == 0) {
-    cfl_max(a.cfl_bits, cfl);
-    if (ndet) atomicAdd(a.flags, ndet);
   }
 }
 
@@ -835,8 +980,13 @@ __global__ void alpha_records_kernel(const AlphaArgs a) {
 }
 
 template <typename T, int KIND>
-int launch_assemble(ovs_ctx* c, const AsmArgs& a) {
-  constexpr int WARPS = sizeof(T) == 8 ? 2 : 4;
+int launch_assemble(ovs_ctx* c, const AsmArgs& a, const SumArgs& sa) {
+  // pass 1: element summaries
+  element_summary_kernel<T, KIND><<<(sa.E + 127) / 128, 128, 0, c->stream>>>(sa);
+  ++c->launches;
+  OVS_CUDA_TRY(cudaGetLastError());
+  // pass 2: rows
+  constexpr int WARPS = 4;
   using S = Smem<T, KIND>;
   const size_t smem = S::bytes(a.max_deg) * WARPS;
   auto kern = assemble_rows_kernel<T, KIND, WARPS>;
@@ -845,7 +995,7 @@ int launch_assemble(ovs_ctx* c, const AsmArgs& a) {
   OVS_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, WARPS * 32, smem));
   if (per_sm < 1) return OVS_ERR_ARG;
   long need = ((long)c->N + WARPS - 1) / WARPS;
-  long grid = (long)per_sm * c->num_sms * 8;
+  long grid = (long)per_sm * c->num_sms * 4;
   if (grid > need) grid = need;
   if (grid < 1) grid = 1;
   kern<<<(int)grid, WARPS * 32, smem, c->stream>>>(a);
@@ -856,19 +1006,31 @@ int launch_assemble(ovs_ctx* c, const AsmArgs& a) {
 
 }  // namespace
 
-static int dispatch_assemble(ovs_ctx* c, int kernel, int prec, const AsmArgs& a) {
-  if (prec == OVS_FP64) {
-    if (kernel == OVS_ASM_NS) return launch_assemble<double, OVS_ASM_NS>(c, a);
-    if (kernel == OVS_ASM_NSVOF) return launch_assemble<double, OVS_ASM_NSVOF>(c, a);
-    return launch_assemble<double, OVS_ASM_TEM>(c, a);
-  }
-  if (kernel == OVS_ASM_NS) return launch_assemble<float, OVS_ASM_NS>(c, a);
-  if (kernel == OVS_ASM_NSVOF) return launch_assemble<float, OVS_ASM_NSVOF>(c, a);
-  return launch_assemble<float, OVS_ASM_TEM>(c, a);
+static int sum_width(int kernel) {
+  return kernel == OVS_ASM_NS ? Lay<OVS_ASM_NS>::SW : (kernel == OVS_ASM_NSVOF ? Lay<OVS_ASM_NSVOF>::SW : Lay<OVS_ASM_TEM>::SW);
 }
 
-static void fill_args(ovs_ctx* c, int prec, SysStore& S, int tensor_flag, AsmArgs& a) {
-  a.rec = c->rec[prec];
+static int dispatch_assemble(ovs_ctx* c, int kernel, int prec, const AsmArgs& a, const SumArgs& sa) {
+  if (prec == OVS_FP64) {
+    if (kernel == OVS_ASM_NS) return launch_assemble<double, OVS_ASM_NS>(c, a, sa);
+    if (kernel == OVS_ASM_NSVOF) return launch_assemble<double, OVS_ASM_NSVOF>(c, a, sa);
+    return launch_assemble<double, OVS_ASM_TEM>(c, a, sa);
+  }
+  if (kernel == OVS_ASM_NS) return launch_assemble<float, OVS_ASM_NS>(c, a, sa);
+  if (kernel == OVS_ASM_NSVOF) return launch_assemble<float, OVS_ASM_NSVOF>(c, a, sa);
+  return launch_assemble<float, OVS_ASM_TEM>(c, a, sa);
+}
+
+static void fill_args(ovs_ctx* c, int prec, SysStore& S, int tensor_flag, AsmArgs& a, SumArgs& sa) {
+  sa.rec = c->rec[prec];
+  sa.ien = c->ien;
+  sa.elm_id = c->elm_id;
+  sa.sum = c->esum[prec];
+  sa.flags = c->flags;
+  sa.cfl_bits = c->cfl_bits;
+  sa.E = c->E;
+  sa.p = c->params;
+  a.rec = c->esum[prec];     // pass 2 reads the summaries
   a.ien = c->ien;
   a.elm_id = c->elm_id;
   a.ibc = c->ibc;
@@ -891,14 +1053,15 @@ int ovs_profile_assemble(ovs_ctx* c, int kernel, int prec, int reps, double* ms)
   if (kernel != OVS_ASM_NS && kernel != OVS_ASM_NSVOF && kernel != OVS_ASM_TEM) return OVS_ERR_ARG;
   const int sys = kernel == OVS_ASM_NS ? OVS_SYS_NS : (kernel == OVS_ASM_NSVOF ? OVS_SYS_NSVOF : OVS_SYS_TEM);
   SysStore& S = c->sys[sys][prec];
-  if (!S.vals || !S.rhs || !c->rec[prec]) return OVS_ERR_STATE;
+  if (!S.vals || !S.rhs || !c->rec[prec] || !c->esum[prec]) return OVS_ERR_STATE;
   AsmArgs a;
-  fill_args(c, prec, S, OVS_TENSOR_MAT | OVS_TENSOR_VEC, a);
+  SumArgs sa;
+  fill_args(c, prec, S, OVS_TENSOR_MAT | OVS_TENSOR_VEC, a, sa);
   int st;
-  if ((st = dispatch_assemble(c, kernel, prec, a))) return st;  // warm
+  if ((st = dispatch_assemble(c, kernel, prec, a, sa))) return st;  // warm
   OVS_CUDA_TRY(cudaEventRecord(c->ev0, c->stream));
   for (int r = 0; r < reps; ++r)
-    if ((st = dispatch_assemble(c, kernel, prec, a))) return st;
+    if ((st = dispatch_assemble(c, kernel, prec, a, sa))) return st;
   OVS_CUDA_TRY(cudaEventRecord(c->ev1, c->stream));
   OVS_CUDA_TRY(cudaEventSynchronize(c->ev1));
   float t = 0.f;
@@ -920,6 +1083,7 @@ int ovs_assemble_impl(ovs_ctx* c, int kernel, int tensor_flag, int prec, double*
   if ((st = ovs_ensure(&S.vals, ts * (size_t)c->nnz * nv))) return st;
   if ((st = ovs_ensure(&S.rhs, ts * (size_t)c->N * nf))) return st;
   if ((st = ovs_ensure(&c->rec[prec], ts * (size_t)c->N * REC))) return st;
+  if ((st = ovs_ensure(&c->esum[prec], ts * (size_t)c->E * Lay<OVS_ASM_NSVOF>::SW))) return st;
   cudaStream_t s = c->stream;
   OVS_CUDA_TRY(cudaMemsetAsync(c->flags, 0, sizeof(int) * 4, s));
   OVS_CUDA_TRY(cudaMemsetAsync(c->cfl_bits, 0, sizeof(unsigned long long), s));
@@ -936,8 +1100,9 @@ int ovs_assemble_impl(ovs_ctx* c, int kernel, int tensor_flag, int prec, double*
   ++c->launches;
   OVS_CUDA_TRY(cudaGetLastError());
   AsmArgs a;
-  fill_args(c, prec, S, tensor_flag, a);
-  if ((st = dispatch_assemble(c, kernel, prec, a))) return st;
+  SumArgs sa;
+  fill_args(c, prec, S, tensor_flag, a, sa);
+  if ((st = dispatch_assemble(c, kernel, prec, a, sa))) return st;
   if (a.mat) S.have_mat = true;
   if (a.vec) S.have_rhs = true;
   int hflags[4];

@@ -219,7 +219,7 @@ int ovs_destroy(ovs_ctx* c) {
   cudaSetDevice(c->device);
   if (c->stream) cudaStreamSynchronize(c->stream);
   void* ptrs[] = {c->ien, c->elm_id, c->ibc, c->rowptr, c->colidx, c->diag, c->n2e_ptr, c->n2e,
-                  c->rec[0], c->rec[1], c->gm, c->basis[0], c->basis[1], c->work64, c->work32,
+                  c->rec[0], c->rec[1], c->esum[0], c->esum[1], c->gm, c->basis[0], c->basis[1], c->work64, c->work32, c->wvec, c->coop_part,
                   c->flags, c->cfl_bits};
   for (void* p : ptrs) if (p) cudaFree(p);
   for (int f = 0; f < OVS_F_COUNT; ++f) if (c->field[f]) cudaFree(c->field[f]);
@@ -632,7 +632,7 @@ int ovs_profile(ovs_ctx* c, int what, int system, int precision, int reps, doubl
   int st;
   if ((st = ovs_activate(c))) return st;
   if (what == OVS_PROF_ASSEMBLE) return ovs_profile_assemble(c, system, precision, reps, avg_ms);
-  if (what != OVS_PROF_SPMV && what != OVS_PROF_MGS) return OVS_ERR_ARG;
+  if (what != OVS_PROF_SPMV && what != OVS_PROF_ARNOLDI) return OVS_ERR_ARG;
   if (!sys_ok(c, system, precision)) return OVS_ERR_ARG;
   return ovs_profile_krylov(c, what, system, precision, reps, avg_ms);
 }

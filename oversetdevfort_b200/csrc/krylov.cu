@@ -22,8 +22,11 @@
 // per batch of iterations.
 #include "ovs_internal.cuh"
 
+#include <cooperative_groups.h>
 #include <math.h>
 #include <string.h>
+
+namespace cg = cooperative_groups;
 
 namespace {
 
@@ -41,27 +44,32 @@ __device__ __forceinline__ void ld4(const double* p, double v[4]) {
   v[0] = a.x; v[1] = a.y; v[2] = b.x; v[3] = b.y;
 }
 
-template <typename A, typename B> struct AccT { using type = double; };
-template <> struct AccT<float, float> { using type = float; };
+// Accumulation precision of the SpMV: FP32 storage accumulates in FP32 on
+// the mixed path (the inner solver of the refinement), FP64 otherwise.
+// (FP64 accumulation and an FP64 work vector in Gram-Schmidt were measured on
+// the 2.1M-node quench system: they converged in as many refinement cycles
+// and ran slower, so the mixed path keeps everything in FP32 except the dots,
+// Givens and the refinement residual.)
+template <typename A, typename B, bool ACC64> struct AccT { using type = double; };
+template <> struct AccT<float, float, false> { using type = float; };
 
 // MODE 0: y = A x ; MODE 1: y = P^-1 A x ; MODE 2: y = b - A x
 // Block systems: NG groups of 4 values per slot, one lane per group.
 //   NS   (NG=4): groups rows u1,u2,u3,p over columns (u1,u2,u3,p)
 //   NSVOF(NG=6): + row phi over (u1,u2,u3,phi), + column phi into (u1,u2,u3,p)
-template <int NG, typename TM, typename TX, typename TY, int MODE>
-__global__ void __launch_bounds__(SPMV_THREADS)
-spmv_block_kernel(int N, const int* __restrict__ rowptr, const int* __restrict__ colidx,
-                  const TM* __restrict__ vals, const TX* __restrict__ x, TY* __restrict__ y,
-                  const TM* __restrict__ pre, const double* __restrict__ b,
-                  const int* __restrict__ done) {
-  using AT = typename AccT<TM, TX>::type;
-  if (done && *done) return;
+// The RPW = 32/NG rows of warp chunk `wglob` (all 32 lanes take part in
+// the shuffles).
+template <int NG, typename TM, typename TX, typename TY, int MODE, bool ACC64>
+__device__ __forceinline__ void spmv_block_warp(long wglob, int N, const int* __restrict__ rowptr,
+                                                const int* __restrict__ colidx, const TM* __restrict__ vals,
+                                                const TX* __restrict__ x, TY* __restrict__ y,
+                                                const TM* __restrict__ pre, const double* __restrict__ b) {
+  using AT = typename AccT<TM, TX, ACC64>::type;
   constexpr int NV = 4 * NG;
   constexpr int RPW = 32 / NG;  // rows per warp
   const int lane = threadIdx.x & 31;
   const int sub = lane / NG;
   const int g = lane - sub * NG;
-  const long wglob = ((long)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   const long rowl = wglob * RPW + sub;
   const bool active = sub < RPW && rowl < N;
   const int row = active ? (int)rowl : 0;
@@ -128,18 +136,26 @@ spmv_block_kernel(int N, const int* __restrict__ rowptr, const int* __restrict__
   y[(size_t)g * N + row] = (TY)z;
 }
 
-// scalar CSR (temperature): 8 lanes per row
-template <typename TM, typename TX, typename TY, int MODE>
+template <int NG, typename TM, typename TX, typename TY, int MODE, bool ACC64>
 __global__ void __launch_bounds__(SPMV_THREADS)
-spmv_scalar_kernel(int N, const int* __restrict__ rowptr, const int* __restrict__ colidx,
-                   const TM* __restrict__ vals, const TX* __restrict__ x, TY* __restrict__ y,
-                   const TM* __restrict__ pre, const double* __restrict__ b,
-                   const int* __restrict__ done) {
-  using AT = typename AccT<TM, TX>::type;
+spmv_block_kernel(int N, const int* __restrict__ rowptr, const int* __restrict__ colidx,
+                  const TM* __restrict__ vals, const TX* __restrict__ x, TY* __restrict__ y,
+                  const TM* __restrict__ pre, const double* __restrict__ b,
+                  const int* __restrict__ done) {
   if (done && *done) return;
+  const long wglob = ((long)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  spmv_block_warp<NG, TM, TX, TY, MODE, ACC64>(wglob, N, rowptr, colidx, vals, x, y, pre, b);
+}
+
+// scalar CSR (temperature): 8 lanes per row
+template <typename TM, typename TX, typename TY, int MODE, bool ACC64>
+__device__ __forceinline__ void spmv_scalar_warp(long wglob, int N, const int* __restrict__ rowptr,
+                                                 const int* __restrict__ colidx, const TM* __restrict__ vals,
+                                                 const TX* __restrict__ x, TY* __restrict__ y,
+                                                 const TM* __restrict__ pre, const double* __restrict__ b) {
+  using AT = typename AccT<TM, TX, ACC64>::type;
   const int lane = threadIdx.x & 31;
   const int sub = lane >> 3, k = lane & 7;
-  const long wglob = ((long)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   const long rowl = wglob * 4 + sub;
   const bool active = rowl < N;
   const int row = active ? (int)rowl : 0;
@@ -158,7 +174,18 @@ spmv_scalar_kernel(int N, const int* __restrict__ rowptr, const int* __restrict_
   y[row] = (TY)z;
 }
 
-template <typename TM, typename TX, typename TY, int MODE>
+template <typename TM, typename TX, typename TY, int MODE, bool ACC64>
+__global__ void __launch_bounds__(SPMV_THREADS)
+spmv_scalar_kernel(int N, const int* __restrict__ rowptr, const int* __restrict__ colidx,
+                   const TM* __restrict__ vals, const TX* __restrict__ x, TY* __restrict__ y,
+                   const TM* __restrict__ pre, const double* __restrict__ b,
+                   const int* __restrict__ done) {
+  if (done && *done) return;
+  const long wglob = ((long)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  spmv_scalar_warp<TM, TX, TY, MODE, ACC64>(wglob, N, rowptr, colidx, vals, x, y, pre, b);
+}
+
+template <typename TM, typename TX, typename TY, int MODE, bool ACC64 = true>
 int launch_spmv(ovs_ctx* c, int sys, const TM* vals, const TX* x, TY* y, const TM* pre,
                 const double* b, const int* done) {
   const int N = c->N;
@@ -167,19 +194,19 @@ int launch_spmv(ovs_ctx* c, int sys, const TM* vals, const TX* x, TY* y, const T
   long blocks = (warps * 32 + SPMV_THREADS - 1) / SPMV_THREADS;
   if (sys == OVS_SYS_NS)
     {
-      spmv_block_kernel<4, TM, TX, TY, MODE><<<(int)blocks, SPMV_THREADS, 0, c->stream>>>(
+      spmv_block_kernel<4, TM, TX, TY, MODE, ACC64><<<(int)blocks, SPMV_THREADS, 0, c->stream>>>(
           N, c->rowptr, c->colidx, vals, x, y, pre, b, done);
       ++c->launches;
     }
   else if (sys == OVS_SYS_NSVOF)
     {
-      spmv_block_kernel<6, TM, TX, TY, MODE><<<(int)blocks, SPMV_THREADS, 0, c->stream>>>(
+      spmv_block_kernel<6, TM, TX, TY, MODE, ACC64><<<(int)blocks, SPMV_THREADS, 0, c->stream>>>(
           N, c->rowptr, c->colidx, vals, x, y, pre, b, done);
       ++c->launches;
     }
   else
     {
-      spmv_scalar_kernel<TM, TX, TY, MODE><<<(int)blocks, SPMV_THREADS, 0, c->stream>>>(
+      spmv_scalar_kernel<TM, TX, TY, MODE, ACC64><<<(int)blocks, SPMV_THREADS, 0, c->stream>>>(
           N, c->rowptr, c->colidx, vals, x, y, pre, b, done);
       ++c->launches;
     }
@@ -289,10 +316,10 @@ dot_kernel(const TA* __restrict__ a, const TB* __restrict__ b, size_t n, GmresDe
 
 // ---------------------------------------------------------------- GMRES
 // v0 = P^-1 rhs (rhs FP64), ||v0||^2 -> unorm0, epsnrm, e(1)
-template <typename TM, typename TV>
+template <typename TM, typename TV = double>
 __global__ void __launch_bounds__(OVS_RED_THREADS)
 gm_start_kernel(int N, int nf, int sys, const double* __restrict__ rhs, const TM* __restrict__ pre,
-                TV* __restrict__ v0, double tol, GmresDev* gm) {
+                TV* __restrict__ v0, double tol, GmresDev* gm) {  // v0: FP64 work vector
   __shared__ double sh[32];
   double s = 0.0;
   for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < (size_t)N;
@@ -334,38 +361,82 @@ gm_start_kernel(int N, int nf, int sys, const double* __restrict__ rhs, const TM
   }
 }
 
-// v /= gm->unorm0 (first vector) or v /= sqrt(gm->beta) (later vectors)
-template <typename TV>
+// Krylov vectors are stored with a padded leading dimension (multiple of
+// 64 values) so every basis vector starts 256-byte aligned.  The vector
+// being orthogonalized, w, is kept in FP64 whatever the basis precision, so
+// the projections of Gram-Schmidt do not lose the small remainder to FP32
+// rounding; only normalized vectors are rounded into the basis.
+inline size_t basis_ld(size_t n) { return (n + 63) & ~(size_t)63; }
+
+__device__ __forceinline__ void ld4v(const float* p, double v[4]) {
+  const float4 q = *reinterpret_cast<const float4*>(p);
+  v[0] = q.x; v[1] = q.y; v[2] = q.z; v[3] = q.w;
+}
+__device__ __forceinline__ void ld4v(const double* p, double v[4]) {
+  const double2 a = reinterpret_cast<const double2*>(p)[0], b = reinterpret_cast<const double2*>(p)[1];
+  v[0] = a.x; v[1] = a.y; v[2] = b.x; v[3] = b.y;
+}
+__device__ __forceinline__ void st4v(float* p, const double v[4]) {
+  *reinterpret_cast<float4*>(p) = make_float4((float)v[0], (float)v[1], (float)v[2], (float)v[3]);
+}
+__device__ __forceinline__ void st4v(double* p, const double v[4]) {
+  reinterpret_cast<double2*>(p)[0] = make_double2(v[0], v[1]);
+  reinterpret_cast<double2*>(p)[1] = make_double2(v[2], v[3]);
+}
+
+// v = w / d with d = unorm0 (first vector) or sqrt(beta) (later vectors):
+// the normalization of SparseGMRES_NS.f90:159-160,291-294
+template <typename TV, typename TW>
 __global__ void __launch_bounds__(OVS_RED_THREADS)
-gm_scale_kernel(TV* __restrict__ v, size_t n, GmresDev* gm, int first) {
+gm_normalize_kernel(const TW* w, TV* v, size_t n, GmresDev* gm, int first) {
   if (gm->done && !first) return;
   const double d = first ? gm->unorm0 : sqrt(gm->beta);
-  if (!(d > 0.0)) return;
-  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x)
-    v[i] = (TV)((double)v[i] / d);
+  if (!(d != 0.0)) return;
+  const size_t n4 = n >> 2, stride = (size_t)gridDim.x * blockDim.x;
+  const size_t t0 = blockIdx.x * (size_t)blockDim.x + threadIdx.x;
+  for (size_t q = t0; q < n4; q += stride) {
+    double a[4];
+    ld4v(w + 4 * q, a);
+    a[0] /= d; a[1] /= d; a[2] /= d; a[3] /= d;
+    st4v(v + 4 * q, a);
+  }
+  for (size_t i = 4 * n4 + t0; i < n; i += stride) v[i] = (TV)((double)w[i] / d);
 }
 
 // One modified Gram-Schmidt step j (1-based) of iteration k:
 //   j >= 2: w -= beta * v_{j-1};  beta = <w, v_j>;  H(j,k) = beta
-// (SparseGMRES_NS.f90:246-287; v_{k+1} is w itself)
-template <typename TV>
+// (SparseGMRES_NS.f90:246-287); vj == nullptr means v_{k+1} = w itself.
+template <typename TV, typename TW>
 __global__ void __launch_bounds__(OVS_RED_THREADS)
-gm_mgs_kernel(TV* w, const TV* __restrict__ vprev, const TV* vj, size_t n,
+gm_mgs_kernel(TW* __restrict__ w, const TV* __restrict__ vprev, const TV* __restrict__ vj, size_t n,
               GmresDev* gm, int j, int k) {
   __shared__ double sh[32];
   if (gm->done) return;
   const double beta = gm->beta;
+  const size_t n4 = n >> 2, stride = (size_t)gridDim.x * blockDim.x;
+  const size_t t0 = blockIdx.x * (size_t)blockDim.x + threadIdx.x;
   double s = 0.0;
-  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) {
-    double wi = (double)w[i];
+  for (size_t q = t0; q < n4; q += stride) {
+    double a[4], p[4];
+    ld4v(w + 4 * q, a);
     if (j >= 2) {
-      wi = wi - beta * (double)vprev[i];
-      const TV ws = (TV)wi;
-      w[i] = ws;
-      wi = (double)ws;
+      ld4v(vprev + 4 * q, p);
+      a[0] = a[0] - beta * p[0]; a[1] = a[1] - beta * p[1];
+      a[2] = a[2] - beta * p[2]; a[3] = a[3] - beta * p[3];
+      st4v(w + 4 * q, a);
+      if (sizeof(TW) == 4) ld4v(w + 4 * q, a);  // continue with the stored (rounded) values
     }
-    const double vv = (vj == w) ? wi : (double)vj[i];
-    s += wi * vv;
+    if (vj) {
+      ld4v(vj + 4 * q, p);
+      s += a[0] * p[0] + a[1] * p[1] + a[2] * p[2] + a[3] * p[3];
+    } else {
+      s += a[0] * a[0] + a[1] * a[1] + a[2] * a[2] + a[3] * a[3];
+    }
+  }
+  for (size_t i = 4 * n4 + t0; i < n; i += stride) {
+    double a = (double)w[i];
+    if (j >= 2) { a = a - beta * (double)vprev[i]; const TW ar = (TW)a; w[i] = ar; a = (double)ar; }
+    s += a * (vj ? (double)vj[i] : a);
   }
   double part = block_sum(s, sh);
   double tot;
@@ -376,9 +447,8 @@ gm_mgs_kernel(TV* w, const TV* __restrict__ vprev, const TV* vj, size_t n,
 }
 
 // H(k+1,k) = sqrt(beta), Givens rotations of column k, e update, exit test
-// (SparseGMRES_NS.f90:289-327); single thread
-__global__ void gm_givens_kernel(GmresDev* gm, int k) {
-  if (gm->done) return;
+// (SparseGMRES_NS.f90:289-327); one thread
+__device__ void givens_step(GmresDev* gm, int k) {
   const int ld = gm->kspace + 1;
   double* Hk = gm->H + (size_t)(k - 1) * ld;
   const double unorm = sqrt(gm->beta);
@@ -409,6 +479,105 @@ __global__ void gm_givens_kernel(GmresDev* gm, int k) {
   }
 }
 
+__global__ void gm_givens_kernel(GmresDev* gm, int k) {
+  if (gm->done) return;
+  givens_step(gm, k);
+}
+
+// One Arnoldi iteration k in a single cooperative launch (all blocks
+// co-resident): w = P^-1 A v_k into basis slot k, the k+1 modified
+// Gram-Schmidt steps of the reference order with one grid-wide barrier
+// each, the normalization and the Givens update.  The Gram-Schmidt partial
+// sums are double buffered, so one barrier per step suffices; every block
+// adds the partials in the same order, so all see the same beta, and the
+// result does not depend on timing.
+template <typename TM, typename TV, int SYS, bool ACC64>
+__global__ void __launch_bounds__(256)
+gm_arnoldi_kernel(int N, const int* __restrict__ rowptr, const int* __restrict__ colidx,
+                  const TM* __restrict__ vals, const TM* __restrict__ pre, TV* V, size_t ld, size_t n,
+                  int k, GmresDev* gm, double* part) {
+  cg::grid_group grid = cg::this_grid();
+  if (gm->done) return;
+  __shared__ double sh[32];
+  __shared__ double sbeta;
+  const TV* vk = V + ld * (size_t)(k - 1);
+  TV* w = V + ld * (size_t)k;
+  // ---- w = P^-1 A v_k
+  {
+    constexpr int RPW = SYS == OVS_SYS_NS ? 8 : (SYS == OVS_SYS_NSVOF ? 5 : 4);
+    const long nwarps = (long)gridDim.x * (blockDim.x >> 5);
+    const long nchunks = ((long)N + RPW - 1) / RPW;
+    for (long c = ((long)blockIdx.x * blockDim.x + threadIdx.x) >> 5; c < nchunks; c += nwarps) {
+      if constexpr (SYS == OVS_SYS_NS)
+        spmv_block_warp<4, TM, TV, TV, 1, ACC64>(c, N, rowptr, colidx, vals, vk, w, pre, nullptr);
+      else if constexpr (SYS == OVS_SYS_NSVOF)
+        spmv_block_warp<6, TM, TV, TV, 1, ACC64>(c, N, rowptr, colidx, vals, vk, w, pre, nullptr);
+      else
+        spmv_scalar_warp<TM, TV, TV, 1, ACC64>(c, N, rowptr, colidx, vals, vk, w, pre, nullptr);
+    }
+  }
+  grid.sync();
+  // ---- modified Gram-Schmidt, SparseGMRES_NS.f90:246-287
+  const size_t n4 = n >> 2, stride = (size_t)gridDim.x * blockDim.x;
+  const size_t t0 = blockIdx.x * (size_t)blockDim.x + threadIdx.x;
+  const int G = gridDim.x;
+  double beta = 0.0;
+  for (int j = 1; j <= k + 1; ++j) {
+    const TV* vprev = j >= 2 ? V + ld * (size_t)(j - 2) : nullptr;
+    const TV* vj = j <= k ? V + ld * (size_t)(j - 1) : nullptr;
+    double sacc = 0.0;
+    for (size_t q = t0; q < n4; q += stride) {
+      double a[4], pv[4];
+      ld4v(w + 4 * q, a);
+      if (j >= 2) {
+        ld4v(vprev + 4 * q, pv);
+        a[0] = a[0] - beta * pv[0]; a[1] = a[1] - beta * pv[1];
+        a[2] = a[2] - beta * pv[2]; a[3] = a[3] - beta * pv[3];
+        st4v(w + 4 * q, a);
+        if (sizeof(TV) == 4) ld4v(w + 4 * q, a);
+      }
+      if (vj) {
+        ld4v(vj + 4 * q, pv);
+        sacc += a[0] * pv[0] + a[1] * pv[1] + a[2] * pv[2] + a[3] * pv[3];
+      } else {
+        sacc += a[0] * a[0] + a[1] * a[1] + a[2] * a[2] + a[3] * a[3];
+      }
+    }
+    for (size_t i = 4 * n4 + t0; i < n; i += stride) {
+      double a = (double)w[i];
+      if (j >= 2) { a = a - beta * (double)vprev[i]; const TV ar = (TV)a; w[i] = ar; a = (double)ar; }
+      sacc += a * (vj ? (double)vj[i] : a);
+    }
+    const double bp = block_sum(sacc, sh);
+    double* pb = part + (size_t)(j & 1) * G;
+    if (threadIdx.x == 0) pb[blockIdx.x] = bp;
+    grid.sync();
+    double v = 0.0;
+    for (int b = threadIdx.x; b < G; b += blockDim.x) v += __ldcg(pb + b);
+    const double tot = block_sum(v, sh);
+    if (threadIdx.x == 0) sbeta = tot;
+    __syncthreads();
+    beta = sbeta;
+    if (blockIdx.x == 0 && threadIdx.x == 0) {
+      gm->H[(size_t)(k - 1) * (gm->kspace + 1) + (j - 1)] = beta;
+      gm->beta = beta;
+    }
+    __syncthreads();
+  }
+  // ---- normalize (SparseGMRES_NS.f90:291-294) and the Givens update
+  const double unorm = sqrt(beta);
+  if (unorm != 0.0) {
+    for (size_t q = t0; q < n4; q += stride) {
+      double a[4];
+      ld4v(w + 4 * q, a);
+      a[0] /= unorm; a[1] /= unorm; a[2] /= unorm; a[3] /= unorm;
+      st4v(w + 4 * q, a);
+    }
+    for (size_t i = 4 * n4 + t0; i < n; i += stride) w[i] = (TV)((double)w[i] / unorm);
+  }
+  if (blockIdx.x == 0 && threadIdx.x == 0) givens_step(gm, k);
+}
+
 // back-substitution (SparseGMRES_NS.f90:341-346); single thread
 __global__ void gm_backsub_kernel(GmresDev* gm) {
   const int iks = gm->iks, ld = gm->kspace + 1;
@@ -421,12 +590,12 @@ __global__ void gm_backsub_kernel(GmresDev* gm) {
 
 // sol += sum_j y_j v_j (SparseGMRES_NS.f90:349-352)
 template <typename TV>
-__global__ void gm_update_kernel(double* __restrict__ sol, const TV* __restrict__ basis, size_t n,
+__global__ void gm_update_kernel(double* __restrict__ sol, const TV* __restrict__ basis, size_t n, size_t ld,
                                  const GmresDev* __restrict__ gm) {
   const int iks = gm->iks;
   for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) {
     double s = sol[i];
-    for (int j = 0; j < iks; ++j) s = s + gm->y[j] * (double)basis[(size_t)j * n + i];
+    for (int j = 0; j < iks; ++j) s = s + gm->y[j] * (double)basis[(size_t)j * ld + i];
     sol[i] = s;
   }
 }
@@ -456,7 +625,7 @@ int ensure_basis(ovs_ctx* c, int prec, size_t bytes) {
 
 // One GMRES cycle on system `sys` with matrix/preconditioner precision TM
 // and basis precision TV.  rhs and sol are FP64 device vectors (nf*N).
-template <typename TM, typename TV>
+template <typename TM, typename TV, typename TW = double, bool ACC64 = true>
 int gmres_cycle(ovs_ctx* c, int sys, const double* rhs, double* sol, double tol, int kspace,
                 int kmin, ovs_gmres_info* info) {
   const int N = c->N, nf = ovs_sys_nf(sys);
@@ -466,9 +635,14 @@ int gmres_cycle(ovs_ctx* c, int sys, const double* rhs, double* sol, double tol,
   if (!S.vals || !S.binv) return OVS_ERR_STATE;
   if (kspace < 1 || kspace > OVS_MAX_KSPACE) return OVS_ERR_ARG;
   const int bprec = sizeof(TV) == 8 ? OVS_FP64 : OVS_FP32;
+  const size_t ld = basis_ld(n);
   int st;
-  if ((st = ensure_basis(c, bprec, sizeof(TV) * n * (size_t)(kspace + 1)))) return st;
+  if ((st = ensure_basis(c, bprec, sizeof(TV) * ld * (size_t)(kspace + 1)))) return st;
+  if ((st = ovs_ensure((void**)&c->wvec, sizeof(double) * basis_ld(5 * (size_t)N)))) return st;
   TV* V = reinterpret_cast<TV*>(c->basis[bprec]);
+  // w: FP64 work vector, or (TW == TV) the next basis vector itself
+  constexpr bool inplace = sizeof(TW) == sizeof(TV);
+  double* wd = c->wvec;
   GmresDev* gm = c->gm;
   cudaStream_t s = c->stream;
   const TM* vals = as<TM>(S.vals);
@@ -478,35 +652,43 @@ int gmres_cycle(ovs_ctx* c, int sys, const double* rhs, double* sol, double tol,
   OVS_CUDA_TRY(cudaMemcpyAsync(&gm->kspace, km, sizeof(km), cudaMemcpyHostToDevice, s));
   OVS_CUDA_TRY(cudaMemsetAsync(gm->H, 0, sizeof(double) * (size_t)(kspace + 1) * kspace, s));
   OVS_CUDA_TRY(cudaMemsetAsync(gm->e, 0, sizeof(double) * (size_t)(kspace + 1), s));
-  gm_start_kernel<TM, TV><<<OVS_RED_BLOCKS, OVS_RED_THREADS, 0, s>>>(N, nf, sys, rhs, pre, V, tol, gm);
-  gm_scale_kernel<TV><<<OVS_RED_BLOCKS, OVS_RED_THREADS, 0, s>>>(V, n, gm, 1);
+  gm_start_kernel<TM, double><<<OVS_RED_BLOCKS, OVS_RED_THREADS, 0, s>>>(N, nf, sys, rhs, pre, wd, tol, gm);
+  gm_normalize_kernel<TV, double><<<OVS_RED_BLOCKS, OVS_RED_THREADS, 0, s>>>(wd, V, n, gm, 1);
   c->launches += 2;
   OVS_CUDA_TRY(cudaGetLastError());
-  const int batch = N > 200000 ? 2 : 8;
+  // one cooperative launch per Arnoldi iteration
+  void (*kern)(int, const int*, const int*, const TM*, const TM*, TV*, size_t, size_t, int, GmresDev*, double*);
+  if (sys == OVS_SYS_NS) kern = gm_arnoldi_kernel<TM, TV, OVS_SYS_NS, ACC64>;
+  else if (sys == OVS_SYS_NSVOF) kern = gm_arnoldi_kernel<TM, TV, OVS_SYS_NSVOF, ACC64>;
+  else kern = gm_arnoldi_kernel<TM, TV, OVS_SYS_TEM, ACC64>;
+  int per_sm = 0;
+  OVS_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, 256, 0));
+  if (per_sm < 1) return OVS_ERR_CUDA;
+  int grid = per_sm * c->num_sms;
+  if (grid > OVS_COOP_MAX_BLOCKS) grid = OVS_COOP_MAX_BLOCKS;
+  if ((st = ovs_ensure((void**)&c->coop_part, sizeof(double) * 2 * OVS_COOP_MAX_BLOCKS))) return st;
+  const int batch = N > 200000 ? 4 : 16;
   int k = 1;
   for (; k <= kspace;) {
     const int kend = (k + batch - 1 < kspace) ? k + batch - 1 : kspace;
     for (; k <= kend; ++k) {
-      TV* w = V + n * (size_t)k;
-      const TV* vk = V + n * (size_t)(k - 1);
-      if ((st = launch_spmv<TM, TV, TV, 1>(c, sys, vals, vk, w, pre, nullptr, &gm->done))) return st;
-      for (int j = 1; j <= k + 1; ++j) {
-        const TV* vprev = j >= 2 ? V + n * (size_t)(j - 2) : nullptr;
-        const TV* vj = V + n * (size_t)(j - 1);
-        gm_mgs_kernel<TV><<<OVS_RED_BLOCKS, OVS_RED_THREADS, 0, s>>>(w, vprev, vj, n, gm, j, k);
-      }
-      gm_givens_kernel<<<1, 1, 0, s>>>(gm, k);
-      gm_scale_kernel<TV><<<OVS_RED_BLOCKS, OVS_RED_THREADS, 0, s>>>(w, n, gm, 0);
-      c->launches += k + 3;
+      int Nn = N, kk = k;
+      const int* rp = c->rowptr;
+      const int* ci = c->colidx;
+      TV* Vp = V;
+      size_t ldv = ld, nn = n;
+      double* part = c->coop_part;
+      void* args[] = {&Nn, &rp, &ci, (void*)&vals, (void*)&pre, &Vp, &ldv, &nn, &kk, &gm, &part};
+      OVS_CUDA_TRY(cudaLaunchCooperativeKernel((void*)kern, grid, 256, args, 0, s));
+      ++c->launches;
     }
-    OVS_CUDA_TRY(cudaGetLastError());
     OVS_CUDA_TRY(cudaMemcpyAsync(c->h_pinned, &gm->done, sizeof(int), cudaMemcpyDeviceToHost, s));
     OVS_CUDA_TRY(cudaStreamSynchronize(s));
     if (c->h_pinned[0]) break;
   }
   gm_backsub_kernel<<<1, 1, 0, s>>>(gm);
   ++c->launches;
-  gm_update_kernel<TV><<<ovs_grid(n, 256, 4 * c->num_sms * 8), 256, 0, s>>>(sol, V, n, gm);
+  gm_update_kernel<TV><<<ovs_grid(n, 256, 4 * c->num_sms * 8), 256, 0, s>>>(sol, V, n, ld, gm);
   ++c->launches;
   OVS_CUDA_TRY(cudaGetLastError());
   if (info) {
@@ -534,33 +716,56 @@ int dot64(ovs_ctx* c, const double* a, const double* b, size_t n, double* out) {
 
 }  // namespace
 
-int ovs_profile_krylov(ovs_ctx* c, int what, int sys, int prec, int reps, double* ms) {
+template <typename TV>
+__global__ void fill_kernel(TV* __restrict__ p, size_t n, double v) {
+  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x)
+    p[i] = (TV)(v * (1.0 + 1e-3 * (double)(i % 97)));
+}
+
+// Time one Arnoldi iteration (k = 25 of a 50-vector cycle) or one
+// preconditioned SpMV on the resident system.
+template <typename TM, bool ACC64>
+int profile_krylov_t(ovs_ctx* c, int what, int sys, int reps, double* ms) {
+  const int prec = sizeof(TM) == 8 ? OVS_FP64 : OVS_FP32;
   SysStore& S = c->sys[sys][prec];
-  const size_t n = (size_t)c->N * ovs_sys_nf(sys);
-  const size_t ts = prec == OVS_FP64 ? 8 : 4;
+  if (!S.vals) return OVS_ERR_STATE;
   int st;
-  if (what == OVS_PROF_SPMV) {
-    if (!S.vals) return OVS_ERR_STATE;
-    if ((st = ovs_precond_setup(c, sys, prec))) return st;
-  }
-  if ((st = ensure_basis(c, prec, ts * n * 3))) return st;
-  OVS_CUDA_TRY(cudaMemsetAsync(c->basis[prec], 0, ts * n * 3, c->stream));
-  OVS_CUDA_TRY(cudaMemsetAsync(&c->gm->done, 0, sizeof(int), c->stream));
-  OVS_CUDA_TRY(cudaMemsetAsync(&c->gm->kspace, 0x7f, sizeof(int), c->stream));
+  if ((st = ovs_precond_setup(c, sys, prec))) return st;
+  const size_t n = (size_t)c->N * ovs_sys_nf(sys);
+  const size_t ld = basis_ld(n);
+  const int kspace = 50, k = 25;
+  if ((st = ensure_basis(c, prec, sizeof(TM) * ld * (kspace + 1)))) return st;
+  TM* V = reinterpret_cast<TM*>(c->basis[prec]);
+  fill_kernel<TM><<<1184, 256, 0, c->stream>>>(V, ld * (kspace + 1), 1.0);
+  GmresDev* gm = c->gm;
+  int km[2] = {kspace, 1};
+  OVS_CUDA_TRY(cudaMemcpyAsync(&gm->kspace, km, sizeof(km), cudaMemcpyHostToDevice, c->stream));
+  OVS_CUDA_TRY(cudaMemsetAsync(&gm->done, 0, sizeof(int), c->stream));
+  OVS_CUDA_TRY(cudaMemsetAsync(&gm->epsnrm, 0, sizeof(double), c->stream));
+  const TM* vals = as<TM>(S.vals);
+  const TM* pre = as<TM>(S.binv);
+  void (*kern)(int, const int*, const int*, const TM*, const TM*, TM*, size_t, size_t, int, GmresDev*, double*);
+  if (sys == OVS_SYS_NS) kern = gm_arnoldi_kernel<TM, TM, OVS_SYS_NS, ACC64>;
+  else if (sys == OVS_SYS_NSVOF) kern = gm_arnoldi_kernel<TM, TM, OVS_SYS_NSVOF, ACC64>;
+  else kern = gm_arnoldi_kernel<TM, TM, OVS_SYS_TEM, ACC64>;
+  int per_sm = 0;
+  OVS_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, 256, 0));
+  int grid = per_sm * c->num_sms;
+  if (grid > OVS_COOP_MAX_BLOCKS) grid = OVS_COOP_MAX_BLOCKS;
+  if ((st = ovs_ensure((void**)&c->coop_part, sizeof(double) * 2 * OVS_COOP_MAX_BLOCKS))) return st;
   auto run = [&]() -> int {
-    if (prec == OVS_FP64) {
-      double* V = reinterpret_cast<double*>(c->basis[prec]);
-      if (what == OVS_PROF_SPMV)
-        return launch_spmv<double, double, double, 1>(c, sys, as<double>(S.vals), V, V + n, as<double>(S.binv), nullptr, nullptr);
-      gm_mgs_kernel<double><<<OVS_RED_BLOCKS, OVS_RED_THREADS, 0, c->stream>>>(V + n, V, V + 2 * n, n, c->gm, 2, 1);
-    } else {
-      float* V = reinterpret_cast<float*>(c->basis[prec]);
-      if (what == OVS_PROF_SPMV)
-        return launch_spmv<float, float, float, 1>(c, sys, as<float>(S.vals), V, V + n, as<float>(S.binv), nullptr, nullptr);
-      gm_mgs_kernel<float><<<OVS_RED_BLOCKS, OVS_RED_THREADS, 0, c->stream>>>(V + n, V, V + 2 * n, n, c->gm, 2, 1);
+    if (what == OVS_PROF_SPMV) {
+      st = launch_spmv<TM, TM, TM, 1, ACC64>(c, sys, vals, V, V + ld, pre, nullptr, nullptr);
+      return st;
     }
+    int Nn = c->N, kk = k;
+    const int* rp = c->rowptr;
+    const int* ci = c->colidx;
+    size_t ldv = ld, nn = n;
+    double* part = c->coop_part;
+    void* args[] = {&Nn, &rp, &ci, (void*)&vals, (void*)&pre, &V, &ldv, &nn, &kk, &gm, &part};
+    OVS_CUDA_TRY(cudaLaunchCooperativeKernel((void*)kern, grid, 256, args, 0, c->stream));
     ++c->launches;
-    OVS_CUDA_TRY(cudaGetLastError());
     return OVS_OK;
   };
   if ((st = run())) return st;
@@ -573,6 +778,11 @@ int ovs_profile_krylov(ovs_ctx* c, int what, int sys, int prec, int reps, double
   OVS_CUDA_TRY(cudaEventElapsedTime(&t, c->ev0, c->ev1));
   *ms = (double)t / reps;
   return OVS_OK;
+}
+
+int ovs_profile_krylov(ovs_ctx* c, int what, int sys, int prec, int reps, double* ms) {
+  if (prec == OVS_FP64) return profile_krylov_t<double, true>(c, what, sys, reps, ms);
+  return profile_krylov_t<float, false>(c, what, sys, reps, ms);
 }
 
 int ovs_dot_impl(ovs_ctx* c, const double* a, const double* b, size_t n, double* out) {
@@ -671,8 +881,8 @@ int ovs_solve_impl(ovs_ctx* c, int sys, int mode, double rtol, int kspace, int m
     if (tin < floor_tol) tin = floor_tol;
     if (tin > 0.5) tin = 0.5;
     ovs_gmres_info gi;
-    if (prec == OVS_FP64) st = gmres_cycle<double, double>(c, sys, r, x, tin, kspace, 1, &gi);
-    else st = gmres_cycle<float, float>(c, sys, r, x, tin, kspace, 1, &gi);
+    if (prec == OVS_FP64) st = gmres_cycle<double, double, double, true>(c, sys, r, x, tin, kspace, 1, &gi);
+    else st = gmres_cycle<float, float, float, false>(c, sys, r, x, tin, kspace, 1, &gi);
     if (st) return st;
     iters += gi.iterations;
     ++cycles;

@@ -10,6 +10,7 @@
 #define OVS_MAX_KSPACE 400     // largest Krylov space
 #define OVS_RED_BLOCKS 592     // fixed grid of every deterministic reduction (4 x 148 SMs)
 #define OVS_RED_THREADS 256
+#define OVS_COOP_MAX_BLOCKS 4096  // largest cooperative grid of the Arnoldi kernel
 
 #define OVS_CUDA_TRY(expr)                                   \
   do {                                                       \
@@ -82,6 +83,8 @@ struct ovs_ctx {
   double* field[OVS_F_COUNT] = {};
   // alpha-stage node records (16 values per node), per precision
   void* rec[2] = {nullptr, nullptr};
+  // per-element summaries of the element pass, per precision
+  void* esum[2] = {nullptr, nullptr};
   // systems [sys][prec]
   SysStore sys[4][2];
   // last solution of each system (FP64, field-major)
@@ -92,6 +95,8 @@ struct ovs_ctx {
   size_t basis_bytes[2] = {0, 0};
   double* work64 = nullptr;              // 3 vectors of 5N doubles (b, r, x)
   float* work32 = nullptr;               // 1 vector of 5N floats
+  double* wvec = nullptr;                // FP64 vector under orthogonalization
+  double* coop_part = nullptr;           // partial sums of the cooperative Arnoldi kernel
   // status words: [0] negative DetJ count, [1] non-finite flag
   int* flags = nullptr;
   unsigned long long* cfl_bits = nullptr;
