@@ -258,6 +258,33 @@ int ovs_last_device_ms(ovs_ctx* ctx, double* ms);
 int ovs_host_alloc(void** p, size_t bytes);
 int ovs_host_free(void* p);
 
+/* ------------------------------------------------- allocation-free solve
+ * No counterpart in the reference: an addition for callers that cannot
+ * allocate device memory at solve time - code inside a framework whose
+ * memory pool owns the device memory, time-critical loops that cannot take
+ * the device-wide synchronization of cudaMalloc/cudaFree, plug-in hosts that
+ * only allow allocation at initialization.
+ *
+ * One GMRES cycle with SparseGMRES_tem semantics (as ovs_gmres with
+ * OVS_SYS_TEM) on a caller-owned scalar CSR system in DEVICE memory:
+ * rowptr[n+1], colidx[nnz] (0-based, rows sorted), vals[nnz], rhs[n] (FP64),
+ * sol[n] accumulated into.  It calls no cudaMalloc/cudaFree and no allocating
+ * library routine: all its temporaries live in one fixed __device__ array of
+ * OVS_NOALLOC_SCRATCH_BYTES inside the library (held by every GPU that loads
+ * the library until the process exits).  Limits: n <= OVS_NOALLOC_MAX_N and
+ * kspace <= OVS_NOALLOC_MAX_KSPACE; larger requests return OVS_ERR_ARG.
+ * The first call on a device looks up the device address of that array, so
+ * make it before any stream capture.  All calls share the array: calls that
+ * overlap on the GPU (other streams, other host threads) race.  `stream` is
+ * a cudaStream_t (NULL: default stream); the call returns after the solve. */
+#define OVS_NOALLOC_MAX_N 16384
+#define OVS_NOALLOC_MAX_KSPACE 40
+#define OVS_NOALLOC_SCRATCH_BYTES 5537792
+int ovs_gmres_tem_noalloc(int n, const int* rowptr, const int* colidx,
+                          const double* vals, const double* rhs, double* sol,
+                          double tol, int kspace, int kspace_min, void* stream,
+                          ovs_gmres_info* info);
+
 #ifdef __cplusplus
 }
 #endif
