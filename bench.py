@@ -101,6 +101,28 @@ class ClockSampler:
                 "power_w_max": max(power) if power else None}
 
 
+# ------------------------------------------------------------- multi-rank
+def max_over_ranks(dist, x: float, device: str) -> float:
+    """Max of a per-rank number over all ranks (identity without a process
+    group).  NCCL needs a CUDA tensor; gloo takes a CPU one."""
+    if dist is None:
+        return x
+    import torch
+    t = torch.tensor([x], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def barrier(dist) -> None:
+    if dist is not None:
+        dist.barrier()
+
+
+def replica_throughput(world: int, elements_per_rank: int, ms_max: float) -> float:
+    """Whole-job Melem/s of `world` replicas timed as the max over ranks."""
+    return world * elements_per_rank / (ms_max * 1e-3) / 1e6
+
+
 # -------------------------------------------------------------- CPU oracle
 def config3_slab(n: int, k0: int, nl: int):
     """Layers k0..k0+nl of the n^3 quench cube, same geometry and fields
@@ -207,17 +229,14 @@ def run_ours(args, world, rank, local_rank, dist):
     nnz = ctx.icnt
     setup_s = time.time() - t_setup
 
-    def barrier():
-        if dist is not None:
-            dist.barrier()
+    dev = f"cuda:{local_rank}"
+    _barrier = barrier
+
+    def barrier_():
+        _barrier(dist)
 
     def maxr(x: float) -> float:
-        if dist is None:
-            return x
-        import torch
-        t = torch.tensor([x], dtype=torch.float64, device=f"cuda:{local_rank}")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        return float(t.item())
+        return max_over_ranks(dist, x, dev)
 
     def assembly_pass(prec):
         ctx.assemble(F.OVS_ASM_NSVOF, 6, prec)
@@ -243,17 +262,17 @@ def run_ours(args, world, rank, local_rank, dist):
     for prec, name in ((F.OVS_FP32, "fp32"), (F.OVS_FP64, "fp64")):
         for _ in range(args.warmup):
             assembly_pass(prec)
-        barrier()
+        barrier_()
         ctx.synchronize()
         t0 = time.time()
         ms = [assembly_pass(prec) for _ in range(args.steps)]
         ctx.synchronize()
         wall = time.time() - t0
-        barrier()
+        barrier_()
         res[name] = {"ms": maxr(statistics.mean(ms)), "wall_s": wall}
     launches_step = (ctx.launch_count() - launches0) / (2 * (args.warmup + args.steps))
     ms_step = res["fp32"]["ms"]
-    value = world * E / (ms_step * 1e-3) / 1e6
+    value = replica_throughput(world, E, ms_step)
 
     # --------------------------------------------- kernel roofline
     prof = {}
@@ -294,9 +313,9 @@ def run_ours(args, world, rank, local_rank, dist):
             for sysid, kern, key in ((F.OVS_SYS_NSVOF, F.OVS_ASM_NSVOF, "nsvof"),
                                      (F.OVS_SYS_TEM, F.OVS_ASM_TEM, "tem")):
                 ctx.assemble(kern, 6, mode)
-                barrier()
+                barrier_()
                 sol, info = ctx.solve(sysid, mode, args.rtol, kspace=args.kspace, max_cycles=args.max_cycles)
-                barrier()
+                barrier_()
                 rec[key] = {"s": maxr(info.seconds), "iterations": info.iterations, "cycles": info.cycles,
                             "rel_residual": info.rel_residual, "converged": bool(info.converged)}
                 sols[(name, key)] = sol
@@ -339,12 +358,12 @@ def run_ours(args, world, rank, local_rank, dist):
 
     for _ in range(args.warmup):
         e2e_step()
-    barrier()
+    barrier_()
     t0 = time.perf_counter()
     for _ in range(args.steps):
         e2e_step()
     e2e_s = maxr((time.perf_counter() - t0) / args.steps)
-    barrier()
+    barrier_()
     clk = clocks.stop()
     total_launches = ctx.launch_count() - launches0
 
