@@ -284,6 +284,8 @@ def run_ours(args, world, rank, local_rank, dist):
     prof["spmv_nsvof_fp64_ms"] = ctx.profile(F.OVS_PROF_SPMV, F.OVS_SYS_NSVOF, F.OVS_FP64, 10)
     prof["arnoldi_k25_nsvof_fp32_ms"] = ctx.profile(F.OVS_PROF_ARNOLDI, F.OVS_SYS_NSVOF, F.OVS_FP32, 10)
     prof["arnoldi_k25_nsvof_fp64_ms"] = ctx.profile(F.OVS_PROF_ARNOLDI, F.OVS_SYS_NSVOF, F.OVS_FP64, 10)
+    prof["arnoldi_fused_k25_nsvof_fp32_ms"] = ctx.profile(F.OVS_PROF_ARNOLDI_FUSED, F.OVS_SYS_NSVOF, F.OVS_FP32, 10)
+    prof["arnoldi_fused_k25_nsvof_fp64_ms"] = ctx.profile(F.OVS_PROF_ARNOLDI_FUSED, F.OVS_SYS_NSVOF, F.OVS_FP64, 10)
 
     def spmv_bytes(s):  # values, colidx, rowptr, x gather (once), y, preconditioner
         return 24 * nnz * s + 4 * nnz + 4 * (N + 1) + 5 * N * s + 5 * N * s + 11 * N * s

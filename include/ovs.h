@@ -236,7 +236,7 @@ int ovs_residual_norms(ovs_ctx* ctx, int precision, double r[4]);
 
 /* ----------------------------------------------------------- measurement
  * Hooks for benchmarking; they have no counterpart in the reference. */
-enum { OVS_PROF_SPMV = 1, OVS_PROF_ASSEMBLE = 2, OVS_PROF_ARNOLDI = 3 };
+enum { OVS_PROF_SPMV = 1, OVS_PROF_ASSEMBLE = 2, OVS_PROF_ARNOLDI = 3, OVS_PROF_ARNOLDI_FUSED = 4 };
 /* Average device time in ms (CUDA events on the context stream) of `reps`
  * back-to-back launches of one internal kernel on the resident data:
  *   OVS_PROF_SPMV      preconditioned SpMV y = P^-1 A x of `system`, matrix
@@ -246,7 +246,11 @@ enum { OVS_PROF_SPMV = 1, OVS_PROF_ASSEMBLE = 2, OVS_PROF_ARNOLDI = 3 };
  *                      the last ovs_assemble of that kernel and precision;
  *   OVS_PROF_ARNOLDI   one Arnoldi iteration (preconditioned SpMV, k+1
  *                      Gram-Schmidt steps, normalization, Givens) at k = 25
- *                      of a 50-vector cycle, `system` in `precision`. */
+ *                      of a 50-vector cycle, `system` in `precision`, as
+ *                      the solvers run it (SpMV launch, then Gram-Schmidt
+ *                      with the new vector held on chip);
+ *   OVS_PROF_ARNOLDI_FUSED  the same iteration as one cooperative launch
+ *                      (the variant selected by OVS_ARNOLDI_FUSED=1). */
 int ovs_profile(ovs_ctx* ctx, int what, int system, int precision, int reps,
                 double* avg_ms);
 /* number of CUDA kernels this context has launched so far */

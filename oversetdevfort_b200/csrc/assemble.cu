@@ -1006,10 +1006,6 @@ int launch_assemble(ovs_ctx* c, const AsmArgs& a, const SumArgs& sa) {
 
 }  // namespace
 
-static int sum_width(int kernel) {
-  return kernel == OVS_ASM_NS ? Lay<OVS_ASM_NS>::SW : (kernel == OVS_ASM_NSVOF ? Lay<OVS_ASM_NSVOF>::SW : Lay<OVS_ASM_TEM>::SW);
-}
-
 static int dispatch_assemble(ovs_ctx* c, int kernel, int prec, const AsmArgs& a, const SumArgs& sa) {
   if (prec == OVS_FP64) {
     if (kernel == OVS_ASM_NS) return launch_assemble<double, OVS_ASM_NS>(c, a, sa);

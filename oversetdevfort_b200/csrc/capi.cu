@@ -1,5 +1,6 @@
 // C ABI of the library (include/ovs.h): context, mesh/state transfer,
 // reference-layout conversions, Newton update and residual norms.
+#include <cstdlib>
 #include "ovs_internal.cuh"
 
 #include <math.h>
@@ -184,6 +185,10 @@ int ovs_create(ovs_ctx** out, const ovs_dims* dims) {
   ovs_ctx* c = new ovs_ctx();
   OVS_CUDA_TRY(cudaGetDevice(&c->device));
   OVS_CUDA_TRY(cudaDeviceGetAttribute(&c->num_sms, cudaDevAttrMultiProcessorCount, c->device));
+  {
+    const char* e = getenv("OVS_ARNOLDI_FUSED");
+    c->arnoldi_fused = e && e[0] == '1';
+  }
   c->N = dims->nnode;
   c->E = dims->nelem;
   c->nshl = dims->nshl;
@@ -632,7 +637,7 @@ int ovs_profile(ovs_ctx* c, int what, int system, int precision, int reps, doubl
   int st;
   if ((st = ovs_activate(c))) return st;
   if (what == OVS_PROF_ASSEMBLE) return ovs_profile_assemble(c, system, precision, reps, avg_ms);
-  if (what != OVS_PROF_SPMV && what != OVS_PROF_ARNOLDI) return OVS_ERR_ARG;
+  if (what != OVS_PROF_SPMV && what != OVS_PROF_ARNOLDI && what != OVS_PROF_ARNOLDI_FUSED) return OVS_ERR_ARG;
   if (!sys_ok(c, system, precision)) return OVS_ERR_ARG;
   return ovs_profile_krylov(c, what, system, precision, reps, avg_ms);
 }

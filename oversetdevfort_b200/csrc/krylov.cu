@@ -403,49 +403,6 @@ gm_normalize_kernel(const TW* w, TV* v, size_t n, GmresDev* gm, int first) {
   for (size_t i = 4 * n4 + t0; i < n; i += stride) v[i] = (TV)((double)w[i] / d);
 }
 
-// One modified Gram-Schmidt step j (1-based) of iteration k:
-//   j >= 2: w -= beta * v_{j-1};  beta = <w, v_j>;  H(j,k) = beta
-// (SparseGMRES_NS.f90:246-287); vj == nullptr means v_{k+1} = w itself.
-template <typename TV, typename TW>
-__global__ void __launch_bounds__(OVS_RED_THREADS)
-gm_mgs_kernel(TW* __restrict__ w, const TV* __restrict__ vprev, const TV* __restrict__ vj, size_t n,
-              GmresDev* gm, int j, int k) {
-  __shared__ double sh[32];
-  if (gm->done) return;
-  const double beta = gm->beta;
-  const size_t n4 = n >> 2, stride = (size_t)gridDim.x * blockDim.x;
-  const size_t t0 = blockIdx.x * (size_t)blockDim.x + threadIdx.x;
-  double s = 0.0;
-  for (size_t q = t0; q < n4; q += stride) {
-    double a[4], p[4];
-    ld4v(w + 4 * q, a);
-    if (j >= 2) {
-      ld4v(vprev + 4 * q, p);
-      a[0] = a[0] - beta * p[0]; a[1] = a[1] - beta * p[1];
-      a[2] = a[2] - beta * p[2]; a[3] = a[3] - beta * p[3];
-      st4v(w + 4 * q, a);
-      if (sizeof(TW) == 4) ld4v(w + 4 * q, a);  // continue with the stored (rounded) values
-    }
-    if (vj) {
-      ld4v(vj + 4 * q, p);
-      s += a[0] * p[0] + a[1] * p[1] + a[2] * p[2] + a[3] * p[3];
-    } else {
-      s += a[0] * a[0] + a[1] * a[1] + a[2] * a[2] + a[3] * a[3];
-    }
-  }
-  for (size_t i = 4 * n4 + t0; i < n; i += stride) {
-    double a = (double)w[i];
-    if (j >= 2) { a = a - beta * (double)vprev[i]; const TW ar = (TW)a; w[i] = ar; a = (double)ar; }
-    s += a * (vj ? (double)vj[i] : a);
-  }
-  double part = block_sum(s, sh);
-  double tot;
-  if (finish_reduction(gm, part, &tot)) {
-    gm->beta = tot;
-    gm->H[(size_t)(k - 1) * (gm->kspace + 1) + (j - 1)] = tot;
-  }
-}
-
 // H(k+1,k) = sqrt(beta), Givens rotations of column k, e update, exit test
 // (SparseGMRES_NS.f90:289-327); one thread
 __device__ void givens_step(GmresDev* gm, int k) {
@@ -477,11 +434,6 @@ __device__ void givens_step(GmresDev* gm, int k) {
     gm->converged = er <= gm->epsnrm;
     gm->breakdown = brk;
   }
-}
-
-__global__ void gm_givens_kernel(GmresDev* gm, int k) {
-  if (gm->done) return;
-  givens_step(gm, k);
 }
 
 // One Arnoldi iteration k in a single cooperative launch (all blocks
@@ -578,6 +530,344 @@ gm_arnoldi_kernel(int N, const int* __restrict__ rowptr, const int* __restrict__
   if (blockIdx.x == 0 && threadIdx.x == 0) givens_step(gm, k);
 }
 
+// Sizes of the on-chip Gram-Schmidt kernel (gm_mgs_onchip_kernel below):
+// 512 threads (16 warps); each warp owns the TMEM lanes of its quarter
+// (warp % 4) and a quarter of the 512 columns (warp / 4), so every thread
+// holds 128 32-bit columns: 32 groups of 4 FP32 values, or 16 groups of 4
+// FP64 values split into low and high words.
+constexpr int ONCHIP_THREADS = 512;
+constexpr int TMEM_COLS = 512;
+constexpr int TMEM_COLS_PER_THREAD = 128;
+template <typename TV> struct TmemGeom {
+  static constexpr int words = (int)(sizeof(TV) / 4);              // columns per value
+  static constexpr int gpp = 16 / (4 * words);                     // groups per 16-column piece
+  static constexpr int pieces = TMEM_COLS_PER_THREAD / 16;         // pieces per thread
+  static constexpr int groups = pieces * gpp;                      // groups per thread
+  static constexpr int cap = 4 * groups * ONCHIP_THREADS;          // values per block
+};
+
+__device__ __forceinline__ void tmem_ld16(uint32_t addr, uint32_t (&r)[16]) {
+  asm volatile(
+      "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, "
+      "%14, %15}, [%16];\n"
+      : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]),
+        "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15])
+      : "r"(addr));
+}
+__device__ __forceinline__ void tmem_st16(uint32_t addr, const uint32_t (&r)[16]) {
+  asm volatile(
+      "tcgen05.st.sync.aligned.32x32b.x16.b32 [%0], {%1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, "
+      "%14, %15, %16};\n"
+      :
+      : "r"(addr), "r"(r[0]), "r"(r[1]), "r"(r[2]), "r"(r[3]), "r"(r[4]), "r"(r[5]), "r"(r[6]), "r"(r[7]),
+        "r"(r[8]), "r"(r[9]), "r"(r[10]), "r"(r[11]), "r"(r[12]), "r"(r[13]), "r"(r[14]), "r"(r[15]));
+}
+__device__ __forceinline__ void tmem_wait_ld() { asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory"); }
+__device__ __forceinline__ void tmem_wait_st() { asm volatile("tcgen05.wait::st.sync.aligned;" ::: "memory"); }
+__device__ __forceinline__ void tc_fence_before() { asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory"); }
+__device__ __forceinline__ void tc_fence_after() { asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory"); }
+
+// group gi of a 16-column piece <-> 4 values
+__device__ __forceinline__ void unpack_group(const uint32_t (&r)[16], int gi, float*, double a[4]) {
+#pragma unroll
+  for (int e = 0; e < 4; ++e) a[e] = (double)__uint_as_float(r[4 * gi + e]);
+}
+__device__ __forceinline__ void unpack_group(const uint32_t (&r)[16], int gi, double*, double a[4]) {
+#pragma unroll
+  for (int e = 0; e < 4; ++e) a[e] = __hiloint2double((int)r[8 * gi + 2 * e + 1], (int)r[8 * gi + 2 * e]);
+}
+__device__ __forceinline__ void pack_group(uint32_t (&r)[16], int gi, float*, const double a[4]) {
+#pragma unroll
+  for (int e = 0; e < 4; ++e) r[4 * gi + e] = __float_as_uint((float)a[e]);
+}
+__device__ __forceinline__ void pack_group(uint32_t (&r)[16], int gi, double*, const double a[4]) {
+#pragma unroll
+  for (int e = 0; e < 4; ++e) {
+    r[8 * gi + 2 * e] = (uint32_t)__double2loint(a[e]);
+    r[8 * gi + 2 * e + 1] = (uint32_t)__double2hiint(a[e]);
+  }
+}
+
+// The on-chip kernel indexes 32-bit within its block's chunk, from base
+// pointers at the chunk start.  ld4m loads the group at local index li (a
+// multiple of 4) or, when !ok, the chunk's first group; the load itself is
+// unconditional so a thread keeps several in flight.  Values at or beyond
+// the chunk end nl, and all four when !ok, come back as zero.  The group
+// stays in the storage type until it is used.
+template <typename TV> struct Vec4;
+template <> struct Vec4<float> { using type = float4; };
+template <> struct Vec4<double> { struct type { double x, y, z, w; }; };
+template <typename TV>
+__device__ __forceinline__ typename Vec4<TV>::type ld4m(const TV* p, int li, int nl, bool ok) {
+  typename Vec4<TV>::type v;
+  const TV* q = p + (ok ? li : 0);
+  if constexpr (sizeof(TV) == 4) {
+    v = *reinterpret_cast<const float4*>(q);
+  } else {
+    const double2 a = reinterpret_cast<const double2*>(q)[0], b = reinterpret_cast<const double2*>(q)[1];
+    v.x = a.x; v.y = a.y; v.z = b.x; v.w = b.y;
+  }
+  if (!ok || li + 4 > nl) {
+    if (!ok || li >= nl) v.x = 0;
+    if (!ok || li + 1 >= nl) v.y = 0;
+    if (!ok || li + 2 >= nl) v.z = 0;
+    if (!ok || li + 3 >= nl) v.w = 0;
+  }
+  return v;
+}
+template <typename TV>
+__device__ __forceinline__ void st4l(TV* p, int li, int nl, const double v[4]) {
+  if (li + 4 <= nl) { st4v(p + li, v); return; }
+#pragma unroll
+  for (int q = 0; q < 4; ++q)
+    if (li + q < nl) p[li + q] = (TV)v[q];
+}
+template <typename V4> __device__ __forceinline__ void widen(const V4& v, double a[4]) {
+  a[0] = (double)v.x; a[1] = (double)v.y; a[2] = (double)v.z; a[3] = (double)v.w;
+}
+// Gram-Schmidt step on one group: a -= beta * p (rounded to TV), dot term
+template <typename TV, typename V4>
+__device__ __forceinline__ double mgs_apply(double a[4], const V4& p, const V4& y, double beta, bool sub,
+                                            bool self) {
+  if (sub) {
+    double pv[4];
+    widen(p, pv);
+#pragma unroll
+    for (int q = 0; q < 4; ++q) a[q] = (double)(TV)(a[q] - beta * pv[q]);
+  }
+  if (self) return a[0] * a[0] + a[1] * a[1] + a[2] * a[2] + a[3] * a[3];
+  double yv[4];
+  widen(y, yv);
+  return a[0] * yv[0] + a[1] * yv[1] + a[2] * yv[2] + a[3] * yv[3];
+}
+
+// FP32 basis: the update w -= beta * v_{j-1} runs in FP32 (one FMA with
+// beta rounded to FP32; w is stored in FP32 either way) and only the dot
+// product is formed in FP64: the products of two FP32 values are exact in
+// FP64 and are summed there.  Two conversions per value instead of five.
+__device__ __forceinline__ double mgs_apply_f(float a[4], const float4& p, const float4& y, float bf, bool sub,
+                                              bool self) {
+  if (sub) {
+    a[0] = fmaf(-bf, p.x, a[0]); a[1] = fmaf(-bf, p.y, a[1]);
+    a[2] = fmaf(-bf, p.z, a[2]); a[3] = fmaf(-bf, p.w, a[3]);
+  }
+  const double a0 = a[0], a1 = a[1], a2 = a[2], a3 = a[3];
+  if (self) return a0 * a0 + a1 * a1 + a2 * a2 + a3 * a3;
+  return a0 * (double)y.x + a1 * (double)y.y + a2 * (double)y.z + a3 * (double)y.w;
+}
+
+// The chunk of w owned by a block is cut into pieces of 16 columns per
+// thread: piece p holds groups p*gpp .. p*gpp+gpp-1 of every thread, group g
+// of thread t at local index 4*(g*512 + t), so each load instruction of a
+// warp covers contiguous memory.  Pieces 0..7 live in tensor memory, the
+// next `spieces` in dynamic shared memory (one 32 KB slot each), the rest
+// stay in global memory (w's own basis slot).
+template <typename TV> struct PieceLoads {
+  typename Vec4<TV>::type p[TmemGeom<TV>::gpp], y[TmemGeom<TV>::gpp];
+};
+template <typename TV> struct PieceGeom {
+  static constexpr int values = 4 * TmemGeom<TV>::gpp * ONCHIP_THREADS;   // values per piece
+  static constexpr int bytes = values * (int)sizeof(TV);                   // 32 KB
+};
+__device__ __forceinline__ int piece_li(int p, int gi, int gpp) {
+  return 4 * ((p * gpp + gi) * ONCHIP_THREADS + (int)threadIdx.x);
+}
+
+// Global loads of v_{j-1} (pp, null in step 1) and v_j (yp, null in step
+// k+1) for one piece, all issued before any is used.
+template <typename TV>
+__device__ __forceinline__ void issue_piece(PieceLoads<TV>& L, const TV* pp, const TV* yp, int p, int nl) {
+  using Geo = TmemGeom<TV>;
+#pragma unroll
+  for (int gi = 0; gi < Geo::gpp; ++gi) {
+    const int li = piece_li(p, gi, Geo::gpp);
+    const bool ok = li < nl;
+    if (pp) L.p[gi] = ld4m(pp, li, nl, ok);
+    if (yp) L.y[gi] = ld4m(yp, li, nl, ok);
+  }
+}
+
+// One Gram-Schmidt step on group gi of a piece whose w values are in r
+// (the 16 columns of the piece, as stored in tensor memory).
+template <typename TV>
+__device__ __forceinline__ double step_group(uint32_t (&r)[16], int gi, const PieceLoads<TV>& L, double beta,
+                                             bool sub, bool self) {
+  if constexpr (sizeof(TV) == 4) {
+    float f[4] = {__uint_as_float(r[4 * gi]), __uint_as_float(r[4 * gi + 1]), __uint_as_float(r[4 * gi + 2]),
+                  __uint_as_float(r[4 * gi + 3])};
+    const double s = mgs_apply_f(f, L.p[gi], L.y[gi], (float)beta, sub, self);
+#pragma unroll
+    for (int e = 0; e < 4; ++e) r[4 * gi + e] = __float_as_uint(f[e]);
+    return s;
+  } else {
+    double a[4];
+    unpack_group(r, gi, (TV*)nullptr, a);
+    const double s = mgs_apply<TV>(a, L.p[gi], L.y[gi], beta, sub, self);
+    pack_group(r, gi, (TV*)nullptr, a);
+    return s;
+  }
+}
+
+// the piece's 16 columns from / to shared or global memory
+template <typename TV>
+__device__ __forceinline__ void mem_to_cols(const TV* base, int p, int nl, bool global, uint32_t (&r)[16]) {
+  using Geo = TmemGeom<TV>;
+#pragma unroll
+  for (int gi = 0; gi < Geo::gpp; ++gi) {
+    const int li = piece_li(p, gi, Geo::gpp);
+    double a[4];
+    if (global) widen(ld4m(base, li, nl, li < nl), a);
+    else ld4v(base + 4 * (gi * ONCHIP_THREADS + (int)threadIdx.x), a);
+    pack_group(r, gi, (TV*)nullptr, a);
+  }
+}
+template <typename TV>
+__device__ __forceinline__ void cols_to_mem(TV* base, int p, int nl, bool global, const uint32_t (&r)[16]) {
+  using Geo = TmemGeom<TV>;
+#pragma unroll
+  for (int gi = 0; gi < Geo::gpp; ++gi) {
+    const int li = piece_li(p, gi, Geo::gpp);
+    double a[4];
+    unpack_group(r, gi, (TV*)nullptr, a);
+    if (global) { if (li < nl) st4l(base, li, nl, a); }
+    else st4v(base + 4 * (gi * ONCHIP_THREADS + (int)threadIdx.x), a);
+  }
+}
+
+// Gram-Schmidt of one Arnoldi iteration with w held on chip (w = P^-1 A v_k
+// already written to basis slot k by the SpMV launch before it).  One block
+// of 512 threads per SM; block b owns a contiguous chunk of w (a multiple of
+// 4 values) and keeps it, for all k+1 steps, in tensor memory (all 512
+// columns of the SM, used as plain storage), then in dynamic shared memory;
+// only what does not fit there stays in global memory.  Each step then
+// streams v_{j-1} and v_j alone, two pieces at a time with all their loads
+// in flight together.  The steps, their order and the fixed-order reductions
+// follow gm_arnoldi_kernel (FP32 basis: see mgs_apply_f); entries at and
+// beyond n are never touched.  Every block allocates its tensor memory after
+// the done test and frees it on the one exit path below.
+template <typename TV>
+__global__ void __launch_bounds__(ONCHIP_THREADS, 1)
+gm_mgs_onchip_kernel(TV* V, size_t ld, size_t n, int k, GmresDev* gm, double* part, size_t chunk, int spieces) {
+  using Geo = TmemGeom<TV>;
+  using PG = PieceGeom<TV>;
+  cg::grid_group grid = cg::this_grid();
+  if (gm->done) return;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  TV* ws = reinterpret_cast<TV*>(smem_raw);
+  __shared__ double sh[32];
+  __shared__ double sbeta;
+  __shared__ uint32_t tmem_base_sh;
+  const int G = gridDim.x, b = blockIdx.x, t = threadIdx.x, wid = t >> 5;
+  if (wid == 0) {
+    const uint32_t dst = (uint32_t)__cvta_generic_to_shared(&tmem_base_sh);
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(dst), "r"(TMEM_COLS));
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::);
+  }
+  tc_fence_before();
+  __syncthreads();
+  tc_fence_after();
+  const uint32_t tbase = tmem_base_sh;
+  // this warp's lanes (quarter wid % 4) and columns (slot wid / 4)
+  const uint32_t taddr = tbase + ((uint32_t)(32 * (wid & 3)) << 16) + (uint32_t)(TMEM_COLS_PER_THREAD * (wid >> 2));
+  const size_t c0 = (size_t)b * chunk;
+  const int nl = c0 < n ? (int)((c0 + chunk < n ? c0 + chunk : n) - c0) : 0;   // values of this chunk
+  const int np = (nl + PG::values - 1) / PG::values;                            // pieces of this chunk
+  const int ponchip = Geo::pieces + spieces;                                    // pieces held on chip
+  TV* wb = V + ld * (size_t)k + c0;
+  // w into tensor and shared memory
+#pragma unroll 1
+  for (int p = 0; p < np && p < ponchip; ++p) {
+    uint32_t r[16];
+    mem_to_cols(wb, p, nl, true, r);
+    if (p < Geo::pieces) tmem_st16(taddr + 16 * p, r);
+    else cols_to_mem(ws + (size_t)(p - Geo::pieces) * PG::values, p, nl, false, r);
+  }
+  tmem_wait_st();
+  double beta = 0.0;
+  PieceLoads<TV> L0, L1;
+  for (int j = 1; j <= k + 1; ++j) {
+    const bool sub = j >= 2, self = j == k + 1;
+    const TV* pp = sub ? V + ld * (size_t)(j - 2) + c0 : nullptr;
+    const TV* yp = self ? nullptr : V + ld * (size_t)(j - 1) + c0;
+    double sacc = 0.0;
+#pragma unroll 1
+    for (int p0 = 0; p0 < np; p0 += 2) {
+      issue_piece(L0, pp, yp, p0, nl);
+      if (p0 + 1 < np) issue_piece(L1, pp, yp, p0 + 1, nl);
+#pragma unroll
+      for (int h = 0; h < 2; ++h) {
+        const int p = p0 + h;
+        if (p >= np) break;
+        const PieceLoads<TV>& L = h ? L1 : L0;
+        uint32_t r[16];
+        const bool in_tmem = p < Geo::pieces, in_smem = !in_tmem && p < ponchip;
+        TV* sbase = ws + (size_t)(p - Geo::pieces) * PG::values;
+        if (in_tmem) {
+          tmem_ld16(taddr + 16 * p, r);
+          tmem_wait_ld();
+        } else {
+          mem_to_cols(in_smem ? sbase : wb, p, nl, !in_smem, r);
+        }
+#pragma unroll
+        for (int gi = 0; gi < Geo::gpp; ++gi) sacc += step_group<TV>(r, gi, L, beta, sub, self);
+        if (sub) {
+          if (in_tmem) tmem_st16(taddr + 16 * p, r);
+          else cols_to_mem(in_smem ? sbase : wb, p, nl, !in_smem, r);
+        }
+      }
+    }
+    tmem_wait_st();
+    const double bp = block_sum(sacc, sh);
+    double* pb = part + (size_t)(j & 1) * G;
+    if (t == 0) pb[b] = bp;
+    grid.sync();
+    // every block adds the partials in the same order (lane-strided, then a
+    // fixed butterfly; lane 0's value is used), so all see the same beta
+    if (t < 32) {
+      double v = 0.0;
+      for (int q = t; q < G; q += 32) v += __ldcg(pb + q);
+#pragma unroll
+      for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+      if (t == 0) sbeta = v;
+    }
+    __syncthreads();
+    beta = sbeta;
+    if (b == 0 && t == 0) {
+      gm->H[(size_t)(k - 1) * (gm->kspace + 1) + (j - 1)] = beta;
+      gm->beta = beta;
+    }
+  }
+  // normalize into basis slot k (SparseGMRES_NS.f90:291-294), Givens update
+  const double unorm = sqrt(beta);
+  const double d = unorm != 0.0 ? unorm : 1.0;
+#pragma unroll 1
+  for (int p = 0; p < np; ++p) {
+    uint32_t r[16];
+    const bool in_tmem = p < Geo::pieces, in_smem = !in_tmem && p < ponchip;
+    if (in_tmem) {
+      tmem_ld16(taddr + 16 * p, r);
+      tmem_wait_ld();
+    } else {
+      mem_to_cols(in_smem ? ws + (size_t)(p - Geo::pieces) * PG::values : wb, p, nl, !in_smem, r);
+    }
+#pragma unroll
+    for (int gi = 0; gi < Geo::gpp; ++gi) {
+      const int li = piece_li(p, gi, Geo::gpp);
+      double a[4];
+      unpack_group(r, gi, (TV*)nullptr, a);
+      a[0] /= d; a[1] /= d; a[2] /= d; a[3] /= d;
+      if (li < nl) st4l(wb, li, nl, a);
+    }
+  }
+  // release the tensor memory (every access to it has completed above)
+  tc_fence_before();
+  __syncthreads();
+  tc_fence_after();
+  if (wid == 0)
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tbase), "r"(TMEM_COLS));
+  if (b == 0 && t == 0) givens_step(gm, k);
+}
+
 // back-substitution (SparseGMRES_NS.f90:341-346); single thread
 __global__ void gm_backsub_kernel(GmresDev* gm) {
   const int iks = gm->iks, ld = gm->kspace + 1;
@@ -623,9 +913,105 @@ int ensure_basis(ovs_ctx* c, int prec, size_t bytes) {
   return OVS_OK;
 }
 
+// Launch plan of one Arnoldi iteration.  Default: the preconditioned SpMV
+// as an ordinary launch, then gm_mgs_onchip_kernel (one 512-thread block
+// per SM, cooperative).  fused = 1 (environment OVS_ARNOLDI_FUSED=1, or when
+// the on-chip kernel cannot be made co-resident): gm_arnoldi_kernel alone.
+struct ArnoldiPlan {
+  bool fused = false;
+  int grid = 0;
+  size_t chunk = 0, smem_bytes = 0;
+  int spieces = 0;
+};
+
+template <typename TM, typename TV, bool ACC64>
+using ArnoldiKern = void (*)(int, const int*, const int*, const TM*, const TM*, TV*, size_t, size_t, int,
+                             GmresDev*, double*);
+
+template <typename TM, typename TV, bool ACC64>
+ArnoldiKern<TM, TV, ACC64> fused_kernel(int sys) {
+  if (sys == OVS_SYS_NS) return gm_arnoldi_kernel<TM, TV, OVS_SYS_NS, ACC64>;
+  if (sys == OVS_SYS_NSVOF) return gm_arnoldi_kernel<TM, TV, OVS_SYS_NSVOF, ACC64>;
+  return gm_arnoldi_kernel<TM, TV, OVS_SYS_TEM, ACC64>;
+}
+
+template <typename TM, typename TV, bool ACC64>
+int plan_arnoldi(ovs_ctx* c, int sys, size_t n, bool want_fused, ArnoldiPlan* pl) {
+  int st;
+  if ((st = ovs_ensure((void**)&c->coop_part, sizeof(double) * 2 * OVS_COOP_MAX_BLOCKS))) return st;
+  pl->fused = want_fused;
+  if (!want_fused) {
+    const int G = c->num_sms;
+    const size_t chunk = ((n + G - 1) / G + 3) & ~(size_t)3;
+    const size_t rcap = (size_t)TmemGeom<TV>::cap;
+    int optin = 0;
+    OVS_CUDA_TRY(cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, c->device));
+    const size_t pv = PieceGeom<TV>::values, pbytes = PieceGeom<TV>::bytes;
+    const size_t max_sp = optin > 2048 ? (size_t)(optin - 2048) / pbytes : 0;   // room for static smem
+    const size_t want = chunk > rcap ? (chunk - rcap + pv - 1) / pv : 0;
+    const size_t sp = want < max_sp ? want : max_sp;
+    // The kernel takes all 512 tensor-memory columns of its SM, so two of
+    // its blocks must never share an SM (the second allocation would wait
+    // for the first block, which waits for it in grid.sync): request more
+    // than half of the SM's shared memory and require exactly one block.
+    const size_t min_bytes = 118784;
+    const size_t bytes = sp * pbytes > min_bytes ? sp * pbytes : min_bytes;
+    auto kern = gm_mgs_onchip_kernel<TV>;
+    if ((size_t)optin >= bytes + 512 && chunk < ((size_t)1 << 30)) {
+      OVS_CUDA_TRY(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes));
+      int per_sm = 0;
+      OVS_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, ONCHIP_THREADS, bytes));
+      if (per_sm == 1) {
+        pl->grid = G;
+        pl->chunk = chunk;
+        pl->spieces = (int)sp;
+        pl->smem_bytes = bytes;
+        return OVS_OK;
+      }
+    }
+    pl->fused = true;
+  }
+  int per_sm = 0;
+  OVS_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fused_kernel<TM, TV, ACC64>(sys), 256, 0));
+  if (per_sm < 1) return OVS_ERR_CUDA;
+  pl->grid = per_sm * c->num_sms;
+  if (pl->grid > OVS_COOP_MAX_BLOCKS) pl->grid = OVS_COOP_MAX_BLOCKS;
+  return OVS_OK;
+}
+
+// Arnoldi iteration k (1-based) on basis V (leading dimension ld, n values)
+template <typename TM, typename TV, bool ACC64>
+int launch_arnoldi(ovs_ctx* c, int sys, const ArnoldiPlan& pl, const TM* vals, const TM* pre, TV* V, size_t ld,
+                   size_t n, int k) {
+  GmresDev* gm = c->gm;
+  double* part = c->coop_part;
+  if (pl.fused) {
+    int Nn = c->N, kk = k;
+    const int* rp = c->rowptr;
+    const int* ci = c->colidx;
+    size_t ldv = ld, nn = n;
+    void* args[] = {&Nn, &rp, &ci, (void*)&vals, (void*)&pre, &V, &ldv, &nn, &kk, &gm, &part};
+    OVS_CUDA_TRY(cudaLaunchCooperativeKernel((void*)fused_kernel<TM, TV, ACC64>(sys), pl.grid, 256, args, 0,
+                                             c->stream));
+    ++c->launches;
+    return OVS_OK;
+  }
+  int st = launch_spmv<TM, TV, TV, 1, ACC64>(c, sys, vals, V + ld * (size_t)(k - 1), V + ld * (size_t)k, pre,
+                                               nullptr, &gm->done);
+  if (st) return st;
+  int kk = k;
+  size_t ldv = ld, nn = n, ch = pl.chunk;
+  int sp = pl.spieces;
+  void* args[] = {&V, &ldv, &nn, &kk, &gm, &part, &ch, &sp};
+  OVS_CUDA_TRY(cudaLaunchCooperativeKernel((void*)gm_mgs_onchip_kernel<TV>, pl.grid, ONCHIP_THREADS, args,
+                                           pl.smem_bytes, c->stream));
+  ++c->launches;
+  return OVS_OK;
+}
+
 // One GMRES cycle on system `sys` with matrix/preconditioner precision TM
 // and basis precision TV.  rhs and sol are FP64 device vectors (nf*N).
-template <typename TM, typename TV, typename TW = double, bool ACC64 = true>
+template <typename TM, typename TV, bool ACC64 = true>
 int gmres_cycle(ovs_ctx* c, int sys, const double* rhs, double* sol, double tol, int kspace,
                 int kmin, ovs_gmres_info* info) {
   const int N = c->N, nf = ovs_sys_nf(sys);
@@ -640,8 +1026,8 @@ int gmres_cycle(ovs_ctx* c, int sys, const double* rhs, double* sol, double tol,
   if ((st = ensure_basis(c, bprec, sizeof(TV) * ld * (size_t)(kspace + 1)))) return st;
   if ((st = ovs_ensure((void**)&c->wvec, sizeof(double) * basis_ld(5 * (size_t)N)))) return st;
   TV* V = reinterpret_cast<TV*>(c->basis[bprec]);
-  // w: FP64 work vector, or (TW == TV) the next basis vector itself
-  constexpr bool inplace = sizeof(TW) == sizeof(TV);
+  // v_1 = P^-1 rhs / ||P^-1 rhs|| through the FP64 work vector; later
+  // vectors are orthogonalized in place in their basis slot
   double* wd = c->wvec;
   GmresDev* gm = c->gm;
   cudaStream_t s = c->stream;
@@ -656,32 +1042,15 @@ int gmres_cycle(ovs_ctx* c, int sys, const double* rhs, double* sol, double tol,
   gm_normalize_kernel<TV, double><<<OVS_RED_BLOCKS, OVS_RED_THREADS, 0, s>>>(wd, V, n, gm, 1);
   c->launches += 2;
   OVS_CUDA_TRY(cudaGetLastError());
-  // one cooperative launch per Arnoldi iteration
-  void (*kern)(int, const int*, const int*, const TM*, const TM*, TV*, size_t, size_t, int, GmresDev*, double*);
-  if (sys == OVS_SYS_NS) kern = gm_arnoldi_kernel<TM, TV, OVS_SYS_NS, ACC64>;
-  else if (sys == OVS_SYS_NSVOF) kern = gm_arnoldi_kernel<TM, TV, OVS_SYS_NSVOF, ACC64>;
-  else kern = gm_arnoldi_kernel<TM, TV, OVS_SYS_TEM, ACC64>;
-  int per_sm = 0;
-  OVS_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, 256, 0));
-  if (per_sm < 1) return OVS_ERR_CUDA;
-  int grid = per_sm * c->num_sms;
-  if (grid > OVS_COOP_MAX_BLOCKS) grid = OVS_COOP_MAX_BLOCKS;
-  if ((st = ovs_ensure((void**)&c->coop_part, sizeof(double) * 2 * OVS_COOP_MAX_BLOCKS))) return st;
+  // one Arnoldi iteration per step (see ArnoldiPlan)
+  ArnoldiPlan pl;
+  if ((st = plan_arnoldi<TM, TV, ACC64>(c, sys, n, c->arnoldi_fused, &pl))) return st;
   const int batch = N > 200000 ? 4 : 16;
   int k = 1;
   for (; k <= kspace;) {
     const int kend = (k + batch - 1 < kspace) ? k + batch - 1 : kspace;
-    for (; k <= kend; ++k) {
-      int Nn = N, kk = k;
-      const int* rp = c->rowptr;
-      const int* ci = c->colidx;
-      TV* Vp = V;
-      size_t ldv = ld, nn = n;
-      double* part = c->coop_part;
-      void* args[] = {&Nn, &rp, &ci, (void*)&vals, (void*)&pre, &Vp, &ldv, &nn, &kk, &gm, &part};
-      OVS_CUDA_TRY(cudaLaunchCooperativeKernel((void*)kern, grid, 256, args, 0, s));
-      ++c->launches;
-    }
+    for (; k <= kend; ++k)
+      if ((st = launch_arnoldi<TM, TV, ACC64>(c, sys, pl, vals, pre, V, ld, n, k))) return st;
     OVS_CUDA_TRY(cudaMemcpyAsync(c->h_pinned, &gm->done, sizeof(int), cudaMemcpyDeviceToHost, s));
     OVS_CUDA_TRY(cudaStreamSynchronize(s));
     if (c->h_pinned[0]) break;
@@ -744,29 +1113,14 @@ int profile_krylov_t(ovs_ctx* c, int what, int sys, int reps, double* ms) {
   OVS_CUDA_TRY(cudaMemsetAsync(&gm->epsnrm, 0, sizeof(double), c->stream));
   const TM* vals = as<TM>(S.vals);
   const TM* pre = as<TM>(S.binv);
-  void (*kern)(int, const int*, const int*, const TM*, const TM*, TM*, size_t, size_t, int, GmresDev*, double*);
-  if (sys == OVS_SYS_NS) kern = gm_arnoldi_kernel<TM, TM, OVS_SYS_NS, ACC64>;
-  else if (sys == OVS_SYS_NSVOF) kern = gm_arnoldi_kernel<TM, TM, OVS_SYS_NSVOF, ACC64>;
-  else kern = gm_arnoldi_kernel<TM, TM, OVS_SYS_TEM, ACC64>;
-  int per_sm = 0;
-  OVS_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, 256, 0));
-  int grid = per_sm * c->num_sms;
-  if (grid > OVS_COOP_MAX_BLOCKS) grid = OVS_COOP_MAX_BLOCKS;
-  if ((st = ovs_ensure((void**)&c->coop_part, sizeof(double) * 2 * OVS_COOP_MAX_BLOCKS))) return st;
+  ArnoldiPlan pl;
+  if ((st = plan_arnoldi<TM, TM, ACC64>(c, sys, n, what == OVS_PROF_ARNOLDI_FUSED, &pl))) return st;
   auto run = [&]() -> int {
     if (what == OVS_PROF_SPMV) {
       st = launch_spmv<TM, TM, TM, 1, ACC64>(c, sys, vals, V, V + ld, pre, nullptr, nullptr);
       return st;
     }
-    int Nn = c->N, kk = k;
-    const int* rp = c->rowptr;
-    const int* ci = c->colidx;
-    size_t ldv = ld, nn = n;
-    double* part = c->coop_part;
-    void* args[] = {&Nn, &rp, &ci, (void*)&vals, (void*)&pre, &V, &ldv, &nn, &kk, &gm, &part};
-    OVS_CUDA_TRY(cudaLaunchCooperativeKernel((void*)kern, grid, 256, args, 0, c->stream));
-    ++c->launches;
-    return OVS_OK;
+    return launch_arnoldi<TM, TM, ACC64>(c, sys, pl, vals, pre, V, ld, n, k);
   };
   if ((st = run())) return st;
   OVS_CUDA_TRY(cudaEventRecord(c->ev0, c->stream));
@@ -881,8 +1235,8 @@ int ovs_solve_impl(ovs_ctx* c, int sys, int mode, double rtol, int kspace, int m
     if (tin < floor_tol) tin = floor_tol;
     if (tin > 0.5) tin = 0.5;
     ovs_gmres_info gi;
-    if (prec == OVS_FP64) st = gmres_cycle<double, double, double, true>(c, sys, r, x, tin, kspace, 1, &gi);
-    else st = gmres_cycle<float, float, float, false>(c, sys, r, x, tin, kspace, 1, &gi);
+    if (prec == OVS_FP64) st = gmres_cycle<double, double, true>(c, sys, r, x, tin, kspace, 1, &gi);
+    else st = gmres_cycle<float, float, false>(c, sys, r, x, tin, kspace, 1, &gi);
     if (st) return st;
     iters += gi.iterations;
     ++cycles;

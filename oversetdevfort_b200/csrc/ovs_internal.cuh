@@ -96,7 +96,8 @@ struct ovs_ctx {
   double* work64 = nullptr;              // 3 vectors of 5N doubles (b, r, x)
   float* work32 = nullptr;               // 1 vector of 5N floats
   double* wvec = nullptr;                // FP64 vector under orthogonalization
-  double* coop_part = nullptr;           // partial sums of the cooperative Arnoldi kernel
+  double* coop_part = nullptr;           // partial sums of the cooperative Arnoldi kernels
+  bool arnoldi_fused = false;            // one-launch Arnoldi variant (env OVS_ARNOLDI_FUSED=1)
   // status words: [0] negative DetJ count, [1] non-finite flag
   int* flags = nullptr;
   unsigned long long* cfl_bits = nullptr;
