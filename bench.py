@@ -40,6 +40,28 @@ sys.path.insert(0, str(ROOT))
 METRIC = "assembly Melem/s & GMRES s/solve at 2.1M nodes, mixed vs FP64 to rel. resid 1e-8"
 
 
+def ncu_traffic_per_tet(name):
+    """DRAM bytes (read + write) per tet of one launch, from the committed
+    ncu summary of the kernel on the 48^3-cell case (663,552 tets); the bench
+    scales it by the tets of its own workload.  (None, reason) when absent."""
+    import re
+    path = os.path.join(os.path.dirname(os.path.abspath(__file__)), "profiles", name)
+    try:
+        txt = open(path).read()
+    except OSError:
+        return None, "no ncu summary"
+    def mb(metric):
+        m = re.search(r"`%s`\) \| ([0-9.]+) (Kbyte|Mbyte|Gbyte|byte)" % re.escape(metric), txt)
+        if not m:
+            return None
+        return float(m.group(1)) * {"byte": 1, "Kbyte": 1e3, "Mbyte": 1e6, "Gbyte": 1e9}[m.group(2)]
+    rd, wr = mb("dram__bytes_read.sum"), mb("dram__bytes_write.sum")
+    if rd is None or wr is None:
+        return None, "no DRAM counters in " + name
+    return (rd + wr) / 663552.0, ("ncu dram__bytes_read.sum + dram__bytes_write.sum of one launch on the "
+                                  "48^3-cell case (profiles/%s), scaled by tets" % name)
+
+
 def _peaks():
     try:
         return json.loads((ROOT / "MEASURED_PEAKS.json").read_text()), "measured"
@@ -297,9 +319,11 @@ def run_ours(args, world, rank, local_rank, dist):
     hbm = float(peaks["hbm_gbs"])
     sp_ach = spmv_bytes(4) / (prof["spmv_nsvof_fp32_ms"] * 1e-3) / 1e9
     as_ach = asm_bytes(4) / (prof["asm_nsvof_fp32_ms"] * 1e-3) / 1e9
+    traffic, traffic_src = ncu_traffic_per_tet("assemble_rows_kernel_quench48.md")
     roof_asm = {"kernel": "assemble_rows_kernel<float,NSVOF> (row-owner element assembly)",
                 "bound": "hbm", "achieved": as_ach, "peak": hbm, "unit": "GB/s",
-                "frac": as_ach / hbm, "traffic": None, "peak_kind": peak_kind,
+                "frac": as_ach / hbm, "traffic": traffic * E if traffic else None,
+                "traffic_source": traffic_src, "peak_kind": peak_kind,
                 "algorithmic_bytes": asm_bytes(4), "avg_ms": prof["asm_nsvof_fp32_ms"]}
     roof_spmv = {"kernel": "spmv_block_kernel<6,float> (P^-1 A x, NS+VOF)", "bound": "hbm",
                  "achieved": sp_ach, "peak": hbm, "unit": "GB/s", "frac": sp_ach / hbm, "traffic": None,
