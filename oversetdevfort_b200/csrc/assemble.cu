@@ -217,10 +217,10 @@ template <> struct Lay<OVS_ASM_NS> {
   static constexpr int SW = 48, GP0 = 16, GPW = 4, RHS0 = 32, NF = 4, NV = 16;
 };
 template <> struct Lay<OVS_ASM_NSVOF> {
-  static constexpr int SW = 80, GP0 = 20, GPW = 10, RHS0 = 60, NF = 5, NV = 24;
+  static constexpr int SW = 88, GP0 = 20, GPW = 12, RHS0 = 68, NF = 5, NV = 24;
 };
 template <> struct Lay<OVS_ASM_TEM> {
-  static constexpr int SW = 44, GP0 = 14, GPW = 6, RHS0 = 38, NF = 1, NV = 1;
+  static constexpr int SW = 52, GP0 = 16, GPW = 8, RHS0 = 48, NF = 1, NV = 1;
 };
 
 struct SumArgs {
@@ -446,6 +446,7 @@ __device__ void summarize_nsvof(const SumArgs& a, const T r[4][16], const T lo[4
     og[7] = fact2 * wf * tauC * dmdi * dmdi;
     og[8] = fact2 * tauC * dmdi * wf;
     og[9] = fact2 * dmdi * wf;
+    og[10] = 0; og[11] = 0;
     if (!fluid) continue;
     KA += fact2 * mupk * w;
     KB += fact2 * (tauC + lambda) * w;
@@ -549,6 +550,7 @@ __device__ void summarize_tem(const SumArgs& a, const T r[4][16], const T lo[4][
     const T dSe = (cpw - cpa) * mdot + ((cpw - cpa) * (Ti - ts) - lh) * dmdT;
     T* og = o + Lay<OVS_ASM_TEM>::GP0 + gp * Lay<OVS_ASM_TEM>::GPW;
     og[3] = rcp;
+    og[6] = 0; og[7] = 0;
     if (fluid) {
       og[0] = uadv[0]; og[1] = uadv[1]; og[2] = uadv[2];
       og[4] = dSe; og[5] = tauT * rcp;
@@ -569,15 +571,14 @@ __device__ void summarize_tem(const SumArgs& a, const T r[4][16], const T lo[4][
   for (int n = 0; n < 4; ++n)
 #pragma unroll
     for (int d = 0; d < 3; ++d) o[3 * n + d] = g[n][d];
-  o[12] = w; o[13] = HK;
+  o[12] = w; o[13] = HK; o[14] = 0; o[15] = 0;
 #pragma unroll
   for (int n = 0; n < 4; ++n) o[Lay<OVS_ASM_TEM>::RHS0 + n] = rt[n];
-  o[42] = 0; o[43] = 0;
 }
 
 // -------------------------------------------------- pass 2: block expansion
-// Blocks of row A (local node la) of one element from its summary, for the
-// column nodes b = 0..3 (formulas factored from the reference's per Gauss
+// Blocks of row A (local node la) of one element from its summary, for a
+// column node b (formulas factored from the reference's per Gauss
 // point sums; see the notes at each kind):
 //   K(i,j) = KA ga_j gb_i + KB ga_i gb_j + delta_ij (KA gab + S_b)
 //   G(i) = -ga_i P_b + gb_i Q        D(i) = gb_i R + ga_i T_b     M = MM gab
@@ -600,8 +601,12 @@ __device__ __forceinline__ void ldv4(const T* p, T* d) {
   }
 }
 
-template <typename T, int KIND>
-__device__ __forceinline__ void expand_row(const ovs_params& p, const T* sm, int la, T* blk, int nvp, T* rv) {
+// Blocks (row node la, column nodes b0 + k*BS, k < NC) of an element from
+// its summary, by the sums above, in one Gauss-point loop.  The 4 lanes of an
+// NS/NS+VOF element take one column each (NC = 1); a T lane takes all four.
+template <typename T, int KIND, int NC>
+__device__ __forceinline__ void expand_block(const ovs_params& p, const T* sm, int la, int b0, int BS,
+                                             T (&o)[NC][Lay<KIND>::NV < 4 ? 1 : Lay<KIND>::NV], T* rv) {
   using L = Lay<KIND>;
   T hd[16];
 #pragma unroll
@@ -612,31 +617,42 @@ __device__ __forceinline__ void expand_row(const ovs_params& p, const T* sm, int
 #pragma unroll
     for (int d = 0; d < 3; ++d) g[n][d] = hd[3 * n + d];
   const T w = hd[12];
-  const T ga[3] = {la == 0 ? g[0][0] : la == 1 ? g[1][0] : la == 2 ? g[2][0] : g[3][0],
-                   la == 0 ? g[0][1] : la == 1 ? g[1][1] : la == 2 ? g[2][1] : g[3][1],
-                   la == 0 ? g[0][2] : la == 1 ? g[1][2] : la == 2 ? g[2][2] : g[3][2]};
-  T gab[4];
+  T ga[3], gb[NC][3];
 #pragma unroll
-  for (int b = 0; b < 4; ++b) gab[b] = ga[0] * g[b][0] + ga[1] * g[b][1] + ga[2] * g[b][2];
+  for (int d = 0; d < 3; ++d) {
+    const T col[4] = {g[0][d], g[1][d], g[2][d], g[3][d]};
+    ga[d] = pick4<T>(col, la);
+#pragma unroll
+    for (int k = 0; k < NC; ++k) gb[k][d] = pick4<T>(col, b0 + k * BS);
+  }
+  T gab[NC];
+#pragma unroll
+  for (int k = 0; k < NC; ++k) gab[k] = ga[0] * gb[k][0] + ga[1] * gb[k][1] + ga[2] * gb[k][2];
   if constexpr (KIND == OVS_ASM_TEM) {
     const T fact1 = (T)p.almi, fact2 = (T)(p.alfi * p.gami * p.delt);
     const T HK = hd[13];
-    T Xb[4] = {0, 0, 0, 0};
+    T X[NC];
+#pragma unroll
+    for (int k = 0; k < NC; ++k) X[k] = 0;
 #pragma unroll
     for (int gp = 0; gp < 4; ++gp) {
       T N[4];
       tet_shape<T>(gp, N);
-      const T* q = sm + L::GP0 + gp * L::GPW;
+      T q[L::GPW];
+#pragma unroll
+      for (int k = 0; k < L::GPW; k += 4) ldv4(sm + L::GP0 + gp * L::GPW + k, q + k);
       const T uadv[3] = {q[0], q[1], q[2]}, rcp = q[3], dSe = q[4], trc = q[5];
-      T c[4];
+      const T ca = ga[0] * uadv[0] + ga[1] * uadv[1] + ga[2] * uadv[2];
+      const T aw = w * (pick4<T>(N, la) + trc * ca);
 #pragma unroll
-      for (int b = 0; b < 4; ++b) c[b] = g[b][0] * uadv[0] + g[b][1] * uadv[1] + g[b][2] * uadv[2];
-      const T aw = w * (pick4<T>(N, la) + trc * pick4<T>(c, la));
-#pragma unroll
-      for (int b = 0; b < 4; ++b) Xb[b] += aw * (rcp * (fact1 * N[b] + fact2 * c[b]) - fact2 * dSe * N[b]);
+      for (int k = 0; k < NC; ++k) {
+        const T cb = gb[k][0] * uadv[0] + gb[k][1] * uadv[1] + gb[k][2] * uadv[2];
+        const T Nb = pick4<T>(N, b0 + k * BS);
+        X[k] += aw * (rcp * (fact1 * Nb + fact2 * cb) - fact2 * dSe * Nb);
+      }
     }
 #pragma unroll
-    for (int b = 0; b < 4; ++b) blk[b * nvp] = Xb[b] + HK * gab[b];
+    for (int k = 0; k < NC; ++k) o[k][0] = X[k] + HK * gab[k];
     rv[0] = sm[L::RHS0 + la];
   } else {
     constexpr bool vof = KIND == OVS_ASM_NSVOF;
@@ -650,71 +666,71 @@ __device__ __forceinline__ void expand_row(const ovs_params& p, const T* sm, int
       KDP = t4[0]; dphi[0] = t4[1]; dphi[1] = t4[2]; dphi[2] = t4[3];
     }
     T Q = 0, R = 0, W = 0;
-    T Sb[4] = {0, 0, 0, 0}, Pb[4] = {0, 0, 0, 0}, Tb[4] = {0, 0, 0, 0};
-    T L1[4] = {0, 0, 0, 0}, Eb[4] = {0, 0, 0, 0}, Ub[4] = {0, 0, 0, 0}, PLb[4] = {0, 0, 0, 0}, Vb[4] = {0, 0, 0, 0};
+    T S[NC], P[NC], Tt[NC], L1[NC], E[NC], U[NC], PL[NC], Vv[NC];
+#pragma unroll
+    for (int k = 0; k < NC; ++k) S[k] = P[k] = Tt[k] = L1[k] = E[k] = U[k] = PL[k] = Vv[k] = 0;
 #pragma unroll
     for (int gp = 0; gp < 4; ++gp) {
       T N[4];
       tet_shape<T>(gp, N);
-      const T* q = sm + L::GP0 + gp * L::GPW;
+      T q[L::GPW];
+#pragma unroll
+      for (int k = 0; k < L::GPW; k += 4) ldv4(sm + L::GP0 + gp * L::GPW + k, q + k);
       T uadv[3], rho, rt;
       if constexpr (vof) {
         uadv[0] = q[0]; uadv[1] = q[1]; uadv[2] = q[2]; rho = q[3]; rt = q[4];
       } else {
         uadv[0] = q[0]; uadv[1] = q[1]; uadv[2] = q[2]; rho = (T)p.rhoa; rt = q[3];
       }
-      T c[4];
-#pragma unroll
-      for (int b = 0; b < 4; ++b) c[b] = uadv[0] * g[b][0] + uadv[1] * g[b][1] + uadv[2] * g[b][2];
-      const T Na = pick4<T>(N, la), ca = pick4<T>(c, la);
+      const T ca = uadv[0] * ga[0] + uadv[1] * ga[1] + uadv[2] * ga[2];
+      const T Na = pick4<T>(N, la);
       const T alpha = w * rho * (Na + rt * ca);
       Q += fact2 * w * rt * ca;
       R += fact2 * w * Na;
-#pragma unroll
-      for (int b = 0; b < 4; ++b) {
-        const T beta = fact1 * N[b] + fact2 * c[b];
-        Sb[b] += alpha * beta;
-        Pb[b] += fact2 * w * N[b];
-        Tb[b] += w * rt * beta;
-      }
+      T gam = 0, tls = 0, src = 0, eps = 0, ufac = 0, plfac = 0;
       if constexpr (vof) {
-        const T tls = q[5], src = q[6], eps = q[7], ufac = q[8], plfac = q[9];
-        const T gam = w * (Na + tls * ca);
+        tls = q[5]; src = q[6]; eps = q[7]; ufac = q[8]; plfac = q[9];
+        gam = w * (Na + tls * ca);
         W += ufac * Na;
+      }
 #pragma unroll
-        for (int b = 0; b < 4; ++b) {
-          const T beta = fact1 * N[b] + fact2 * c[b];
-          L1[b] += gam * (beta + fact2 * N[b] * src);
-          Eb[b] += eps * Na * N[b];
-          Ub[b] += ufac * N[b];
-          PLb[b] -= plfac * Na * N[b];
-          Vb[b] += fact2 * gam * N[b];
+      for (int k = 0; k < NC; ++k) {
+        const T cb = uadv[0] * gb[k][0] + uadv[1] * gb[k][1] + uadv[2] * gb[k][2];
+        const T Nb = pick4<T>(N, b0 + k * BS);
+        const T beta = fact1 * Nb + fact2 * cb;
+        S[k] += alpha * beta;
+        P[k] += fact2 * w * Nb;
+        Tt[k] += w * rt * beta;
+        if constexpr (vof) {
+          L1[k] += gam * (beta + fact2 * Nb * src);
+          E[k] += eps * Na * Nb;
+          U[k] += ufac * Nb;
+          PL[k] -= plfac * Na * Nb;
+          Vv[k] += fact2 * gam * Nb;
         }
       }
     }
 #pragma unroll
-    for (int b = 0; b < 4; ++b) {
-      T o[L::NV];
-      const T* gb = g[b];
-      const T dg = KA * gab[b] + Sb[b];
+    for (int k = 0; k < NC; ++k) {
+      const T* gk = gb[k];
+      const T dg = KA * gab[k] + S[k];
 #pragma unroll
       for (int i = 0; i < 3; ++i) {
 #pragma unroll
-        for (int j = 0; j < 3; ++j) o[4 * i + j] = KA * ga[j] * gb[i] + KB * ga[i] * gb[j] + (i == j ? dg : (T)0);
-        o[4 * i + 3] = -ga[i] * Pb[b] + gb[i] * Q;
+        for (int j = 0; j < 3; ++j) o[k][4 * i + j] = KA * ga[j] * gk[i] + KB * ga[i] * gk[j] + (i == j ? dg : (T)0);
+        o[k][4 * i + 3] = -ga[i] * P[k] + gk[i] * Q;
       }
 #pragma unroll
-      for (int d = 0; d < 3; ++d) o[12 + d] = gb[d] * R + ga[d] * Tb[b];
-      o[15] = MM * gab[b];
+      for (int d = 0; d < 3; ++d) o[k][12 + d] = gk[d] * R + ga[d] * Tt[k];
+      o[k][15] = MM * gab[k];
       if constexpr (vof) {
 #pragma unroll
-        for (int d = 0; d < 3; ++d) o[16 + d] = dphi[d] * Vb[b] - gb[d] * W;
-        o[19] = L1[b] + KDP * gab[b] + Eb[b];
+        for (int d = 0; d < 3; ++d) o[k][16 + d] = dphi[d] * Vv[k] - gk[d] * W;
+        o[k][19] = L1[k] + KDP * gab[k] + E[k];
 #pragma unroll
-        for (int d = 0; d < 3; ++d) o[20 + d] = ga[d] * Ub[b];
-        o[23] = PLb[b];
+        for (int d = 0; d < 3; ++d) o[k][20 + d] = ga[d] * U[k];
+        o[k][23] = PL[k];
       }
-      store_row<L::NV>(blk + b * nvp, o);
     }
 #pragma unroll
     for (int f = 0; f < L::NF; ++f) rv[f] = sm[L::RHS0 + L::NF * la + f];
@@ -740,25 +756,34 @@ template <> struct Vec4<double> {
   }
 };
 
-// shared-memory layout per warp
+// shared-memory layout per warp: the blocks of the chunk's elements
+// [CH elements][4 columns][BSTR] (stride padded so the 16-byte stores of a
+// quarter warp hit distinct banks), their RHS rows [8][RSTR], the row
+// accumulator [max_deg][NVP], then the slots [8][4] and the columns
 template <typename T, int KIND> struct Smem {
   static constexpr int NV = Lay<KIND>::NV, NF = Lay<KIND>::NF;
-  // per-lane stride of the element rows, padded so that 16-byte stores of
-  // the 32 lanes spread over all banks
+  static constexpr int LPE = (NV < 4) ? 1 : 4;       // lanes per element
+  static constexpr int CH = 32 / LPE;                // elements per chunk
   static constexpr int NVP = (NV < 4) ? 1 : NV;
-  static constexpr int LSTR = 4 * NVP + (16 / (int)sizeof(T));
+  static constexpr int BSTR = (NV < 4) ? 1 : NV + 16 / (int)sizeof(T);
   static constexpr int RSTR = NF + 1;
   __host__ __device__ static size_t bytes(int max_deg) {
-    size_t b = sizeof(T) * ((size_t)32 * LSTR + (size_t)32 * RSTR + (size_t)max_deg * NVP);
+    size_t b = sizeof(T) * ((size_t)4 * CH * BSTR + (size_t)CH * RSTR + (size_t)max_deg * NVP);
     b = (b + 15) & ~(size_t)15;
-    b += sizeof(int) * ((size_t)32 * 4 + max_deg);
+    b += sizeof(int) * ((size_t)4 * CH + max_deg);
     return (b + 15) & ~(size_t)15;
   }
 };
 
 // ---------------------------------------------------------- pass 1 kernel
+// blocks per SM the element pass is compiled for: the FP32 NS+VOF pass at 3
+// (168 registers, measured faster than the unbounded 178), the others as
+// the compiler chooses (tighter bounds spill)
+template <typename T, int KIND> struct SumMinBlocks { static constexpr int v = 1; };
+template <> struct SumMinBlocks<float, OVS_ASM_NSVOF> { static constexpr int v = 3; };
+
 template <typename T, int KIND>
-__global__ void __launch_bounds__(128)
+__global__ void __launch_bounds__(128, SumMinBlocks<T, KIND>::v)
 element_summary_kernel(const SumArgs a) {
   using L = Lay<KIND>;
   const int e = blockIdx.x * blockDim.x + threadIdx.x;
@@ -810,23 +835,27 @@ __global__ void __launch_bounds__(WARPS * 32)
 assemble_rows_kernel(const AsmArgs a) {
   using S = Smem<T, KIND>;
   using L = Lay<KIND>;
-  constexpr int NV = S::NV, NF = S::NF, NVP = S::NVP, LSTR = S::LSTR, RSTR = S::RSTR;
+  constexpr int NV = S::NV, NF = S::NF, NVP = S::NVP, BSTR = S::BSTR, RSTR = S::RSTR, CH = S::CH;
   extern __shared__ __align__(16) unsigned char smem_raw[];
   __shared__ unsigned masks[24];
   if (threadIdx.x < 24) masks[threadIdx.x] = (KIND == OVS_ASM_TEM) ? (TB | (TB << 8) | (TB << 16)) : mask_of(threadIdx.x);
   __syncthreads();
   const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
   unsigned char* base = smem_raw + (size_t)wid * S::bytes(a.max_deg);
-  T* blk = reinterpret_cast<T*>(base);                 // [32][LSTR]
-  T* rvs = blk + 32 * LSTR;                            // [32][RSTR]
-  T* acc = rvs + 32 * RSTR;                            // [max_deg][NVP]
-  size_t off = sizeof(T) * ((size_t)32 * LSTR + (size_t)32 * RSTR + (size_t)a.max_deg * NVP);
+  T* blk = reinterpret_cast<T*>(base);                 // [CH][4][BSTR]
+  T* rvs = blk + 4 * CH * BSTR;                        // [CH][RSTR]
+  T* acc = rvs + CH * RSTR;                            // [max_deg][NVP]
+  size_t off = sizeof(T) * ((size_t)4 * CH * BSTR + (size_t)CH * RSTR + (size_t)a.max_deg * NVP);
   off = (off + 15) & ~(size_t)15;
-  int* slot = reinterpret_cast<int*>(base + off);      // [32][4]
-  int* cols = slot + 32 * 4;                           // [max_deg]
+  int* slot = reinterpret_cast<int*>(base + off);      // [CH][4]
+  int* cols = slot + 4 * CH;                           // [max_deg]
 
   const T* sum = reinterpret_cast<const T*>(a.rec);
   const int nwarps_total = gridDim.x * WARPS;
+  // lane = (element jl of the chunk, first column node bl0 of that element);
+  // with one lane per element (T) a lane takes all 4 columns
+  constexpr int LPE = S::LPE, CPL = 4 / LPE;
+  const int jl = lane / LPE, bl0 = lane % LPE;
   for (int A = blockIdx.x * WARPS + wid; A < a.N; A += nwarps_total) {
     const int rp = a.rowptr[A], deg = a.rowptr[A + 1] - rp;
     const int ep = a.n2e_ptr[A], ne = a.n2e_ptr[A + 1] - ep;
@@ -834,33 +863,42 @@ assemble_rows_kernel(const AsmArgs a) {
     for (int q = lane; q < deg * NVP; q += 32) acc[q] = (T)0;
     T racc = (T)0;
     __syncwarp();
-    for (int c0 = 0; c0 < ne; c0 += 32) {
-      const int nc = min(32, ne - c0);
-      // ---------------- phase 1: lane = element: A's row of its matrix
-      if (lane < nc) {
-        const int packed = __ldg(a.n2e + ep + c0 + lane);
+    for (int c0 = 0; c0 < ne; c0 += CH) {
+      const int nc = min(CH, ne - c0);
+      // ---------------- phase 1: block (A's row, column bl) of element jl
+      if (jl < nc) {
+        const int packed = __ldg(a.n2e + ep + c0 + jl);
         const int e = packed >> 3, la = packed & 7;
-        const int4 nd = __ldg(reinterpret_cast<const int4*>(a.ien) + e);
-        const int nodes[4] = {nd.x, nd.y, nd.z, nd.w};
-        T rv[NF];
-        expand_row<T, KIND>(a.p, sum + (size_t)e * L::SW, la, blk + lane * LSTR, NVP, rv);
+        T o[CPL][NVP], rv[NF];
+        expand_block<T, KIND, CPL>(a.p, sum + (size_t)e * L::SW, la, bl0, LPE, o, rv);
 #pragma unroll
-        for (int f = 0; f < NF; ++f) rvs[lane * RSTR + f] = rv[f];
-        // slot of each column node in row A (cols is sorted ascending)
+        for (int k = 0; k < CPL; ++k) {
+          const int bl = bl0 + k * LPE;
+          const int node_b = __ldg(a.ien + 4 * (size_t)e + bl);
+          T* dst = blk + (jl * 4 + bl) * BSTR;
+          if constexpr (NV >= 4) {
 #pragma unroll
-        for (int b = 0; b < 4; ++b) {
+            for (int v = 0; v < NV; v += 4) store_row<4>(dst + v, o[k] + v);
+          } else {
+            dst[0] = o[k][0];
+          }
+          // slot of the column node in row A (cols is sorted ascending)
           int lo = 0, hi = deg;
           while (hi - lo > 1) {
             const int mid = (lo + hi) >> 1;
-            if (cols[mid] > nodes[b]) hi = mid; else lo = mid;
+            if (cols[mid] > node_b) hi = mid; else lo = mid;
           }
-          slot[lane * 4 + b] = lo;
+          slot[jl * 4 + bl] = lo;
+        }
+        if (bl0 == 0) {
+#pragma unroll
+          for (int f = 0; f < NF; ++f) rvs[jl * RSTR + f] = rv[f];
         }
       }
       __syncwarp();
       // ---------------- phase 2: ordered segmented reduction into acc
       // elements are added one after another in ascending element id; the
-      // nshl blocks of one element go to distinct slots (elements with a
+      // 4 blocks of one element go to distinct slots (elements with a
       // repeated node are rejected at upload)
       if constexpr (NV >= 4) {
         constexpr int NG = NV / 4;
@@ -868,13 +906,13 @@ assemble_rows_kernel(const AsmArgs a) {
           if (lane < 4 * NG) {
             const int b = lane / NG, gidx = lane - b * NG;
             const int s = slot[j * 4 + b];
-            Vec4<T>::add(acc + s * NVP + gidx * 4, blk + j * LSTR + b * NVP + gidx * 4);
+            Vec4<T>::add(acc + s * NVP + gidx * 4, blk + (j * 4 + b) * BSTR + gidx * 4);
           }
           __syncwarp();
         }
       } else {
         for (int j = 0; j < nc; ++j) {
-          if (lane < 4) acc[slot[j * 4 + lane]] += blk[j * LSTR + lane];
+          if (lane < 4) acc[slot[j * 4 + lane]] += blk[j * 4 + lane];
           __syncwarp();
         }
       }
