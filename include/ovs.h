@@ -236,14 +236,17 @@ int ovs_residual_norms(ovs_ctx* ctx, int precision, double r[4]);
 
 /* ----------------------------------------------------------- measurement
  * Hooks for benchmarking; they have no counterpart in the reference. */
-enum { OVS_PROF_SPMV = 1, OVS_PROF_ASSEMBLE = 2, OVS_PROF_ARNOLDI = 3, OVS_PROF_ARNOLDI_FUSED = 4 };
+enum { OVS_PROF_SPMV = 1, OVS_PROF_ASSEMBLE = 2, OVS_PROF_ARNOLDI = 3, OVS_PROF_ARNOLDI_FUSED = 4,
+       OVS_PROF_ASSEMBLE_ELEMENTS = 5, OVS_PROF_ASSEMBLE_ROWS = 6 };
 /* Average device time in ms (CUDA events on the context stream) of `reps`
  * back-to-back launches of one internal kernel on the resident data:
  *   OVS_PROF_SPMV      preconditioned SpMV y = P^-1 A x of `system`, matrix
  *                      and vectors in `precision` (needs the matrix);
- *   OVS_PROF_ASSEMBLE  the element/row kernel of assembly kernel `system`
- *                      (an OVS_ASM_* value), MAT+VEC, on the node records of
- *                      the last ovs_assemble of that kernel and precision;
+ *   OVS_PROF_ASSEMBLE  the element and row passes of assembly kernel
+ *                      `system` (an OVS_ASM_* value), MAT+VEC, on the node
+ *                      records of the last ovs_assemble of that kernel and
+ *                      precision; OVS_PROF_ASSEMBLE_ELEMENTS and
+ *                      OVS_PROF_ASSEMBLE_ROWS time each pass alone;
  *   OVS_PROF_ARNOLDI   one Arnoldi iteration (preconditioned SpMV, k+1
  *                      Gram-Schmidt steps, normalization, Givens) at k = 25
  *                      of a 50-vector cycle, `system` in `precision`, as

@@ -29,6 +29,7 @@ OVS_ASM_NS, OVS_ASM_NSVOF, OVS_ASM_TEM = 1, 2, 3
 OVS_SYS_NS, OVS_SYS_NSVOF, OVS_SYS_TEM = 1, 2, 3
 OVS_TENSOR_VEC, OVS_TENSOR_MAT = 2, 4
 OVS_PROF_SPMV, OVS_PROF_ASSEMBLE, OVS_PROF_ARNOLDI, OVS_PROF_ARNOLDI_FUSED = 1, 2, 3, 4
+OVS_PROF_ASSEMBLE_ELEMENTS, OVS_PROF_ASSEMBLE_ROWS = 5, 6
 OVS_NOALLOC_MAX_N, OVS_NOALLOC_MAX_KSPACE = 16384, 40
 (OVS_BLK_K11, OVS_BLK_G, OVS_BLK_D1, OVS_BLK_M, OVS_BLK_LS, OVS_BLK_LSU,
  OVS_BLK_ULS, OVS_BLK_PLS, OVS_BLK_TEM) = range(9)

@@ -1017,12 +1017,16 @@ __global__ void alpha_records_kernel(const AlphaArgs a) {
   for (int k = 0; k < REC; ++k) o[k] = r[k];
 }
 
+// parts: bit 0 the element pass, bit 1 the row pass
 template <typename T, int KIND>
-int launch_assemble(ovs_ctx* c, const AsmArgs& a, const SumArgs& sa) {
+int launch_assemble(ovs_ctx* c, const AsmArgs& a, const SumArgs& sa, int parts = 3) {
   // pass 1: element summaries
-  element_summary_kernel<T, KIND><<<(sa.E + 127) / 128, 128, 0, c->stream>>>(sa);
-  ++c->launches;
-  OVS_CUDA_TRY(cudaGetLastError());
+  if (parts & 1) {
+    element_summary_kernel<T, KIND><<<(sa.E + 127) / 128, 128, 0, c->stream>>>(sa);
+    ++c->launches;
+    OVS_CUDA_TRY(cudaGetLastError());
+  }
+  if (!(parts & 2)) return OVS_OK;
   // pass 2: rows
   constexpr int WARPS = 4;
   using S = Smem<T, KIND>;
@@ -1044,15 +1048,16 @@ int launch_assemble(ovs_ctx* c, const AsmArgs& a, const SumArgs& sa) {
 
 }  // namespace
 
-static int dispatch_assemble(ovs_ctx* c, int kernel, int prec, const AsmArgs& a, const SumArgs& sa) {
+static int dispatch_assemble(ovs_ctx* c, int kernel, int prec, const AsmArgs& a, const SumArgs& sa,
+                             int parts = 3) {
   if (prec == OVS_FP64) {
-    if (kernel == OVS_ASM_NS) return launch_assemble<double, OVS_ASM_NS>(c, a, sa);
-    if (kernel == OVS_ASM_NSVOF) return launch_assemble<double, OVS_ASM_NSVOF>(c, a, sa);
-    return launch_assemble<double, OVS_ASM_TEM>(c, a, sa);
+    if (kernel == OVS_ASM_NS) return launch_assemble<double, OVS_ASM_NS>(c, a, sa, parts);
+    if (kernel == OVS_ASM_NSVOF) return launch_assemble<double, OVS_ASM_NSVOF>(c, a, sa, parts);
+    return launch_assemble<double, OVS_ASM_TEM>(c, a, sa, parts);
   }
-  if (kernel == OVS_ASM_NS) return launch_assemble<float, OVS_ASM_NS>(c, a, sa);
-  if (kernel == OVS_ASM_NSVOF) return launch_assemble<float, OVS_ASM_NSVOF>(c, a, sa);
-  return launch_assemble<float, OVS_ASM_TEM>(c, a, sa);
+  if (kernel == OVS_ASM_NS) return launch_assemble<float, OVS_ASM_NS>(c, a, sa, parts);
+  if (kernel == OVS_ASM_NSVOF) return launch_assemble<float, OVS_ASM_NSVOF>(c, a, sa, parts);
+  return launch_assemble<float, OVS_ASM_TEM>(c, a, sa, parts);
 }
 
 static void fill_args(ovs_ctx* c, int prec, SysStore& S, int tensor_flag, AsmArgs& a, SumArgs& sa) {
@@ -1083,7 +1088,9 @@ static void fill_args(ovs_ctx* c, int prec, SysStore& S, int tensor_flag, AsmArg
   a.p = c->params;
 }
 
-int ovs_profile_assemble(ovs_ctx* c, int kernel, int prec, int reps, double* ms) {
+// parts: 3 both passes, 1 the element pass, 2 the row pass (on the summaries
+// of the warm-up run)
+int ovs_profile_assemble(ovs_ctx* c, int kernel, int prec, int reps, double* ms, int parts) {
   if (kernel != OVS_ASM_NS && kernel != OVS_ASM_NSVOF && kernel != OVS_ASM_TEM) return OVS_ERR_ARG;
   const int sys = kernel == OVS_ASM_NS ? OVS_SYS_NS : (kernel == OVS_ASM_NSVOF ? OVS_SYS_NSVOF : OVS_SYS_TEM);
   SysStore& S = c->sys[sys][prec];
@@ -1095,7 +1102,7 @@ int ovs_profile_assemble(ovs_ctx* c, int kernel, int prec, int reps, double* ms)
   if ((st = dispatch_assemble(c, kernel, prec, a, sa))) return st;  // warm
   OVS_CUDA_TRY(cudaEventRecord(c->ev0, c->stream));
   for (int r = 0; r < reps; ++r)
-    if ((st = dispatch_assemble(c, kernel, prec, a, sa))) return st;
+    if ((st = dispatch_assemble(c, kernel, prec, a, sa, parts))) return st;
   OVS_CUDA_TRY(cudaEventRecord(c->ev1, c->stream));
   OVS_CUDA_TRY(cudaEventSynchronize(c->ev1));
   float t = 0.f;

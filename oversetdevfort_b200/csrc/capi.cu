@@ -636,7 +636,9 @@ int ovs_profile(ovs_ctx* c, int what, int system, int precision, int reps, doubl
   if (!c || !avg_ms || reps < 1 || (precision != OVS_FP64 && precision != OVS_FP32)) return OVS_ERR_ARG;
   int st;
   if ((st = ovs_activate(c))) return st;
-  if (what == OVS_PROF_ASSEMBLE) return ovs_profile_assemble(c, system, precision, reps, avg_ms);
+  if (what == OVS_PROF_ASSEMBLE) return ovs_profile_assemble(c, system, precision, reps, avg_ms, 3);
+  if (what == OVS_PROF_ASSEMBLE_ELEMENTS) return ovs_profile_assemble(c, system, precision, reps, avg_ms, 1);
+  if (what == OVS_PROF_ASSEMBLE_ROWS) return ovs_profile_assemble(c, system, precision, reps, avg_ms, 2);
   if (what != OVS_PROF_SPMV && what != OVS_PROF_ARNOLDI && what != OVS_PROF_ARNOLDI_FUSED) return OVS_ERR_ARG;
   if (!sys_ok(c, system, precision)) return OVS_ERR_ARG;
   return ovs_profile_krylov(c, what, system, precision, reps, avg_ms);

@@ -134,7 +134,7 @@ int ovs_update_impl(ovs_ctx* c, int sys);
 int ovs_resnorm_impl(ovs_ctx* c, int prec, double r[4]);
 int ovs_dot_impl(ovs_ctx* c, const double* a, const double* b, size_t n,
                  double* out);
-int ovs_profile_assemble(ovs_ctx* c, int kernel, int prec, int reps, double* ms);
+int ovs_profile_assemble(ovs_ctx* c, int kernel, int prec, int reps, double* ms, int parts);
 int ovs_profile_krylov(ovs_ctx* c, int what, int sys, int prec, int reps, double* ms);
 
 // launch geometry helper
