@@ -41,6 +41,7 @@ struct AsmArgs {
   const int* colidx;
   const int* n2e_ptr;
   const int* n2e;
+  const unsigned* n2s;    // slots of each entry's element nodes in the row
   void* vals;             // nnz*NV
   void* rhs;              // NF*N field-major
   int* flags;             // [0] non-positive DetJ count, [1] non-finite residual
@@ -868,13 +869,13 @@ assemble_rows_kernel(const AsmArgs a) {
       // ---------------- phase 1: block (A's row, column bl) of element jl
       if (jl < nc) {
         const int packed = __ldg(a.n2e + ep + c0 + jl);
+        const unsigned slots4 = __ldg(a.n2s + ep + c0 + jl);
         const int e = packed >> 3, la = packed & 7;
         T o[CPL][NVP], rv[NF];
         expand_block<T, KIND, CPL>(a.p, sum + (size_t)e * L::SW, la, bl0, LPE, o, rv);
 #pragma unroll
         for (int k = 0; k < CPL; ++k) {
           const int bl = bl0 + k * LPE;
-          const int node_b = __ldg(a.ien + 4 * (size_t)e + bl);
           T* dst = blk + (jl * 4 + bl) * BSTR;
           if constexpr (NV >= 4) {
 #pragma unroll
@@ -882,13 +883,7 @@ assemble_rows_kernel(const AsmArgs a) {
           } else {
             dst[0] = o[k][0];
           }
-          // slot of the column node in row A (cols is sorted ascending)
-          int lo = 0, hi = deg;
-          while (hi - lo > 1) {
-            const int mid = (lo + hi) >> 1;
-            if (cols[mid] > node_b) hi = mid; else lo = mid;
-          }
-          slot[jl * 4 + bl] = lo;
+          slot[jl * 4 + bl] = (int)((slots4 >> (8 * bl)) & 0xffu);
         }
         if (bl0 == 0) {
 #pragma unroll
@@ -1084,6 +1079,7 @@ static void fill_args(ovs_ctx* c, int prec, SysStore& S, int tensor_flag, AsmArg
   a.N = c->N;
   a.mat = (tensor_flag & OVS_TENSOR_MAT) != 0;
   a.vec = (tensor_flag & OVS_TENSOR_VEC) != 0;
+  a.n2s = c->n2s;
   a.max_deg = c->max_deg;
   a.p = c->params;
 }

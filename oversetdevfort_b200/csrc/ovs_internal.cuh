@@ -77,6 +77,7 @@ struct ovs_ctx {
   int* diag = nullptr;       // N: slot of the diagonal entry
   int* n2e_ptr = nullptr;    // N+1
   int* n2e = nullptr;        // nshl*E: (element << 3) | local index, sorted by element
+  unsigned* n2s = nullptr;   // nshl*E: slots of the element's 4 nodes in the row, one byte each (tets)
   int nnz = 0;
   int max_deg = 0, max_elem = 0;
   // nodal state (FP64, reference layout)

@@ -162,6 +162,32 @@ __global__ void row_fill_kernel(const int* __restrict__ ien, int nshl, int N,
   diag[i] = d;
 }
 
+// Slot map: for node-to-element entry k of row A (element e, sorted by
+// element), the slots in A's column list of e's 4 nodes, one byte each
+// (rows have at most OVS_MAX_DEG <= 255 columns).  The assembly row pass
+// reads it instead of searching the row for every element block.
+__global__ void slot_map_kernel(const int* __restrict__ ien, int N, const int* __restrict__ n2e_ptr,
+                                const int* __restrict__ n2e, const int* __restrict__ rowptr,
+                                const int* __restrict__ colidx, unsigned* __restrict__ n2s) {
+  const int A = blockIdx.x * blockDim.x + threadIdx.x;
+  if (A >= N) return;
+  const int rp = rowptr[A], deg = rowptr[A + 1] - rp;
+  for (int k = n2e_ptr[A]; k < n2e_ptr[A + 1]; ++k) {
+    const int4 nd = reinterpret_cast<const int4*>(ien)[n2e[k] >> 3];
+    const int nodes[4] = {nd.x, nd.y, nd.z, nd.w};
+    unsigned packed = 0;
+    for (int b = 0; b < 4; ++b) {
+      int lo = 0, hi = deg;   // last index with colidx <= node (SparseMatLoc_3D)
+      while (hi - lo > 1) {
+        const int mid = (lo + hi) >> 1;
+        if (colidx[rp + mid] > nodes[b]) hi = mid; else lo = mid;
+      }
+      packed |= (unsigned)lo << (8 * b);
+    }
+    n2s[k] = packed;
+  }
+}
+
 __global__ void to_one_based_kernel(const int* __restrict__ in, int* __restrict__ out, size_t n) {
   size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x;
   if (i < n) out[i] = in[i] + 1;
@@ -225,6 +251,11 @@ int ovs_pattern_build(ovs_ctx* c) {
   if ((st = ovs_ensure((void**)&c->colidx, sizeof(int) * (size_t)(nnz > 0 ? nnz : 1)))) return st;
   row_fill_kernel<<<ovs_grid(N, 128, 1 << 30), 128, 0, s>>>(c->ien, nshl, N, c->n2e_ptr, c->n2e,
                                                             c->rowptr, c->colidx, c->diag);
+  if (nshl == 4) {
+    if ((st = ovs_ensure((void**)&c->n2s, sizeof(unsigned) * (size_t)(EN > 0 ? EN : 1)))) return st;
+    slot_map_kernel<<<ovs_grid(N, 128, 1 << 30), 128, 0, s>>>(c->ien, N, c->n2e_ptr, c->n2e, c->rowptr,
+                                                              c->colidx, c->n2s);
+  }
   OVS_CUDA_TRY(cudaFreeAsync(cnt, s));
   OVS_CUDA_TRY(cudaFreeAsync(tmp, s));
   OVS_CUDA_TRY(cudaFreeAsync(stats, s));
