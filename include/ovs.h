@@ -265,6 +265,32 @@ int ovs_last_device_ms(ovs_ctx* ctx, double* ms);
 int ovs_host_alloc(void** p, size_t bytes);
 int ovs_host_free(void* p);
 
+/* ------------------------------------------------------------- adjoint
+ * No counterpart in the reference (the reference has no adjoint): the
+ * vector-Jacobian product of the assembled residual and a GMRES on the
+ * transposed temperature matrix, for sensitivities of functionals. */
+/* fields of the VJP result, N values each (field-major): node coordinates
+ * xg (3), velocity ug (3), pressure pg, VOF phig, temperature Tg,
+ * acceleration acg (3), VOF rate rphig, temperature rate rTg */
+enum { OVS_VJP_XG = 0, OVS_VJP_UG = 3, OVS_VJP_PG = 6, OVS_VJP_PHIG = 7, OVS_VJP_TG = 8,
+       OVS_VJP_ACG = 9, OVS_VJP_RPHIG = 12, OVS_VJP_RTG = 13, OVS_VJP_COUNT = 14 };
+/* grad = (d RHS / d state)^T cot: RHS is the FP64 right-hand side that
+ * ovs_assemble(kernel, OVS_TENSOR_VEC, OVS_FP64) would write for the current
+ * state, parameters and IBC (kernel OVS_ASM_NSVOF: cot is N x 5 field-major
+ * u1 u2 u3 p phi; OVS_ASM_TEM: N x 1), the state the nodal fields above.
+ * Each element's Gauss-point quantities are recomputed in forward-mode
+ * dual arithmetic per nodal input (nothing is stored between assembly and
+ * adjoint); the node sums run in ascending element id, so the result is
+ * deterministic.  grad is N x OVS_VJP_COUNT (fields the kernel does not
+ * depend on come back 0).  Host arrays; synchronous. */
+int ovs_residual_vjp(ovs_ctx* ctx, int kernel, const double* cot, double* grad);
+/* Solve A^T x = rhs by GMRES (the reference-semantics cycle of ovs_gmres,
+ * diagonal preconditioner, zero initial guess), A the assembled FP64
+ * temperature matrix (system OVS_SYS_TEM), through a transposed copy of its
+ * values on the same (symmetric) pattern.  rhs and sol: N values (host). */
+int ovs_gmres_transposed(ovs_ctx* ctx, int system, const double* rhs, double tol, int kspace,
+                         int kspace_min, double* sol, ovs_gmres_info* info);
+
 /* ------------------------------------------------- allocation-free solve
  * No counterpart in the reference: an addition for callers that cannot
  * allocate device memory at solve time - code inside a framework whose

@@ -30,6 +30,9 @@ OVS_SYS_NS, OVS_SYS_NSVOF, OVS_SYS_TEM = 1, 2, 3
 OVS_TENSOR_VEC, OVS_TENSOR_MAT = 2, 4
 OVS_PROF_SPMV, OVS_PROF_ASSEMBLE, OVS_PROF_ARNOLDI, OVS_PROF_ARNOLDI_FUSED = 1, 2, 3, 4
 OVS_PROF_ASSEMBLE_ELEMENTS, OVS_PROF_ASSEMBLE_ROWS = 5, 6
+# fields of the residual VJP (ovs_residual_vjp), N values each
+OVS_VJP_XG, OVS_VJP_UG, OVS_VJP_PG, OVS_VJP_PHIG, OVS_VJP_TG = 0, 3, 6, 7, 8
+OVS_VJP_ACG, OVS_VJP_RPHIG, OVS_VJP_RTG, OVS_VJP_COUNT = 9, 12, 13, 14
 OVS_NOALLOC_MAX_N, OVS_NOALLOC_MAX_KSPACE = 16384, 40
 (OVS_BLK_K11, OVS_BLK_G, OVS_BLK_D1, OVS_BLK_M, OVS_BLK_LS, OVS_BLK_LSU,
  OVS_BLK_ULS, OVS_BLK_PLS, OVS_BLK_TEM) = range(9)
@@ -47,7 +50,8 @@ EXPORTS = [
     "ovs_get_field", "ovs_assemble", "ovs_get_rhs", "ovs_set_rhs", "ovs_get_lhs_block",
     "ovs_set_lhs_block", "ovs_spmv", "ovs_gmres", "ovs_solve", "ovs_newton_update",
     "ovs_residual_norms", "ovs_profile", "ovs_launch_count", "ovs_last_device_ms",
-    "ovs_host_alloc", "ovs_host_free", "ovs_gmres_tem_noalloc",
+    "ovs_host_alloc", "ovs_host_free", "ovs_residual_vjp", "ovs_gmres_transposed",
+    "ovs_gmres_tem_noalloc",
 ]
 
 
@@ -121,6 +125,9 @@ def load(path: str | os.PathLike | None = None) -> C.CDLL:
         "ovs_last_device_ms": ([vp, dp], C.c_int),
         "ovs_host_alloc": ([C.POINTER(vp), C.c_size_t], C.c_int),
         "ovs_host_free": ([vp], C.c_int),
+        "ovs_residual_vjp": ([vp, C.c_int, dp, dp], C.c_int),
+        "ovs_gmres_transposed": ([vp, C.c_int, dp, C.c_double, C.c_int, C.c_int, dp, C.POINTER(OvsGmresInfo)],
+                                 C.c_int),
         "ovs_gmres_tem_noalloc": ([C.c_int, vp, vp, vp, vp, vp, C.c_double, C.c_int, C.c_int, vp,
                                    C.POINTER(OvsGmresInfo)], C.c_int),
     }

@@ -211,6 +211,26 @@ class Context:
                                    _dptr(s) if s is not None else None, C.byref(info)), "ovs_solve")
         return s, info
 
+    def residual_vjp(self, kernel: int, cot: np.ndarray) -> np.ndarray:
+        """(d RHS / d state)^T cot for the FP64 RHS of `kernel` (OVS_ASM_NSVOF:
+        cot (N,5); OVS_ASM_TEM: cot (N,) or (N,1)); returns (N, OVS_VJP_COUNT)
+        with the columns OVS_VJP_* (coordinates, u, p, phi, T, a, phidot,
+        Tdot)."""
+        nf = 1 if kernel == F.OVS_ASM_TEM else 5
+        c = _f64(np.reshape(cot, (self.N, nf), order="F"))
+        g = np.zeros((self.N, F.OVS_VJP_COUNT), order="F")
+        F.check(self.lib.ovs_residual_vjp(self.h, kernel, _dptr(c), _dptr(g)), "ovs_residual_vjp")
+        return g
+
+    def gmres_transposed(self, system: int, rhs: np.ndarray, tol: float, kspace: int, kspace_min: int = 1):
+        """A^T x = rhs for the assembled FP64 temperature matrix (zero start)."""
+        b = _f64(np.reshape(rhs, (self.N,)))
+        x = np.zeros(self.N)
+        info = F.OvsGmresInfo()
+        F.check(self.lib.ovs_gmres_transposed(self.h, system, _dptr(b), tol, kspace, kspace_min, _dptr(x),
+                                              C.byref(info)), "ovs_gmres_transposed")
+        return x, info
+
     def newton_update(self, system: int):
         F.check(self.lib.ovs_newton_update(self.h, system), "ovs_newton_update")
 

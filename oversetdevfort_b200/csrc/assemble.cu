@@ -25,6 +25,7 @@
 //     stores.
 // Gauss-point physics is recomputed by each of the element's nshl rows
 // instead of being staged through HBM.
+#include "dual.cuh"
 #include "ovs_internal.cuh"
 
 #include <math.h>
@@ -85,17 +86,29 @@ __device__ __forceinline__ void tet_shape(int g, T N[4]) {
   N[3] = (T)1.0 - xi - eta - ze;
 }
 
+// Type of the VOF value and of the property blend: FP64 for the FP32 and
+// FP64 routines, the dual number itself for the adjoint.
+template <typename T> struct Wide { using type = double; };
+template <> struct Wide<Dual> { using type = Dual; };
+
 // VOF field at tet Gauss point g in FP64 from the record value (slot k)
 // plus its rounding remainder (lo[.][3]): sum_a N_a phi_a, in node order
 template <typename T>
-__device__ __forceinline__ double gp_phi(const T r[4][16], const T lo[4][4], int k, int g) {
+__device__ __forceinline__ typename Wide<T>::type gp_phi(const T r[4][16], const T lo[4][4], int k, int g) {
+  using W = typename Wide<T>::type;
   const double a = 0.5854101966249685, b = 0.1381966011250105;
   const double xi = (g == 0) ? a : b, eta = (g == 1) ? a : b, ze = (g == 2) ? a : b;
   const double N[4] = {xi, eta, ze, 1.0 - xi - eta - ze};
-  double s = 0.0;
+  W s = 0.0;
 #pragma unroll
-  for (int n = 0; n < 4; ++n) s += ((double)r[n][k] + (double)lo[n][3]) * N[n];
+  for (int n = 0; n < 4; ++n) s += ((W)r[n][k] + (W)lo[n][3]) * N[n];
   return s;
+}
+
+// the clamp of prop_interp (src/e3int.f90:4-13): phic = min(max(phi, 0), 1)
+__device__ __forceinline__ double clamp01(double x) { return fmax(fmin(x, 1.0), 0.0); }
+__device__ __forceinline__ Dual clamp01(const Dual& x) {
+  return x.v < 0.0 ? Dual(0.0) : (x.v > 1.0 ? Dual(1.0) : x);
 }
 
 // store NV (multiple of 4) register values to 16-byte aligned shared memory
@@ -337,6 +350,7 @@ __device__ void summarize_ns(const SumArgs& a, const T r[4][16], const T lo[4][4
 template <typename T>
 __device__ void summarize_nsvof(const SumArgs& a, const T r[4][16], const T lo[4][4], bool fluid, T* o,
                                 double& cfl, T& detj_out) {
+  using W = typename Wide<T>::type;
   const ovs_params& p = a.p;
   T g[4][3], G[3][3], detj, GG, trG;
   element_geometry<T>(r, lo, g, G, detj, GG, trG);
@@ -386,11 +400,11 @@ __device__ void summarize_nsvof(const SumArgs& a, const T r[4][16], const T lo[4
       aci[d] = r[0][9 + d] * N[0] + r[1][9 + d] * N[1] + r[2][9 + d] * N[2] + r[3][9 + d] * N[3];
     }
     const T pri = r[0][12] * N[0] + r[1][12] * N[1] + r[2][12] * N[2] + r[3][12] * N[3];
-    const double phid = gp_phi(r, lo, 13, gp);   // VOF in FP64 for the 1000:1 property blend
+    const W phid = gp_phi<T>(r, lo, 13, gp);   // VOF in FP64 for the 1000:1 property blend
     const T phii = (T)phid;
     const T rphii = r[0][14] * N[0] + r[1][14] * N[1] + r[2][14] * N[2] + r[3][14] * N[3];
     const T Ti = r[0][15] * N[0] + r[1][15] * N[1] + r[2][15] * N[2] + r[3][15] * N[3];
-    const double phicd = fmax(fmin(phid, 1.0), 0.0);
+    const W phicd = clamp01(phid);
     const T phic = (T)phicd;
     T mdot, dmd;
     if (Ti > ts) {
@@ -431,7 +445,7 @@ __device__ void summarize_nsvof(const SumArgs& a, const T r[4][16], const T lo[4
     }
     T kdc = 0;
     if (kdc_on) {
-      const double nk = p.ns_kdc_w * (1.0 - phicd) + p.ns_kdc_a * phicd;
+      const double nk = (double)(p.ns_kdc_w * (1.0 - phicd) + p.ns_kdc_a * phicd);
       const T rr = rL[0] * rL[0] + rL[1] * rL[1] + rL[2] * rL[2];
       kdc = (T)low_word(nk) * sqrt(rr / GG);
     }
@@ -486,6 +500,7 @@ __device__ void summarize_nsvof(const SumArgs& a, const T r[4][16], const T lo[4
 template <typename T>
 __device__ void summarize_tem(const SumArgs& a, const T r[4][16], const T lo[4][4], bool fluid, T* o,
                               double& cfl, T& detj_out) {
+  using W = typename Wide<T>::type;
   const ovs_params& p = a.p;
   T g[4][3], G[3][3], detj, GG, trG;
   element_geometry<T>(r, lo, g, G, detj, GG, trG);
@@ -505,7 +520,7 @@ __device__ void summarize_tem(const SumArgs& a, const T r[4][16], const T lo[4][
   for (int gp = 0; gp < 4; ++gp) {
     T N[4];
     tet_shape<T>(gp, N);
-    const double phid = gp_phi(r, lo, 9, gp);
+    const W phid = gp_phi<T>(r, lo, 9, gp);
     const T Ti = r[0][10] * N[0] + r[1][10] * N[1] + r[2][10] * N[2] + r[3][10] * N[3];
     const T rTi = r[0][11] * N[0] + r[1][11] * N[1] + r[2][11] * N[2] + r[3][11] * N[3];
     T ui[3], umi[3];
@@ -514,7 +529,7 @@ __device__ void summarize_tem(const SumArgs& a, const T r[4][16], const T lo[4][
       ui[d] = r[0][3 + d] * N[0] + r[1][3 + d] * N[1] + r[2][3 + d] * N[2] + r[3][3 + d] * N[3];
       umi[d] = r[0][6 + d] * N[0] + r[1][6 + d] * N[1] + r[2][6 + d] * N[2] + r[3][6 + d] * N[3];
     }
-    const double phicd = fmax(fmin(phid, 1.0), 0.0);
+    const W phicd = clamp01(phid);
     const T phic = (T)phicd;
     T mdot, dmdT;
     if (Ti > ts) {
@@ -1041,6 +1056,119 @@ int launch_assemble(ovs_ctx* c, const AsmArgs& a, const SumArgs& sa, int parts =
   return OVS_OK;
 }
 
+
+// ------------------------------------------------ adjoint of the residual
+// VJP of the assembled residual (the RHS the row pass writes, FP64) with
+// respect to the nodal state.  One thread per element recomputes the
+// element's residual rows on dual numbers once per nodal input of the
+// element (Gauss-point quantities are recomputed, not stored) and contracts
+// the tangent rows with the cotangent, which is zero on Dirichlet rows (the
+// row pass writes 0 there).  A node pass then sums the element terms in
+// ascending element id (deterministic) and applies the alpha-stage chain
+// factors: x+d_a = xg + ..., u_a = .. + alfi ug, p, phi_a = .. + alfi phig,
+// T_a = .. + alfi Tg, a_a = .. + almi acg, phidot_a = .. + almi rphig,
+// Tdot_a = .. + almi rTg (src/solveQuenching.f90:26-37).
+struct VjpArgs {
+  const double* rec;      // FP64 alpha-stage records of the kernel's layout
+  const int* ien;
+  const int* elm_id;
+  const uint8_t* ibc;
+  const double* cot;      // NF*N field-major
+  double* ge;             // E*4*NC element terms
+  int E, N;
+  ovs_params p;
+};
+
+template <int KIND> struct VjpMap;
+// record slot, output field (OVS_VJP_* order), chain factor kind (0: 1, 1: alfi, 2: almi)
+template <> struct VjpMap<OVS_ASM_NSVOF> {
+  static constexpr int NC = 13;
+  __device__ static int slot(int q) { const int s[13] = {0, 1, 2, 3, 4, 5, 12, 13, 15, 9, 10, 11, 14}; return s[q]; }
+};
+template <> struct VjpMap<OVS_ASM_TEM> {
+  static constexpr int NC = 9;
+  __device__ static int slot(int q) { const int s[9] = {0, 1, 2, 3, 4, 5, 9, 10, 11}; return s[q]; }
+};
+static const int h_vjp_out_nsvof[13] = {0, 1, 2, 3, 4, 5, 6, 7, 8, 9, 10, 11, 12};
+static const int h_vjp_fac_nsvof[13] = {0, 0, 0, 1, 1, 1, 0, 1, 1, 2, 2, 2, 2};
+static const int h_vjp_out_tem[9] = {0, 1, 2, 3, 4, 5, 7, 8, 13};
+static const int h_vjp_fac_tem[9] = {0, 0, 0, 1, 1, 1, 1, 1, 2};
+
+template <int KIND>
+__global__ void __launch_bounds__(128) residual_vjp_kernel(const VjpArgs a) {
+  using L = Lay<KIND>;
+  using M = VjpMap<KIND>;
+  constexpr int NF = L::NF;
+  const int e = blockIdx.x * blockDim.x + threadIdx.x;
+  if (e >= a.E) return;
+  const int4 nd = __ldg(reinterpret_cast<const int4*>(a.ien) + e);
+  const int nodes[4] = {nd.x, nd.y, nd.z, nd.w};
+  double r[4][16], lo[4][4];
+#pragma unroll
+  for (int n = 0; n < 4; ++n) load_rec(a.rec, nodes[n], r[n], lo[n]);
+  const bool fluid = __ldg(a.elm_id + e) == a.p.fluid_elm_id;
+  double vv[4][NF];
+#pragma unroll
+  for (int m = 0; m < 4; ++m) {
+    const unsigned ib = __ldg(a.ibc + nodes[m]);
+#pragma unroll
+    for (int f = 0; f < NF; ++f) {
+      const unsigned bit = KIND == OVS_ASM_TEM ? TB : (f < 3 ? (1u << f) : (f == 3 ? PB : FB));
+      vv[m][f] = (ib & bit) ? 0.0 : a.cot[(size_t)f * a.N + nodes[m]];
+    }
+  }
+  SumArgs sa;
+  sa.p = a.p;
+  for (int n = 0; n < 4; ++n) {
+    for (int q = 0; q < M::NC; ++q) {
+      Dual rd[4][16], ld[4][4];
+#pragma unroll
+      for (int m = 0; m < 4; ++m) {
+#pragma unroll
+        for (int k = 0; k < 16; ++k) rd[m][k] = Dual(r[m][k]);
+#pragma unroll
+        for (int k = 0; k < 4; ++k) ld[m][k] = Dual(lo[m][k]);
+      }
+      rd[n][M::slot(q)].d = 1.0;
+      Dual o[L::SW];
+      double cfl = 0.0;
+      Dual detj;
+      if constexpr (KIND == OVS_ASM_NSVOF) summarize_nsvof<Dual>(sa, rd, ld, fluid, o, cfl, detj);
+      else summarize_tem<Dual>(sa, rd, ld, fluid, o, cfl, detj);
+      double acc = 0.0;
+#pragma unroll
+      for (int m = 0; m < 4; ++m)
+#pragma unroll
+        for (int f = 0; f < NF; ++f) acc += vv[m][f] * o[L::RHS0 + NF * m + f].d;
+      a.ge[((size_t)e * 4 + n) * M::NC + q] = acc;
+    }
+  }
+}
+
+struct VjpGatherArgs {
+  const int* n2e_ptr;
+  const int* n2e;
+  const double* ge;
+  double* grad;           // OVS_VJP_COUNT*N field-major
+  int N, NC;
+  int out[16];
+  double fac[16];
+};
+
+__global__ void vjp_gather_kernel(const VjpGatherArgs a) {
+  const int A = blockIdx.x * blockDim.x + threadIdx.x;
+  if (A >= a.N) return;
+  double s[16];
+  for (int q = 0; q < a.NC; ++q) s[q] = 0.0;
+  for (int k = a.n2e_ptr[A]; k < a.n2e_ptr[A + 1]; ++k) {
+    const int packed = a.n2e[k];
+    const double* g = a.ge + ((size_t)(packed >> 3) * 4 + (packed & 7)) * a.NC;
+    for (int q = 0; q < a.NC; ++q) s[q] += g[q];
+  }
+  for (int f = 0; f < OVS_VJP_COUNT; ++f) a.grad[(size_t)f * a.N + A] = 0.0;
+  for (int q = 0; q < a.NC; ++q) a.grad[(size_t)a.out[q] * a.N + A] = a.fac[q] * s[q];
+}
+
 }  // namespace
 
 static int dispatch_assemble(ovs_ctx* c, int kernel, int prec, const AsmArgs& a, const SumArgs& sa,
@@ -1154,5 +1282,65 @@ int ovs_assemble_impl(ovs_ctx* c, int kernel, int tensor_flag, int prec, double*
   }
   if (hflags[1]) return OVS_ERR_NONFINITE;
   if (hflags[0]) return OVS_WARN_NEG_DETJ;
+  return OVS_OK;
+}
+
+int ovs_residual_vjp_impl(ovs_ctx* c, int kernel, const double* cot_host, double* grad_host) {
+  if (!c->have_pattern || !c->have_params) return OVS_ERR_STATE;
+  if (c->nshl != 4) return OVS_ERR_ARG;
+  if (kernel != OVS_ASM_NSVOF && kernel != OVS_ASM_TEM) return OVS_ERR_ARG;
+  if (!cot_host || !grad_host) return OVS_ERR_ARG;
+  const int tem = kernel == OVS_ASM_TEM;
+  const int nf = tem ? 1 : 5, NC = tem ? VjpMap<OVS_ASM_TEM>::NC : VjpMap<OVS_ASM_NSVOF>::NC;
+  const size_t N = c->N, E = c->E;
+  int st;
+  if ((st = ovs_ensure(&c->rec[OVS_FP64], sizeof(double) * N * REC))) return st;
+  if ((st = ovs_ensure((void**)&c->vjp_cot, sizeof(double) * N * 5))) return st;
+  if ((st = ovs_ensure((void**)&c->vjp_ge, sizeof(double) * E * 4 * 13))) return st;
+  if ((st = ovs_ensure((void**)&c->vjp_grad, sizeof(double) * N * OVS_VJP_COUNT))) return st;
+  cudaStream_t s = c->stream;
+  AlphaArgs aa;
+  for (int f = 0; f < OVS_F_COUNT; ++f) aa.f[f] = c->field[f];
+  aa.xg = c->field[OVS_F_XG];
+  aa.rec = c->rec[OVS_FP64];
+  aa.N = c->N;
+  aa.tem = tem;
+  aa.almi = c->params.almi;
+  aa.alfi = c->params.alfi;
+  alpha_records_kernel<double><<<ovs_grid(c->N, 256, 1 << 30), 256, 0, s>>>(aa);
+  ++c->launches;
+  OVS_CUDA_TRY(cudaMemcpyAsync(c->vjp_cot, cot_host, sizeof(double) * N * nf, cudaMemcpyHostToDevice, s));
+  VjpArgs va;
+  va.rec = reinterpret_cast<const double*>(c->rec[OVS_FP64]);
+  va.ien = c->ien;
+  va.elm_id = c->elm_id;
+  va.ibc = c->ibc;
+  va.cot = c->vjp_cot;
+  va.ge = c->vjp_ge;
+  va.E = c->E;
+  va.N = c->N;
+  va.p = c->params;
+  const int eb = (int)((E + 127) / 128);
+  if (tem) residual_vjp_kernel<OVS_ASM_TEM><<<eb, 128, 0, s>>>(va);
+  else residual_vjp_kernel<OVS_ASM_NSVOF><<<eb, 128, 0, s>>>(va);
+  ++c->launches;
+  OVS_CUDA_TRY(cudaGetLastError());
+  VjpGatherArgs ga;
+  ga.n2e_ptr = c->n2e_ptr;
+  ga.n2e = c->n2e;
+  ga.ge = c->vjp_ge;
+  ga.grad = c->vjp_grad;
+  ga.N = c->N;
+  ga.NC = NC;
+  for (int q = 0; q < NC; ++q) {
+    const int fk = tem ? h_vjp_fac_tem[q] : h_vjp_fac_nsvof[q];
+    ga.out[q] = tem ? h_vjp_out_tem[q] : h_vjp_out_nsvof[q];
+    ga.fac[q] = fk == 0 ? 1.0 : (fk == 1 ? c->params.alfi : c->params.almi);
+  }
+  vjp_gather_kernel<<<ovs_grid(c->N, 128, 1 << 30), 128, 0, s>>>(ga);
+  ++c->launches;
+  OVS_CUDA_TRY(cudaGetLastError());
+  OVS_CUDA_TRY(cudaMemcpyAsync(grad_host, c->vjp_grad, sizeof(double) * N * OVS_VJP_COUNT, cudaMemcpyDeviceToHost, s));
+  OVS_CUDA_TRY(cudaStreamSynchronize(s));
   return OVS_OK;
 }

@@ -223,7 +223,7 @@ int ovs_destroy(ovs_ctx* c) {
   if (!c) return OVS_OK;
   cudaSetDevice(c->device);
   if (c->stream) cudaStreamSynchronize(c->stream);
-  void* ptrs[] = {c->ien, c->elm_id, c->ibc, c->rowptr, c->colidx, c->diag, c->n2e_ptr, c->n2e, c->n2s,
+  void* ptrs[] = {c->ien, c->elm_id, c->ibc, c->rowptr, c->colidx, c->diag, c->n2e_ptr, c->n2e, c->n2s, c->tmap, c->vals_t, c->vjp_cot, c->vjp_ge, c->vjp_grad,
                   c->rec[0], c->rec[1], c->esum[0], c->esum[1], c->gm, c->basis[0], c->basis[1], c->work64, c->work32, c->wvec, c->coop_part,
                   c->flags, c->cfl_bits};
   for (void* p : ptrs) if (p) cudaFree(p);
@@ -664,6 +664,48 @@ int ovs_host_alloc(void** p, size_t bytes) {
 
 int ovs_host_free(void* p) {
   if (p) OVS_CUDA_TRY(cudaFreeHost(p));
+  return OVS_OK;
+}
+
+
+int ovs_residual_vjp(ovs_ctx* c, int kernel, const double* cot, double* grad) {
+  if (!c) return OVS_ERR_ARG;
+  int st;
+  if ((st = ovs_activate(c))) return st;
+  OVS_CUDA_TRY(cudaEventRecord(c->ev0, c->stream));
+  if ((st = ovs_residual_vjp_impl(c, kernel, cot, grad))) return st;
+  OVS_CUDA_TRY(cudaEventRecord(c->ev1, c->stream));
+  OVS_CUDA_TRY(cudaEventSynchronize(c->ev1));
+  float ms = 0.f;
+  OVS_CUDA_TRY(cudaEventElapsedTime(&ms, c->ev0, c->ev1));
+  c->last_ms = ms;
+  return OVS_OK;
+}
+
+int ovs_gmres_transposed(ovs_ctx* c, int sys, const double* rhs, double tol, int kspace, int kspace_min,
+                         double* sol, ovs_gmres_info* info) {
+  if (!c || sys != OVS_SYS_TEM || !rhs || !sol) return OVS_ERR_ARG;
+  if (!sys_ok(c, sys, OVS_FP64)) return OVS_ERR_ARG;
+  if (kspace < 1 || kspace > OVS_MAX_KSPACE) return OVS_ERR_ARG;
+  int st;
+  if ((st = ovs_activate(c))) return st;
+  const size_t n = (size_t)c->N;
+  if ((st = ovs_ensure((void**)&c->sol[sys], sizeof(double) * 5 * n))) return st;
+  if ((st = ovs_ensure((void**)&c->work64, sizeof(double) * 15 * n))) return st;
+  OVS_CUDA_TRY(cudaMemcpyAsync(c->work64, rhs, sizeof(double) * n, cudaMemcpyHostToDevice, c->stream));
+  OVS_CUDA_TRY(cudaMemsetAsync(c->sol[sys], 0, sizeof(double) * n, c->stream));
+  ovs_gmres_info gi;
+  memset(&gi, 0, sizeof(gi));
+  OVS_CUDA_TRY(cudaEventRecord(c->ev0, c->stream));
+  if ((st = ovs_gmres_transposed_impl(c, sys, c->work64, tol, kspace, kspace_min, c->sol[sys], &gi))) return st;
+  OVS_CUDA_TRY(cudaEventRecord(c->ev1, c->stream));
+  OVS_CUDA_TRY(cudaEventSynchronize(c->ev1));
+  float ms = 0.f;
+  OVS_CUDA_TRY(cudaEventElapsedTime(&ms, c->ev0, c->ev1));
+  c->last_ms = ms;
+  OVS_CUDA_TRY(cudaMemcpyAsync(sol, c->sol[sys], sizeof(double) * n, cudaMemcpyDeviceToHost, c->stream));
+  OVS_CUDA_TRY(cudaStreamSynchronize(c->stream));
+  if (info) *info = gi;
   return OVS_OK;
 }
 

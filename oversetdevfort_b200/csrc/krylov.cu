@@ -1291,3 +1291,74 @@ int ovs_solve_impl(ovs_ctx* c, int sys, int mode, double rtol, int kspace, int m
   }
   return OVS_OK;
 }
+
+// ------------------------------------------------------ transposed solve
+// Slot of (j, i) for every slot (i, j): the pattern of a finite-element
+// matrix is symmetric, so row j holds column i; a missing entry flags an
+// error instead.
+__global__ void transpose_map_kernel(int N, const int* __restrict__ rowptr, const int* __restrict__ colidx,
+                                     int* __restrict__ tmap, int* __restrict__ err) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= N) return;
+  for (int k = rowptr[i]; k < rowptr[i + 1]; ++k) {
+    const int j = colidx[k];
+    int lo = rowptr[j], hi = rowptr[j + 1];
+    while (hi - lo > 1) {
+      const int mid = (lo + hi) >> 1;
+      if (colidx[mid] > i) hi = mid; else lo = mid;
+    }
+    if (colidx[lo] != i) { atomicOr(err, 1); tmap[k] = k; }
+    else tmap[k] = lo;
+  }
+}
+
+__global__ void gather_vals_kernel(const double* __restrict__ v, const int* __restrict__ tmap,
+                                   double* __restrict__ vt, size_t nnz) {
+  for (size_t k = blockIdx.x * (size_t)blockDim.x + threadIdx.x; k < nnz; k += (size_t)gridDim.x * blockDim.x)
+    vt[k] = v[tmap[k]];
+}
+
+// A^T x = rhs for the scalar temperature system: the transposed values
+// stand in for the system's values during one reference-semantics cycle;
+// the diagonal, and so the Jacobi preconditioner, is the same.
+int ovs_gmres_transposed_impl(ovs_ctx* c, int sys, const double* drhs, double tol, int kspace, int kmin,
+                              double* dsol, ovs_gmres_info* info) {
+  if (sys != OVS_SYS_TEM) return OVS_ERR_ARG;
+  SysStore& S = c->sys[sys][OVS_FP64];
+  if (!S.vals) return OVS_ERR_STATE;
+  int st;
+  cudaStream_t s = c->stream;
+  const size_t nnz = c->nnz;
+  if (!c->tmap) {
+    if ((st = ovs_ensure((void**)&c->tmap, sizeof(int) * (nnz > 0 ? nnz : 1)))) return st;
+    OVS_CUDA_TRY(cudaMemsetAsync(c->flags, 0, sizeof(int) * 4, s));
+    transpose_map_kernel<<<ovs_grid(c->N, 128, 1 << 30), 128, 0, s>>>(c->N, c->rowptr, c->colidx, c->tmap,
+                                                                      c->flags + 2);
+    ++c->launches;
+    int herr = 0;
+    OVS_CUDA_TRY(cudaMemcpyAsync(&herr, c->flags + 2, sizeof(int), cudaMemcpyDeviceToHost, s));
+    OVS_CUDA_TRY(cudaStreamSynchronize(s));
+    if (herr) { cudaFree(c->tmap); c->tmap = nullptr; return OVS_ERR_PATTERN; }
+  }
+  if ((st = ovs_ensure(&c->vals_t, sizeof(double) * (nnz > 0 ? nnz : 1)))) return st;
+  gather_vals_kernel<<<4 * c->num_sms, 256, 0, s>>>(reinterpret_cast<const double*>(S.vals), c->tmap,
+                                                    reinterpret_cast<double*>(c->vals_t), nnz);
+  ++c->launches;
+  OVS_CUDA_TRY(cudaGetLastError());
+  if ((st = ovs_precond_setup(c, sys, OVS_FP64))) return st;
+  double rr;
+  if ((st = dot64(c, drhs, drhs, (size_t)c->N, &rr))) return st;
+  if (rr == 0.0) {   // SparseGMRES_tem.f90:63-71
+    OVS_CUDA_TRY(cudaMemsetAsync(dsol, 0, sizeof(double) * c->N, s));
+    OVS_CUDA_TRY(cudaStreamSynchronize(s));
+    if (info) { memset(info, 0, sizeof(*info)); info->converged = 1; }
+    return OVS_OK;
+  }
+  void* saved = S.vals;
+  S.vals = c->vals_t;
+  st = gmres_cycle<double, double>(c, sys, drhs, dsol, tol, kspace, kmin, info);
+  S.vals = saved;
+  if (st) return st;
+  OVS_CUDA_TRY(cudaStreamSynchronize(s));
+  return OVS_OK;
+}

@@ -77,6 +77,11 @@ struct ovs_ctx {
   int* diag = nullptr;       // N: slot of the diagonal entry
   int* n2e_ptr = nullptr;    // N+1
   int* n2e = nullptr;        // nshl*E: (element << 3) | local index, sorted by element
+  int* tmap = nullptr;       // nnz: slot of (j, i) for slot (i, j), transposed solves
+  void* vals_t = nullptr;    // transposed FP64 values of the temperature system
+  double* vjp_cot = nullptr; // residual VJP work: cotangent, element terms, nodal result
+  double* vjp_ge = nullptr;
+  double* vjp_grad = nullptr;
   unsigned* n2s = nullptr;   // nshl*E: slots of the element's 4 nodes in the row, one byte each (tets)
   int nnz = 0;
   int max_deg = 0, max_elem = 0;
@@ -136,6 +141,9 @@ int ovs_resnorm_impl(ovs_ctx* c, int prec, double r[4]);
 int ovs_dot_impl(ovs_ctx* c, const double* a, const double* b, size_t n,
                  double* out);
 int ovs_profile_assemble(ovs_ctx* c, int kernel, int prec, int reps, double* ms, int parts);
+int ovs_residual_vjp_impl(ovs_ctx* c, int kernel, const double* cot_host, double* grad_host);
+int ovs_gmres_transposed_impl(ovs_ctx* c, int sys, const double* drhs, double tol, int kspace, int kmin,
+                              double* dsol, ovs_gmres_info* info);
 int ovs_profile_krylov(ovs_ctx* c, int what, int sys, int prec, int reps, double* ms);
 
 // launch geometry helper

@@ -246,6 +246,7 @@ int ovs_pattern_build(ovs_ctx* c) {
   if (h[0] != 0) { cudaFreeAsync(cnt, s); cudaFreeAsync(tmp, s); cudaFreeAsync(stats, s); return OVS_ERR_ARG; }
   if (h[1] != 0) { cudaFreeAsync(cnt, s); cudaFreeAsync(tmp, s); cudaFreeAsync(stats, s); return OVS_ERR_PATTERN; }
   c->max_elem = h[2];
+  if (c->tmap) { cudaFree(c->tmap); c->tmap = nullptr; }   // transpose map of an earlier pattern
   c->max_deg = h[3];
   c->nnz = nnz;
   if ((st = ovs_ensure((void**)&c->colidx, sizeof(int) * (size_t)(nnz > 0 ? nnz : 1)))) return st;

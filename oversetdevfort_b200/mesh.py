@@ -238,6 +238,66 @@ def config5(n: int = 32) -> Case:
     return quench_case(box_tet(n, n, n), f"config5_quench_{n}cube")
 
 
+def adjoint_case(n: int = 32, seed: int = 5) -> Case:
+    """Config 5 for the adjoint checks: the config-2 quench physics on an
+    n^3-cell unit cube (n = 32: 196,608 tets, 35,937 nodes) with two changes
+    that make the residual differentiable where it is probed.  The VOF field
+    stays inside (0, 1), phi = 0.5 + 0.49 tanh((z - 1/2)/0.02), because the
+    clamp of prop_interp has no derivative at 0 and 1 and a finite-difference
+    stencil across it measures the kink.  A seeded random velocity
+    (U[-0.01, 0.01], walls kept at 0) and pressure (U[-1, 1]) make the
+    advective and stabilisation terms depend on every input."""
+    c = quench_case(box_tet(n, n, n), f"config5_adjoint_{n}cube")
+    m, st, p = c.mesh, c.state, c.params
+    rng = np.random.default_rng(seed)
+    N = m.nnode
+    phi = 0.5 + 0.49 * np.tanh((m.xg[:, 2] - 0.5 * m.lengths[2]) / 0.02)
+    st["phig"][:] = phi
+    st["phigold"][:] = phi
+    wall = np.zeros(N, dtype=bool)
+    for f in range(6):
+        wall[m.faces[f]] = True
+    u = rng.uniform(-0.01, 0.01, (N, 3))
+    u[wall] = 0.0
+    st["ug"][:] = u
+    st["ugold"][:] = u
+    st["pg"][:] = rng.uniform(-1.0, 1.0, N)
+    st["rtg"][:] = rng.uniform(-10.0, 10.0, N)
+    st["rtgold"][:] = st["rtg"]
+    c.extra["seed"] = seed
+    return c
+
+
+def bottom_heat_flux_weights(case: Case, phi: np.ndarray | None = None) -> np.ndarray:
+    """Weights c of the integrated heat flux through the bottom wall z = 0,
+    J(T) = c . T = sum over the boundary triangles on z = 0 of
+    area * k_e * dT/dz, with dT/dz the z-derivative of the linear tet that
+    owns the triangle and k_e = prop_interp(kappaw, kappaa, phi_e) at the tet
+    (phi_e the mean of its nodal VOF values, clamped to [0, 1]; phi = 1 gas).
+    The functional is defined here: the reference's convective-heat face
+    assembly, which such a functional would use, is not in its sources."""
+    m = case.mesh
+    p = case.params
+    if phi is None:
+        phi = case.state["phig"]
+    ien0 = np.asarray(m.ien, dtype=np.int64) - 1
+    on = m.xg[:, 2] <= 1e-12
+    sel = np.nonzero(on[ien0].sum(axis=1) == 3)[0]
+    X = m.xg[ien0[sel]]                                     # (Eb, 4, 3)
+    M = np.concatenate([np.ones((sel.size, 4, 1)), X], axis=2)
+    grad = np.linalg.inv(M)[:, 1:4, :]                      # (Eb, 3, 4): d N_a / d x_i
+    c = np.zeros(m.nnode)
+    for e in range(sel.size):
+        nodes = ien0[sel[e]]
+        b = [a for a in range(4) if on[nodes[a]]]
+        P = m.xg[nodes[b]]
+        area = 0.5 * np.linalg.norm(np.cross(P[1] - P[0], P[2] - P[0]))
+        ph = min(max(float(np.mean(phi[nodes])), 0.0), 1.0)
+        k = p["kappaw"] * (1.0 - ph) + p["kappaa"] * ph
+        np.add.at(c, nodes, area * k * grad[e, 2, :])
+    return c
+
+
 def random_case(nx=4, ny=3, nz=3, seed=0, kernel=F.OVS_ASM_NSVOF, solid_frac=0.15,
                 bc_frac=0.2, phase_change=True) -> Case:
     """Small case with every code path switched on: random state fields,
