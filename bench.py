@@ -234,6 +234,70 @@ def run_reference(args, world, rank):
     print(json.dumps(line), flush=True)
 
 
+# ------------------------------------------------------------ adjoint
+def run_adjoint(local_rank):
+    """Config 5 (32^3 cells x6 tets): device time of the residual VJP (NS+VOF
+    and T passes) and of the transposed temperature solve, one central
+    difference check (h = 1e-6) of the VJP, and the gap between A^T v of the
+    assembled NS+VOF matrix and J^T v of the Newton Jacobian (informative:
+    that matrix is not the exact Jacobian of its residual)."""
+    import numpy as np
+    from oversetdevfort_b200 import _ffi as F
+    from oversetdevfort_b200 import adjoint as AD
+    from oversetdevfort_b200 import mesh as M
+    from oversetdevfort_b200.api import Context
+
+    case = M.adjoint_case(32)
+    ctx = Context.from_case(case, device=local_rank)
+    N = ctx.N
+    rng = np.random.default_rng(5)
+    v1, v2 = rng.standard_normal((N, 5)), rng.standard_normal(N)
+    ctx.residual_vjp(F.OVS_ASM_NSVOF, v1)
+    g = ctx.residual_vjp(F.OVS_ASM_NSVOF, v1)
+    ms_ns = ctx.last_device_ms()
+    g = g + ctx.residual_vjp(F.OVS_ASM_TEM, v2)
+    ms_t = ctx.last_device_ms()
+    names = {"ug": (F.OVS_VJP_UG, 0.01), "pg": (F.OVS_VJP_PG, 1.0), "phig": (F.OVS_VJP_PHIG, 0.1),
+             "tg": (F.OVS_VJP_TG, 300.0), "xg": (F.OVS_VJP_XG, 1.0 / 32)}
+    st0 = {n: ctx.get_field(n).copy() for n in names}
+    w = {n: sc * rng.standard_normal(st0[n].shape) for n, (_, sc) in names.items()}
+    h, vals = 1e-6, []
+    for sgn in (1.0, -1.0):
+        for n in names:
+            ctx.set_field(n, st0[n] + sgn * h * w[n])
+        r1, r2 = AD.residuals(ctx)
+        vals.append(float(np.sum(v1 * r1) + np.sum(v2 * r2)))
+    for n in names:
+        ctx.set_field(n, st0[n])
+    fd = (vals[0] - vals[1]) / (2 * h)
+    ad = 0.0
+    for n, (col, _) in names.items():
+        width = 3 if st0[n].ndim == 2 else 1
+        ad += float(np.sum(g[:, col:col + width].reshape(st0[n].shape) * w[n]))
+    c = M.bottom_heat_flux_weights(case)
+    ctx.assemble(F.OVS_ASM_TEM, F.OVS_TENSOR_MAT | F.OVS_TENSOR_VEC, F.OVS_FP64)
+    pr = ctx.params
+    lam, info = ctx.gmres_transposed(F.OVS_SYS_TEM, pr["gami"] * pr["delt"] * c, 1e-14, 200)
+    ms_tr = ctx.last_device_ms()
+    # Dirichlet rows and columns are replaced in the assembled matrix
+    # (diagonal = element count), so v is zero on constrained rows and only
+    # free dofs are compared
+    free = case.ibc[:, 0:5] == 0
+    vm = np.where(free, v1, 0.0)
+    ctx.assemble(F.OVS_ASM_NSVOF, F.OVS_TENSOR_MAT | F.OVS_TENSOR_VEC, F.OVS_FP64)
+    atv = np.where(free, AD.lhs_transpose_times(ctx, vm), 0.0)
+    jtv = np.where(free, AD.newton_jacobian_transpose_times(ctx, vm), 0.0)
+    gap = {k: float(np.abs(atv[:, sl] - jtv[:, sl]).max() / max(np.abs(jtv[:, sl]).max(), 1e-300))
+           for k, sl in (("u", slice(0, 3)), ("p", slice(3, 4)), ("phi", slice(4, 5)))}
+    ctx.close()
+    return {"workload": f"config5: {case.mesh.nelem} tets, {N} nodes (32^3 cells x6)",
+            "vjp_ms": {"nsvof": ms_ns, "tem": ms_t},
+            "vjp_melem_s": case.mesh.nelem / ((ms_ns + ms_t) * 1e-3) / 1e6,
+            "fd_check_rel_err": abs(fd - ad) / abs(ad),
+            "transposed_gmres": {"ms": ms_tr, "iterations": info.iterations, "converged": bool(info.converged)},
+            "lhs_t_v_vs_newton_jacobian_t_v_rel_gap": gap}
+
+
 # --------------------------------------------------------------- GPU arm
 def run_ours(args, world, rank, local_rank, dist):
     import numpy as np
@@ -412,6 +476,7 @@ def run_ours(args, world, rank, local_rank, dist):
     barrier_()
     clk = clocks.stop()
     total_launches = ctx.launch_count() - launches0
+    adj = None if args.no_adjoint else run_adjoint(local_rank)
 
     line = {
         "metric": METRIC, "value": value, "unit": "Melem/s", "n_gpus": world, "steps": args.steps,
@@ -432,6 +497,7 @@ def run_ours(args, world, rank, local_rank, dist):
                              "fp64": world * E / (res["fp64"]["ms"] * 1e-3) / 1e6,
                              "ms_fp32": res["fp32"]["ms"], "ms_fp64": res["fp64"]["ms"]},
         "gmres": gm,
+        "adjoint": adj,
         "kernel_ms": prof,
         "launches_total": total_launches,
         "setup_s": setup_s,
@@ -456,6 +522,7 @@ def main():
     ap.add_argument("--kspace", type=int, default=50)
     ap.add_argument("--max-cycles", type=int, default=400)
     ap.add_argument("--no-solve", action="store_true")
+    ap.add_argument("--no-adjoint", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
     args = ap.parse_args()
     if args.warmup < 3:

@@ -97,3 +97,39 @@ def heat_flux_sensitivity(ctx: Context, c: np.ndarray, tol: float = 1e-14, kspac
     lam, info = ctx.gmres_transposed(F.OVS_SYS_TEM, p["gami"] * p["delt"] * c, tol, kspace)
     g = ctx.residual_vjp(F.OVS_ASM_TEM, lam)
     return c + g[:, F.OVS_VJP_TG], g[:, F.OVS_VJP_RTG], lam, info
+
+
+def lhs_transpose_times(ctx: Context, v: np.ndarray) -> np.ndarray:
+    """A^T v for the assembled FP64 NS+VOF block matrix (host arithmetic on
+    the reference block arrays; v and the result (N, 5): u1 u2 u3 p phi).
+    Blocks per slot (row node a, column node b): K(i,j) row u_i col u_j,
+    G(i) row u_i col p, ULS(i) row u_i col phi, D(j) row p col u_j, M p-p,
+    PLS row p col phi, LSU(j) row phi col u_j, LS phi-phi."""
+    s = ctx.get_system(F.OVS_SYS_NSVOF, F.OVS_FP64)
+    col, row = ctx.get_pattern()
+    a = np.repeat(np.arange(ctx.N), np.diff(col))
+    b = row - 1
+    K = s["K11"].reshape(-1, 3, 3)          # [slot, i, j]: row comp i, col comp j
+    y = np.zeros((ctx.N, 5))
+    va = v[a]
+    for j in range(3):
+        np.add.at(y[:, j], b, np.einsum("ki,ki->k", K[:, :, j], va[:, 0:3]) + s["D1"][:, j] * va[:, 3]
+                  + s["LSU"][:, j] * va[:, 4])
+    np.add.at(y[:, 3], b, np.einsum("ki,ki->k", s["G"], va[:, 0:3]) + s["M"] * va[:, 3])
+    np.add.at(y[:, 4], b, np.einsum("ki,ki->k", s["ULS"], va[:, 0:3]) + s["PLS"] * va[:, 3] + s["LS"] * va[:, 4])
+    return y
+
+
+def newton_jacobian_transpose_times(ctx: Context, v: np.ndarray) -> np.ndarray:
+    """J^T v with J = -d RHS_NSVOF / d(Newton increment): acg += du,
+    ug += gami delt du; pg += alfi gami delt dp; rphig += dphi,
+    phig += gami delt dphi (src/solveFlow.f90:99-104) -- the matrix the
+    assembled LHS stands for, from the VJP."""
+    p = ctx.params
+    g = ctx.residual_vjp(F.OVS_ASM_NSVOF, v)
+    gd = p["gami"] * p["delt"]
+    y = np.zeros((ctx.N, 5))
+    y[:, 0:3] = g[:, F.OVS_VJP_ACG:F.OVS_VJP_ACG + 3] + gd * g[:, F.OVS_VJP_UG:F.OVS_VJP_UG + 3]
+    y[:, 3] = p["alfi"] * gd * g[:, F.OVS_VJP_PG]
+    y[:, 4] = g[:, F.OVS_VJP_RPHIG] + gd * g[:, F.OVS_VJP_PHIG]
+    return -y

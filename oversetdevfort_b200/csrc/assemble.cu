@@ -222,8 +222,9 @@ __device__ __forceinline__ void cfl_max(unsigned long long* bits, double v) {
 // and zero residuals, which makes every expanded block exactly zero.
 //   NS   : g(12) w KA KB MM | GP x4: uadv(3) rt        | residual 4x4 = 48
 //   NSVOF: g(12) w KA KB MM KDP dphi(3) | GP x4: uadv(3) rho rt tauLS src
-//          eps ufac plfac                              | residual 4x5 = 80
-//   TEM  : g(12) w HK | GP x4: uadv(3) rcp dSe trc     | residual 4 +pad = 44
+//          eps ufac plfac pad(2)                       | residual 4x5 = 88
+//   TEM  : g(12) w HK pad(2) | GP x4: uadv(3) rcp dSe trc pad(2) | residual 4 = 52
+// (Gauss-point records padded to 16-byte groups for vector loads)
 // with rt = rho tauM, trc = tauT rho cp and the factors of the block sums
 // below (src, eps, ufac, plfac of the phase-change terms).
 template <int KIND> struct Lay;
