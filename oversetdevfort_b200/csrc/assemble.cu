@@ -1170,10 +1170,20 @@ __global__ void vjp_gather_kernel(const VjpGatherArgs a) {
   for (int q = 0; q < a.NC; ++q) a.grad[(size_t)a.out[q] * a.N + A] = a.fac[q] * s[q];
 }
 
+#include "assemble_hex.cuh"
+
 }  // namespace
 
 static int dispatch_assemble(ovs_ctx* c, int kernel, int prec, const AsmArgs& a, const SumArgs& sa,
                              int parts = 3) {
+  if (c->nshl == 8) {   // trilinear hexahedra: NS+VOF and temperature passes
+    if (kernel == OVS_ASM_NS) return OVS_ERR_ARG;
+    if (prec == OVS_FP64)
+      return kernel == OVS_ASM_NSVOF ? launch_assemble_hex<double, OVS_ASM_NSVOF>(c, a, sa, parts)
+                                     : launch_assemble_hex<double, OVS_ASM_TEM>(c, a, sa, parts);
+    return kernel == OVS_ASM_NSVOF ? launch_assemble_hex<float, OVS_ASM_NSVOF>(c, a, sa, parts)
+                                   : launch_assemble_hex<float, OVS_ASM_TEM>(c, a, sa, parts);
+  }
   if (prec == OVS_FP64) {
     if (kernel == OVS_ASM_NS) return launch_assemble<double, OVS_ASM_NS>(c, a, sa, parts);
     if (kernel == OVS_ASM_NSVOF) return launch_assemble<double, OVS_ASM_NSVOF>(c, a, sa, parts);
@@ -1238,7 +1248,8 @@ int ovs_profile_assemble(ovs_ctx* c, int kernel, int prec, int reps, double* ms,
 
 int ovs_assemble_impl(ovs_ctx* c, int kernel, int tensor_flag, int prec, double* cfl) {
   if (!c->have_pattern || !c->have_params) return OVS_ERR_STATE;
-  if (c->nshl != 4) return OVS_ERR_ARG;
+  if (c->nshl != 4 && c->nshl != 8) return OVS_ERR_ARG;
+  if (c->nshl == 8 && kernel == OVS_ASM_NS) return OVS_ERR_ARG;
   if (kernel != OVS_ASM_NS && kernel != OVS_ASM_NSVOF && kernel != OVS_ASM_TEM) return OVS_ERR_ARG;
   if (prec != OVS_FP64 && prec != OVS_FP32) return OVS_ERR_ARG;
   const int sys = kernel == OVS_ASM_NS ? OVS_SYS_NS : (kernel == OVS_ASM_NSVOF ? OVS_SYS_NSVOF : OVS_SYS_TEM);
@@ -1249,7 +1260,8 @@ int ovs_assemble_impl(ovs_ctx* c, int kernel, int tensor_flag, int prec, double*
   if ((st = ovs_ensure(&S.vals, ts * (size_t)c->nnz * nv))) return st;
   if ((st = ovs_ensure(&S.rhs, ts * (size_t)c->N * nf))) return st;
   if ((st = ovs_ensure(&c->rec[prec], ts * (size_t)c->N * REC))) return st;
-  if ((st = ovs_ensure(&c->esum[prec], ts * (size_t)c->E * Lay<OVS_ASM_NSVOF>::SW))) return st;
+  const size_t sw = c->nshl == 8 ? (size_t)HexLay<OVS_ASM_NSVOF>::SW : (size_t)Lay<OVS_ASM_NSVOF>::SW;
+  if ((st = ovs_ensure(&c->esum[prec], ts * (size_t)c->E * sw))) return st;
   cudaStream_t s = c->stream;
   OVS_CUDA_TRY(cudaMemsetAsync(c->flags, 0, sizeof(int) * 4, s));
   OVS_CUDA_TRY(cudaMemsetAsync(c->cfl_bits, 0, sizeof(unsigned long long), s));
@@ -1288,7 +1300,7 @@ int ovs_assemble_impl(ovs_ctx* c, int kernel, int tensor_flag, int prec, double*
 
 int ovs_residual_vjp_impl(ovs_ctx* c, int kernel, const double* cot_host, double* grad_host) {
   if (!c->have_pattern || !c->have_params) return OVS_ERR_STATE;
-  if (c->nshl != 4) return OVS_ERR_ARG;
+  if (c->nshl != 4) return OVS_ERR_ARG;   // the adjoint covers the tet routines
   if (kernel != OVS_ASM_NSVOF && kernel != OVS_ASM_TEM) return OVS_ERR_ARG;
   if (!cot_host || !grad_host) return OVS_ERR_ARG;
   const int tem = kernel == OVS_ASM_TEM;

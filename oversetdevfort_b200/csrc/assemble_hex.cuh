@@ -1,0 +1,612 @@
+// Trilinear hexahedra (nshl = 8): the NS+VOF quench and temperature
+// element routines (src/solveQuenching.f90:122-882) with the 2x2x2 rule
+// (src/genGP_GW.f90:355-389) and linhexshl (src/eval_shape_FEM.f90:148-196),
+// assembled like the tets: an element pass writes per-Gauss-point records
+// and the element's residual rows, a row pass (one warp per CSR row) expands
+// the blocks of A's row and adds them in ascending element id.  Unlike a
+// linear tet, a hex has different gradients at every Gauss point, so the
+// row pass sums each block over the 8 points.  Included into assemble.cu's
+// anonymous namespace (it uses its helpers).
+
+// node signs of linhexshl: N_a = (1 + sx xi)(1 + sy eta)(1 + sz zeta) / 8
+__constant__ signed char c_hex_sign[8][3] = {{-1, 1, -1}, {1, 1, -1}, {1, 1, 1}, {-1, 1, 1},
+                                             {-1, -1, -1}, {1, -1, -1}, {1, -1, 1}, {-1, -1, 1}};
+// 2x2x2 points (genGPandGW, weights 1)
+__device__ __forceinline__ void hex_gp(int g, double& xi, double& eta, double& ze) {
+  const double q = 0.57735026918963;
+  xi = (g & 1) ? q : -q;
+  eta = (g & 2) ? q : -q;
+  ze = (g & 4) ? q : -q;
+}
+template <typename T>
+__device__ __forceinline__ T hex_N(int g, int a) {
+  double xi, eta, ze;
+  hex_gp(g, xi, eta, ze);
+  return (T)((1.0 + c_hex_sign[a][0] * xi) * (1.0 + c_hex_sign[a][1] * eta) * (1.0 + c_hex_sign[a][2] * ze) * 0.125);
+}
+
+template <int KIND> struct HexLay;
+//   NS+VOF record per point: g(8x3) w KA KB MM KDP dphi(3) uadv(3) rho rt
+//   tauLS src eps ufac plfac pad(2); then the residual rows 8x5
+template <> struct HexLay<OVS_ASM_NSVOF> {
+  static constexpr int GPW = 44, RHS0 = 8 * 44, NF = 5, SW = 8 * 44 + 40, NV = 24;
+};
+//   T record per point: g(8x3) w HK uadv(3) rcp dSe trc; then 8 residuals
+template <> struct HexLay<OVS_ASM_TEM> {
+  static constexpr int GPW = 32, RHS0 = 8 * 32, NF = 1, SW = 8 * 32 + 8, NV = 1;
+};
+
+// eval_shape_fem for a hex at point g on x+d: global gradients, DetJ, G
+template <typename T>
+__device__ __forceinline__ T hex_geometry(int gp, const T r[8][16], const T lo[8][4], T g[8][3], T G[3][3]) {
+  double xi, eta, ze;
+  hex_gp(gp, xi, eta, ze);
+  T dN[8][3];
+#pragma unroll
+  for (int a = 0; a < 8; ++a) {
+    const double sx = c_hex_sign[a][0], sy = c_hex_sign[a][1], sz = c_hex_sign[a][2];
+    dN[a][0] = (T)(sx * (1.0 + sy * eta) * (1.0 + sz * ze) * 0.125);
+    dN[a][1] = (T)(sy * (1.0 + sx * xi) * (1.0 + sz * ze) * 0.125);
+    dN[a][2] = (T)(sz * (1.0 + sx * xi) * (1.0 + sy * eta) * 0.125);
+  }
+  // dx/dxi from coordinates relative to node 0 (sum_a dN_a = 0), so the
+  // FP32 path keeps the edge lengths to full precision
+  T A[3][3], Ai[3][3];
+#pragma unroll
+  for (int i = 0; i < 3; ++i)
+#pragma unroll
+    for (int j = 0; j < 3; ++j) {
+      T s = 0;
+#pragma unroll
+      for (int a = 1; a < 8; ++a) s += ((r[a][i] - r[0][i]) + (lo[a][i] - lo[0][i])) * dN[a][j];
+      A[i][j] = s;
+    }
+  Ai[0][0] = A[1][1] * A[2][2] - A[2][1] * A[1][2];
+  Ai[0][1] = A[2][1] * A[0][2] - A[0][1] * A[2][2];
+  Ai[0][2] = A[0][1] * A[1][2] - A[0][2] * A[1][1];
+  T tmp = (T)1.0 / (Ai[0][0] * A[0][0] + Ai[0][1] * A[1][0] + Ai[0][2] * A[2][0]);
+  Ai[0][0] *= tmp; Ai[0][1] *= tmp; Ai[0][2] *= tmp;
+  Ai[1][0] = (A[1][2] * A[2][0] - A[1][0] * A[2][2]) * tmp;
+  Ai[1][1] = (A[0][0] * A[2][2] - A[2][0] * A[0][2]) * tmp;
+  Ai[1][2] = (A[1][0] * A[0][2] - A[0][0] * A[1][2]) * tmp;
+  Ai[2][0] = (A[1][0] * A[2][1] - A[1][1] * A[2][0]) * tmp;
+  Ai[2][1] = (A[2][0] * A[0][1] - A[0][0] * A[2][1]) * tmp;
+  Ai[2][2] = (A[0][0] * A[1][1] - A[0][1] * A[1][0]) * tmp;
+#pragma unroll
+  for (int a = 0; a < 8; ++a)
+#pragma unroll
+    for (int j = 0; j < 3; ++j) g[a][j] = dN[a][0] * Ai[0][j] + dN[a][1] * Ai[1][j] + dN[a][2] * Ai[2][j];
+#pragma unroll
+  for (int i = 0; i < 3; ++i)
+#pragma unroll
+    for (int j = 0; j < 3; ++j) G[i][j] = Ai[0][i] * Ai[0][j] + Ai[1][i] * Ai[1][j] + Ai[2][i] * Ai[2][j];
+  return (T)1.0 / tmp;
+}
+
+template <typename T>
+__device__ __forceinline__ typename Wide<T>::type hex_phi(const T r[8][16], const T lo[8][4], int k, int gp) {
+  using W = typename Wide<T>::type;
+  W s = 0.0;
+#pragma unroll
+  for (int a = 0; a < 8; ++a) s += ((W)r[a][k] + (W)lo[a][3]) * hex_N<double>(gp, a);
+  return s;
+}
+
+template <typename T>
+__device__ __forceinline__ void store_n(T* dst, const T* v, int n) {
+  for (int k = 0; k < n; ++k) dst[k] = v[k];
+}
+
+// element pass, NS+VOF quench on a hex (src/solveQuenching.f90:295-523)
+template <typename T>
+__device__ void hex_summarize_nsvof(const ovs_params& p, const T r[8][16], const T lo[8][4], bool fluid,
+                                    T* out, double& cfl, int& nbad) {
+  using W = typename Wide<T>::type;
+  using L = HexLay<OVS_ASM_NSVOF>;
+  const T fact2 = (T)(p.alfi * p.delt * p.gami);
+  const T taut = (T)(4.0 / (p.delt * p.delt));
+  const T rhoa = (T)p.rhoa, rhow = (T)p.rhow, ts = (T)p.ts;
+  const T ira = (T)1.0 / rhoa - (T)1.0 / rhow;
+  const bool kdc_on = fabs(p.ns_kdc_w) + fabs(p.ns_kdc_a) > 0.0;
+  const bool kdcphi_on = fabs(p.lsc_kdc) > 0.0;
+  T ru[8][3], rp[8], rf[8];
+#pragma unroll
+  for (int n = 0; n < 8; ++n) { ru[n][0] = ru[n][1] = ru[n][2] = 0; rp[n] = 0; rf[n] = 0; }
+  for (int gp = 0; gp < 8; ++gp) {
+    T g[8][3], G[3][3];
+    const T detj = hex_geometry<T>(gp, r, lo, g, G);
+    if (!(detj > (T)0)) nbad = 1;
+    const T w = detj;   // hex weights are 1
+    T GG = 0;
+#pragma unroll
+    for (int j = 0; j < 3; ++j)
+#pragma unroll
+      for (int i = 0; i < 3; ++i) GG += G[i][j] * G[i][j];
+    const T trG = G[0][0] + G[1][1] + G[2][2];
+    T N[8];
+#pragma unroll
+    for (int a = 0; a < 8; ++a) N[a] = hex_N<T>(gp, a);
+    T du[3][3], dp[3], dphi[3], ui[3], umi[3], aci[3];
+#pragma unroll
+    for (int i = 0; i < 3; ++i) {
+      ui[i] = umi[i] = aci[i] = 0;
+#pragma unroll
+      for (int j = 0; j < 3; ++j) du[i][j] = 0;
+      dp[i] = dphi[i] = 0;
+    }
+    T pri = 0, rphii = 0, Ti = 0;
+#pragma unroll
+    for (int a = 0; a < 8; ++a) {
+#pragma unroll
+      for (int i = 0; i < 3; ++i) {
+        ui[i] += r[a][3 + i] * N[a];
+        umi[i] += r[a][6 + i] * N[a];
+        aci[i] += r[a][9 + i] * N[a];
+#pragma unroll
+        for (int j = 0; j < 3; ++j) du[i][j] += r[a][3 + i] * g[a][j];
+        dp[i] += r[a][12] * g[a][i];
+        dphi[i] += r[a][13] * g[a][i];
+      }
+      pri += r[a][12] * N[a];
+      rphii += r[a][14] * N[a];
+      Ti += r[a][15] * N[a];
+    }
+    const T divu = du[0][0] + du[1][1] + du[2][2];
+    const W phid = hex_phi<T>(r, lo, 13, gp);
+    const T phii = (T)phid;
+    const W phicd = clamp01(phid);
+    const T phic = (T)phicd;
+    T mdot, dmd;
+    if (Ti > ts) {
+      mdot = (T)p.c_evap * (T)(1.0 - phicd) * rhow * (Ti - ts) / ts;
+      dmd = -(T)p.c_evap * rhow * (Ti - ts) / ts * (T)p.c_dmdot;
+    } else {
+      mdot = (T)p.c_cond * phic * rhoa * (Ti - ts) / ts;
+      dmd = (T)p.c_cond * rhoa * (Ti - ts) / ts * (T)p.c_dmdot;
+    }
+    const T vdot = mdot / rhoa - mdot / rhow;
+    T rho, mu;
+    if (fluid) {
+      rho = (T)(p.rhow * (1.0 - phicd) + p.rhoa * phicd);
+      mu = (T)(p.muw * (1.0 - phicd) + p.mua * phicd);
+    } else {
+      rho = (T)p.rhos; mu = (T)p.mus;
+    }
+    const T lambda = (T)(-2.0 / 3.0) * mu;
+    if (phid < 0.0 || phid > 1.0) dmd = 0;
+    const T uadv[3] = {ui[0] - umi[0], ui[1] - umi[1], ui[2] - umi[2]};
+    T tmp1[3], rL[3];
+#pragma unroll
+    for (int i = 0; i < 3; ++i) {
+      const T conv = du[i][0] * uadv[0] + du[i][1] * uadv[1] + du[i][2] * uadv[2];
+      tmp1[i] = rho * aci[i] + rho * conv - (T)p.gravvec[i] * rho;
+      rL[i] = tmp1[i] + dp[i];
+    }
+    const T res_phi = rphii + (uadv[0] * dphi[0] + uadv[1] * dphi[1] + uadv[2] * dphi[2]) + phii * vdot - mdot / rhoa;
+    const T taua = quad_uGu<T>(uadv, G);
+    const T nu = mu / rho;
+    const T taud = nu * nu * (T)12.0 * GG;
+    const T tauM = (T)1.0 / (rho * sqrt(taut + taua + taud));
+    const T tauLS = (T)1.0 / sqrt(taut + taua);
+    const T tauC = rho * sqrt(taua + taud) / trG;
+    {
+      const double cf = (double)p.delt * sqrt((double)taua);
+      if (cf > cfl) cfl = cf;
+    }
+    T kdc = 0;
+    if (kdc_on) {
+      const double nk = (double)(p.ns_kdc_w * (1.0 - phicd) + p.ns_kdc_a * phicd);
+      const T rr = rL[0] * rL[0] + rL[1] * rL[1] + rL[2] * rL[2];
+      kdc = (T)low_word(nk) * sqrt(rr / GG);
+    }
+    T kdphi = 0;
+    if (kdcphi_on) kdphi = (T)p.lsc_kdc * fabs(res_phi) / sqrt(GG);
+    const T mupk = mu + kdc;
+    const T dmdi = dmd * ira;
+    const T wf = fluid ? w : (T)0;   // solid elements contribute nothing
+    T rec[L::GPW];
+#pragma unroll
+    for (int a = 0; a < 8; ++a)
+#pragma unroll
+      for (int d = 0; d < 3; ++d) rec[3 * a + d] = g[a][d];
+    rec[24] = wf;
+    rec[25] = fluid ? fact2 * mupk * w : (T)0;
+    rec[26] = fluid ? fact2 * (tauC + lambda) * w : (T)0;
+    rec[27] = fluid ? fact2 * w * tauM : (T)0;
+    rec[28] = fluid ? fact2 * w * kdphi : (T)0;
+    rec[29] = dphi[0]; rec[30] = dphi[1]; rec[31] = dphi[2];
+    rec[32] = uadv[0]; rec[33] = uadv[1]; rec[34] = uadv[2];
+    rec[35] = rho; rec[36] = rho * tauM; rec[37] = tauLS;
+    rec[38] = vdot + phii * ira * dmd - dmd / rhoa;
+    rec[39] = fact2 * wf * tauC * dmdi * dmdi;
+    rec[40] = fact2 * tauC * dmdi * wf;
+    rec[41] = fact2 * dmdi * wf;
+    rec[42] = 0; rec[43] = 0;
+    store_n(out + gp * L::GPW, rec, L::GPW);
+    if (!fluid) continue;
+    T svis[8], gdphi[8], c[8];
+#pragma unroll
+    for (int n = 0; n < 8; ++n) {
+      T sv = 0;
+#pragma unroll
+      for (int k = 0; k < 3; ++k)
+        sv += g[n][0] * (du[0][k] + du[k][0]) + g[n][1] * (du[1][k] + du[k][1]) + g[n][2] * (du[2][k] + du[k][2]);
+      svis[n] = sv;
+      gdphi[n] = g[n][0] * dphi[0] + g[n][1] * dphi[1] + g[n][2] * dphi[2];
+      c[n] = uadv[0] * g[n][0] + uadv[1] * g[n][1] + uadv[2] * g[n][2];
+    }
+    const T tdiv = -pri + tauC * divu;
+#pragma unroll
+    for (int n = 0; n < 8; ++n) {
+#pragma unroll
+      for (int i = 0; i < 3; ++i)
+        ru[n][i] += w * (-N[n] * tmp1[i] - g[n][i] * tdiv + g[n][i] * tauC * vdot - g[n][i] * lambda * divu -
+                         mupk * svis[n] + rho * c[n] * (-tauM * rL[i]));
+      rp[n] += w * (-N[n] * (divu - vdot) + (g[n][0] * rL[0] + g[n][1] * rL[1] + g[n][2] * rL[2]) * (-tauM));
+      rf[n] += w * (-(N[n] + tauLS * c[n]) * res_phi - kdphi * gdphi[n] + N[n] * dmdi * tauC * (divu - vdot));
+    }
+  }
+#pragma unroll
+  for (int n = 0; n < 8; ++n) {
+    T* orh = out + L::RHS0 + 5 * n;
+    orh[0] = ru[n][0]; orh[1] = ru[n][1]; orh[2] = ru[n][2]; orh[3] = rp[n]; orh[4] = rf[n];
+  }
+}
+
+// element pass, temperature on a hex (src/solveQuenching.f90:712-856);
+// record layout of this pass: xd(0:2) u(3:5) um(6:8) phi(9) T(10) rT(11)
+template <typename T>
+__device__ void hex_summarize_tem(const ovs_params& p, const T r[8][16], const T lo[8][4], bool fluid, T* out,
+                                  double& cfl, int& nbad) {
+  using W = typename Wide<T>::type;
+  using L = HexLay<OVS_ASM_TEM>;
+  const T fact2 = (T)(p.alfi * p.gami * p.delt);
+  const T ts = (T)p.ts, cpw = (T)p.cpw, cpa = (T)p.cpa, lh = (T)p.lh;
+  const bool kdc_on = fabs(p.tem_kdc) > 0.0;
+  T rt[8];
+#pragma unroll
+  for (int n = 0; n < 8; ++n) rt[n] = 0;
+  for (int gp = 0; gp < 8; ++gp) {
+    T g[8][3], G[3][3];
+    const T detj = hex_geometry<T>(gp, r, lo, g, G);
+    if (!(detj > (T)0)) nbad = 1;
+    const T w = detj;
+    T GG = 0;
+#pragma unroll
+    for (int j = 0; j < 3; ++j)
+#pragma unroll
+      for (int i = 0; i < 3; ++i) GG += G[i][j] * G[i][j];
+    T N[8];
+#pragma unroll
+    for (int a = 0; a < 8; ++a) N[a] = hex_N<T>(gp, a);
+    T dT[3] = {0, 0, 0}, ui[3] = {0, 0, 0}, umi[3] = {0, 0, 0};
+    T Ti = 0, rTi = 0;
+#pragma unroll
+    for (int a = 0; a < 8; ++a) {
+#pragma unroll
+      for (int j = 0; j < 3; ++j) {
+        dT[j] += r[a][10] * g[a][j];
+        ui[j] += r[a][3 + j] * N[a];
+        umi[j] += r[a][6 + j] * N[a];
+      }
+      Ti += r[a][10] * N[a];
+      rTi += r[a][11] * N[a];
+    }
+    T gdT[8];
+#pragma unroll
+    for (int n = 0; n < 8; ++n) gdT[n] = g[n][0] * dT[0] + g[n][1] * dT[1] + g[n][2] * dT[2];
+    const W phid = hex_phi<T>(r, lo, 9, gp);
+    const W phicd = clamp01(phid);
+    const T phic = (T)phicd;
+    T mdot, dmdT;
+    if (Ti > ts) {
+      mdot = (T)p.c_evap * (T)(1.0 - phicd) * (T)p.rhow * (Ti - ts) / ts;
+      dmdT = (T)p.c_evap * (T)(1.0 - phicd) * (T)p.rhow / ts * (T)p.c_dmdot;
+    } else {
+      mdot = (T)p.c_cond * phic * (T)p.rhoa * (Ti - ts) / ts;
+      dmdT = (T)p.c_cond * phic * (T)p.rhoa / ts * (T)p.c_dmdot;
+    }
+    T rho, cp, hk, rcp;
+    if (fluid) {
+      rho = (T)(p.rhow * (1.0 - phicd) + p.rhoa * phicd);
+      cp = (T)(p.cpw * (1.0 - phicd) + p.cpa * phicd);
+      hk = (T)(p.kappaw * (1.0 - phicd) + p.kappaa * phicd);
+      rcp = (T)((p.rhow * p.cpw) * (1.0 - phicd) + (p.rhoa * p.cpa) * phicd);
+    } else {
+      rho = (T)p.rhos; cp = (T)p.cps; hk = (T)p.kappas; rcp = (T)(p.rhos * p.cps);
+    }
+    const T uadv[3] = {ui[0] - umi[0], ui[1] - umi[1], ui[2] - umi[2]};
+    const T Se = ((cpw - cpa) * (Ti - ts) - lh) * mdot;
+    const T udT = uadv[0] * dT[0] + uadv[1] * dT[1] + uadv[2] * dT[2];
+    const T res = rcp * (rTi + udT) - Se;
+    const T taua = quad_uGu<T>(uadv, G);
+    T tt = taua + (T)(4.0 / (p.delt * p.delt));
+    const T kk = hk / (rho * cp);
+    tt = tt + kk * kk * (T)12.0 * GG;
+    const T tauT = (T)1.0 / (rho * cp * sqrt(tt));
+    {
+      const double cf = (double)p.delt * sqrt((double)taua);
+      if (cf > cfl) cfl = cf;
+    }
+    T kdcT = 0;
+    if (kdc_on && fluid) kdcT = (T)p.tem_kdc * fabs(res) / sqrt(GG) / (T)p.tref;
+    const T dSe = (cpw - cpa) * mdot + ((cpw - cpa) * (Ti - ts) - lh) * dmdT;
+    T rec[L::GPW];
+#pragma unroll
+    for (int a = 0; a < 8; ++a)
+#pragma unroll
+      for (int d = 0; d < 3; ++d) rec[3 * a + d] = g[a][d];
+    rec[24] = w;
+    rec[29] = rcp;
+    if (fluid) {
+      rec[25] = fact2 * (hk + kdcT) * w;
+      rec[26] = uadv[0]; rec[27] = uadv[1]; rec[28] = uadv[2];
+      rec[30] = dSe; rec[31] = tauT * rcp;
+#pragma unroll
+      for (int n = 0; n < 8; ++n) {
+        const T cn = uadv[0] * g[n][0] + uadv[1] * g[n][1] + uadv[2] * g[n][2];
+        rt[n] += w * (-N[n] * rcp * (rTi + udT) + N[n] * Se - rcp * tauT * cn * res - (hk + kdcT) * gdT[n]);
+      }
+    } else {
+      rec[25] = fact2 * hk * w;
+      rec[26] = rec[27] = rec[28] = 0; rec[30] = 0; rec[31] = 0;
+#pragma unroll
+      for (int n = 0; n < 8; ++n) rt[n] += w * (-N[n] * rcp * rTi - hk * gdT[n]);
+    }
+    store_n(out + gp * L::GPW, rec, L::GPW);
+  }
+#pragma unroll
+  for (int n = 0; n < 8; ++n) out[L::RHS0 + n] = rt[n];
+}
+
+template <typename T, int KIND>
+__global__ void __launch_bounds__(64) hex_element_kernel(const SumArgs a) {
+  using L = HexLay<KIND>;
+  const int e = blockIdx.x * blockDim.x + threadIdx.x;
+  double cfl = 0.0;
+  int nbad = 0;
+  if (e < a.E) {
+    T r[8][16], lo[8][4];
+    const T* rec = reinterpret_cast<const T*>(a.rec);
+#pragma unroll
+    for (int n = 0; n < 8; ++n) load_rec(rec, a.ien[8 * (size_t)e + n], r[n], lo[n]);
+    const bool fluid = __ldg(a.elm_id + e) == a.p.fluid_elm_id;
+    T* out = reinterpret_cast<T*>(a.sum) + (size_t)e * L::SW;
+    if constexpr (KIND == OVS_ASM_NSVOF) hex_summarize_nsvof<T>(a.p, r, lo, fluid, out, cfl, nbad);
+    else hex_summarize_tem<T>(a.p, r, lo, fluid, out, cfl, nbad);
+  }
+#pragma unroll
+  for (int off = 16; off > 0; off >>= 1) {
+    cfl = fmax(cfl, __shfl_xor_sync(0xffffffffu, cfl, off));
+    nbad += __shfl_xor_sync(0xffffffffu, nbad, off);
+  }
+  if ((threadIdx.x & 31) == 0) {
+    cfl_max(a.cfl_bits, cfl);
+    if (nbad) atomicAdd(a.flags, nbad);
+  }
+}
+
+// Block (row node la, column node b) of a hex from its records: the
+// per-point forms of the tet block sums (see expand_block), summed over the
+// 8 points.
+template <typename T, int KIND>
+__device__ __forceinline__ void hex_expand_block(const ovs_params& p, const T* sm, int la, int b, T* o, T* rv) {
+  using L = HexLay<KIND>;
+  if constexpr (KIND == OVS_ASM_TEM) {
+    const T fact1 = (T)p.almi, fact2 = (T)(p.alfi * p.gami * p.delt);
+    T X = 0;
+    for (int gp = 0; gp < 8; ++gp) {
+      const T* q = sm + gp * L::GPW;
+      const T ga[3] = {q[3 * la], q[3 * la + 1], q[3 * la + 2]};
+      const T gb[3] = {q[3 * b], q[3 * b + 1], q[3 * b + 2]};
+      const T w = q[24], HK = q[25], rcp = q[29], dSe = q[30], trc = q[31];
+      const T uadv[3] = {q[26], q[27], q[28]};
+      const T Na = hex_N<T>(gp, la), Nb = hex_N<T>(gp, b);
+      const T ca = ga[0] * uadv[0] + ga[1] * uadv[1] + ga[2] * uadv[2];
+      const T cb = gb[0] * uadv[0] + gb[1] * uadv[1] + gb[2] * uadv[2];
+      const T aw = w * (Na + trc * ca);
+      X += aw * (rcp * (fact1 * Nb + fact2 * cb) - fact2 * dSe * Nb) + HK * (ga[0] * gb[0] + ga[1] * gb[1] + ga[2] * gb[2]);
+    }
+    o[0] = X;
+    rv[0] = sm[L::RHS0 + la];
+  } else {
+    const T fact1 = (T)p.almi, fact2 = (T)(p.alfi * p.delt * p.gami);
+#pragma unroll
+    for (int v = 0; v < 24; ++v) o[v] = 0;
+    for (int gp = 0; gp < 8; ++gp) {
+      const T* q = sm + gp * L::GPW;
+      const T ga[3] = {q[3 * la], q[3 * la + 1], q[3 * la + 2]};
+      const T gb[3] = {q[3 * b], q[3 * b + 1], q[3 * b + 2]};
+      T s[20];
+#pragma unroll
+      for (int k = 0; k < 20; k += 4) ldv4(q + 24 + k, s + k);
+      const T w = s[0], KA = s[1], KB = s[2], MM = s[3], KDP = s[4];
+      const T dphi[3] = {s[5], s[6], s[7]}, uadv[3] = {s[8], s[9], s[10]};
+      const T rho = s[11], rt = s[12], tls = s[13], src = s[14], eps = s[15], ufac = s[16], plfac = s[17];
+      const T Na = hex_N<T>(gp, la), Nb = hex_N<T>(gp, b);
+      const T ca = uadv[0] * ga[0] + uadv[1] * ga[1] + uadv[2] * ga[2];
+      const T cb = uadv[0] * gb[0] + uadv[1] * gb[1] + uadv[2] * gb[2];
+      const T gab = ga[0] * gb[0] + ga[1] * gb[1] + ga[2] * gb[2];
+      const T beta = fact1 * Nb + fact2 * cb;
+      const T S = w * rho * (Na + rt * ca) * beta;
+      const T P = fact2 * w * Nb, Q = fact2 * w * rt * ca, R = fact2 * w * Na, Tt = w * rt * beta;
+#pragma unroll
+      for (int i = 0; i < 3; ++i) {
+#pragma unroll
+        for (int j = 0; j < 3; ++j) o[4 * i + j] += KA * ga[j] * gb[i] + KB * ga[i] * gb[j] + (i == j ? KA * gab + S : (T)0);
+        o[4 * i + 3] += -ga[i] * P + gb[i] * Q;
+      }
+#pragma unroll
+      for (int d = 0; d < 3; ++d) o[12 + d] += gb[d] * R + ga[d] * Tt;
+      o[15] += MM * gab;
+      const T gam = w * (Na + tls * ca);
+#pragma unroll
+      for (int d = 0; d < 3; ++d) o[16 + d] += dphi[d] * (fact2 * gam * Nb) - gb[d] * (ufac * Na);
+      o[19] += gam * (beta + fact2 * Nb * src) + KDP * gab + eps * Na * Nb;
+#pragma unroll
+      for (int d = 0; d < 3; ++d) o[20 + d] += ga[d] * (ufac * Nb);
+      o[23] += -plfac * Na * Nb;
+    }
+#pragma unroll
+    for (int f = 0; f < 5; ++f) rv[f] = sm[L::RHS0 + 5 * la + f];
+  }
+}
+
+// shared memory per warp: blocks [4 elements][8 columns][BSTR], RHS rows
+// [4][RSTR], row accumulator [max_deg][NVP]; ints: slots [4][8], columns
+template <typename T, int KIND> struct HexSmem {
+  static constexpr int NV = HexLay<KIND>::NV, NF = HexLay<KIND>::NF;
+  static constexpr int CH = 4;
+  static constexpr int NVP = (NV < 4) ? 1 : NV;
+  static constexpr int BSTR = (NV < 4) ? 1 : NV + 16 / (int)sizeof(T);
+  static constexpr int RSTR = NF + 1;
+  __host__ __device__ static size_t bytes(int max_deg) {
+    size_t b = sizeof(T) * ((size_t)8 * CH * BSTR + (size_t)CH * RSTR + (size_t)max_deg * NVP);
+    b = (b + 15) & ~(size_t)15;
+    b += sizeof(int) * ((size_t)8 * CH + max_deg);
+    return (b + 15) & ~(size_t)15;
+  }
+};
+
+template <typename T, int KIND>
+__global__ void __launch_bounds__(128) hex_rows_kernel(const AsmArgs a) {
+  using S = HexSmem<T, KIND>;
+  using L = HexLay<KIND>;
+  constexpr int NV = S::NV, NF = S::NF, NVP = S::NVP, BSTR = S::BSTR, RSTR = S::RSTR, CH = S::CH;
+  constexpr int WARPS = 4;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  __shared__ unsigned masks[24];
+  if (threadIdx.x < 24) masks[threadIdx.x] = (KIND == OVS_ASM_TEM) ? (TB | (TB << 8) | (TB << 16)) : mask_of(threadIdx.x);
+  __syncthreads();
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+  unsigned char* base = smem_raw + (size_t)wid * S::bytes(a.max_deg);
+  T* blk = reinterpret_cast<T*>(base);                 // [CH][8][BSTR]
+  T* rvs = blk + 8 * CH * BSTR;                        // [CH][RSTR]
+  T* acc = rvs + CH * RSTR;                            // [max_deg][NVP]
+  size_t off = sizeof(T) * ((size_t)8 * CH * BSTR + (size_t)CH * RSTR + (size_t)a.max_deg * NVP);
+  off = (off + 15) & ~(size_t)15;
+  int* slot = reinterpret_cast<int*>(base + off);      // [CH][8]
+  int* cols = slot + 8 * CH;                           // [max_deg]
+  const T* sum = reinterpret_cast<const T*>(a.rec);
+  const uint2* n2s8 = reinterpret_cast<const uint2*>(a.n2s);
+  const int jl = lane >> 3, bl = lane & 7;
+  for (int A = blockIdx.x * WARPS + wid; A < a.N; A += gridDim.x * WARPS) {
+    const int rp = a.rowptr[A], deg = a.rowptr[A + 1] - rp;
+    const int ep = a.n2e_ptr[A], ne = a.n2e_ptr[A + 1] - ep;
+    for (int s = lane; s < deg; s += 32) cols[s] = a.colidx[rp + s];
+    for (int q = lane; q < deg * NVP; q += 32) acc[q] = (T)0;
+    T racc = (T)0;
+    __syncwarp();
+    for (int c0 = 0; c0 < ne; c0 += CH) {
+      const int nc = min(CH, ne - c0);
+      if (jl < nc) {
+        const int packed = __ldg(a.n2e + ep + c0 + jl);
+        const uint2 sl = __ldg(n2s8 + ep + c0 + jl);
+        const int e = packed >> 3, la = packed & 7;
+        T o[NVP], rv[NF];
+        hex_expand_block<T, KIND>(a.p, sum + (size_t)e * L::SW, la, bl, o, rv);
+        T* dst = blk + (jl * 8 + bl) * BSTR;
+        if constexpr (NV >= 4) {
+#pragma unroll
+          for (int v = 0; v < NV; v += 4) store_row<4>(dst + v, o + v);
+        } else {
+          dst[0] = o[0];
+        }
+        const unsigned word = bl < 4 ? sl.x : sl.y;
+        slot[jl * 8 + bl] = (int)((word >> (8 * (bl & 3))) & 0xffu);
+        if (bl == 0) {
+#pragma unroll
+          for (int f = 0; f < NF; ++f) rvs[jl * RSTR + f] = rv[f];
+        }
+      }
+      __syncwarp();
+      // ordered reduction: the 8 blocks of one element go to distinct slots
+      if constexpr (NV >= 4) {
+        constexpr int NG = NV / 4;
+        for (int j = 0; j < nc; ++j) {
+          for (int q = lane; q < 8 * NG; q += 32) {
+            const int b = q / NG, gidx = q - b * NG;
+            Vec4<T>::add(acc + slot[j * 8 + b] * NVP + gidx * 4, blk + (j * 8 + b) * BSTR + gidx * 4);
+          }
+          __syncwarp();
+        }
+      } else {
+        for (int j = 0; j < nc; ++j) {
+          if (lane < 8) acc[slot[j * 8 + lane]] += blk[j * 8 + lane];
+          __syncwarp();
+        }
+      }
+      if (lane < NF)
+        for (int j = 0; j < nc; ++j) racc += rvs[j * RSTR + lane];
+      __syncwarp();
+    }
+    // row write with the Dirichlet treatment (as for the tets)
+    const unsigned ibA = a.ibc[A];
+    if (a.mat) {
+      T* outp = reinterpret_cast<T*>(a.vals) + (size_t)rp * NV;
+      const T cnt = (T)ne;
+      if constexpr (NV >= 4) {
+        constexpr int NG = NV / 4;
+        for (int q = lane; q < deg * NG; q += 32) {
+          const int s = q / NG, gidx = q - s * NG;
+          const int B = cols[s];
+          const unsigned ibB = __ldg(a.ibc + B);
+          const bool dg = B == A;
+          T v4[4];
+#pragma unroll
+          for (int t = 0; t < 4; ++t) {
+            const unsigned m = masks[4 * gidx + t];
+            T val = acc[s * NVP + 4 * gidx + t];
+            if ((ibA & m & 0xffu) || ((ibB << 8) & m & 0xff00u)) val = (T)0;
+            if (dg && ((ibA << 16) & m & 0xff0000u)) val = cnt;
+            v4[t] = val;
+          }
+          store_row<4>(outp + (size_t)s * NV + 4 * gidx, v4);
+        }
+      } else {
+        for (int q = lane; q < deg; q += 32) {
+          const int B = cols[q];
+          const unsigned ibB = __ldg(a.ibc + B);
+          T val = acc[q];
+          if ((ibA & TB) || (ibB & TB)) val = (T)0;
+          if (B == A && (ibA & TB)) val = cnt;
+          outp[q] = val;
+        }
+      }
+    }
+    if (a.vec && lane < NF) {
+      unsigned bit;
+      if (KIND == OVS_ASM_TEM) bit = TB;
+      else bit = (lane < 3) ? (1u << lane) : (lane == 3 ? PB : FB);
+      T v = (ibA & bit) ? (T)0 : racc;
+      if (!isfinite((double)v)) atomicOr(a.flags + 1, 1);
+      reinterpret_cast<T*>(a.rhs)[(size_t)lane * a.N + A] = v;
+    }
+    __syncwarp();
+  }
+}
+
+template <typename T, int KIND>
+int launch_assemble_hex(ovs_ctx* c, const AsmArgs& a, const SumArgs& sa, int parts) {
+  if (parts & 1) {
+    hex_element_kernel<T, KIND><<<(sa.E + 63) / 64, 64, 0, c->stream>>>(sa);
+    ++c->launches;
+    OVS_CUDA_TRY(cudaGetLastError());
+  }
+  if (!(parts & 2)) return OVS_OK;
+  using S = HexSmem<T, KIND>;
+  const size_t smem = S::bytes(a.max_deg) * 4;
+  auto kern = hex_rows_kernel<T, KIND>;
+  OVS_CUDA_TRY(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  int per_sm = 0;
+  OVS_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, 128, smem));
+  if (per_sm < 1) return OVS_ERR_ARG;
+  long need = ((long)c->N + 3) / 4;
+  long grid = (long)per_sm * c->num_sms * 4;
+  if (grid > need) grid = need;
+  if (grid < 1) grid = 1;
+  kern<<<(int)grid, 128, smem, c->stream>>>(a);
+  ++c->launches;
+  OVS_CUDA_TRY(cudaGetLastError());
+  return OVS_OK;
+}

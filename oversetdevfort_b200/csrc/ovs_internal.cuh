@@ -82,7 +82,8 @@ struct ovs_ctx {
   double* vjp_cot = nullptr; // residual VJP work: cotangent, element terms, nodal result
   double* vjp_ge = nullptr;
   double* vjp_grad = nullptr;
-  unsigned* n2s = nullptr;   // nshl*E: slots of the element's 4 nodes in the row, one byte each (tets)
+  unsigned* n2s = nullptr;   // nshl*E entries: slots of the element's nodes in the row, one byte each
+                             // (one word per entry for tets, two for hexahedra)
   int nnz = 0;
   int max_deg = 0, max_elem = 0;
   // nodal state (FP64, reference layout)

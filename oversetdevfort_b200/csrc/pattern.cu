@@ -188,6 +188,29 @@ __global__ void slot_map_kernel(const int* __restrict__ ien, int N, const int* _
   }
 }
 
+// The same for hexahedra: 8 slots, bytes 0-3 in the first word and 4-7 in
+// the second.
+__global__ void slot_map8_kernel(const int* __restrict__ ien, int N, const int* __restrict__ n2e_ptr,
+                                 const int* __restrict__ n2e, const int* __restrict__ rowptr,
+                                 const int* __restrict__ colidx, uint2* __restrict__ n2s) {
+  const int A = blockIdx.x * blockDim.x + threadIdx.x;
+  if (A >= N) return;
+  const int rp = rowptr[A], deg = rowptr[A + 1] - rp;
+  for (int k = n2e_ptr[A]; k < n2e_ptr[A + 1]; ++k) {
+    const int* nodes = ien + 8 * (size_t)(n2e[k] >> 3);
+    unsigned w[2] = {0u, 0u};
+    for (int b = 0; b < 8; ++b) {
+      int lo = 0, hi = deg;
+      while (hi - lo > 1) {
+        const int mid = (lo + hi) >> 1;
+        if (colidx[rp + mid] > nodes[b]) hi = mid; else lo = mid;
+      }
+      w[b >> 2] |= (unsigned)lo << (8 * (b & 3));
+    }
+    n2s[k] = make_uint2(w[0], w[1]);
+  }
+}
+
 __global__ void to_one_based_kernel(const int* __restrict__ in, int* __restrict__ out, size_t n) {
   size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x;
   if (i < n) out[i] = in[i] + 1;
@@ -252,6 +275,11 @@ int ovs_pattern_build(ovs_ctx* c) {
   if ((st = ovs_ensure((void**)&c->colidx, sizeof(int) * (size_t)(nnz > 0 ? nnz : 1)))) return st;
   row_fill_kernel<<<ovs_grid(N, 128, 1 << 30), 128, 0, s>>>(c->ien, nshl, N, c->n2e_ptr, c->n2e,
                                                             c->rowptr, c->colidx, c->diag);
+  if (nshl == 8) {
+    if ((st = ovs_ensure((void**)&c->n2s, 2 * sizeof(unsigned) * (size_t)(EN > 0 ? EN : 1)))) return st;
+    slot_map8_kernel<<<ovs_grid(N, 128, 1 << 30), 128, 0, s>>>(c->ien, N, c->n2e_ptr, c->n2e, c->rowptr,
+                                                               c->colidx, reinterpret_cast<uint2*>(c->n2s));
+  }
   if (nshl == 4) {
     if ((st = ovs_ensure((void**)&c->n2s, sizeof(unsigned) * (size_t)(EN > 0 ? EN : 1)))) return st;
     slot_map_kernel<<<ovs_grid(N, 128, 1 << 30), 128, 0, s>>>(c->ien, N, c->n2e_ptr, c->n2e, c->rowptr,

@@ -234,6 +234,14 @@ def config3(n: int = 128) -> Case:
     return quench_case(box_tet(n, n, n), f"config3_quench_{n}cube")
 
 
+def config4(n: int = 96) -> Case:
+    """Hex path: the quench physics on n^3 trilinear hexahedra (n = 96:
+    884,736 elements, 912,673 nodes), 2x2x2 Gauss points, GMRES restart 100."""
+    c = quench_case(box_hex(n, n, n), f"config4_hex_{n}cube")
+    c.kspace = 100
+    return c
+
+
 def config5(n: int = 32) -> Case:
     return quench_case(box_tet(n, n, n), f"config5_quench_{n}cube")
 
@@ -299,12 +307,13 @@ def bottom_heat_flux_weights(case: Case, phi: np.ndarray | None = None) -> np.nd
 
 
 def random_case(nx=4, ny=3, nz=3, seed=0, kernel=F.OVS_ASM_NSVOF, solid_frac=0.15,
-                bc_frac=0.2, phase_change=True) -> Case:
+                bc_frac=0.2, phase_change=True, hex=False) -> Case:
     """Small case with every code path switched on: random state fields,
     mesh motion, mixed fluid/solid elements, random Dirichlet flags in all
-    six IBC columns, phase change and discontinuity capturing."""
+    six IBC columns, phase change and discontinuity capturing (tets, or
+    trilinear hexahedra with hex=True)."""
     rng = np.random.default_rng(seed)
-    m = box_tet(nx, ny, nz, 1.0, 0.8, 0.9)
+    m = box_hex(nx, ny, nz, 1.0, 0.8, 0.9) if hex else box_tet(nx, ny, nz, 1.0, 0.8, 0.9)
     N, E = m.nnode, m.nelem
     h = min(1.0 / nx, 0.8 / ny, 0.9 / nz)
     p = base_params(delt=rng.uniform(5e-4, 2e-3), c_evap=0.3 if phase_change else 0.0,
@@ -338,4 +347,5 @@ def random_case(nx=4, ny=3, nz=3, seed=0, kernel=F.OVS_ASM_NSVOF, solid_frac=0.1
     m.elm_id[rng.random(E) < 0.1] = 103
     ibc = (rng.random((N, 8)) < bc_frac).astype(np.int32)
     ibc = np.asfortranarray(ibc)
-    return Case(f"random_{nx}x{ny}x{nz}_s{seed}", m, p, st, ibc, kernel, kspace=30, gmres_tol=1e-8)
+    return Case(f"random_{'hex' if hex else 'tet'}_{nx}x{ny}x{nz}_s{seed}", m, p, st, ibc, kernel, kspace=30,
+                gmres_tol=1e-8)
