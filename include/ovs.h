@@ -234,6 +234,35 @@ int ovs_newton_update(ovs_ctx* ctx, int system);
  * of RHSGu, RHSGp, RHSGls, RHSGtem of the given precision. */
 int ovs_residual_norms(ovs_ctx* ctx, int precision, double r[4]);
 
+/* The Newton loop of one quench time step, on the device:
+ * solmultiphasethermofluid_stag (src/solveFlow.f90:4-164).  residual0 from a
+ * vector assembly of all fields; then up to newton_max times: assemble the
+ * NS+VOF system, solve, Newton update (acg, ug, pg, rphig, phig); if
+ * solve_tem, the same for the temperature (rTg, Tg); assemble the vectors
+ * of all fields and stop when every field passes check_convergence (:190-215:
+ * residual < utol * residual0 or residual < atol, sums of squares as
+ * calculate_residual).  mode OVS_FP64: FP64 assembly and the reference GMRES
+ * cycle (tol, kspace, kspace_min, zero start); OVS_FP32: FP32 assembly and
+ * the mixed-precision refined solve to relative residual tol (max_cycles).
+ * The predictor of driver.f90:83-85 and the BC producers stay with the
+ * caller (set the fields and IBC before the call).  Only the 4 residual
+ * norms per iteration travel to the host. */
+typedef struct ovs_newton_opts {
+  int mode, newton_max, solve_tem;
+  int kspace, kspace_min, max_cycles;
+  double tol_ns, tol_tem;
+  double utol[4];    /* NS_NL_UTOL, NS_NL_PTOL, LSC_NL_TOL, TEM_NL_TOL */
+  double atol[4];    /* NS_GMRES_atol (u, p), LSC_GMRES_atol, TEM_GMRES_atol */
+} ovs_newton_opts;
+typedef struct ovs_newton_info {
+  int iterations, converged;
+  int field_converged[4];
+  double residual0[4], residual[4];
+  int krylov_iterations_ns, krylov_iterations_tem;
+  double seconds;    /* wall time of the call */
+} ovs_newton_info;
+int ovs_quench_newton(ovs_ctx* ctx, const ovs_newton_opts* opts, ovs_newton_info* info);
+
 /* ----------------------------------------------------------- measurement
  * Hooks for benchmarking; they have no counterpart in the reference. */
 enum { OVS_PROF_SPMV = 1, OVS_PROF_ASSEMBLE = 2, OVS_PROF_ARNOLDI = 3, OVS_PROF_ARNOLDI_FUSED = 4,

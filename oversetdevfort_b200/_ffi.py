@@ -50,7 +50,7 @@ EXPORTS = [
     "ovs_get_field", "ovs_assemble", "ovs_get_rhs", "ovs_set_rhs", "ovs_get_lhs_block",
     "ovs_set_lhs_block", "ovs_spmv", "ovs_gmres", "ovs_solve", "ovs_newton_update",
     "ovs_residual_norms", "ovs_profile", "ovs_launch_count", "ovs_last_device_ms",
-    "ovs_host_alloc", "ovs_host_free", "ovs_residual_vjp", "ovs_gmres_transposed",
+    "ovs_host_alloc", "ovs_host_free", "ovs_residual_vjp", "ovs_gmres_transposed", "ovs_quench_newton",
     "ovs_gmres_tem_noalloc",
 ]
 
@@ -68,6 +68,18 @@ class OvsParams(C.Structure):
     _fields_ = ([(n, C.c_double) for n in PARAM_DOUBLES] +
                 [("gravvec", C.c_double * 3), ("fluid_elm_id", C.c_int),
                  ("subdomain_flag", C.c_int), ("elm_id_set", C.c_int * 2)])
+
+
+class OvsNewtonOpts(C.Structure):
+    _fields_ = [("mode", C.c_int), ("newton_max", C.c_int), ("solve_tem", C.c_int), ("kspace", C.c_int),
+                ("kspace_min", C.c_int), ("max_cycles", C.c_int), ("tol_ns", C.c_double),
+                ("tol_tem", C.c_double), ("utol", C.c_double * 4), ("atol", C.c_double * 4)]
+
+
+class OvsNewtonInfo(C.Structure):
+    _fields_ = [("iterations", C.c_int), ("converged", C.c_int), ("field_converged", C.c_int * 4),
+                ("residual0", C.c_double * 4), ("residual", C.c_double * 4),
+                ("krylov_iterations_ns", C.c_int), ("krylov_iterations_tem", C.c_int), ("seconds", C.c_double)]
 
 
 class OvsGmresInfo(C.Structure):
@@ -126,6 +138,7 @@ def load(path: str | os.PathLike | None = None) -> C.CDLL:
         "ovs_host_alloc": ([C.POINTER(vp), C.c_size_t], C.c_int),
         "ovs_host_free": ([vp], C.c_int),
         "ovs_residual_vjp": ([vp, C.c_int, dp, dp], C.c_int),
+        "ovs_quench_newton": ([vp, C.POINTER(OvsNewtonOpts), C.POINTER(OvsNewtonInfo)], C.c_int),
         "ovs_gmres_transposed": ([vp, C.c_int, dp, C.c_double, C.c_int, C.c_int, dp, C.POINTER(OvsGmresInfo)],
                                  C.c_int),
         "ovs_gmres_tem_noalloc": ([C.c_int, vp, vp, vp, vp, vp, C.c_double, C.c_int, C.c_int, vp,

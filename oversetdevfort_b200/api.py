@@ -231,6 +231,17 @@ class Context:
                                               C.byref(info)), "ovs_gmres_transposed")
         return x, info
 
+    def quench_newton(self, mode: int = F.OVS_FP64, newton_max: int = 3, solve_tem: bool = True,
+                      kspace: int = 50, kspace_min: int = 1, max_cycles: int = 100, tol_ns: float = 1e-6,
+                      tol_tem: float = 1e-6, utol=(1e-3, 1e-3, 1e-3, 1e-3), atol=(1e-15, 1e-15, 1e-15, 1e-15)):
+        """The Newton loop of one quench time step on the device
+        (solmultiphasethermofluid_stag): returns the OvsNewtonInfo."""
+        o = F.OvsNewtonOpts(mode, newton_max, int(solve_tem), kspace, kspace_min, max_cycles, tol_ns, tol_tem,
+                            (C.c_double * 4)(*utol), (C.c_double * 4)(*atol))
+        info = F.OvsNewtonInfo()
+        F.check(self.lib.ovs_quench_newton(self.h, C.byref(o), C.byref(info)), "ovs_quench_newton")
+        return info
+
     def newton_update(self, system: int):
         F.check(self.lib.ovs_newton_update(self.h, system), "ovs_newton_update")
 

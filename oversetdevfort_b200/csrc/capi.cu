@@ -1,5 +1,6 @@
 // C ABI of the library (include/ovs.h): context, mesh/state transfer,
 // reference-layout conversions, Newton update and residual norms.
+#include <chrono>
 #include <cstdlib>
 #include "ovs_internal.cuh"
 
@@ -706,6 +707,72 @@ int ovs_gmres_transposed(ovs_ctx* c, int sys, const double* rhs, double tol, int
   OVS_CUDA_TRY(cudaMemcpyAsync(sol, c->sol[sys], sizeof(double) * n, cudaMemcpyDeviceToHost, c->stream));
   OVS_CUDA_TRY(cudaStreamSynchronize(c->stream));
   if (info) *info = gi;
+  return OVS_OK;
+}
+
+
+// solmultiphasethermofluid_stag (src/solveFlow.f90:4-164) on the context
+int ovs_quench_newton(ovs_ctx* c, const ovs_newton_opts* o, ovs_newton_info* info) {
+  if (!c || !o || (o->mode != OVS_FP64 && o->mode != OVS_FP32) || o->newton_max < 0) return OVS_ERR_ARG;
+  if (o->kspace < 1 || o->kspace > OVS_MAX_KSPACE || o->max_cycles < 1) return OVS_ERR_ARG;
+  int st;
+  if ((st = ovs_activate(c))) return st;
+  const auto t0 = std::chrono::steady_clock::now();
+  const int prec = o->mode;
+  ovs_newton_info ni;
+  memset(&ni, 0, sizeof(ni));
+  auto check = [&](const double* r) {   // check_convergence, all three field groups
+    int all = 1;
+    for (int k = 0; k < 4; ++k) {
+      ni.field_converged[k] = (r[k] < o->utol[k] * ni.residual0[k]) || (r[k] < o->atol[k]);
+      all &= ni.field_converged[k];
+    }
+    return all;
+  };
+  auto solve = [&](int sys, double tol, int* its) -> int {
+    const size_t n = (size_t)c->N * ovs_sys_nf(sys);
+    int s2;
+    if (prec == OVS_FP64) {
+      if ((s2 = ovs_ensure((void**)&c->sol[sys], sizeof(double) * 5 * (size_t)c->N))) return s2;
+      OVS_CUDA_TRY(cudaMemsetAsync(c->sol[sys], 0, sizeof(double) * n, c->stream));
+      ovs_gmres_info gi;
+      memset(&gi, 0, sizeof(gi));
+      if ((s2 = ovs_gmres_ref_impl(c, sys, tol, o->kspace, o->kspace_min, c->sol[sys], &gi))) return s2;
+      *its += gi.iterations;
+    } else {
+      ovs_solve_info si;
+      memset(&si, 0, sizeof(si));
+      if ((s2 = ovs_solve_impl(c, sys, OVS_FP32, tol, o->kspace, o->max_cycles, &si))) return s2;
+      *its += si.iterations;
+    }
+    return ovs_newton_update(c, sys);
+  };
+  const int vec = OVS_TENSOR_VEC, both = OVS_TENSOR_MAT | OVS_TENSOR_VEC;
+  auto vec_all = [&]() -> int {
+    int s2;
+    if ((s2 = ovs_assemble_impl(c, OVS_ASM_NSVOF, vec, prec, nullptr)) < 0) return s2;
+    if ((s2 = ovs_assemble_impl(c, OVS_ASM_TEM, vec, prec, nullptr)) < 0) return s2;
+    return OVS_OK;
+  };
+  if ((st = vec_all())) return st;
+  if ((st = ovs_residual_norms(c, prec, ni.residual0))) return st;
+  memcpy(ni.residual, ni.residual0, sizeof(ni.residual));
+  ni.converged = check(ni.residual);
+  for (int it = 1; it <= o->newton_max; ++it) {
+    if ((st = ovs_assemble_impl(c, OVS_ASM_NSVOF, both, prec, nullptr)) < 0) return st;
+    if ((st = solve(OVS_SYS_NSVOF, o->tol_ns, &ni.krylov_iterations_ns))) return st;
+    if (o->solve_tem) {
+      if ((st = ovs_assemble_impl(c, OVS_ASM_TEM, both, prec, nullptr)) < 0) return st;
+      if ((st = solve(OVS_SYS_TEM, o->tol_tem, &ni.krylov_iterations_tem))) return st;
+    }
+    if ((st = vec_all())) return st;
+    if ((st = ovs_residual_norms(c, prec, ni.residual))) return st;
+    ni.iterations = it;
+    ni.converged = check(ni.residual);
+    if (ni.converged) break;
+  }
+  ni.seconds = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+  if (info) *info = ni;
   return OVS_OK;
 }
 
