@@ -520,7 +520,7 @@ def run_ours(args, world, rank, local_rank, dist):
         "vs_baseline": None, "dtype": "f32", "data": "synthetic",
         "config": {"workload": f"config3: NS+VOF+T quench assembly pass, {n}^3 cells x6 Kuhn tets "
                                f"({E} tets, {N} nodes, {nnz} CSR slots), FP32 mixed path",
-                   "cache": "inputs larger than L2 (FP32 CSR values alone 2.9 GB); no flush",
+                   "cache": f"inputs larger than L2 (FP32 CSR values alone {24 * nnz * 4 / 1e9:.2f} GB); no flush",
                    "parallelism": f"replicas x{world}" if world > 1 else "1 GPU"},
         "e2e": {"value": world * E / e2e_s / 1e6, "unit": "Melem/s", "h2d_bytes_per_step": h2d,
                 "d2h_bytes_per_step": d2h},
