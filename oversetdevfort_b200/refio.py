@@ -1,0 +1,215 @@
+"""The reference's on-disk formats, so its meshes and restarts run through
+this path: the partition mesh ``part<id>.dat`` (read by input_mesh,
+src/input.f90:15-120; written by genmesh_overset/mesh.f90:140-204) and the
+text restart ``restart<step><rank>`` (readSol / writeSol,
+src/iosol.f90:122-194, 377-454).  Both are Fortran list-directed text; this
+module reads and writes them with numpy and builds the `mesh.Case` inputs
+from them.  The overset boundary maps (``l2b.<id>.dat``) belong to the
+overset coupling, which is outside this path, and are not read.
+"""
+from __future__ import annotations
+
+from dataclasses import dataclass, field
+
+import numpy as np
+
+from . import mesh as M
+
+
+@dataclass
+class Boundary:
+    face_id: int
+    face_ien: np.ndarray      # (NFACE, NSHLBmax) 1-based node ids
+    f2e: np.ndarray           # (NFACE,) owning element, 1-based
+    face_or: np.ndarray       # (NFACE,) face orientation code
+    bnodes: np.ndarray        # (NNODE_b,) 1-based node ids
+    nshlb: np.ndarray | None = None   # per-face node counts (non-FEM files only)
+
+
+@dataclass
+class PartMesh:
+    nsd: int
+    nshl: int
+    nshlb_max: int
+    xg: np.ndarray            # (N, NSD)
+    node_id: np.ndarray       # (N,) NodeID (FEM files)
+    elmnshl: np.ndarray       # (E,)
+    ien: np.ndarray           # (E, NSHL) 1-based
+    elm_id: np.ndarray        # (E,)
+    bounds: list = field(default_factory=list)
+    wg: np.ndarray | None = None      # NURBS weights (NPATCH > 0)
+    epid: np.ndarray | None = None
+    eijk: np.ndarray | None = None
+
+
+class _Tokens:
+    """Whitespace tokens of a list-directed file, one record per line."""
+
+    def __init__(self, path):
+        with open(path) as f:
+            self.lines = [ln.split() for ln in f if ln.strip()]
+        self.i = 0
+
+    def record(self):
+        t = self.lines[self.i]
+        self.i += 1
+        return t
+
+    def block(self, nrec):
+        rows = self.lines[self.i:self.i + nrec]
+        self.i += nrec
+        return rows
+
+
+def _float(s: str) -> float:
+    return float(s.replace("D", "E").replace("d", "e"))
+
+
+def read_part(path, fem_flag: int = 1) -> PartMesh:
+    """input_mesh (src/input.f90:31-120)."""
+    tk = _Tokens(path)
+    nsd, nshl, nshlb_max = (int(v) for v in tk.record()[:3])
+    nnode, nelem, nbound, npatch = (int(v) for v in tk.record()[:4])
+    rows = tk.block(nnode)
+    xg = np.array([[_float(v) for v in r[:nsd]] for r in rows])
+    node_id = np.array([int(r[nsd]) for r in rows], dtype=np.int32) if fem_flag == 1 else np.zeros(nnode, np.int32)
+    rows = tk.block(nelem)
+    elmnshl = np.array([int(r[0]) for r in rows], dtype=np.int32)
+    ien = np.zeros((nelem, nshl), dtype=np.int32)
+    elm_id = np.zeros(nelem, dtype=np.int32)
+    for e, r in enumerate(rows):
+        k = elmnshl[e]
+        ien[e, :k] = [int(v) for v in r[1:1 + k]]
+        if fem_flag == 1:
+            elm_id[e] = int(r[1 + k])
+    bounds = []
+    for _ in range(nbound):
+        face_id, nface, nbn = (int(v) for v in tk.record()[:3])
+        rows = tk.block(nface)
+        if fem_flag == 1:
+            face_ien = np.array([[int(v) for v in r[:nshlb_max]] for r in rows], dtype=np.int32).reshape(nface, nshlb_max)
+            nshlb = None
+        else:
+            nshlb = np.array([int(r[0]) for r in rows], dtype=np.int32)
+            face_ien = np.array([[int(v) for v in r[1:1 + nshlb_max]] for r in rows], dtype=np.int32).reshape(nface, nshlb_max)
+        rows = tk.block(nface)
+        f2e = np.array([int(r[0]) for r in rows], dtype=np.int32)
+        face_or = np.array([int(r[1]) for r in rows], dtype=np.int32)
+        bnodes = np.array([int(r[0]) for r in tk.block(nbn)], dtype=np.int32)
+        bounds.append(Boundary(face_id, face_ien, f2e, face_or, bnodes, nshlb))
+    pm = PartMesh(nsd, nshl, nshlb_max, xg, node_id, elmnshl, ien, elm_id, bounds)
+    if npatch > 0:
+        pm.wg = np.array([_float(r[0]) for r in tk.block(nnode)])
+        rows = tk.block(nelem)
+        pm.epid = np.array([int(r[0]) for r in rows], dtype=np.int32)
+        pm.eijk = np.array([[int(v) for v in r[1:1 + nsd]] for r in rows], dtype=np.int32)
+    return pm
+
+
+def write_part(path, pm: PartMesh, fem_flag: int = 1) -> None:
+    """The same records in the order input_mesh reads them."""
+    npatch = 1 if pm.wg is not None else 0
+    with open(path, "w") as f:
+        f.write(f"{pm.nsd} {pm.nshl} {pm.nshlb_max}\n")
+        f.write(f"{pm.xg.shape[0]} {pm.ien.shape[0]} {len(pm.bounds)} {npatch}\n")
+        for i in range(pm.xg.shape[0]):
+            xs = " ".join(repr(float(v)) for v in pm.xg[i])
+            f.write(f"{xs} {int(pm.node_id[i])}\n" if fem_flag == 1 else f"{xs}\n")
+        for e in range(pm.ien.shape[0]):
+            k = int(pm.elmnshl[e])
+            ids = " ".join(str(int(v)) for v in pm.ien[e, :k])
+            f.write(f"{k} {ids} {int(pm.elm_id[e])}\n" if fem_flag == 1 else f"{k} {ids}\n")
+        for b in pm.bounds:
+            f.write(f"{b.face_id} {b.face_ien.shape[0]} {b.bnodes.size}\n")
+            for j in range(b.face_ien.shape[0]):
+                ids = " ".join(str(int(v)) for v in b.face_ien[j])
+                f.write(f"{ids}\n" if fem_flag == 1 else f"{int(b.nshlb[j])} {ids}\n")
+            for j in range(b.face_ien.shape[0]):
+                f.write(f"{int(b.f2e[j])} {int(b.face_or[j])}\n")
+            for v in b.bnodes:
+                f.write(f"{int(v)}\n")
+        if npatch:
+            for v in pm.wg:
+                f.write(f"{repr(float(v))}\n")
+            for e in range(pm.ien.shape[0]):
+                f.write(f"{int(pm.epid[e])} " + " ".join(str(int(v)) for v in pm.eijk[e]) + "\n")
+
+
+def part_from_mesh(m: "M.Mesh", face_ids=(1, 2, 3, 4, 5, 6)) -> PartMesh:
+    """A PartMesh of one of this package's box meshes: node ids 0, one
+    boundary per box face (its nodes; faces are not enumerated, NFACE = 0)."""
+    N, E = m.nnode, m.nelem
+    bounds = [Boundary(int(fid), np.zeros((0, 3 if m.nshl == 4 else 4), np.int32), np.zeros(0, np.int32),
+                       np.zeros(0, np.int32), (np.asarray(nodes) + 1).astype(np.int32))
+              for fid, nodes in zip(face_ids, m.faces)]
+    return PartMesh(3, m.nshl, 3 if m.nshl == 4 else 4, np.asarray(m.xg, dtype=np.float64),
+                    np.zeros(N, np.int32), np.full(E, m.nshl, np.int32), np.asarray(m.ien, dtype=np.int32),
+                    np.asarray(m.elm_id, dtype=np.int32), bounds)
+
+
+def mesh_from_part(pm: PartMesh) -> "M.Mesh":
+    """mesh.Mesh of a partition: the FE element block (one element type per
+    partition, as this path assembles), 1-based ien, the boundary node sets
+    in file order as faces."""
+    if np.any(pm.elmnshl != pm.nshl):
+        raise ValueError("mixed element types in one partition are not assembled by this path")
+    lo, hi = pm.xg.min(axis=0), pm.xg.max(axis=0)
+    faces = [np.sort(b.bnodes.astype(np.int64) - 1) for b in pm.bounds]
+    return M.Mesh(np.asfortranarray(pm.xg[:, :3]), np.asfortranarray(pm.ien.astype(np.int32)),
+                  pm.elm_id.astype(np.int32).copy(), faces, None, tuple(float(v) for v in (hi - lo)))
+
+
+# the records of a restart, in file order, and the state arrays they fill
+RESTART_READ = ("dgold", "ugold", "ugmold", "acgold", "acgmold", "phigold", "rphigold", "pgold", "tgold", "rtgold")
+RESTART_WRITE = ("dg", "ug", "ugm", "acg", "acgm", "phig", "rphig", "pg", "tgold", "rtgold")
+
+
+def read_restart(path, nnode: int) -> tuple[int, float, dict]:
+    """readSol (src/iosol.f90:122-194): (step, time, arrays) with the arrays
+    named as readSol fills them (the *old fields, pgold included)."""
+    tk = _Tokens(path)
+    head = tk.record()
+    step, time = int(head[0]), _float(head[1])
+    out = {}
+    for name in RESTART_READ:
+        rows = tk.block(nnode)
+        a = np.array([[_float(v) for v in r] for r in rows])
+        out[name] = a if a.shape[1] == 3 else a[:, 0].copy()
+    return step, time, out
+
+
+def write_restart(path, step: int, time: float, state: dict) -> None:
+    """writeSol (src/iosol.f90:377-454): the current dg, ug, ugm, acg, acgm,
+    phig, rphig, pg and, as the reference writes them, the OLD temperature
+    arrays Tgold and rTgold."""
+    with open(path, "w") as f:
+        f.write(f"{step} {repr(float(time))}\n")
+        for name in RESTART_WRITE:
+            a = np.asarray(state[name])
+            if a.ndim == 2:
+                for row in a:
+                    f.write(" ".join(repr(float(v)) for v in row) + "\n")
+            else:
+                for v in a:
+                    f.write(repr(float(v)) + "\n")
+
+
+def state_from_restart(arrays: dict, gami: float) -> dict:
+    """The package state after readSol and the predictor of driver.f90:83-85
+    (ug = ugold, acg = (gami - 1)/gami acgold, pg = pgold; the other current
+    fields start from their old values)."""
+    N = arrays["ugold"].shape[0]
+    st = M.empty_state(N)
+    for name in ("dgold", "ugold", "ugmold", "acgold", "acgmold", "phigold", "rphigold", "tgold", "rtgold"):
+        st[name][:] = arrays[name]
+    st["dg"][:] = arrays["dgold"]
+    st["ug"][:] = arrays["ugold"]
+    st["ugm"][:] = arrays["ugmold"]
+    st["acg"][:] = (gami - 1.0) / gami * arrays["acgold"]
+    st["acgm"][:] = arrays["acgmold"]
+    st["pg"][:] = arrays["pgold"]
+    st["phig"][:] = arrays["phigold"]
+    st["rphig"][:] = arrays["rphigold"]
+    st["tg"][:] = arrays["tgold"]
+    st["rtg"][:] = arrays["rtgold"]
+    return st

@@ -1,0 +1,91 @@
+"""The reference's mesh and restart files (oversetdevfort_b200.refio): round
+trips of box meshes through part.dat (the CSR pattern of the read mesh is
+the original's, by the oracle's genSparStruc), the non-FEM and NURBS
+branches of input_mesh on a hand-written file, and restart round trips
+including writeSol's old-temperature quirk.  CPU only."""
+import numpy as np
+import pytest
+
+from oversetdevfort_b200 import mesh as M
+from oversetdevfort_b200 import refio
+
+
+@pytest.mark.parametrize("mk", [lambda: M.box_tet(3, 2, 2, 1.0, 0.5, 2.0), lambda: M.box_hex(2, 3, 2)])
+def test_part_round_trip_and_pattern(tmp_path, oracle, mk):
+    m = mk()
+    m.elm_id[::3] = 101
+    pm = refio.part_from_mesh(m)
+    pm.node_id[:] = np.arange(m.nnode) % 5
+    path = tmp_path / "part1.dat"
+    refio.write_part(path, pm)
+    back = refio.read_part(path)
+    np.testing.assert_array_equal(back.xg, m.xg)
+    np.testing.assert_array_equal(back.ien, m.ien)
+    np.testing.assert_array_equal(back.elm_id, m.elm_id)
+    np.testing.assert_array_equal(back.node_id, pm.node_id)
+    m2 = refio.mesh_from_part(back)
+    for a, b in zip(m2.faces, m.faces):
+        np.testing.assert_array_equal(a, b)
+    c1, r1 = oracle.gen_spar_struc(m.ien, m.nnode)
+    c2, r2 = oracle.gen_spar_struc(m2.ien, m2.nnode)
+    np.testing.assert_array_equal(c1, c2)
+    np.testing.assert_array_equal(r1, r2)
+
+
+def test_part_non_fem_and_nurbs_records(tmp_path):
+    # one tet with one boundary and NURBS data: every branch of input_mesh
+    text = """3 4 3
+4 1 1 1
+0.0 0.0 0.0
+1.0D0 0.0 0.0
+0.0 1.0 0.0
+0.0 0.0 1.0
+4 1 2 3 4
+7 1 3
+3 1 2 3
+1 4
+1
+2
+3
+1.0
+0.5D0
+1.0
+1.0
+1 0 0 0
+"""
+    path = tmp_path / "part2.dat"
+    path.write_text(text)
+    pm = refio.read_part(path, fem_flag=0)
+    assert (pm.nsd, pm.nshl, pm.nshlb_max) == (3, 4, 3)
+    assert pm.xg[1, 0] == 1.0 and pm.ien.tolist() == [[1, 2, 3, 4]]
+    b = pm.bounds[0]
+    assert b.face_id == 7 and b.nshlb.tolist() == [3] and b.face_ien.tolist() == [[1, 2, 3]]
+    assert b.f2e.tolist() == [1] and b.face_or.tolist() == [4] and b.bnodes.tolist() == [1, 2, 3]
+    assert pm.wg.tolist() == [1.0, 0.5, 1.0, 1.0] and pm.epid.tolist() == [1] and pm.eijk.tolist() == [[0, 0, 0]]
+    back = tmp_path / "part3.dat"
+    refio.write_part(back, pm, fem_flag=0)
+    pm2 = refio.read_part(back, fem_flag=0)
+    np.testing.assert_array_equal(pm2.xg, pm.xg)
+    np.testing.assert_array_equal(pm2.wg, pm.wg)
+    assert pm2.bounds[0].nshlb.tolist() == [3]
+
+
+def test_restart_round_trip_and_predictor(tmp_path):
+    rng = np.random.default_rng(3)
+    N = 17
+    st = M.empty_state(N)
+    for k, a in st.items():
+        a[...] = rng.standard_normal(a.shape)
+    path = tmp_path / "restart1"
+    refio.write_restart(path, 12, 0.125, st)
+    step, time, arr = refio.read_restart(path, N)
+    assert step == 12 and time == 0.125
+    # writeSol stores the current fields but the OLD temperature arrays;
+    # readSol puts every record into the *old fields
+    for rd, wr in zip(refio.RESTART_READ, refio.RESTART_WRITE):
+        np.testing.assert_array_equal(arr[rd], st[wr])
+    s2 = refio.state_from_restart(arr, gami=0.8)
+    np.testing.assert_array_equal(s2["ug"], st["ug"])
+    np.testing.assert_array_equal(s2["pg"], st["pg"])
+    np.testing.assert_allclose(s2["acg"], (0.8 - 1.0) / 0.8 * st["acg"])
+    np.testing.assert_array_equal(s2["tg"], st["tgold"])
