@@ -40,10 +40,10 @@ sys.path.insert(0, str(ROOT))
 METRIC = "assembly Melem/s & GMRES s/solve at 2.1M nodes, mixed vs FP64 to rel. resid 1e-8"
 
 
-def ncu_traffic_per_tet(name):
-    """DRAM bytes (read + write) per tet of one launch, from the committed
-    ncu summary of the kernel on the 48^3-cell case (663,552 tets); the bench
-    scales it by the tets of its own workload.  (None, reason) when absent."""
+def ncu_traffic_per_tet(name, tets=663552):
+    """DRAM bytes (read + write) per tet of one launch, from a committed ncu
+    summary of the kernel on a workload of `tets` tets; the bench scales it
+    by the tets of its own workload.  (None, reason) when absent."""
     import re
     path = os.path.join(os.path.dirname(os.path.abspath(__file__)), "profiles", name)
     try:
@@ -58,8 +58,9 @@ def ncu_traffic_per_tet(name):
     rd, wr = mb("dram__bytes_read.sum"), mb("dram__bytes_write.sum")
     if rd is None or wr is None:
         return None, "no DRAM counters in " + name
-    return (rd + wr) / 663552.0, ("ncu dram__bytes_read.sum + dram__bytes_write.sum of one launch on the "
-                                  "48^3-cell case (profiles/%s), scaled by tets" % name)
+    return (rd + wr) / float(tets), ("ncu dram__bytes_read.sum + dram__bytes_write.sum of one launch on a "
+                                     "%d-tet case (profiles/%s), per tet times the tets of this workload"
+                                     % (tets, name))
 
 
 def _peaks():
@@ -434,7 +435,7 @@ def run_ours(args, world, rank, local_rank, dist):
     sp_ach = spmv_bytes(4) / (prof["spmv_nsvof_fp32_ms"] * 1e-3) / 1e9
     as_ach = rows_bytes(4) / (prof["asm_nsvof_fp32_rows_ms"] * 1e-3) / 1e9
     pa_ach = pass_bytes(4) / (prof["asm_nsvof_fp32_ms"] * 1e-3) / 1e9
-    traffic, traffic_src = ncu_traffic_per_tet("assemble_rows_kernel_quench48.md")
+    traffic, traffic_src = ncu_traffic_per_tet("assemble_rows_kernel_quench128_dram.md", 12582912)
     roof_asm = {"kernel": "assemble_rows_kernel<float,NSVOF> (row-owner element assembly)",
                 "bound": "hbm", "achieved": as_ach, "peak": hbm, "unit": "GB/s",
                 "frac": as_ach / hbm, "traffic": traffic * E if traffic else None,
