@@ -262,6 +262,16 @@ typedef struct ovs_newton_info {
   double seconds;    /* wall time of the call */
 } ovs_newton_info;
 int ovs_quench_newton(ovs_ctx* ctx, const ovs_newton_opts* opts, ovs_newton_info* info);
+/* nsteps time steps of the reference driver (src/driver.f90:70-100) from
+ * step first_step: predictor (ug = ugold, acg = (gami-1)/gami acgold), the
+ * Newton loop above (a single Newton iteration while istep <= 1 and no
+ * temperature solve at istep 0, src/solveFlow.f90:50-54,109), then the old
+ * values the driver updates: ugold, acgold, dgold, ugmold, acgmold (the
+ * driver leaves phigold, rphigold, Tgold, rTgold alone; update_vof_tem_old
+ * = 1 copies them too).  last: the Newton info of the last step;
+ * krylov_total: Krylov iterations over all steps (either may be NULL). */
+int ovs_quench_time_steps(ovs_ctx* ctx, int first_step, int nsteps, const ovs_newton_opts* opts,
+                          int update_vof_tem_old, ovs_newton_info* last, int* krylov_total);
 
 /* ----------------------------------------------------------- measurement
  * Hooks for benchmarking; they have no counterpart in the reference. */

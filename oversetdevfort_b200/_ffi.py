@@ -51,6 +51,7 @@ EXPORTS = [
     "ovs_set_lhs_block", "ovs_spmv", "ovs_gmres", "ovs_solve", "ovs_newton_update",
     "ovs_residual_norms", "ovs_profile", "ovs_launch_count", "ovs_last_device_ms",
     "ovs_host_alloc", "ovs_host_free", "ovs_residual_vjp", "ovs_gmres_transposed", "ovs_quench_newton",
+    "ovs_quench_time_steps",
     "ovs_gmres_tem_noalloc",
 ]
 
@@ -139,6 +140,8 @@ def load(path: str | os.PathLike | None = None) -> C.CDLL:
         "ovs_host_free": ([vp], C.c_int),
         "ovs_residual_vjp": ([vp, C.c_int, dp, dp], C.c_int),
         "ovs_quench_newton": ([vp, C.POINTER(OvsNewtonOpts), C.POINTER(OvsNewtonInfo)], C.c_int),
+        "ovs_quench_time_steps": ([vp, C.c_int, C.c_int, C.POINTER(OvsNewtonOpts), C.c_int,
+                                   C.POINTER(OvsNewtonInfo), C.POINTER(C.c_int)], C.c_int),
         "ovs_gmres_transposed": ([vp, C.c_int, dp, C.c_double, C.c_int, C.c_int, dp, C.POINTER(OvsGmresInfo)],
                                  C.c_int),
         "ovs_gmres_tem_noalloc": ([C.c_int, vp, vp, vp, vp, vp, C.c_double, C.c_int, C.c_int, vp,

@@ -242,6 +242,22 @@ class Context:
         F.check(self.lib.ovs_quench_newton(self.h, C.byref(o), C.byref(info)), "ovs_quench_newton")
         return info
 
+    def quench_time_steps(self, first_step: int, nsteps: int, update_vof_tem_old: bool = False, **newton):
+        """nsteps time steps of the reference driver on the device (predictor,
+        Newton loop, old-value update); returns (last step's OvsNewtonInfo,
+        Krylov iterations over all steps).  Keyword arguments as quench_newton."""
+        d = dict(mode=F.OVS_FP64, newton_max=3, solve_tem=True, kspace=50, kspace_min=1, max_cycles=100,
+                 tol_ns=1e-6, tol_tem=1e-6, utol=(1e-3,) * 4, atol=(1e-15,) * 4)
+        d.update(newton)
+        o = F.OvsNewtonOpts(d["mode"], d["newton_max"], int(d["solve_tem"]), d["kspace"], d["kspace_min"],
+                            d["max_cycles"], d["tol_ns"], d["tol_tem"], (C.c_double * 4)(*d["utol"]),
+                            (C.c_double * 4)(*d["atol"]))
+        info = F.OvsNewtonInfo()
+        kt = C.c_int(0)
+        F.check(self.lib.ovs_quench_time_steps(self.h, first_step, nsteps, C.byref(o), int(update_vof_tem_old),
+                                               C.byref(info), C.byref(kt)), "ovs_quench_time_steps")
+        return info, kt.value
+
     def newton_update(self, system: int):
         F.check(self.lib.ovs_newton_update(self.h, system), "ovs_newton_update")
 

@@ -108,6 +108,17 @@ __global__ void copy_convert_kernel(const TS* __restrict__ a, TD* __restrict__ b
   if (i < n) b[i] = (TD)a[i];
 }
 
+// predictor of a time step (src/driver.f90:83-85): ug = ugold,
+// acg = (gami - 1)/gami acgold (pg = pgold is the identity here: the old
+// pressure is the pressure left by the previous step)
+__global__ void predictor_kernel(size_t n3, double c, const double* __restrict__ ugold, const double* __restrict__ acgold,
+                                 double* __restrict__ ug, double* __restrict__ acg) {
+  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n3; i += (size_t)gridDim.x * blockDim.x) {
+    ug[i] = ugold[i];
+    acg[i] = c * acgold[i];
+  }
+}
+
 // Newton update, src/solveFlow.f90:99-104,139-140
 __global__ void newton_update_kernel(int N, int sys, double gdt, double agdt, const double* __restrict__ sol,
                                      double* acg, double* ug, double* pg, double* rphig, double* phig,
@@ -773,6 +784,52 @@ int ovs_quench_newton(ovs_ctx* c, const ovs_newton_opts* o, ovs_newton_info* inf
   }
   ni.seconds = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
   if (info) *info = ni;
+  return OVS_OK;
+}
+
+
+// The time loop of the reference driver around solmultiphasethermofluid_stag
+// (src/driver.f90:70-100): predictor, the Newton loop (one Newton iteration
+// and no temperature solve while istep <= 1 / istep == 0, solveFlow.f90:50-54,
+// :109), then the old values the driver updates (:95-100: ug, acg, dg, ugm,
+// acgm; pg is its own old value here).  The driver does not update phigold,
+// rphigold, Tgold, rTgold; update_vof_tem_old = 1 updates them too.
+int ovs_quench_time_steps(ovs_ctx* c, int first_step, int nsteps, const ovs_newton_opts* o,
+                          int update_vof_tem_old, ovs_newton_info* last, int* krylov_total) {
+  if (!c || !o || nsteps < 0) return OVS_ERR_ARG;
+  int st;
+  if ((st = ovs_activate(c))) return st;
+  const size_t N = c->N;
+  const double gami = c->params.gami;
+  int kt = 0;
+  for (int s = 0; s < nsteps; ++s) {
+    const int istep = first_step + s;
+    predictor_kernel<<<ovs_grid(3 * N, 256, 1 << 30), 256, 0, c->stream>>>(
+        3 * N, (gami - 1.0) / gami, c->field[OVS_F_UGOLD], c->field[OVS_F_ACGOLD], c->field[OVS_F_UG], c->field[OVS_F_ACG]);
+    ++c->launches;
+    OVS_CUDA_TRY(cudaGetLastError());
+    ovs_newton_opts os = *o;
+    if (istep <= 1) os.newton_max = 1;
+    os.solve_tem = o->solve_tem && istep > 0;
+    ovs_newton_info ni;
+    if ((st = ovs_quench_newton(c, &os, &ni))) return st;
+    kt += ni.krylov_iterations_ns + ni.krylov_iterations_tem;
+    const int pairs3[][2] = {{OVS_F_UG, OVS_F_UGOLD}, {OVS_F_ACG, OVS_F_ACGOLD}, {OVS_F_DG, OVS_F_DGOLD},
+                             {OVS_F_UGM, OVS_F_UGMOLD}, {OVS_F_ACGM, OVS_F_ACGMOLD}};
+    for (auto& pr : pairs3)
+      OVS_CUDA_TRY(cudaMemcpyAsync(c->field[pr[1]], c->field[pr[0]], sizeof(double) * 3 * N,
+                                   cudaMemcpyDeviceToDevice, c->stream));
+    if (update_vof_tem_old) {
+      const int pairs1[][2] = {{OVS_F_PHIG, OVS_F_PHIGOLD}, {OVS_F_RPHIG, OVS_F_RPHIGOLD}, {OVS_F_TG, OVS_F_TGOLD},
+                               {OVS_F_RTG, OVS_F_RTGOLD}};
+      for (auto& pr : pairs1)
+        OVS_CUDA_TRY(cudaMemcpyAsync(c->field[pr[1]], c->field[pr[0]], sizeof(double) * N,
+                                     cudaMemcpyDeviceToDevice, c->stream));
+    }
+    OVS_CUDA_TRY(cudaStreamSynchronize(c->stream));
+    if (last) *last = ni;
+  }
+  if (krylov_total) *krylov_total = kt;
   return OVS_OK;
 }
 

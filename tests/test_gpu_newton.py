@@ -60,3 +60,28 @@ def test_device_newton_mixed_mode_converges():
     assert info.iterations >= 1 and info.krylov_iterations_ns > 0
     assert info.residual[0] < 1e-3 * info.residual0[0], (list(info.residual), list(info.residual0))
     ctx.close()
+
+
+def test_device_time_steps_match_host_driver():
+    """ovs_quench_time_steps (driver.f90:70-100 around the Newton loop) against
+    the host doing the predictor, quench_newton and the old-value copies."""
+    case = M.quench_case(M.box_tet(6, 6, 8, 1.0, 1.0, 1.25), "steps6")
+    kw = dict(mode=F.OVS_FP64, newton_max=2, kspace=40, tol_ns=1e-6, tol_tem=1e-6, utol=(1e-4,) * 4,
+              atol=(1e-30,) * 4)
+    a = Context.from_case(case)
+    info, kt = a.quench_time_steps(0, 3, **kw)
+    b = Context.from_case(case)
+    g = case.params["gami"]
+    for istep in range(3):
+        b.set_field("ug", b.get_field("ugold"))
+        b.set_field("acg", (g - 1.0) / g * b.get_field("acgold"))
+        b.quench_newton(kw["mode"], 1 if istep <= 1 else kw["newton_max"], istep > 0, kw["kspace"], 1, 100,
+                        kw["tol_ns"], kw["tol_tem"], kw["utol"], kw["atol"])
+        for cur, old in (("ug", "ugold"), ("acg", "acgold"), ("dg", "dgold"), ("ugm", "ugmold"),
+                         ("acgm", "acgmold")):
+            b.set_field(old, b.get_field(cur))
+    for f in FIELDS + ("ugold", "acgold", "phigold", "tgold"):
+        np.testing.assert_array_equal(a.get_field(f), b.get_field(f))
+    assert kt > 0
+    a.close()
+    b.close()
