@@ -95,6 +95,13 @@ enum {
   OVS_F_COUNT
 };
 
+/* boundary-face flags (ovs_set_faces) */
+enum {
+  OVS_FACE_WEAK = 1,   /* face of a boundary with BCugType(b,d) == 2: the weak Dirichlet
+                          (Nitsche) and outflow face terms, src/FaceAssembly_weak.f90 */
+  OVS_FACE_CONVH = 2   /* convective heat flux h (T - T_inf) on the temperature system */
+};
+
 /* ---------------------------------------------------------------- types */
 typedef struct ovs_ctx ovs_ctx;
 
@@ -178,6 +185,27 @@ int ovs_set_params(ovs_ctx* ctx, const ovs_params* p);
 /* IBC(N,nibc) column-major, entries 0/1 (src/setBCs.f90:183-187: columns
  * 1-3 velocity, 4 pressure, 5 VOF, 6 temperature) */
 int ovs_set_ibc(ovs_ctx* ctx, const int* ibc, int nibc);
+/* Boundary faces for the face assemblies, in the reference's loop order
+ * (boundary b = 1..NBOUND, then the faces of bound(b)): f2e = bound(b)%F2E
+ * (1-based owning element), face_or = bound(b)%FACE_OR (1..4), flags
+ * OVS_FACE_*; hconv / tinf (may be NULL without OVS_FACE_CONVH) give h and
+ * T_inf per face.  Every later ovs_assemble adds, after the element pass:
+ *   OVS_ASM_NS:    FaceAssembly_NS_weak, then FaceAssembly_NS_outflow, on the
+ *                  OVS_FACE_WEAK faces (src/FaceAssembly_weak.f90:4-409,
+ *                  called at src/assembleNavSto.f90:55-61);
+ *   OVS_ASM_NSVOF: the same two routines on the velocity/pressure blocks, every
+ *                  element a target (the quench driver's face calls,
+ *                  src/solveQuenching.f90:75-83, name an undefined routine and
+ *                  pass 11 arguments to the 8-argument outflow routine);
+ *   OVS_ASM_TEM:   the convective heat flux h (T - T_inf) on OVS_FACE_CONVH
+ *                  faces (FaceAssembly_ConvectiveH, called at
+ *                  src/solveQuenching.f90:92, is not defined by the reference).
+ * Each face's arrays pass through BCLhs_3D / BCLhs_tem before the scatter, as
+ * in the reference.  Linear tets only (OVS_ERR_ARG otherwise); nface = 0
+ * clears the set.  ovs_residual_vjp returns OVS_ERR_STATE while a face set is
+ * active (face terms are not differentiated). */
+int ovs_set_faces(ovs_ctx* ctx, int nface, const int* f2e, const int* face_or,
+                  const int* flags, const double* hconv, const double* tinf);
 int ovs_set_field(ovs_ctx* ctx, int field, const double* host);
 int ovs_get_field(ovs_ctx* ctx, int field, double* host);
 

@@ -169,10 +169,10 @@ static double get_inverse_3x3(double A[3][3], double Ai[3][3]) {
 /* eval_shape_fem src/eval_shape_FEM.f90:4-61: basis, dx/dxi on the CURRENT
  * configuration x+d (:31-36), inverse, global gradients (:41-45) and the
  * metric G_ij = sum_k dxi_k/dx_i dxi_k/dx_j (:47-52).  Returns DetJ. */
-static double eval_shape_fem(int nshl, const double* gp, double xl[][3],
-                             double dl[][3], double* shl, double shg[][3],
-                             double Gij[3][3]) {
-  double shgl[NSHL_MAX][3], dxdxi[3][3], dxidx[3][3];
+static double eval_shape_fem_dx(int nshl, const double* gp, double xl[][3],
+                                double dl[][3], double* shl, double shg[][3],
+                                double Gij[3][3], double dxidx[3][3]) {
+  double shgl[NSHL_MAX][3], dxdxi[3][3];
   if (nshl == 4) lintetshl(gp, shl, shgl); else linhexshl(gp, shl, shgl);
   for (int i = 0; i < 3; ++i)
     for (int j = 0; j < 3; ++j) {
@@ -194,6 +194,13 @@ static double eval_shape_fem(int nshl, const double* gp, double xl[][3],
       Gij[i][j] = s;
     }
   return detj;
+}
+
+static double eval_shape_fem(int nshl, const double* gp, double xl[][3],
+                             double dl[][3], double* shl, double shg[][3],
+                             double Gij[3][3]) {
+  double dxidx[3][3];
+  return eval_shape_fem_dx(nshl, gp, xl, dl, shl, shg, Gij, dxidx);
 }
 
 /* prop_interp src/e3int.f90:4-13 */
@@ -908,8 +915,271 @@ static int alpha_alloc(int N, alpha_buf* b) {
   return 0;
 }
 
+/* ----------------------------------------------------------------------
+ * Face assemblies (linear tets; genGPMap src/genGP_GW.f90:42-62 maps face
+ * points for nshl = 4 and 6 only).
+ * -------------------------------------------------------------------- */
+
+/* genGPtritet src/genGP_GW.f90:478-572 with NGAUSSB = NSHLB = 3
+ * (src/input.f90:161): volume coordinates of the three face points for
+ * FACE_OR = 1..4; genGPandGWtri :453-465 gives each the weight 1/6. */
+#define SIXTH 0.166666666666666666667
+#define TWO3 0.666666666666666666667
+static const double c_tri_mgp[4][3][3] = {
+    {{SIXTH, TWO3, SIXTH}, {SIXTH, SIXTH, TWO3}, {TWO3, SIXTH, SIXTH}},
+    {{0.0, SIXTH, SIXTH}, {0.0, SIXTH, TWO3}, {0.0, TWO3, SIXTH}},
+    {{TWO3, 0.0, SIXTH}, {SIXTH, 0.0, TWO3}, {SIXTH, 0.0, SIXTH}},
+    {{SIXTH, TWO3, 0.0}, {TWO3, SIXTH, 0.0}, {SIXTH, SIXTH, 0.0}}};
+static const double c_tri_gw = SIXTH;
+
+/* the element nodes of the face, in the order eval_faceshape_tet takes them
+ * (src/eval_shape_FEM.f90:90-106), 0-based */
+static const int c_face_nodes[4][3] = {{1, 2, 0}, {3, 2, 1}, {0, 2, 3}, {1, 0, 3}};
+
+/* eval_faceshape_tet src/eval_shape_FEM.f90:66-143: tangents of the face
+ * triangle (lintrishl :261-282), unit normal and DetJb (:108-126), then
+ * eval_shape_fem at the face point in volume coordinates.  Returns DetJb. */
+static double eval_faceshape_tet(int fo, const double* mgp, double xl[][3],
+                                 double dl[][3], double* shl, double shg[][3],
+                                 double dxidx[3][3], double nor[3]) {
+  double bx[3][3], t1[3], t2[3], Gij[3][3];
+  for (int i = 0; i < 3; ++i) {
+    const int a = c_face_nodes[fo - 1][i];
+    for (int d = 0; d < 3; ++d) bx[i][d] = xl[a][d] + dl[a][d];
+  }
+  for (int d = 0; d < 3; ++d) {
+    t1[d] = bx[0][d] - bx[2][d];
+    t2[d] = bx[1][d] - bx[2][d];
+  }
+  nor[0] = t1[1] * t2[2] - t1[2] * t2[1];
+  nor[1] = t1[2] * t2[0] - t1[0] * t2[2];
+  nor[2] = t1[0] * t2[1] - t1[1] * t2[0];
+  const double detjb = sqrt(nor[0] * nor[0] + nor[1] * nor[1] + nor[2] * nor[2]);
+  for (int d = 0; d < 3; ++d) nor[d] = nor[d] / detjb;
+  eval_shape_fem_dx(4, mgp, xl, dl, shl, shg, Gij, dxidx);
+  return detjb;
+}
+
+/* e3bSTAB_weak src/e3STAB.f90:256-287: tauB = 4 mu / h_n with
+ * h_n = 2 / |dxi/dx n| (the non-tet branch, as written); tauNor = tauB */
+static double e3bstab_weak(const double* nor, double dxidx[3][3], double mui) {
+  double t[3];
+  for (int i = 0; i < 3; ++i) t[i] = dxidx[i][0] * nor[0] + dxidx[i][1] * nor[1] + dxidx[i][2] * nor[2];
+  const double hn = 2.0 / sqrt(t[0] * t[0] + t[1] * t[1] + t[2] * t[2]);
+  return 4.0 * mui / hn;
+}
+
+/* e3bRHS_weak src/e3RHS.f90:105-170 */
+static void e3brhs_weak(double rhoi, double mui, const double* nor, double tauB,
+                        double tauNor, double gwt, double detjb, const double* shl,
+                        double shg[][3], const double* ui, const double* umi, double pri,
+                        double du[3][3], const double* gi, elm_arrays* L) {
+  double ti[3], tmp1[3], tmp2[3][3];
+  for (int i = 0; i < 3; ++i)
+    ti[i] = -pri * nor[i] + mui * (du[i][0] * nor[0] + du[i][1] * nor[1] + du[i][2] * nor[2] +
+                                   du[0][i] * nor[0] + du[1][i] * nor[1] + du[2][i] * nor[2]);
+  double unor = (ui[0] - umi[0]) * nor[0] + (ui[1] - umi[1]) * nor[1] + (ui[2] - umi[2]) * nor[2];
+  const double uneg = 0.5 * (unor - fabs(unor));
+  const double gnor = gi[0] * nor[0] + gi[1] * nor[1] + gi[2] * nor[2];
+  unor = ui[0] * nor[0] + ui[1] * nor[1] + ui[2] * nor[2];
+  for (int i = 0; i < 3; ++i)
+    tmp1[i] = -ti[i] + tauB * (ui[i] - gi[i]) - uneg * rhoi * (ui[i] - gi[i]) +
+              (tauNor - tauB) * unor * nor[i];
+  const double gmul = 1.0;
+  for (int a = 0; a < 3; ++a)
+    for (int b = 0; b < 3; ++b)
+      tmp2[a][b] = -gmul * mui * ((ui[a] - gi[a]) * nor[b] + (ui[b] - gi[b]) * nor[a]);
+  for (int aa = 0; aa < 4; ++aa) {
+    for (int i = 0; i < 3; ++i)
+      L->Ru[i][aa] = L->Ru[i][aa] -
+                     (shl[aa] * tmp1[i] + (shg[aa][0] * tmp2[i][0] + shg[aa][1] * tmp2[i][1] +
+                                           shg[aa][2] * tmp2[i][2])) * detjb * gwt;
+    L->Rp[aa] = L->Rp[aa] + shl[aa] * (unor - gnor) * detjb * gwt;
+  }
+}
+
+/* e3bLHS_weak src/e3LHS.f90:167-294 (gmul = 1, munor = tauNor - tauB) */
+static void e3blhs_weak(double rhoi, double mui, const double* ui, const double* umi,
+                        double tauB, double tauNor, double gwt, double detjb,
+                        const double* shl, double shg[][3], const double* nor,
+                        double fact2, elm_arrays* L) {
+  double tmp1[4], tmp2[4][4];
+  for (int a = 0; a < 4; ++a) tmp1[a] = shg[a][0] * nor[0] + shg[a][1] * nor[1] + shg[a][2] * nor[2];
+  const double unor = (ui[0] - umi[0]) * nor[0] + (ui[1] - umi[1]) * nor[1] + (ui[2] - umi[2]) * nor[2];
+  const double uneg = 0.5 * (unor - fabs(unor));
+  const double munor = tauNor - tauB, gmul = 1.0;
+  for (int bb = 0; bb < 4; ++bb)
+    for (int aa = 0; aa < 4; ++aa)
+      tmp2[aa][bb] = -shl[aa] * mui * tmp1[bb] - gmul * tmp1[aa] * mui * shl[bb] +
+                     shl[aa] * tauB * shl[bb] - shl[aa] * uneg * rhoi * shl[bb];
+  for (int bb = 0; bb < 4; ++bb)
+    for (int aa = 0; aa < 4; ++aa)
+      for (int i = 0; i < 3; ++i)
+        for (int j = 0; j < 3; ++j) {
+          /* xKebe((i-1)*3+j): row component i, column component j */
+          double v = -shl[aa] * mui * shg[bb][i] * nor[j] - gmul * shg[aa][j] * nor[i] * mui * shl[bb] +
+                     shl[aa] * nor[i] * munor * nor[j] * shl[bb];
+          if (i == j) v = tmp2[aa][bb] + v;
+          L->K[3 * i + j][aa][bb] += fact2 * v * detjb * gwt;
+        }
+  for (int bb = 0; bb < 4; ++bb)
+    for (int aa = 0; aa < 4; ++aa)
+      for (int d = 0; d < 3; ++d) {
+        L->D[d][aa][bb] -= fact2 * shl[aa] * shl[bb] * nor[d] * detjb * gwt;
+        L->G[d][aa][bb] += fact2 * shl[aa] * shl[bb] * nor[d] * detjb * gwt;
+      }
+}
+
+/* FaceAssembly_NS_weak src/FaceAssembly_weak.f90:4-193 (rho_a, mu_a, wall
+ * velocity g = mesh velocity, element ELM_ID selection by subdomain_flag
+ * :102-109 when use_subdomain), then FaceAssembly_NS_outflow :197-409
+ * (backflow term, no ELM_ID selection), each over the faces of the
+ * boundaries with BCugType == 2, each face followed by BCLhs_3D and the
+ * scatter (:165-176, :381-392).  tauB is evaluated at every face point; the
+ * reference evaluates it only under ASSEMBLE_TENSOR_VEC (:152) although the
+ * matrix terms (:160-164) read it too. */
+void orc_face_ns(const orc_mesh* m, const ovs_params* p, const orc_state* A,
+                 orc_system* S, int tensor_flag, int use_subdomain) {
+  if (m->nface <= 0 || m->nshl != 4) return;
+  const int N = m->nnode;
+  const int mat = (tensor_flag & OVS_TENSOR_MAT) != 0;
+  const int vec = (tensor_flag & OVS_TENSOR_VEC) != 0;
+  const double fact2 = p->alfi * p->gami * p->delt;
+  const double rhoi = p->rhoa, mui = p->mua;
+  elm_arrays L;
+  for (int pass = 0; pass < 2; ++pass) {
+    for (int f = 0; f < m->nface; ++f) {
+      if (!(m->fflag[f] & OVS_FACE_WEAK)) continue;
+      const int e = m->f2e[f] - 1, fo = m->face_or[f];
+      int is_target = 1;
+      if (pass == 0 && use_subdomain) {
+        const int eid = m->elm_id ? m->elm_id[e] : 102;
+        is_target = 0;
+        if (p->subdomain_flag & 1) is_target = is_target || eid == p->elm_id_set[0];
+        if (p->subdomain_flag & 2) is_target = is_target || eid == p->elm_id_set[1];
+      }
+      double xl[NSHL_MAX][3], dl[NSHL_MAX][3], ul[NSHL_MAX][3], uml[NSHL_MAX][3], pl[NSHL_MAX];
+      for (int a = 0; a < 4; ++a) {
+        const int idx = m->ien[cm(e, m->nelem, a)] - 1;
+        gather3(m->xg, N, idx, xl[a]); gather3(A->dg, N, idx, dl[a]);
+        gather3(A->ug, N, idx, ul[a]); gather3(A->ugm, N, idx, uml[a]);
+        pl[a] = A->pg[idx];
+      }
+      memset(&L, 0, sizeof(L));
+      for (int ig = 0; ig < 3; ++ig) {
+        double shl[NSHL_MAX], shg[NSHL_MAX][3], dxidx[3][3], nor[3];
+        const double detjb = eval_faceshape_tet(fo, c_tri_mgp[fo - 1][ig], xl, dl, shl, shg, dxidx, nor);
+        double ui[3], umi[3], pri = 0.0, du[3][3];
+        for (int d = 0; d < 3; ++d) {
+          double s1 = 0, s2 = 0;
+          for (int a = 0; a < 4; ++a) { s1 += ul[a][d] * shl[a]; s2 += uml[a][d] * shl[a]; }
+          ui[d] = s1; umi[d] = s2;
+        }
+        for (int a = 0; a < 4; ++a) pri += pl[a] * shl[a];
+        for (int i = 0; i < 3; ++i)
+          for (int j = 0; j < 3; ++j) {
+            double s = 0.0;
+            for (int a = 0; a < 4; ++a) s += ul[a][i] * shg[a][j];
+            du[i][j] = s;
+          }
+        const double* gi = umi;
+        if (pass == 0) {
+          const double tauB = e3bstab_weak(nor, dxidx, mui), tauNor = tauB;
+          if (vec && is_target)
+            e3brhs_weak(rhoi, mui, nor, tauB, tauNor, c_tri_gw, detjb, shl, shg, ui, umi, pri, du, gi, &L);
+          if (mat && is_target)
+            e3blhs_weak(rhoi, mui, ui, umi, tauB, tauNor, c_tri_gw, detjb, shl, shg, nor, fact2, &L);
+        } else {
+          const double detjgw = detjb * c_tri_gw;
+          const double unor = (ui[0] - umi[0]) * nor[0] + (ui[1] - umi[1]) * nor[1] + (ui[2] - umi[2]) * nor[2];
+          const double uneg = 0.5 * (unor - fabs(unor));
+          if (vec)
+            for (int aa = 0; aa < 4; ++aa)
+              for (int d = 0; d < 3; ++d)
+                L.Ru[d][aa] = L.Ru[d][aa] + shl[aa] * rhoi * uneg * (ui[d] - gi[d]) * detjgw;
+          if (mat)
+            for (int bb = 0; bb < 4; ++bb)
+              for (int aa = 0; aa < 4; ++aa) {
+                const double t2 = -shl[aa] * uneg * rhoi * shl[bb];
+                for (int ii = 0; ii < 3; ++ii) L.K[4 * ii][aa][bb] += fact2 * t2 * detjgw;
+              }
+        }
+      }
+      bclhs_3d(m, e, 4, &L);
+      if (mat) fill_sparse(m, e, 4, &L, S, 0);
+      if (vec)
+        for (int b = 0; b < 4; ++b) {
+          const int g = m->ien[cm(e, m->nelem, b)] - 1;
+          for (int d = 0; d < 3; ++d) S->rhsu[cm(g, N, d)] += L.Ru[d][b];
+          S->rhsp[g] += L.Rp[b];
+        }
+    }
+  }
+}
+
+/* Convective heat flux on the temperature system, the FaceAssembly_ConvectiveH
+ * the quench driver calls (src/solveQuenching.f90:92) and the reference does
+ * not define: q = h (T^alpha - T_inf) on flagged faces, residual
+ * -int N_a q dGamma, tangent alpha_f gamma Delt int N_a h N_b dGamma (the
+ * factor of the element conductivity term), with the face points and
+ * surface Jacobian of the other face routines and BCLhs_tem after each face. */
+void orc_face_convh(const orc_mesh* m, const ovs_params* p, const orc_state* A,
+                    orc_system* S, int tensor_flag) {
+  if (m->nface <= 0 || m->nshl != 4) return;
+  const int N = m->nnode;
+  const int mat = (tensor_flag & OVS_TENSOR_MAT) != 0;
+  const int vec = (tensor_flag & OVS_TENSOR_VEC) != 0;
+  const double fact2 = p->alfi * p->gami * p->delt;
+  for (int f = 0; f < m->nface; ++f) {
+    if (!(m->fflag[f] & OVS_FACE_CONVH)) continue;
+    const int e = m->f2e[f] - 1, fo = m->face_or[f];
+    const double h = m->hconv[f], tinf = m->tinf[f];
+    double xl[NSHL_MAX][3], dl[NSHL_MAX][3], Tl[NSHL_MAX];
+    for (int a = 0; a < 4; ++a) {
+      const int idx = m->ien[cm(e, m->nelem, a)] - 1;
+      gather3(m->xg, N, idx, xl[a]); gather3(A->dg, N, idx, dl[a]);
+      Tl[a] = A->tg[idx];
+    }
+    double xT[4][4], RT[4];
+    memset(xT, 0, sizeof(xT));
+    memset(RT, 0, sizeof(RT));
+    for (int ig = 0; ig < 3; ++ig) {
+      double shl[NSHL_MAX], shg[NSHL_MAX][3], dxidx[3][3], nor[3];
+      const double detjgw = eval_faceshape_tet(fo, c_tri_mgp[fo - 1][ig], xl, dl, shl, shg, dxidx, nor) * c_tri_gw;
+      double Ti = 0.0;
+      for (int a = 0; a < 4; ++a) Ti += Tl[a] * shl[a];
+      const double q = h * (Ti - tinf);
+      if (mat)
+        for (int aa = 0; aa < 4; ++aa)
+          for (int bb = 0; bb < 4; ++bb) xT[aa][bb] += fact2 * shl[aa] * h * shl[bb] * detjgw;
+      if (vec)
+        for (int aa = 0; aa < 4; ++aa) RT[aa] -= shl[aa] * q * detjgw;
+    }
+    for (int aa = 0; aa < 4; ++aa) {  /* BCLhs_tem */
+      const int cc = m->ien[cm(e, m->nelem, aa)] - 1;
+      if (IBC(m, cc, 6) == 1) {
+        for (int t = 0; t < 4; ++t) { xT[aa][t] = 0.0; xT[t][aa] = 0.0; }
+        xT[aa][aa] = 1.0;
+        RT[aa] = 0.0;
+      }
+    }
+    if (mat)
+      for (int a = 0; a < 4; ++a) {
+        const int i = m->ien[cm(e, m->nelem, a)] - 1;
+        const int cc = m->col[i], n = m->col[i + 1] - cc;
+        for (int b = 0; b < 4; ++b) {
+          const int locn = orc_sparse_mat_loc(m->row + (cc - 1), n, m->ien[cm(e, m->nelem, b)]);
+          S->TEM[(size_t)(locn + cc - 1) - 1] += xT[a][b];
+        }
+      }
+    if (vec)
+      for (int a = 0; a < 4; ++a) S->rhstem[m->ien[cm(e, m->nelem, a)] - 1] += RT[a];
+  }
+}
+
 /* assembleNavSto src/assembleNavSto.f90:4-72 (single rank: commu is the
- * identity; the face assemblies are no-ops without BCugType==2) */
+ * identity); the face assemblies :55-61 act on the faces flagged
+ * OVS_FACE_WEAK (boundaries with BCugType == 2) */
 double orc_assemble_navsto(const orc_mesh* m, const ovs_params* p,
                            const orc_state* s, orc_system* S, int tensor_flag) {
   const size_t N = (size_t)m->nnode, K = (size_t)m->icnt;
@@ -925,11 +1195,18 @@ double orc_assemble_navsto(const orc_mesh* m, const ovs_params* p,
     memset(S->D1, 0, sizeof(double) * 3 * K); memset(S->M, 0, sizeof(double) * K);
   }
   double cfl = orc_elmloop_ns(m, p, &b.a, S, tensor_flag, 0, m->nelem);
+  orc_face_ns(m, p, &b.a, S, tensor_flag, 1);
   free(b.mem);
   return cfl;
 }
 
-/* assembleQuenching src/solveQuenching.f90:4-117 */
+/* assembleQuenching src/solveQuenching.f90:4-117.  Its face calls (:75-95)
+ * name two routines the reference does not define (FaceAssembly_NS_weak_CF,
+ * FaceAssembly_ConvectiveH) and pass 11 arguments to the 8-argument
+ * FaceAssembly_NS_outflow; here the NS+VOF pass runs the defined weak and
+ * outflow face routines on the velocity/pressure blocks (every element a
+ * target: the quench pass has no subdomain flag) and the temperature pass
+ * the convective heat term. */
 double orc_assemble_quenching(const orc_mesh* m, const ovs_params* p,
                               const orc_state* s, orc_system* S,
                               int tensor_flag, int field_flag) {
@@ -949,9 +1226,13 @@ double orc_assemble_quenching(const orc_mesh* m, const ovs_params* p,
     for (int t = 0; t < 9; ++t) if (arr[t]) memset(arr[t], 0, sizeof(double) * w[t] * K);
   }
   double cfl = 0.0;
-  if (field_flag & 3) cfl = orc_elmloop_nsvof(m, p, &b.a, S, tensor_flag, 0, m->nelem);
+  if (field_flag & 3) {
+    cfl = orc_elmloop_nsvof(m, p, &b.a, S, tensor_flag, 0, m->nelem);
+    orc_face_ns(m, p, &b.a, S, tensor_flag, 0);
+  }
   if (field_flag & 4) {
     double c2 = orc_elmloop_tem(m, p, &b.a, S, tensor_flag, 0, m->nelem);
+    orc_face_convh(m, p, &b.a, S, tensor_flag);
     if (!(field_flag & 3)) cfl = c2;
   }
   free(b.mem);

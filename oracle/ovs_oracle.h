@@ -33,6 +33,14 @@ typedef struct orc_mesh {
   const int* row;     /* (icnt)    */
   int icnt;
   int quench_literal; /* 1: literal signature-mismatch semantics (VOF frozen) */
+  /* boundary faces in the reference's loop order (boundary b = 1..NBOUND,
+   * then the faces of bound(b)); nface = 0: no face assembly */
+  int nface;
+  const int* f2e;      /* owning element, 1-based (bound(b)%F2E)   */
+  const int* face_or;  /* face orientation 1..4 (bound(b)%FACE_OR) */
+  const int* fflag;    /* OVS_FACE_WEAK | OVS_FACE_CONVH           */
+  const double* hconv; /* heat transfer coefficient per face       */
+  const double* tinf;  /* ambient temperature per face             */
 } orc_mesh;
 
 /* nodal state, module aAdjKeep (src/modules.f90:235-320) */
@@ -71,6 +79,13 @@ double orc_elmloop_nsvof(const orc_mesh* m, const ovs_params* p,
 double orc_elmloop_tem(const orc_mesh* m, const ovs_params* p,
                        const orc_state* a, orc_system* sys, int tensor_flag,
                        int e0, int e1);
+/* face assemblies on the alpha-stage arrays `a` (FaceAssembly_NS_weak then
+ * FaceAssembly_NS_outflow, src/FaceAssembly_weak.f90:4-409; the convective
+ * heat term on the temperature system) */
+void orc_face_ns(const orc_mesh* m, const ovs_params* p, const orc_state* a,
+                 orc_system* sys, int tensor_flag, int use_subdomain);
+void orc_face_convh(const orc_mesh* m, const ovs_params* p, const orc_state* a,
+                    orc_system* sys, int tensor_flag);
 void orc_alpha_stage(int nnode, const ovs_params* p, const orc_state* s,
                      orc_state* a);
 

@@ -28,7 +28,9 @@ def build() -> Path:
 class OrcMesh(C.Structure):
     _fields_ = [("nnode", C.c_int), ("nelem", C.c_int), ("nshl", C.c_int), ("nibc", C.c_int),
                 ("xg", _dp), ("ien", _ip), ("elm_id", _ip), ("ibc", _ip), ("col", _ip),
-                ("row", _ip), ("icnt", C.c_int), ("quench_literal", C.c_int)]
+                ("row", _ip), ("icnt", C.c_int), ("quench_literal", C.c_int),
+                ("nface", C.c_int), ("f2e", _ip), ("face_or", _ip), ("fflag", _ip), ("hconv", _dp),
+                ("tinf", _dp)]
 
 
 _STATE = ["dg", "dgold", "ug", "ugold", "acg", "acgold", "ugm", "ugmold", "acgm", "acgmold",
@@ -130,6 +132,17 @@ class OracleCase:
         self.mesh = OrcMesh(self.N, self.E, self.nshl, self.ibc.shape[1], _d(self.xg), _i(self.ien),
                             _i(self.elm), _i(self.ibc), _i(self.col), _i(self.row), self.icnt,
                             1 if literal else 0)
+        bf = getattr(case, "bfaces", None)
+        if bf is not None and len(bf.f2e):
+            self._faces = (np.ascontiguousarray(bf.f2e, dtype=np.int32),
+                           np.ascontiguousarray(bf.face_or, dtype=np.int32),
+                           np.ascontiguousarray(bf.flags, dtype=np.int32),
+                           np.ascontiguousarray(bf.hconv, dtype=np.float64),
+                           np.ascontiguousarray(bf.tinf, dtype=np.float64))
+            f2e, fo, fl, hc, ti = self._faces
+            self.mesh.nface = len(f2e)
+            self.mesh.f2e, self.mesh.face_or, self.mesh.fflag = _i(f2e), _i(fo), _i(fl)
+            self.mesh.hconv, self.mesh.tinf = _d(hc), _d(ti)
         self.params = to_ovs_params(case.params)
         self.state_arrays = {n: np.asfortranarray(case.state[n], dtype=np.float64).copy(order="F")
                              for n in _STATE}

@@ -102,6 +102,8 @@ class Context:
         ctx.set_params(case.params)
         ctx.set_ibc(case.ibc)
         ctx.set_state(case.state)
+        if case.bfaces is not None:
+            ctx.set_faces(case.bfaces)
         return ctx
 
     # ----------------------------------------------------------------- mesh
@@ -134,6 +136,19 @@ class Context:
     def set_ibc(self, ibc: np.ndarray):
         a = _i32(ibc)
         F.check(self.lib.ovs_set_ibc(self.h, _iptr(a), a.shape[1]), "ovs_set_ibc")
+
+    def set_faces(self, bf):
+        """Boundary faces for the face assemblies (mesh.BoundaryFaces, or None
+        to clear): FaceAssembly_NS_weak / _outflow on OVS_FACE_WEAK faces and
+        the convective heat term on OVS_FACE_CONVH faces."""
+        if bf is None or len(bf.f2e) == 0:
+            F.check(self.lib.ovs_set_faces(self.h, 0, None, None, None, None, None), "ovs_set_faces")
+            return
+        f2e, fo, fl = _i32(bf.f2e), _i32(bf.face_or), _i32(bf.flags)
+        hc = np.ascontiguousarray(bf.hconv, dtype=np.float64)
+        ti = np.ascontiguousarray(bf.tinf, dtype=np.float64)
+        F.check(self.lib.ovs_set_faces(self.h, len(f2e), _iptr(f2e), _iptr(fo), _iptr(fl), _dptr(hc), _dptr(ti)),
+                "ovs_set_faces")
 
     def set_field(self, name: str, arr: np.ndarray):
         a = _f64(arr)

@@ -1281,6 +1281,7 @@ int ovs_assemble_impl(ovs_ctx* c, int kernel, int tensor_flag, int prec, double*
   SumArgs sa;
   fill_args(c, prec, S, tensor_flag, a, sa);
   if ((st = dispatch_assemble(c, kernel, prec, a, sa))) return st;
+  if ((st = ovs_faces_assemble(c, kernel, prec, a.mat, a.vec))) return st;
   if (a.mat) S.have_mat = true;
   if (a.vec) S.have_rhs = true;
   int hflags[4];
@@ -1293,6 +1294,7 @@ int ovs_assemble_impl(ovs_ctx* c, int kernel, int tensor_flag, int prec, double*
     memcpy(&v, &hcfl, sizeof(v));
     *cfl = v;
   }
+  if (hflags[3]) return OVS_ERR_PATTERN;
   if (hflags[1]) return OVS_ERR_NONFINITE;
   if (hflags[0]) return OVS_WARN_NEG_DETJ;
   return OVS_OK;
@@ -1301,6 +1303,7 @@ int ovs_assemble_impl(ovs_ctx* c, int kernel, int tensor_flag, int prec, double*
 int ovs_residual_vjp_impl(ovs_ctx* c, int kernel, const double* cot_host, double* grad_host) {
   if (!c->have_pattern || !c->have_params) return OVS_ERR_STATE;
   if (c->nshl != 4) return OVS_ERR_ARG;   // the adjoint covers the tet routines
+  if (c->face_flags_all) return OVS_ERR_STATE;   // face terms are not differentiated
   if (kernel != OVS_ASM_NSVOF && kernel != OVS_ASM_TEM) return OVS_ERR_ARG;
   if (!cot_host || !grad_host) return OVS_ERR_ARG;
   const int tem = kernel == OVS_ASM_TEM;

@@ -235,6 +235,7 @@ int ovs_destroy(ovs_ctx* c) {
   if (!c) return OVS_OK;
   cudaSetDevice(c->device);
   if (c->stream) cudaStreamSynchronize(c->stream);
+  ovs_faces_free(c);
   void* ptrs[] = {c->ien, c->elm_id, c->ibc, c->rowptr, c->colidx, c->diag, c->n2e_ptr, c->n2e, c->n2s, c->tmap, c->vals_t, c->vjp_cot, c->vjp_ge, c->vjp_grad,
                   c->rec[0], c->rec[1], c->esum[0], c->esum[1], c->gm, c->basis[0], c->basis[1], c->work64, c->work32, c->wvec, c->coop_part,
                   c->flags, c->cfl_bits};
@@ -362,6 +363,12 @@ int ovs_set_ibc(ovs_ctx* c, const int* ibc, int nibc) {
   OVS_CUDA_TRY(cudaFreeAsync(tmp, s));
   OVS_CUDA_TRY(cudaStreamSynchronize(s));
   return OVS_OK;
+}
+
+int ovs_set_faces(ovs_ctx* c, int nface, const int* f2e, const int* face_or, const int* flags,
+                  const double* hconv, const double* tinf) {
+  if (!c) return OVS_ERR_ARG;
+  return ovs_faces_set_impl(c, nface, f2e, face_or, flags, hconv, tinf);
 }
 
 int ovs_set_field(ovs_ctx* c, int field, const double* host) {

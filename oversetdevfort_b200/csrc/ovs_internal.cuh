@@ -86,6 +86,15 @@ struct ovs_ctx {
                              // (one word per entry for tets, two for hexahedra)
   int nnz = 0;
   int max_deg = 0, max_elem = 0;
+  // boundary faces of the face assemblies (ovs_set_faces)
+  int nface = 0, nfnode = 0, face_flags_all = 0;
+  int* face_e = nullptr;      // nface owning elements, 0-based
+  int* face_info = nullptr;   // nface: (FACE_OR - 1) | flags << 2
+  double* face_h = nullptr;   // nface pairs (h, T_inf)
+  int* fnode = nullptr;       // nfnode nodes touched by a face element, ascending
+  int* fnode_ptr = nullptr;   // nfnode + 1
+  int* fnode_ent = nullptr;   // 4 nface entries (face << 2) | local node, ascending face per node
+  void* fbuf[2] = {nullptr, nullptr};   // per-face element arrays, per precision
   // nodal state (FP64, reference layout)
   double* field[OVS_F_COUNT] = {};
   // alpha-stage node records (16 values per node), per precision
@@ -105,7 +114,7 @@ struct ovs_ctx {
   double* wvec = nullptr;                // FP64 vector under orthogonalization
   double* coop_part = nullptr;           // partial sums of the cooperative Arnoldi kernels
   bool arnoldi_fused = false;            // one-launch Arnoldi variant (env OVS_ARNOLDI_FUSED=1)
-  // status words: [0] negative DetJ count, [1] non-finite flag
+  // status words: [0] negative DetJ count, [1] non-finite flag, [3] face column missing from a row
   int* flags = nullptr;
   unsigned long long* cfl_bits = nullptr;
   // pinned host mirror
@@ -128,6 +137,12 @@ int ovs_pattern_to_host(ovs_ctx* c, int* col, int* row);
 // assemble.cu
 int ovs_assemble_impl(ovs_ctx* c, int kernel, int tensor_flag, int prec,
                       double* cfl);
+
+// faces.cu
+int ovs_faces_set_impl(ovs_ctx* c, int nface, const int* f2e, const int* face_or, const int* flags,
+                       const double* hconv, const double* tinf);
+int ovs_faces_assemble(ovs_ctx* c, int kernel, int prec, int mat, int vec);
+void ovs_faces_free(ovs_ctx* c);
 
 // spmv.cu / gmres.cu
 int ovs_precond_setup(ovs_ctx* c, int sys, int prec);

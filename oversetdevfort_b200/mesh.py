@@ -98,6 +98,64 @@ def box_hex(nx, ny, nz, lx=1.0, ly=1.0, lz=1.0) -> Mesh:
     return Mesh(xg, ien, elm, faces, (nx, ny, nz), (lx, ly, lz))
 
 
+# element-local nodes (0-based) of the tet face with FACE_OR = 1..4, in the
+# order eval_faceshape_tet takes them (src/eval_shape_FEM.f90:90-106)
+TET_FACE_NODES = ((1, 2, 0), (3, 2, 1), (0, 2, 3), (1, 0, 3))
+
+
+@dataclass
+class BoundaryFaces:
+    """Boundary faces in the reference's loop order (boundary b = 1..NBOUND,
+    then the faces of bound(b)): owning element (1-based, bound(b)%F2E), its
+    FACE_OR, OVS_FACE_* flags and, for OVS_FACE_CONVH, the heat transfer
+    coefficient and ambient temperature."""
+    f2e: np.ndarray
+    face_or: np.ndarray
+    flags: np.ndarray
+    hconv: np.ndarray
+    tinf: np.ndarray
+
+
+def box_boundary_faces(m: Mesh) -> list:
+    """(F2E, FACE_OR) of the triangles on each box face (x0, x1, y0, y1, z0,
+    z1), ordered by element then orientation (tets only)."""
+    if m.nshl != 4:
+        raise ValueError("face assembly covers linear tets")
+    ien0 = np.asarray(m.ien, dtype=np.int64) - 1
+    out = []
+    for nodes in m.faces:
+        on = np.zeros(m.nnode, dtype=bool)
+        on[nodes] = True
+        es, fos = [], []
+        for fo, loc in enumerate(TET_FACE_NODES, 1):
+            e = np.nonzero(on[ien0[:, list(loc)]].all(axis=1))[0]
+            es.append(e)
+            fos.append(np.full(e.size, fo, dtype=np.int32))
+        e, fo = np.concatenate(es), np.concatenate(fos)
+        order = np.lexsort((fo, e))
+        out.append(((e[order] + 1).astype(np.int32), fo[order]))
+    return out
+
+
+def face_set(m: Mesh, weak=(), convective=None) -> BoundaryFaces:
+    """Faces of a box mesh for the face assemblies.  `weak`: box face ids
+    (1..6 = x0, x1, y0, y1, z0, z1) with BCugType == 2; `convective`:
+    {face id: (h, T_inf)}.  Boundaries in id order, as NBOUND loops."""
+    convective = convective or {}
+    parts = []
+    for fid, (f2e, fo) in enumerate(box_boundary_faces(m), 1):
+        fl = (F.OVS_FACE_WEAK if fid in weak else 0) | (F.OVS_FACE_CONVH if fid in convective else 0)
+        if not fl:
+            continue
+        h, tinf = convective.get(fid, (0.0, 0.0))
+        n = f2e.size
+        parts.append((f2e, fo, np.full(n, fl, np.int32), np.full(n, h), np.full(n, tinf)))
+    if not parts:
+        z = np.zeros(0)
+        return BoundaryFaces(z.astype(np.int32), z.astype(np.int32), z.astype(np.int32), z, z)
+    return BoundaryFaces(*(np.concatenate(c) for c in zip(*parts)))
+
+
 def expected_nnz_kuhn(nx, ny, nz) -> int:
     """Closed-form nnz of the Kuhn-split pattern: every node couples to itself
     and to the neighbours along the 7 edge directions +-{x,y,z,xy,xz,yz,xyz}
@@ -127,6 +185,7 @@ class Case:
     gmres_tol: float = 1e-6
     newton_iters: int = 1
     extra: dict = field(default_factory=dict)
+    bfaces: "BoundaryFaces | None" = None   # faces for the face assemblies
 
 
 def genalpha(rhoinf: float) -> dict:

@@ -13,6 +13,7 @@ from dataclasses import dataclass, field
 
 import numpy as np
 
+from . import _ffi as F
 from . import mesh as M
 
 
@@ -137,11 +138,19 @@ def write_part(path, pm: PartMesh, fem_flag: int = 1) -> None:
 
 def part_from_mesh(m: "M.Mesh", face_ids=(1, 2, 3, 4, 5, 6)) -> PartMesh:
     """A PartMesh of one of this package's box meshes: node ids 0, one
-    boundary per box face (its nodes; faces are not enumerated, NFACE = 0)."""
+    boundary per box face with its nodes and, for tets, its triangles
+    (FACE_IEN, F2E, FACE_OR); hexahedral boundaries list nodes only."""
     N, E = m.nnode, m.nelem
-    bounds = [Boundary(int(fid), np.zeros((0, 3 if m.nshl == 4 else 4), np.int32), np.zeros(0, np.int32),
-                       np.zeros(0, np.int32), (np.asarray(nodes) + 1).astype(np.int32))
-              for fid, nodes in zip(face_ids, m.faces)]
+    ien0 = np.asarray(m.ien, dtype=np.int32)
+    if m.nshl == 4:
+        tri = M.box_boundary_faces(m)
+        fien = [ien0[f2e - 1][np.arange(f2e.size)[:, None], np.asarray(M.TET_FACE_NODES)[fo - 1]]
+                for f2e, fo in tri]
+    else:
+        tri = [(np.zeros(0, np.int32), np.zeros(0, np.int32))] * len(m.faces)
+        fien = [np.zeros((0, 4), np.int32)] * len(m.faces)
+    bounds = [Boundary(int(fid), fi.astype(np.int32), f2e, fo, (np.asarray(nodes) + 1).astype(np.int32))
+              for fid, nodes, (f2e, fo), fi in zip(face_ids, m.faces, tri, fien)]
     return PartMesh(3, m.nshl, 3 if m.nshl == 4 else 4, np.asarray(m.xg, dtype=np.float64),
                     np.zeros(N, np.int32), np.full(E, m.nshl, np.int32), np.asarray(m.ien, dtype=np.int32),
                     np.asarray(m.elm_id, dtype=np.int32), bounds)
@@ -157,6 +166,27 @@ def mesh_from_part(pm: PartMesh) -> "M.Mesh":
     faces = [np.sort(b.bnodes.astype(np.int64) - 1) for b in pm.bounds]
     return M.Mesh(np.asfortranarray(pm.xg[:, :3]), np.asfortranarray(pm.ien.astype(np.int32)),
                   pm.elm_id.astype(np.int32).copy(), faces, None, tuple(float(v) for v in (hi - lo)))
+
+
+def faces_from_part(pm: PartMesh, weak=(), convective=None) -> "M.BoundaryFaces":
+    """The face set of a partition for the face assemblies: the boundary
+    faces (F2E, FACE_OR) in file order, as the reference's NBOUND loop visits
+    them.  `weak`: FACE_IDs with BCugType == 2; `convective`: {FACE_ID:
+    (h, T_inf)} for the convective heat term."""
+    convective = convective or {}
+    parts = []
+    for b in pm.bounds:
+        fl = (F.OVS_FACE_WEAK if b.face_id in weak else 0) | (F.OVS_FACE_CONVH if b.face_id in convective else 0)
+        if not fl or b.f2e.size == 0:
+            continue
+        h, tinf = convective.get(b.face_id, (0.0, 0.0))
+        n = b.f2e.size
+        parts.append((b.f2e.astype(np.int32), b.face_or.astype(np.int32), np.full(n, fl, np.int32),
+                      np.full(n, float(h)), np.full(n, float(tinf))))
+    if not parts:
+        z = np.zeros(0)
+        return M.BoundaryFaces(z.astype(np.int32), z.astype(np.int32), z.astype(np.int32), z, z)
+    return M.BoundaryFaces(*(np.concatenate(c) for c in zip(*parts)))
 
 
 # the records of a restart, in file order, and the state arrays they fill

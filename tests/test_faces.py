@@ -1,0 +1,141 @@
+"""Face assemblies in the oracle (CPU): the box-face enumeration, and known
+answers that pin the face rule, outward normals and surface Jacobian of
+eval_faceshape_tet, the weak-Dirichlet coupling blocks and backflow terms
+(FaceAssembly_NS_weak + FaceAssembly_NS_outflow) and the convective heat
+term, on uniform states where the face integrals have closed forms."""
+import numpy as np
+import pytest
+
+from oversetdevfort_b200 import _ffi as F
+from oversetdevfort_b200 import mesh as M
+
+LX, LY, LZ = 1.5, 1.0, 2.0
+NORMALS = [(-1, 0, 0), (1, 0, 0), (0, -1, 0), (0, 1, 0), (0, 0, -1), (0, 0, 1)]
+AREAS = [LY * LZ, LY * LZ, LX * LZ, LX * LZ, LX * LY, LX * LY]
+
+
+def test_box_face_enumeration():
+    nx, ny, nz = 3, 2, 4
+    m = M.box_tet(nx, ny, nz, LX, LY, LZ)
+    fs = M.box_boundary_faces(m)
+    assert [f.size for f, _ in fs] == [2 * ny * nz] * 2 + [2 * nx * nz] * 2 + [2 * nx * ny] * 2
+    ien0 = np.asarray(m.ien) - 1
+    for (f2e, fo), nodes in zip(fs, m.faces):
+        assert np.all(np.diff(f2e) >= 0)
+        for e, o in zip(f2e, fo):
+            loc = M.TET_FACE_NODES[o - 1]
+            assert np.isin(ien0[e - 1, list(loc)], nodes).all()
+    bf = M.face_set(m, weak=(1, 6), convective={6: (5.0, 300.0)})
+    assert len(bf.f2e) == 2 * (2 * ny * nz) // 2 + 2 * nx * ny
+    assert set(bf.flags.tolist()) == {F.OVS_FACE_WEAK, F.OVS_FACE_WEAK | F.OVS_FACE_CONVH}
+
+
+def _uniform_case(kernel, U, Um, p0, T0, **par):
+    m = M.box_tet(3, 2, 4, LX, LY, LZ)
+    N = m.nnode
+    st = M.empty_state(N)
+    for n in ("ug", "ugold"):
+        st[n][:] = U
+    for n in ("ugm", "ugmold"):
+        st[n][:] = Um
+    st["pg"][:] = p0
+    for n in ("tg", "tgold"):
+        st[n][:] = T0
+    p = M.base_params(**par)
+    ibc = np.asfortranarray(np.zeros((N, 8), dtype=np.int32))
+    return M.Case("uniform", m, p, st, ibc, kernel)
+
+
+def _with_and_without(oracle, case, bf, kind):
+    out = []
+    for faces in (None, bf):
+        case.bfaces = faces
+        oc = oracle.OracleCase(case)
+        if kind == "ns":
+            oc.assemble_navsto(6)
+        else:
+            oc.assemble_quenching(6, 3 if kind == "nsvof" else 4)
+        out.append(oc.system(kind))
+    return out
+
+
+@pytest.mark.parametrize("kind", ["ns", "nsvof"])
+@pytest.mark.parametrize("fid", range(1, 7))
+def test_weak_face_known_answers(oracle, kind, fid):
+    U, Um, p0 = np.array([0.3, -0.2, 0.5]), np.array([0.05, 0.1, -0.02]), 2.5
+    kernel = F.OVS_ASM_NS if kind == "ns" else F.OVS_ASM_NSVOF
+    case = _uniform_case(kernel, U, Um, p0, 350.0, mua=0.0, muw=0.0)
+    bf = M.face_set(case.mesh, weak=(fid,))
+    s0, s1 = _with_and_without(oracle, case, bf, kind)
+    par = case.params
+    fact2 = par["alfi"] * par["gami"] * par["delt"]
+    n, area = np.array(NORMALS[fid - 1], dtype=float), AREAS[fid - 1]
+    dG = (s1["G"] - s0["G"]).sum(axis=0)
+    dD = (s1["D1"] - s0["D1"]).sum(axis=0)
+    np.testing.assert_allclose(dG, fact2 * area * n, atol=1e-14)
+    np.testing.assert_allclose(dD, -fact2 * area * n, atol=1e-14)
+    drhs = (s1["rhs"] - s0["rhs"]).sum(axis=0)
+    w = U - Um
+    uneg = min(float(w @ n), 0.0)
+    rho = par["rhoa"]
+    # weak: -int (p n + (tauB - rho u_n^-) w) with mu = 0 (tauB = 0); outflow: +int rho u_n^- w
+    # (differences of residuals that also hold the element terms: roundoff of their size)
+    np.testing.assert_allclose(drhs[:3], area * (-p0 * n + 2.0 * rho * uneg * w), rtol=1e-10, atol=1e-10)
+    np.testing.assert_allclose(drhs[3], area * float(w @ n), rtol=1e-10, atol=1e-12)
+    # backflow on the velocity diagonal: -2 fact2 rho u_n^- area per component
+    dK = (s1["K11"] - s0["K11"]).sum(axis=0)
+    np.testing.assert_allclose(dK[[0, 4, 8]], -2.0 * fact2 * rho * uneg * area, atol=1e-14)
+    np.testing.assert_allclose(dK[[1, 2, 3, 5, 6, 7]], 0.0, atol=1e-14)
+    if kind == "nsvof":
+        for b in ("LS", "LSU", "ULS", "PLS"):
+            np.testing.assert_array_equal(s1[b], s0[b])
+        np.testing.assert_array_equal(s1["rhs"][:, 4], s0["rhs"][:, 4])
+
+
+@pytest.mark.parametrize("fid", [1, 4, 5])
+def test_convective_heat_known_answers(oracle, fid):
+    T0, h, tinf = 350.0, 12.5, 290.0
+    case = _uniform_case(F.OVS_ASM_NSVOF, np.zeros(3), np.zeros(3), 0.0, T0)
+    bf = M.face_set(case.mesh, convective={fid: (h, tinf)})
+    s0, s1 = _with_and_without(oracle, case, bf, "tem")
+    par = case.params
+    fact2 = par["alfi"] * par["gami"] * par["delt"]
+    area = AREAS[fid - 1]
+    # differences of systems that also hold the element terms (rho cp ~ 4e6):
+    # roundoff of their size, not of the face terms'
+    eps_m = 1e-14 * np.abs(s0["TEM"]).max() * len(s0["TEM"])
+    eps_r = 1e-14 * np.abs(s0["rhs"]).max() * len(s0["rhs"])
+    np.testing.assert_allclose((s1["TEM"] - s0["TEM"]).sum(), fact2 * h * area, atol=eps_m)
+    np.testing.assert_allclose((s1["rhs"] - s0["rhs"]).sum(), -h * (T0 - tinf) * area, atol=eps_r)
+    # the convective term is a weighted face mass matrix: symmetric, couples face nodes only
+    oc = oracle.OracleCase(case)
+    col, row = oc.col.astype(np.int64) - 1, oc.row.astype(np.int64) - 1
+    dT = s1["TEM"] - s0["TEM"]
+    on = np.zeros(case.mesh.nnode, dtype=bool)
+    on[case.mesh.faces[fid - 1]] = True
+    for i in range(case.mesh.nnode):
+        for k in range(col[i], col[i + 1]):
+            j = row[k]
+            if abs(dT[k]) > 1e-3 * fact2 * h * area / len(case.mesh.faces[fid - 1]):
+                assert on[i] and on[j]
+                kt = col[j] + np.nonzero(row[col[j]:col[j + 1]] == i)[0][0]
+                assert abs(dT[kt] - dT[k]) <= 1e-13 * np.abs(s0["TEM"]).max()
+
+
+def test_constrained_nodes_get_face_diagonal(oracle):
+    """BCLhs_3D runs on each face routine's arrays too: every weak face
+    touching a node with a velocity Dirichlet flag adds 1 to that node's
+    diagonal once in FaceAssembly_NS_weak and once in _outflow."""
+    case = _uniform_case(F.OVS_ASM_NS, np.array([0.1, 0.0, 0.0]), np.zeros(3), 1.0, 300.0)
+    node = int(case.mesh.faces[4][3])
+    case.ibc[node, 0] = 1
+    bf = M.face_set(case.mesh, weak=(5,))
+    s0, s1 = _with_and_without(oracle, case, bf, "ns")
+    oc = oracle.OracleCase(case)
+    col, row = oc.col.astype(np.int64) - 1, oc.row.astype(np.int64) - 1
+    kd = col[node] + np.nonzero(row[col[node]:col[node + 1]] == node)[0][0]
+    f2e = bf.f2e - 1
+    touching = np.isin(np.asarray(case.mesh.ien)[f2e] - 1, node).any(axis=1).sum()
+    assert touching > 0
+    assert s1["K11"][kd, 0] - s0["K11"][kd, 0] == 2 * touching
+    assert np.all(s1["rhs"][node, 0] == 0.0)

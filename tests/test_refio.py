@@ -89,3 +89,20 @@ def test_restart_round_trip_and_predictor(tmp_path):
     np.testing.assert_array_equal(s2["pg"], st["pg"])
     np.testing.assert_allclose(s2["acg"], (0.8 - 1.0) / 0.8 * st["acg"])
     np.testing.assert_array_equal(s2["tg"], st["tgold"])
+
+
+def test_part_faces_round_trip_to_face_set(tmp_path):
+    """Boundary triangles written to part.dat (FACE_IEN, F2E, FACE_OR) come
+    back as the same face set the box enumeration gives, in file order."""
+    m = M.box_tet(3, 2, 2, 1.0, 0.5, 2.0)
+    pm = refio.part_from_mesh(m)
+    path = tmp_path / "part4.dat"
+    refio.write_part(path, pm)
+    back = refio.read_part(path)
+    for b, nodes in zip(back.bounds, m.faces):
+        assert np.isin(b.face_ien - 1, nodes).all()
+    bf = refio.faces_from_part(back, weak=(2, 6), convective={5: (4.0, 300.0)})
+    ref = M.face_set(m, weak=(2, 6), convective={5: (4.0, 300.0)})
+    for a, b in zip((bf.f2e, bf.face_or, bf.flags, bf.hconv, bf.tinf),
+                    (ref.f2e, ref.face_or, ref.flags, ref.hconv, ref.tinf)):
+        np.testing.assert_array_equal(a, b)
