@@ -206,6 +206,40 @@ int ovs_set_ibc(ovs_ctx* ctx, const int* ibc, int nibc);
  * active (face terms are not differentiated). */
 int ovs_set_faces(ovs_ctx* ctx, int nface, const int* f2e, const int* face_or,
                   const int* flags, const double* hconv, const double* tinf);
+
+/* Boundary data of setBCs_NSVOF / setBCs_Tem (src/setBCs.f90:172-278) as the
+ * reference holds it: the node sets of the boundaries and the tables read by
+ * src/param.f90:296-340.  setBCs reads the *Type tables by FACE_ID and the
+ * *Valu tables by boundary number; both are kept. */
+typedef struct ovs_bc_spec {
+  int nbound;                 /* NBOUND                                          */
+  int ntype;                  /* rows of the *Type tables (NBOUND in the reference) */
+  const int* face_id;         /* bound(b)%FACE_ID, nbound values in 1..ntype     */
+  const int* bnode_ptr;       /* nbound + 1 offsets into bnodes, bnode_ptr[0] = 0 */
+  const int* bnodes;          /* bound(b)%BNODES concatenated, 1-based node ids  */
+  const int* node_id;         /* NodeID (N values), or NULL when no node is 101  */
+  const int* bcug_type;       /* BCugType, column-major (ntype, 3)              */
+  const double* bcug_valu;    /* BCugValu, column-major (nbound, 3)             */
+  const int* bcphig_type;     /* BCphigType (ntype)                             */
+  const double* bcphig_valu;  /* BCphigValu (nbound)                            */
+  const int* bctg_type;       /* BCTgType (ntype)                               */
+  const double* bctg_valu;    /* BCTgValu (nbound)                              */
+} ovs_bc_spec;
+
+/* Registers the boundary data (NULL clears it).  While it is set,
+ * ovs_quench_newton applies setBCs_NSVOF and setBCs_Tem where the
+ * reference's Newton routine calls them (src/solveFlow.f90:35-36 before the
+ * first residual, :58-60 at the top of every Newton iteration). */
+int ovs_set_bc_spec(ovs_ctx* ctx, const ovs_bc_spec* spec);
+
+/* which & 1: setBCs_NSVOF (IBC = 0; NodeID 101 -> IBC(1:5) = 1; Dirichlet
+ * velocity / VOF values with acg, rphig = ((v - vold) Dtgl + (gami - 1)
+ * rate_old) / gami); which & 2: setBCs_Tem (IBC(:,6) = 0; Dirichlet T, rTg).
+ * On the device state and IBC of the context. */
+int ovs_apply_bcs(ovs_ctx* ctx, int which);
+
+/* The context's IBC as an (N, nibc) column-major array of 0/1. */
+int ovs_get_ibc(ovs_ctx* ctx, int* ibc, int nibc);
 int ovs_set_field(ovs_ctx* ctx, int field, const double* host);
 int ovs_get_field(ovs_ctx* ctx, int field, double* host);
 

@@ -1177,6 +1177,54 @@ void orc_face_convh(const orc_mesh* m, const ovs_params* p, const orc_state* A,
   }
 }
 
+/* setBCs_NSVOF src/setBCs.f90:172-244 and setBCs_Tem :248-278.  The *Type
+ * tables are read by FACE_ID, the *Valu tables by boundary number (:212-216,
+ * :230-234, :266-268), as written; Dtgl = 1/Delt (src/param.f90:488). */
+void orc_set_bcs(int N, int nibc, int* ibc, const ovs_params* p, orc_state* s,
+                 const ovs_bc_spec* sp, int which) {
+  const double dtgl = 1.0 / p->delt, gami = p->gami;
+  const int nb = sp->nbound, nt = sp->ntype;
+  if (which & 1) {
+    for (size_t i = 0; i < (size_t)N * nibc; ++i) ibc[i] = 0;            /* IBC = 0 */
+    for (int i = 0; i < N; ++i)
+      if (sp->node_id && sp->node_id[i] == 101)
+        for (int c = 0; c < 5 && c < nibc; ++c) ibc[cm(i, N, c)] = 1;     /* :201-208 */
+    for (int b = 0; b < nb; ++b) {
+      const int fid = sp->face_id[b];
+      for (int d = 0; d < 3; ++d)
+        if (sp->bcug_type[cm(fid - 1, nt, d)] == 1)
+          for (int j = sp->bnode_ptr[b]; j < sp->bnode_ptr[b + 1]; ++j) {
+            const int k = sp->bnodes[j] - 1;
+            ibc[cm(k, N, d)] = 1;
+            s->ug[cm(k, N, d)] = sp->bcug_valu[cm(b, nb, d)];
+            s->acg[cm(k, N, d)] = ((s->ug[cm(k, N, d)] - s->ugold[cm(k, N, d)]) * dtgl +
+                                   (gami - 1.0) * s->acgold[cm(k, N, d)]) / gami;
+          }
+      if (sp->bcphig_type[fid - 1] == 1)
+        for (int j = sp->bnode_ptr[b]; j < sp->bnode_ptr[b + 1]; ++j) {
+          const int k = sp->bnodes[j] - 1;
+          if (nibc > 4) ibc[cm(k, N, 4)] = 1;
+          s->phig[k] = sp->bcphig_valu[b];
+          s->rphig[k] = ((s->phig[k] - s->phigold[k]) * dtgl + (gami - 1.0) * s->rphigold[k]) / gami;
+        }
+    }
+  }
+  if (which & 2) {
+    if (nibc > 5)
+      for (int i = 0; i < N; ++i) ibc[cm(i, N, 5)] = 0;                   /* IBC(:, 6) = 0 */
+    for (int b = 0; b < nb; ++b) {
+      const int fid = sp->face_id[b];
+      if (sp->bctg_type[fid - 1] == 1)
+        for (int j = sp->bnode_ptr[b]; j < sp->bnode_ptr[b + 1]; ++j) {
+          const int k = sp->bnodes[j] - 1;
+          if (nibc > 5) ibc[cm(k, N, 5)] = 1;
+          s->tg[k] = sp->bctg_valu[b];
+          s->rtg[k] = ((s->tg[k] - s->tgold[k]) * dtgl + (gami - 1.0) * s->rtgold[k]) / gami;
+        }
+    }
+  }
+}
+
 /* assembleNavSto src/assembleNavSto.f90:4-72 (single rank: commu is the
  * identity); the face assemblies :55-61 act on the faces flagged
  * OVS_FACE_WEAK (boundaries with BCugType == 2) */

@@ -86,6 +86,10 @@ void orc_face_ns(const orc_mesh* m, const ovs_params* p, const orc_state* a,
                  orc_system* sys, int tensor_flag, int use_subdomain);
 void orc_face_convh(const orc_mesh* m, const ovs_params* p, const orc_state* a,
                     orc_system* sys, int tensor_flag);
+/* setBCs_NSVOF (which & 1) and setBCs_Tem (which & 2), src/setBCs.f90:
+ * 172-278, on the state and on IBC (nnode, nibc) column-major */
+void orc_set_bcs(int nnode, int nibc, int* ibc, const ovs_params* p,
+                 orc_state* s, const ovs_bc_spec* sp, int which);
 void orc_alpha_stage(int nnode, const ovs_params* p, const orc_state* s,
                      orc_state* a);
 

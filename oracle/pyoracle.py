@@ -72,6 +72,8 @@ def load():
         getattr(lib, fn).argtypes = [C.POINTER(OrcMesh), pp, C.POINTER(OrcState), C.POINTER(OrcSystem),
                                      C.c_int, C.c_int, C.c_int]
         getattr(lib, fn).restype = C.c_double
+    from oversetdevfort_b200._ffi import OvsBcSpec
+    lib.orc_set_bcs.argtypes = [C.c_int, C.c_int, _ip, pp, C.POINTER(OrcState), C.POINTER(OvsBcSpec), C.c_int]
     lib.orc_alpha_stage.argtypes = [C.c_int, pp, C.POINTER(OrcState), C.POINTER(OrcState)]
     lib.orc_sparse_prod_up_3d.argtypes = [C.c_int, _ip, _ip, C.POINTER(OrcSystem), _dp, _dp, _dp, _dp]
     lib.orc_sparse_prod_ns_conv.argtypes = [C.c_int, _ip, _ip, C.POINTER(OrcSystem), _dp, _dp, _dp,
@@ -153,6 +155,14 @@ class OracleCase:
                     "PLS": np.zeros(K), "TEM": np.zeros(K), "rhsu": np.zeros((N, 3), order="F"),
                     "rhsp": np.zeros(N), "rhsls": np.zeros(N), "rhstem": np.zeros(N)}
         self.csys = OrcSystem(*[_d(self.sys[n]) for n in _SYS])
+
+    # ------------------------------------------------------- BC producers
+    def set_bcs(self, spec, which: int):
+        """setBCs_NSVOF (which & 1) / setBCs_Tem (which & 2) on this case's
+        state and IBC arrays."""
+        keep, cs = spec.to_c()
+        load().orc_set_bcs(self.N, self.ibc.shape[1], _i(self.ibc), C.byref(self.params), C.byref(self.state),
+                           C.byref(cs), which)
 
     # ----------------------------------------------------------- assembly
     def assemble_navsto(self, tensor_flag: int) -> float:

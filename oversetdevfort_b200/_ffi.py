@@ -52,7 +52,7 @@ EXPORTS = [
     "ovs_set_lhs_block", "ovs_spmv", "ovs_gmres", "ovs_solve", "ovs_newton_update",
     "ovs_residual_norms", "ovs_profile", "ovs_launch_count", "ovs_last_device_ms",
     "ovs_host_alloc", "ovs_host_free", "ovs_residual_vjp", "ovs_gmres_transposed", "ovs_quench_newton",
-    "ovs_quench_time_steps", "ovs_set_faces",
+    "ovs_quench_time_steps", "ovs_set_faces", "ovs_set_bc_spec", "ovs_apply_bcs", "ovs_get_ibc",
     "ovs_gmres_tem_noalloc",
 ]
 
@@ -70,6 +70,15 @@ class OvsParams(C.Structure):
     _fields_ = ([(n, C.c_double) for n in PARAM_DOUBLES] +
                 [("gravvec", C.c_double * 3), ("fluid_elm_id", C.c_int),
                  ("subdomain_flag", C.c_int), ("elm_id_set", C.c_int * 2)])
+
+
+class OvsBcSpec(C.Structure):
+    _fields_ = [("nbound", C.c_int), ("ntype", C.c_int), ("face_id", C.POINTER(C.c_int)),
+                ("bnode_ptr", C.POINTER(C.c_int)), ("bnodes", C.POINTER(C.c_int)),
+                ("node_id", C.POINTER(C.c_int)), ("bcug_type", C.POINTER(C.c_int)),
+                ("bcug_valu", C.POINTER(C.c_double)), ("bcphig_type", C.POINTER(C.c_int)),
+                ("bcphig_valu", C.POINTER(C.c_double)), ("bctg_type", C.POINTER(C.c_int)),
+                ("bctg_valu", C.POINTER(C.c_double))]
 
 
 class OvsNewtonOpts(C.Structure):
@@ -122,6 +131,9 @@ def load(path: str | os.PathLike | None = None) -> C.CDLL:
         "ovs_set_params": ([vp, C.POINTER(OvsParams)], C.c_int),
         "ovs_set_ibc": ([vp, ip, C.c_int], C.c_int),
         "ovs_set_faces": ([vp, C.c_int, ip, ip, ip, dp, dp], C.c_int),
+        "ovs_set_bc_spec": ([vp, C.POINTER(OvsBcSpec)], C.c_int),
+        "ovs_apply_bcs": ([vp, C.c_int], C.c_int),
+        "ovs_get_ibc": ([vp, ip, C.c_int], C.c_int),
         "ovs_set_field": ([vp, C.c_int, dp], C.c_int),
         "ovs_get_field": ([vp, C.c_int, dp], C.c_int),
         "ovs_assemble": ([vp, C.c_int, C.c_int, C.c_int, dp], C.c_int),

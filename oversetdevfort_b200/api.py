@@ -150,6 +150,24 @@ class Context:
         F.check(self.lib.ovs_set_faces(self.h, len(f2e), _iptr(f2e), _iptr(fo), _iptr(fl), _dptr(hc), _dptr(ti)),
                 "ovs_set_faces")
 
+    def set_bc_spec(self, spec):
+        """Boundary data of setBCs_NSVOF / setBCs_Tem (mesh.BcSpec, or None to
+        clear); applied by quench_newton where the reference calls them."""
+        if spec is None:
+            F.check(self.lib.ovs_set_bc_spec(self.h, None), "ovs_set_bc_spec")
+            return
+        keep, cs = spec.to_c()
+        F.check(self.lib.ovs_set_bc_spec(self.h, C.byref(cs)), "ovs_set_bc_spec")
+
+    def apply_bcs(self, which: int = 3):
+        """setBCs_NSVOF (which & 1) and setBCs_Tem (which & 2) on the device."""
+        F.check(self.lib.ovs_apply_bcs(self.h, which), "ovs_apply_bcs")
+
+    def get_ibc(self, nibc: int = 8) -> np.ndarray:
+        out = np.zeros((self.N, nibc), dtype=np.int32, order="F")
+        F.check(self.lib.ovs_get_ibc(self.h, _iptr(out), nibc), "ovs_get_ibc")
+        return out
+
     def set_field(self, name: str, arr: np.ndarray):
         a = _f64(arr)
         F.check(self.lib.ovs_set_field(self.h, F.FIELD_ID[name], _dptr(a)), f"ovs_set_field({name})")

@@ -236,6 +236,7 @@ int ovs_destroy(ovs_ctx* c) {
   cudaSetDevice(c->device);
   if (c->stream) cudaStreamSynchronize(c->stream);
   ovs_faces_free(c);
+  ovs_bcs_free(c);
   void* ptrs[] = {c->ien, c->elm_id, c->ibc, c->rowptr, c->colidx, c->diag, c->n2e_ptr, c->n2e, c->n2s, c->tmap, c->vals_t, c->vjp_cot, c->vjp_ge, c->vjp_grad,
                   c->rec[0], c->rec[1], c->esum[0], c->esum[1], c->gm, c->basis[0], c->basis[1], c->work64, c->work32, c->wvec, c->coop_part,
                   c->flags, c->cfl_bits};
@@ -772,11 +773,16 @@ int ovs_quench_newton(ovs_ctx* c, const ovs_newton_opts* o, ovs_newton_info* inf
     if ((s2 = ovs_assemble_impl(c, OVS_ASM_TEM, vec, prec, nullptr)) < 0) return s2;
     return OVS_OK;
   };
+  // setBCs_NSVOF + setBCs_Tem before the first residual and at the top of
+  // every Newton iteration (src/solveFlow.f90:35-36, :58-60), when registered
+  auto bcs = [&]() -> int { return c->have_bcs ? ovs_apply_bcs_impl(c, 3) : OVS_OK; };
+  if ((st = bcs())) return st;
   if ((st = vec_all())) return st;
   if ((st = ovs_residual_norms(c, prec, ni.residual0))) return st;
   memcpy(ni.residual, ni.residual0, sizeof(ni.residual));
   ni.converged = check(ni.residual);
   for (int it = 1; it <= o->newton_max; ++it) {
+    if ((st = bcs())) return st;
     if ((st = ovs_assemble_impl(c, OVS_ASM_NSVOF, both, prec, nullptr)) < 0) return st;
     if ((st = solve(OVS_SYS_NSVOF, o->tol_ns, &ni.krylov_iterations_ns))) return st;
     if (o->solve_tem) {

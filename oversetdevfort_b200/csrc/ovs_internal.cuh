@@ -1,5 +1,6 @@
 // Internal declarations of the B200 hot-path library (not part of the ABI).
 #pragma once
+#include <vector>
 #include <cuda_runtime.h>
 #include <stdint.h>
 #include <stddef.h>
@@ -54,6 +55,16 @@ struct GmresDev {
   double scal[8];     // misc scalar results (norms)
 };
 
+// one boundary of setBCs_NSVOF / setBCs_Tem with its types (read by FACE_ID)
+// and values (read by boundary number) resolved on the host
+struct BcBound {
+  int off = 0, n = 0;        // node range in bc_nodes
+  int ut[3] = {0, 0, 0};     // BCugType(FACE_ID, d)
+  double uv[3] = {0, 0, 0};  // BCugValu(b, d)
+  int pt = 0, tt = 0;        // BCphigType(FACE_ID), BCTgType(FACE_ID)
+  double pv = 0, tv = 0;     // BCphigValu(b), BCTgValu(b)
+};
+
 struct SysStore {
   void* vals = nullptr;   // nnz * nv values (internal slot layout)
   void* rhs = nullptr;    // nf * N, field-major
@@ -95,6 +106,11 @@ struct ovs_ctx {
   int* fnode_ptr = nullptr;   // nfnode + 1
   int* fnode_ent = nullptr;   // 4 nface entries (face << 2) | local node, ascending face per node
   void* fbuf[2] = {nullptr, nullptr};   // per-face element arrays, per precision
+  // boundary-condition producers (ovs_set_bc_spec)
+  bool have_bcs = false;
+  int* bc_nodes = nullptr;               // BNODES of all boundaries, 0-based
+  uint8_t* bc_n101 = nullptr;            // NodeID == 101 per node (or null)
+  std::vector<BcBound> bc_bounds;        // in NBOUND order
   // nodal state (FP64, reference layout)
   double* field[OVS_F_COUNT] = {};
   // alpha-stage node records (16 values per node), per precision
@@ -143,6 +159,10 @@ int ovs_faces_set_impl(ovs_ctx* c, int nface, const int* f2e, const int* face_or
                        const double* hconv, const double* tinf);
 int ovs_faces_assemble(ovs_ctx* c, int kernel, int prec, int mat, int vec);
 void ovs_faces_free(ovs_ctx* c);
+
+// bcs.cu
+int ovs_apply_bcs_impl(ovs_ctx* c, int which);
+void ovs_bcs_free(ovs_ctx* c);
 
 // spmv.cu / gmres.cu
 int ovs_precond_setup(ovs_ctx* c, int sys, int prec);

@@ -156,6 +156,69 @@ def face_set(m: Mesh, weak=(), convective=None) -> BoundaryFaces:
     return BoundaryFaces(*(np.concatenate(c) for c in zip(*parts)))
 
 
+@dataclass
+class BcSpec:
+    """Boundary data of setBCs_NSVOF / setBCs_Tem as the reference holds it
+    (src/param.f90:296-340): per boundary b its FACE_ID and node set, and the
+    tables BCugType (ntype, 3), BCphigType, BCTgType (read by FACE_ID) and
+    BCugValu (nbound, 3), BCphigValu, BCTgValu (read by b); NodeID per node or
+    None."""
+    face_id: np.ndarray
+    bnodes: list                      # per boundary, 1-based node ids
+    bcug_type: np.ndarray
+    bcug_valu: np.ndarray
+    bcphig_type: np.ndarray
+    bcphig_valu: np.ndarray
+    bctg_type: np.ndarray
+    bctg_valu: np.ndarray
+    node_id: np.ndarray | None = None
+
+    def to_c(self):
+        """(arrays to keep alive, ovs_bc_spec ctypes structure)."""
+        import ctypes as C
+        ip, dp = C.POINTER(C.c_int), C.POINTER(C.c_double)
+        nb = len(self.face_id)
+        ptr = np.zeros(nb + 1, dtype=np.int32)
+        ptr[1:] = np.cumsum([len(b) for b in self.bnodes])
+        keep = dict(
+            face_id=np.ascontiguousarray(self.face_id, dtype=np.int32), ptr=ptr,
+            bnodes=np.ascontiguousarray(np.concatenate(self.bnodes) if nb else np.zeros(1), dtype=np.int32),
+            ut=np.asfortranarray(self.bcug_type, dtype=np.int32), uv=np.asfortranarray(self.bcug_valu, dtype=np.float64),
+            pt=np.ascontiguousarray(self.bcphig_type, dtype=np.int32),
+            pv=np.ascontiguousarray(self.bcphig_valu, dtype=np.float64),
+            tt=np.ascontiguousarray(self.bctg_type, dtype=np.int32),
+            tv=np.ascontiguousarray(self.bctg_valu, dtype=np.float64))
+        if self.node_id is not None:
+            keep["nid"] = np.ascontiguousarray(self.node_id, dtype=np.int32)
+        g = lambda k, t: keep[k].ctypes.data_as(t)
+        cs = F.OvsBcSpec(nb, int(keep["ut"].shape[0]), g("face_id", ip), g("ptr", ip), g("bnodes", ip),
+                         g("nid", ip) if "nid" in keep else None, g("ut", ip), g("uv", dp), g("pt", ip), g("pv", dp),
+                         g("tt", ip), g("tv", dp))
+        return keep, cs
+
+
+def box_bc_spec(m: Mesh, u=None, phi=None, T=None, node_id=None, face_ids=(1, 2, 3, 4, 5, 6)) -> BcSpec:
+    """BcSpec of a box: boundary b = the box face b (x0, x1, y0, y1, z0, z1)
+    with FACE_ID face_ids[b].  u: {b: (v1, v2, v3)} with None for a free
+    component; phi, T: {b: value}.  Types are written at the FACE_ID row of
+    boundary b, so a permuted face_ids reproduces setBCs' FACE_ID/b mix."""
+    u, phi, T = u or {}, phi or {}, T or {}
+    nb = len(face_ids)
+    ut, uv = np.zeros((nb, 3), np.int32), np.zeros((nb, 3))
+    pt, pv, tt, tv = np.zeros(nb, np.int32), np.zeros(nb), np.zeros(nb, np.int32), np.zeros(nb)
+    for b in range(nb):
+        r = face_ids[b] - 1
+        for d, v in enumerate(u.get(b + 1, (None, None, None))):
+            if v is not None:
+                ut[r, d], uv[b, d] = 1, v
+        if b + 1 in phi:
+            pt[r], pv[b] = 1, phi[b + 1]
+        if b + 1 in T:
+            tt[r], tv[b] = 1, T[b + 1]
+    bn = [(np.asarray(m.faces[b]) + 1).astype(np.int32) for b in range(nb)]
+    return BcSpec(np.asarray(face_ids, np.int32), bn, ut, uv, pt, pv, tt, tv, node_id)
+
+
 def expected_nnz_kuhn(nx, ny, nz) -> int:
     """Closed-form nnz of the Kuhn-split pattern: every node couples to itself
     and to the neighbours along the 7 edge directions +-{x,y,z,xy,xz,yz,xyz}
