@@ -95,6 +95,13 @@ enum {
   OVS_F_COUNT
 };
 
+/* per-context options (ovs_set_option) */
+enum {
+  OVS_OPT_HEX_TC = 1,          /* 1 (default; env OVS_HEX_TC=0 turns it off): FP32 NS+VOF hexahedra take
+                                  the tensor-core element-matrix pass; 0: the CUDA-core row expansion */
+  OVS_OPT_ARNOLDI_FUSED = 2    /* 1: one-launch Arnoldi variant (default 0; env OVS_ARNOLDI_FUSED=1) */
+};
+
 /* boundary-face flags (ovs_set_faces) */
 enum {
   OVS_FACE_WEAK = 1,   /* face of a boundary with BCugType(b,d) == 2: the weak Dirichlet
@@ -185,6 +192,9 @@ int ovs_set_params(ovs_ctx* ctx, const ovs_params* p);
 /* IBC(N,nibc) column-major, entries 0/1 (src/setBCs.f90:183-187: columns
  * 1-3 velocity, 4 pressure, 5 VOF, 6 temperature) */
 int ovs_set_ibc(ovs_ctx* ctx, const int* ibc, int nibc);
+/* Sets a per-context option (OVS_OPT_*); OVS_ERR_ARG for an unknown one. */
+int ovs_set_option(ovs_ctx* ctx, int option, int value);
+
 /* Boundary faces for the face assemblies, in the reference's loop order
  * (boundary b = 1..NBOUND, then the faces of bound(b)): f2e = bound(b)%F2E
  * (1-based owning element), face_or = bound(b)%FACE_OR (1..4), flags

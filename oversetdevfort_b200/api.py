@@ -137,6 +137,10 @@ class Context:
         a = _i32(ibc)
         F.check(self.lib.ovs_set_ibc(self.h, _iptr(a), a.shape[1]), "ovs_set_ibc")
 
+    def set_option(self, option: int, value: int):
+        """OVS_OPT_HEX_TC / OVS_OPT_ARNOLDI_FUSED for this context."""
+        F.check(self.lib.ovs_set_option(self.h, option, int(value)), "ovs_set_option")
+
     def set_faces(self, bf):
         """Boundary faces for the face assemblies (mesh.BoundaryFaces, or None
         to clear): FaceAssembly_NS_weak / _outflow on OVS_FACE_WEAK faces and

@@ -29,6 +29,10 @@
 #include "ovs_internal.cuh"
 
 #include <math.h>
+#include <string.h>
+
+#include <type_traits>
+#include <vector>
 
 namespace {
 
@@ -45,6 +49,7 @@ struct AsmArgs {
   const unsigned* n2s;    // slots of each entry's element nodes in the row
   void* vals;             // nnz*NV
   void* rhs;              // NF*N field-major
+  const void* kbuf;       // hex tensor-core block values (E x 64 x 24), or null
   int* flags;             // [0] non-positive DetJ count, [1] non-finite residual
   unsigned long long* cfl_bits;
   int N;
@@ -1174,6 +1179,52 @@ __global__ void vjp_gather_kernel(const VjpGatherArgs a) {
 
 }  // namespace
 
+// W = f_g (x) f_g of the hex tensor-core pass, split into TF32 hi + lo, in
+// the canonical K-major no-swizzle layout: row n = 8 a + b, k = 16 g + 4 r + s,
+// byte offset (k / 4) * 1024 + (n / 8) * 128 + (n % 8) * 16 + (k % 4) * 4.
+static float host_tf32(double x) {   // round to the nearest TF32, ties away (cvt.rna)
+  float f = (float)x;
+  uint32_t b;
+  memcpy(&b, &f, 4);
+  b = (b + 0x1000u) & 0xFFFFE000u;
+  memcpy(&f, &b, 4);
+  return f;
+}
+
+int hex_tc_prepare(ovs_ctx* c) {
+  int st;
+  if ((st = ovs_ensure(&c->hex_kbuf, sizeof(float) * (size_t)c->E * 64 * 24))) return st;
+  if (c->hex_w) return OVS_OK;
+  static const int sgn[8][3] = {{-1, 1, -1}, {1, 1, -1}, {1, 1, 1}, {-1, 1, 1},
+                                {-1, -1, -1}, {1, -1, -1}, {1, -1, 1}, {-1, -1, 1}};
+  const double q = 0.57735026918963;   // the 2x2x2 points of hex_gp
+  double f[8][4][8];
+  for (int g = 0; g < 8; ++g) {
+    const double xi = (g & 1) ? q : -q, eta = (g & 2) ? q : -q, ze = (g & 4) ? q : -q;
+    for (int a = 0; a < 8; ++a) {
+      const double sx = sgn[a][0], sy = sgn[a][1], sz = sgn[a][2];
+      f[g][0][a] = (1.0 + sx * xi) * (1.0 + sy * eta) * (1.0 + sz * ze) * 0.125;
+      f[g][1][a] = sx * (1.0 + sy * eta) * (1.0 + sz * ze) * 0.125;
+      f[g][2][a] = sy * (1.0 + sx * xi) * (1.0 + sz * ze) * 0.125;
+      f[g][3][a] = sz * (1.0 + sx * xi) * (1.0 + sy * eta) * 0.125;
+    }
+  }
+  std::vector<float> hw(2 * 8192, 0.f);
+  for (int n = 0; n < 64; ++n)
+    for (int k = 0; k < 128; ++k) {
+      const int a = n >> 3, b = n & 7, g = k >> 4, r = (k >> 2) & 3, s = k & 3;
+      const double v = f[g][r][a] * f[g][s][b];
+      const float hi = host_tf32(v), lo = host_tf32(v - (double)hi);
+      const size_t off = ((size_t)(k >> 2) * 1024 + (n >> 3) * 128 + (n & 7) * 16 + (k & 3) * 4) / 4;
+      hw[off] = hi;
+      hw[8192 + off] = lo;
+    }
+  if ((st = ovs_ensure((void**)&c->hex_w, sizeof(float) * 2 * 8192))) return st;
+  OVS_CUDA_TRY(cudaMemcpyAsync(c->hex_w, hw.data(), sizeof(float) * 2 * 8192, cudaMemcpyHostToDevice, c->stream));
+  OVS_CUDA_TRY(cudaStreamSynchronize(c->stream));
+  return OVS_OK;
+}
+
 static int dispatch_assemble(ovs_ctx* c, int kernel, int prec, const AsmArgs& a, const SumArgs& sa,
                              int parts = 3) {
   if (c->nshl == 8) {   // trilinear hexahedra: NS+VOF and temperature passes
@@ -1221,6 +1272,7 @@ static void fill_args(ovs_ctx* c, int prec, SysStore& S, int tensor_flag, AsmArg
   a.n2s = c->n2s;
   a.max_deg = c->max_deg;
   a.p = c->params;
+  a.kbuf = nullptr;
 }
 
 // parts: 3 both passes, 1 the element pass, 2 the row pass (on the summaries
@@ -1295,6 +1347,7 @@ int ovs_assemble_impl(ovs_ctx* c, int kernel, int tensor_flag, int prec, double*
     *cfl = v;
   }
   if (hflags[3]) return OVS_ERR_PATTERN;
+  if (hflags[2]) return OVS_ERR_TIMEOUT;
   if (hflags[1]) return OVS_ERR_NONFINITE;
   if (hflags[0]) return OVS_WARN_NEG_DETJ;
   return OVS_OK;

@@ -36,9 +36,17 @@ template <> struct HexLay<OVS_ASM_TEM> {
   static constexpr int GPW = 32, RHS0 = 8 * 32, NF = 1, SW = 8 * 32 + 8, NV = 1;
 };
 
+//   NS+VOF record per point for the tensor-core path: dxi/dx (3x3, row k =
+//   xi_k) w KA KB MM KDP dphi(3) v(3) = dxi/dx uadv, rho rt tauLS src eps
+//   ufac plfac pad; then the residual rows 8x5
+struct HexTcLay {
+  static constexpr int GPW = 28, RHS0 = 8 * 28, SW = 8 * 28 + 40;
+};
+
 // eval_shape_fem for a hex at point g on x+d: global gradients, DetJ, G
 template <typename T>
-__device__ __forceinline__ T hex_geometry(int gp, const T r[8][16], const T lo[8][4], T g[8][3], T G[3][3]) {
+__device__ __forceinline__ T hex_geometry(int gp, const T r[8][16], const T lo[8][4], T g[8][3], T G[3][3],
+                                          T (*Aio)[3] = nullptr) {
   double xi, eta, ze;
   hex_gp(gp, xi, eta, ze);
   T dN[8][3];
@@ -80,6 +88,11 @@ __device__ __forceinline__ T hex_geometry(int gp, const T r[8][16], const T lo[8
   for (int i = 0; i < 3; ++i)
 #pragma unroll
     for (int j = 0; j < 3; ++j) G[i][j] = Ai[0][i] * Ai[0][j] + Ai[1][i] * Ai[1][j] + Ai[2][i] * Ai[2][j];
+  if (Aio)
+#pragma unroll
+    for (int i = 0; i < 3; ++i)
+#pragma unroll
+      for (int j = 0; j < 3; ++j) Aio[i][j] = Ai[i][j];
   return (T)1.0 / tmp;
 }
 
@@ -97,12 +110,14 @@ __device__ __forceinline__ void store_n(T* dst, const T* v, int n) {
   for (int k = 0; k < n; ++k) dst[k] = v[k];
 }
 
-// element pass, NS+VOF quench on a hex (src/solveQuenching.f90:295-523)
-template <typename T>
+// element pass, NS+VOF quench on a hex (src/solveQuenching.f90:295-523);
+// TC: write the compact records of the tensor-core matrix pass instead
+template <typename T, bool TC = false>
 __device__ void hex_summarize_nsvof(const ovs_params& p, const T r[8][16], const T lo[8][4], bool fluid,
                                     T* out, double& cfl, int& nbad) {
   using W = typename Wide<T>::type;
   using L = HexLay<OVS_ASM_NSVOF>;
+  constexpr int RHS0 = TC ? HexTcLay::RHS0 : L::RHS0;
   const T fact2 = (T)(p.alfi * p.delt * p.gami);
   const T taut = (T)(4.0 / (p.delt * p.delt));
   const T rhoa = (T)p.rhoa, rhow = (T)p.rhow, ts = (T)p.ts;
@@ -113,8 +128,8 @@ __device__ void hex_summarize_nsvof(const ovs_params& p, const T r[8][16], const
 #pragma unroll
   for (int n = 0; n < 8; ++n) { ru[n][0] = ru[n][1] = ru[n][2] = 0; rp[n] = 0; rf[n] = 0; }
   for (int gp = 0; gp < 8; ++gp) {
-    T g[8][3], G[3][3];
-    const T detj = hex_geometry<T>(gp, r, lo, g, G);
+    T g[8][3], G[3][3], Ai[3][3];
+    const T detj = hex_geometry<T>(gp, r, lo, g, G, Ai);
     if (!(detj > (T)0)) nbad = 1;
     const T w = detj;   // hex weights are 1
     T GG = 0;
@@ -204,25 +219,48 @@ __device__ void hex_summarize_nsvof(const ovs_params& p, const T r[8][16], const
     const T mupk = mu + kdc;
     const T dmdi = dmd * ira;
     const T wf = fluid ? w : (T)0;   // solid elements contribute nothing
-    T rec[L::GPW];
+    if constexpr (TC) {
+      T rec[HexTcLay::GPW];
 #pragma unroll
-    for (int a = 0; a < 8; ++a)
+      for (int k = 0; k < 3; ++k)
 #pragma unroll
-      for (int d = 0; d < 3; ++d) rec[3 * a + d] = g[a][d];
-    rec[24] = wf;
-    rec[25] = fluid ? fact2 * mupk * w : (T)0;
-    rec[26] = fluid ? fact2 * (tauC + lambda) * w : (T)0;
-    rec[27] = fluid ? fact2 * w * tauM : (T)0;
-    rec[28] = fluid ? fact2 * w * kdphi : (T)0;
-    rec[29] = dphi[0]; rec[30] = dphi[1]; rec[31] = dphi[2];
-    rec[32] = uadv[0]; rec[33] = uadv[1]; rec[34] = uadv[2];
-    rec[35] = rho; rec[36] = rho * tauM; rec[37] = tauLS;
-    rec[38] = vdot + phii * ira * dmd - dmd / rhoa;
-    rec[39] = fact2 * wf * tauC * dmdi * dmdi;
-    rec[40] = fact2 * tauC * dmdi * wf;
-    rec[41] = fact2 * dmdi * wf;
-    rec[42] = 0; rec[43] = 0;
-    store_n(out + gp * L::GPW, rec, L::GPW);
+        for (int j = 0; j < 3; ++j) rec[3 * k + j] = Ai[k][j];
+      rec[9] = wf;
+      rec[10] = fluid ? fact2 * mupk * w : (T)0;
+      rec[11] = fluid ? fact2 * (tauC + lambda) * w : (T)0;
+      rec[12] = fluid ? fact2 * w * tauM : (T)0;
+      rec[13] = fluid ? fact2 * w * kdphi : (T)0;
+      rec[14] = dphi[0]; rec[15] = dphi[1]; rec[16] = dphi[2];
+#pragma unroll
+      for (int k = 0; k < 3; ++k) rec[17 + k] = Ai[k][0] * uadv[0] + Ai[k][1] * uadv[1] + Ai[k][2] * uadv[2];
+      rec[20] = rho; rec[21] = rho * tauM; rec[22] = tauLS;
+      rec[23] = vdot + phii * ira * dmd - dmd / rhoa;
+      rec[24] = fact2 * wf * tauC * dmdi * dmdi;
+      rec[25] = fact2 * tauC * dmdi * wf;
+      rec[26] = fact2 * dmdi * wf;
+      rec[27] = 0;
+      store_n(out + gp * HexTcLay::GPW, rec, HexTcLay::GPW);
+    } else {
+      T rec[L::GPW];
+#pragma unroll
+      for (int a = 0; a < 8; ++a)
+#pragma unroll
+        for (int d = 0; d < 3; ++d) rec[3 * a + d] = g[a][d];
+      rec[24] = wf;
+      rec[25] = fluid ? fact2 * mupk * w : (T)0;
+      rec[26] = fluid ? fact2 * (tauC + lambda) * w : (T)0;
+      rec[27] = fluid ? fact2 * w * tauM : (T)0;
+      rec[28] = fluid ? fact2 * w * kdphi : (T)0;
+      rec[29] = dphi[0]; rec[30] = dphi[1]; rec[31] = dphi[2];
+      rec[32] = uadv[0]; rec[33] = uadv[1]; rec[34] = uadv[2];
+      rec[35] = rho; rec[36] = rho * tauM; rec[37] = tauLS;
+      rec[38] = vdot + phii * ira * dmd - dmd / rhoa;
+      rec[39] = fact2 * wf * tauC * dmdi * dmdi;
+      rec[40] = fact2 * tauC * dmdi * wf;
+      rec[41] = fact2 * dmdi * wf;
+      rec[42] = 0; rec[43] = 0;
+      store_n(out + gp * L::GPW, rec, L::GPW);
+    }
     if (!fluid) continue;
     T svis[8], gdphi[8], c[8];
 #pragma unroll
@@ -248,7 +286,7 @@ __device__ void hex_summarize_nsvof(const ovs_params& p, const T r[8][16], const
   }
 #pragma unroll
   for (int n = 0; n < 8; ++n) {
-    T* orh = out + L::RHS0 + 5 * n;
+    T* orh = out + RHS0 + 5 * n;
     orh[0] = ru[n][0]; orh[1] = ru[n][1]; orh[2] = ru[n][2]; orh[3] = rp[n]; orh[4] = rf[n];
   }
 }
@@ -359,9 +397,10 @@ __device__ void hex_summarize_tem(const ovs_params& p, const T r[8][16], const T
   for (int n = 0; n < 8; ++n) out[L::RHS0 + n] = rt[n];
 }
 
-template <typename T, int KIND>
+template <typename T, int KIND, bool TC = false>
 __global__ void __launch_bounds__(64) hex_element_kernel(const SumArgs a) {
   using L = HexLay<KIND>;
+  constexpr int SW = TC ? HexTcLay::SW : L::SW;
   const int e = blockIdx.x * blockDim.x + threadIdx.x;
   double cfl = 0.0;
   int nbad = 0;
@@ -371,8 +410,8 @@ __global__ void __launch_bounds__(64) hex_element_kernel(const SumArgs a) {
 #pragma unroll
     for (int n = 0; n < 8; ++n) load_rec(rec, a.ien[8 * (size_t)e + n], r[n], lo[n]);
     const bool fluid = __ldg(a.elm_id + e) == a.p.fluid_elm_id;
-    T* out = reinterpret_cast<T*>(a.sum) + (size_t)e * L::SW;
-    if constexpr (KIND == OVS_ASM_NSVOF) hex_summarize_nsvof<T>(a.p, r, lo, fluid, out, cfl, nbad);
+    T* out = reinterpret_cast<T*>(a.sum) + (size_t)e * SW;
+    if constexpr (KIND == OVS_ASM_NSVOF) hex_summarize_nsvof<T, TC>(a.p, r, lo, fluid, out, cfl, nbad);
     else hex_summarize_tem<T>(a.p, r, lo, fluid, out, cfl, nbad);
   }
 #pragma unroll
@@ -452,6 +491,294 @@ __device__ __forceinline__ void hex_expand_block(const ovs_params& p, const T* s
   }
 }
 
+// ------------------------------------------------------------------------
+// Tensor-core element matrices (FP32 NS+VOF hexahedra).
+//
+// Every block value t of the quench matrix is, per Gauss point g, a bilinear
+// form in the features (N, grad N) of the row node a and the column node b.
+// Written with the reference-element features f_g = (N, dN/dxi) (the same
+// for every element), the element's block is
+//     K_t[a][b] = sum_g sum_{r,s} C'_{t,g}[r][s] f_g[r][a] f_g[s][b],
+// with C' = T^T C T, T = diag(1, dxi/dx^T) mapping reference to physical
+// gradients.  So all element matrices of a tile are ONE dense product
+//     D[(t, e), (a, b)] = A[(t, e), (g, r, s)] * W[(g, r, s), (a, b)],
+// M = 8 types x 16 elements = 128, K = 8 points x 16 = 128, N = 64, with
+// the constant W = f_g (x) f_g shared by all elements, on tcgen05 (kind::tf32,
+// A and W K-major in shared memory without swizzle, D in TMEM).  FP32
+// accuracy comes from the 3xTF32 split A_hi W_hi + A_hi W_lo + A_lo W_hi
+// (W's split precomputed on the host).  One CTA of 128 threads per SM loops
+// over tiles of 16 elements; thread (element el, point g) builds its point's
+// 4x4 C' for 8 types at a time (three groups of 8 cover the 24 slot values),
+// thread 0 issues the 48 MMAs of a group into its 64 TMEM columns and
+// commits them to an mbarrier; the epilogue reads the 192 columns back and
+// writes each element's 64 x 24 block values (slot order) through shared
+// memory with coalesced stores.
+
+constexpr int TC_EB = 16;                                 // elements per tile
+constexpr int TC_KST = 64 * 24 + 4;                       // staging floats per element (padded)
+constexpr int TC_A_BYTES = 128 * 128 * 4;                 // one A operand (hi or lo)
+constexpr int TC_W_BYTES = 64 * 128 * 4;                  // one W operand (hi or lo)
+constexpr int TC_SMEM = 2 * TC_A_BYTES + 2 * TC_W_BYTES;  // 192 KB
+constexpr int TC_TMEM_COLS = 256;                         // 3 groups x 64 columns
+constexpr long TC_WAIT_LIMIT = 1L << 26;                  // bounded mbarrier wait (iterations)
+
+struct HexTcArgs {
+  const float* rec;    // element records, HexTcLay
+  const float* w;      // W hi then W lo, canonical K-major no-swizzle layout (2 x 8192 floats)
+  float* kbuf;         // E x 64 x 24 block values
+  int* flags;          // [2] set when an mbarrier wait gave up
+  int E;
+  float fact1, fact2;
+};
+
+__device__ __forceinline__ uint32_t tc_smem(const void* p) { return (uint32_t)__cvta_generic_to_shared(p); }
+__device__ __forceinline__ float tc_tf32(float x) {
+  uint32_t r;
+  asm("cvt.rna.tf32.f32 %0, %1;" : "=r"(r) : "f"(x));
+  return __uint_as_float(r);
+}
+// shared-memory matrix descriptor: SWIZZLE_NONE, K-major, version 1
+__device__ __forceinline__ uint64_t tc_desc(uint32_t addr, uint32_t lbo, uint32_t sbo) {
+  return (uint64_t)((addr >> 4) & 0x3FFF) | ((uint64_t)((lbo >> 4) & 0x3FFF) << 16) |
+         ((uint64_t)((sbo >> 4) & 0x3FFF) << 32) | ((uint64_t)1 << 46);
+}
+__device__ __forceinline__ void tc_mma(uint32_t dcol, uint64_t da, uint64_t db, uint32_t idesc, uint32_t acc) {
+  asm volatile("{\n\t.reg .pred p;\n\tsetp.ne.b32 p, %4, 0;\n\t"
+               "tcgen05.mma.cta_group::1.kind::tf32 [%0], %1, %2, %3, {%5, %6, %7, %8}, p;\n\t}\n"
+               ::"r"(dcol), "l"(da), "l"(db), "r"(idesc), "r"(acc), "r"(0), "r"(0), "r"(0), "r"(0));
+}
+__device__ __forceinline__ bool tc_wait(uint32_t bar, uint32_t parity) {
+  uint32_t done = 0;
+  for (long it = 0; it < TC_WAIT_LIMIT && !done; ++it)
+    asm volatile("{\n\t.reg .pred p;\n\tmbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+                 "selp.u32 %0, 1, 0, p;\n\t}\n" : "=r"(done) : "r"(bar), "r"(parity) : "memory");
+  return done != 0;
+}
+__device__ __forceinline__ void tc_ld16(uint32_t addr, float* v) {
+  uint32_t r[16];
+  asm volatile("tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15}, [%16];"
+               : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]),
+                 "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15])
+               : "r"(addr));
+  asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+#pragma unroll
+  for (int j = 0; j < 16; ++j) v[j] = __uint_as_float(r[j]);
+}
+
+// C' (reference features, row-major 4x4: [r][s], r on the row node a) of slot
+// value t at one point, from the point record q (HexTcLay): the per-point
+// forms of hex_expand_block with u.grad N = v . dN/dxi (v = dxi/dx uadv),
+// grad N_a . grad N_b = dN_a/dxi Gh dN_b/dxi (Gh = dxi/dx dxi/dx^T) and the
+// physical derivative j = dN/dxi . a_j (a_j column j of dxi/dx).
+__device__ __forceinline__ void tc_coeffs(int t, const float* q, const float Gh[3][3], float f1, float f2,
+                                          float C[16]) {
+#pragma unroll
+  for (int k = 0; k < 16; ++k) C[k] = 0.f;
+  const float w = q[9], KA = q[10], KB = q[11], MM = q[12], KDP = q[13];
+  const float v[3] = {q[17], q[18], q[19]};
+  const float rho = q[20], rt = q[21], tls = q[22], src = q[23], eps = q[24], ufac = q[25], plfac = q[26];
+  auto A = [&](int k, int j) { return q[3 * k + j]; };   // dxi_k/dx_j
+  if (t < 12 && (t & 3) != 3) {            // K(i, j)
+    const int i = t >> 2, j = t & 3;
+#pragma unroll
+    for (int k = 0; k < 3; ++k)
+#pragma unroll
+      for (int l = 0; l < 3; ++l) C[4 * (1 + k) + 1 + l] = KA * A(k, j) * A(l, i) + KB * A(k, i) * A(l, j);
+    if (i == j) {
+      const float al[4] = {1.f, rt * v[0], rt * v[1], rt * v[2]};
+      const float be[4] = {f1, f2 * v[0], f2 * v[1], f2 * v[2]};
+      const float wr = w * rho;
+#pragma unroll
+      for (int r = 0; r < 4; ++r)
+#pragma unroll
+        for (int c = 0; c < 4; ++c) C[4 * r + c] += wr * al[r] * be[c];
+#pragma unroll
+      for (int k = 0; k < 3; ++k)
+#pragma unroll
+        for (int l = 0; l < 3; ++l) C[4 * (1 + k) + 1 + l] += KA * Gh[k][l];
+    }
+  } else if (t < 12) {                     // G(i)
+    const int i = t >> 2;
+    const float fw = f2 * w;
+#pragma unroll
+    for (int k = 0; k < 3; ++k) {
+      C[4 * (1 + k)] = -fw * A(k, i);
+#pragma unroll
+      for (int l = 0; l < 3; ++l) C[4 * (1 + k) + 1 + l] = fw * rt * v[k] * A(l, i);
+    }
+  } else if (t < 15) {                     // D(d)
+    const int d = t - 12;
+    const float wrt = w * rt;
+#pragma unroll
+    for (int l = 0; l < 3; ++l) C[1 + l] = f2 * w * A(l, d);
+#pragma unroll
+    for (int k = 0; k < 3; ++k) {
+      C[4 * (1 + k)] = wrt * A(k, d) * f1;
+#pragma unroll
+      for (int l = 0; l < 3; ++l) C[4 * (1 + k) + 1 + l] = wrt * A(k, d) * f2 * v[l];
+    }
+  } else if (t == 15) {                    // M
+#pragma unroll
+    for (int k = 0; k < 3; ++k)
+#pragma unroll
+      for (int l = 0; l < 3; ++l) C[4 * (1 + k) + 1 + l] = MM * Gh[k][l];
+  } else if (t < 19) {                     // LSU(d)
+    const int d = t - 16;
+    const float c0 = q[14 + d] * f2 * w;
+    C[0] = c0;
+#pragma unroll
+    for (int k = 0; k < 3; ++k) C[4 * (1 + k)] = c0 * tls * v[k];
+#pragma unroll
+    for (int l = 0; l < 3; ++l) C[1 + l] = -ufac * A(l, d);
+  } else if (t == 19) {                    // LS
+    const float al[4] = {1.f, tls * v[0], tls * v[1], tls * v[2]};
+    const float ga[4] = {f1 + f2 * src, f2 * v[0], f2 * v[1], f2 * v[2]};
+#pragma unroll
+    for (int r = 0; r < 4; ++r)
+#pragma unroll
+      for (int c = 0; c < 4; ++c) C[4 * r + c] = w * al[r] * ga[c];
+#pragma unroll
+    for (int k = 0; k < 3; ++k)
+#pragma unroll
+      for (int l = 0; l < 3; ++l) C[4 * (1 + k) + 1 + l] += KDP * Gh[k][l];
+    C[0] += eps;
+  } else if (t < 23) {                     // ULS(d)
+    const int d = t - 20;
+#pragma unroll
+    for (int k = 0; k < 3; ++k) C[4 * (1 + k)] = ufac * A(k, d);
+  } else {                                 // PLS
+    C[0] = -plfac;
+  }
+}
+
+__global__ void __launch_bounds__(128, 1) hex_tc_matrix_kernel(const HexTcArgs a) {
+  extern __shared__ __align__(1024) unsigned char tc_sm[];
+  __shared__ __align__(8) uint64_t bar;
+  __shared__ uint32_t tbase;
+  unsigned char* sAh = tc_sm;
+  unsigned char* sAl = tc_sm + TC_A_BYTES;
+  unsigned char* sWh = tc_sm + 2 * TC_A_BYTES;
+  unsigned char* sWl = sWh + TC_W_BYTES;
+  float* kst = reinterpret_cast<float*>(tc_sm);             // epilogue staging over the A operands
+  const int t = threadIdx.x, wid = t >> 5, lane = t & 31;
+  const int el = t & 15, g = t >> 4;                        // this thread's element and point
+  {  // W hi / lo into shared memory (already in the canonical layout)
+    const float4* src = reinterpret_cast<const float4*>(a.w);
+    float4* dst = reinterpret_cast<float4*>(sWh);
+    for (int i = t; i < 2 * TC_W_BYTES / 16; i += 128) dst[i] = src[i];
+  }
+  if (t == 0) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(tc_smem(&bar)));
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  }
+  if (wid == 0) {
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(tc_smem(&tbase)),
+                 "r"(TC_TMEM_COLS));
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
+  }
+  asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+  asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+  __syncthreads();
+  asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+  const uint32_t tm = tbase, barp = tc_smem(&bar);
+  // kind::tf32, F32 accumulate, A and B K-major, N = 64, M = 128
+  const uint32_t idesc = (1u << 4) | (2u << 7) | (2u << 10) | ((64u >> 3) << 17) | ((128u >> 4) << 24);
+  uint32_t phase = 0;
+  bool ok = true;
+  const int ntiles = (a.E + TC_EB - 1) / TC_EB;
+  for (int tile = blockIdx.x; tile < ntiles && ok; tile += gridDim.x) {
+    const int e0 = tile * TC_EB, e = e0 + el;
+    float q[HexTcLay::GPW];
+    if (e < a.E) {
+      const float4* r4 = reinterpret_cast<const float4*>(a.rec + (size_t)e * HexTcLay::SW + g * HexTcLay::GPW);
+#pragma unroll
+      for (int k = 0; k < HexTcLay::GPW / 4; ++k) {
+        const float4 x = __ldg(r4 + k);
+        q[4 * k] = x.x; q[4 * k + 1] = x.y; q[4 * k + 2] = x.z; q[4 * k + 3] = x.w;
+      }
+    } else {
+#pragma unroll
+      for (int k = 0; k < HexTcLay::GPW; ++k) q[k] = 0.f;
+    }
+    float Gh[3][3];
+#pragma unroll
+    for (int k = 0; k < 3; ++k)
+#pragma unroll
+      for (int l = 0; l < 3; ++l) Gh[k][l] = q[3 * k] * q[3 * l] + q[3 * k + 1] * q[3 * l + 1] + q[3 * k + 2] * q[3 * l + 2];
+    for (int grp = 0; grp < 3 && ok; ++grp) {
+      // A[(t8, el), (g, r, s)]: row m = 16 t8 + el, 16-byte chunk kc = 4 g + r
+      for (int t8 = 0; t8 < 8; ++t8) {
+        float C[16];
+        tc_coeffs(8 * grp + t8, q, Gh, a.fact1, a.fact2, C);
+        const int m = 16 * t8 + el;
+#pragma unroll
+        for (int r = 0; r < 4; ++r) {
+          const int off = (4 * g + r) * 2048 + (m >> 3) * 128 + (m & 7) * 16;
+          float4 h, l;
+          h.x = tc_tf32(C[4 * r]); h.y = tc_tf32(C[4 * r + 1]); h.z = tc_tf32(C[4 * r + 2]); h.w = tc_tf32(C[4 * r + 3]);
+          l.x = tc_tf32(C[4 * r] - h.x); l.y = tc_tf32(C[4 * r + 1] - h.y);
+          l.z = tc_tf32(C[4 * r + 2] - h.z); l.w = tc_tf32(C[4 * r + 3] - h.w);
+          *reinterpret_cast<float4*>(sAh + off) = h;
+          *reinterpret_cast<float4*>(sAl + off) = l;
+        }
+      }
+      asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+      asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+      __syncthreads();
+      asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+      if (t == 0) {
+        const uint32_t dcol = tm + 64 * grp;
+        const uint32_t ah = tc_smem(sAh), al = tc_smem(sAl), wh = tc_smem(sWh), wl = tc_smem(sWl);
+        for (int ks = 0; ks < 16; ++ks)
+          tc_mma(dcol, tc_desc(ah + ks * 4096, 2048, 128), tc_desc(wh + ks * 2048, 1024, 128), idesc, ks > 0);
+        for (int ks = 0; ks < 16; ++ks)
+          tc_mma(dcol, tc_desc(ah + ks * 4096, 2048, 128), tc_desc(wl + ks * 2048, 1024, 128), idesc, 1u);
+        for (int ks = 0; ks < 16; ++ks)
+          tc_mma(dcol, tc_desc(al + ks * 4096, 2048, 128), tc_desc(wh + ks * 2048, 1024, 128), idesc, 1u);
+        asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(barp)
+                     : "memory");
+      }
+      // the operands are free again (and, after the last group, D is complete)
+      const bool done = tc_wait(barp, phase);
+      ok = __syncthreads_and(done) != 0;
+      if (ok) phase ^= 1u;
+      asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+    }
+    if (!ok) break;
+    // epilogue: lane m = 32 wid + lane of each group's 64 columns -> staging
+    {
+      const int m = 32 * wid + lane, t8 = m >> 4, eli = m & 15;
+      float* dst = kst + eli * TC_KST;
+      for (int grp = 0; grp < 3; ++grp)
+#pragma unroll
+        for (int c0 = 0; c0 < 64; c0 += 16) {
+          float v[16];
+          tc_ld16(tm + ((uint32_t)(32 * wid) << 16) + 64 * grp + c0, v);
+#pragma unroll
+          for (int j = 0; j < 16; ++j) dst[(c0 + j) * 24 + 8 * grp + t8] = v[j];
+        }
+    }
+    asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+    __syncthreads();
+    {
+      const int nel = min(TC_EB, a.E - e0);
+      float4* out = reinterpret_cast<float4*>(a.kbuf + (size_t)e0 * 1536);
+      for (int i = t; i < nel * 384; i += 128) {
+        const int ee = i / 384, j4 = i - ee * 384;
+        out[i] = *reinterpret_cast<const float4*>(kst + ee * TC_KST + 4 * j4);
+      }
+    }
+    __syncthreads();   // staging (the A operands) free for the next tile
+  }
+  if (!ok) {   // give the MMAs in flight one more bounded wait before TMEM is released
+    tc_wait(barp, phase);
+    if (t == 0) atomicOr(a.flags + 2, 1);
+  }
+  asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+  __syncthreads();
+  if (wid == 0) asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tm), "r"(TC_TMEM_COLS));
+}
+
 // shared memory per warp: blocks [4 elements][8 columns][BSTR], RHS rows
 // [4][RSTR], row accumulator [max_deg][NVP]; ints: slots [4][8], columns
 template <typename T, int KIND> struct HexSmem {
@@ -468,7 +795,7 @@ template <typename T, int KIND> struct HexSmem {
   }
 };
 
-template <typename T, int KIND>
+template <typename T, int KIND, bool TC = false>
 __global__ void __launch_bounds__(128) hex_rows_kernel(const AsmArgs a) {
   using S = HexSmem<T, KIND>;
   using L = HexLay<KIND>;
@@ -504,7 +831,19 @@ __global__ void __launch_bounds__(128) hex_rows_kernel(const AsmArgs a) {
         const uint2 sl = __ldg(n2s8 + ep + c0 + jl);
         const int e = packed >> 3, la = packed & 7;
         T o[NVP], rv[NF];
-        hex_expand_block<T, KIND>(a.p, sum + (size_t)e * L::SW, la, bl, o, rv);
+        if constexpr (TC) {   // block values of the tensor-core pass, slot order
+          const float4* kb = reinterpret_cast<const float4*>(reinterpret_cast<const float*>(a.kbuf) +
+                                                             ((size_t)e * 64 + la * 8 + bl) * 24);
+#pragma unroll
+          for (int v = 0; v < 6; ++v) {
+            const float4 x = __ldg(kb + v);
+            o[4 * v] = x.x; o[4 * v + 1] = x.y; o[4 * v + 2] = x.z; o[4 * v + 3] = x.w;
+          }
+#pragma unroll
+          for (int f = 0; f < NF; ++f) rv[f] = sum[(size_t)e * HexTcLay::SW + HexTcLay::RHS0 + 5 * la + f];
+        } else {
+          hex_expand_block<T, KIND>(a.p, sum + (size_t)e * L::SW, la, bl, o, rv);
+        }
         T* dst = blk + (jl * 8 + bl) * BSTR;
         if constexpr (NV >= 4) {
 #pragma unroll
@@ -587,16 +926,48 @@ __global__ void __launch_bounds__(128) hex_rows_kernel(const AsmArgs a) {
 }
 
 template <typename T, int KIND>
-int launch_assemble_hex(ovs_ctx* c, const AsmArgs& a, const SumArgs& sa, int parts) {
+int launch_assemble_hex(ovs_ctx* c, const AsmArgs& a0, const SumArgs& sa, int parts) {
+  constexpr bool can_tc = std::is_same<T, float>::value && KIND == OVS_ASM_NSVOF;
+  const bool tc = can_tc && c->hex_tc;
+  AsmArgs a = a0;
+  if (tc) {
+    int st;
+    if ((st = hex_tc_prepare(c))) return st;
+    a.kbuf = c->hex_kbuf;
+  }
   if (parts & 1) {
-    hex_element_kernel<T, KIND><<<(sa.E + 63) / 64, 64, 0, c->stream>>>(sa);
-    ++c->launches;
-    OVS_CUDA_TRY(cudaGetLastError());
+    if (tc) {
+      if constexpr (can_tc) {
+        hex_element_kernel<T, KIND, true><<<(sa.E + 63) / 64, 64, 0, c->stream>>>(sa);
+        ++c->launches;
+        OVS_CUDA_TRY(cudaGetLastError());
+        HexTcArgs ta;
+        ta.rec = reinterpret_cast<const float*>(sa.sum);
+        ta.w = c->hex_w;
+        ta.kbuf = reinterpret_cast<float*>(c->hex_kbuf);
+        ta.flags = c->flags;
+        ta.E = sa.E;
+        ta.fact1 = (float)sa.p.almi;
+        ta.fact2 = (float)(sa.p.alfi * sa.p.delt * sa.p.gami);
+        OVS_CUDA_TRY(cudaFuncSetAttribute(hex_tc_matrix_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, TC_SMEM));
+        const int ntiles = (sa.E + TC_EB - 1) / TC_EB;
+        const int grid = ntiles < c->num_sms ? ntiles : c->num_sms;
+        if (grid > 0) {
+          hex_tc_matrix_kernel<<<grid, 128, TC_SMEM, c->stream>>>(ta);
+          ++c->launches;
+          OVS_CUDA_TRY(cudaGetLastError());
+        }
+      }
+    } else {
+      hex_element_kernel<T, KIND><<<(sa.E + 63) / 64, 64, 0, c->stream>>>(sa);
+      ++c->launches;
+      OVS_CUDA_TRY(cudaGetLastError());
+    }
   }
   if (!(parts & 2)) return OVS_OK;
   using S = HexSmem<T, KIND>;
   const size_t smem = S::bytes(a.max_deg) * 4;
-  auto kern = hex_rows_kernel<T, KIND>;
+  auto kern = tc ? hex_rows_kernel<T, KIND, can_tc> : hex_rows_kernel<T, KIND, false>;
   OVS_CUDA_TRY(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
   int per_sm = 0;
   OVS_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, 128, smem));

@@ -200,6 +200,8 @@ int ovs_create(ovs_ctx** out, const ovs_dims* dims) {
   {
     const char* e = getenv("OVS_ARNOLDI_FUSED");
     c->arnoldi_fused = e && e[0] == '1';
+    const char* h = getenv("OVS_HEX_TC");
+    c->hex_tc = !(h && h[0] == '0');
   }
   c->N = dims->nnode;
   c->E = dims->nelem;
@@ -237,6 +239,8 @@ int ovs_destroy(ovs_ctx* c) {
   if (c->stream) cudaStreamSynchronize(c->stream);
   ovs_faces_free(c);
   ovs_bcs_free(c);
+  if (c->hex_kbuf) cudaFree(c->hex_kbuf);
+  if (c->hex_w) cudaFree(c->hex_w);
   void* ptrs[] = {c->ien, c->elm_id, c->ibc, c->rowptr, c->colidx, c->diag, c->n2e_ptr, c->n2e, c->n2s, c->tmap, c->vals_t, c->vjp_cot, c->vjp_ge, c->vjp_grad,
                   c->rec[0], c->rec[1], c->esum[0], c->esum[1], c->gm, c->basis[0], c->basis[1], c->work64, c->work32, c->wvec, c->coop_part,
                   c->flags, c->cfl_bits};
@@ -364,6 +368,15 @@ int ovs_set_ibc(ovs_ctx* c, const int* ibc, int nibc) {
   OVS_CUDA_TRY(cudaFreeAsync(tmp, s));
   OVS_CUDA_TRY(cudaStreamSynchronize(s));
   return OVS_OK;
+}
+
+int ovs_set_option(ovs_ctx* c, int option, int value) {
+  if (!c) return OVS_ERR_ARG;
+  switch (option) {
+    case OVS_OPT_HEX_TC: c->hex_tc = value != 0; return OVS_OK;
+    case OVS_OPT_ARNOLDI_FUSED: c->arnoldi_fused = value != 0; return OVS_OK;
+    default: return OVS_ERR_ARG;
+  }
 }
 
 int ovs_set_faces(ovs_ctx* c, int nface, const int* f2e, const int* face_or, const int* flags,

@@ -106,6 +106,10 @@ struct ovs_ctx {
   int* fnode_ptr = nullptr;   // nfnode + 1
   int* fnode_ent = nullptr;   // 4 nface entries (face << 2) | local node, ascending face per node
   void* fbuf[2] = {nullptr, nullptr};   // per-face element arrays, per precision
+  // hex tensor-core pass (FP32 NS+VOF): on unless OVS_HEX_TC=0
+  int hex_tc = 1;
+  void* hex_kbuf = nullptr;              // E x 64 x 24 block values
+  float* hex_w = nullptr;                // W hi + lo, canonical layout
   // boundary-condition producers (ovs_set_bc_spec)
   bool have_bcs = false;
   int* bc_nodes = nullptr;               // BNODES of all boundaries, 0-based
@@ -153,6 +157,9 @@ int ovs_pattern_to_host(ovs_ctx* c, int* col, int* row);
 // assemble.cu
 int ovs_assemble_impl(ovs_ctx* c, int kernel, int tensor_flag, int prec,
                       double* cfl);
+
+// assemble.cu: W operand and block buffer of the hex tensor-core pass
+int hex_tc_prepare(ovs_ctx* c);
 
 // faces.cu
 int ovs_faces_set_impl(ovs_ctx* c, int nface, const int* f2e, const int* face_or, const int* flags,
