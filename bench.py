@@ -304,7 +304,9 @@ def run_hex(local_rank, args):
     """Config 4 (96^3 trilinear hexahedra, 2x2x2 Gauss points): NS+VOF + T
     assembly pass (FP32 and FP64, device time) and the mixed-precision
     refined solve of the NS+VOF system to the bench's relative residual with
-    Krylov space 100.  Built on CUDA cores; see DESIGN for the tensor cores."""
+    Krylov space 100.  The FP32 NS+VOF pass is timed both ways: element
+    matrices on tcgen05 (3xTF32) and the CUDA-core row expansion (the
+    default, faster as measured)."""
     import statistics
     from oversetdevfort_b200 import _ffi as F
     from oversetdevfort_b200 import mesh as M
@@ -324,6 +326,19 @@ def run_hex(local_rank, args):
                 ms.append(a + ctx.last_device_ms())
         out[f"assembly_ms_{name}"] = statistics.mean(ms)
         out[f"assembly_melem_s_{name}"] = E / (statistics.mean(ms) * 1e-3) / 1e6
+    # FP32 NS+VOF pass: tensor-core element matrices vs the CUDA-core expansion
+    for tc, name in ((1, "tensor_cores"), (0, "cuda_cores")):
+        ctx.set_option(F.OVS_OPT_HEX_TC, tc)
+        ctx.assemble(F.OVS_ASM_NSVOF, 6, F.OVS_FP32)
+        out[f"nsvof_fp32_{name}"] = {
+            "pass_ms": ctx.profile(F.OVS_PROF_ASSEMBLE, F.OVS_ASM_NSVOF, F.OVS_FP32, 5),
+            "element_and_matrix_ms": ctx.profile(F.OVS_PROF_ASSEMBLE_ELEMENTS, F.OVS_ASM_NSVOF, F.OVS_FP32, 5),
+            "rows_ms": ctx.profile(F.OVS_PROF_ASSEMBLE_ROWS, F.OVS_ASM_NSVOF, F.OVS_FP32, 5)}
+    ctx.set_option(F.OVS_OPT_HEX_TC, 0)
+    # tcgen05 work of one pass: 3 MMA products (3xTF32) of 128 x 64 x 128 per
+    # 8 slot values of 16 elements; the algorithmic contraction is one of them
+    tiles = (E + 15) // 16
+    out["tc_mma_tflop_per_pass"] = tiles * 3 * 3 * 2 * 128 * 64 * 128 / 1e12
     ctx.assemble(F.OVS_ASM_NSVOF, 6, F.OVS_FP32)
     ctx.assemble(F.OVS_ASM_NSVOF, 6, F.OVS_FP64)
     sol, info = ctx.solve(F.OVS_SYS_NSVOF, F.OVS_FP32, args.rtol, kspace=100, max_cycles=args.max_cycles,

@@ -97,8 +97,9 @@ enum {
 
 /* per-context options (ovs_set_option) */
 enum {
-  OVS_OPT_HEX_TC = 1,          /* 1 (default; env OVS_HEX_TC=0 turns it off): FP32 NS+VOF hexahedra take
-                                  the tensor-core element-matrix pass; 0: the CUDA-core row expansion */
+  OVS_OPT_HEX_TC = 1,          /* 1: FP32 NS+VOF hexahedra take the tcgen05 element-matrix pass (3xTF32);
+                                  0 (default, the faster one measured; env OVS_HEX_TC=1 sets 1): the
+                                  CUDA-core row expansion */
   OVS_OPT_ARNOLDI_FUSED = 2    /* 1: one-launch Arnoldi variant (default 0; env OVS_ARNOLDI_FUSED=1) */
 };
 

@@ -507,8 +507,9 @@ __device__ __forceinline__ void hex_expand_block(const ovs_params& p, const T* s
 // A and W K-major in shared memory without swizzle, D in TMEM).  FP32
 // accuracy comes from the 3xTF32 split A_hi W_hi + A_hi W_lo + A_lo W_hi
 // (W's split precomputed on the host).  One CTA of 128 threads per SM loops
-// over tiles of 16 elements; thread (element el, point g) builds its point's
-// 4x4 C' for 8 types at a time (three groups of 8 cover the 24 slot values),
+// over tiles of 16 elements with 256 threads; thread (element el, point g)
+// of each half builds its point's 4x4 C' for 4 of a group's 8 slot values
+// (three groups of 8 cover the 24; the value is a template parameter),
 // thread 0 issues the 48 MMAs of a group into its 64 TMEM columns and
 // commits them to an mbarrier; the epilogue reads the 192 columns back and
 // writes each element's 64 x 24 block values (slot order) through shared
@@ -570,21 +571,21 @@ __device__ __forceinline__ void tc_ld16(uint32_t addr, float* v) {
 // forms of hex_expand_block with u.grad N = v . dN/dxi (v = dxi/dx uadv),
 // grad N_a . grad N_b = dN_a/dxi Gh dN_b/dxi (Gh = dxi/dx dxi/dx^T) and the
 // physical derivative j = dN/dxi . a_j (a_j column j of dxi/dx).
-__device__ __forceinline__ void tc_coeffs(int t, const float* q, const float Gh[3][3], float f1, float f2,
-                                          float C[16]) {
+template <int t>
+__device__ __forceinline__ void tc_coeffs(const float* q, const float Gh[3][3], float f1, float f2, float C[16]) {
 #pragma unroll
   for (int k = 0; k < 16; ++k) C[k] = 0.f;
   const float w = q[9], KA = q[10], KB = q[11], MM = q[12], KDP = q[13];
   const float v[3] = {q[17], q[18], q[19]};
   const float rho = q[20], rt = q[21], tls = q[22], src = q[23], eps = q[24], ufac = q[25], plfac = q[26];
   auto A = [&](int k, int j) { return q[3 * k + j]; };   // dxi_k/dx_j
-  if (t < 12 && (t & 3) != 3) {            // K(i, j)
-    const int i = t >> 2, j = t & 3;
+  if constexpr (t < 12 && (t & 3) != 3) {  // K(i, j)
+    constexpr int i = t >> 2, j = t & 3;
 #pragma unroll
     for (int k = 0; k < 3; ++k)
 #pragma unroll
       for (int l = 0; l < 3; ++l) C[4 * (1 + k) + 1 + l] = KA * A(k, j) * A(l, i) + KB * A(k, i) * A(l, j);
-    if (i == j) {
+    if constexpr (i == j) {
       const float al[4] = {1.f, rt * v[0], rt * v[1], rt * v[2]};
       const float be[4] = {f1, f2 * v[0], f2 * v[1], f2 * v[2]};
       const float wr = w * rho;
@@ -597,8 +598,8 @@ __device__ __forceinline__ void tc_coeffs(int t, const float* q, const float Gh[
 #pragma unroll
         for (int l = 0; l < 3; ++l) C[4 * (1 + k) + 1 + l] += KA * Gh[k][l];
     }
-  } else if (t < 12) {                     // G(i)
-    const int i = t >> 2;
+  } else if constexpr (t < 12) {           // G(i)
+    constexpr int i = t >> 2;
     const float fw = f2 * w;
 #pragma unroll
     for (int k = 0; k < 3; ++k) {
@@ -606,8 +607,8 @@ __device__ __forceinline__ void tc_coeffs(int t, const float* q, const float Gh[
 #pragma unroll
       for (int l = 0; l < 3; ++l) C[4 * (1 + k) + 1 + l] = fw * rt * v[k] * A(l, i);
     }
-  } else if (t < 15) {                     // D(d)
-    const int d = t - 12;
+  } else if constexpr (t < 15) {           // D(d)
+    constexpr int d = t - 12;
     const float wrt = w * rt;
 #pragma unroll
     for (int l = 0; l < 3; ++l) C[1 + l] = f2 * w * A(l, d);
@@ -617,20 +618,20 @@ __device__ __forceinline__ void tc_coeffs(int t, const float* q, const float Gh[
 #pragma unroll
       for (int l = 0; l < 3; ++l) C[4 * (1 + k) + 1 + l] = wrt * A(k, d) * f2 * v[l];
     }
-  } else if (t == 15) {                    // M
+  } else if constexpr (t == 15) {          // M
 #pragma unroll
     for (int k = 0; k < 3; ++k)
 #pragma unroll
       for (int l = 0; l < 3; ++l) C[4 * (1 + k) + 1 + l] = MM * Gh[k][l];
-  } else if (t < 19) {                     // LSU(d)
-    const int d = t - 16;
+  } else if constexpr (t < 19) {           // LSU(d)
+    constexpr int d = t - 16;
     const float c0 = q[14 + d] * f2 * w;
     C[0] = c0;
 #pragma unroll
     for (int k = 0; k < 3; ++k) C[4 * (1 + k)] = c0 * tls * v[k];
 #pragma unroll
     for (int l = 0; l < 3; ++l) C[1 + l] = -ufac * A(l, d);
-  } else if (t == 19) {                    // LS
+  } else if constexpr (t == 19) {          // LS
     const float al[4] = {1.f, tls * v[0], tls * v[1], tls * v[2]};
     const float ga[4] = {f1 + f2 * src, f2 * v[0], f2 * v[1], f2 * v[2]};
 #pragma unroll
@@ -642,8 +643,8 @@ __device__ __forceinline__ void tc_coeffs(int t, const float* q, const float Gh[
 #pragma unroll
       for (int l = 0; l < 3; ++l) C[4 * (1 + k) + 1 + l] += KDP * Gh[k][l];
     C[0] += eps;
-  } else if (t < 23) {                     // ULS(d)
-    const int d = t - 20;
+  } else if constexpr (t < 23) {           // ULS(d)
+    constexpr int d = t - 20;
 #pragma unroll
     for (int k = 0; k < 3; ++k) C[4 * (1 + k)] = ufac * A(k, d);
   } else {                                 // PLS
@@ -651,7 +652,76 @@ __device__ __forceinline__ void tc_coeffs(int t, const float* q, const float Gh[
   }
 }
 
-__global__ void __launch_bounds__(128, 1) hex_tc_matrix_kernel(const HexTcArgs a) {
+// A rows m = 16 t8 + el, 16-byte chunk kc = 4 g + r (hi and lo operands)
+template <int t>
+__device__ __forceinline__ void tc_store_type(const float* q, const float Gh[3][3], float f1, float f2,
+                                              unsigned char* sAh, unsigned char* sAl, int el, int g) {
+  float C[16];
+  tc_coeffs<t>(q, Gh, f1, f2, C);
+  const int m = 16 * (t & 7) + el;
+#pragma unroll
+  for (int r = 0; r < 4; ++r) {
+    const int off = (4 * g + r) * 2048 + (m >> 3) * 128 + (m & 7) * 16;
+    float4 h, l;
+    h.x = tc_tf32(C[4 * r]); h.y = tc_tf32(C[4 * r + 1]); h.z = tc_tf32(C[4 * r + 2]); h.w = tc_tf32(C[4 * r + 3]);
+    l.x = tc_tf32(C[4 * r] - h.x); l.y = tc_tf32(C[4 * r + 1] - h.y);
+    l.z = tc_tf32(C[4 * r + 2] - h.z); l.w = tc_tf32(C[4 * r + 3] - h.w);
+    *reinterpret_cast<float4*>(sAh + off) = h;
+    *reinterpret_cast<float4*>(sAl + off) = l;
+  }
+}
+
+// the 8 slot values of group GRP: the warp-uniform half hf of the CTA builds 4 of them
+template <int GRP>
+__device__ __forceinline__ void tc_store_group(int hf, const float* q, const float Gh[3][3], float f1, float f2,
+                                               unsigned char* sAh, unsigned char* sAl, int el, int g) {
+  if (hf == 0) {
+    tc_store_type<8 * GRP + 0>(q, Gh, f1, f2, sAh, sAl, el, g);
+    tc_store_type<8 * GRP + 1>(q, Gh, f1, f2, sAh, sAl, el, g);
+    tc_store_type<8 * GRP + 2>(q, Gh, f1, f2, sAh, sAl, el, g);
+    tc_store_type<8 * GRP + 3>(q, Gh, f1, f2, sAh, sAl, el, g);
+  } else {
+    tc_store_type<8 * GRP + 4>(q, Gh, f1, f2, sAh, sAl, el, g);
+    tc_store_type<8 * GRP + 5>(q, Gh, f1, f2, sAh, sAl, el, g);
+    tc_store_type<8 * GRP + 6>(q, Gh, f1, f2, sAh, sAl, el, g);
+    tc_store_type<8 * GRP + 7>(q, Gh, f1, f2, sAh, sAl, el, g);
+  }
+}
+
+constexpr int TC_THREADS = 256;
+
+// builds group GRP's operands, issues its MMAs and waits for them; false when the wait gave up
+template <int GRP>
+__device__ __forceinline__ bool tc_group(int hf, const float* q, const float Gh[3][3], float f1, float f2,
+                                         unsigned char* sAh, unsigned char* sAl, unsigned char* sWh,
+                                         unsigned char* sWl, int el, int g, uint32_t tm, uint32_t barp,
+                                         uint32_t idesc, uint32_t& phase) {
+  tc_store_group<GRP>(hf, q, Gh, f1, f2, sAh, sAl, el, g);
+  asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+  asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+  __syncthreads();
+  asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+  if (threadIdx.x == 0) {
+    const uint32_t dcol = tm + 64 * GRP;
+    const uint32_t ah = tc_smem(sAh), al = tc_smem(sAl), wh = tc_smem(sWh), wl = tc_smem(sWl);
+    for (int ks = 0; ks < 16; ++ks)
+      tc_mma(dcol, tc_desc(ah + ks * 4096, 2048, 128), tc_desc(wh + ks * 2048, 1024, 128), idesc, ks > 0);
+    for (int ks = 0; ks < 16; ++ks)
+      tc_mma(dcol, tc_desc(ah + ks * 4096, 2048, 128), tc_desc(wl + ks * 2048, 1024, 128), idesc, 1u);
+    for (int ks = 0; ks < 16; ++ks)
+      tc_mma(dcol, tc_desc(al + ks * 4096, 2048, 128), tc_desc(wh + ks * 2048, 1024, 128), idesc, 1u);
+    asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(barp)
+                 : "memory");
+  }
+  // the operands are free again (and, after the last group, D is complete)
+  const bool done = tc_wait(barp, phase);
+  const bool ok = __syncthreads_and(done) != 0;
+  if (ok) phase ^= 1u;
+  asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+  return ok;
+}
+
+__global__ void __launch_bounds__(TC_THREADS, 1) hex_tc_matrix_kernel(const HexTcArgs a) {
   extern __shared__ __align__(1024) unsigned char tc_sm[];
   __shared__ __align__(8) uint64_t bar;
   __shared__ uint32_t tbase;
@@ -661,11 +731,12 @@ __global__ void __launch_bounds__(128, 1) hex_tc_matrix_kernel(const HexTcArgs a
   unsigned char* sWl = sWh + TC_W_BYTES;
   float* kst = reinterpret_cast<float*>(tc_sm);             // epilogue staging over the A operands
   const int t = threadIdx.x, wid = t >> 5, lane = t & 31;
-  const int el = t & 15, g = t >> 4;                        // this thread's element and point
+  const int hf = t >> 7, tt = t & 127;                      // half of the CTA (4 of each group's 8 values)
+  const int el = tt & 15, g = tt >> 4;                      // this thread's element and point
   {  // W hi / lo into shared memory (already in the canonical layout)
     const float4* src = reinterpret_cast<const float4*>(a.w);
     float4* dst = reinterpret_cast<float4*>(sWh);
-    for (int i = t; i < 2 * TC_W_BYTES / 16; i += 128) dst[i] = src[i];
+    for (int i = t; i < 2 * TC_W_BYTES / 16; i += TC_THREADS) dst[i] = src[i];
   }
   if (t == 0) {
     asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(tc_smem(&bar)));
@@ -683,10 +754,11 @@ __global__ void __launch_bounds__(128, 1) hex_tc_matrix_kernel(const HexTcArgs a
   const uint32_t tm = tbase, barp = tc_smem(&bar);
   // kind::tf32, F32 accumulate, A and B K-major, N = 64, M = 128
   const uint32_t idesc = (1u << 4) | (2u << 7) | (2u << 10) | ((64u >> 3) << 17) | ((128u >> 4) << 24);
+  const float f1 = a.fact1, f2 = a.fact2;
   uint32_t phase = 0;
   bool ok = true;
   const int ntiles = (a.E + TC_EB - 1) / TC_EB;
-  for (int tile = blockIdx.x; tile < ntiles && ok; tile += gridDim.x) {
+  for (int tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
     const int e0 = tile * TC_EB, e = e0 + el;
     float q[HexTcLay::GPW];
     if (e < a.E) {
@@ -705,55 +777,21 @@ __global__ void __launch_bounds__(128, 1) hex_tc_matrix_kernel(const HexTcArgs a
     for (int k = 0; k < 3; ++k)
 #pragma unroll
       for (int l = 0; l < 3; ++l) Gh[k][l] = q[3 * k] * q[3 * l] + q[3 * k + 1] * q[3 * l + 1] + q[3 * k + 2] * q[3 * l + 2];
-    for (int grp = 0; grp < 3 && ok; ++grp) {
-      // A[(t8, el), (g, r, s)]: row m = 16 t8 + el, 16-byte chunk kc = 4 g + r
-      for (int t8 = 0; t8 < 8; ++t8) {
-        float C[16];
-        tc_coeffs(8 * grp + t8, q, Gh, a.fact1, a.fact2, C);
-        const int m = 16 * t8 + el;
-#pragma unroll
-        for (int r = 0; r < 4; ++r) {
-          const int off = (4 * g + r) * 2048 + (m >> 3) * 128 + (m & 7) * 16;
-          float4 h, l;
-          h.x = tc_tf32(C[4 * r]); h.y = tc_tf32(C[4 * r + 1]); h.z = tc_tf32(C[4 * r + 2]); h.w = tc_tf32(C[4 * r + 3]);
-          l.x = tc_tf32(C[4 * r] - h.x); l.y = tc_tf32(C[4 * r + 1] - h.y);
-          l.z = tc_tf32(C[4 * r + 2] - h.z); l.w = tc_tf32(C[4 * r + 3] - h.w);
-          *reinterpret_cast<float4*>(sAh + off) = h;
-          *reinterpret_cast<float4*>(sAl + off) = l;
-        }
-      }
-      asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
-      asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
-      __syncthreads();
-      asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-      if (t == 0) {
-        const uint32_t dcol = tm + 64 * grp;
-        const uint32_t ah = tc_smem(sAh), al = tc_smem(sAl), wh = tc_smem(sWh), wl = tc_smem(sWl);
-        for (int ks = 0; ks < 16; ++ks)
-          tc_mma(dcol, tc_desc(ah + ks * 4096, 2048, 128), tc_desc(wh + ks * 2048, 1024, 128), idesc, ks > 0);
-        for (int ks = 0; ks < 16; ++ks)
-          tc_mma(dcol, tc_desc(ah + ks * 4096, 2048, 128), tc_desc(wl + ks * 2048, 1024, 128), idesc, 1u);
-        for (int ks = 0; ks < 16; ++ks)
-          tc_mma(dcol, tc_desc(al + ks * 4096, 2048, 128), tc_desc(wh + ks * 2048, 1024, 128), idesc, 1u);
-        asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(barp)
-                     : "memory");
-      }
-      // the operands are free again (and, after the last group, D is complete)
-      const bool done = tc_wait(barp, phase);
-      ok = __syncthreads_and(done) != 0;
-      if (ok) phase ^= 1u;
-      asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-    }
+    ok = tc_group<0>(hf, q, Gh, f1, f2, sAh, sAl, sWh, sWl, el, g, tm, barp, idesc, phase) &&
+         tc_group<1>(hf, q, Gh, f1, f2, sAh, sAl, sWh, sWl, el, g, tm, barp, idesc, phase) &&
+         tc_group<2>(hf, q, Gh, f1, f2, sAh, sAl, sWh, sWl, el, g, tm, barp, idesc, phase);
     if (!ok) break;
-    // epilogue: lane m = 32 wid + lane of each group's 64 columns -> staging
+    // epilogue: warp quartet hf reads columns [32 hf, 32 hf + 32) of each group's 64, lanes 32 (wid % 4) + lane
     {
-      const int m = 32 * wid + lane, t8 = m >> 4, eli = m & 15;
+      const int w4 = wid & 3, m = 32 * w4 + lane, t8 = m >> 4, eli = m & 15;
       float* dst = kst + eli * TC_KST;
+#pragma unroll
       for (int grp = 0; grp < 3; ++grp)
 #pragma unroll
-        for (int c0 = 0; c0 < 64; c0 += 16) {
+        for (int c = 0; c < 32; c += 16) {
+          const int c0 = 32 * hf + c;
           float v[16];
-          tc_ld16(tm + ((uint32_t)(32 * wid) << 16) + 64 * grp + c0, v);
+          tc_ld16(tm + ((uint32_t)(32 * w4) << 16) + 64 * grp + c0, v);
 #pragma unroll
           for (int j = 0; j < 16; ++j) dst[(c0 + j) * 24 + 8 * grp + t8] = v[j];
         }
@@ -763,7 +801,7 @@ __global__ void __launch_bounds__(128, 1) hex_tc_matrix_kernel(const HexTcArgs a
     {
       const int nel = min(TC_EB, a.E - e0);
       float4* out = reinterpret_cast<float4*>(a.kbuf + (size_t)e0 * 1536);
-      for (int i = t; i < nel * 384; i += 128) {
+      for (int i = t; i < nel * 384; i += TC_THREADS) {
         const int ee = i / 384, j4 = i - ee * 384;
         out[i] = *reinterpret_cast<const float4*>(kst + ee * TC_KST + 4 * j4);
       }
@@ -953,7 +991,7 @@ int launch_assemble_hex(ovs_ctx* c, const AsmArgs& a0, const SumArgs& sa, int pa
         const int ntiles = (sa.E + TC_EB - 1) / TC_EB;
         const int grid = ntiles < c->num_sms ? ntiles : c->num_sms;
         if (grid > 0) {
-          hex_tc_matrix_kernel<<<grid, 128, TC_SMEM, c->stream>>>(ta);
+          hex_tc_matrix_kernel<<<grid, TC_THREADS, TC_SMEM, c->stream>>>(ta);
           ++c->launches;
           OVS_CUDA_TRY(cudaGetLastError());
         }

@@ -201,7 +201,7 @@ int ovs_create(ovs_ctx** out, const ovs_dims* dims) {
     const char* e = getenv("OVS_ARNOLDI_FUSED");
     c->arnoldi_fused = e && e[0] == '1';
     const char* h = getenv("OVS_HEX_TC");
-    c->hex_tc = !(h && h[0] == '0');
+    c->hex_tc = h && h[0] == '1';
   }
   c->N = dims->nnode;
   c->E = dims->nelem;

@@ -106,8 +106,8 @@ struct ovs_ctx {
   int* fnode_ptr = nullptr;   // nfnode + 1
   int* fnode_ent = nullptr;   // 4 nface entries (face << 2) | local node, ascending face per node
   void* fbuf[2] = {nullptr, nullptr};   // per-face element arrays, per precision
-  // hex tensor-core pass (FP32 NS+VOF): on unless OVS_HEX_TC=0
-  int hex_tc = 1;
+  // hex tensor-core pass (FP32 NS+VOF): off unless OVS_HEX_TC=1 or OVS_OPT_HEX_TC
+  int hex_tc = 0;
   void* hex_kbuf = nullptr;              // E x 64 x 24 block values
   float* hex_w = nullptr;                // W hi + lo, canonical layout
   // boundary-condition producers (ovs_set_bc_spec)
