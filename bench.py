@@ -63,6 +63,28 @@ def ncu_traffic_per_tet(name, tets=663552):
                                      % (tets, name))
 
 
+def ncu_flops_per_tet(name, tets):
+    """Executed FP32 flops per tet of one launch (FFMA x 2 + FADD + FMUL
+    thread instructions) from a committed ncu summary of the kernel on a
+    workload of `tets` tets.  (None, reason) when absent."""
+    import re
+    path = os.path.join(os.path.dirname(os.path.abspath(__file__)), "profiles", name)
+    try:
+        txt = open(path).read()
+    except OSError:
+        return None, "no ncu summary"
+    def cnt(metric):
+        m = re.search(r"`%s` \| ([0-9.eE+]+)" % re.escape(metric), txt)
+        return float(m.group(1)) if m else None
+    ffma = cnt("smsp__sass_thread_inst_executed_op_ffma_pred_on.sum")
+    fadd = cnt("smsp__sass_thread_inst_executed_op_fadd_pred_on.sum")
+    fmul = cnt("smsp__sass_thread_inst_executed_op_fmul_pred_on.sum")
+    if None in (ffma, fadd, fmul):
+        return None, "no FP32 instruction counters in " + name
+    return (2 * ffma + fadd + fmul) / float(tets), ("ncu FFMA x 2 + FADD + FMUL thread instructions of one launch "
+                                                   "on a %d-tet case (profiles/%s), per tet" % (tets, name))
+
+
 def _peaks():
     try:
         return json.loads((ROOT / "MEASURED_PEAKS.json").read_text()), "measured"
@@ -456,6 +478,23 @@ def run_ours(args, world, rank, local_rank, dist):
                 "frac": as_ach / hbm, "traffic": traffic * E if traffic else None,
                 "traffic_source": traffic_src, "peak_kind": peak_kind,
                 "algorithmic_bytes": rows_bytes(4), "avg_ms": prof["asm_nsvof_fp32_rows_ms"]}
+    # compute side: executed FP32 flops of the row kernel (ncu counters) against
+    # the FMA throughput measured now on this device
+    fp32_peak = ctx.measure_fp32_peak()
+    fpt, fpt_src = ncu_flops_per_tet("assemble_rows_kernel_quench48_flops.md", 663552)
+    if fpt:
+        fl = fpt * E
+        t_hbm, t_fp = rows_bytes(4) / (hbm * 1e9), fl / (fp32_peak * 1e12)
+        roof_asm["compute"] = {"bound": "fp32", "unit": "TFLOP/s", "peak": fp32_peak, "peak_kind": "measured now",
+                               "executed_flops": fl,
+                               "achieved": fl / (prof["asm_nsvof_fp32_rows_ms"] * 1e-3) / 1e12,
+                               "frac": fl / (prof["asm_nsvof_fp32_rows_ms"] * 1e-3) / 1e12 / fp32_peak,
+                               "source": fpt_src,
+                               "bound_ms": 1e3 * max(t_hbm, t_fp),
+                               "frac_of_bound": 1e3 * max(t_hbm, t_fp) / prof["asm_nsvof_fp32_rows_ms"]}
+    else:
+        roof_asm["compute"] = {"bound": "fp32", "peak": fp32_peak, "unit": "TFLOP/s", "executed_flops": None,
+                               "source": fpt_src}
     roof_pass = {"kernels": "element_summary_kernel + assemble_rows_kernel <float,NSVOF>", "bound": "hbm",
                  "achieved": pa_ach, "peak": hbm, "unit": "GB/s", "frac": pa_ach / hbm,
                  "algorithmic_bytes": pass_bytes(4), "avg_ms": prof["asm_nsvof_fp32_ms"],

@@ -348,6 +348,11 @@ int ovs_quench_time_steps(ovs_ctx* ctx, int first_step, int nsteps, const ovs_ne
 
 /* ----------------------------------------------------------- measurement
  * Hooks for benchmarking; they have no counterpart in the reference. */
+/* Measured FP32 FMA throughput of the context's device in TFLOP/s (the
+ * compute-side roofline denominator of the CUDA-core assembly kernels);
+ * no reference counterpart (a measurement helper). */
+int ovs_measure_fp32_peak(ovs_ctx* ctx, double* tflops);
+
 enum { OVS_PROF_SPMV = 1, OVS_PROF_ASSEMBLE = 2, OVS_PROF_ARNOLDI = 3, OVS_PROF_ARNOLDI_FUSED = 4,
        OVS_PROF_ASSEMBLE_ELEMENTS = 5, OVS_PROF_ASSEMBLE_ROWS = 6 };
 /* Average device time in ms (CUDA events on the context stream) of `reps`

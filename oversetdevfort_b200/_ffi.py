@@ -53,7 +53,7 @@ EXPORTS = [
     "ovs_set_lhs_block", "ovs_spmv", "ovs_gmres", "ovs_solve", "ovs_newton_update",
     "ovs_residual_norms", "ovs_profile", "ovs_launch_count", "ovs_last_device_ms",
     "ovs_host_alloc", "ovs_host_free", "ovs_residual_vjp", "ovs_gmres_transposed", "ovs_quench_newton",
-    "ovs_quench_time_steps", "ovs_set_option", "ovs_set_faces", "ovs_set_bc_spec", "ovs_apply_bcs", "ovs_get_ibc",
+    "ovs_quench_time_steps", "ovs_measure_fp32_peak", "ovs_set_option", "ovs_set_faces", "ovs_set_bc_spec", "ovs_apply_bcs", "ovs_get_ibc",
     "ovs_gmres_tem_noalloc",
 ]
 
@@ -133,6 +133,7 @@ def load(path: str | os.PathLike | None = None) -> C.CDLL:
         "ovs_set_ibc": ([vp, ip, C.c_int], C.c_int),
         "ovs_set_faces": ([vp, C.c_int, ip, ip, ip, dp, dp], C.c_int),
         "ovs_set_option": ([vp, C.c_int, C.c_int], C.c_int),
+        "ovs_measure_fp32_peak": ([vp, dp], C.c_int),
         "ovs_set_bc_spec": ([vp, C.POINTER(OvsBcSpec)], C.c_int),
         "ovs_apply_bcs": ([vp, C.c_int], C.c_int),
         "ovs_get_ibc": ([vp, ip, C.c_int], C.c_int),

@@ -313,6 +313,12 @@ class Context:
         F.check(self.lib.ovs_profile(self.h, what, system, precision, reps, C.byref(ms)), "ovs_profile")
         return ms.value
 
+    def measure_fp32_peak(self) -> float:
+        """Measured FP32 FMA throughput of the device, TFLOP/s."""
+        t = C.c_double(0.0)
+        F.check(self.lib.ovs_measure_fp32_peak(self.h, C.byref(t)), "ovs_measure_fp32_peak")
+        return t.value
+
     def launch_count(self) -> int:
         n = C.c_longlong(0)
         F.check(self.lib.ovs_launch_count(self.h, C.byref(n)), "ovs_launch_count")

@@ -677,6 +677,48 @@ int ovs_profile(ovs_ctx* c, int what, int system, int precision, int reps, doubl
   return ovs_profile_krylov(c, what, system, precision, reps, avg_ms);
 }
 
+// FP32 FMA throughput of the device: 8 independent chains per thread,
+// 4 blocks of 256 threads per SM; the compute-side roofline denominator of
+// the assembly kernels (their work is FP32 arithmetic on the CUDA cores).
+__global__ void __launch_bounds__(256) fma_peak_kernel(float* out, int iters, float seed) {
+  float a[8];
+#pragma unroll
+  for (int k = 0; k < 8; ++k) a[k] = seed + 1e-7f * (float)threadIdx.x + (float)k;
+  const float m = 1.0000001f, b = 1e-7f;
+  for (int i = 0; i < iters; ++i) {
+#pragma unroll
+    for (int k = 0; k < 8; ++k) a[k] = fmaf(a[k], m, b);
+  }
+  float s = 0.f;
+#pragma unroll
+  for (int k = 0; k < 8; ++k) s += a[k];
+  if (threadIdx.x == 0) out[blockIdx.x] = s;
+}
+
+int ovs_measure_fp32_peak(ovs_ctx* c, double* tflops) {
+  if (!c || !tflops) return OVS_ERR_ARG;
+  int st;
+  if ((st = ovs_activate(c))) return st;
+  const int blocks = 4 * c->num_sms, iters = 1 << 14;
+  float* out = nullptr;
+  OVS_CUDA_TRY(cudaMallocAsync(&out, sizeof(float) * blocks, c->stream));
+  for (int w = 0; w < 3; ++w) fma_peak_kernel<<<blocks, 256, 0, c->stream>>>(out, iters, 1.0f);
+  OVS_CUDA_TRY(cudaEventRecord(c->ev0, c->stream));
+  const int reps = 10;
+  for (int r = 0; r < reps; ++r) fma_peak_kernel<<<blocks, 256, 0, c->stream>>>(out, iters, 1.0f);
+  OVS_CUDA_TRY(cudaEventRecord(c->ev1, c->stream));
+  c->launches += 3 + reps;
+  OVS_CUDA_TRY(cudaGetLastError());
+  OVS_CUDA_TRY(cudaEventSynchronize(c->ev1));
+  float ms = 0.f;
+  OVS_CUDA_TRY(cudaEventElapsedTime(&ms, c->ev0, c->ev1));
+  OVS_CUDA_TRY(cudaFreeAsync(out, c->stream));
+  OVS_CUDA_TRY(cudaStreamSynchronize(c->stream));
+  const double flops = 2.0 * 8.0 * iters * 256.0 * blocks * reps;
+  *tflops = flops / (ms * 1e-3) / 1e12;
+  return OVS_OK;
+}
+
 int ovs_launch_count(ovs_ctx* c, long long* n) {
   if (!c || !n) return OVS_ERR_ARG;
   *n = c->launches;
