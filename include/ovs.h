@@ -279,6 +279,24 @@ int ovs_set_lhs_block(ovs_ctx* ctx, int system, int precision, int block,
 int ovs_spmv(ovs_ctx* ctx, int system, int precision, const double* x,
              double* y);
 
+/* Device-vector building blocks of a distributed Krylov solve over
+ * owner-computes partitions (the reference's SparseGMRES_* with their commu
+ * and MPI_ALLREDUCE steps, src/SparseGMRES_NS_conv.f:65-76,169-176,210-251,
+ * 287-308,391-395): dx, dy are FP64 device vectors on this context's device
+ * in the reference layout (field-major, N x nf); each call synchronizes the
+ * context's stream before returning.
+ * ovs_build_precond: the block-diagonal preconditioner of SparseGMRES_*
+ * (3x3 velocity blocks, 1/M, 1/LS; 1/M for the temperature system) from the
+ * assembled `system`/`precision`, rebuilt on every call.
+ * ovs_spmv_device: y = A x, or y = P^-1 A x with OVS_SPMV_PRECOND.
+ * ovs_precond_device: y = P^-1 x. */
+#define OVS_SPMV_PRECOND 1
+int ovs_build_precond(ovs_ctx* ctx, int system, int precision);
+int ovs_spmv_device(ovs_ctx* ctx, int system, int precision, int flags,
+                    const double* dx, double* dy);
+int ovs_precond_device(ovs_ctx* ctx, int system, int precision,
+                       const double* dx, double* dy);
+
 /* One GMRES cycle with the reference's exact semantics, in FP64 on the FP64
  * system: SparseGMRES_up (src/SparseGMRES_NS.f90:4-369),
  * SparseGMRES_ns_conv (src/SparseGMRES_NS_conv.f:1-406),

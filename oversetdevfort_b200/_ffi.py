@@ -36,6 +36,7 @@ OVS_VJP_ACG, OVS_VJP_RPHIG, OVS_VJP_RTG, OVS_VJP_COUNT = 9, 12, 13, 14
 OVS_NOALLOC_MAX_N, OVS_NOALLOC_MAX_KSPACE = 16384, 40
 OVS_FACE_WEAK, OVS_FACE_CONVH = 1, 2
 OVS_OPT_HEX_TC, OVS_OPT_ARNOLDI_FUSED = 1, 2
+OVS_SPMV_PRECOND = 1
 (OVS_BLK_K11, OVS_BLK_G, OVS_BLK_D1, OVS_BLK_M, OVS_BLK_LS, OVS_BLK_LSU,
  OVS_BLK_ULS, OVS_BLK_PLS, OVS_BLK_TEM) = range(9)
 FIELDS = ["xg", "dg", "dgold", "ug", "ugold", "acg", "acgold", "ugm", "ugmold",
@@ -53,7 +54,7 @@ EXPORTS = [
     "ovs_set_lhs_block", "ovs_spmv", "ovs_gmres", "ovs_solve", "ovs_newton_update",
     "ovs_residual_norms", "ovs_profile", "ovs_launch_count", "ovs_last_device_ms",
     "ovs_host_alloc", "ovs_host_free", "ovs_residual_vjp", "ovs_gmres_transposed", "ovs_quench_newton",
-    "ovs_quench_time_steps", "ovs_measure_fp32_peak", "ovs_set_option", "ovs_set_faces", "ovs_set_bc_spec", "ovs_apply_bcs", "ovs_get_ibc",
+    "ovs_quench_time_steps", "ovs_build_precond", "ovs_spmv_device", "ovs_precond_device", "ovs_measure_fp32_peak", "ovs_set_option", "ovs_set_faces", "ovs_set_bc_spec", "ovs_apply_bcs", "ovs_get_ibc",
     "ovs_gmres_tem_noalloc",
 ]
 
@@ -133,6 +134,9 @@ def load(path: str | os.PathLike | None = None) -> C.CDLL:
         "ovs_set_ibc": ([vp, ip, C.c_int], C.c_int),
         "ovs_set_faces": ([vp, C.c_int, ip, ip, ip, dp, dp], C.c_int),
         "ovs_set_option": ([vp, C.c_int, C.c_int], C.c_int),
+        "ovs_build_precond": ([vp, C.c_int, C.c_int], C.c_int),
+        "ovs_spmv_device": ([vp, C.c_int, C.c_int, C.c_int, vp, vp], C.c_int),
+        "ovs_precond_device": ([vp, C.c_int, C.c_int, vp, vp], C.c_int),
         "ovs_measure_fp32_peak": ([vp, dp], C.c_int),
         "ovs_set_bc_spec": ([vp, C.POINTER(OvsBcSpec)], C.c_int),
         "ovs_apply_bcs": ([vp, C.c_int], C.c_int),

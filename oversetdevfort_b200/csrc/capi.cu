@@ -568,6 +568,34 @@ int ovs_spmv(ovs_ctx* c, int sys, int prec, const double* x, double* y) {
   return st;
 }
 
+int ovs_build_precond(ovs_ctx* c, int sys, int prec) {
+  if (!sys_ok(c, sys, prec)) return OVS_ERR_ARG;
+  int st;
+  if ((st = ovs_activate(c))) return st;
+  if ((st = ovs_precond_setup(c, sys, prec))) return st;
+  OVS_CUDA_TRY(cudaStreamSynchronize(c->stream));
+  return OVS_OK;
+}
+
+int ovs_spmv_device(ovs_ctx* c, int sys, int prec, int flags, const double* dx, double* dy) {
+  if (!sys_ok(c, sys, prec) || !dx || !dy || (flags & ~OVS_SPMV_PRECOND)) return OVS_ERR_ARG;
+  int st;
+  if ((st = ovs_activate(c))) return st;
+  st = (flags & OVS_SPMV_PRECOND) ? ovs_spmv_pre_impl(c, sys, prec, dx, dy) : ovs_spmv_impl(c, sys, prec, dx, dy);
+  if (st) return st;
+  OVS_CUDA_TRY(cudaStreamSynchronize(c->stream));
+  return OVS_OK;
+}
+
+int ovs_precond_device(ovs_ctx* c, int sys, int prec, const double* dx, double* dy) {
+  if (!sys_ok(c, sys, prec) || !dx || !dy) return OVS_ERR_ARG;
+  int st;
+  if ((st = ovs_activate(c))) return st;
+  if ((st = ovs_precond_apply_impl(c, sys, prec, dx, dy))) return st;
+  OVS_CUDA_TRY(cudaStreamSynchronize(c->stream));
+  return OVS_OK;
+}
+
 int ovs_gmres(ovs_ctx* c, int sys, double tol, int kspace, int kspace_min, double* sol, ovs_gmres_info* info) {
   if (!sys_ok(c, sys, OVS_FP64) || !sol) return OVS_ERR_ARG;
   if (kspace < 1 || kspace > OVS_MAX_KSPACE) return OVS_ERR_ARG;

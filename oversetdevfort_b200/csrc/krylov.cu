@@ -1194,6 +1194,45 @@ int ovs_precond_setup(ovs_ctx* c, int sys, int prec) {
   return OVS_OK;
 }
 
+// y = P^-1 x with the block-diagonal preconditioner in `pre` (the layout of
+// precond_setup_kernel: 3x3 velocity inverses, then 1/M and 1/LS per node;
+// one value per node for the temperature system)
+template <typename TM>
+__global__ void precond_apply_kernel(int N, int sys, const TM* __restrict__ pre, const double* __restrict__ x,
+                                     double* __restrict__ y) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= N) return;
+  const size_t n = N;
+  if (sys == OVS_SYS_TEM) { y[i] = (double)pre[i] * x[i]; return; }
+  const TM* B = pre + (size_t)i * 9;
+  const double x0 = x[i], x1 = x[n + i], x2 = x[2 * n + i];
+  for (int g = 0; g < 3; ++g)
+    y[g * n + i] = (double)B[3 * g] * x0 + (double)B[3 * g + 1] * x1 + (double)B[3 * g + 2] * x2;
+  y[3 * n + i] = x[3 * n + i] * (double)pre[9 * n + i];
+  if (sys == OVS_SYS_NSVOF) y[4 * n + i] = x[4 * n + i] * (double)pre[10 * n + i];
+}
+
+int ovs_precond_apply_impl(ovs_ctx* c, int sys, int prec, const double* dx, double* dy) {
+  SysStore& S = c->sys[sys][prec];
+  if (!S.binv) return OVS_ERR_STATE;
+  if (prec == OVS_FP64)
+    precond_apply_kernel<double><<<ovs_grid(c->N, 256, 1 << 30), 256, 0, c->stream>>>(c->N, sys, as<double>(S.binv), dx, dy);
+  else
+    precond_apply_kernel<float><<<ovs_grid(c->N, 256, 1 << 30), 256, 0, c->stream>>>(c->N, sys, as<float>(S.binv), dx, dy);
+  ++c->launches;
+  OVS_CUDA_TRY(cudaGetLastError());
+  return OVS_OK;
+}
+
+// y = P^-1 A x (dx, dy FP64 device vectors), preconditioned product
+int ovs_spmv_pre_impl(ovs_ctx* c, int sys, int prec, const double* dx, double* dy) {
+  SysStore& S = c->sys[sys][prec];
+  if (!S.vals || !S.binv) return OVS_ERR_STATE;
+  if (prec == OVS_FP64)
+    return launch_spmv<double, double, double, 1>(c, sys, as<double>(S.vals), dx, dy, as<double>(S.binv), nullptr, nullptr);
+  return launch_spmv<float, double, double, 1>(c, sys, as<float>(S.vals), dx, dy, as<float>(S.binv), nullptr, nullptr);
+}
+
 // y = A x (dx, dy FP64 device vectors), plain product
 int ovs_spmv_impl(ovs_ctx* c, int sys, int prec, const double* dx, double* dy) {
   SysStore& S = c->sys[sys][prec];

@@ -1,0 +1,266 @@
+"""Distributed Krylov solve over owner-computes partitions (one rank per GPU).
+
+The reference runs SparseGMRES_ns_conv / SparseGMRES_up / SparseGMRES_tem on
+METIS element partitions and keeps shared nodes consistent with commu: after
+each product the partial rows of shared nodes are summed on their master
+('in') and the master values are copied back ('out'), and every dot product
+is an MPI_ALLREDUCE (src/SparseGMRES_NS_conv.f:65-76, 169-176, 210-251,
+287-308, 391-395; src/commu.f90:118-266).
+
+Here every rank owns a contiguous range of nodes and holds every element
+touching them (`partition.make_parts`), so the rows of its owned nodes are
+complete after a purely local assembly.  The same GMRES cycle then needs two
+exchanges per Arnoldi step:
+
+* a halo update before each product: the ghost entries of the vector (local
+  nodes owned by another rank) receive their owners' values; the product's
+  owned rows are then exact;
+* a global sum for every dot product, over owned entries only (each node
+  counted once).
+
+The algebra of the cycle is the reference's, step for step (modified
+Gram-Schmidt with the norm as the last dot, Givens rotations, back
+substitution), as in `ovs_gmres` for one context; only the summation order
+of the dot products differs.  `LocalComm` runs several partitions in one
+process (one GPU, or the host); `TorchComm` runs one partition per process
+over `torch.distributed` (NCCL between GPUs, gloo on the host), with
+point-to-point halo messages and one all-reduce per dot product.  The local
+products are this package's CUDA kernels (`DeviceOperator`, through
+`ovs_spmv_device` / `ovs_precond_device`); the exchanges and the small
+Hessenberg algebra run on the host side of each rank.
+"""
+from __future__ import annotations
+
+import math
+from dataclasses import dataclass
+
+import numpy as np
+
+from . import _ffi as F
+
+
+@dataclass
+class HaloPlan:
+    owned: list     # per part: local indices of the owned nodes (ascending global id)
+    send: list      # send[r][s]: local indices (in r) of r's owned nodes that part s holds as ghosts
+    recv: list      # recv[r][s]: local indices (in r) of r's ghosts owned by part s
+    nlocal: list    # per part: local node count
+
+
+def halo_plan(parts) -> HaloPlan:
+    """Exchange lists of a set of `partition.Part`s (all parts of the mesh)."""
+    nparts = len(parts)
+    N = int(max(int(p.nodes.max()) for p in parts if p.nodes.size)) + 1
+    owner = np.full(N, -1, dtype=np.int64)
+    loc = []
+    for r, p in enumerate(parts):
+        owner[p.nodes[p.owned]] = r
+        lr = np.full(N, -1, dtype=np.int64)
+        lr[p.nodes] = np.arange(p.nodes.size)
+        loc.append(lr)
+    if np.any(owner < 0):
+        raise ValueError("every node must be owned by one part")
+    send = [[np.zeros(0, np.int64) for _ in range(nparts)] for _ in range(nparts)]
+    recv = [[np.zeros(0, np.int64) for _ in range(nparts)] for _ in range(nparts)]
+    for r, p in enumerate(parts):
+        own_of = owner[p.nodes]
+        for s in range(nparts):
+            if s == r:
+                continue
+            g = np.nonzero(own_of == s)[0]          # r's ghosts owned by s, ascending global id
+            recv[r][s] = g
+            send[s][r] = loc[s][p.nodes[g]]
+    return HaloPlan([np.asarray(p.owned, dtype=np.int64) for p in parts], send, recv,
+                    [int(p.nodes.size) for p in parts])
+
+
+class _Index:
+    """Index tensors of a plan on a device, made once."""
+
+    def __init__(self, plan: HaloPlan):
+        self.plan = plan
+        self.cache = {}
+
+    def get(self, key, arr, device):
+        import torch
+        k = (key, str(device))
+        if k not in self.cache:
+            self.cache[k] = torch.as_tensor(arr, dtype=torch.long, device=device)
+        return self.cache[k]
+
+
+class LocalComm:
+    """All partitions in this process: halo copies between their vectors,
+    global sums as plain sums in part order."""
+
+    def __init__(self, plan: HaloPlan):
+        self.plan = plan
+        self.idx = _Index(plan)
+
+    def parts(self):
+        return list(range(len(self.plan.owned)))
+
+    def allreduce(self, vals):
+        s = 0.0
+        for v in vals:
+            s += v
+        return s
+
+    def halo(self, vecs: dict):
+        pl = self.plan
+        for r in vecs:
+            for s in vecs:
+                if s == r or pl.recv[r][s].size == 0:
+                    continue
+                dev = vecs[r].device
+                vecs[r][:, self.idx.get(("r", r, s), pl.recv[r][s], dev)] = \
+                    vecs[s][:, self.idx.get(("s", s, r), pl.send[s][r], vecs[s].device)].to(dev)
+
+
+class TorchComm:
+    """One partition per process over torch.distributed (rank = part)."""
+
+    def __init__(self, plan: HaloPlan, rank: int, device="cpu"):
+        self.plan = plan
+        self.rank = rank
+        self.device = device
+        self.idx = _Index(plan)
+
+    def parts(self):
+        return [self.rank]
+
+    def allreduce(self, vals):
+        import torch
+        import torch.distributed as dist
+        t = torch.tensor([float(vals[0])], dtype=torch.float64, device=self.device)
+        dist.all_reduce(t)
+        return float(t.item())
+
+    def halo(self, vecs: dict):
+        import torch
+        import torch.distributed as dist
+        r, pl = self.rank, self.plan
+        x = vecs[r]
+        ops, bufs = [], []
+        for s in range(len(pl.owned)):
+            if s == r:
+                continue
+            if pl.send[r][s].size:
+                sb = x[:, self.idx.get(("s", r, s), pl.send[r][s], x.device)].contiguous()
+                ops.append(dist.P2POp(dist.isend, sb, s))
+            if pl.recv[r][s].size:
+                rb = torch.empty((x.shape[0], pl.recv[r][s].size), dtype=x.dtype, device=x.device)
+                ops.append(dist.P2POp(dist.irecv, rb, s))
+                bufs.append((s, rb))
+        if ops:
+            for q in dist.batch_isend_irecv(ops):
+                q.wait()
+        for s, rb in bufs:
+            x[:, self.idx.get(("r", r, s), pl.recv[r][s], x.device)] = rb
+
+
+class DeviceOperator:
+    """P^-1 A and P^-1 of one partition's assembled system on its context
+    (FP64 device vectors of shape (nf, N_local), field-major)."""
+
+    def __init__(self, ctx, system: int, precision: int = F.OVS_FP64):
+        self.ctx, self.system, self.precision = ctx, system, precision
+        F.check(ctx.lib.ovs_build_precond(ctx.h, system, precision), "ovs_build_precond")
+
+    @staticmethod
+    def _sync():
+        import torch
+        torch.cuda.current_stream().synchronize()
+
+    def matvec(self, x, y):
+        self._sync()
+        F.check(self.ctx.lib.ovs_spmv_device(self.ctx.h, self.system, self.precision, F.OVS_SPMV_PRECOND,
+                                             x.data_ptr(), y.data_ptr()), "ovs_spmv_device")
+
+    def precond(self, x, y):
+        self._sync()
+        F.check(self.ctx.lib.ovs_precond_device(self.ctx.h, self.system, self.precision, x.data_ptr(),
+                                                y.data_ptr()), "ovs_precond_device")
+
+
+def gmres_cycle(comm, ops: dict, rhs: dict, tol: float, kspace: int, kspace_min: int = 1, tem: bool = False):
+    """One GMRES(kspace) cycle from a zero start on the partitions of `comm`
+    (SparseGMRES_ns_conv / _up / _tem semantics): `ops[r]` the operator of
+    part r, `rhs[r]` its right-hand side (nf, N_local) with the owned rows
+    valid.  Returns (solution per part with ghosts filled, info dict)."""
+    import torch
+    P = comm.parts()
+    pl = comm.plan
+    ow = {r: torch.as_tensor(pl.owned[r], dtype=torch.long, device=rhs[r].device) for r in P}
+
+    def gdot(a, b):
+        return comm.allreduce([float((a[r][:, ow[r]] * b[r][:, ow[r]]).sum()) for r in P])
+
+    sol = {r: torch.zeros_like(rhs[r]) for r in P}
+    info = {"iterations": 0, "converged": False, "ercheck": 0.0, "res0": 0.0}
+    if tem and gdot(rhs, rhs) == 0.0:   # SparseGMRES_tem.f90:68-71
+        info["converged"] = True
+        return sol, info
+    U = [{r: torch.empty_like(rhs[r]) for r in P}]
+    for r in P:
+        ops[r].precond(rhs[r], U[0][r])
+    unorm = math.sqrt(gdot(U[0], U[0]))
+    info["res0"] = unorm
+    epsnrm = tol * unorm
+    H = np.zeros((kspace + 1, kspace))
+    e = np.zeros(kspace + 1)
+    rc, rs = np.zeros(kspace), np.zeros(kspace)
+    e[0] = unorm
+    for r in P:
+        U[0][r] = U[0][r] * (1.0 / unorm) if tem else U[0][r] / unorm
+    iks, ercheck = 0, 0.0
+    for ik in range(1, kspace + 1):
+        iks = ik
+        comm.halo(U[ik - 1])
+        w = {r: torch.empty_like(rhs[r]) for r in P}
+        for r in P:
+            ops[r].matvec(U[ik - 1][r], w[r])
+        U.append(w)
+        beta = 0.0
+        for jk in range(1, ik + 2):
+            if jk > 1:
+                for r in P:
+                    w[r] = w[r] - beta * U[jk - 2][r]
+                U[ik] = w
+            beta = gdot(w, U[jk - 1] if jk - 1 < ik else w)
+            H[jk - 1, ik - 1] = beta
+        unorm = math.sqrt(beta)
+        H[ik, ik - 1] = unorm
+        for r in P:
+            w[r] = w[r] * (1.0 / unorm) if tem else w[r] / unorm
+        U[ik] = w
+        for jk in range(1, ik):
+            t = rc[jk - 1] * H[jk - 1, ik - 1] + rs[jk - 1] * H[jk, ik - 1]
+            H[jk, ik - 1] = -rs[jk - 1] * H[jk - 1, ik - 1] + rc[jk - 1] * H[jk, ik - 1]
+            H[jk - 1, ik - 1] = t
+        a, b = H[ik - 1, ik - 1], H[ik, ik - 1]
+        t = math.sqrt(a * a + b * b)
+        if tem:
+            t1 = 1.0 / t
+            rc[ik - 1], rs[ik - 1] = a * t1, b * t1
+        else:
+            rc[ik - 1], rs[ik - 1] = a / t, b / t
+        H[ik - 1, ik - 1] = t
+        H[ik, ik - 1] = 0.0
+        t = rc[ik - 1] * e[ik - 1] + rs[ik - 1] * e[ik]
+        e[ik] = -rs[ik - 1] * e[ik - 1] + rc[ik - 1] * e[ik]
+        e[ik - 1] = t
+        ercheck = abs(e[ik])
+        if ercheck <= epsnrm and ik >= kspace_min:
+            break
+    y = np.zeros(iks)
+    for jk in range(iks, 0, -1):
+        y[jk - 1] = e[jk - 1] / H[jk - 1, jk - 1]
+        for lk in range(1, jk):
+            e[lk - 1] = e[lk - 1] - y[jk - 1] * H[lk - 1, jk - 1]
+    for jk in range(1, iks + 1):
+        for r in P:
+            sol[r] = sol[r] + float(y[jk - 1]) * U[jk - 1][r]
+    comm.halo(sol)   # commu 'out': ghosts take their owners' values
+    info.update(iterations=iks, ercheck=ercheck, converged=bool(ercheck <= epsnrm))
+    return sol, info

@@ -1,0 +1,190 @@
+"""Distributed GMRES over owner-computes partitions (oversetdevfort_b200.
+distributed), CPU: the halo plan, and the reference GMRES cycle run on
+partitions -- three in one process (LocalComm) and two gloo ranks
+(TorchComm) -- against the oracle's single-domain GMRES of the same system:
+the same iteration count and the same solution to 1e-10, ghosts included.
+The local products here use the oracle's local system (test stand-in for
+the GPU operator, which tests/test_gpu_distributed.py covers)."""
+import os
+import socket
+
+import numpy as np
+import pytest
+import torch
+
+from oversetdevfort_b200 import _ffi as F
+from oversetdevfort_b200 import distributed as D
+from oversetdevfort_b200 import mesh as M
+from oversetdevfort_b200 import partition as P
+
+NF = {"nsvof": 5, "tem": 1, "ns": 4}
+
+
+class OracleOperator:
+    """P^-1 A and P^-1 of a partition's local system assembled by the oracle
+    (block-diagonal preconditioner of SparseGMRES_*, as gm_setup_precond)."""
+
+    def __init__(self, oc, kind):
+        self.oc, self.kind = oc, kind
+        N = oc.N
+        col, row = oc.col.astype(np.int64) - 1, oc.row.astype(np.int64) - 1
+        dslot = np.zeros(N, dtype=np.int64)
+        for i in range(N):
+            j = np.nonzero(row[col[i]:col[i + 1]] == i)[0][0]
+            dslot[i] = col[i] + j
+        with np.errstate(divide="ignore", invalid="ignore"):   # singular ghost blocks, overwritten before use
+            self._setup(oc.sys, dslot, kind)
+
+    def _setup(self, s, dslot, kind):
+        if kind == "tem":
+            md = s["TEM"][dslot]
+            self.pinv = np.where(md == 0.0, 1.0, 1.0 / np.where(md == 0.0, 1.0, md))
+            return
+        K = s["K11"][dslot]
+        b11 = K[:, 4] * K[:, 8] - K[:, 7] * K[:, 5]
+        b12 = K[:, 7] * K[:, 2] - K[:, 1] * K[:, 8]
+        b13 = K[:, 1] * K[:, 5] - K[:, 2] * K[:, 4]
+        tmp = 1.0 / (b11 * K[:, 0] + b12 * K[:, 3] + b13 * K[:, 6])
+        B = np.stack([b11 * tmp, b12 * tmp, b13 * tmp,
+                      (K[:, 5] * K[:, 6] - K[:, 3] * K[:, 8]) * tmp, (K[:, 0] * K[:, 8] - K[:, 6] * K[:, 2]) * tmp,
+                      (K[:, 3] * K[:, 2] - K[:, 0] * K[:, 5]) * tmp, (K[:, 3] * K[:, 7] - K[:, 4] * K[:, 6]) * tmp,
+                      (K[:, 6] * K[:, 1] - K[:, 0] * K[:, 7]) * tmp, (K[:, 0] * K[:, 4] - K[:, 1] * K[:, 3]) * tmp], 1)
+        self.B = B
+        md = s["M"][dslot]
+        self.pinv = np.where(md == 0.0, 1.0, 1.0 / np.where(md == 0.0, 1.0, md))
+        if kind == "nsvof":
+            ld = s["LS"][dslot]
+            self.lsinv = np.where(ld == 0.0, 0.0, 1.0 / np.where(ld == 0.0, 1.0, ld))
+
+    def _pre(self, x):   # x (nf, N) numpy; ghost rows are incomplete and may be singular
+        if self.kind == "tem":
+            return self.pinv[None, :] * x
+        y = np.empty_like(x)
+        for g in range(3):
+            y[g] = self.B[:, 3 * g] * x[0] + self.B[:, 3 * g + 1] * x[1] + self.B[:, 3 * g + 2] * x[2]
+        y[3] = x[3] * self.pinv
+        if self.kind == "nsvof":
+            y[4] = x[4] * self.lsinv
+        return y
+
+    def precond(self, x, y):
+        with np.errstate(invalid="ignore"):
+            y.copy_(torch.from_numpy(self._pre(x.numpy())))
+
+    def matvec(self, x, y):
+        ax = self.oc.spmv(self.kind, np.asfortranarray(x.numpy().T))
+        with np.errstate(invalid="ignore"):
+            y.copy_(torch.from_numpy(self._pre(np.ascontiguousarray(ax.T))))
+
+
+def _case(kind):
+    # a quench box: every node in fluid elements, so every diagonal block is
+    # regular (random cases with solid-only nodes give singular blocks, and
+    # the reference preconditioner NaNs on them in one domain or many)
+    return M.quench_case(M.box_tet(6, 5, 8, 1.0, 1.0, 1.25), "dist")
+
+
+def _local(oracle, case, part, kind):
+    oc = oracle.OracleCase(P.local_case(case, part))
+    oc.assemble_quenching(6, 4 if kind == "tem" else 3)
+    return oc
+
+
+def _global(oracle, case, kind, tol, kspace):
+    og = oracle.OracleCase(case)
+    og.assemble_quenching(6, 4 if kind == "tem" else 3)
+    s, it, er, r0 = og.gmres(kind, tol, kspace, 1)
+    assert np.isfinite(s).all() and it < kspace   # converged inside the cycle
+    return s, it
+
+
+def test_halo_plan_and_exchange():
+    case = _case("nsvof")
+    parts = P.make_parts(case.mesh, 3)
+    plan = D.halo_plan(parts)
+    N = case.mesh.nnode
+    covered = np.zeros(N, dtype=int)
+    for r, p in enumerate(parts):
+        covered[p.nodes[plan.owned[r]]] += 1
+        ghosts = np.setdiff1d(np.arange(p.nodes.size), plan.owned[r])
+        got = np.concatenate([plan.recv[r][s] for s in range(3) if s != r])
+        np.testing.assert_array_equal(np.sort(got), ghosts)
+        for s in range(3):
+            if s != r:   # what s sends to r are the same global nodes, in the same order
+                np.testing.assert_array_equal(parts[s].nodes[plan.send[s][r]], p.nodes[plan.recv[r][s]])
+    assert np.all(covered == 1)
+    g = np.random.default_rng(0).standard_normal((2, N))
+    vecs = {r: torch.from_numpy(np.where(np.isin(np.arange(p.nodes.size), plan.owned[r]), g[:, p.nodes], -7.0))
+            for r, p in enumerate(parts)}
+    D.LocalComm(plan).halo(vecs)
+    for r, p in enumerate(parts):
+        np.testing.assert_array_equal(vecs[r].numpy(), g[:, p.nodes])
+
+
+@pytest.mark.parametrize("kind", ["nsvof", "tem"])
+def test_local_comm_gmres_matches_single_domain(oracle, kind):
+    case = _case(kind)
+    tol, kspace = 1e-8, 200
+    sg, itg = _global(oracle, case, kind, tol, kspace)
+    parts = P.make_parts(case.mesh, 3)
+    plan = D.halo_plan(parts)
+    ops, rhs = {}, {}
+    for r, p in enumerate(parts):
+        oc = _local(oracle, case, p, kind)
+        ops[r] = OracleOperator(oc, kind)
+        rhs[r] = torch.from_numpy(np.ascontiguousarray(oc.system(kind)["rhs"].T))
+    sol, info = D.gmres_cycle(D.LocalComm(plan), ops, rhs, tol, kspace, 1, tem=kind == "tem")
+    assert info["converged"] and info["iterations"] == itg
+    scale = np.abs(sg).max()
+    for r, p in enumerate(parts):
+        np.testing.assert_allclose(sol[r].numpy().T, sg[p.nodes], atol=1e-10 * scale, rtol=0)
+
+
+def _free_port() -> int:
+    s = socket.socket()
+    s.bind(("127.0.0.1", 0))
+    port = s.getsockname()[1]
+    s.close()
+    return port
+
+
+def _rank_main(rank, world, port, q):
+    import datetime
+    import torch.distributed as dist
+    from oracle import pyoracle
+    os.environ["MASTER_ADDR"] = "127.0.0.1"
+    os.environ["MASTER_PORT"] = str(port)
+    dist.init_process_group("gloo", rank=rank, world_size=world, timeout=datetime.timedelta(seconds=120))
+    kind, tol, kspace = "nsvof", 1e-8, 200
+    case = _case(kind)
+    parts = P.make_parts(case.mesh, world)
+    plan = D.halo_plan(parts)
+    oc = _local(pyoracle, case, parts[rank], kind)
+    ops = {rank: OracleOperator(oc, kind)}
+    rhs = {rank: torch.from_numpy(np.ascontiguousarray(oc.system(kind)["rhs"].T))}
+    sol, info = D.gmres_cycle(D.TorchComm(plan, rank), ops, rhs, tol, kspace, 1)
+    gathered = [None] * world if rank == 0 else None
+    dist.gather_object((parts[rank].nodes, sol[rank].numpy(), info["iterations"]), gathered, dst=0)
+    if rank == 0:
+        sg, itg = _global(pyoracle, case, kind, tol, kspace)
+        scale = np.abs(sg).max()
+        ok = all(it == itg and np.isfinite(s).all() and np.abs(s.T - sg[nodes]).max() <= 1e-10 * scale
+                 for nodes, s, it in gathered)
+        q.put(bool(ok))
+    dist.barrier()
+    dist.destroy_process_group()
+
+
+def test_two_gloo_ranks_gmres(oracle):
+    import torch.multiprocessing as mp
+    ctx = mp.get_context("spawn")
+    q = ctx.Queue()
+    port = _free_port()
+    procs = [ctx.Process(target=_rank_main, args=(r, 2, port, q)) for r in range(2)]
+    for p in procs:
+        p.start()
+    ok = q.get(timeout=300)
+    for p in procs:
+        p.join(timeout=120)
+        assert p.exitcode == 0
+    assert ok
