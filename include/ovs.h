@@ -297,6 +297,27 @@ int ovs_spmv_device(ovs_ctx* ctx, int system, int precision, int flags,
 int ovs_precond_device(ovs_ctx* ctx, int system, int precision,
                        const double* dx, double* dy);
 
+/* Streaming time steps (the Newton drivers push the state and read the
+ * residual back every iteration, src/solveFlow.f90:39-40, 71-72, 116-117,
+ * 148-149): copies that overlap the assembly instead of preceding it.
+ * ovs_stage_fields: copies host fields (ids OVS_F_*, reference layout;
+ *   page-locked host memory lets the copies run asynchronously) into a second
+ *   device buffer per field on an upload stream, after the work committed
+ *   so far has stopped reading those buffers; returns at once; the host
+ *   arrays must stay unchanged until ovs_sync_copies or the next commit has
+ *   waited for them.
+ * ovs_commit_staged: work issued afterwards waits for the staged copies and
+ *   reads the staged fields (the swap covers only the fields staged since the
+ *   last commit); OVS_ERR_STATE when nothing is staged.
+ * ovs_get_rhs_async: the right-hand side of `system` as FP64 into `host`
+ *   through a download stream, after the work issued so far; `host` is valid
+ *   after ovs_sync_copies.
+ * ovs_sync_copies: waits for both copy streams. */
+int ovs_stage_fields(ovs_ctx* ctx, int nfields, const int* ids, const double* const* host);
+int ovs_commit_staged(ovs_ctx* ctx);
+int ovs_get_rhs_async(ovs_ctx* ctx, int system, int precision, double* host);
+int ovs_sync_copies(ovs_ctx* ctx);
+
 /* One GMRES cycle with the reference's exact semantics, in FP64 on the FP64
  * system: SparseGMRES_up (src/SparseGMRES_NS.f90:4-369),
  * SparseGMRES_ns_conv (src/SparseGMRES_NS_conv.f:1-406),

@@ -172,6 +172,35 @@ class Context:
         F.check(self.lib.ovs_get_ibc(self.h, _iptr(out), nibc), "ovs_get_ibc")
         return out
 
+    # ------------------------------------------------ streaming time steps
+    def stage_fields(self, arrays: dict):
+        """Copies {field name: host array (reference layout; page-locked for
+        asynchronous copies, e.g. PinnedArray.array)} into the staging buffers
+        on the upload stream; returns at once.  The arrays must stay alive and
+        unchanged until the next commit has been followed by sync_copies."""
+        names = list(arrays)
+        ids = (C.c_int * len(names))(*[F.FIELD_ID[n] for n in names])
+        self._staged_keep = [np.asarray(arrays[n]) for n in names]
+        for a in self._staged_keep:
+            if a.dtype != np.float64 or not (a.flags.f_contiguous or a.ndim == 1):
+                raise ValueError("stage_fields wants float64 arrays in reference (column-major) layout")
+        ptrs = (C.POINTER(C.c_double) * len(names))(*[_dptr(a) for a in self._staged_keep])
+        F.check(self.lib.ovs_stage_fields(self.h, len(names), ids, ptrs), "ovs_stage_fields")
+
+    def commit_staged(self):
+        F.check(self.lib.ovs_commit_staged(self.h), "ovs_commit_staged")
+
+    def get_rhs_async(self, system: int, precision: int, out: np.ndarray):
+        """Queues the read-back of the right-hand side into `out` ((N, nf)
+        float64, column-major; page-locked for an asynchronous copy); valid
+        after sync_copies."""
+        if out.dtype != np.float64 or out.shape != (self.N, NF[system]) or not out.flags.f_contiguous:
+            raise ValueError("out must be a column-major float64 (N, nf) array")
+        F.check(self.lib.ovs_get_rhs_async(self.h, system, precision, _dptr(out)), "ovs_get_rhs_async")
+
+    def sync_copies(self):
+        F.check(self.lib.ovs_sync_copies(self.h), "ovs_sync_copies")
+
     def set_field(self, name: str, arr: np.ndarray):
         a = _f64(arr)
         F.check(self.lib.ovs_set_field(self.h, F.FIELD_ID[name], _dptr(a)), f"ovs_set_field({name})")

@@ -239,6 +239,7 @@ int ovs_destroy(ovs_ctx* c) {
   if (c->stream) cudaStreamSynchronize(c->stream);
   ovs_faces_free(c);
   ovs_bcs_free(c);
+  ovs_streaming_free(c);
   if (c->hex_kbuf) cudaFree(c->hex_kbuf);
   if (c->hex_w) cudaFree(c->hex_w);
   void* ptrs[] = {c->ien, c->elm_id, c->ibc, c->rowptr, c->colidx, c->diag, c->n2e_ptr, c->n2e, c->n2s, c->tmap, c->vals_t, c->vjp_cot, c->vjp_ge, c->vjp_grad,

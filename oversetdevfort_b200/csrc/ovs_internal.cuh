@@ -106,6 +106,13 @@ struct ovs_ctx {
   int* fnode_ptr = nullptr;   // nfnode + 1
   int* fnode_ent = nullptr;   // 4 nface entries (face << 2) | local node, ascending face per node
   void* fbuf[2] = {nullptr, nullptr};   // per-face element arrays, per precision
+  // streaming time steps (streaming.cu): staged field buffers, copy streams
+  double* stage[OVS_F_COUNT] = {};
+  unsigned staged_mask = 0;
+  double* rhs_out[4] = {};                // FP64 read-back buffer per system
+  cudaStream_t up_stream = nullptr, up_stream2 = nullptr, down_stream = nullptr;
+  cudaEvent_t ev_staged = nullptr, ev_staged2 = nullptr, ev_commit = nullptr, ev_rhs_ready = nullptr,
+              ev_rhs_out = nullptr;
   // hex tensor-core pass (FP32 NS+VOF): off unless OVS_HEX_TC=1 or OVS_OPT_HEX_TC
   int hex_tc = 0;
   void* hex_kbuf = nullptr;              // E x 64 x 24 block values
@@ -160,6 +167,9 @@ int ovs_assemble_impl(ovs_ctx* c, int kernel, int tensor_flag, int prec,
 
 // assemble.cu: W operand and block buffer of the hex tensor-core pass
 int hex_tc_prepare(ovs_ctx* c);
+
+// streaming.cu
+void ovs_streaming_free(ovs_ctx* c);
 
 // faces.cu
 int ovs_faces_set_impl(ovs_ctx* c, int nface, const int* f2e, const int* face_or, const int* flags,
