@@ -304,8 +304,9 @@ int ovs_precond_device(ovs_ctx* ctx, int system, int precision,
  *   page-locked host memory lets the copies run asynchronously) into a second
  *   device buffer per field on an upload stream, after the work committed
  *   so far has stopped reading those buffers; returns at once; the host
- *   arrays must stay unchanged until ovs_sync_copies or the next commit has
- *   waited for them.
+ *   arrays must stay unchanged until, after the commit that consumes them, a
+ *   call that waits for the compute stream (ovs_assemble, ovs_sync_copies)
+ *   has returned.
  * ovs_commit_staged: work issued afterwards waits for the staged copies and
  *   reads the staged fields (the swap covers only the fields staged since the
  *   last commit); OVS_ERR_STATE when nothing is staged.
