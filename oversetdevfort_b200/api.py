@@ -176,8 +176,9 @@ class Context:
     def stage_fields(self, arrays: dict):
         """Copies {field name: host array (reference layout; page-locked for
         asynchronous copies, e.g. PinnedArray.array)} into the staging buffers
-        on the upload stream; returns at once.  The arrays must stay alive and
-        unchanged until the next commit has been followed by sync_copies."""
+        on the upload streams; returns at once.  The arrays must stay alive
+        and unchanged until, after the commit that consumes them, a call that
+        waits for the compute stream (assemble, sync_copies) has returned."""
         names = list(arrays)
         ids = (C.c_int * len(names))(*[F.FIELD_ID[n] for n in names])
         self._staged_keep = [np.asarray(arrays[n]) for n in names]
