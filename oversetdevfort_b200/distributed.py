@@ -24,7 +24,8 @@ substitution), as in `ovs_gmres` for one context; only the summation order
 of the dot products differs.  `LocalComm` runs several partitions in one
 process (one GPU, or the host); `TorchComm` runs one partition per process
 over `torch.distributed` (NCCL between GPUs, gloo on the host), with
-point-to-point halo messages and one all-reduce per dot product.  The local
+point-to-point halo messages and one all-reduce per dot product (or, with
+orthog="cgs2", two vector all-reduces and one norm per Arnoldi step).  The local
 products are this package's CUDA kernels (`DeviceOperator`, through
 `ovs_spmv_device` / `ovs_precond_device`); the exchanges and the small
 Hessenberg algebra run on the host side of each rank.
@@ -106,6 +107,12 @@ class LocalComm:
             s += v
         return s
 
+    def allreduce_vec(self, vals):
+        s = np.zeros_like(vals[0])
+        for v in vals:
+            s = s + v
+        return s
+
     def halo(self, vecs: dict):
         pl = self.plan
         for r in vecs:
@@ -135,6 +142,13 @@ class TorchComm:
         t = torch.tensor([float(vals[0])], dtype=torch.float64, device=self.device)
         dist.all_reduce(t)
         return float(t.item())
+
+    def allreduce_vec(self, vals):
+        import torch
+        import torch.distributed as dist
+        t = torch.as_tensor(np.asarray(vals[0], dtype=np.float64), device=self.device).clone()
+        dist.all_reduce(t)
+        return t.cpu().numpy()
 
     def halo(self, vecs: dict):
         import torch
@@ -183,11 +197,18 @@ class DeviceOperator:
                                                 y.data_ptr()), "ovs_precond_device")
 
 
-def gmres_cycle(comm, ops: dict, rhs: dict, tol: float, kspace: int, kspace_min: int = 1, tem: bool = False):
+def gmres_cycle(comm, ops: dict, rhs: dict, tol: float, kspace: int, kspace_min: int = 1, tem: bool = False,
+                orthog: str = "mgs"):
     """One GMRES(kspace) cycle from a zero start on the partitions of `comm`
     (SparseGMRES_ns_conv / _up / _tem semantics): `ops[r]` the operator of
     part r, `rhs[r]` its right-hand side (nf, N_local) with the owned rows
-    valid.  Returns (solution per part with ghosts filled, info dict)."""
+    valid.  orthog "mgs" is the reference's modified Gram-Schmidt (one global
+    sum per dot, k + 1 at step k); "cgs2" orthogonalizes with classical
+    Gram-Schmidt twice (two vector sums and one norm per step, whatever k),
+    for ranks where the latency of a collective outweighs its size.
+    Returns (solution per part with ghosts filled, info dict)."""
+    if orthog not in ("mgs", "cgs2"):
+        raise ValueError("orthog must be 'mgs' or 'cgs2'")
     import torch
     P = comm.parts()
     pl = comm.plan
@@ -221,14 +242,25 @@ def gmres_cycle(comm, ops: dict, rhs: dict, tol: float, kspace: int, kspace_min:
         for r in P:
             ops[r].matvec(U[ik - 1][r], w[r])
         U.append(w)
-        beta = 0.0
-        for jk in range(1, ik + 2):
-            if jk > 1:
+        if orthog == "mgs":
+            beta = 0.0
+            for jk in range(1, ik + 2):
+                if jk > 1:
+                    for r in P:
+                        w[r] = w[r] - beta * U[jk - 2][r]
+                    U[ik] = w
+                beta = gdot(w, U[jk - 1] if jk - 1 < ik else w)
+                H[jk - 1, ik - 1] = beta
+        else:
+            for _ in range(2):
+                loc = [np.array([float((U[j][r][:, ow[r]] * w[r][:, ow[r]]).sum()) for j in range(ik)]) for r in P]
+                h = comm.allreduce_vec(loc)
                 for r in P:
-                    w[r] = w[r] - beta * U[jk - 2][r]
-                U[ik] = w
-            beta = gdot(w, U[jk - 1] if jk - 1 < ik else w)
-            H[jk - 1, ik - 1] = beta
+                    for j in range(ik):
+                        w[r] = w[r] - float(h[j]) * U[j][r]
+                H[:ik, ik - 1] += h
+            U[ik] = w
+            beta = gdot(w, w)
         unorm = math.sqrt(beta)
         H[ik, ik - 1] = unorm
         for r in P:

@@ -140,6 +140,31 @@ def test_local_comm_gmres_matches_single_domain(oracle, kind):
         np.testing.assert_allclose(sol[r].numpy().T, sg[p.nodes], atol=1e-10 * scale, rtol=0)
 
 
+def test_cgs2_orthogonalization_converges_to_the_same_solution(oracle):
+    """The batched (classical, twice) Gram-Schmidt variant: two vector sums
+    per Arnoldi step instead of k + 1 scalar ones; it reaches the tolerance
+    within a few iterations of the reference's modified Gram-Schmidt and the
+    same solution to the tolerance's order."""
+    kind = "nsvof"
+    case = _case(kind)
+    tol, kspace = 1e-8, 200
+    sg, itg = _global(oracle, case, kind, tol, kspace)
+    parts = P.make_parts(case.mesh, 3)
+    plan = D.halo_plan(parts)
+    ops, rhs = {}, {}
+    for r, p in enumerate(parts):
+        oc = _local(oracle, case, p, kind)
+        ops[r] = OracleOperator(oc, kind)
+        rhs[r] = torch.from_numpy(np.ascontiguousarray(oc.system(kind)["rhs"].T))
+    sol, info = D.gmres_cycle(D.LocalComm(plan), ops, rhs, tol, kspace, 1, orthog="cgs2")
+    assert info["converged"] and abs(info["iterations"] - itg) <= 3
+    scale = np.abs(sg).max()
+    for r, p in enumerate(parts):
+        np.testing.assert_allclose(sol[r].numpy().T, sg[p.nodes], atol=1e-6 * scale, rtol=0)
+    with pytest.raises(ValueError):
+        D.gmres_cycle(D.LocalComm(plan), ops, rhs, tol, kspace, 1, orthog="householder")
+
+
 def _free_port() -> int:
     s = socket.socket()
     s.bind(("127.0.0.1", 0))
