@@ -439,12 +439,14 @@ int ovs_get_rhs(ovs_ctx* c, int sys, int prec, double* rhs) {
   if (prec == OVS_FP64) {
     OVS_CUDA_TRY(cudaMemcpyAsync(rhs, S.rhs, sizeof(double) * n, cudaMemcpyDeviceToHost, c->stream));
   } else {
-    double* tmp = nullptr;
-    OVS_CUDA_TRY(cudaMallocAsync(&tmp, sizeof(double) * n, c->stream));
+    // through the context's FP64 read-back buffer of this system (no
+    // allocation per call), after any asynchronous read-back still using it
+    if ((st = ovs_ensure((void**)&c->rhs_out[sys], sizeof(double) * n))) return st;
+    if (c->ev_rhs_out) OVS_CUDA_TRY(cudaStreamWaitEvent(c->stream, c->ev_rhs_out, 0));
+    double* tmp = c->rhs_out[sys];
     copy_convert_kernel<float, double><<<ovs_grid(n, 256, 1 << 30), 256, 0, c->stream>>>((const float*)S.rhs, tmp, n);
     ++c->launches;
     OVS_CUDA_TRY(cudaMemcpyAsync(rhs, tmp, sizeof(double) * n, cudaMemcpyDeviceToHost, c->stream));
-    OVS_CUDA_TRY(cudaFreeAsync(tmp, c->stream));
   }
   OVS_CUDA_TRY(cudaStreamSynchronize(c->stream));
   return OVS_OK;
