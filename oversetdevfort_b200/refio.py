@@ -189,6 +189,27 @@ def faces_from_part(pm: PartMesh, weak=(), convective=None) -> "M.BoundaryFaces"
     return M.BoundaryFaces(*(np.concatenate(c) for c in zip(*parts)))
 
 
+def bc_spec_from_part(pm: PartMesh, bcug_type, bcug_valu, bcphig_type, bcphig_valu, bctg_type, bctg_valu,
+                      node_id=None) -> "M.BcSpec":
+    """The input of setBCs_NSVOF / setBCs_Tem for a partition read from
+    part.dat: per boundary in file order its FACE_ID and BNODES, with the
+    tables of src/param.f90:296-340 as the reference holds them (the *Type
+    tables read by FACE_ID, the *Valu tables by boundary number); NodeID from
+    the file unless given."""
+    nb = len(pm.bounds)
+    fid = np.array([b.face_id for b in pm.bounds], dtype=np.int32)
+    spec = M.BcSpec(fid, [np.asarray(b.bnodes, dtype=np.int32) for b in pm.bounds],
+                    np.asarray(bcug_type, dtype=np.int32).reshape(-1, 3),
+                    np.asarray(bcug_valu, dtype=np.float64).reshape(nb, 3),
+                    np.asarray(bcphig_type, dtype=np.int32), np.asarray(bcphig_valu, dtype=np.float64),
+                    np.asarray(bctg_type, dtype=np.int32), np.asarray(bctg_valu, dtype=np.float64),
+                    np.asarray(pm.node_id if node_id is None else node_id, dtype=np.int32))
+    nt = spec.bcug_type.shape[0]
+    if fid.size and (fid.min() < 1 or fid.max() > nt):
+        raise ValueError("a FACE_ID is outside the *Type tables (setBCs reads them by FACE_ID)")
+    return spec
+
+
 # the records of a restart, in file order, and the state arrays they fill
 RESTART_READ = ("dgold", "ugold", "ugmold", "acgold", "acgmold", "phigold", "rphigold", "pgold", "tgold", "rtgold")
 RESTART_WRITE = ("dg", "ug", "ugm", "acg", "acgm", "phig", "rphig", "pg", "tgold", "rtgold")

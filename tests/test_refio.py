@@ -106,3 +106,42 @@ def test_part_faces_round_trip_to_face_set(tmp_path):
     for a, b in zip((bf.f2e, bf.face_or, bf.flags, bf.hconv, bf.tinf),
                     (ref.f2e, ref.face_or, ref.flags, ref.hconv, ref.tinf)):
         np.testing.assert_array_equal(a, b)
+
+
+def test_bc_spec_from_part_drives_setbcs_like_the_box_spec(tmp_path, oracle):
+    """setBCs on a mesh read back from part.dat, with the boundaries and
+    NodeID of the file, gives the state and IBC of the same BCs given on the
+    box mesh directly."""
+    m = M.box_tet(3, 2, 2, 1.0, 0.5, 2.0)
+    pm = refio.part_from_mesh(m)
+    pm.node_id[:] = 0
+    pm.node_id[[1, 7]] = 101
+    path = tmp_path / "part5.dat"
+    refio.write_part(path, pm)
+    back = refio.read_part(path)
+    ut = np.zeros((6, 3), np.int32)
+    uv = np.zeros((6, 3))
+    ut[5] = (1, 0, 1)
+    uv[5] = (1.0, 0.0, -0.5)
+    ut[0] = (1, 1, 1)
+    pt, pv = np.zeros(6, np.int32), np.zeros(6)
+    pt[4], pv[4] = 1, 1.0
+    tt, tv = np.zeros(6, np.int32), np.zeros(6)
+    tt[4], tv[4] = 1, 420.0
+    spec_file = refio.bc_spec_from_part(back, ut, uv, pt, pv, tt, tv)
+    spec_box = M.box_bc_spec(m, u={6: (1.0, None, -0.5), 1: (0.0, 0.0, 0.0)}, phi={5: 1.0}, T={5: 420.0},
+                             node_id=pm.node_id)
+    rng = np.random.default_rng(4)
+    st = M.empty_state(m.nnode)
+    for k, a in st.items():
+        a[...] = rng.standard_normal(a.shape)
+    ibc = np.asfortranarray(np.zeros((m.nnode, 8), dtype=np.int32))
+    a = oracle.OracleCase(M.Case("f", m, M.base_params(), {k: v.copy() for k, v in st.items()}, ibc.copy(), 2))
+    b = oracle.OracleCase(M.Case("b", m, M.base_params(), {k: v.copy() for k, v in st.items()}, ibc.copy(), 2))
+    a.set_bcs(spec_file, 3)
+    b.set_bcs(spec_box, 3)
+    for k in a.state_arrays:
+        np.testing.assert_array_equal(a.state_arrays[k], b.state_arrays[k])
+    np.testing.assert_array_equal(a.ibc, b.ibc)
+    with pytest.raises(ValueError):
+        refio.bc_spec_from_part(back, ut[:3], uv, pt, pv, tt, tv)
