@@ -127,9 +127,16 @@ class LocalComm:
 class TorchComm:
     """One partition per process over torch.distributed (rank = part)."""
 
-    def __init__(self, plan: HaloPlan, rank: int, device="cpu"):
+    def __init__(self, plan: HaloPlan, rank: int, device=None):
+        """device: where the all-reduce buffers live; by default the current
+        CUDA device with the NCCL backend, the host otherwise."""
         self.plan = plan
         self.rank = rank
+        if device is None:
+            import torch
+            import torch.distributed as dist
+            nccl = dist.is_initialized() and dist.get_backend() == "nccl"
+            device = f"cuda:{torch.cuda.current_device()}" if nccl else "cpu"
         self.device = device
         self.idx = _Index(plan)
 
