@@ -3,8 +3,10 @@
 The reference ships no tests or golden vectors, so the oracle is pinned by
 answers known in closed form: pattern counts of the Kuhn split and of the
 27-point hex stencil, the binary-search semantics of SparseMatLoc_3D, the
-Galerkin mass of a single tet, the domain volume, partition of unity, and
-GMRES against dense LU.
+Galerkin mass of a single tet, the domain volume, partition of unity,
+GMRES against dense LU, and two patch tests of the quench element routines
+(a linear temperature field leaves no interior conduction residual; a
+linear pressure field gives -grad p times the lumped nodal volume).
 """
 import numpy as np
 import pytest
@@ -259,3 +261,72 @@ def test_golden_fixture_regression(oracle):
     fresh = mg.compute()
     for k in g.files:
         np.testing.assert_array_equal(g[k], fresh[k], err_msg=k)
+
+
+def _interior(m):
+    nx, ny, nz = m.dims
+    i = np.arange(m.nnode)
+    ix, iy, iz = i % (nx + 1), (i // (nx + 1)) % (ny + 1), i // ((nx + 1) * (ny + 1))
+    return (ix > 0) & (ix < nx) & (iy > 0) & (iy < ny) & (iz > 0) & (iz < nz)
+
+
+def _lumped_volume(m):
+    """sum over the elements around each node of |T| / 4"""
+    x = np.asarray(m.xg)
+    ien0 = np.asarray(m.ien) - 1
+    a, b, c, d = (x[ien0[:, k]] for k in range(4))
+    vol = np.abs(np.einsum("ij,ij->i", b - a, np.cross(c - a, d - a))) / 6.0
+    out = np.zeros(m.nnode)
+    for k in range(4):
+        np.add.at(out, ien0[:, k], vol / 4.0)
+    return out
+
+
+def _still_case(m, **par):
+    p = M.base_params(c_evap=0.0, c_cond=0.0, ns_kdc_w=0.0, ns_kdc_a=0.0, lsc_kdc=0.0, tem_kdc=0.0,
+                      gravvec=(0.0, 0.0, 0.0), **par)
+    st = M.empty_state(m.nnode)
+    ibc = np.zeros((m.nnode, 8), dtype=np.int32, order="F")
+    return p, st, ibc
+
+
+def test_temperature_patch_and_mass(oracle):
+    """No flow, no rate, no phase change, T linear in x: the conduction
+    residual of every interior node is zero (linear elements reproduce a
+    linear field exactly), and the temperature mass entries sum to
+    alpha_m rho c_p volume."""
+    m = M.box_tet(3, 3, 4, 1.0, 0.8, 1.1)
+    p, st, ibc = _still_case(m)
+    x = np.asarray(m.xg)
+    T = 300.0 + 5.0 * x[:, 0] + 2.0 * x[:, 1] - 3.0 * x[:, 2]
+    for f in ("tg", "tgold"):
+        st[f][:] = T
+    oc = oracle.OracleCase(M.Case("tpatch", m, p, st, ibc, F.OVS_ASM_NSVOF))
+    oc.assemble_quenching(F.OVS_TENSOR_MAT | F.OVS_TENSOR_VEC, 4)
+    r = oc.sys["rhstem"]
+    inner = _interior(m)
+    assert inner.sum() > 0
+    scale = np.abs(r).max()
+    assert scale > 0.0 and np.abs(r[inner]).max() <= 1e-12 * scale
+    rcp = p["rhow"] * p["cpw"]
+    want = p["almi"] * rcp * 1.0 * 0.8 * 1.1
+    assert abs(oc.sys["TEM"].sum() - want) <= 1e-12 * want
+
+
+def test_pressure_gradient_patch(oracle):
+    """No flow, no acceleration, no gravity, p linear: the momentum residual
+    of an interior node is -grad p times the node's lumped volume
+    (sum of |T|/4 over its elements), and the VOF residual vanishes."""
+    m = M.box_tet(4, 3, 3, 1.2, 0.9, 0.75)
+    p, st, ibc = _still_case(m)
+    x = np.asarray(m.xg)
+    g = np.array([2.0, -1.5, 0.75])
+    st["pg"][:] = 10.0 + x @ g
+    oc = oracle.OracleCase(M.Case("ppatch", m, p, st, ibc, F.OVS_ASM_NSVOF))
+    oc.assemble_quenching(F.OVS_TENSOR_VEC, 3)
+    inner = _interior(m)
+    lv = _lumped_volume(m)
+    ru = oc.sys["rhsu"]
+    want = -lv[inner, None] * g[None, :]
+    np.testing.assert_allclose(ru[inner], want, rtol=1e-12, atol=1e-12 * np.abs(want).max())
+    assert np.abs(oc.sys["rhsls"]).max() == 0.0
