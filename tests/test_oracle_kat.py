@@ -4,9 +4,11 @@ The reference ships no tests or golden vectors, so the oracle is pinned by
 answers known in closed form: pattern counts of the Kuhn split and of the
 27-point hex stencil, the binary-search semantics of SparseMatLoc_3D, the
 Galerkin mass of a single tet, the domain volume, partition of unity,
-GMRES against dense LU, and two patch tests of the quench element routines
-(a linear temperature field leaves no interior conduction residual; a
-linear pressure field gives -grad p times the lumped nodal volume).
+GMRES against dense LU, and patch tests of the element routines (a linear
+temperature field leaves no interior conduction residual; a linear pressure
+field gives -grad p times the lumped nodal volume; a linear divergence-free
+velocity moving with the mesh leaves no interior momentum or continuity
+residual).
 """
 import numpy as np
 import pytest
@@ -313,7 +315,15 @@ def test_temperature_patch_and_mass(oracle):
     assert abs(oc.sys["TEM"].sum() - want) <= 1e-12 * want
 
 
-def test_pressure_gradient_patch(oracle):
+def _assemble_vec(oc, kernel):
+    if kernel == F.OVS_ASM_NS:
+        oc.assemble_navsto(F.OVS_TENSOR_VEC)
+    else:
+        oc.assemble_quenching(F.OVS_TENSOR_VEC, 3)
+
+
+@pytest.mark.parametrize("kernel", [F.OVS_ASM_NSVOF, F.OVS_ASM_NS])
+def test_pressure_gradient_patch(oracle, kernel):
     """No flow, no acceleration, no gravity, p linear: the momentum residual
     of an interior node is -grad p times the node's lumped volume
     (sum of |T|/4 over its elements), and the VOF residual vanishes."""
@@ -322,11 +332,36 @@ def test_pressure_gradient_patch(oracle):
     x = np.asarray(m.xg)
     g = np.array([2.0, -1.5, 0.75])
     st["pg"][:] = 10.0 + x @ g
-    oc = oracle.OracleCase(M.Case("ppatch", m, p, st, ibc, F.OVS_ASM_NSVOF))
-    oc.assemble_quenching(F.OVS_TENSOR_VEC, 3)
+    oc = oracle.OracleCase(M.Case("ppatch", m, p, st, ibc, kernel))
+    _assemble_vec(oc, kernel)
     inner = _interior(m)
     lv = _lumped_volume(m)
     ru = oc.sys["rhsu"]
     want = -lv[inner, None] * g[None, :]
     np.testing.assert_allclose(ru[inner], want, rtol=1e-12, atol=1e-12 * np.abs(want).max())
-    assert np.abs(oc.sys["rhsls"]).max() == 0.0
+    if kernel == F.OVS_ASM_NSVOF:
+        assert np.abs(oc.sys["rhsls"]).max() == 0.0
+
+
+@pytest.mark.parametrize("kernel", [F.OVS_ASM_NSVOF, F.OVS_ASM_NS])
+def test_viscous_patch(oracle, kernel):
+    """A linear, divergence-free velocity carried by the mesh (no advection),
+    no acceleration, no pressure: the viscous term of linear elements
+    reproduces it exactly, so every interior node has zero momentum and
+    continuity residual (the stabilisation and divergence terms vanish
+    with the advection velocity and div u)."""
+    m = M.box_tet(4, 4, 3, 1.0, 1.0, 0.8)
+    p, st, ibc = _still_case(m, muw=0.7, mua=0.7)
+    x = np.asarray(m.xg)
+    A = np.array([[0.3, 1.2, -0.4], [0.5, -0.9, 0.8], [-0.2, 0.6, 0.6]])   # trace 0
+    u = x @ A.T
+    for f in ("ug", "ugold", "ugm", "ugmold"):
+        st[f][:] = u
+    oc = oracle.OracleCase(M.Case("vpatch", m, p, st, ibc, kernel))
+    _assemble_vec(oc, kernel)
+    inner = _interior(m)
+    ru, rp = oc.sys["rhsu"], oc.sys["rhsp"]
+    scale = max(np.abs(ru).max(), 1e-300)
+    assert np.abs(ru).max() > 0.0                    # boundary nodes carry the traction
+    assert np.abs(ru[inner]).max() <= 1e-12 * scale
+    assert np.abs(rp[inner]).max() <= 1e-12 * max(np.abs(rp).max(), scale)
