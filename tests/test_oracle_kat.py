@@ -273,9 +273,17 @@ def _interior(m):
 
 
 def _lumped_volume(m):
-    """sum over the elements around each node of |T| / 4"""
+    """sum over the elements around each node of |T| / 4 (|cell| / 8 for the
+    box's hexahedra)"""
     x = np.asarray(m.xg)
     ien0 = np.asarray(m.ien) - 1
+    if m.nshl == 8:
+        lx, ly, lz = m.lengths
+        nx, ny, nz = m.dims
+        out = np.zeros(m.nnode)
+        for k in range(8):
+            np.add.at(out, ien0[:, k], lx * ly * lz / (nx * ny * nz) / 8.0)
+        return out
     a, b, c, d = (x[ien0[:, k]] for k in range(4))
     vol = np.abs(np.einsum("ij,ij->i", b - a, np.cross(c - a, d - a))) / 6.0
     out = np.zeros(m.nnode)
@@ -292,12 +300,13 @@ def _still_case(m, **par):
     return p, st, ibc
 
 
-def test_temperature_patch_and_mass(oracle):
+@pytest.mark.parametrize("box", [M.box_tet, M.box_hex])
+def test_temperature_patch_and_mass(oracle, box):
     """No flow, no rate, no phase change, T linear in x: the conduction
     residual of every interior node is zero (linear elements reproduce a
     linear field exactly), and the temperature mass entries sum to
     alpha_m rho c_p volume."""
-    m = M.box_tet(3, 3, 4, 1.0, 0.8, 1.1)
+    m = box(3, 3, 4, 1.0, 0.8, 1.1)
     p, st, ibc = _still_case(m)
     x = np.asarray(m.xg)
     T = 300.0 + 5.0 * x[:, 0] + 2.0 * x[:, 1] - 3.0 * x[:, 2]
@@ -322,12 +331,13 @@ def _assemble_vec(oc, kernel):
         oc.assemble_quenching(F.OVS_TENSOR_VEC, 3)
 
 
-@pytest.mark.parametrize("kernel", [F.OVS_ASM_NSVOF, F.OVS_ASM_NS])
-def test_pressure_gradient_patch(oracle, kernel):
+@pytest.mark.parametrize("kernel,box", [(F.OVS_ASM_NSVOF, M.box_tet), (F.OVS_ASM_NS, M.box_tet),
+                                        (F.OVS_ASM_NSVOF, M.box_hex)])
+def test_pressure_gradient_patch(oracle, kernel, box):
     """No flow, no acceleration, no gravity, p linear: the momentum residual
     of an interior node is -grad p times the node's lumped volume
     (sum of |T|/4 over its elements), and the VOF residual vanishes."""
-    m = M.box_tet(4, 3, 3, 1.2, 0.9, 0.75)
+    m = box(4, 3, 3, 1.2, 0.9, 0.75)
     p, st, ibc = _still_case(m)
     x = np.asarray(m.xg)
     g = np.array([2.0, -1.5, 0.75])
@@ -343,14 +353,15 @@ def test_pressure_gradient_patch(oracle, kernel):
         assert np.abs(oc.sys["rhsls"]).max() == 0.0
 
 
-@pytest.mark.parametrize("kernel", [F.OVS_ASM_NSVOF, F.OVS_ASM_NS])
-def test_viscous_patch(oracle, kernel):
+@pytest.mark.parametrize("kernel,box", [(F.OVS_ASM_NSVOF, M.box_tet), (F.OVS_ASM_NS, M.box_tet),
+                                        (F.OVS_ASM_NSVOF, M.box_hex)])
+def test_viscous_patch(oracle, kernel, box):
     """A linear, divergence-free velocity carried by the mesh (no advection),
     no acceleration, no pressure: the viscous term of linear elements
     reproduces it exactly, so every interior node has zero momentum and
     continuity residual (the stabilisation and divergence terms vanish
     with the advection velocity and div u)."""
-    m = M.box_tet(4, 4, 3, 1.0, 1.0, 0.8)
+    m = box(4, 4, 3, 1.0, 1.0, 0.8)
     p, st, ibc = _still_case(m, muw=0.7, mua=0.7)
     x = np.asarray(m.xg)
     A = np.array([[0.3, 1.2, -0.4], [0.5, -0.9, 0.8], [-0.2, 0.6, 0.6]])   # trace 0
