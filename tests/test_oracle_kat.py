@@ -8,7 +8,8 @@ GMRES against dense LU, and patch tests of the element routines (a linear
 temperature field leaves no interior conduction residual; a linear pressure
 field gives -grad p times the lumped nodal volume; a linear divergence-free
 velocity moving with the mesh leaves no interior momentum or continuity
-residual).
+residual; uniform advection of linear phi and T with the rates that cancel
+it leaves no VOF residual and no interior temperature residual).
 """
 import numpy as np
 import pytest
@@ -376,3 +377,48 @@ def test_viscous_patch(oracle, kernel, box):
     assert np.abs(ru).max() > 0.0                    # boundary nodes carry the traction
     assert np.abs(ru[inner]).max() <= 1e-12 * scale
     assert np.abs(rp[inner]).max() <= 1e-12 * max(np.abs(rp).max(), scale)
+
+
+@pytest.mark.parametrize("box", [M.box_tet, M.box_hex])
+def test_advection_patch(oracle, box):
+    """Uniform advection velocity, linear phi and T, and the rates that make
+    their transport residuals vanish pointwise (rphi = -u.grad phi,
+    rT = -u.grad T, no phase change): the Galerkin and SUPG terms, both
+    weighted by that residual, give nothing, so the VOF residual is zero at
+    every node and the temperature residual at every interior node (linear
+    conduction leaves only the boundary flux)."""
+    m = box(4, 3, 3, 1.0, 0.9, 0.8)
+    p, st, ibc = _still_case(m)
+    x = np.asarray(m.xg)
+    u = np.array([0.6, -0.25, 0.4])
+    gphi, gT = np.array([0.1, 0.05, -0.08]), np.array([4.0, -2.0, 1.0])
+    for f in ("ug", "ugold"):
+        st[f][:] = u
+    phi = 0.4 + x @ gphi
+    T = 320.0 + x @ gT
+    for f in ("phig", "phigold"):
+        st[f][:] = phi
+    for f in ("rphig", "rphigold"):
+        st[f][:] = -(u @ gphi)
+    for f in ("tg", "tgold"):
+        st[f][:] = T
+    for f in ("rtg", "rtgold"):
+        st[f][:] = -(u @ gT)
+    oc = oracle.OracleCase(M.Case("apatch", m, p, st, ibc, F.OVS_ASM_NSVOF))
+    oc.assemble_quenching(F.OVS_TENSOR_VEC, 3)
+    rl = oc.sys["rhsls"]
+    assert np.abs(rl).max() <= 1e-13
+    # temperature with a uniform phase (variable conductivity would add a flux)
+    for f in ("phig", "phigold"):
+        st[f][:] = 0.0
+    for f in ("rphig", "rphigold"):
+        st[f][:] = 0.0
+    oc = oracle.OracleCase(M.Case("apatch_t", m, p, st, ibc, F.OVS_ASM_NSVOF))
+    oc.assemble_quenching(F.OVS_TENSOR_VEC, 4)
+    rt = oc.sys["rhstem"]
+    inner = _interior(m)
+    assert np.abs(rt).max() > 0.0
+    # the cancelled terms are rho c_p |u.grad T| per unit volume (~4e4 per node
+    # here): round-off of their size, not of the boundary flux
+    terms = p["rhow"] * p["cpw"] * abs(u @ gT) * _lumped_volume(m).max()
+    assert np.abs(rt[inner]).max() <= 1e-12 * terms
