@@ -422,3 +422,66 @@ def test_advection_patch(oracle, box):
     # here): round-off of their size, not of the boundary flux
     terms = p["rhow"] * p["cpw"] * abs(u @ gT) * _lumped_volume(m).max()
     assert np.abs(rt[inner]).max() <= 1e-12 * terms
+
+
+@pytest.mark.parametrize("box", [M.box_tet, M.box_hex])
+def test_temperature_matrix_is_the_residual_jacobian(oracle, box):
+    """No flow, no phase change, one phase: the temperature residual is
+    linear in the state, so after the Newton update with a vector d
+    (rT += d, T += gamma Delt d, src/solveFlow.f90:139-140) the residual
+    changes by exactly -K d, K the assembled temperature matrix
+    (alpha_m mass + alpha_f gamma Delt conduction)."""
+    m = box(3, 3, 3, 1.0, 0.9, 1.1)
+    p, st, ibc = _still_case(m)
+    rng = np.random.default_rng(11)
+    for f in ("tg", "tgold"):
+        st[f][:] = 320.0 + 10.0 * rng.standard_normal(m.nnode)
+    for f in ("rtg", "rtgold"):
+        st[f][:] = rng.standard_normal(m.nnode)
+    oc = oracle.OracleCase(M.Case("tjac", m, p, st, ibc, F.OVS_ASM_NSVOF))
+    oc.assemble_quenching(F.OVS_TENSOR_MAT | F.OVS_TENSOR_VEC, 4)
+    r0 = oc.sys["rhstem"].copy()
+    d = rng.standard_normal(m.nnode)
+    kd = oc.spmv("tem", np.asfortranarray(d[:, None]))[:, 0]
+    oc.newton_update(F.OVS_SYS_TEM, np.asfortranarray(d[:, None]))
+    oc.assemble_quenching(F.OVS_TENSOR_VEC, 4)
+    dr = oc.sys["rhstem"] - r0
+    np.testing.assert_allclose(dr, -kd, rtol=0, atol=1e-11 * np.abs(kd).max())
+
+
+def test_ns_matrix_is_the_residual_jacobian_at_rest(oracle):
+    """NS-only routine at a uniform flow carried by the mesh (u_adv = 0,
+    grad u = 0) with random acceleration and pressure: the stabilisation
+    parameters and the convection term have no first-order change there, so
+    after a Newton update with eps d (acg += d, ug += gamma Delt d,
+    pg += alpha_f gamma Delt d_p) the momentum residual changes by -K eps d up
+    to O(eps^2).  The continuity rows are not the residual's Jacobian: the
+    routine hands zeros to e3RHS as uprime (src/assembleNavSto.f90:284-288),
+    so its residual has no PSPG term while its matrix keeps the PSPG blocks;
+    a pressure-only update leaves the continuity residual unchanged."""
+    m = M.box_tet(3, 3, 3, 1.0, 1.0, 1.0)
+    p, st, ibc = _still_case(m, rhoa=1.3, mua=0.05, subdomain_flag=1, elm_id_set=(102, 0))
+    rng = np.random.default_rng(5)
+    U = np.array([0.3, -0.2, 0.1])
+    for f in ("ug", "ugold", "ugm", "ugmold"):
+        st[f][:] = U
+    for f in ("acg", "acgold"):
+        st[f][:] = rng.standard_normal((m.nnode, 3))
+    st["pg"][:] = rng.standard_normal(m.nnode)
+
+    def change(d):
+        oc = oracle.OracleCase(M.Case("nsjac", m, p, {k: v.copy() for k, v in st.items()}, ibc, F.OVS_ASM_NS))
+        oc.assemble_navsto(F.OVS_TENSOR_MAT | F.OVS_TENSOR_VEC)
+        r0 = np.concatenate([oc.sys["rhsu"], oc.sys["rhsp"][:, None]], axis=1)
+        kd = oc.spmv("ns", np.asfortranarray(d))
+        oc.newton_update(F.OVS_SYS_NS, np.asfortranarray(d))
+        oc.assemble_navsto(F.OVS_TENSOR_VEC)
+        return np.concatenate([oc.sys["rhsu"], oc.sys["rhsp"][:, None]], axis=1) - r0, kd
+
+    eps = 1e-6
+    dr, kd = change(eps * rng.standard_normal((m.nnode, 4)))
+    np.testing.assert_allclose(dr[:, :3], -kd[:, :3], rtol=0, atol=1e-8 * np.abs(kd[:, :3]).max())
+    dp = np.zeros((m.nnode, 4))
+    dp[:, 3] = eps * rng.standard_normal(m.nnode)
+    dr, kd = change(dp)
+    assert np.all(dr[:, 3] == 0.0) and np.abs(kd[:, 3]).max() > 0.0
