@@ -485,3 +485,45 @@ def test_ns_matrix_is_the_residual_jacobian_at_rest(oracle):
     dp[:, 3] = eps * rng.standard_normal(m.nnode)
     dr, kd = change(dp)
     assert np.all(dr[:, 3] == 0.0) and np.abs(kd[:, 3]).max() > 0.0
+
+
+def test_nsvof_matrix_against_residual_change_at_rest(oracle):
+    """NS+VOF quench routine at a uniform flow carried by the mesh, one
+    phase, no phase change: under the Newton update (acg += d_u,
+    ug += gamma Delt d_u, pg += alpha_f gamma Delt d_p, rphig += d_phi,
+    phig += gamma Delt d_phi) the residual changes by -K d in the continuity
+    rows for a velocity update and in the momentum rows for a pressure update
+    (exactly: linear there), in the momentum rows for a small velocity update
+    up to O(eps), and in the VOF rows for a VOF update (exactly); the momentum
+    rows do not follow a VOF update (rho(phi) and mu(phi) are not in the
+    matrix's u-row/phi-column blocks)."""
+    m = M.box_tet(3, 3, 3, 1.0, 1.0, 1.0)
+    p, st, ibc = _still_case(m, muw=0.05, mua=0.05)
+    rng = np.random.default_rng(5)
+    for f in ("ug", "ugold", "ugm", "ugmold"):
+        st[f][:] = np.array([0.3, -0.2, 0.1])
+    for f in ("acg", "acgold"):
+        st[f][:] = rng.standard_normal((m.nnode, 3))
+    st["pg"][:] = rng.standard_normal(m.nnode)
+
+    def change(cols, eps):
+        oc = oracle.OracleCase(M.Case("vjac", m, p, {k: v.copy() for k, v in st.items()}, ibc, F.OVS_ASM_NSVOF))
+        oc.assemble_quenching(F.OVS_TENSOR_MAT | F.OVS_TENSOR_VEC, 3)
+        cat = lambda: np.concatenate([oc.sys["rhsu"], oc.sys["rhsp"][:, None], oc.sys["rhsls"][:, None]], axis=1)
+        r0 = cat()
+        d = np.zeros((m.nnode, 5))
+        d[:, cols] = eps * rng.standard_normal((m.nnode, len(cols)))
+        kd = oc.spmv("nsvof", np.asfortranarray(d))
+        oc.newton_update(F.OVS_SYS_NSVOF, np.asfortranarray(d))
+        oc.assemble_quenching(F.OVS_TENSOR_VEC, 3)
+        return cat() - r0, kd
+
+    dr, kd = change([0, 1, 2], 1e-6)
+    sc = np.abs(kd).max()
+    assert np.abs(dr[:, 3] + kd[:, 3]).max() <= 1e-9 * sc          # continuity rows: exact
+    assert np.abs(dr[:, :3] + kd[:, :3]).max() <= 1e-4 * sc        # momentum rows: O(eps)
+    dr, kd = change([3], 1.0)
+    assert np.abs(dr[:, :4] + kd[:, :4]).max() <= 1e-9 * np.abs(kd).max()   # linear in p
+    dr, kd = change([4], 1e-6)
+    assert np.abs(dr[:, 4] + kd[:, 4]).max() <= 1e-9 * np.abs(kd[:, 4]).max()   # VOF rows: exact
+    assert np.abs(kd[:, :3]).max() == 0.0 and np.abs(dr[:, :3]).max() > 0.0      # no phi columns in u rows
