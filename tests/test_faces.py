@@ -139,3 +139,46 @@ def test_constrained_nodes_get_face_diagonal(oracle):
     assert touching > 0
     assert s1["K11"][kd, 0] - s0["K11"][kd, 0] == 2 * touching
     assert np.all(s1["rhs"][node, 0] == 0.0)
+
+
+def test_weak_face_matrix_is_its_residual_jacobian(oracle):
+    """FaceAssembly_NS_weak + _outflow at a uniform flow carried by the mesh
+    (every wall weak): the face terms are linear in u and p there (the
+    backflow term is second order), so with them the NS momentum rows stay
+    the Jacobian of the residual under the Newton update, and the continuity
+    rows' departure (the NS routine's missing PSPG residual) is the same as
+    without faces."""
+    m = M.box_tet(3, 3, 3, 1.0, 1.0, 1.0)
+    p = M.base_params(gravvec=(0.0, 0.0, 0.0), rhoa=1.3, mua=0.05, ns_kdc_a=0.0, subdomain_flag=1,
+                      elm_id_set=(102, 0))
+    st = M.empty_state(m.nnode)
+    rng = np.random.default_rng(5)
+    for f in ("ug", "ugold", "ugm", "ugmold"):
+        st[f][:] = np.array([0.3, -0.2, 0.1])
+    for f in ("acg", "acgold"):
+        st[f][:] = rng.standard_normal((m.nnode, 3))
+    st["pg"][:] = rng.standard_normal(m.nnode)
+    ibc = np.asfortranarray(np.zeros((m.nnode, 8), dtype=np.int32))
+    bf = M.face_set(m, weak=(1, 2, 3, 4, 5, 6))
+
+    def miss(d, faces):
+        case = M.Case("fjac", m, p, {k: v.copy() for k, v in st.items()}, ibc, F.OVS_ASM_NS)
+        case.bfaces = bf if faces else None
+        oc = oracle.OracleCase(case)
+        oc.assemble_navsto(6)
+        r0 = np.concatenate([oc.sys["rhsu"], oc.sys["rhsp"][:, None]], axis=1)
+        kd = oc.spmv("ns", np.asfortranarray(d))
+        oc.newton_update(F.OVS_SYS_NS, np.asfortranarray(d))
+        oc.assemble_navsto(2)
+        return np.concatenate([oc.sys["rhsu"], oc.sys["rhsp"][:, None]], axis=1) - r0 + kd, kd
+
+    du = np.zeros((m.nnode, 4))
+    du[:, :3] = 1e-6 * rng.standard_normal((m.nnode, 3))
+    dp = np.zeros((m.nnode, 4))
+    dp[:, 3] = rng.standard_normal(m.nnode)
+    for d, tol in ((du, 1e-8), (dp, 1e-11)):
+        e1, k1 = miss(d, True)
+        e0, k0 = miss(d, False)
+        assert np.abs(k1 - k0).max() > 0.0                         # the faces are in the matrix
+        assert np.abs(e1[:, :3]).max() <= tol * np.abs(k1).max()    # momentum rows: Jacobian
+        assert np.abs(e1[:, 3] - e0[:, 3]).max() <= 1e-9 * np.abs(k1).max()
