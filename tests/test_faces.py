@@ -182,3 +182,28 @@ def test_weak_face_matrix_is_its_residual_jacobian(oracle):
         assert np.abs(k1 - k0).max() > 0.0                         # the faces are in the matrix
         assert np.abs(e1[:, :3]).max() <= tol * np.abs(k1).max()    # momentum rows: Jacobian
         assert np.abs(e1[:, 3] - e0[:, 3]).max() <= 1e-9 * np.abs(k1).max()
+
+
+def test_convective_face_matrix_is_its_residual_jacobian(oracle):
+    """The convective heat term is linear in T: with it on three walls the
+    temperature matrix stays the exact Jacobian of the temperature residual
+    under the Newton update (rT += d, T += gamma Delt d)."""
+    m = M.box_tet(3, 3, 3, 1.0, 0.9, 1.1)
+    p = M.base_params(c_evap=0.0, c_cond=0.0, tem_kdc=0.0)
+    st = M.empty_state(m.nnode)
+    rng = np.random.default_rng(11)
+    for f in ("tg", "tgold"):
+        st[f][:] = 320.0 + 10.0 * rng.standard_normal(m.nnode)
+    for f in ("rtg", "rtgold"):
+        st[f][:] = rng.standard_normal(m.nnode)
+    ibc = np.asfortranarray(np.zeros((m.nnode, 8), dtype=np.int32))
+    case = M.Case("cjac", m, p, st, ibc, F.OVS_ASM_NSVOF)
+    case.bfaces = M.face_set(m, convective={1: (40.0, 290.0), 4: (15.0, 300.0), 6: (80.0, 280.0)})
+    oc = oracle.OracleCase(case)
+    oc.assemble_quenching(6, 4)
+    r0 = oc.sys["rhstem"].copy()
+    d = rng.standard_normal(m.nnode)
+    kd = oc.spmv("tem", np.asfortranarray(d[:, None]))[:, 0]
+    oc.newton_update(F.OVS_SYS_TEM, np.asfortranarray(d[:, None]))
+    oc.assemble_quenching(2, 4)
+    np.testing.assert_allclose(oc.sys["rhstem"] - r0, -kd, rtol=0, atol=1e-11 * np.abs(kd).max())
