@@ -1,0 +1,28 @@
+"""The bench's readers of the committed ncu summaries (CPU): the DRAM
+traffic and the executed FP32 flops per tet that bench.py puts into its
+roofline entries come out of profiles/ with the expected values, and a
+missing summary is reported rather than guessed."""
+import os
+import sys
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+sys.path.insert(0, ROOT)
+
+import bench  # noqa: E402
+
+
+def test_dram_traffic_per_tet_from_profile():
+    per_tet, src = bench.ncu_traffic_per_tet("assemble_rows_kernel_quench128_dram.md", 12582912)
+    assert per_tet is not None and "profiles/assemble_rows_kernel_quench128_dram.md" in src
+    # 8.28 GB per launch of the 128^3 case
+    assert abs(per_tet * 12582912 / 1e9 - 8.28) < 0.01
+
+
+def test_fp32_flops_per_tet_from_profile():
+    per_tet, src = bench.ncu_flops_per_tet("assemble_rows_kernel_quench48_flops.md", 663552)
+    assert per_tet == 4948.0 and "FFMA" in src
+
+
+def test_missing_summaries_are_reported():
+    assert bench.ncu_traffic_per_tet("no_such_summary.md", 1) == (None, "no ncu summary")
+    assert bench.ncu_flops_per_tet("no_such_summary.md", 1) == (None, "no ncu summary")
