@@ -17,6 +17,7 @@ HERE = Path(__file__).resolve().parent
 LIB = HERE / "_build" / "libovs_oracle.so"
 
 _dp = C.POINTER(C.c_double)
+OVS_SYS_NSVOF, OVS_SYS_TEM = 2, 3   # system ids of include/ovs.h
 _ip = C.POINTER(C.c_int)
 
 
@@ -257,6 +258,43 @@ class OracleCase:
     def newton_update(self, system: int, sol: np.ndarray):
         s = np.asfortranarray(sol, dtype=np.float64)
         load().orc_newton_update(self.N, system, C.byref(self.params), C.byref(self.state), _d(s))
+
+    def quench_newton(self, newton_max: int, solve_tem: bool, kspace: int, kspace_min: int, tol_ns: float,
+                      tol_tem: float, utol, atol):
+        """The Newton loop of solmultiphasethermofluid_stag
+        (src/solveFlow.f90:4-164) on this case's state: the residual of all
+        fields first (:39-46), then per Newton iteration the NS+VOF matrix and
+        residual, one reference GMRES cycle from zero (SparseGMRES_ns_conv),
+        its update (:99-104); the temperature likewise when solve_tem
+        (:116-140); the residual of all fields again and check_convergence
+        (:190-215: r < utol r0 or r < atol per field group, all groups).
+        Returns a dict with iterations, converged, residual0, residual and
+        the Krylov iterations."""
+        def vec_all():   # one call for all fields, as :39-40 and :148-149 (a call zeroes every RHS)
+            self.assemble_quenching(2, 7)
+            return self.calculate_residual()
+
+        r0 = vec_all()
+        r = r0.copy()
+        conv = lambda rr: all(rr[k] < utol[k] * r0[k] or rr[k] < atol[k] for k in range(4))
+        out = {"iterations": 0, "converged": conv(r), "residual0": r0, "krylov_ns": 0, "krylov_tem": 0}
+        for it in range(1, newton_max + 1):
+            self.assemble_quenching(6, 3)
+            s, k, _, _ = self.gmres("nsvof", tol_ns, kspace, kspace_min)
+            out["krylov_ns"] += k
+            self.newton_update(OVS_SYS_NSVOF, s)
+            if solve_tem:
+                self.assemble_quenching(6, 4)
+                s, k, _, _ = self.gmres("tem", tol_tem, kspace, kspace_min)
+                out["krylov_tem"] += k
+                self.newton_update(OVS_SYS_TEM, s)
+            r = vec_all()
+            out["iterations"] = it
+            out["converged"] = conv(r)
+            if out["converged"]:
+                break
+        out["residual"] = r
+        return out
 
     def calculate_residual(self) -> np.ndarray:
         r = np.zeros(4)

@@ -527,3 +527,25 @@ def test_nsvof_matrix_against_residual_change_at_rest(oracle):
     dr, kd = change([4], 1e-6)
     assert np.abs(dr[:, 4] + kd[:, 4]).max() <= 1e-9 * np.abs(kd[:, 4]).max()   # VOF rows: exact
     assert np.abs(kd[:, :3]).max() == 0.0 and np.abs(dr[:, :3]).max() > 0.0      # no phi columns in u rows
+
+
+def test_oracle_newton_loop_reduces_the_residuals(oracle):
+    """The oracle's solmultiphasethermofluid_stag loop on a small quench box:
+    every Newton iteration solves the NS+VOF and temperature systems with one
+    reference GMRES cycle and updates the state; three iterations cut the
+    momentum, continuity and temperature residuals (sums of squares) by
+    orders of magnitude, and the iteration stops once check_convergence
+    holds."""
+    case = M.quench_case(M.box_tet(5, 5, 6, 1.0, 1.0, 1.25), "onewton")
+    rng = np.random.default_rng(3)   # a stirred start: the box at rest has no momentum residual
+    free = np.asarray(case.ibc)[:, 0] == 0
+    for f in ("ug", "ugold"):
+        case.state[f][free] = 0.05 * rng.standard_normal((int(free.sum()), 3))
+    oc = oracle.OracleCase(case)
+    out = oc.quench_newton(3, True, 100, 1, 1e-8, 1e-8, (1e-6,) * 4, (1e-30,) * 4)
+    r0, r = out["residual0"], out["residual"]
+    assert out["iterations"] >= 1 and out["krylov_ns"] > 0 and out["krylov_tem"] > 0
+    for k in (0, 1, 3):
+        assert r0[k] > 0.0 and r[k] < 1e-3 * r0[k], (k, r[k], r0[k])
+    loose = oracle.OracleCase(case).quench_newton(5, True, 100, 1, 1e-8, 1e-8, (1e30,) * 4, (1e-30,) * 4)
+    assert loose["converged"] and loose["iterations"] == 1   # the loop body runs before the first check
