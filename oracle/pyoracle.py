@@ -296,6 +296,28 @@ class OracleCase:
         out["residual"] = r
         return out
 
+    def quench_time_steps(self, first_step: int, nsteps: int, newton_max: int, solve_tem: bool, kspace: int,
+                          kspace_min: int, tol_ns: float, tol_tem: float, utol, atol):
+        """The driver's time loop around the Newton routine (src/driver.f90:
+        70-100): per step the predictor ug = ugold, acg = (gami - 1)/gami
+        acgold (:83-85), the Newton loop with NL_max = 1 while istep <= 1
+        (src/solveFlow.f90:50-54) and no temperature solve at istep 0
+        (:109), then the old values the driver updates (ug, acg, dg, ugm,
+        acgm).  Returns the last step's Newton record."""
+        st = self.state_arrays
+        g = self.params.gami
+        out = None
+        for k in range(nsteps):
+            istep = first_step + k
+            st["ug"][...] = st["ugold"]
+            st["acg"][...] = (g - 1.0) / g * st["acgold"]
+            out = self.quench_newton(1 if istep <= 1 else newton_max, solve_tem and istep > 0, kspace,
+                                     kspace_min, tol_ns, tol_tem, utol, atol)
+            for cur, old in (("ug", "ugold"), ("acg", "acgold"), ("dg", "dgold"), ("ugm", "ugmold"),
+                             ("acgm", "acgmold")):
+                st[old][...] = st[cur]
+        return out
+
     def calculate_residual(self) -> np.ndarray:
         r = np.zeros(4)
         load().orc_calculate_residual(self.N, C.byref(self.csys), _d(r))

@@ -549,3 +549,20 @@ def test_oracle_newton_loop_reduces_the_residuals(oracle):
         assert r0[k] > 0.0 and r[k] < 1e-3 * r0[k], (k, r[k], r0[k])
     loose = oracle.OracleCase(case).quench_newton(5, True, 100, 1, 1e-8, 1e-8, (1e30,) * 4, (1e-30,) * 4)
     assert loose["converged"] and loose["iterations"] == 1   # the loop body runs before the first check
+
+
+def test_oracle_time_loop(oracle):
+    """The oracle's driver loop: after each step the old velocity and
+    acceleration equal the new ones, step 0 solves no temperature and takes
+    one Newton iteration, and two steps move the state."""
+    case = M.quench_case(M.box_tet(4, 4, 5, 1.0, 1.0, 1.25), "otime")
+    oc = oracle.OracleCase(case)
+    t0 = oc.state_arrays["tg"].copy()
+    out = oc.quench_time_steps(0, 1, 3, True, 80, 1, 1e-8, 1e-8, (1e-6,) * 4, (1e-30,) * 4)
+    assert out["iterations"] == 1 and out["krylov_tem"] == 0
+    np.testing.assert_array_equal(oc.state_arrays["tg"], t0)          # no temperature solve at step 0
+    out = oc.quench_time_steps(1, 2, 3, True, 80, 1, 1e-8, 1e-8, (1e-6,) * 4, (1e-30,) * 4)
+    assert out["krylov_tem"] > 0
+    for cur, old in (("ug", "ugold"), ("acg", "acgold")):
+        np.testing.assert_array_equal(oc.state_arrays[cur], oc.state_arrays[old])
+    assert np.abs(oc.state_arrays["tg"] - t0).max() > 0.0
