@@ -57,12 +57,28 @@ def make_parts(m: "M.Mesh", nparts: int) -> list[Part]:
     return parts
 
 
+def local_faces(bf: "M.BoundaryFaces", part: Part) -> "M.BoundaryFaces":
+    """The boundary faces whose element is in the partition, in the global
+    loop order, with local element ids.  Every element touching an owned
+    node is local, so the face terms of the owned rows are all there."""
+    loc = np.full(int(part.elements.max()) + 2 if part.elements.size else 1, -1, dtype=np.int64)
+    loc[part.elements] = np.arange(part.elements.size)
+    e = np.asarray(bf.f2e, dtype=np.int64) - 1
+    keep = (e < loc.size) & (loc[np.minimum(e, loc.size - 1)] >= 0)
+    return M.BoundaryFaces((loc[e[keep]] + 1).astype(np.int32), np.asarray(bf.face_or)[keep],
+                           np.asarray(bf.flags)[keep], np.asarray(bf.hconv)[keep], np.asarray(bf.tinf)[keep])
+
+
 def local_case(case: "M.Case", part: Part) -> "M.Case":
-    """The case restricted to a partition: local mesh, state, IBC."""
+    """The case restricted to a partition: local mesh, state, IBC and
+    boundary faces."""
     st = {k: np.asfortranarray(np.asarray(v)[part.nodes]) for k, v in case.state.items()}
     ibc = np.asfortranarray(np.asarray(case.ibc)[part.nodes])
-    return M.Case(f"{case.name}_p{part.rank}", part.mesh, dict(case.params), st, ibc, case.kernel,
-                  case.kspace, case.gmres_tol, case.newton_iters, dict(case.extra))
+    lc = M.Case(f"{case.name}_p{part.rank}", part.mesh, dict(case.params), st, ibc, case.kernel,
+                case.kspace, case.gmres_tol, case.newton_iters, dict(case.extra))
+    if case.bfaces is not None:
+        lc.bfaces = local_faces(case.bfaces, part)
+    return lc
 
 
 def owned_rows(col: np.ndarray, row: np.ndarray, vals: np.ndarray, part: Part):

@@ -41,6 +41,32 @@ def test_owned_rows_match_global_assembly(oracle, kind, hexm):
         np.testing.assert_array_equal(lsys["rhs"][part.owned], gsys["rhs"][part.global_rows])
 
 
+@pytest.mark.parametrize("kind", ["nsvof", "tem"])
+def test_owned_rows_with_faces_match_global_assembly(oracle, kind):
+    """With weak and convective boundary faces: each partition keeps the
+    faces of its elements (global order), and its owned rows, face terms
+    included, stay bit-identical to the global rows."""
+    case = M.random_case(nx=5, ny=3, nz=3, seed=13)
+    case.bfaces = M.face_set(case.mesh, weak=(1, 3, 6), convective={2: (20.0, 300.0), 5: (7.5, 350.0)})
+    og = _assemble(oracle, case, kind)
+    gsys = og.system(kind)
+    gcol = og.col.astype(np.int64) - 1
+    plain = case.bfaces
+    case_nf = M.random_case(nx=5, ny=3, nz=3, seed=13)
+    assert not np.array_equal(_assemble(oracle, case_nf, kind).system(kind)["rhs"], gsys["rhs"])  # faces act
+    for part in P.make_parts(case.mesh, 3):
+        lc = P.local_case(case, part)
+        assert lc.bfaces is not None and 0 < len(lc.bfaces.f2e) <= len(plain.f2e)
+        ol = _assemble(oracle, lc, kind)
+        lsys = ol.system(kind)
+        for b in BLOCKS[kind]:
+            rp, gcols, vals = P.owned_rows(ol.col, ol.row, lsys[b], part)
+            for i, A in enumerate(part.global_rows):
+                a, e = gcol[A], gcol[A + 1]
+                np.testing.assert_array_equal(vals[rp[i]:rp[i + 1]], gsys[b][a:e])
+        np.testing.assert_array_equal(lsys["rhs"][part.owned], gsys["rhs"][part.global_rows])
+
+
 def _free_port() -> int:
     s = socket.socket()
     s.bind(("127.0.0.1", 0))
