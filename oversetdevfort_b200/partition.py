@@ -69,6 +69,24 @@ def local_faces(bf: "M.BoundaryFaces", part: Part) -> "M.BoundaryFaces":
                            np.asarray(bf.flags)[keep], np.asarray(bf.hconv)[keep], np.asarray(bf.tinf)[keep])
 
 
+def local_bc_spec(spec: "M.BcSpec", part: Part) -> "M.BcSpec":
+    """setBCs input of a partition: every boundary keeps its nodes that are
+    local (1-based local ids, in the boundary's order), the FACE_ID and the
+    tables as they are, NodeID restricted to the local nodes."""
+    n = int(part.nodes.max()) + 1 if part.nodes.size else 0
+    loc = np.full(max(n, int(max((int(b.max()) for b in spec.bnodes if len(b)), default=0))) + 1, -1,
+                  dtype=np.int64)
+    loc[part.nodes] = np.arange(part.nodes.size)
+    bn = []
+    for b in spec.bnodes:
+        g = np.asarray(b, dtype=np.int64) - 1
+        lg = loc[g]
+        bn.append((lg[lg >= 0] + 1).astype(np.int32))
+    nid = None if spec.node_id is None else np.asarray(spec.node_id)[part.nodes].astype(np.int32)
+    return M.BcSpec(spec.face_id, bn, spec.bcug_type, spec.bcug_valu, spec.bcphig_type, spec.bcphig_valu,
+                    spec.bctg_type, spec.bctg_valu, nid)
+
+
 def local_case(case: "M.Case", part: Part) -> "M.Case":
     """The case restricted to a partition: local mesh, state, IBC and
     boundary faces."""

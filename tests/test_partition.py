@@ -67,6 +67,25 @@ def test_owned_rows_with_faces_match_global_assembly(oracle, kind):
         np.testing.assert_array_equal(lsys["rhs"][part.owned], gsys["rhs"][part.global_rows])
 
 
+def test_local_bc_spec_reproduces_global_setbcs(oracle):
+    """setBCs on each partition (its boundary nodes and NodeID) gives, on
+    every local node, the state and IBC of setBCs on the whole mesh."""
+    case = M.random_case(nx=5, ny=3, nz=3, seed=17)
+    m = case.mesh
+    nid = np.zeros(m.nnode, np.int32)
+    nid[::11] = 101
+    spec = M.box_bc_spec(m, u={1: (0.0, 0.0, 0.0), 6: (1.0, None, 0.0)}, phi={5: 1.0}, T={2: 400.0, 5: 300.0},
+                         node_id=nid, face_ids=(2, 1, 3, 4, 6, 5))
+    og = oracle.OracleCase(case)
+    og.set_bcs(spec, 3)
+    for part in P.make_parts(m, 3):
+        ol = oracle.OracleCase(P.local_case(case, part))
+        ol.set_bcs(P.local_bc_spec(spec, part), 3)
+        for k in ol.state_arrays:
+            np.testing.assert_array_equal(ol.state_arrays[k], og.state_arrays[k][part.nodes])
+        np.testing.assert_array_equal(ol.ibc, og.ibc[part.nodes])
+
+
 def _free_port() -> int:
     s = socket.socket()
     s.bind(("127.0.0.1", 0))
