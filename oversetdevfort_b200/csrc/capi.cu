@@ -185,16 +185,10 @@ int ovs_params_genalpha(double rhoinf, ovs_params* p) {
   return OVS_OK;
 }
 
-int ovs_create(ovs_ctx** out, const ovs_dims* dims) {
-  if (!out || !dims) return OVS_ERR_ARG;
-  *out = nullptr;
-  if (dims->nnode <= 0 || dims->nelem <= 0 || (dims->nshl != 4 && dims->nshl != 8)) return OVS_ERR_ARG;
-  if ((long)dims->nelem * dims->nshl >= (1L << 31) || dims->nelem >= (1 << 28)) return OVS_ERR_ARG;
-  int ndev = 0;
-  if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) { cudaGetLastError(); return OVS_ERR_NODEVICE; }
-  if (dims->device >= ndev) return OVS_ERR_ARG;
-  if (dims->device >= 0) OVS_CUDA_TRY(cudaSetDevice(dims->device));
-  ovs_ctx* c = new ovs_ctx();
+namespace {
+// Everything ovs_create allocates; on an error the caller destroys the
+// partly built context (ovs_destroy frees whatever is non-null).
+int create_resources(ovs_ctx* c, const ovs_dims* dims) {
   OVS_CUDA_TRY(cudaGetDevice(&c->device));
   OVS_CUDA_TRY(cudaDeviceGetAttribute(&c->num_sms, cudaDevAttrMultiProcessorCount, c->device));
   {
@@ -212,7 +206,7 @@ int ovs_create(ovs_ctx** out, const ovs_dims* dims) {
   int st;
   const size_t N = c->N;
   for (int f = 0; f < OVS_F_COUNT; ++f) {
-    if ((st = ovs_ensure((void**)&c->field[f], sizeof(double) * N * field_width(f)))) { ovs_destroy(c); return st; }
+    if ((st = ovs_ensure((void**)&c->field[f], sizeof(double) * N * field_width(f)))) return st;
     OVS_CUDA_TRY(cudaMemsetAsync(c->field[f], 0, sizeof(double) * N * field_width(f), c->stream));
   }
   if ((st = ovs_ensure((void**)&c->ien, sizeof(int) * (size_t)c->E * c->nshl)) ||
@@ -220,15 +214,33 @@ int ovs_create(ovs_ctx** out, const ovs_dims* dims) {
       (st = ovs_ensure((void**)&c->ibc, N)) ||
       (st = ovs_ensure((void**)&c->gm, sizeof(GmresDev))) ||
       (st = ovs_ensure((void**)&c->flags, sizeof(int) * 4)) ||
-      (st = ovs_ensure((void**)&c->cfl_bits, sizeof(unsigned long long)))) {
-    ovs_destroy(c);
+      (st = ovs_ensure((void**)&c->cfl_bits, sizeof(unsigned long long))))
     return st;
-  }
   OVS_CUDA_TRY(cudaMemsetAsync(c->ibc, 0, N, c->stream));
   OVS_CUDA_TRY(cudaMemsetAsync(c->gm, 0, sizeof(GmresDev), c->stream));
   OVS_CUDA_TRY(cudaMallocHost(&c->h_pinned, sizeof(int) * 16));
   OVS_CUDA_TRY(cudaMallocHost(&c->h_pinned_d, sizeof(double) * 16));
   OVS_CUDA_TRY(cudaStreamSynchronize(c->stream));
+  return OVS_OK;
+}
+}  // namespace
+
+int ovs_create(ovs_ctx** out, const ovs_dims* dims) {
+  if (!out || !dims) return OVS_ERR_ARG;
+  *out = nullptr;
+  if (dims->nnode <= 0 || dims->nelem <= 0 || (dims->nshl != 4 && dims->nshl != 8)) return OVS_ERR_ARG;
+  if ((long)dims->nelem * dims->nshl >= (1L << 31) || dims->nelem >= (1 << 28)) return OVS_ERR_ARG;
+  int ndev = 0;
+  if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) { cudaGetLastError(); return OVS_ERR_NODEVICE; }
+  if (dims->device >= ndev) return OVS_ERR_ARG;
+  if (dims->device >= 0) OVS_CUDA_TRY(cudaSetDevice(dims->device));
+  ovs_ctx* c = new ovs_ctx();
+  if (dims->device >= 0) c->device = dims->device;
+  const int st = create_resources(c, dims);
+  if (st) {
+    ovs_destroy(c);
+    return st;
+  }
   *out = c;
   return OVS_OK;
 }
