@@ -342,6 +342,13 @@ int ovs_solve(ovs_ctx* ctx, int system, int mode, double rtol, int kspace,
  *   NSVOF:    rphig += dphi; phig += gami*Delt*dphi;
  *   TEM:      rTg += dT; Tg += gami*Delt*dT. */
 int ovs_newton_update(ovs_ctx* ctx, int system);
+/* The solution the next ovs_newton_update of `system` applies, from `sol`
+ * (reference layout, N x nf FP64, in host memory or in this context's
+ * device memory): for a solution computed outside the context, such as the
+ * partitioned GMRES over several contexts, whose per-rank solutions the
+ * reference applies as the same update after SparseGMRES_* returns
+ * (src/solveFlow.f90:99-104, 139-140). */
+int ovs_set_solution(ovs_ctx* ctx, int system, const double* sol);
 
 /* calculate_residual (src/solveFlow.f90:169-187): sums of squares (no sqrt)
  * of RHSGu, RHSGp, RHSGls, RHSGtem of the given precision. */

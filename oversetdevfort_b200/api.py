@@ -328,6 +328,25 @@ class Context:
     def newton_update(self, system: int):
         F.check(self.lib.ovs_newton_update(self.h, system), "ovs_newton_update")
 
+    def set_solution(self, system: int, sol):
+        """ovs_set_solution: the solution the next `newton_update` of `system`
+        applies.  `sol` is a host array (N, nf) or a contiguous FP64 CUDA
+        tensor (nf, N) on this context's device (the same field-major
+        layout)."""
+        nf = {F.OVS_SYS_NS: 4, F.OVS_SYS_NSVOF: 5, F.OVS_SYS_TEM: 1}[system]
+        if hasattr(sol, "data_ptr"):
+            import torch
+            if sol.dtype != torch.float64 or not sol.is_cuda or not sol.is_contiguous() \
+                    or tuple(sol.shape) != (nf, self.N):
+                raise ValueError(f"expected a contiguous float64 CUDA tensor of shape ({nf}, {self.N})")
+            torch.cuda.current_stream(sol.device).synchronize()
+            ptr = C.c_void_p(sol.data_ptr())
+        else:
+            a = np.asfortranarray(sol, dtype=np.float64).reshape(self.N, nf, order="F")
+            self._sol_keep = a
+            ptr = a.ctypes.data_as(C.c_void_p)
+        F.check(self.lib.ovs_set_solution(self.h, system, ptr), "ovs_set_solution")
+
     def residual_norms(self, precision: int = F.OVS_FP64) -> np.ndarray:
         r = np.zeros(4)
         F.check(self.lib.ovs_residual_norms(self.h, precision, _dptr(r)), "ovs_residual_norms")

@@ -671,6 +671,18 @@ int ovs_newton_update(ovs_ctx* c, int sys) {
   return OVS_OK;
 }
 
+int ovs_set_solution(ovs_ctx* c, int sys, const double* sol) {
+  if (!sys_ok(c, sys, OVS_FP64) || !sol) return OVS_ERR_ARG;
+  int st;
+  if ((st = ovs_activate(c))) return st;
+  const size_t n = (size_t)c->N * ovs_sys_nf(sys);
+  if ((st = ovs_ensure((void**)&c->sol[sys], sizeof(double) * 5 * (size_t)c->N))) return st;
+  // host or device source: the unified address space tells them apart
+  OVS_CUDA_TRY(cudaMemcpyAsync(c->sol[sys], sol, sizeof(double) * n, cudaMemcpyDefault, c->stream));
+  OVS_CUDA_TRY(cudaStreamSynchronize(c->stream));
+  return OVS_OK;
+}
+
 int ovs_residual_norms(ovs_ctx* c, int prec, double r[4]) {
   if (!c || !r || (prec != OVS_FP64 && prec != OVS_FP32)) return OVS_ERR_ARG;
   int st;

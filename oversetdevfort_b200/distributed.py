@@ -303,3 +303,124 @@ def gmres_cycle(comm, ops: dict, rhs: dict, tol: float, kspace: int, kspace_min:
     comm.halo(sol)   # commu 'out': ghosts take their owners' values
     info.update(iterations=iks, ercheck=ercheck, converged=bool(ercheck <= epsnrm))
     return sol, info
+
+
+# assembleQuenching field flags (commonpars, src/modules.f90:218-222)
+FIELD_NS, FIELD_VOF, FIELD_TEM = 1, 2, 4
+_KIND_SYS = {"nsvof": F.OVS_SYS_NSVOF, "tem": F.OVS_SYS_TEM}
+
+
+class ContextPartition:
+    """One partition's local system on its own context (`api.Context` of
+    `partition.local_case`) for `quench_newton`: FP64 assembly, the sums of
+    squares of its owned residual rows, the right-hand sides as FP64 device
+    vectors (nf, N_local), the preconditioned operators, and the Newton
+    update with a solution from the partitioned GMRES (ovs_set_solution,
+    then ovs_newton_update)."""
+
+    def __init__(self, ctx, owned, device=None):
+        import torch
+        self.ctx = ctx
+        self.owned = np.asarray(owned, dtype=np.int64)
+        self.device = device if device is not None else f"cuda:{torch.cuda.current_device()}"
+
+    def apply_bcs(self):
+        self.ctx.apply_bcs(3)
+
+    def assemble(self, tensor_flag: int, field_flag: int):
+        if field_flag & (FIELD_NS | FIELD_VOF):
+            self.ctx.assemble(F.OVS_ASM_NSVOF, tensor_flag, F.OVS_FP64)
+        if field_flag & FIELD_TEM:
+            self.ctx.assemble(F.OVS_ASM_TEM, tensor_flag, F.OVS_FP64)
+
+    def residual_sq(self) -> np.ndarray:
+        o = self.owned
+        f = self.ctx.get_rhs(F.OVS_SYS_NSVOF)[o]
+        t = self.ctx.get_rhs(F.OVS_SYS_TEM)[o]
+        return np.array([np.sum(f[:, :3] ** 2), np.sum(f[:, 3] ** 2), np.sum(f[:, 4] ** 2), np.sum(t ** 2)])
+
+    def rhs(self, kind: str):
+        import torch
+        r = self.ctx.get_rhs(_KIND_SYS[kind])
+        return torch.as_tensor(np.ascontiguousarray(r.T), device=self.device)
+
+    def operator(self, kind: str):
+        return DeviceOperator(self.ctx, _KIND_SYS[kind])
+
+    def update(self, kind: str, sol):
+        self.ctx.set_solution(_KIND_SYS[kind], sol.contiguous())
+        self.ctx.newton_update(_KIND_SYS[kind])
+
+
+def quench_newton(comm, parts: dict, newton_max: int = 3, solve_tem: bool = True, kspace: int = 50,
+                  kspace_min: int = 1, tol_ns: float = 1e-6, tol_tem: float = 1e-6, utol=(1e-3,) * 4,
+                  atol=(1e-15,) * 4, orthog: str = "mgs", bcs: bool = False) -> dict:
+    """The Newton loop of one quench time step over owner-computes partitions:
+    solmultiphasethermofluid_stag (src/solveFlow.f90:4-164) as the reference
+    runs it on several ranks.  `parts[r]` is part r's local system
+    (`ContextPartition`, or any object with the same methods).
+
+    The steps, in the reference's order:
+
+    * with `bcs`, the BC producers on every part (setBCs_NSVOF and
+      setBCs_Tem, :34-36, :57-59);
+    * the residual of all fields, then the NS+VOF matrix and residual and one
+      GMRES cycle from zero over all parts (`gmres_cycle`);
+    * the update (:99-104); with `solve_tem`, the temperature the same way
+      (:109-140);
+    * the residual of all fields again and check_convergence (:148-157,
+      :192-215).
+
+    Every part assembles only its local elements, and its owned rows are then
+    complete.  Residuals are sums of squares over the owned rows, one global
+    sum per evaluation, as calculate_residual's MPI_ALLREDUCE (:169-187).
+    The loop body runs at least once.  The returned dict has iterations,
+    converged, field_converged, residual0, residual and the Krylov
+    iterations of both systems."""
+    P = comm.parts()
+
+    def residual():
+        return np.asarray(comm.allreduce_vec([np.asarray(parts[r].residual_sq(), dtype=np.float64) for r in P]))
+
+    def set_bcs():
+        if bcs:
+            for r in P:
+                parts[r].apply_bcs()
+
+    def solve(kind, tol):
+        rhs = {r: parts[r].rhs(kind) for r in P}
+        ops = {r: parts[r].operator(kind) for r in P}
+        sol, info = gmres_cycle(comm, ops, rhs, tol, kspace, kspace_min, tem=kind == "tem", orthog=orthog)
+        for r in P:
+            parts[r].update(kind, sol[r])
+        return info["iterations"]
+
+    def check(r, r0):
+        return [bool(r[k] < utol[k] * r0[k] or r[k] < atol[k]) for k in range(4)]
+
+    set_bcs()
+    for r in P:
+        parts[r].assemble(F.OVS_TENSOR_VEC, FIELD_NS | FIELD_VOF | FIELD_TEM)
+    r0 = residual()
+    res = r0.copy()
+    fc = check(res, r0)
+    out = {"iterations": 0, "converged": all(fc), "field_converged": fc, "residual0": r0,
+           "krylov_iterations_ns": 0, "krylov_iterations_tem": 0}
+    for it in range(1, newton_max + 1):
+        set_bcs()
+        for r in P:
+            parts[r].assemble(F.OVS_TENSOR_MAT | F.OVS_TENSOR_VEC, FIELD_NS | FIELD_VOF)
+        out["krylov_iterations_ns"] += solve("nsvof", tol_ns)
+        if solve_tem:
+            for r in P:
+                parts[r].assemble(F.OVS_TENSOR_MAT | F.OVS_TENSOR_VEC, FIELD_TEM)
+            out["krylov_iterations_tem"] += solve("tem", tol_tem)
+        for r in P:
+            parts[r].assemble(F.OVS_TENSOR_VEC, FIELD_NS | FIELD_VOF | FIELD_TEM)
+        res = residual()
+        fc = check(res, r0)
+        out.update(iterations=it, converged=all(fc), field_converged=fc)
+        if out["converged"]:
+            break
+    out["residual"] = res
+    return out

@@ -218,3 +218,129 @@ def test_two_gloo_ranks_gmres(oracle, orthog):
         p.join(timeout=120)
         assert p.exitcode == 0
     assert ok
+
+
+# ------------------------------------------------- partitioned Newton loop
+
+class OraclePartition:
+    """A partition's local system on the oracle, with the methods
+    distributed.quench_newton calls (stand-in for ContextPartition)."""
+
+    def __init__(self, oc, owned):
+        self.oc, self.owned = oc, np.asarray(owned)
+
+    def assemble(self, tensor_flag, field_flag):
+        self.oc.assemble_quenching(tensor_flag, field_flag)
+
+    def residual_sq(self):
+        s, o = self.oc.sys, self.owned
+        return np.array([np.sum(s["rhsu"][o] ** 2), np.sum(s["rhsp"][o] ** 2), np.sum(s["rhsls"][o] ** 2),
+                         np.sum(s["rhstem"][o] ** 2)])
+
+    def rhs(self, kind):
+        return torch.from_numpy(np.ascontiguousarray(self.oc.system(kind)["rhs"].T))
+
+    def operator(self, kind):
+        return OracleOperator(self.oc, kind)
+
+    def update(self, kind, sol):
+        self.oc.newton_update(F.OVS_SYS_NSVOF if kind == "nsvof" else F.OVS_SYS_TEM,
+                              np.asfortranarray(sol.numpy().T))
+
+
+NEWTON = dict(newton_max=3, solve_tem=True, kspace=150, kspace_min=1, tol_ns=1e-8, tol_tem=1e-8,
+              utol=(1e-6,) * 4, atol=(1e-30,) * 4)
+
+
+def _stirred_case():
+    case = M.quench_case(M.box_tet(5, 5, 6, 1.0, 1.0, 1.25), "dnewton")
+    rng = np.random.default_rng(3)   # the box at rest has no momentum residual
+    free = np.asarray(case.ibc)[:, 0] == 0
+    for f in ("ug", "ugold"):
+        case.state[f][free] = 0.05 * rng.standard_normal((int(free.sum()), 3))
+    return case
+
+
+def _one_domain_newton(oracle, case):
+    og = oracle.OracleCase(case)
+    n = NEWTON
+    out = og.quench_newton(n["newton_max"], n["solve_tem"], n["kspace"], n["kspace_min"], n["tol_ns"],
+                           n["tol_tem"], n["utol"], n["atol"])
+    return og, out
+
+
+def _compare_newton(out, ref, states, og, parts):
+    """Same iterations and Krylov counts; the residuals to 1e-4 relative
+    (the temperature residual ends 24 orders below its start, where the
+    summation order of the dots shows) plus 1e-16 of the initial one; the
+    state of every local node (ghosts too) to 1e-10 (measured: 2e-13)."""
+    assert out["iterations"] == ref["iterations"] >= 1
+    assert out["krylov_iterations_ns"] == ref["krylov_ns"] > 0
+    assert out["krylov_iterations_tem"] == ref["krylov_tem"] > 0
+    assert out["converged"] == ref["converged"]
+    np.testing.assert_allclose(out["residual0"], ref["residual0"], rtol=1e-12)
+    r0, r, rr = (np.asarray(ref["residual0"]), np.asarray(out["residual"]), np.asarray(ref["residual"]))
+    assert np.all(np.abs(r - rr) <= 1e-4 * np.abs(rr) + 1e-16 * r0), (r, rr)
+    for name in ("ug", "acg", "pg", "phig", "rphig", "tg", "rtg"):
+        g = og.state_arrays[name]
+        scale = max(np.abs(g).max(), 1e-300)
+        for st, p in zip(states, parts):
+            np.testing.assert_allclose(st[name], g[p.nodes], rtol=0, atol=1e-10 * scale, err_msg=name)
+
+
+@pytest.mark.parametrize("nparts", [2, 3, 4])
+def test_partitioned_newton_matches_one_domain(oracle, nparts):
+    """distributed.quench_newton over partitions in one process against the
+    oracle's one-domain solmultiphasethermofluid_stag loop."""
+    case = _stirred_case()
+    og, ref = _one_domain_newton(oracle, case)
+    parts = P.make_parts(case.mesh, nparts)
+    plan = D.halo_plan(parts)
+    ocs = {r: oracle.OracleCase(P.local_case(case, p)) for r, p in enumerate(parts)}
+    sys_parts = {r: OraclePartition(ocs[r], plan.owned[r]) for r in ocs}
+    with np.errstate(divide="ignore", invalid="ignore"):
+        out = D.quench_newton(D.LocalComm(plan), sys_parts, **NEWTON)
+    _compare_newton(out, ref, [ocs[r].state_arrays for r in ocs], og, parts)
+    assert out["residual"][0] < 1e-3 * out["residual0"][0]
+
+
+def _newton_rank_main(rank, world, port, q):
+    import datetime
+    import torch.distributed as dist
+    from oracle import pyoracle
+    os.environ["MASTER_ADDR"] = "127.0.0.1"
+    os.environ["MASTER_PORT"] = str(port)
+    dist.init_process_group("gloo", rank=rank, world_size=world, timeout=datetime.timedelta(seconds=120))
+    case = _stirred_case()
+    parts = P.make_parts(case.mesh, world)
+    plan = D.halo_plan(parts)
+    oc = pyoracle.OracleCase(P.local_case(case, parts[rank]))
+    with np.errstate(divide="ignore", invalid="ignore"):
+        out = D.quench_newton(D.TorchComm(plan, rank), {rank: OraclePartition(oc, plan.owned[rank])}, **NEWTON)
+    gathered = [None] * world if rank == 0 else None
+    dist.gather_object({k: oc.state_arrays[k] for k in ("ug", "acg", "pg", "phig", "rphig", "tg", "rtg")},
+                       gathered, dst=0)
+    if rank == 0:
+        try:
+            og, ref = _one_domain_newton(pyoracle, case)
+            _compare_newton(out, ref, gathered, og, parts)
+            q.put(True)
+        except AssertionError as e:
+            q.put(str(e))
+    dist.barrier()
+    dist.destroy_process_group()
+
+
+def test_two_gloo_ranks_newton(oracle):
+    import torch.multiprocessing as mp
+    ctx = mp.get_context("spawn")
+    q = ctx.Queue()
+    port = _free_port()
+    procs = [ctx.Process(target=_newton_rank_main, args=(r, 2, port, q)) for r in range(2)]
+    for p in procs:
+        p.start()
+    ok = q.get(timeout=300)
+    for p in procs:
+        p.join(timeout=120)
+        assert p.exitcode == 0
+    assert ok is True, ok
