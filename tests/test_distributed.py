@@ -344,3 +344,52 @@ def test_two_gloo_ranks_newton(oracle):
         p.join(timeout=120)
         assert p.exitcode == 0
     assert ok is True, ok
+
+
+class OracleBcPartition(OraclePartition):
+    """OraclePartition whose BC producers run on its part of the setBCs input."""
+
+    def __init__(self, oc, owned, spec):
+        super().__init__(oc, owned)
+        self.spec = spec
+
+    def apply_bcs(self):
+        self.oc.set_bcs(self.spec, 3)
+
+
+def test_partitioned_newton_with_bc_producers(oracle):
+    """quench_newton(bcs=True): setBCs_NSVOF/setBCs_Tem on every part's own
+    boundary nodes (partition.local_bc_spec) where the reference calls them;
+    three parts follow the one-part run: Newton and Krylov iterations equal,
+    the state of every local node to 1e-10, IBC equal."""
+    case = _stirred_case()
+    m = case.mesh
+    # walls and floor no-slip, the top free (its natural condition fixes the
+    # pressure level), the floor at 300 K, the top kept gas
+    spec = M.box_bc_spec(m, u={b: (0.0, 0.0, 0.0) for b in range(1, 6)}, phi={6: 1.0}, T={5: 300.0},
+                         face_ids=(2, 1, 3, 4, 6, 5))
+    runs = {}
+    for nparts in (1, 3):
+        parts = P.make_parts(m, nparts)
+        plan = D.halo_plan(parts)
+        ocs = {r: oracle.OracleCase(P.local_case(case, p)) for r, p in enumerate(parts)}
+        sp = {r: OracleBcPartition(ocs[r], plan.owned[r], P.local_bc_spec(spec, parts[r])) for r in ocs}
+        with np.errstate(divide="ignore", invalid="ignore"):
+            out = D.quench_newton(D.LocalComm(plan), sp, bcs=True, **NEWTON)
+        runs[nparts] = (out, ocs, parts)
+    (o1, oc1, p1), (o3, oc3, p3) = runs[1], runs[3]
+    assert o1["iterations"] >= 1 and o1["krylov_iterations_ns"] > 0 and o1["krylov_iterations_tem"] > 0
+    assert np.all(np.isfinite(o1["residual"])) and o1["residual"][0] < 1e-3 * o1["residual0"][0]
+    assert (o3["iterations"], o3["krylov_iterations_ns"], o3["krylov_iterations_tem"]) == \
+        (o1["iterations"], o1["krylov_iterations_ns"], o1["krylov_iterations_tem"])
+    g = oc1[0].state_arrays
+    for r, p in enumerate(p3):
+        np.testing.assert_array_equal(oc3[r].ibc, oc1[0].ibc[p.nodes])
+        for name in ("ug", "acg", "pg", "phig", "rphig", "tg", "rtg"):
+            scale = max(np.abs(g[name]).max(), 1e-300)
+            np.testing.assert_allclose(oc3[r].state_arrays[name], g[name][p.nodes], rtol=0, atol=1e-10 * scale,
+                                       err_msg=name)
+    # the producers ran: the floor holds 300 K and the top phi = 1
+    floor, top = np.asarray(m.faces[4]), np.asarray(m.faces[5])
+    np.testing.assert_array_equal(g["tg"][floor], 300.0)
+    np.testing.assert_array_equal(g["phig"][top], 1.0)
