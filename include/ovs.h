@@ -392,6 +392,15 @@ int ovs_quench_newton(ovs_ctx* ctx, const ovs_newton_opts* opts, ovs_newton_info
  * krylov_total: Krylov iterations over all steps (either may be NULL). */
 int ovs_quench_time_steps(ovs_ctx* ctx, int first_step, int nsteps, const ovs_newton_opts* opts,
                           int update_vof_tem_old, ovs_newton_info* last, int* krylov_total);
+/* The two halves of a driver step around the Newton loop, for a time loop
+ * driven from outside (over partitions, say).  ovs_predictor is
+ * src/driver.f90:83-85: ug = ugold, acg = (gami-1)/gami acgold
+ * (OVS_ERR_STATE before ovs_set_params).  ovs_commit_old copies the old
+ * values of :98-103: ugold, acgold, dgold, ugmold, acgmold, and with
+ * update_vof_tem_old = 1 also phigold, rphigold, Tgold, rTgold.  The
+ * pg = pgold / pgold = pg pair of the driver is the identity here. */
+int ovs_predictor(ovs_ctx* ctx);
+int ovs_commit_old(ovs_ctx* ctx, int update_vof_tem_old);
 
 /* ----------------------------------------------------------- measurement
  * Hooks for benchmarking; they have no counterpart in the reference. */

@@ -328,6 +328,16 @@ class Context:
     def newton_update(self, system: int):
         F.check(self.lib.ovs_newton_update(self.h, system), "ovs_newton_update")
 
+    def predictor(self):
+        """ovs_predictor: ug = ugold, acg = (gami - 1)/gami acgold
+        (src/driver.f90:83-85)."""
+        F.check(self.lib.ovs_predictor(self.h), "ovs_predictor")
+
+    def commit_old(self, update_vof_tem_old: bool = False):
+        """ovs_commit_old: the old values the driver updates after a step
+        (src/driver.f90:98-103)."""
+        F.check(self.lib.ovs_commit_old(self.h, int(update_vof_tem_old)), "ovs_commit_old")
+
     def set_solution(self, system: int, sol):
         """ovs_set_solution: the solution the next `newton_update` of `system`
         applies.  `sol` is a host array (N, nf) or a contiguous FP64 CUDA

@@ -917,38 +917,72 @@ int ovs_quench_newton(ovs_ctx* c, const ovs_newton_opts* o, ovs_newton_info* inf
 // :109), then the old values the driver updates (:95-100: ug, acg, dg, ugm,
 // acgm; pg is its own old value here).  The driver does not update phigold,
 // rphigold, Tgold, rTgold; update_vof_tem_old = 1 updates them too.
+// The driver's predictor (src/driver.f90:83-85; pg = pgold is the identity
+// here, as pgold = pg closes every step): ug = ugold,
+// acg = (gami - 1)/gami acgold, on the context stream.
+static int launch_predictor(ovs_ctx* c) {
+  const size_t N = c->N;
+  const double gami = c->params.gami;
+  predictor_kernel<<<ovs_grid(3 * N, 256, 1 << 30), 256, 0, c->stream>>>(
+      3 * N, (gami - 1.0) / gami, c->field[OVS_F_UGOLD], c->field[OVS_F_ACGOLD], c->field[OVS_F_UG], c->field[OVS_F_ACG]);
+  ++c->launches;
+  OVS_CUDA_TRY(cudaGetLastError());
+  return OVS_OK;
+}
+
+// The old values the driver updates after a step (src/driver.f90:98-103),
+// queued on the context stream; update_vof_tem_old also copies phig, rphig,
+// Tg and rTg, which the driver leaves alone.
+static int copy_old_values(ovs_ctx* c, int update_vof_tem_old) {
+  const size_t N = c->N;
+  const int pairs3[][2] = {{OVS_F_UG, OVS_F_UGOLD}, {OVS_F_ACG, OVS_F_ACGOLD}, {OVS_F_DG, OVS_F_DGOLD},
+                           {OVS_F_UGM, OVS_F_UGMOLD}, {OVS_F_ACGM, OVS_F_ACGMOLD}};
+  for (auto& pr : pairs3)
+    OVS_CUDA_TRY(cudaMemcpyAsync(c->field[pr[1]], c->field[pr[0]], sizeof(double) * 3 * N,
+                                 cudaMemcpyDeviceToDevice, c->stream));
+  if (update_vof_tem_old) {
+    const int pairs1[][2] = {{OVS_F_PHIG, OVS_F_PHIGOLD}, {OVS_F_RPHIG, OVS_F_RPHIGOLD}, {OVS_F_TG, OVS_F_TGOLD},
+                             {OVS_F_RTG, OVS_F_RTGOLD}};
+    for (auto& pr : pairs1)
+      OVS_CUDA_TRY(cudaMemcpyAsync(c->field[pr[1]], c->field[pr[0]], sizeof(double) * N,
+                                   cudaMemcpyDeviceToDevice, c->stream));
+  }
+  return OVS_OK;
+}
+
+int ovs_predictor(ovs_ctx* c) {
+  if (!c) return OVS_ERR_ARG;
+  if (!c->have_params) return OVS_ERR_STATE;
+  int st;
+  if ((st = ovs_activate(c)) || (st = launch_predictor(c))) return st;
+  OVS_CUDA_TRY(cudaStreamSynchronize(c->stream));
+  return OVS_OK;
+}
+
+int ovs_commit_old(ovs_ctx* c, int update_vof_tem_old) {
+  if (!c) return OVS_ERR_ARG;
+  int st;
+  if ((st = ovs_activate(c)) || (st = copy_old_values(c, update_vof_tem_old))) return st;
+  OVS_CUDA_TRY(cudaStreamSynchronize(c->stream));
+  return OVS_OK;
+}
+
 int ovs_quench_time_steps(ovs_ctx* c, int first_step, int nsteps, const ovs_newton_opts* o,
                           int update_vof_tem_old, ovs_newton_info* last, int* krylov_total) {
   if (!c || !o || nsteps < 0) return OVS_ERR_ARG;
   int st;
   if ((st = ovs_activate(c))) return st;
-  const size_t N = c->N;
-  const double gami = c->params.gami;
   int kt = 0;
   for (int s = 0; s < nsteps; ++s) {
     const int istep = first_step + s;
-    predictor_kernel<<<ovs_grid(3 * N, 256, 1 << 30), 256, 0, c->stream>>>(
-        3 * N, (gami - 1.0) / gami, c->field[OVS_F_UGOLD], c->field[OVS_F_ACGOLD], c->field[OVS_F_UG], c->field[OVS_F_ACG]);
-    ++c->launches;
-    OVS_CUDA_TRY(cudaGetLastError());
+    if ((st = launch_predictor(c))) return st;
     ovs_newton_opts os = *o;
     if (istep <= 1) os.newton_max = 1;
     os.solve_tem = o->solve_tem && istep > 0;
     ovs_newton_info ni;
     if ((st = ovs_quench_newton(c, &os, &ni))) return st;
     kt += ni.krylov_iterations_ns + ni.krylov_iterations_tem;
-    const int pairs3[][2] = {{OVS_F_UG, OVS_F_UGOLD}, {OVS_F_ACG, OVS_F_ACGOLD}, {OVS_F_DG, OVS_F_DGOLD},
-                             {OVS_F_UGM, OVS_F_UGMOLD}, {OVS_F_ACGM, OVS_F_ACGMOLD}};
-    for (auto& pr : pairs3)
-      OVS_CUDA_TRY(cudaMemcpyAsync(c->field[pr[1]], c->field[pr[0]], sizeof(double) * 3 * N,
-                                   cudaMemcpyDeviceToDevice, c->stream));
-    if (update_vof_tem_old) {
-      const int pairs1[][2] = {{OVS_F_PHIG, OVS_F_PHIGOLD}, {OVS_F_RPHIG, OVS_F_RPHIGOLD}, {OVS_F_TG, OVS_F_TGOLD},
-                               {OVS_F_RTG, OVS_F_RTGOLD}};
-      for (auto& pr : pairs1)
-        OVS_CUDA_TRY(cudaMemcpyAsync(c->field[pr[1]], c->field[pr[0]], sizeof(double) * N,
-                                     cudaMemcpyDeviceToDevice, c->stream));
-    }
+    if ((st = copy_old_values(c, update_vof_tem_old))) return st;
     OVS_CUDA_TRY(cudaStreamSynchronize(c->stream));
     if (last) *last = ni;
   }

@@ -314,9 +314,10 @@ class ContextPartition:
     """One partition's local system on its own context (`api.Context` of
     `partition.local_case`) for `quench_newton`: FP64 assembly, the sums of
     squares of its owned residual rows, the right-hand sides as FP64 device
-    vectors (nf, N_local), the preconditioned operators, and the Newton
-    update with a solution from the partitioned GMRES (ovs_set_solution,
-    then ovs_newton_update)."""
+    vectors (nf, N_local), the preconditioned operators, the Newton update
+    with a solution from the partitioned GMRES (ovs_set_solution, then
+    ovs_newton_update), and, for `quench_time_steps`, the driver's predictor
+    and old-value copies (ovs_predictor, ovs_commit_old)."""
 
     def __init__(self, ctx, owned, device=None):
         import torch
@@ -350,6 +351,12 @@ class ContextPartition:
     def update(self, kind: str, sol):
         self.ctx.set_solution(_KIND_SYS[kind], sol.contiguous())
         self.ctx.newton_update(_KIND_SYS[kind])
+
+    def predictor(self):
+        self.ctx.predictor()
+
+    def commit_old(self, update_vof_tem_old: bool):
+        self.ctx.commit_old(update_vof_tem_old)
 
 
 def quench_newton(comm, parts: dict, newton_max: int = 3, solve_tem: bool = True, kspace: int = 50,
@@ -424,3 +431,26 @@ def quench_newton(comm, parts: dict, newton_max: int = 3, solve_tem: bool = True
             break
     out["residual"] = res
     return out
+
+
+def quench_time_steps(comm, parts: dict, first_step: int, nsteps: int, update_vof_tem_old: bool = False,
+                      newton_max: int = 3, solve_tem: bool = True, **newton):
+    """`nsteps` steps of the reference driver's time loop (src/driver.f90:
+    70-103) over the partitions.  Every step runs the predictor on every
+    part (:83-85), then `quench_newton` (a single Newton iteration while
+    istep <= 1, and no temperature solve at istep 0, src/solveFlow.f90:50-54,
+    109), then the old-value copies (:98-103).  The parts also need
+    predictor() and commit_old(flag).  Returns (the last step's Newton
+    record, the Krylov iterations over all steps)."""
+    P = comm.parts()
+    last, kt = None, 0
+    for k in range(nsteps):
+        istep = first_step + k
+        for r in P:
+            parts[r].predictor()
+        last = quench_newton(comm, parts, newton_max=1 if istep <= 1 else newton_max,
+                             solve_tem=solve_tem and istep > 0, **newton)
+        kt += last["krylov_iterations_ns"] + last["krylov_iterations_tem"]
+        for r in P:
+            parts[r].commit_old(update_vof_tem_old)
+    return last, kt
