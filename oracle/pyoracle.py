@@ -8,13 +8,18 @@ vectors and cannot be compiled here, so analytic known-answer tests pin it.
 from __future__ import annotations
 
 import ctypes as C
+import os
 import subprocess
 from pathlib import Path
 
 import numpy as np
 
 HERE = Path(__file__).resolve().parent
-LIB = HERE / "_build" / "libovs_oracle.so"
+# OVS_ORACLE_LIB selects another build of the same source, e.g. the
+# sanitizer build of `make -C oracle asan` (run with the sanitizer runtimes
+# in LD_PRELOAD); that build is made by its own make target, not here.
+_OVERRIDE = os.environ.get("OVS_ORACLE_LIB")
+LIB = Path(_OVERRIDE) if _OVERRIDE else HERE / "_build" / "libovs_oracle.so"
 
 _dp = C.POINTER(C.c_double)
 OVS_SYS_NSVOF, OVS_SYS_TEM = 2, 3   # system ids of include/ovs.h
@@ -22,7 +27,8 @@ _ip = C.POINTER(C.c_int)
 
 
 def build() -> Path:
-    subprocess.run(["make", "-s", "-C", str(HERE)], check=True)
+    if not _OVERRIDE:
+        subprocess.run(["make", "-s", "-C", str(HERE)], check=True)
     return LIB
 
 
