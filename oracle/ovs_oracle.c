@@ -203,6 +203,30 @@ static double eval_shape_fem(int nshl, const double* gp, double xl[][3],
   return eval_shape_fem_dx(nshl, gp, xl, dl, shl, shg, Gij, dxidx);
 }
 
+/* Test hook, no reference counterpart: point igp of the element's rule
+ * (gen_gp_gw with NGAUSS = NSHL, src/input.f90:158) and eval_shape_fem
+ * there, for nodal coordinates xl and displacements dl (node a at
+ * [3a..3a+2]; dl may be NULL): N_a, grad N_a (shg[3a+i]), G_ij
+ * (gij[3i+j]) and the weight; returns DetJ. */
+double orc_eval_shape(int nshl, int igp, const double* xl, const double* dl, double* shl,
+                      double* shg, double* gij, double* gw_out) {
+  double gp[8][3], gw[8], x[NSHL_MAX][3], d[NSHL_MAX][3], sg[NSHL_MAX][3], G[3][3];
+  if ((nshl != 4 && nshl != 8) || igp < 0 || igp >= nshl) return 0.0;
+  gen_gp_gw(nshl, gp, gw);
+  for (int a = 0; a < nshl; ++a)
+    for (int k = 0; k < 3; ++k) {
+      x[a][k] = xl[3 * a + k];
+      d[a][k] = dl ? dl[3 * a + k] : 0.0;
+    }
+  const double detj = eval_shape_fem(nshl, gp[igp], x, d, shl, sg, G);
+  for (int a = 0; a < nshl; ++a)
+    for (int k = 0; k < 3; ++k) shg[3 * a + k] = sg[a][k];
+  for (int i = 0; i < 3; ++i)
+    for (int j = 0; j < 3; ++j) gij[3 * i + j] = G[i][j];
+  *gw_out = gw[igp];
+  return detj;
+}
+
 /* prop_interp src/e3int.f90:4-13 */
 static double prop_interp(double a, double b, double phi) {
   double pc = fmax(0.0, fmin(1.0, phi));

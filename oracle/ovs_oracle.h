@@ -120,6 +120,9 @@ int orc_gmres_tem(int nnode, const int* col, const int* row,
 void orc_newton_update(int nnode, int system, const ovs_params* p,
                        orc_state* s, const double* sol);
 void orc_calculate_residual(int nnode, const orc_system* sys, double r[4]);
+/* test hook: eval_shape_fem at point igp of the element's rule */
+double orc_eval_shape(int nshl, int igp, const double* xl, const double* dl, double* shl,
+                      double* shg, double* gij, double* gw_out);
 
 #ifdef __cplusplus
 }

@@ -68,6 +68,8 @@ def load():
     from oversetdevfort_b200._ffi import OvsParams
     pp = C.POINTER(OvsParams)
     lib.orc_gen_spar_struc.argtypes = [C.c_int, C.c_int, C.c_int, _ip, _ip, _ip, _ip]
+    lib.orc_eval_shape.argtypes = [C.c_int, C.c_int, _dp, _dp, _dp, _dp, _dp, _dp]
+    lib.orc_eval_shape.restype = C.c_double
     lib.orc_sparse_mat_loc.argtypes = [_ip, C.c_int, C.c_int]
     for fn in ("orc_assemble_navsto",):
         getattr(lib, fn).argtypes = [C.POINTER(OrcMesh), pp, C.POINTER(OrcState), C.POINTER(OrcSystem), C.c_int]
@@ -118,6 +120,18 @@ def gen_spar_struc(ien: np.ndarray, nnode: int):
     st = lib.orc_gen_spar_struc(nnode, E, nshl, _i(ien), _i(col), _i(row), C.byref(icnt))
     assert st == 0, st
     return col, row[: icnt.value]
+
+
+def eval_shape(nshl: int, igp: int, xl: np.ndarray, dl: np.ndarray | None = None):
+    """eval_shape_fem at point igp of the element's rule: (DetJ, N (nshl),
+    grad N (nshl, 3), G (3, 3), weight).  xl, dl: (nshl, 3)."""
+    lib = load()
+    x = np.ascontiguousarray(xl, dtype=np.float64)
+    d = None if dl is None else np.ascontiguousarray(dl, dtype=np.float64)
+    shl, shg, gij, gw = np.zeros(nshl), np.zeros((nshl, 3)), np.zeros((3, 3)), C.c_double(0)
+    detj = lib.orc_eval_shape(nshl, igp, _d(x), None if d is None else _d(d), _d(shl), _d(shg), _d(gij),
+                              C.byref(gw))
+    return detj, shl, shg, gij, gw.value
 
 
 class OracleCase:

@@ -9,7 +9,11 @@ temperature field leaves no interior conduction residual; a linear pressure
 field gives -grad p times the lumped nodal volume; a linear divergence-free
 velocity moving with the mesh leaves no interior momentum or continuity
 residual; uniform advection of linear phi and T with the rates that cancel
-it leaves no VOF residual and no interior temperature residual).
+it leaves no VOF residual and no interior temperature residual), the shape
+functions and metric of tets and hexes in closed form, and every block of
+the NS, NS+VOF and temperature element matrices of one tet at rest in
+closed form (mass, viscous, grad-div, pressure and PSPG blocks with the
+stabilisation parameters of e3STAB).
 """
 import numpy as np
 import pytest
@@ -566,3 +570,228 @@ def test_oracle_time_loop(oracle):
     for cur, old in (("ug", "ugold"), ("acg", "acgold")):
         np.testing.assert_array_equal(oc.state_arrays[cur], oc.state_arrays[old])
     assert np.abs(oc.state_arrays["tg"] - t0).max() > 0.0
+
+
+# ------------------------------------------------------------ geometry KATs
+
+def _random_tet(rng):
+    while True:
+        x = rng.standard_normal((4, 3))
+        J = np.stack([x[0] - x[3], x[1] - x[3], x[2] - x[3]], axis=1)
+        d = np.linalg.det(J)
+        if abs(d) > 0.2:
+            if d < 0:
+                x[[0, 1]] = x[[1, 0]]
+                J = np.stack([x[0] - x[3], x[1] - x[3], x[2] - x[3]], axis=1)
+            return x, J
+
+
+def test_tet_shape_functions_closed_form(oracle):
+    """eval_shape_fem on linear tets (src/eval_shape_FEM.f90:4-61) against
+    the closed form: x = x4 + J xi, so grad N_k = row k of J^-1 (k = 1..3),
+    grad N_4 = -(sum of the others), DetJ = det J, G = sum_k grad xi_k
+    grad xi_k^T the same at every point, the weights summing to |T| = det J
+    / 6; N is the barycentric coordinate of the point; the current
+    configuration x + d is used (:31-36)."""
+    rng = np.random.default_rng(7)
+    for _ in range(20):
+        x, J = _random_tet(rng)
+        Ji = np.linalg.inv(J)
+        grad = np.vstack([Ji, -Ji.sum(axis=0)])
+        Gw = Ji.T @ Ji
+        vol = 0.0
+        for g in range(4):
+            detj, N, shg, G, w = oracle.eval_shape(4, g, x)
+            assert abs(detj - np.linalg.det(J)) < 1e-12 * abs(detj)
+            assert abs(N.sum() - 1.0) < 1e-15
+            np.testing.assert_allclose(shg, grad, rtol=0, atol=1e-12 * np.abs(grad).max())
+            np.testing.assert_allclose(G, Gw, rtol=0, atol=1e-12 * np.abs(Gw).max())
+            xp = N @ x   # the Gauss point maps to the barycentric combination
+            np.testing.assert_allclose(np.linalg.solve(J, xp - x[3]), N[:3], atol=1e-12)
+            vol += w * detj
+        assert abs(vol - np.linalg.det(J) / 6.0) < 1e-14 * vol
+        d = 0.1 * rng.standard_normal((4, 3))
+        a = oracle.eval_shape(4, 2, x, d)
+        b = oracle.eval_shape(4, 2, x + d)
+        assert a[0] == b[0] and all(np.array_equal(u, v) for u, v in zip(a[1:4], b[1:4]))
+
+
+_HEX_XI = 2.0 * np.array([(0, 1, 0), (1, 1, 0), (1, 1, 1), (0, 1, 1), (0, 0, 0), (1, 0, 0), (1, 0, 1), (0, 0, 1)]) - 1.0
+
+
+def test_hex_shape_functions(oracle):
+    """linhexshl + eval_shape_fem on trilinear hexahedra (the hex extension):
+    partition of unity, gradients summing to zero, a linear field c.x + e
+    reproduced with its exact gradient c on distorted hexes; on a
+    parallelepiped x = x0 + A xi, DetJ = det A at every point, G = A^-T A^-1
+    and the 8-point weights sum to the volume 8 det A."""
+    rng = np.random.default_rng(11)
+    for distort in (0.0, 0.08):
+        for _ in range(10):
+            A = np.eye(3) + 0.3 * rng.standard_normal((3, 3))
+            if np.linalg.det(A) < 0.3:
+                continue
+            x = rng.standard_normal(3) + _HEX_XI @ A.T + distort * rng.standard_normal((8, 3))
+            c, e = rng.standard_normal(3), rng.standard_normal()
+            f = x @ c + e
+            vol = 0.0
+            for g in range(8):
+                detj, N, shg, G, w = oracle.eval_shape(8, g, x)
+                assert abs(N.sum() - 1.0) < 1e-14
+                assert np.abs(shg.sum(axis=0)).max() < 1e-12 * np.abs(shg).max()
+                np.testing.assert_allclose(f @ shg, c, rtol=0, atol=1e-11 * (1 + np.abs(c).max()))
+                vol += w * detj
+                if distort == 0.0:
+                    Ai = np.linalg.inv(A)
+                    assert abs(detj - np.linalg.det(A)) < 1e-12 * abs(detj)
+                    np.testing.assert_allclose(G, Ai.T @ Ai, rtol=0, atol=1e-12 * np.abs(Ai).max() ** 2)
+            if distort == 0.0:
+                assert abs(vol - 8.0 * np.linalg.det(A)) < 1e-12 * vol
+
+
+def test_ns_element_matrix_at_rest_closed_form(oracle):
+    """IntElmAss_NS_overset on one tet with the fluid and mesh at rest
+    (u = ugm = 0), mu > 0: every block in closed form from e3STAB_3D
+    (src/e3STAB.f90:4-44: tau_M = tau_P = 1/(rho sqrt(4/dt^2 + 12 nu^2
+    G:G)), tau_C = rho sqrt(12 nu^2 G:G)/tr G) and e3LHS_3D_fluid_Old
+    (src/e3LHS.f90:4-161) with f1 = alpha_m, f2 = alpha_f gamma dt:
+      K_ij = delta_ij (f1 rho M_ab + f2 mu |T| gN_a.gN_b)
+             + f2 |T| (mu d_jN_a d_iN_b + tau_C d_iN_a d_jN_b)
+      G_d = -f2 |T|/4 d_dN_a;  D_d = |T|/4 (f2 d_dN_b + f1 tau_P rho d_dN_a)
+      M = f2 tau_P |T| gN_a.gN_b
+    with M_ab = |T| (1 + delta_ab)/20 (the 4-point rule is exact)."""
+    rho, mu = 1.7, 0.37
+    case, vol = _single_tet_case(rho)
+    case.params.update(mua=mu, muw=mu, delt=0.05)
+    case.kernel = F.OVS_ASM_NS
+    oc = oracle.OracleCase(case)
+    oc.assemble_navsto(F.OVS_TENSOR_MAT | F.OVS_TENSOR_VEC)
+    p = case.params
+    f1, f2 = p["almi"], p["alfi"] * p["gami"] * p["delt"]
+    x = np.asarray(case.mesh.xg)
+    J = np.stack([x[0] - x[3], x[1] - x[3], x[2] - x[3]], axis=1)
+    Ji = np.linalg.inv(J)
+    gN = np.vstack([Ji, -Ji.sum(axis=0)])
+    G = Ji.T @ Ji
+    nu = mu / rho
+    GG = (G * G).sum()
+    tauM = 1.0 / (rho * np.sqrt(4.0 / p["delt"] ** 2 + 12.0 * nu * nu * GG))
+    tauC = rho * np.sqrt(12.0 * nu * nu * GG) / np.trace(G)
+    col, row = oc.col, oc.row
+    s = oc.sys
+    checked = 0
+    for a in range(4):
+        for k in range(col[a] - 1, col[a + 1] - 1):
+            b = row[k] - 1
+            Mab = vol * (1 + (a == b)) / 20.0
+            lap = gN[a] @ gN[b]
+            for i in range(3):
+                for j in range(3):
+                    want = (i == j) * (f1 * rho * Mab + f2 * mu * vol * lap) \
+                        + f2 * vol * (mu * gN[a, j] * gN[b, i] + tauC * gN[a, i] * gN[b, j])
+                    got = s["K11"][k, 3 * i + j]
+                    assert abs(got - want) < 1e-12 * (abs(want) + f2 * mu * vol * np.abs(gN).max() ** 2), (a, b, i, j)
+            for d in range(3):
+                wg = -f2 * vol / 4.0 * gN[a, d]
+                wd = vol / 4.0 * (f2 * gN[b, d] + f1 * tauM * rho * gN[a, d])
+                assert abs(s["G"][k, d] - wg) < 1e-12 * abs(f2 * vol * np.abs(gN).max())
+                assert abs(s["D1"][k, d] - wd) < 1e-12 * abs(f2 * vol * np.abs(gN).max())
+            wm = f2 * tauM * vol * lap
+            assert abs(s["M"][k] - wm) < 1e-12 * f2 * tauM * vol * np.abs(gN).max() ** 2
+            checked += 1
+    assert checked == 16
+
+
+def test_nsvof_element_matrix_at_rest_closed_form(oracle):
+    """IntElmAss_NSVOF_Quenching_STAB on one fluid tet at rest (u = ugm = 0),
+    uniform phi = 0.25 between the phases, T below Ts and no phase change:
+    rho, mu = prop_interp(w, a, phi) (src/solveQuenching.f90:352-358),
+    lambda = -2/3 mu (:359), the taus of e3STAB_3D_NSVOF (src/e3STAB.f90:
+    292-333) and the blocks of :434-494 in closed form:
+      K_ij = delta_ij (f1 rho M_ab + f2 mu |T| gN_a.gN_b)
+             + f2 |T| (mu d_jN_a d_iN_b + (tau_C + lambda) d_iN_a d_jN_b)
+      G_d = -f2 |T|/4 d_dN_a;  D_d = |T|/4 (f2 d_dN_b + f1 tau_M rho d_dN_a)
+      M = f2 tau_M |T| gN_a.gN_b;  LS = f1 M_ab;  ULS = PLS = 0; LSU = 0
+    (grad phi = 0)."""
+    case, vol = _single_tet_case(1.0)
+    rhow, rhoa, muw, mua, phi = 3.0, 1.0, 0.5, 0.1, 0.25
+    case.params.update(rhow=rhow, rhoa=rhoa, muw=muw, mua=mua, delt=0.02)
+    for f in ("phig", "phigold"):
+        case.state[f][:] = phi
+    for f in ("tg", "tgold"):
+        case.state[f][:] = 300.0
+    oc = oracle.OracleCase(case)
+    oc.assemble_quenching(F.OVS_TENSOR_MAT | F.OVS_TENSOR_VEC, 3)
+    p = case.params
+    assert p["c_evap"] == 0.0 and p["c_cond"] == 0.0 and 300.0 < p["ts"]
+    f1, f2 = p["almi"], p["alfi"] * p["gami"] * p["delt"]
+    rho, mu = rhow * (1 - phi) + rhoa * phi, muw * (1 - phi) + mua * phi
+    lam = -2.0 / 3.0 * mu
+    x = np.asarray(case.mesh.xg)
+    J = np.stack([x[0] - x[3], x[1] - x[3], x[2] - x[3]], axis=1)
+    Ji = np.linalg.inv(J)
+    gN = np.vstack([Ji, -Ji.sum(axis=0)])
+    G = Ji.T @ Ji
+    nu, GG = mu / rho, (G * G).sum()
+    tauM = 1.0 / (rho * np.sqrt(4.0 / p["delt"] ** 2 + 12.0 * nu * nu * GG))
+    tauC = rho * np.sqrt(12.0 * nu * nu * GG) / np.trace(G)
+    s, col, row = oc.sys, oc.col, oc.row
+    gmax = np.abs(gN).max()
+    kscale = f2 * mu * vol * gmax ** 2 + f1 * rho * vol
+    for a in range(4):
+        for k in range(col[a] - 1, col[a + 1] - 1):
+            b = row[k] - 1
+            Mab = vol * (1 + (a == b)) / 20.0
+            lap = gN[a] @ gN[b]
+            for i in range(3):
+                for j in range(3):
+                    want = (i == j) * (f1 * rho * Mab + f2 * mu * vol * lap) \
+                        + f2 * vol * (mu * gN[a, j] * gN[b, i] + (tauC + lam) * gN[a, i] * gN[b, j])
+                    assert abs(s["K11"][k, 3 * i + j] - want) < 1e-12 * kscale, (a, b, i, j)
+            for d in range(3):
+                assert abs(s["G"][k, d] + f2 * vol / 4.0 * gN[a, d]) < 1e-12 * f2 * vol * gmax
+                wd = vol / 4.0 * (f2 * gN[b, d] + f1 * tauM * rho * gN[a, d])
+                assert abs(s["D1"][k, d] - wd) < 1e-12 * f2 * vol * gmax
+                assert s["ULS"][k, d] == 0.0
+                assert abs(s["LSU"][k, d]) < 1e-14 * f2 * vol * gmax
+            assert abs(s["M"][k] - f2 * tauM * vol * lap) < 1e-12 * f2 * tauM * vol * gmax ** 2
+            assert abs(s["LS"][k] - f1 * Mab) < 1e-14 * f1 * vol
+            assert s["PLS"][k] == 0.0
+
+
+@pytest.mark.parametrize("solid", [False, True])
+def test_temperature_element_matrix_at_rest_closed_form(oracle, solid):
+    """IntElmAss_Tem_Quenching_STAB on one tet at rest, no phase change
+    (src/solveQuenching.f90:758-839): the SUPG and source terms vanish and
+    TEM = f1 (rho c_p) M_ab + f2 kappa |T| gN_a.gN_b, with rho c_p and kappa
+    interpolated by phi in a fluid element (prop_interp of rho_w c_pw and
+    rho_a c_pa) and the solid's own in a solid one (ELM_ID != 102)."""
+    case, vol = _single_tet_case(1.0)
+    phi = 0.4
+    case.params.update(delt=0.03)
+    if solid:
+        case.mesh.elm_id[:] = 103
+    for f in ("phig", "phigold"):
+        case.state[f][:] = phi
+    for f in ("tg", "tgold"):
+        case.state[f][:] = 320.0
+    oc = oracle.OracleCase(case)
+    oc.assemble_quenching(F.OVS_TENSOR_MAT | F.OVS_TENSOR_VEC, 4)
+    p = case.params
+    f1, f2 = p["almi"], p["alfi"] * p["gami"] * p["delt"]
+    if solid:
+        rhocp, kap = p["rhos"] * p["cps"], p["kappas"]
+    else:
+        rhocp = p["rhow"] * p["cpw"] * (1 - phi) + p["rhoa"] * p["cpa"] * phi
+        kap = p["kappaw"] * (1 - phi) + p["kappaa"] * phi
+    x = np.asarray(case.mesh.xg)
+    J = np.stack([x[0] - x[3], x[1] - x[3], x[2] - x[3]], axis=1)
+    Ji = np.linalg.inv(J)
+    gN = np.vstack([Ji, -Ji.sum(axis=0)])
+    col, row, T = oc.col, oc.row, oc.sys["TEM"]
+    scale = f1 * rhocp * vol + f2 * kap * vol * np.abs(gN).max() ** 2
+    for a in range(4):
+        for k in range(col[a] - 1, col[a + 1] - 1):
+            b = row[k] - 1
+            want = f1 * rhocp * vol * (1 + (a == b)) / 20.0 + f2 * kap * vol * (gN[a] @ gN[b])
+            assert abs(T[k] - want) < 1e-12 * scale, (a, b, T[k], want)
