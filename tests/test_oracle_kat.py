@@ -795,3 +795,69 @@ def test_temperature_element_matrix_at_rest_closed_form(oracle, solid):
             b = row[k] - 1
             want = f1 * rhocp * vol * (1 + (a == b)) / 20.0 + f2 * kap * vol * (gN[a] @ gN[b])
             assert abs(T[k] - want) < 1e-12 * scale, (a, b, T[k], want)
+
+
+def test_hex_nsvof_element_matrix_at_rest(oracle):
+    """The NS+VOF element matrices of one trilinear hexahedron (the hex
+    extension: linhexshl with the 2x2x2 rule) on a parallelepiped at rest,
+    against the same closed form as the tet, with the integrals taken here
+    by a 3x3x3 Gauss-Legendre rule (both rules are exact for these
+    integrands: degree <= 2 in each reference coordinate)."""
+    rng = np.random.default_rng(5)
+    A = np.diag([0.4, 0.3, 0.5]) + 0.05 * rng.standard_normal((3, 3))
+    x0 = np.array([0.2, -0.1, 0.3])
+    xg = np.asfortranarray(x0 + _HEX_XI @ A.T)
+    ien = np.asfortranarray(np.arange(1, 9, dtype=np.int32)[None, :])
+    m = M.Mesh(xg, ien, np.array([102], dtype=np.int32), [np.arange(8)] * 6, (1, 1, 1), (1, 1, 1))
+    rhow, rhoa, muw, mua, phi = 2.0, 0.5, 0.3, 0.05, 0.6
+    p = M.base_params(rhow=rhow, rhoa=rhoa, muw=muw, mua=mua, delt=0.04)
+    st = M.empty_state(8)
+    for f in ("phig", "phigold"):
+        st[f][:] = phi
+    for f in ("tg", "tgold"):
+        st[f][:] = 300.0
+    case = M.Case("single_hex", m, p, st, np.zeros((8, 8), dtype=np.int32, order="F"), F.OVS_ASM_NSVOF)
+    oc = oracle.OracleCase(case)
+    oc.assemble_quenching(F.OVS_TENSOR_MAT | F.OVS_TENSOR_VEC, 3)
+    f1, f2 = p["almi"], p["alfi"] * p["gami"] * p["delt"]
+    rho, mu = rhow * (1 - phi) + rhoa * phi, muw * (1 - phi) + mua * phi
+    lam = -2.0 / 3.0 * mu
+    Ai = np.linalg.inv(A)
+    G = Ai.T @ Ai
+    nu, GG = mu / rho, (G * G).sum()
+    tauM = 1.0 / (rho * np.sqrt(4.0 / p["delt"] ** 2 + 12.0 * nu * nu * GG))
+    tauC = rho * np.sqrt(12.0 * nu * nu * GG) / np.trace(G)
+    # integrals over the element by a 3-point rule per direction
+    q, w = np.polynomial.legendre.leggauss(3)
+    NN, gg, gN_N = np.zeros((8, 8)), np.zeros((8, 8, 3, 3)), np.zeros((8, 8, 3))
+    detA = np.linalg.det(A)
+    for i1 in range(3):
+        for i2 in range(3):
+            for i3 in range(3):
+                xi = np.array([q[i1], q[i2], q[i3]])
+                wt = w[i1] * w[i2] * w[i3] * detA
+                f = 1.0 + _HEX_XI * xi                       # (8, 3) factors (1 + xi_a,k xi_k)
+                N = np.prod(f, axis=1) / 8.0
+                dN = np.stack([_HEX_XI[:, k] * np.prod(np.delete(f, k, axis=1), axis=1) / 8.0 for k in range(3)], 1)
+                g = dN @ Ai                                  # physical gradients (8, 3)
+                NN += wt * np.outer(N, N)
+                gg += wt * g[:, None, :, None] * g[None, :, None, :]   # [a, b, i, j] = d_iN_a d_jN_b
+                gN_N += wt * g[:, None, :] * N[None, :, None]        # [a, b, d] = d_dN_a N_b
+    lap = np.einsum("abii->ab", gg)
+    s, col, row = oc.sys, oc.col, oc.row
+    kscale = np.abs(f2 * mu * lap).max() + f1 * rho * NN.max()
+    gscale = f2 * np.abs(gN_N).max()
+    for a in range(8):
+        for k in range(col[a] - 1, col[a + 1] - 1):
+            b = row[k] - 1
+            for i in range(3):
+                for j in range(3):
+                    want = (i == j) * (f1 * rho * NN[a, b] + f2 * mu * lap[a, b]) \
+                        + f2 * (mu * gg[a, b, j, i] + (tauC + lam) * gg[a, b, i, j])
+                    assert abs(s["K11"][k, 3 * i + j] - want) < 1e-12 * kscale, (a, b, i, j)
+            for d in range(3):
+                assert abs(s["G"][k, d] + f2 * gN_N[a, b, d]) < 1e-12 * gscale
+                wd = f2 * gN_N[b, a, d] + f1 * tauM * rho * gN_N[a, b, d]
+                assert abs(s["D1"][k, d] - wd) < 1e-12 * gscale
+            assert abs(s["M"][k] - f2 * tauM * lap[a, b]) < 1e-12 * f2 * tauM * np.abs(lap).max()
+            assert abs(s["LS"][k] - f1 * NN[a, b]) < 1e-13 * f1 * NN.max()
