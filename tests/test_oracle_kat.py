@@ -861,3 +861,55 @@ def test_hex_nsvof_element_matrix_at_rest(oracle):
                 assert abs(s["D1"][k, d] - wd) < 1e-12 * gscale
             assert abs(s["M"][k] - f2 * tauM * lap[a, b]) < 1e-12 * f2 * tauM * np.abs(lap).max()
             assert abs(s["LS"][k] - f1 * NN[a, b]) < 1e-13 * f1 * NN.max()
+
+
+def test_viscous_residual_broadcast_quirk_closed_form(oracle):
+    """Momentum and continuity residuals of one tet with a linear velocity
+    u = B x carried by the mesh (u - ugm = 0: no advection, uprime = 0), no
+    acceleration, pressure or gravity, s_i(a) = sum_k d_kN_a (B_ki + B_ik):
+
+    * NS+VOF (src/solveQuenching.f90:501-512): every component of node a
+      receives -|T| [d_cN_a (tau_C + lambda) tr B + mu (s_1 + s_2 + s_3)],
+      the three scalar viscous terms broadcast to all three components, as
+      the reference writes them;
+    * NS-only e3Rhs_3D_fluid (src/e3RHS.f90:26-95): the stress per component,
+      -|T| [d_cN_a tau_C tr B + mu s_c(a)];
+    * continuity in both: -|T|/4 tr B."""
+    rng = np.random.default_rng(9)
+    B = 0.3 * rng.standard_normal((3, 3))
+    trB = np.trace(B)
+    rho, mu = 1.3, 0.21
+    out = {}
+    for kernel in (F.OVS_ASM_NSVOF, F.OVS_ASM_NS):
+        case, vol = _single_tet_case(rho)
+        case.params.update(mua=mu, muw=mu, delt=0.02, gravvec=(0.0, 0.0, 0.0))
+        x = np.asarray(case.mesh.xg)
+        for f in ("ug", "ugold", "ugm", "ugmold"):
+            case.state[f][:] = x @ B.T
+        for f in ("tg", "tgold"):
+            case.state[f][:] = 300.0
+        oc = oracle.OracleCase(case)
+        if kernel == F.OVS_ASM_NS:
+            oc.assemble_navsto(F.OVS_TENSOR_VEC)
+        else:
+            oc.assemble_quenching(F.OVS_TENSOR_VEC, 3)
+        out[kernel] = (oc.sys["rhsu"].copy(), oc.sys["rhsp"].copy())
+    J = np.stack([x[0] - x[3], x[1] - x[3], x[2] - x[3]], axis=1)
+    Ji = np.linalg.inv(J)
+    gN = np.vstack([Ji, -Ji.sum(axis=0)])
+    G = Ji.T @ Ji
+    nu, GG = mu / rho, (G * G).sum()
+    tauC = rho * np.sqrt(12.0 * nu * nu * GG) / np.trace(G)
+    lam = -2.0 / 3.0 * mu
+    s = gN @ (B + B.T)                      # s[a, i] = sum_k d_kN_a (B_ki + B_ik)
+    quench = -vol * (gN * (tauC + lam) * trB + mu * s.sum(axis=1)[:, None])
+    ns = -vol * (gN * tauC * trB + mu * s)
+    scale = vol * (np.abs(gN).max() * (tauC + mu) * np.abs(B).max())
+    ru, rp = out[F.OVS_ASM_NSVOF]
+    np.testing.assert_allclose(ru, quench, rtol=0, atol=1e-12 * scale)
+    np.testing.assert_allclose(rp, -vol / 4.0 * trB * np.ones(4), rtol=0, atol=1e-13 * vol * abs(trB))
+    ru, rp = out[F.OVS_ASM_NS]
+    np.testing.assert_allclose(ru, ns, rtol=0, atol=1e-12 * scale)
+    np.testing.assert_allclose(rp, -vol / 4.0 * trB * np.ones(4), rtol=0, atol=1e-13 * vol * abs(trB))
+    # the quirk is visible: the two routines differ by more than rounding
+    assert np.abs(out[F.OVS_ASM_NSVOF][0] - ns).max() > 1e-6 * scale
