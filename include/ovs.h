@@ -41,7 +41,9 @@ enum {
   OVS_ERR_NOMEM = -3,         /* device allocation failed */
   OVS_ERR_STATE = -4,         /* call order (e.g. assemble before pattern) */
   OVS_ERR_NONFINITE = -5,     /* NaN/Inf in an assembled residual */
-  OVS_ERR_PATTERN = -6,       /* a node has more neighbours than supported */
+  OVS_ERR_PATTERN = -6,       /* a node's CSR row would exceed 128 entries
+                                 (the reference stops at 27*nshl: 108 for
+                                 tets, 216 for hexes; src/genSparStruc.f90:93) */
   OVS_ERR_NODEVICE = -7,      /* no CUDA device */
   OVS_ERR_TIMEOUT = -8        /* a bounded host wait on the device expired */
 };

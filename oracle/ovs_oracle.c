@@ -32,7 +32,7 @@ int orc_gen_spar_struc(int nnode, int nelem, int nshl, const int* ien,
   int* fill = (int*)calloc((size_t)nnode * maxlen, sizeof(int));
   int* adjcnt = (int*)calloc((size_t)nnode, sizeof(int));
   int* tmpr = (int*)malloc(sizeof(int) * (size_t)maxlen);
-  if (!fill || !adjcnt || !tmpr) return OVS_ERR_NOMEM;
+  if (!fill || !adjcnt || !tmpr) { free(fill); free(adjcnt); free(tmpr); return OVS_ERR_NOMEM; }
   int overflow = 0;
   for (int e = 0; e < nelem; ++e) {
     int ndlist[NSHL_MAX];

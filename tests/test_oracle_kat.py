@@ -913,3 +913,33 @@ def test_viscous_residual_broadcast_quirk_closed_form(oracle):
     np.testing.assert_allclose(rp, -vol / 4.0 * trB * np.ones(4), rtol=0, atol=1e-13 * vol * abs(trB))
     # the quirk is visible: the two routines differ by more than rounding
     assert np.abs(out[F.OVS_ASM_NSVOF][0] - ns).max() > 1e-6 * scale
+
+
+def test_pattern_row_limit_of_the_reference(oracle):
+    """Asadj's row bound (src/genSparStruc.f90:14, :93): a node's list holds at
+    most 27*nshl entries, self included (108 for tets).  A star of tets
+    around node 1 with exactly 108 entries builds; one more distinct
+    neighbour is "Stop the Music!!!" (OVS_ERR_PATTERN)."""
+    import ctypes as C
+
+    def star(nbrs):
+        # tets (1, a, b, c) over consecutive neighbour triples; the last
+        # triple wraps to reuse earlier neighbours, so node 1 sees exactly
+        # `nbrs` distinct neighbours
+        ids = list(range(2, nbrs + 2))
+        tets = []
+        for t in range(0, nbrs, 3):
+            tri = [ids[(t + k) % nbrs] for k in range(3)]
+            tets.append([1] + tri)
+        return np.asfortranarray(np.array(tets, dtype=np.int32)), nbrs + 1
+
+    lib = oracle.load()
+    for nbrs, ok in ((107, True), (108, False)):
+        ien, N = star(nbrs)
+        col = np.zeros(N + 1, dtype=np.int32)
+        icnt = C.c_int(0)
+        st = lib.orc_gen_spar_struc(N, ien.shape[0], 4, oracle._i(ien), oracle._i(col), None, C.byref(icnt))
+        if ok:
+            assert st == 0 and col[1] - col[0] == 108
+        else:
+            assert st == F.OVS_ERR_PATTERN
