@@ -480,3 +480,44 @@ def calculate_residual(ctx: Context, precision: int = F.OVS_FP64) -> np.ndarray:
     """src/solveFlow.f90:169-187: sums of squares (no square root) of the
     momentum, continuity, VOF and temperature residuals."""
     return ctx.residual_norms(precision)
+
+
+def check_convergence(residual, residual0, tol, assemble_field_flag: int, atol) -> np.ndarray:
+    """src/solveFlow.f90:192-222: converged(4) as 0/1 ints.  Momentum and
+    continuity (entries 1, 2) when NS is flagged, VOF (3) when VOF is,
+    temperature (4) when TEM is; a field converges when residual < tol *
+    residual0 or residual < its absolute tolerance (strict comparisons;
+    the reference uses NS_GMRES_atol for both NS entries, LSC_GMRES_atol and
+    TEM_GMRES_atol for the others: atol holds the four in that order).
+    Fields outside the flag stay 0, as the reference leaves them."""
+    r, r0 = np.asarray(residual, dtype=np.float64), np.asarray(residual0, dtype=np.float64)
+    out = np.zeros(4, dtype=np.int32)
+    groups = ((ASSEMBLE_FIELD_NS, (0, 1)), (ASSEMBLE_FIELD_VOF, (2,)), (ASSEMBLE_FIELD_TEM, (3,)))
+    for bit, ks in groups:
+        if assemble_field_flag & bit:
+            for k in ks:
+                out[k] = int(r[k] < tol[k] * r0[k] or r[k] < atol[k])
+    return out
+
+
+def setBCs_NSVOF(ctx: Context):
+    """src/setBCs.f90:172-244 on the registered BC spec (Context.set_bc_spec):
+    IBC columns 1-5 reset and set, Dirichlet velocity and VOF values with
+    their rates."""
+    ctx.apply_bcs(1)
+
+
+def setBCs_Tem(ctx: Context):
+    """src/setBCs.f90:248-278: Dirichlet temperature and its rate."""
+    ctx.apply_bcs(2)
+
+
+def solmultiphasethermofluid_stag(ctx: Context, istep: int, **newton):
+    """The Newton routine of one quench time step (src/solveFlow.f90:4-164)
+    as the driver calls it with istep: a single Newton iteration while
+    istep <= 1 (:50-54) and no temperature solve at istep 0 (:109); the
+    other keyword arguments as Context.quench_newton.  Returns its
+    OvsNewtonInfo."""
+    nm = newton.pop("newton_max", 3)
+    tem = newton.pop("solve_tem", True)
+    return ctx.quench_newton(newton_max=1 if istep <= 1 else nm, solve_tem=bool(tem and istep > 0), **newton)

@@ -38,6 +38,7 @@ from dataclasses import dataclass
 import numpy as np
 
 from . import _ffi as F
+from .api import check_convergence
 
 
 @dataclass
@@ -402,8 +403,8 @@ def quench_newton(comm, parts: dict, newton_max: int = 3, solve_tem: bool = True
             parts[r].update(kind, sol[r])
         return info["iterations"]
 
-    def check(r, r0):
-        return [bool(r[k] < utol[k] * r0[k] or r[k] < atol[k]) for k in range(4)]
+    def check(r, r0):   # check_convergence with all fields flagged, as the reference calls it
+        return [bool(v) for v in check_convergence(r, r0, utol, FIELD_NS | FIELD_VOF | FIELD_TEM, atol)]
 
     set_bcs()
     for r in P:
