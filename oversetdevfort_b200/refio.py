@@ -1,8 +1,9 @@
 """The reference's on-disk formats, so its meshes and restarts run through
-this path: the partition mesh ``part<id>.dat`` (read by input_mesh,
-src/input.f90:15-120; written by genmesh_overset/mesh.f90:140-204) and the
-text restart ``restart<step><rank>`` (readSol / writeSol,
-src/iosol.f90:122-194, 377-454).  Both are Fortran list-directed text; this
+this path: the partition mesh ``part.<id>.dat`` (read by input_mesh,
+src/input.f90:15-120; written by genmesh_overset/mesh.f90:140-204), the
+text restart ``restart.<step>.<rank+1>`` (readSol / writeSol,
+src/iosol.f90:122-194, 377-454) and its ``step.dat`` (readStep, :82-117),
+with the reference's file names (cname, src/cname.f90:4-37).  Both are Fortran list-directed text; this
 module reads and writes them with numpy and builds the `mesh.Case` inputs
 from them.  The overset boundary maps (``l2b.<id>.dat``) belong to the
 overset coupling, which is outside this path, and are not read.
@@ -213,6 +214,46 @@ def bc_spec_from_part(pm: PartMesh, bcug_type, bcug_valu, bcphig_type, bcphig_va
 # the records of a restart, in file order, and the state arrays they fill
 RESTART_READ = ("dgold", "ugold", "ugmold", "acgold", "acgmold", "phigold", "rphigold", "pgold", "tgold", "rtgold")
 RESTART_WRITE = ("dg", "ug", "ugm", "acg", "acgm", "phig", "rphig", "pg", "tgold", "rtgold")
+
+
+def cname(i: int) -> str:
+    """cname (src/cname.f90:4-37): "." and the decimal digits of i without
+    leading zeros, from the lowest nine digits the routine keeps
+    (cname(0) = ".0", cname(1234567890) = ".234567890")."""
+    if i < 0:
+        raise ValueError("cname takes a non-negative integer")
+    return "." + str(int(i) % 10 ** 9)
+
+
+def part_name(part_id: int) -> str:
+    """The partition mesh file input_mesh opens: 'part'//trim(cname(id))//'.dat'
+    (src/input.f90:31)."""
+    return "part" + cname(part_id) + ".dat"
+
+
+def restart_name(step: int, rank: int) -> str:
+    """The restart file of readSol / writeSol for 0-based MPI rank `rank`:
+    trim('restart'//cname(step))//cname(myid + 1) (src/iosol.f90:137, 390)."""
+    return "restart" + cname(step) + cname(rank + 1)
+
+
+def read_step(path) -> tuple[int, float | None]:
+    """readStep (src/iosol.f90:82-117): (Rstep, x_inflow) from step.dat;
+    (0, None) when the file cannot be opened, as its iostat branch leaves
+    Rstep = 0."""
+    try:
+        tk = _Tokens(path)
+    except OSError:
+        return 0, None
+    head = tk.record()
+    return int(head[0]), _float(head[1])
+
+
+def write_step(path, istep: int, x_inflow: float) -> None:
+    """The step.dat record writeSol leaves on the master rank
+    (src/iosol.f90:447-452): istep and x_inflow."""
+    with open(path, "w") as f:
+        f.write(f"{int(istep)} {repr(float(x_inflow))}\n")
 
 
 def read_restart(path, nnode: int) -> tuple[int, float, dict]:

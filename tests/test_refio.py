@@ -145,3 +145,19 @@ def test_bc_spec_from_part_drives_setbcs_like_the_box_spec(tmp_path, oracle):
     np.testing.assert_array_equal(a.ibc, b.ibc)
     with pytest.raises(ValueError):
         refio.bc_spec_from_part(back, ut[:3], uv, pt, pv, tt, tv)
+
+
+def test_reference_file_names_and_step_file(tmp_path):
+    """cname (src/cname.f90:4-37) and the names built from it: part.<id>.dat
+    (src/input.f90:31), restart.<step>.<rank+1> (src/iosol.f90:137, 390);
+    step.dat written and read back (readStep, a missing file gives step 0)."""
+    assert refio.cname(0) == ".0" and refio.cname(7) == ".7" and refio.cname(120) == ".120"
+    assert refio.cname(123456789) == ".123456789" and refio.cname(1234567890) == ".234567890"
+    assert refio.part_name(3) == "part.3.dat"
+    assert refio.restart_name(250, 0) == "restart.250.1" and refio.restart_name(0, 11) == "restart.0.12"
+    assert refio.read_step(tmp_path / "step.dat") == (0, None)
+    refio.write_step(tmp_path / "step.dat", 42, 0.125)
+    assert refio.read_step(tmp_path / "step.dat") == (42, 0.125)
+    # the list-directed record a Fortran compiler writes reads the same
+    (tmp_path / "step2.dat").write_text("          17   1.2500000000000000D-01\n")
+    assert refio.read_step(tmp_path / "step2.dat") == (17, 0.125)
