@@ -218,6 +218,15 @@ def _cpu_worker(args):
     return oc.E, times
 
 
+def _host_cores() -> int:
+    """Cores this process may run on (its affinity set, which a container's
+    CPU limits narrow), not the machine's count."""
+    try:
+        return max(1, len(os.sched_getaffinity(0)))
+    except (AttributeError, OSError):
+        return os.cpu_count() or 1
+
+
 def run_reference(args, world, rank):
     """--impl reference: the reference's CPU algorithm (the oracle port; the
     Fortran reference cannot be compiled here) on all host cores, one
@@ -226,7 +235,7 @@ def run_reference(args, world, rank):
     if rank != 0:
         return
     import multiprocessing as mp
-    cores = os.cpu_count() or 1
+    cores = _host_cores()
     n, nl = args.n, 2
     nslab = max(1, n // nl)
     jobs = [(n, (i * nl) % (n - nl + 1), nl, args.steps, args.warmup) for i in range(cores)]

@@ -26,3 +26,12 @@ def test_fp32_flops_per_tet_from_profile():
 def test_missing_summaries_are_reported():
     assert bench.ncu_traffic_per_tet("no_such_summary.md", 1) == (None, "no ncu summary")
     assert bench.ncu_flops_per_tet("no_such_summary.md", 1) == (None, "no ncu summary")
+
+
+def test_reference_arm_counts_usable_cores():
+    import os
+    import bench
+    n = bench._host_cores()
+    assert 1 <= n <= (os.cpu_count() or n)
+    if hasattr(os, "sched_getaffinity"):
+        assert n == len(os.sched_getaffinity(0))
