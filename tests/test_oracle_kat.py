@@ -943,3 +943,94 @@ def test_pattern_row_limit_of_the_reference(oracle):
             assert st == 0 and col[1] - col[0] == 108
         else:
             assert st == F.OVS_ERR_PATTERN
+
+
+def test_phase_change_terms_at_rest_closed_form(oracle):
+    """The phase-change terms of both quench element routines on one fluid
+    tet at rest, uniform phi = 0.3, phi rate 0.2, T = 400 > Ts, T rate 1.5,
+    c_evap > 0, C_DMDOT = 0.7, gravity on, derived from the reference text:
+    mdot = c_evap (1 - phi) rho_w (T - Ts)/Ts, dmdphi = -c_evap rho_w
+    (T - Ts)/Ts C_DMDOT (src/solveQuenching.f90:343-350), vdot = mdot/rho_a
+    - mdot/rho_w, D = 1/rho_a - 1/rho_w, uprime = tau_M rho g (rL = -rho g),
+    tau_LS irrelevant (no convection):
+      LS  = M_ab [f1 + f2 (vdot + phi D dmdphi - dmdphi/rho_a + tau_C (dmdphi D)^2)]
+      ULS_d = f2 tau_C dmdphi D |T|/4 d_dN_a;  PLS = -f2 dmdphi D M_ab
+      LSU_d = -f2 dmdphi D tau_C |T|/4 d_dN_b
+      RHSu_a = rho g |T|/4 + tau_C vdot |T| gN_a
+      RHSp_a = vdot |T|/4 + |T| gN_a . uprime
+      RHSphi_a = -|T|/4 (rphi + phi vdot - mdot/rho_a + dmdphi D tau_C vdot)
+    (:434-521), and for the temperature (:743-855), with dmdT = c_evap
+    (1 - phi) rho_w/Ts C_DMDOT, Se = ((c_pw - c_pa)(T - Ts) - L) mdot,
+    dSedT = (c_pw - c_pa) mdot + ((c_pw - c_pa)(T - Ts) - L) dmdT:
+      TEM = M_ab (f1 rho c_p - f2 dSedT) + f2 kappa |T| gN_a.gN_b
+      RHST_a = |T|/4 (Se - rho c_p rT)."""
+    case, vol = _single_tet_case(1.0)
+    p = case.params
+    p.update(rhow=1000.0, rhoa=1.0, muw=1e-3, mua=1e-5, delt=1e-3, c_evap=0.05, c_cond=0.02, c_dmdot=0.7)
+    phi, rphi, T, rT = 0.3, 0.2, 400.0, 1.5
+    st = case.state
+    for f, v in (("phig", phi), ("phigold", phi), ("rphig", rphi), ("rphigold", rphi), ("tg", T), ("tgold", T),
+                 ("rtg", rT), ("rtgold", rT)):
+        st[f][:] = v
+    oc = oracle.OracleCase(case)
+    oc.assemble_quenching(F.OVS_TENSOR_MAT | F.OVS_TENSOR_VEC, 3)
+    ns = {k: oc.sys[k].copy() for k in ("LS", "ULS", "PLS", "LSU", "rhsu", "rhsp", "rhsls")}
+    oc.assemble_quenching(F.OVS_TENSOR_MAT | F.OVS_TENSOR_VEC, 4)
+    tem, rhst = oc.sys["TEM"].copy(), oc.sys["rhstem"].copy()
+
+    f1, f2 = p["almi"], p["alfi"] * p["gami"] * p["delt"]
+    rw, ra, Ts = p["rhow"], p["rhoa"], p["ts"]
+    rho = rw * (1 - phi) + ra * phi
+    mu = p["muw"] * (1 - phi) + p["mua"] * phi
+    mdot = p["c_evap"] * (1 - phi) * rw * (T - Ts) / Ts
+    dmdphi = -p["c_evap"] * rw * (T - Ts) / Ts * p["c_dmdot"]
+    dmdT = p["c_evap"] * (1 - phi) * rw / Ts * p["c_dmdot"]
+    vdot = mdot / ra - mdot / rw
+    D = 1.0 / ra - 1.0 / rw
+    x = np.asarray(case.mesh.xg)
+    J = np.stack([x[0] - x[3], x[1] - x[3], x[2] - x[3]], axis=1)
+    Ji = np.linalg.inv(J)
+    gN = np.vstack([Ji, -Ji.sum(axis=0)])
+    G = Ji.T @ Ji
+    nu, GG = mu / rho, (G * G).sum()
+    tauM = 1.0 / (rho * np.sqrt(4.0 / p["delt"] ** 2 + 12.0 * nu * nu * GG))
+    tauC = rho * np.sqrt(12.0 * nu * nu * GG) / np.trace(G)
+    g = np.asarray(p["gravvec"], dtype=float)
+    uprime = tauM * rho * g
+    cpw, cpa = p["cpw"], p["cpa"]
+    rhocp = rw * cpw * (1 - phi) + ra * cpa * phi
+    kap = p["kappaw"] * (1 - phi) + p["kappaa"] * phi
+    Se = ((cpw - cpa) * (T - Ts) - p["lh"]) * mdot
+    dSedT = (cpw - cpa) * mdot + ((cpw - cpa) * (T - Ts) - p["lh"]) * dmdT
+
+    def close(got, want, scale, what):
+        assert abs(got - want) <= 1e-11 * scale, (what, got, want)
+
+    col, row = oc.col, oc.row
+    ls_fac = f1 + f2 * (vdot + phi * D * dmdphi - dmdphi / ra + tauC * (dmdphi * D) ** 2)
+    gs = vol * np.abs(gN).max()
+    for a in range(4):
+        for k in range(col[a] - 1, col[a + 1] - 1):
+            b = row[k] - 1
+            Mab = vol * (1 + (a == b)) / 20.0
+            close(ns["LS"][k], ls_fac * Mab, abs(ls_fac) * vol, ("LS", a, b))
+            close(ns["PLS"][k], -f2 * dmdphi * D * Mab, abs(f2 * dmdphi * D) * vol, ("PLS", a, b))
+            for d in range(3):
+                close(ns["ULS"][k, d], f2 * tauC * dmdphi * D * vol / 4.0 * gN[a, d],
+                      abs(f2 * tauC * dmdphi * D) * gs, ("ULS", a, b, d))
+                close(ns["LSU"][k, d], -f2 * dmdphi * D * tauC * vol / 4.0 * gN[b, d],
+                      abs(f2 * tauC * dmdphi * D) * gs, ("LSU", a, b, d))
+            tw = Mab * (f1 * rhocp - f2 * dSedT) + f2 * kap * vol * (gN[a] @ gN[b])
+            close(tem[k], tw, abs(f1 * rhocp * vol) + abs(f2 * dSedT * vol) + f2 * kap * gs * np.abs(gN).max(),
+                  ("TEM", a, b))
+    for a in range(4):
+        for c in range(3):
+            w = rho * g[c] * vol / 4.0 + tauC * vdot * vol * gN[a, c]
+            close(ns["rhsu"][a, c], w, rho * 9.81 * vol + abs(tauC * vdot) * gs, ("rhsu", a, c))
+        close(ns["rhsp"][a], vdot * vol / 4.0 + vol * gN[a] @ uprime, abs(vdot) * vol + gs * np.abs(uprime).max(),
+              ("rhsp", a))
+        wphi = -vol / 4.0 * (rphi + phi * vdot - mdot / ra + dmdphi * D * tauC * vdot)
+        close(ns["rhsls"][a], wphi, vol * (abs(rphi) + abs(phi * vdot) + abs(mdot / ra) + abs(dmdphi * D * tauC * vdot)),
+              ("rhsphi", a))
+        close(rhst[a], vol / 4.0 * (Se - rhocp * rT), vol * (abs(Se) + abs(rhocp * rT)), ("rhstem", a))
+    assert mdot > 0 and dmdphi < 0 and abs(Se) > 0   # the terms are really present
