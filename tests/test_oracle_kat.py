@@ -945,7 +945,8 @@ def test_pattern_row_limit_of_the_reference(oracle):
             assert st == F.OVS_ERR_PATTERN
 
 
-def test_phase_change_terms_at_rest_closed_form(oracle):
+@pytest.mark.parametrize("T, phi", [(400.0, 0.3), (350.0, 0.3), (350.0, 1.2)])
+def test_phase_change_terms_at_rest_closed_form(oracle, T, phi):
     """The phase-change terms of both quench element routines on one fluid
     tet at rest, uniform phi = 0.3, phi rate 0.2, T = 400 > Ts, T rate 1.5,
     c_evap > 0, C_DMDOT = 0.7, gravity on, derived from the reference text:
@@ -963,11 +964,16 @@ def test_phase_change_terms_at_rest_closed_form(oracle):
     (1 - phi) rho_w/Ts C_DMDOT, Se = ((c_pw - c_pa)(T - Ts) - L) mdot,
     dSedT = (c_pw - c_pa) mdot + ((c_pw - c_pa)(T - Ts) - L) dmdT:
       TEM = M_ab (f1 rho c_p - f2 dSedT) + f2 kappa |T| gN_a.gN_b
-      RHST_a = |T|/4 (Se - rho c_p rT)."""
+      RHST_a = |T|/4 (Se - rho c_p rT).
+    Also the condensation branch (T < Ts: mdot = c_cond phi_c rho_a (T -
+    Ts)/Ts, dmdphi = c_cond rho_a (T - Ts)/Ts C_DMDOT, dmdT = c_cond phi_c
+    rho_a/Ts C_DMDOT), and phi outside [0, 1], where the properties and mdot
+    take the clamped phi_c, the VOF residual the unclamped phi, and dmdphi
+    is zeroed (:362-366)."""
     case, vol = _single_tet_case(1.0)
     p = case.params
     p.update(rhow=1000.0, rhoa=1.0, muw=1e-3, mua=1e-5, delt=1e-3, c_evap=0.05, c_cond=0.02, c_dmdot=0.7)
-    phi, rphi, T, rT = 0.3, 0.2, 400.0, 1.5
+    rphi, rT = 0.2, 1.5
     st = case.state
     for f, v in (("phig", phi), ("phigold", phi), ("rphig", rphi), ("rphigold", rphi), ("tg", T), ("tgold", T),
                  ("rtg", rT), ("rtgold", rT)):
@@ -980,11 +986,19 @@ def test_phase_change_terms_at_rest_closed_form(oracle):
 
     f1, f2 = p["almi"], p["alfi"] * p["gami"] * p["delt"]
     rw, ra, Ts = p["rhow"], p["rhoa"], p["ts"]
-    rho = rw * (1 - phi) + ra * phi
-    mu = p["muw"] * (1 - phi) + p["mua"] * phi
-    mdot = p["c_evap"] * (1 - phi) * rw * (T - Ts) / Ts
-    dmdphi = -p["c_evap"] * rw * (T - Ts) / Ts * p["c_dmdot"]
-    dmdT = p["c_evap"] * (1 - phi) * rw / Ts * p["c_dmdot"]
+    pc = min(max(phi, 0.0), 1.0)
+    rho = rw * (1 - pc) + ra * pc
+    mu = p["muw"] * (1 - pc) + p["mua"] * pc
+    if T > Ts:
+        mdot = p["c_evap"] * (1 - pc) * rw * (T - Ts) / Ts
+        dmdphi = -p["c_evap"] * rw * (T - Ts) / Ts * p["c_dmdot"]
+        dmdT = p["c_evap"] * (1 - pc) * rw / Ts * p["c_dmdot"]
+    else:
+        mdot = p["c_cond"] * pc * ra * (T - Ts) / Ts
+        dmdphi = p["c_cond"] * ra * (T - Ts) / Ts * p["c_dmdot"]
+        dmdT = p["c_cond"] * pc * ra / Ts * p["c_dmdot"]
+    if phi < 0.0 or phi > 1.0:
+        dmdphi = 0.0
     vdot = mdot / ra - mdot / rw
     D = 1.0 / ra - 1.0 / rw
     x = np.asarray(case.mesh.xg)
@@ -998,8 +1012,8 @@ def test_phase_change_terms_at_rest_closed_form(oracle):
     g = np.asarray(p["gravvec"], dtype=float)
     uprime = tauM * rho * g
     cpw, cpa = p["cpw"], p["cpa"]
-    rhocp = rw * cpw * (1 - phi) + ra * cpa * phi
-    kap = p["kappaw"] * (1 - phi) + p["kappaa"] * phi
+    rhocp = rw * cpw * (1 - pc) + ra * cpa * pc
+    kap = p["kappaw"] * (1 - pc) + p["kappaa"] * pc
     Se = ((cpw - cpa) * (T - Ts) - p["lh"]) * mdot
     dSedT = (cpw - cpa) * mdot + ((cpw - cpa) * (T - Ts) - p["lh"]) * dmdT
 
@@ -1014,12 +1028,12 @@ def test_phase_change_terms_at_rest_closed_form(oracle):
             b = row[k] - 1
             Mab = vol * (1 + (a == b)) / 20.0
             close(ns["LS"][k], ls_fac * Mab, abs(ls_fac) * vol, ("LS", a, b))
-            close(ns["PLS"][k], -f2 * dmdphi * D * Mab, abs(f2 * dmdphi * D) * vol, ("PLS", a, b))
-            for d in range(3):
+            close(ns["PLS"][k], -f2 * dmdphi * D * Mab, abs(f2 * dmdphi * D) * vol + 1e-300, ("PLS", a, b))
+            for d in range(3):   # LSU's convection term f2 N_a N_b dphi/dx rounds to ~1e-16 of f2 phi |T| |gN|
                 close(ns["ULS"][k, d], f2 * tauC * dmdphi * D * vol / 4.0 * gN[a, d],
-                      abs(f2 * tauC * dmdphi * D) * gs, ("ULS", a, b, d))
+                      abs(f2 * tauC * dmdphi * D) * gs + 1e-300, ("ULS", a, b, d))
                 close(ns["LSU"][k, d], -f2 * dmdphi * D * tauC * vol / 4.0 * gN[b, d],
-                      abs(f2 * tauC * dmdphi * D) * gs, ("LSU", a, b, d))
+                      abs(f2 * tauC * dmdphi * D) * gs + f2 * gs * abs(phi), ("LSU", a, b, d))
             tw = Mab * (f1 * rhocp - f2 * dSedT) + f2 * kap * vol * (gN[a] @ gN[b])
             close(tem[k], tw, abs(f1 * rhocp * vol) + abs(f2 * dSedT * vol) + f2 * kap * gs * np.abs(gN).max(),
                   ("TEM", a, b))
@@ -1033,4 +1047,5 @@ def test_phase_change_terms_at_rest_closed_form(oracle):
         close(ns["rhsls"][a], wphi, vol * (abs(rphi) + abs(phi * vdot) + abs(mdot / ra) + abs(dmdphi * D * tauC * vdot)),
               ("rhsphi", a))
         close(rhst[a], vol / 4.0 * (Se - rhocp * rT), vol * (abs(Se) + abs(rhocp * rT)), ("rhstem", a))
-    assert mdot > 0 and dmdphi < 0 and abs(Se) > 0   # the terms are really present
+    assert mdot != 0.0 and abs(Se) > 0   # the terms are really present
+    assert (dmdphi == 0.0) == (phi > 1.0)
