@@ -1049,3 +1049,104 @@ def test_phase_change_terms_at_rest_closed_form(oracle, T, phi):
         close(rhst[a], vol / 4.0 * (Se - rhocp * rT), vol * (abs(Se) + abs(rhocp * rT)), ("rhstem", a))
     assert mdot != 0.0 and abs(Se) > 0   # the terms are really present
     assert (dmdphi == 0.0) == (phi > 1.0)
+
+
+def test_uniform_advection_element_matrices_closed_form(oracle):
+    """Both quench routines on one tet with a uniform velocity u relative to
+    the fixed mesh (shconv_a = u.gN_a constant), uniform phi = 0.3, uniform
+    T below Ts, T rate 1.5, gravity on, no phase change: every convection,
+    SUPG and PSPG block, the residuals and the CFL number in closed form
+    (src/solveQuenching.f90:400-521, :786-855), with the taus of e3STAB
+    (uGu now in tau_M, tau_C, tau_LS, tau_T; tau_T built from rho_i c_p,i,
+    the product of the separately interpolated properties, while the
+    Galerkin terms use the interpolated rho c_p) and e3CFL = dt sqrt(uGu):
+      K_ij = delta_ij [f1 rho M + f2 rho sc_b |T|/4 + f2 mu |T| lap
+                      + f1 rho^2 tau_M sc_a |T|/4 + f2 rho^2 tau_M sc_a sc_b |T|]
+             + f2 |T| (mu d_jN_a d_iN_b + (tau_C + lambda) d_iN_a d_jN_b)
+      G_d = -f2 |T|/4 d_dN_a + f2 rho tau_M sc_a d_dN_b |T|
+      D_d = f2 |T|/4 d_dN_b + f1 tau_M rho |T|/4 d_dN_a + f2 tau_M rho sc_b d_dN_a |T|
+      LS  = f1 M + f2 sc_b |T|/4 + tau_LS sc_a (f1 |T|/4 + f2 sc_b |T|)
+      TEM = rhocp (f1 M + f2 sc_b |T|/4) + tau_T rhocp^2 sc_a (f1 |T|/4 + f2 sc_b |T|) + f2 kappa |T| lap
+      RHSu = rho g |T|/4 + rho sc_a uprime |T|, uprime = tau_M rho g;  RHSp = |T| gN_a.uprime
+      RHSphi = 0;  RHST = -rhocp rT (|T|/4 + tau_T rhocp sc_a |T|)."""
+    case, vol = _single_tet_case(1.0)
+    p = case.params
+    p.update(rhow=3.0, rhoa=1.2, muw=0.02, mua=0.004, delt=0.01)
+    u = np.array([0.3, -0.2, 0.5])
+    phi, T, rT = 0.3, 300.0, 1.5
+    st = case.state
+    st["ug"][:] = u
+    st["ugold"][:] = u
+    for f, v in (("phig", phi), ("phigold", phi), ("tg", T), ("tgold", T), ("rtg", rT), ("rtgold", rT)):
+        st[f][:] = v
+    oc = oracle.OracleCase(case)
+    cfl_ns = oc.assemble_quenching(F.OVS_TENSOR_MAT | F.OVS_TENSOR_VEC, 3)
+    ns = {k: oc.sys[k].copy() for k in ("K11", "G", "D1", "M", "LS", "LSU", "ULS", "PLS", "rhsu", "rhsp", "rhsls")}
+    oc.assemble_quenching(F.OVS_TENSOR_MAT | F.OVS_TENSOR_VEC, 4)
+    tem, rhst = oc.sys["TEM"].copy(), oc.sys["rhstem"].copy()
+
+    f1, f2 = p["almi"], p["alfi"] * p["gami"] * p["delt"]
+    dt = p["delt"]
+    rho = p["rhow"] * (1 - phi) + p["rhoa"] * phi
+    mu = p["muw"] * (1 - phi) + p["mua"] * phi
+    lam = -2.0 / 3.0 * mu
+    cp = p["cpw"] * (1 - phi) + p["cpa"] * phi
+    rhocp = p["rhow"] * p["cpw"] * (1 - phi) + p["rhoa"] * p["cpa"] * phi
+    kap = p["kappaw"] * (1 - phi) + p["kappaa"] * phi
+    x = np.asarray(case.mesh.xg)
+    J = np.stack([x[0] - x[3], x[1] - x[3], x[2] - x[3]], axis=1)
+    Ji = np.linalg.inv(J)
+    gN = np.vstack([Ji, -Ji.sum(axis=0)])
+    G = Ji.T @ Ji
+    uGu, GG = u @ G @ u, (G * G).sum()
+    nu = mu / rho
+    tauM = 1.0 / (rho * np.sqrt(4.0 / dt ** 2 + uGu + 12.0 * nu * nu * GG))
+    tauC = rho * np.sqrt(uGu + 12.0 * nu * nu * GG) / np.trace(G)
+    tauLS = 1.0 / np.sqrt(4.0 / dt ** 2 + uGu)
+    kk = kap / (rho * cp)
+    tauT = 1.0 / (rho * cp * np.sqrt(uGu + 4.0 / dt ** 2 + 12.0 * kk * kk * GG))
+    sc = gN @ u
+    g = np.asarray(p["gravvec"], dtype=float)
+    uprime = tauM * rho * g
+    assert abs(cfl_ns - dt * np.sqrt(uGu)) <= 1e-14 * cfl_ns
+
+    def close(got, want, scale, what):
+        assert abs(got - want) <= 1e-11 * scale, (what, got, want)
+
+    col, row = oc.col, oc.row
+    gm = np.abs(gN).max()
+    kscale = vol * (f1 * rho + f2 * rho * np.abs(sc).max() + f2 * mu * gm * gm
+                    + f2 * rho * rho * tauM * np.abs(sc).max() ** 2 + f2 * tauC * gm * gm)
+    for a in range(4):
+        for k in range(col[a] - 1, col[a + 1] - 1):
+            b = row[k] - 1
+            Mab = vol * (1 + (a == b)) / 20.0
+            lap = gN[a] @ gN[b]
+            diag = (f1 * rho * Mab + f2 * rho * sc[b] * vol / 4.0 + f2 * mu * vol * lap
+                    + f1 * rho * rho * tauM * sc[a] * vol / 4.0 + f2 * rho * rho * tauM * sc[a] * sc[b] * vol)
+            for i in range(3):
+                for j in range(3):
+                    want = (i == j) * diag + f2 * vol * (mu * gN[a, j] * gN[b, i] + (tauC + lam) * gN[a, i] * gN[b, j])
+                    close(ns["K11"][k, 3 * i + j], want, kscale, ("K", a, b, i, j))
+            for d in range(3):
+                wg = -f2 * vol / 4.0 * gN[a, d] + f2 * rho * tauM * sc[a] * gN[b, d] * vol
+                wd = f2 * vol / 4.0 * gN[b, d] + f1 * tauM * rho * vol / 4.0 * gN[a, d] + f2 * tauM * rho * sc[b] * gN[a, d] * vol
+                close(ns["G"][k, d], wg, f2 * vol * gm, ("G", a, b, d))
+                close(ns["D1"][k, d], wd, f2 * vol * gm, ("D", a, b, d))
+                assert ns["ULS"][k, d] == 0.0 and abs(ns["LSU"][k, d]) <= 1e-14 * f2 * vol * gm
+            close(ns["M"][k], f2 * tauM * vol * lap, f2 * tauM * vol * gm * gm, ("M", a, b))
+            wls = f1 * Mab + f2 * sc[b] * vol / 4.0 + tauLS * sc[a] * (f1 * vol / 4.0 + f2 * sc[b] * vol)
+            close(ns["LS"][k], wls, vol * (f1 + f2 * np.abs(sc).max() * (1 + tauLS * np.abs(sc).max())), ("LS", a, b))
+            assert ns["PLS"][k] == 0.0
+            wt = (rhocp * (f1 * Mab + f2 * sc[b] * vol / 4.0)
+                  + tauT * rhocp * rhocp * sc[a] * (f1 * vol / 4.0 + f2 * sc[b] * vol) + f2 * kap * vol * lap)
+            close(tem[k], wt, vol * rhocp * (f1 + f2 * np.abs(sc).max()) * (1 + tauT * rhocp * np.abs(sc).max())
+                  + f2 * kap * vol * gm * gm, ("TEM", a, b))
+    for a in range(4):
+        for c in range(3):
+            close(ns["rhsu"][a, c], rho * g[c] * vol / 4.0 + rho * sc[a] * uprime[c] * vol,
+                  rho * 9.81 * vol * (1 + tauM * rho * np.abs(sc).max()), ("rhsu", a, c))
+        close(ns["rhsp"][a], vol * gN[a] @ uprime, vol * gm * np.abs(uprime).max(), ("rhsp", a))
+        assert abs(ns["rhsls"][a]) <= 1e-14 * vol
+        close(rhst[a], -rhocp * rT * (vol / 4.0 + tauT * rhocp * sc[a] * vol),
+              rhocp * rT * vol * (1 + tauT * rhocp * np.abs(sc).max()), ("rhstem", a))
