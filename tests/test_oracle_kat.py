@@ -1051,7 +1051,8 @@ def test_phase_change_terms_at_rest_closed_form(oracle, T, phi):
     assert (dmdphi == 0.0) == (phi > 1.0)
 
 
-def test_uniform_advection_element_matrices_closed_form(oracle):
+@pytest.mark.parametrize("lsc_kdc, tem_kdc, rphi", [(0.0, 0.0, 0.0), (0.3, 0.2, 0.4)])
+def test_uniform_advection_element_matrices_closed_form(oracle, lsc_kdc, tem_kdc, rphi):
     """Both quench routines on one tet with a uniform velocity u relative to
     the fixed mesh (shconv_a = u.gN_a constant), uniform phi = 0.3, uniform
     T below Ts, T rate 1.5, gravity on, no phase change: every convection,
@@ -1068,16 +1069,21 @@ def test_uniform_advection_element_matrices_closed_form(oracle):
       LS  = f1 M + f2 sc_b |T|/4 + tau_LS sc_a (f1 |T|/4 + f2 sc_b |T|)
       TEM = rhocp (f1 M + f2 sc_b |T|/4) + tau_T rhocp^2 sc_a (f1 |T|/4 + f2 sc_b |T|) + f2 kappa |T| lap
       RHSu = rho g |T|/4 + rho sc_a uprime |T|, uprime = tau_M rho g;  RHSp = |T| gN_a.uprime
-      RHSphi = 0;  RHST = -rhocp rT (|T|/4 + tau_T rhocp sc_a |T|)."""
+      RHSphi = 0;  RHST = -rhocp rT (|T|/4 + tau_T rhocp sc_a |T|).
+    With the discontinuity-capturing constants on (:419-423, :795-801) and a
+    phi rate: k_dc_phi = LSC_kdc |rphi| / |G|_F adds f2 k_dc_phi |T| lap to
+    LS, k_dc_T = TEM_kdc |rhocp rT| / |G|_F / Tref adds f2 k_dc_T |T| lap to
+    TEM, and RHSphi = -rphi (|T|/4 + tau_LS sc_a |T|)."""
     case, vol = _single_tet_case(1.0)
     p = case.params
-    p.update(rhow=3.0, rhoa=1.2, muw=0.02, mua=0.004, delt=0.01)
+    p.update(rhow=3.0, rhoa=1.2, muw=0.02, mua=0.004, delt=0.01, lsc_kdc=lsc_kdc, tem_kdc=tem_kdc, tref=2.0)
     u = np.array([0.3, -0.2, 0.5])
     phi, T, rT = 0.3, 300.0, 1.5
     st = case.state
     st["ug"][:] = u
     st["ugold"][:] = u
-    for f, v in (("phig", phi), ("phigold", phi), ("tg", T), ("tgold", T), ("rtg", rT), ("rtgold", rT)):
+    for f, v in (("phig", phi), ("phigold", phi), ("tg", T), ("tgold", T), ("rtg", rT), ("rtgold", rT),
+                 ("rphig", rphi), ("rphigold", rphi)):
         st[f][:] = v
     oc = oracle.OracleCase(case)
     cfl_ns = oc.assemble_quenching(F.OVS_TENSOR_MAT | F.OVS_TENSOR_VEC, 3)
@@ -1108,6 +1114,8 @@ def test_uniform_advection_element_matrices_closed_form(oracle):
     sc = gN @ u
     g = np.asarray(p["gravvec"], dtype=float)
     uprime = tauM * rho * g
+    kdc_phi = lsc_kdc * abs(rphi) / np.sqrt(GG)
+    kdc_T = tem_kdc * abs(rhocp * rT) / np.sqrt(GG) / p["tref"]
     assert abs(cfl_ns - dt * np.sqrt(uGu)) <= 1e-14 * cfl_ns
 
     def close(got, want, scale, what):
@@ -1135,18 +1143,21 @@ def test_uniform_advection_element_matrices_closed_form(oracle):
                 close(ns["D1"][k, d], wd, f2 * vol * gm, ("D", a, b, d))
                 assert ns["ULS"][k, d] == 0.0 and abs(ns["LSU"][k, d]) <= 1e-14 * f2 * vol * gm
             close(ns["M"][k], f2 * tauM * vol * lap, f2 * tauM * vol * gm * gm, ("M", a, b))
-            wls = f1 * Mab + f2 * sc[b] * vol / 4.0 + tauLS * sc[a] * (f1 * vol / 4.0 + f2 * sc[b] * vol)
-            close(ns["LS"][k], wls, vol * (f1 + f2 * np.abs(sc).max() * (1 + tauLS * np.abs(sc).max())), ("LS", a, b))
+            wls = (f1 * Mab + f2 * sc[b] * vol / 4.0 + tauLS * sc[a] * (f1 * vol / 4.0 + f2 * sc[b] * vol)
+                   + f2 * kdc_phi * vol * lap)
+            close(ns["LS"][k], wls, vol * (f1 + f2 * np.abs(sc).max() * (1 + tauLS * np.abs(sc).max())
+                                           + f2 * kdc_phi * gm * gm), ("LS", a, b))
             assert ns["PLS"][k] == 0.0
             wt = (rhocp * (f1 * Mab + f2 * sc[b] * vol / 4.0)
-                  + tauT * rhocp * rhocp * sc[a] * (f1 * vol / 4.0 + f2 * sc[b] * vol) + f2 * kap * vol * lap)
+                  + tauT * rhocp * rhocp * sc[a] * (f1 * vol / 4.0 + f2 * sc[b] * vol) + f2 * (kap + kdc_T) * vol * lap)
             close(tem[k], wt, vol * rhocp * (f1 + f2 * np.abs(sc).max()) * (1 + tauT * rhocp * np.abs(sc).max())
-                  + f2 * kap * vol * gm * gm, ("TEM", a, b))
+                  + f2 * (kap + kdc_T) * vol * gm * gm, ("TEM", a, b))
     for a in range(4):
         for c in range(3):
             close(ns["rhsu"][a, c], rho * g[c] * vol / 4.0 + rho * sc[a] * uprime[c] * vol,
                   rho * 9.81 * vol * (1 + tauM * rho * np.abs(sc).max()), ("rhsu", a, c))
         close(ns["rhsp"][a], vol * gN[a] @ uprime, vol * gm * np.abs(uprime).max(), ("rhsp", a))
-        assert abs(ns["rhsls"][a]) <= 1e-14 * vol
+        close(ns["rhsls"][a], -rphi * (vol / 4.0 + tauLS * sc[a] * vol),
+              vol * (abs(rphi) * (1 + tauLS * np.abs(sc).max()) + 1e-3), ("rhsphi", a))
         close(rhst[a], -rhocp * rT * (vol / 4.0 + tauT * rhocp * sc[a] * vol),
               rhocp * rT * vol * (1 + tauT * rhocp * np.abs(sc).max()), ("rhstem", a))
