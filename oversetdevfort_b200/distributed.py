@@ -204,6 +204,12 @@ class DeviceOperator:
         F.check(self.ctx.lib.ovs_precond_device(self.ctx.h, self.system, self.precision, x.data_ptr(),
                                                 y.data_ptr()), "ovs_precond_device")
 
+    def apply(self, x, y):
+        """y = A x without the preconditioner (the refinement residual)."""
+        self._sync()
+        F.check(self.ctx.lib.ovs_spmv_device(self.ctx.h, self.system, self.precision, 0, x.data_ptr(),
+                                             y.data_ptr()), "ovs_spmv_device")
+
 
 def gmres_cycle(comm, ops: dict, rhs: dict, tol: float, kspace: int, kspace_min: int = 1, tem: bool = False,
                 orthog: str = "mgs"):
@@ -304,6 +310,48 @@ def gmres_cycle(comm, ops: dict, rhs: dict, tol: float, kspace: int, kspace_min:
     comm.halo(sol)   # commu 'out': ghosts take their owners' values
     info.update(iterations=iks, ercheck=ercheck, converged=bool(ercheck <= epsnrm))
     return sol, info
+
+
+def solve_refined(comm, inner: dict, outer: dict, rhs: dict, rtol: float, kspace: int = 50,
+                  max_cycles: int = 100, tem: bool = False, orthog: str = "mgs", floor_tol: float = 1e-6):
+    """A x = b to a true relative residual ||b - A x||_2 <= rtol ||b||_2 over
+    the partitions: `ovs_solve`'s refinement loop on distributed vectors.
+    Each cycle solves the current residual with one GMRES cycle on the
+    `inner` operators (P^-1 A and P^-1 of the FP32 system for mixed
+    precision) to the relative tolerance rtol/rel, clamped to
+    [floor_tol, 0.5], adds the correction, and forms r = b - A x with the
+    `outer` operators' plain FP64 product (`apply`) after a halo update of x.
+    Norms are global sums over owned rows.  Returns (x per part with ghosts
+    filled, info: cycles, iterations, converged, rel_residual)."""
+    import torch
+    P = comm.parts()
+    pl = comm.plan
+    ow = {r: torch.as_tensor(pl.owned[r], dtype=torch.long, device=rhs[r].device) for r in P}
+
+    def gnorm2(v):
+        return comm.allreduce([float((v[r][:, ow[r]] ** 2).sum()) for r in P])
+
+    x = {r: torch.zeros_like(rhs[r]) for r in P}
+    res = {r: rhs[r].clone() for r in P}
+    bnorm = math.sqrt(gnorm2(rhs))
+    rel = 1.0 if bnorm > 0.0 else 0.0
+    cycles = iters = 0
+    while rel > rtol and cycles < max_cycles:
+        tin = min(max(rtol / rel, floor_tol), 0.5)
+        dx, info = gmres_cycle(comm, inner, res, tin, kspace, 1, tem=tem, orthog=orthog)
+        iters += info["iterations"]
+        cycles += 1
+        for r in P:
+            x[r] = x[r] + dx[r]
+        comm.halo(x)
+        for r in P:
+            ax = torch.empty_like(x[r])
+            outer[r].apply(x[r], ax)
+            res[r] = rhs[r] - ax
+        rel = math.sqrt(gnorm2(res)) / bnorm
+        if rel != rel or info["iterations"] == 0:
+            break
+    return x, {"cycles": cycles, "iterations": iters, "converged": bool(rel <= rtol), "rel_residual": rel}
 
 
 # assembleQuenching field flags (commonpars, src/modules.f90:218-222)

@@ -438,3 +438,54 @@ def test_partitioned_time_loop_matches_one_domain(oracle):
             g = og.state_arrays[name]
             np.testing.assert_allclose(ocs[r].state_arrays[name], g[p.nodes], rtol=0,
                                        atol=1e-10 * np.abs(g).max(), err_msg=name)
+
+
+class OracleApply(OracleOperator):
+    """OracleOperator with the plain product y = A x (refinement residual)."""
+
+    def apply(self, x, y):
+        y.copy_(torch.from_numpy(np.ascontiguousarray(self.oc.spmv(self.kind, np.asfortranarray(x.numpy().T)).T)))
+
+
+def _fp32_copy(oracle, case, part, kind, oc64):
+    """The same local system with every matrix value rounded to FP32 (the
+    inner operator of the mixed-precision refinement)."""
+    oc = oracle.OracleCase(P.local_case(case, part))
+    d = oc64.system(kind)
+    oc.load_system(kind, {k: (v if k == "rhs" else v.astype(np.float32).astype(np.float64)) for k, v in d.items()})
+    return oc
+
+
+@pytest.mark.parametrize("kind", ["nsvof", "tem"])
+def test_partitioned_refined_solve_reaches_true_residual(oracle, kind):
+    """distributed.solve_refined over three parts: inner GMRES cycles on the
+    FP32-rounded system (floor 1e-6 per cycle), the FP64 residual outside;
+    the true relative residual, recomputed here on the one-domain FP64
+    system from the gathered owned rows, is below 1e-8, and it took more
+    than one cycle."""
+    case = _case(kind)
+    rtol = 1e-8
+    parts = P.make_parts(case.mesh, 3)
+    plan = D.halo_plan(parts)
+    inner, outer, rhs = {}, {}, {}
+    for r, p in enumerate(parts):
+        oc = _local(oracle, case, p, kind)
+        outer[r] = OracleApply(oc, kind)
+        inner[r] = OracleOperator(_fp32_copy(oracle, case, p, kind, oc), kind)
+        rhs[r] = torch.from_numpy(np.ascontiguousarray(oc.system(kind)["rhs"].T))
+    x, info = D.solve_refined(D.LocalComm(plan), inner, outer, rhs, rtol, kspace=60, max_cycles=50,
+                              tem=kind == "tem")
+    assert info["converged"] and info["cycles"] > 1 and info["rel_residual"] <= rtol
+    og = oracle.OracleCase(case)
+    og.assemble_quenching(6, 4 if kind == "tem" else 3)
+    nf = NF[kind]
+    xg = np.zeros((case.mesh.nnode, nf))
+    for r, p in enumerate(parts):
+        xg[p.nodes[plan.owned[r]]] = x[r].numpy().T[plan.owned[r]]
+    for r, p in enumerate(parts):   # ghosts hold their owners' values exactly
+        np.testing.assert_array_equal(x[r].numpy().T, xg[p.nodes])
+    b = og.system(kind)["rhs"]
+    res = b - og.spmv(kind, np.asfortranarray(xg))
+    true_rel = np.linalg.norm(res) / np.linalg.norm(b)
+    assert true_rel <= 1.01 * rtol, true_rel
+    assert abs(true_rel - info["rel_residual"]) <= 1e-3 * rtol
