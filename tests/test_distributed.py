@@ -489,3 +489,51 @@ def test_partitioned_refined_solve_reaches_true_residual(oracle, kind):
     true_rel = np.linalg.norm(res) / np.linalg.norm(b)
     assert true_rel <= 1.01 * rtol, true_rel
     assert abs(true_rel - info["rel_residual"]) <= 1e-3 * rtol
+
+
+def _refined_rank_main(rank, world, port, q):
+    import datetime
+    import torch.distributed as dist
+    from oracle import pyoracle
+    os.environ["MASTER_ADDR"] = "127.0.0.1"
+    os.environ["MASTER_PORT"] = str(port)
+    dist.init_process_group("gloo", rank=rank, world_size=world, timeout=datetime.timedelta(seconds=120))
+    kind, rtol = "nsvof", 1e-8
+    case = _case(kind)
+    parts = P.make_parts(case.mesh, world)
+    plan = D.halo_plan(parts)
+    oc = _local(pyoracle, case, parts[rank], kind)
+    inner = {rank: OracleOperator(_fp32_copy(pyoracle, case, parts[rank], kind, oc), kind)}
+    outer = {rank: OracleApply(oc, kind)}
+    rhs = {rank: torch.from_numpy(np.ascontiguousarray(oc.system(kind)["rhs"].T))}
+    with np.errstate(divide="ignore", invalid="ignore"):
+        x, info = D.solve_refined(D.TorchComm(plan, rank), inner, outer, rhs, rtol, kspace=60, max_cycles=50)
+    gathered = [None] * world if rank == 0 else None
+    dist.gather_object((parts[rank].nodes, plan.owned[rank], x[rank].numpy(), info), gathered, dst=0)
+    if rank == 0:
+        og = pyoracle.OracleCase(case)
+        og.assemble_quenching(6, 3)
+        xg = np.zeros((case.mesh.nnode, NF[kind]))
+        for nodes, owned, xl, _ in gathered:
+            xg[nodes[owned]] = xl.T[owned]
+        b = og.system(kind)["rhs"]
+        true_rel = np.linalg.norm(b - og.spmv(kind, np.asfortranarray(xg))) / np.linalg.norm(b)
+        same = len({(i["cycles"], i["iterations"]) for *_, i in gathered}) == 1
+        q.put(bool(info["converged"] and info["cycles"] > 1 and true_rel <= 1.01 * rtol and same))
+    dist.barrier()
+    dist.destroy_process_group()
+
+
+def test_two_gloo_ranks_refined_solve(oracle):
+    import torch.multiprocessing as mp
+    ctx = mp.get_context("spawn")
+    q = ctx.Queue()
+    port = _free_port()
+    procs = [ctx.Process(target=_refined_rank_main, args=(r, 2, port, q)) for r in range(2)]
+    for p in procs:
+        p.start()
+    ok = q.get(timeout=300)
+    for p in procs:
+        p.join(timeout=120)
+        assert p.exitcode == 0
+    assert ok
