@@ -244,6 +244,11 @@ typedef struct ovs_bc_spec {
  * reference's Newton routine calls them (src/solveFlow.f90:35-36 before the
  * first residual, :58-60 at the top of every Newton iteration). */
 int ovs_set_bc_spec(ovs_ctx* ctx, const ovs_bc_spec* spec);
+/* The checks ovs_set_bc_spec makes, without a context or a device, for a
+ * mesh of nnode nodes: OVS_OK, or OVS_ERR_ARG for a FACE_ID outside
+ * 1..ntype, offsets that do not ascend from 0, a node id outside 1..nnode,
+ * a node listed twice in one boundary, or a missing table. */
+int ovs_check_bc_spec(const ovs_bc_spec* spec, int nnode);
 
 /* which & 1: setBCs_NSVOF (IBC = 0; NodeID 101 -> IBC(1:5) = 1; Dirichlet
  * velocity / VOF values with acg, rphig = ((v - vold) Dtgl + (gami - 1)

@@ -521,3 +521,11 @@ def solmultiphasethermofluid_stag(ctx: Context, istep: int, **newton):
     nm = newton.pop("newton_max", 3)
     tem = newton.pop("solve_tem", True)
     return ctx.quench_newton(newton_max=1 if istep <= 1 else nm, solve_tem=bool(tem and istep > 0), **newton)
+
+
+def check_bc_spec(spec, nnode: int) -> int:
+    """ovs_check_bc_spec: the checks of Context.set_bc_spec for a mesh of
+    nnode nodes, without a device.  Returns the status (OVS_OK or
+    OVS_ERR_ARG)."""
+    keep, cs = spec.to_c()
+    return int(F.load().ovs_check_bc_spec(C.byref(cs), int(nnode)))

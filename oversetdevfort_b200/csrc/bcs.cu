@@ -85,12 +85,13 @@ void ovs_bcs_free(ovs_ctx* c) {
   c->have_bcs = false;
 }
 
-int ovs_set_bc_spec(ovs_ctx* c, const ovs_bc_spec* sp) {
-  if (!c) return OVS_ERR_ARG;
-  int st;
-  if ((st = ovs_activate(c))) return st;
-  OVS_CUDA_TRY(cudaStreamSynchronize(c->stream));
-  if (!sp) { ovs_bcs_free(c); return OVS_OK; }
+namespace {
+// The checks of a setBCs input for a mesh of N nodes: FACE_IDs index the
+// *Type tables, offsets ascend from 0, node ids lie in 1..N and are
+// distinct within a boundary (one writer per node per launch).  Fills the
+// per-boundary records (types read by FACE_ID, values by boundary number)
+// and the 0-based node ids when the outputs are given.
+int validate_bc_spec(const ovs_bc_spec* sp, int N, std::vector<BcBound>* bbo, std::vector<int>* nodeso) {
   const int nb = sp->nbound, nt = sp->ntype;
   if (nb < 0 || nt < 0 || (nb > 0 && (!sp->face_id || !sp->bnode_ptr))) return OVS_ERR_ARG;
   if (nb > 0 && (!sp->bcug_type || !sp->bcug_valu || !sp->bcphig_type || !sp->bcphig_valu ||
@@ -103,7 +104,7 @@ int ovs_set_bc_spec(ovs_ctx* c, const ovs_bc_spec* sp) {
     const int fid = sp->face_id[b];
     if (fid < 1 || fid > nt) return OVS_ERR_ARG;   // the *Type tables are read by FACE_ID
     const int o0 = sp->bnode_ptr[b], o1 = sp->bnode_ptr[b + 1];
-    if (o1 < o0 || o1 > total) return OVS_ERR_ARG;
+    if (o0 < 0 || o1 < o0 || o1 > total) return OVS_ERR_ARG;
     BcBound& r = bb[b];
     r.off = o0;
     r.n = o1 - o0;
@@ -118,7 +119,7 @@ int ovs_set_bc_spec(ovs_ctx* c, const ovs_bc_spec* sp) {
   }
   std::vector<int> nodes(total);
   for (int k = 0; k < total; ++k) {
-    if (sp->bnodes[k] < 1 || sp->bnodes[k] > c->N) return OVS_ERR_ARG;
+    if (sp->bnodes[k] < 1 || sp->bnodes[k] > N) return OVS_ERR_ARG;
     nodes[k] = sp->bnodes[k] - 1;
   }
   for (int b = 0; b < nb; ++b) {   // BNODES of one boundary are distinct (one writer per node per launch)
@@ -126,6 +127,27 @@ int ovs_set_bc_spec(ovs_ctx* c, const ovs_bc_spec* sp) {
     std::sort(v.begin(), v.end());
     if (std::adjacent_find(v.begin(), v.end()) != v.end()) return OVS_ERR_ARG;
   }
+  if (bbo) *bbo = std::move(bb);
+  if (nodeso) *nodeso = std::move(nodes);
+  return OVS_OK;
+}
+}  // namespace
+
+int ovs_check_bc_spec(const ovs_bc_spec* sp, int nnode) {
+  if (!sp || nnode <= 0) return OVS_ERR_ARG;
+  return validate_bc_spec(sp, nnode, nullptr, nullptr);
+}
+
+int ovs_set_bc_spec(ovs_ctx* c, const ovs_bc_spec* sp) {
+  if (!c) return OVS_ERR_ARG;
+  int st;
+  if ((st = ovs_activate(c))) return st;
+  OVS_CUDA_TRY(cudaStreamSynchronize(c->stream));
+  if (!sp) { ovs_bcs_free(c); return OVS_OK; }
+  std::vector<BcBound> bb;
+  std::vector<int> nodes;
+  if ((st = validate_bc_spec(sp, c->N, &bb, &nodes))) return st;
+  const int total = (int)nodes.size();
   ovs_bcs_free(c);
   cudaStream_t s = c->stream;
   if (total > 0) {

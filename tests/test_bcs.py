@@ -75,3 +75,40 @@ def test_set_bcs_face_id_and_boundary_indexing(oracle):
     # T: type row 2 (FACE_ID 2) is Dirichlet -> boundary 1 with value 111
     np.testing.assert_array_equal(s["tg"][x0], 111.0)
     np.testing.assert_array_equal(ibc[x1, 5], 0)
+
+
+def test_bc_spec_checks_without_a_device(lib):
+    """ovs_check_bc_spec, the checks ovs_set_bc_spec makes, on the host:
+    the box spec passes (boundaries sharing edge nodes are fine); a FACE_ID
+    beyond the type tables, a node id outside 1..N, a node twice in one
+    boundary, offsets not starting at 0 and a missing table are rejected."""
+    import ctypes as C
+    from oversetdevfort_b200 import _ffi as F
+    from oversetdevfort_b200 import api
+    m = M.box_tet(3, 2, 2)
+    good = M.box_bc_spec(m, u={1: (0.0, 0.0, 0.0), 6: (1.0, None, 0.0)}, phi={5: 1.0}, T={5: 300.0},
+                         face_ids=(2, 1, 3, 4, 6, 5))
+    assert api.check_bc_spec(good, m.nnode) == F.OVS_OK
+    assert api.check_bc_spec(good, m.nnode - 1) == F.OVS_ERR_ARG      # the last node is out of range
+    bad_fid = M.box_bc_spec(m)
+    bad_fid.face_id = bad_fid.face_id.copy()
+    bad_fid.face_id[0] = 7
+    assert api.check_bc_spec(bad_fid, m.nnode) == F.OVS_ERR_ARG
+    bad_node = M.box_bc_spec(m)
+    bad_node.bnodes = [b.copy() for b in bad_node.bnodes]
+    bad_node.bnodes[2][0] = 0
+    assert api.check_bc_spec(bad_node, m.nnode) == F.OVS_ERR_ARG
+    dup = M.box_bc_spec(m)
+    dup.bnodes = [b.copy() for b in dup.bnodes]
+    dup.bnodes[3][1] = dup.bnodes[3][0]
+    assert api.check_bc_spec(dup, m.nnode) == F.OVS_ERR_ARG
+    keep, cs = good.to_c()
+    keep["ptr"][0] = 1                                                # offsets must start at 0
+    assert lib.ovs_check_bc_spec(C.byref(cs), m.nnode) == F.OVS_ERR_ARG
+    keep, cs = good.to_c()
+    cs.bctg_type = None                                               # a missing table
+    assert lib.ovs_check_bc_spec(C.byref(cs), m.nnode) == F.OVS_ERR_ARG
+    assert lib.ovs_check_bc_spec(None, m.nnode) == F.OVS_ERR_ARG
+    empty = M.BcSpec(np.zeros(0, np.int32), [], np.zeros((0, 3), np.int32), np.zeros((0, 3)), np.zeros(0, np.int32),
+                     np.zeros(0), np.zeros(0, np.int32), np.zeros(0), None)
+    assert api.check_bc_spec(empty, m.nnode) == F.OVS_OK              # no boundaries
