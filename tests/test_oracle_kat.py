@@ -797,6 +797,68 @@ def test_temperature_element_matrix_at_rest_closed_form(oracle, solid):
             assert abs(T[k] - want) < 1e-12 * scale, (a, b, T[k], want)
 
 
+def _hex_integrals(A):
+    """Integrals over the parallelepiped x = x0 + A xi of a trilinear hex by
+    a 3-point Gauss-Legendre rule per direction: int N_a N_b, int d_iN_a
+    d_jN_b ([a, b, i, j]) and int d_dN_a N_b ([a, b, d])."""
+    Ai = np.linalg.inv(A)
+    q, w = np.polynomial.legendre.leggauss(3)
+    NN, gg, gN_N = np.zeros((8, 8)), np.zeros((8, 8, 3, 3)), np.zeros((8, 8, 3))
+    detA = np.linalg.det(A)
+    for i1 in range(3):
+        for i2 in range(3):
+            for i3 in range(3):
+                xi = np.array([q[i1], q[i2], q[i3]])
+                wt = w[i1] * w[i2] * w[i3] * detA
+                f = 1.0 + _HEX_XI * xi                       # (8, 3) factors (1 + xi_a,k xi_k)
+                N = np.prod(f, axis=1) / 8.0
+                dN = np.stack([_HEX_XI[:, k] * np.prod(np.delete(f, k, axis=1), axis=1) / 8.0 for k in range(3)], 1)
+                g = dN @ Ai                                  # physical gradients (8, 3)
+                NN += wt * np.outer(N, N)
+                gg += wt * g[:, None, :, None] * g[None, :, None, :]
+                gN_N += wt * g[:, None, :] * N[None, :, None]
+    return NN, gg, gN_N
+
+
+def _single_hex_case(A, rhow, rhoa, muw, mua, phi, T, delt):
+    x0 = np.array([0.2, -0.1, 0.3])
+    xg = np.asfortranarray(x0 + _HEX_XI @ A.T)
+    ien = np.asfortranarray(np.arange(1, 9, dtype=np.int32)[None, :])
+    m = M.Mesh(xg, ien, np.array([102], dtype=np.int32), [np.arange(8)] * 6, (1, 1, 1), (1, 1, 1))
+    p = M.base_params(rhow=rhow, rhoa=rhoa, muw=muw, mua=mua, delt=delt)
+    st = M.empty_state(8)
+    for f in ("phig", "phigold"):
+        st[f][:] = phi
+    for f in ("tg", "tgold"):
+        st[f][:] = T
+    return M.Case("single_hex", m, p, st, np.zeros((8, 8), dtype=np.int32, order="F"), F.OVS_ASM_NSVOF)
+
+
+def test_hex_temperature_element_matrix_at_rest(oracle):
+    """The temperature matrix of one trilinear hex at rest, no phase change:
+    TEM = f1 rho c_p int N_a N_b + f2 kappa int gN_a.gN_b, the integrals by
+    the 3-point rule."""
+    rng = np.random.default_rng(6)
+    A = np.diag([0.3, 0.45, 0.35]) + 0.05 * rng.standard_normal((3, 3))
+    phi = 0.7
+    case = _single_hex_case(A, 2.0, 0.5, 0.3, 0.05, phi, 300.0, 0.05)
+    oc = oracle.OracleCase(case)
+    oc.assemble_quenching(F.OVS_TENSOR_MAT | F.OVS_TENSOR_VEC, 4)
+    p = case.params
+    f1, f2 = p["almi"], p["alfi"] * p["gami"] * p["delt"]
+    rhocp = p["rhow"] * p["cpw"] * (1 - phi) + p["rhoa"] * p["cpa"] * phi
+    kap = p["kappaw"] * (1 - phi) + p["kappaa"] * phi
+    NN, gg, _ = _hex_integrals(A)
+    lap = np.einsum("abii->ab", gg)
+    want_all = f1 * rhocp * NN + f2 * kap * lap
+    scale = np.abs(want_all).max()
+    col, row, T = oc.col, oc.row, oc.sys["TEM"]
+    for a in range(8):
+        for k in range(col[a] - 1, col[a + 1] - 1):
+            b = row[k] - 1
+            assert abs(T[k] - want_all[a, b]) <= 1e-12 * scale, (a, b)
+
+
 def test_hex_nsvof_element_matrix_at_rest(oracle):
     """The NS+VOF element matrices of one trilinear hexahedron (the hex
     extension: linhexshl with the 2x2x2 rule) on a parallelepiped at rest,
@@ -827,22 +889,7 @@ def test_hex_nsvof_element_matrix_at_rest(oracle):
     nu, GG = mu / rho, (G * G).sum()
     tauM = 1.0 / (rho * np.sqrt(4.0 / p["delt"] ** 2 + 12.0 * nu * nu * GG))
     tauC = rho * np.sqrt(12.0 * nu * nu * GG) / np.trace(G)
-    # integrals over the element by a 3-point rule per direction
-    q, w = np.polynomial.legendre.leggauss(3)
-    NN, gg, gN_N = np.zeros((8, 8)), np.zeros((8, 8, 3, 3)), np.zeros((8, 8, 3))
-    detA = np.linalg.det(A)
-    for i1 in range(3):
-        for i2 in range(3):
-            for i3 in range(3):
-                xi = np.array([q[i1], q[i2], q[i3]])
-                wt = w[i1] * w[i2] * w[i3] * detA
-                f = 1.0 + _HEX_XI * xi                       # (8, 3) factors (1 + xi_a,k xi_k)
-                N = np.prod(f, axis=1) / 8.0
-                dN = np.stack([_HEX_XI[:, k] * np.prod(np.delete(f, k, axis=1), axis=1) / 8.0 for k in range(3)], 1)
-                g = dN @ Ai                                  # physical gradients (8, 3)
-                NN += wt * np.outer(N, N)
-                gg += wt * g[:, None, :, None] * g[None, :, None, :]   # [a, b, i, j] = d_iN_a d_jN_b
-                gN_N += wt * g[:, None, :] * N[None, :, None]        # [a, b, d] = d_dN_a N_b
+    NN, gg, gN_N = _hex_integrals(A)
     lap = np.einsum("abii->ab", gg)
     s, col, row = oc.sys, oc.col, oc.row
     kscale = np.abs(f2 * mu * lap).max() + f1 * rho * NN.max()
@@ -1161,3 +1208,55 @@ def test_uniform_advection_element_matrices_closed_form(oracle, lsc_kdc, tem_kdc
               vol * (abs(rphi) * (1 + tauLS * np.abs(sc).max()) + 1e-3), ("rhsphi", a))
         close(rhst[a], -rhocp * rT * (vol / 4.0 + tauT * rhocp * sc[a] * vol),
               rhocp * rT * vol * (1 + tauT * rhocp * np.abs(sc).max()), ("rhstem", a))
+
+
+def test_ns_uniform_advection_matrix_closed_form(oracle):
+    """IntElmAss_NS_overset on one tet with a uniform velocity u relative to
+    the fixed mesh: e3LHS_3D_fluid_Old (src/e3LHS.f90:4-161) with tmp1_a =
+    rho u.gN_a, tauBar = 0 and the taus of e3STAB_3D (src/e3STAB.f90:4-44)
+    with uGu:
+      K_ij = delta_ij [f1 rho M + f1 tmp1_a tau_M rho |T|/4 + f2 tmp1_b |T|/4
+                      + f2 tmp1_a tau_M tmp1_b |T| + f2 mu |T| lap]
+             + f2 |T| (mu d_jN_a d_iN_b + tau_C d_iN_a d_jN_b)
+      G_d = -f2 |T|/4 d_dN_a + f2 tmp1_a tau_M d_dN_b |T|
+      D_d = f2 |T|/4 d_dN_b + f2 d_dN_a tau_P tmp1_b |T| + f1 tau_P rho |T|/4 d_dN_a
+      M = f2 tau_P |T| lap."""
+    rho, mu = 1.4, 0.05
+    case, vol = _single_tet_case(rho)
+    case.params.update(mua=mu, muw=mu, delt=0.02)
+    u = np.array([0.4, 0.1, -0.3])
+    for f in ("ug", "ugold"):
+        case.state[f][:] = u
+    oc = oracle.OracleCase(case)
+    oc.assemble_navsto(F.OVS_TENSOR_MAT)
+    p = case.params
+    f1, f2 = p["almi"], p["alfi"] * p["gami"] * p["delt"]
+    x = np.asarray(case.mesh.xg)
+    J = np.stack([x[0] - x[3], x[1] - x[3], x[2] - x[3]], axis=1)
+    Ji = np.linalg.inv(J)
+    gN = np.vstack([Ji, -Ji.sum(axis=0)])
+    G = Ji.T @ Ji
+    uGu, GG, nu = u @ G @ u, (G * G).sum(), mu / rho
+    tauM = 1.0 / (rho * np.sqrt(4.0 / p["delt"] ** 2 + uGu + 12.0 * nu * nu * GG))
+    tauC = rho * np.sqrt(uGu + 12.0 * nu * nu * GG) / np.trace(G)
+    t1 = rho * (gN @ u)
+    s, col, row = oc.sys, oc.col, oc.row
+    gm = np.abs(gN).max()
+    kscale = vol * (f1 * rho + f2 * np.abs(t1).max() * (1 + tauM * np.abs(t1).max()) + f2 * (mu + tauC) * gm * gm)
+    for a in range(4):
+        for k in range(col[a] - 1, col[a + 1] - 1):
+            b = row[k] - 1
+            Mab = vol * (1 + (a == b)) / 20.0
+            lap = gN[a] @ gN[b]
+            diag = (f1 * rho * Mab + f1 * t1[a] * tauM * rho * vol / 4.0 + f2 * t1[b] * vol / 4.0
+                    + f2 * t1[a] * tauM * t1[b] * vol + f2 * mu * vol * lap)
+            for i in range(3):
+                for j in range(3):
+                    want = (i == j) * diag + f2 * vol * (mu * gN[a, j] * gN[b, i] + tauC * gN[a, i] * gN[b, j])
+                    assert abs(s["K11"][k, 3 * i + j] - want) <= 1e-11 * kscale, ("K", a, b, i, j)
+            for d in range(3):
+                wg = -f2 * vol / 4.0 * gN[a, d] + f2 * t1[a] * tauM * gN[b, d] * vol
+                wd = f2 * vol / 4.0 * gN[b, d] + f2 * gN[a, d] * tauM * t1[b] * vol + f1 * tauM * rho * vol / 4.0 * gN[a, d]
+                assert abs(s["G"][k, d] - wg) <= 1e-11 * f2 * vol * gm * (1 + tauM * np.abs(t1).max())
+                assert abs(s["D1"][k, d] - wd) <= 1e-11 * f2 * vol * gm * (1 + tauM * np.abs(t1).max())
+            assert abs(s["M"][k] - f2 * tauM * vol * lap) <= 1e-11 * f2 * tauM * vol * gm * gm
