@@ -305,3 +305,32 @@ def state_from_restart(arrays: dict, gami: float) -> dict:
     st["tg"][:] = arrays["tgold"]
     st["rtg"][:] = arrays["rtgold"]
     return st
+
+
+def load_rank(directory, rank: int, params: dict, initial_state: dict | None = None):
+    """What the reference driver reads at start-up on MPI rank `rank`
+    (src/driver.f90:39-60): the partition mesh part.<rank+1>.dat (input),
+    step.dat (readStep), and for a step above 0 the restart
+    restart.<step>.<rank+1> (readSol) with the predictor of the first step
+    it resumes (driver.f90:83-85, applied by state_from_restart).  At step 0
+    the reference generates its initial condition (generateIC, a harness of
+    its own); here `initial_state` supplies it, zeros by default.  IBC starts
+    at zero: the setBCs producers fill it.  Returns (mesh.Case, step, time,
+    the PartMesh)."""
+    from pathlib import Path
+    d = Path(directory)
+    pm = read_part(d / part_name(rank + 1))
+    m = mesh_from_part(pm)
+    N = m.nnode
+    step, _x_inflow = read_step(d / "step.dat")
+    time = 0.0
+    if step > 0:
+        _, time, arrays = read_restart(d / restart_name(step, rank), N)
+        state = state_from_restart(arrays, params["gami"])
+    else:
+        state = M.empty_state(N)
+        for k, v in (initial_state or {}).items():
+            state[k][...] = v
+    ibc = np.zeros((N, 8), dtype=np.int32, order="F")
+    case = M.Case(f"part{rank + 1}", m, params, state, ibc, F.OVS_ASM_NSVOF)
+    return case, step, time, pm

@@ -161,3 +161,32 @@ def test_reference_file_names_and_step_file(tmp_path):
     # the list-directed record a Fortran compiler writes reads the same
     (tmp_path / "step2.dat").write_text("          17   1.2500000000000000D-01\n")
     assert refio.read_step(tmp_path / "step2.dat") == (17, 0.125)
+
+
+def test_load_rank_follows_the_driver_start_up(tmp_path):
+    """refio.load_rank reads what rank r of the reference reads at start-up:
+    part.<r+1>.dat, step.dat and restart.<step>.<r+1>, giving the state of
+    the first resumed step after the predictor; without step.dat it starts
+    at step 0 from the given initial state."""
+    case = M.quench_case(M.box_tet(3, 2, 4, 1.0, 1.0, 1.25), "load_rank")
+    m = case.mesh
+    refio.write_part(tmp_path / refio.part_name(2), refio.part_from_mesh(m))
+    rng = np.random.default_rng(4)
+    st = {k: rng.standard_normal(np.shape(v)) for k, v in case.state.items()}
+    # step 0: no step.dat, the caller's initial state
+    c0, step, time, pm = refio.load_rank(tmp_path, 1, case.params, {"tg": case.state["tg"]})
+    assert step == 0 and time == 0.0 and c0.name == "part2"
+    np.testing.assert_array_equal(c0.mesh.ien, m.ien)
+    np.testing.assert_array_equal(c0.state["tg"], case.state["tg"])
+    assert not c0.ibc.any()
+    # a restart at step 7
+    refio.write_restart(tmp_path / refio.restart_name(7, 1), 7, 0.007, st)
+    refio.write_step(tmp_path / "step.dat", 7, 0.0)
+    c7, step, time, _ = refio.load_rank(tmp_path, 1, case.params)
+    assert step == 7 and time == 0.007
+    g = case.params["gami"]
+    np.testing.assert_array_equal(c7.state["ugold"], st["ug"])          # writeSol's ug is readSol's ugold
+    np.testing.assert_array_equal(c7.state["ug"], st["ug"])             # predictor ug = ugold
+    np.testing.assert_allclose(c7.state["acg"], (g - 1.0) / g * st["acg"], rtol=1e-15)
+    np.testing.assert_array_equal(c7.state["tgold"], st["tgold"])       # writeSol writes Tgold
+    np.testing.assert_array_equal(c7.state["pg"], st["pg"])
