@@ -1260,3 +1260,26 @@ def test_ns_uniform_advection_matrix_closed_form(oracle):
                 assert abs(s["G"][k, d] - wg) <= 1e-11 * f2 * vol * gm * (1 + tauM * np.abs(t1).max())
                 assert abs(s["D1"][k, d] - wd) <= 1e-11 * f2 * vol * gm * (1 + tauM * np.abs(t1).max())
             assert abs(s["M"][k] - f2 * tauM * vol * lap) <= 1e-11 * f2 * tauM * vol * gm * gm
+
+
+def test_bottom_heat_flux_weights_closed_form():
+    """mesh.bottom_heat_flux_weights (the config-5 functional J = c . T): a
+    linear temperature T = t0 + a x + b y + g z has dT/dz = g on every bottom
+    tet, so J = kappa g (bottom area), with kappa = prop_interp(kappa_w,
+    kappa_a, phi) for a uniform phi; only bottom-touching tets' nodes carry
+    weight."""
+    lx, ly, lz = 1.2, 0.8, 0.5
+    case = M.quench_case(M.box_tet(4, 3, 2, lx, ly, lz), "flux")
+    p = case.params
+    x = case.mesh.xg
+    phi = 0.35
+    c = M.bottom_heat_flux_weights(case, np.full(case.mesh.nnode, phi))
+    t0, a, b, g = 310.0, 2.0, -3.0, 7.5
+    T = t0 + a * x[:, 0] + b * x[:, 1] + g * x[:, 2]
+    kap = p["kappaw"] * (1 - phi) + p["kappaa"] * phi
+    assert abs(c @ T - kap * g * lx * ly) <= 1e-12 * kap * abs(g) * lx * ly
+    # constants and in-plane gradients carry no flux
+    assert abs(c.sum()) <= 1e-12 * np.abs(c).max()
+    assert abs(c @ x[:, 0]) <= 1e-12 * np.abs(c).max() and abs(c @ x[:, 1]) <= 1e-12 * np.abs(c).max()
+    # weights only on the nodes of tets with a face on z = 0 (the bottom layer of nodes and one above)
+    assert np.all(c[x[:, 2] > lz / 2 + 1e-12] == 0.0)
