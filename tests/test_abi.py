@@ -101,3 +101,10 @@ def test_product_code_never_imports_the_oracle():
         head = bench[: m.start()]
         fn = re.findall(r"^def (\w+)\(", head, re.M)
         assert fn and ("cpu" in fn[-1] or "reference" in fn[-1] or "baseline" in fn[-1]), (fn[-1:], m.group(0))
+
+
+def test_integration_guide_lists_every_entry_point():
+    """Every entry point of include/ovs.h appears in INTEGRATION.md."""
+    doc = (ROOT / "INTEGRATION.md").read_text()
+    missing = [n for n in _declared() if n not in doc]
+    assert not missing, missing
