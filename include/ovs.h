@@ -269,6 +269,15 @@ int ovs_get_field(ovs_ctx* ctx, int field, double* host);
  * cfl (may be NULL) receives the largest element CFL number. */
 int ovs_assemble(ovs_ctx* ctx, int kernel, int tensor_flag, int precision,
                  double* cfl);
+/* ovs_assemble without the wait: the pass is queued on the context stream
+ * and the call returns; its status and CFL number are read by
+ * ovs_assemble_wait, which waits for every pass queued since the last wait
+ * and returns the status ovs_assemble would have (the first error in queue
+ * order, else OVS_WARN_NEG_DETJ if any pass warned) and the largest CFL.
+ * At most 16 passes between waits (OVS_ERR_STATE beyond).  Lets a caller
+ * queue the next step's copies (ovs_stage_fields) while a pass runs. */
+int ovs_assemble_async(ovs_ctx* ctx, int kernel, int tensor_flag, int precision);
+int ovs_assemble_wait(ovs_ctx* ctx, double* cfl);
 
 /* RHS of `system` in reference layout: NS -> RHSGu(N,3),RHSGp(N);
  * NSVOF -> additionally RHSGls(N); TEM -> RHSGtem(N).  Concatenated. */

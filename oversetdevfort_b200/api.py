@@ -224,6 +224,17 @@ class Context:
         self.last_status = F.check(st, "ovs_assemble")
         return cfl.value
 
+    def assemble_async(self, kernel: int, tensor_flag: int, precision: int = F.OVS_FP64):
+        """ovs_assemble_async: queue the pass and return at once."""
+        F.check(self.lib.ovs_assemble_async(self.h, kernel, tensor_flag, precision), "ovs_assemble_async")
+
+    def assemble_wait(self) -> float:
+        """ovs_assemble_wait: wait for the queued passes; raises on an error,
+        keeps a warning in last_status; returns the largest CFL number."""
+        cfl = C.c_double(0.0)
+        self.last_status = F.check(self.lib.ovs_assemble_wait(self.h, C.byref(cfl)), "ovs_assemble_wait")
+        return cfl.value
+
     def get_rhs(self, system: int, precision: int = F.OVS_FP64) -> np.ndarray:
         a = np.zeros((self.N, NF[system]), order="F")
         F.check(self.lib.ovs_get_rhs(self.h, system, precision, _dptr(a)), "ovs_get_rhs")

@@ -1336,6 +1336,13 @@ int ovs_assemble_impl(ovs_ctx* c, int kernel, int tensor_flag, int prec, double*
   if ((st = ovs_faces_assemble(c, kernel, prec, a.mat, a.vec))) return st;
   if (a.mat) S.have_mat = true;
   if (a.vec) S.have_rhs = true;
+  if (c->defer_status) {   // ovs_assemble_async: the status travels to a page-locked slot, read at the wait
+    const int k = c->async_n++;
+    OVS_CUDA_TRY(cudaMemcpyAsync(c->h_async_flags + 4 * k, c->flags, sizeof(int) * 4, cudaMemcpyDeviceToHost, s));
+    OVS_CUDA_TRY(cudaMemcpyAsync(c->h_async_cfl + k, c->cfl_bits, sizeof(unsigned long long), cudaMemcpyDeviceToHost,
+                                 s));
+    return OVS_OK;
+  }
   int hflags[4];
   unsigned long long hcfl = 0;
   OVS_CUDA_TRY(cudaMemcpyAsync(hflags, c->flags, sizeof(hflags), cudaMemcpyDeviceToHost, s));

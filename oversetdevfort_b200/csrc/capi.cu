@@ -270,6 +270,8 @@ int ovs_destroy(ovs_ctx* c) {
   }
   if (c->h_pinned) cudaFreeHost(c->h_pinned);
   if (c->h_pinned_d) cudaFreeHost(c->h_pinned_d);
+  if (c->h_async_flags) cudaFreeHost(c->h_async_flags);
+  if (c->h_async_cfl) cudaFreeHost(c->h_async_cfl);
   if (c->ev0) cudaEventDestroy(c->ev0);
   if (c->ev1) cudaEventDestroy(c->ev1);
   if (c->stream) cudaStreamDestroy(c->stream);
@@ -432,6 +434,43 @@ int ovs_assemble(ovs_ctx* c, int kernel, int tensor_flag, int precision, double*
   OVS_CUDA_TRY(cudaEventElapsedTime(&ms, c->ev0, c->ev1));
   c->last_ms = ms;
   return st;
+}
+
+int ovs_assemble_async(ovs_ctx* c, int kernel, int tensor_flag, int precision) {
+  if (!c) return OVS_ERR_ARG;
+  if ((tensor_flag & (OVS_TENSOR_VEC | OVS_TENSOR_MAT)) == 0) return OVS_ERR_ARG;
+  int st;
+  if ((st = ovs_activate(c))) return st;
+  if (c->async_n >= OVS_ASYNC_SLOTS) return OVS_ERR_STATE;   // ovs_assemble_wait first
+  if (!c->h_async_flags) {
+    OVS_CUDA_TRY(cudaMallocHost(&c->h_async_flags, sizeof(int) * 4 * OVS_ASYNC_SLOTS));
+    OVS_CUDA_TRY(cudaMallocHost(&c->h_async_cfl, sizeof(unsigned long long) * OVS_ASYNC_SLOTS));
+  }
+  c->defer_status = true;
+  st = ovs_assemble_impl(c, kernel, tensor_flag, precision, nullptr);
+  c->defer_status = false;
+  return st;
+}
+
+int ovs_assemble_wait(ovs_ctx* c, double* cfl) {
+  if (!c) return OVS_ERR_ARG;
+  int st;
+  if ((st = ovs_activate(c))) return st;
+  OVS_CUDA_TRY(cudaStreamSynchronize(c->stream));
+  int err = OVS_OK, warn = OVS_OK;
+  double mx = 0.0;
+  for (int k = 0; k < c->async_n; ++k) {   // the status ovs_assemble would have returned, per pass
+    const int* f = c->h_async_flags + 4 * k;
+    const int s1 = f[3] ? OVS_ERR_PATTERN : f[2] ? OVS_ERR_TIMEOUT : f[1] ? OVS_ERR_NONFINITE : OVS_OK;
+    if (s1 && !err) err = s1;
+    if (f[0]) warn = OVS_WARN_NEG_DETJ;
+    double v;
+    memcpy(&v, c->h_async_cfl + k, sizeof(v));
+    if (v > mx) mx = v;
+  }
+  c->async_n = 0;
+  if (cfl) *cfl = mx;
+  return err ? err : warn;
 }
 
 static int sys_ok(ovs_ctx* c, int sys, int prec) {

@@ -9,6 +9,7 @@
 
 #define OVS_MAX_DEG 128        // longest CSR row supported (27*nshl hex bound = 216 not needed)
 #define OVS_MAX_KSPACE 400     // largest Krylov space
+#define OVS_ASYNC_SLOTS 16     // assembly passes ovs_assemble_async queues before a wait
 #define OVS_RED_BLOCKS 592     // fixed grid of every deterministic reduction (4 x 148 SMs)
 #define OVS_RED_THREADS 256
 #define OVS_COOP_MAX_BLOCKS 4096  // largest cooperative grid of the Arnoldi kernel
@@ -147,6 +148,12 @@ struct ovs_ctx {
   // pinned host mirror
   int* h_pinned = nullptr;
   double* h_pinned_d = nullptr;
+  // ovs_assemble_async: status words and CFL bits of the queued passes, read
+  // by ovs_assemble_wait (page-locked, OVS_ASYNC_SLOTS entries)
+  bool defer_status = false;
+  int async_n = 0;
+  int* h_async_flags = nullptr;
+  unsigned long long* h_async_cfl = nullptr;
   ovs_params params{};
   bool have_mesh = false, have_pattern = false, have_params = false;
   long long launches = 0;                // kernels launched by this context

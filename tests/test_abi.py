@@ -46,6 +46,8 @@ def test_create_argument_errors(lib):
     bad = F.OvsDims(10, 10, 5, 0)
     assert lib.ovs_create(ctypes.byref(h), ctypes.byref(bad)) == F.OVS_ERR_ARG
     assert lib.ovs_destroy(None) == 0
+    assert lib.ovs_assemble_async(None, F.OVS_ASM_NSVOF, 6, F.OVS_FP32) == F.OVS_ERR_ARG
+    assert lib.ovs_assemble_wait(None, None) == F.OVS_ERR_ARG
 
 
 def test_params_struct_layout():
