@@ -377,25 +377,25 @@ class ContextPartition:
     def apply_bcs(self):
         self.ctx.apply_bcs(3)
 
-    def assemble(self, tensor_flag: int, field_flag: int):
+    def assemble(self, tensor_flag: int, field_flag: int, precision: int = F.OVS_FP64):
         if field_flag & (FIELD_NS | FIELD_VOF):
-            self.ctx.assemble(F.OVS_ASM_NSVOF, tensor_flag, F.OVS_FP64)
+            self.ctx.assemble(F.OVS_ASM_NSVOF, tensor_flag, precision)
         if field_flag & FIELD_TEM:
-            self.ctx.assemble(F.OVS_ASM_TEM, tensor_flag, F.OVS_FP64)
+            self.ctx.assemble(F.OVS_ASM_TEM, tensor_flag, precision)
 
-    def residual_sq(self) -> np.ndarray:
+    def residual_sq(self, precision: int = F.OVS_FP64) -> np.ndarray:
         o = self.owned
-        f = self.ctx.get_rhs(F.OVS_SYS_NSVOF)[o]
-        t = self.ctx.get_rhs(F.OVS_SYS_TEM)[o]
+        f = self.ctx.get_rhs(F.OVS_SYS_NSVOF, precision)[o]
+        t = self.ctx.get_rhs(F.OVS_SYS_TEM, precision)[o]
         return np.array([np.sum(f[:, :3] ** 2), np.sum(f[:, 3] ** 2), np.sum(f[:, 4] ** 2), np.sum(t ** 2)])
 
-    def rhs(self, kind: str):
+    def rhs(self, kind: str, precision: int = F.OVS_FP64):
         import torch
-        r = self.ctx.get_rhs(_KIND_SYS[kind])
+        r = self.ctx.get_rhs(_KIND_SYS[kind], precision)
         return torch.as_tensor(np.ascontiguousarray(r.T), device=self.device)
 
-    def operator(self, kind: str):
-        return DeviceOperator(self.ctx, _KIND_SYS[kind])
+    def operator(self, kind: str, precision: int = F.OVS_FP64):
+        return DeviceOperator(self.ctx, _KIND_SYS[kind], precision)
 
     def update(self, kind: str, sol):
         self.ctx.set_solution(_KIND_SYS[kind], sol.contiguous())
@@ -410,7 +410,8 @@ class ContextPartition:
 
 def quench_newton(comm, parts: dict, newton_max: int = 3, solve_tem: bool = True, kspace: int = 50,
                   kspace_min: int = 1, tol_ns: float = 1e-6, tol_tem: float = 1e-6, utol=(1e-3,) * 4,
-                  atol=(1e-15,) * 4, orthog: str = "mgs", bcs: bool = False) -> dict:
+                  atol=(1e-15,) * 4, orthog: str = "mgs", bcs: bool = False, mode: int = F.OVS_FP64,
+                  max_cycles: int = 100) -> dict:
     """The Newton loop of one quench time step over owner-computes partitions:
     solmultiphasethermofluid_stag (src/solveFlow.f90:4-164) as the reference
     runs it on several ranks.  `parts[r]` is part r's local system
@@ -432,11 +433,21 @@ def quench_newton(comm, parts: dict, newton_max: int = 3, solve_tem: bool = True
     sum per evaluation, as calculate_residual's MPI_ALLREDUCE (:169-187).
     The loop body runs at least once.  The returned dict has iterations,
     converged, field_converged, residual0, residual and the Krylov
-    iterations of both systems."""
+    iterations of both systems.
+
+    mode OVS_FP32 is ovs_quench_newton's mixed mode over the partitions:
+    FP32 assembly, residuals from the FP32 right-hand sides, and each solve
+    by `solve_refined` on the FP32 operators to the relative residual tol_ns
+    / tol_tem (max_cycles refinement cycles) instead of one FP64 cycle.  The
+    parts then take a precision argument in assemble, residual_sq, rhs and
+    operator, and their operators provide `apply`."""
     P = comm.parts()
+    mixed = mode == F.OVS_FP32
+    prec = F.OVS_FP32 if mixed else F.OVS_FP64
+    pk = {"precision": prec} if mixed else {}
 
     def residual():
-        return np.asarray(comm.allreduce_vec([np.asarray(parts[r].residual_sq(), dtype=np.float64) for r in P]))
+        return np.asarray(comm.allreduce_vec([np.asarray(parts[r].residual_sq(**pk), dtype=np.float64) for r in P]))
 
     def set_bcs():
         if bcs:
@@ -444,9 +455,12 @@ def quench_newton(comm, parts: dict, newton_max: int = 3, solve_tem: bool = True
                 parts[r].apply_bcs()
 
     def solve(kind, tol):
-        rhs = {r: parts[r].rhs(kind) for r in P}
-        ops = {r: parts[r].operator(kind) for r in P}
-        sol, info = gmres_cycle(comm, ops, rhs, tol, kspace, kspace_min, tem=kind == "tem", orthog=orthog)
+        rhs = {r: parts[r].rhs(kind, **pk) for r in P}
+        ops = {r: parts[r].operator(kind, **pk) for r in P}
+        if mixed:
+            sol, info = solve_refined(comm, ops, ops, rhs, tol, kspace, max_cycles, tem=kind == "tem", orthog=orthog)
+        else:
+            sol, info = gmres_cycle(comm, ops, rhs, tol, kspace, kspace_min, tem=kind == "tem", orthog=orthog)
         for r in P:
             parts[r].update(kind, sol[r])
         return info["iterations"]
@@ -456,7 +470,7 @@ def quench_newton(comm, parts: dict, newton_max: int = 3, solve_tem: bool = True
 
     set_bcs()
     for r in P:
-        parts[r].assemble(F.OVS_TENSOR_VEC, FIELD_NS | FIELD_VOF | FIELD_TEM)
+        parts[r].assemble(F.OVS_TENSOR_VEC, FIELD_NS | FIELD_VOF | FIELD_TEM, **pk)
     r0 = residual()
     res = r0.copy()
     fc = check(res, r0)
@@ -465,14 +479,14 @@ def quench_newton(comm, parts: dict, newton_max: int = 3, solve_tem: bool = True
     for it in range(1, newton_max + 1):
         set_bcs()
         for r in P:
-            parts[r].assemble(F.OVS_TENSOR_MAT | F.OVS_TENSOR_VEC, FIELD_NS | FIELD_VOF)
+            parts[r].assemble(F.OVS_TENSOR_MAT | F.OVS_TENSOR_VEC, FIELD_NS | FIELD_VOF, **pk)
         out["krylov_iterations_ns"] += solve("nsvof", tol_ns)
         if solve_tem:
             for r in P:
-                parts[r].assemble(F.OVS_TENSOR_MAT | F.OVS_TENSOR_VEC, FIELD_TEM)
+                parts[r].assemble(F.OVS_TENSOR_MAT | F.OVS_TENSOR_VEC, FIELD_TEM, **pk)
             out["krylov_iterations_tem"] += solve("tem", tol_tem)
         for r in P:
-            parts[r].assemble(F.OVS_TENSOR_VEC, FIELD_NS | FIELD_VOF | FIELD_TEM)
+            parts[r].assemble(F.OVS_TENSOR_VEC, FIELD_NS | FIELD_VOF | FIELD_TEM, **pk)
         res = residual()
         fc = check(res, r0)
         out.update(iterations=it, converged=all(fc), field_converged=fc)

@@ -537,3 +537,58 @@ def test_two_gloo_ranks_refined_solve(oracle):
         p.join(timeout=120)
         assert p.exitcode == 0
     assert ok
+
+
+_ROUND32 = ("K11", "G", "D1", "M", "LS", "LSU", "ULS", "PLS", "TEM", "rhsu", "rhsp", "rhsls", "rhstem")
+
+
+class OracleMixedPartition(OraclePartition):
+    """OraclePartition with a precision argument: FP32 assembly emulated by
+    rounding the assembled matrix and right-hand sides to FP32."""
+
+    def assemble(self, tensor_flag, field_flag, precision=F.OVS_FP64):
+        self.oc.assemble_quenching(tensor_flag, field_flag)
+        if precision == F.OVS_FP32:
+            for k in _ROUND32:
+                a = self.oc.sys[k]
+                a[...] = a.astype(np.float32).astype(np.float64)
+
+    def residual_sq(self, precision=F.OVS_FP64):
+        return super().residual_sq()
+
+    def rhs(self, kind, precision=F.OVS_FP64):
+        return super().rhs(kind)
+
+    def operator(self, kind, precision=F.OVS_FP64):
+        return OracleApply(self.oc, kind)
+
+
+def test_partitioned_newton_mixed_mode(oracle):
+    """quench_newton(mode=OVS_FP32): FP32 assembly and refined solves to
+    tol_ns / tol_tem over the partitions.  Three parts follow one part
+    (Newton and Krylov iterations equal, state to 1e-10), take the Newton
+    iterations of the FP64 one-domain loop, and end within 1e-4 of its state
+    (FP32 rounding of the system: measured 2.2e-5 for u)."""
+    case = _stirred_case()
+    og, ref = _one_domain_newton(oracle, case)
+    runs = {}
+    for nparts in (1, 3):
+        parts = P.make_parts(case.mesh, nparts)
+        plan = D.halo_plan(parts)
+        ocs = {r: oracle.OracleCase(P.local_case(case, p)) for r, p in enumerate(parts)}
+        sp = {r: OracleMixedPartition(ocs[r], plan.owned[r]) for r in ocs}
+        with np.errstate(divide="ignore", invalid="ignore"):
+            out = D.quench_newton(D.LocalComm(plan), sp, mode=F.OVS_FP32, max_cycles=40, **NEWTON)
+        runs[nparts] = (out, ocs, parts)
+    (o1, oc1, _), (o3, oc3, p3) = runs[1], runs[3]
+    assert o1["converged"] and o1["iterations"] == ref["iterations"]
+    assert (o3["iterations"], o3["krylov_iterations_ns"], o3["krylov_iterations_tem"]) == \
+        (o1["iterations"], o1["krylov_iterations_ns"], o1["krylov_iterations_tem"])
+    assert o3["residual"][0] < 1e-3 * o3["residual0"][0]
+    for name in ("ug", "pg", "phig", "tg"):
+        g1, g = oc1[0].state_arrays[name], og.state_arrays[name]
+        scale = np.abs(g).max()
+        np.testing.assert_allclose(g1, g, rtol=0, atol=1e-4 * scale, err_msg=name)
+        for r, p in enumerate(p3):
+            np.testing.assert_allclose(oc3[r].state_arrays[name], g1[p.nodes], rtol=0, atol=1e-10 * scale,
+                                       err_msg=name)
