@@ -1098,8 +1098,9 @@ def test_phase_change_terms_at_rest_closed_form(oracle, T, phi):
     assert (dmdphi == 0.0) == (phi > 1.0)
 
 
-@pytest.mark.parametrize("lsc_kdc, tem_kdc, rphi", [(0.0, 0.0, 0.0), (0.3, 0.2, 0.4)])
-def test_uniform_advection_element_matrices_closed_form(oracle, lsc_kdc, tem_kdc, rphi):
+@pytest.mark.parametrize("lsc_kdc, tem_kdc, rphi, blend", [(0.0, 0.0, 0.0, False), (0.3, 0.2, 0.4, False),
+                                                            (0.3, 0.2, 0.4, True)])
+def test_uniform_advection_element_matrices_closed_form(oracle, lsc_kdc, tem_kdc, rphi, blend):
     """Both quench routines on one tet with a uniform velocity u relative to
     the fixed mesh (shconv_a = u.gN_a constant), uniform phi = 0.3, uniform
     T below Ts, T rate 1.5, gravity on, no phase change: every convection,
@@ -1120,18 +1121,27 @@ def test_uniform_advection_element_matrices_closed_form(oracle, lsc_kdc, tem_kdc
     With the discontinuity-capturing constants on (:419-423, :795-801) and a
     phi rate: k_dc_phi = LSC_kdc |rphi| / |G|_F adds f2 k_dc_phi |T| lap to
     LS, k_dc_T = TEM_kdc |rhocp rT| / |G|_F / Tref adds f2 k_dc_T |T| lap to
-    TEM, and RHSphi = -rphi (|T|/4 + tau_LS sc_a |T|)."""
+    TEM, and RHSphi = -rphi (|T|/4 + tau_LS sc_a |T|).
+    With `blend`, the old and new nodal values differ and the values above
+    are the alpha-stage ones of src/solveQuenching.f90:26-37 (u, phi, T with
+    alfi; acceleration, phi and T rates with almi), with a nonzero
+    acceleration a: uprime = tau_M rho (g - a), RHSu = rho (g - a) |T|/4 +
+    rho sc_a uprime |T|."""
     case, vol = _single_tet_case(1.0)
     p = case.params
     p.update(rhow=3.0, rhoa=1.2, muw=0.02, mua=0.004, delt=0.01, lsc_kdc=lsc_kdc, tem_kdc=tem_kdc, tref=2.0)
     u = np.array([0.3, -0.2, 0.5])
+    acc = np.array([0.5, -1.0, 2.0]) if blend else np.zeros(3)
     phi, T, rT = 0.3, 300.0, 1.5
     st = case.state
-    st["ug"][:] = u
-    st["ugold"][:] = u
-    for f, v in (("phig", phi), ("phigold", phi), ("tg", T), ("tgold", T), ("rtg", rT), ("rtgold", rT),
-                 ("rphig", rphi), ("rphigold", rphi)):
-        st[f][:] = v
+    af, am = p["alfi"], p["almi"]
+    # old values, and new ones whose alpha-stage blend is the value above
+    olds = {"ug": np.array([0.1, 0.2, -0.1]), "acg": np.array([-0.3, 0.4, 0.1]), "phig": 0.2, "rphig": -0.1,
+            "tg": 320.0, "rtg": 0.7} if blend else {"ug": u, "acg": acc, "phig": phi, "rphig": rphi, "tg": T, "rtg": rT}
+    for name, val, alpha in (("ug", u, af), ("acg", acc, am), ("phig", phi, af), ("rphig", rphi, am), ("tg", T, af),
+                             ("rtg", rT, am)):
+        st[name + "old"][:] = olds[name]
+        st[name][:] = olds[name] + (val - olds[name]) / alpha
     oc = oracle.OracleCase(case)
     cfl_ns = oc.assemble_quenching(F.OVS_TENSOR_MAT | F.OVS_TENSOR_VEC, 3)
     ns = {k: oc.sys[k].copy() for k in ("K11", "G", "D1", "M", "LS", "LSU", "ULS", "PLS", "rhsu", "rhsp", "rhsls")}
@@ -1160,7 +1170,7 @@ def test_uniform_advection_element_matrices_closed_form(oracle, lsc_kdc, tem_kdc
     tauT = 1.0 / (rho * cp * np.sqrt(uGu + 4.0 / dt ** 2 + 12.0 * kk * kk * GG))
     sc = gN @ u
     g = np.asarray(p["gravvec"], dtype=float)
-    uprime = tauM * rho * g
+    uprime = tauM * rho * (g - acc)
     kdc_phi = lsc_kdc * abs(rphi) / np.sqrt(GG)
     kdc_T = tem_kdc * abs(rhocp * rT) / np.sqrt(GG) / p["tref"]
     assert abs(cfl_ns - dt * np.sqrt(uGu)) <= 1e-14 * cfl_ns
@@ -1201,8 +1211,8 @@ def test_uniform_advection_element_matrices_closed_form(oracle, lsc_kdc, tem_kdc
                   + f2 * (kap + kdc_T) * vol * gm * gm, ("TEM", a, b))
     for a in range(4):
         for c in range(3):
-            close(ns["rhsu"][a, c], rho * g[c] * vol / 4.0 + rho * sc[a] * uprime[c] * vol,
-                  rho * 9.81 * vol * (1 + tauM * rho * np.abs(sc).max()), ("rhsu", a, c))
+            close(ns["rhsu"][a, c], rho * (g[c] - acc[c]) * vol / 4.0 + rho * sc[a] * uprime[c] * vol,
+                  rho * 12.0 * vol * (1 + tauM * rho * np.abs(sc).max()), ("rhsu", a, c))
         close(ns["rhsp"][a], vol * gN[a] @ uprime, vol * gm * np.abs(uprime).max(), ("rhsp", a))
         close(ns["rhsls"][a], -rphi * (vol / 4.0 + tauLS * sc[a] * vol),
               vol * (abs(rphi) * (1 + tauLS * np.abs(sc).max()) + 1e-3), ("rhsphi", a))
