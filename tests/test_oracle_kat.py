@@ -1293,3 +1293,43 @@ def test_bottom_heat_flux_weights_closed_form():
     assert abs(c @ x[:, 0]) <= 1e-12 * np.abs(c).max() and abs(c @ x[:, 1]) <= 1e-12 * np.abs(c).max()
     # weights only on the nodes of tets with a face on z = 0 (the bottom layer of nodes and one above)
     assert np.all(c[x[:, 2] > lz / 2 + 1e-12] == 0.0)
+
+
+@pytest.mark.parametrize("routine", ["quench", "ns"])
+def test_assembly_uses_the_current_configuration(oracle, routine):
+    """The element routines evaluate the geometry at x + d_alpha, d_alpha =
+    dgold + alfi (dg - dgold) (src/solveQuenching.f90:30, src/eval_shape_FEM.f90:
+    31-36): assembling with a displacement field equals, bit for bit,
+    assembling on the displaced coordinates with no displacement."""
+    case = M.random_case(nx=3, ny=3, nz=2, seed=21)
+    rng = np.random.default_rng(2)
+    x = np.asarray(case.mesh.xg)
+    S = 0.05 * rng.standard_normal((3, 3))
+    dgold = np.asfortranarray(x @ S.T)
+    dg = np.asfortranarray(dgold + 0.01 * rng.standard_normal(x.shape))
+    p = case.params
+    d_alpha = dgold + p["alfi"] * (dg - dgold)
+    moved = M.Case(case.name, M.Mesh(np.asfortranarray(x + d_alpha), case.mesh.ien, case.mesh.elm_id,
+                                     case.mesh.faces, case.mesh.dims, case.mesh.lengths),
+                   p, {k: v.copy() for k, v in case.state.items()}, case.ibc, case.kernel)
+    case.state["dg"][:] = dg
+    case.state["dgold"][:] = dgold
+    moved.state["dg"][:] = 0.0
+    moved.state["dgold"][:] = 0.0
+    out = []
+    for c in (case, moved):
+        oc = oracle.OracleCase(c)
+        if routine == "ns":
+            oc.assemble_navsto(6)
+            keys = ("K11", "G", "D1", "M", "rhsu", "rhsp")
+            out.append({k: oc.sys[k].copy() for k in keys})
+        else:
+            oc.assemble_quenching(6, 3)
+            d = {k: oc.sys[k].copy() for k in ("K11", "G", "D1", "M", "LS", "LSU", "ULS", "PLS", "rhsu", "rhsp",
+                                               "rhsls")}
+            oc.assemble_quenching(6, 4)
+            d.update(TEM=oc.sys["TEM"].copy(), rhstem=oc.sys["rhstem"].copy())
+            out.append(d)
+    assert np.abs(d_alpha).max() > 1e-3
+    for k in out[0]:
+        np.testing.assert_array_equal(out[0][k], out[1][k], err_msg=k)
