@@ -1333,3 +1333,25 @@ def test_assembly_uses_the_current_configuration(oracle, routine):
     assert np.abs(d_alpha).max() > 1e-3
     for k in out[0]:
         np.testing.assert_array_equal(out[0][k], out[1][k], err_msg=k)
+
+
+def test_solid_elements_carry_no_flow_terms(oracle):
+    """ELM_ID != 102 is solid: the NS+VOF routine adds nothing for it, matrix
+    or residual (src/solveQuenching.f90:250, 434, 496), while the temperature
+    routine assembles its solid conduction (tested in closed form above)."""
+    case, vol = _single_tet_case(2.0)
+    case.mesh.elm_id[:] = 103
+    st = case.state
+    st["ug"][:] = np.array([0.3, -0.1, 0.2])
+    st["acg"][:] = 1.0
+    for f in ("phig", "phigold"):
+        st[f][:] = 0.4
+    for f in ("tg", "tgold"):
+        st[f][:] = 350.0
+    oc = oracle.OracleCase(case)
+    oc.assemble_quenching(F.OVS_TENSOR_MAT | F.OVS_TENSOR_VEC, 3)
+    for k in ("K11", "G", "D1", "M", "LS", "LSU", "ULS", "PLS", "rhsu", "rhsp", "rhsls"):
+        assert not np.any(oc.sys[k]), k
+    oc.assemble_quenching(F.OVS_TENSOR_MAT | F.OVS_TENSOR_VEC, 4)
+    diag = [k for i in range(4) for k in range(oc.col[i] - 1, oc.col[i + 1] - 1) if oc.row[k] == i + 1]
+    assert np.all(oc.sys["TEM"][diag] > 0.0)
