@@ -1355,3 +1355,72 @@ def test_solid_elements_carry_no_flow_terms(oracle):
     oc.assemble_quenching(F.OVS_TENSOR_MAT | F.OVS_TENSOR_VEC, 4)
     diag = [k for i in range(4) for k in range(oc.col[i] - 1, oc.col[i + 1] - 1) if oc.row[k] == i + 1]
     assert np.all(oc.sys["TEM"][diag] > 0.0)
+
+
+def test_quench_bc_masks_follow_bclhs_ns_conv(oracle):
+    """Element Dirichlet masks of the quench path, BCLhs_NS_conv
+    (src/BCLhs_3D.f90:278-428) with pressure at IBC column 4 and VOF at
+    column 5, checked on the assembled system:
+      velocity d at node i: row i of K(d,:), G(d), LSU(d) and column i of
+        K(:,d), D(d), LSU(d) are zero except the K(d,d) diagonal = number of
+        elements at i; RHSu(i,d) = 0.  As the template has it, ULS(d) of
+        row i is NOT cleared (a constrained velocity row keeps its phi
+        coupling), while LSU(d) of row i -- a phi row -- is;
+      pressure at i: row i of M, D, PLS and column i of G are zero, M
+        diagonal = count, RHSp(i) = 0;
+      VOF at i: row and column i of LS, row i of LSU, column i of PLS and
+        ULS are zero, LS diagonal = count, RHSphi(i) = 0."""
+    case = M.random_case(nx=4, ny=3, nz=3, seed=13, solid_frac=0.0, bc_frac=0.0)
+    m = case.mesh
+    N = m.nnode
+    rng = np.random.default_rng(1)
+    perm = rng.permutation(N)
+    vel, pre, vof = perm[:8], perm[8:14], perm[14:20]
+    ibc = np.zeros((N, 8), dtype=np.int32, order="F")
+    ibc[vel, 0:3] = 1
+    ibc[pre, 3] = 1
+    ibc[vof, 4] = 1
+    case.ibc = ibc
+    oc = oracle.OracleCase(case)
+    oc.assemble_quenching(F.OVS_TENSOR_MAT | F.OVS_TENSOR_VEC, 3)
+    s, col, row = oc.sys, oc.col, oc.row
+    cnt = np.bincount(np.asarray(m.ien).ravel() - 1, minlength=N)
+    rows_of = lambda i: range(col[i] - 1, col[i + 1] - 1)
+    r_of = np.repeat(np.arange(N), np.diff(col))          # row of every slot
+    c_of = row - 1                                        # column of every slot
+    for i in vel:
+        for k in rows_of(i):
+            diag = c_of[k] == i
+            for d in range(3):
+                for j in range(3):
+                    want = cnt[i] if (diag and j == d) else 0.0
+                    assert s["K11"][k, 3 * d + j] == want
+                assert s["G"][k, d] == 0.0 and s["LSU"][k, d] == 0.0
+        colk = np.nonzero(c_of == i)[0]
+        for d in range(3):
+            for c in range(3):
+                vals = s["K11"][colk, 3 * c + d]
+                assert np.all(vals[r_of[colk] != i] == 0.0)
+            assert np.all(s["D1"][colk, d] == 0.0) and np.all(s["LSU"][colk, d] == 0.0)
+        assert np.all(s["rhsu"][i] == 0.0)
+    # the template leaves ULS of constrained velocity rows in place
+    uls_rows = np.concatenate([np.abs(s["ULS"][list(rows_of(i))]).ravel() for i in vel])
+    assert uls_rows.max() > 0.0
+    for i in pre:
+        for k in rows_of(i):
+            assert s["M"][k] == (cnt[i] if c_of[k] == i else 0.0)
+            assert np.all(s["D1"][k] == 0.0) and s["PLS"][k] == 0.0
+        colk = np.nonzero(c_of == i)[0]
+        assert np.all(s["G"][colk] == 0.0)
+        assert s["rhsp"][i] == 0.0
+    for i in vof:
+        for k in rows_of(i):
+            assert s["LS"][k] == (cnt[i] if c_of[k] == i else 0.0)
+            assert np.all(s["LSU"][k] == 0.0)
+        colk = np.nonzero(c_of == i)[0]
+        assert np.all(s["LS"][colk][r_of[colk] != i] == 0.0)
+        assert np.all(s["PLS"][colk] == 0.0) and np.all(s["ULS"][colk] == 0.0)
+        assert s["rhsls"][i] == 0.0
+    # unconstrained phi rows do couple to velocity (the LSU clearing above is the BC's doing)
+    free = np.setdiff1d(np.arange(N), np.concatenate([vel, vof]))
+    assert np.abs(s["LSU"][np.isin(r_of, free)]).max() > 0.0
