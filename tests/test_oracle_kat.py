@@ -1424,3 +1424,30 @@ def test_quench_bc_masks_follow_bclhs_ns_conv(oracle):
     # unconstrained phi rows do couple to velocity (the LSU clearing above is the BC's doing)
     free = np.setdiff1d(np.arange(N), np.concatenate([vel, vof]))
     assert np.abs(s["LSU"][np.isin(r_of, free)]).max() > 0.0
+
+
+def test_temperature_bc_masks_follow_bclhs_tem(oracle):
+    """BCLhs_tem (src/BCLhs_3D.f90:247-274) on IBC column 6, assembled: row i
+    and column i of the temperature matrix are zero except the diagonal,
+    which counts the elements at i; RHStem(i) = 0; other rows keep their
+    entries."""
+    case = M.random_case(nx=4, ny=3, nz=3, seed=17, solid_frac=0.2, bc_frac=0.0)
+    m = case.mesh
+    N = m.nnode
+    tn = np.random.default_rng(3).permutation(N)[:10]
+    ibc = np.zeros((N, 8), dtype=np.int32, order="F")
+    ibc[tn, 5] = 1
+    case.ibc = ibc
+    oc = oracle.OracleCase(case)
+    oc.assemble_quenching(F.OVS_TENSOR_MAT | F.OVS_TENSOR_VEC, 4)
+    T, col, row = oc.sys["TEM"], oc.col, oc.row
+    cnt = np.bincount(np.asarray(m.ien).ravel() - 1, minlength=N)
+    r_of = np.repeat(np.arange(N), np.diff(col))
+    c_of = row - 1
+    for i in tn:
+        sel = (r_of == i) | (c_of == i)
+        diag = (r_of == i) & (c_of == i)
+        assert np.all(T[sel & ~diag] == 0.0) and T[diag][0] == cnt[i]
+        assert oc.sys["rhstem"][i] == 0.0
+    free = ~np.isin(r_of, tn) & ~np.isin(c_of, tn)
+    assert np.all(T[free & (r_of == c_of)] > 0.0)
