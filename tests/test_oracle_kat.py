@@ -1451,3 +1451,42 @@ def test_temperature_bc_masks_follow_bclhs_tem(oracle):
         assert oc.sys["rhstem"][i] == 0.0
     free = ~np.isin(r_of, tn) & ~np.isin(c_of, tn)
     assert np.all(T[free & (r_of == c_of)] > 0.0)
+
+
+def test_ns_bc_masks_follow_bclhs_3d(oracle):
+    """BCLhs_3D (src/BCLhs_3D.f90:4-122) on the NS-only path, assembled:
+    velocity d at node i clears row i of K(d,:) and G(d) and column i of
+    K(:,d) and D(d), the K(d,d) diagonal counting the elements at i;
+    pressure (IBC column 4) clears row i of M and D and column i of G, the
+    M diagonal counting the elements; the constrained RHS entries are 0."""
+    case = M.random_case(nx=4, ny=3, nz=3, seed=19, kernel=F.OVS_ASM_NS, solid_frac=0.0, bc_frac=0.0)
+    m = case.mesh
+    N = m.nnode
+    perm = np.random.default_rng(4).permutation(N)
+    vel, pre = perm[:8], perm[8:14]
+    ibc = np.zeros((N, 8), dtype=np.int32, order="F")
+    ibc[vel, 0:3] = 1
+    ibc[pre, 3] = 1
+    case.ibc = ibc
+    oc = oracle.OracleCase(case)
+    oc.assemble_navsto(F.OVS_TENSOR_MAT | F.OVS_TENSOR_VEC)
+    s, col, row = oc.sys, oc.col, oc.row
+    cnt = np.bincount(np.asarray(m.ien).ravel() - 1, minlength=N)
+    r_of = np.repeat(np.arange(N), np.diff(col))
+    c_of = row - 1
+    for i in vel:
+        ri, ci = r_of == i, c_of == i
+        for d in range(3):
+            for j in range(3):
+                v = s["K11"][ri, 3 * d + j]
+                assert np.all(v[~(ci[ri] & (j == d))] == 0.0)
+                w = s["K11"][ci, 3 * j + d]
+                assert np.all(w[r_of[ci] != i] == 0.0)
+            assert s["K11"][ri & ci, 4 * d][0] == cnt[i]
+            assert np.all(s["G"][ri, d] == 0.0) and np.all(s["D1"][ci, d] == 0.0)
+        assert np.all(s["rhsu"][i] == 0.0)
+    for i in pre:
+        ri, ci = r_of == i, c_of == i
+        assert np.all(s["M"][ri & ~ci] == 0.0) and s["M"][ri & ci][0] == cnt[i]
+        assert np.all(s["D1"][ri] == 0.0) and np.all(s["G"][ci] == 0.0)
+        assert s["rhsp"][i] == 0.0
