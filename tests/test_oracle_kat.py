@@ -1490,3 +1490,40 @@ def test_ns_bc_masks_follow_bclhs_3d(oracle):
         assert np.all(s["M"][ri & ~ci] == 0.0) and s["M"][ri & ci][0] == cnt[i]
         assert np.all(s["D1"][ri] == 0.0) and np.all(s["G"][ci] == 0.0)
         assert s["rhsp"][i] == 0.0
+
+
+def test_scatter_is_the_sum_of_element_assemblies(oracle):
+    """FillSparseMat / LocaltoGlobal through SparseMatLoc_3D (src/
+    FillSparseMat.f90:4-67, 237-288; src/LocaltoGlobal.f90:26-51): the
+    assembled matrix and RHS equal the sum, entry by entry over (row,
+    column) pairs, of the same case assembled one element at a time (each a
+    one-element mesh over the same nodes), BC masks included -- every
+    element contributes its own unit diagonal at a constrained dof."""
+    case = M.random_case(nx=3, ny=2, nz=2, seed=23, bc_frac=0.2)
+    m = case.mesh
+    N, E = m.nnode, m.nelem
+    oc = oracle.OracleCase(case)
+    oc.assemble_quenching(F.OVS_TENSOR_MAT | F.OVS_TENSOR_VEC, 3)
+    r_of = np.repeat(np.arange(N), np.diff(oc.col))
+    slot = {(int(r), int(c) - 1): k for k, (r, c) in enumerate(zip(r_of, oc.row))}
+    keys = ("K11", "G", "D1", "M", "LS", "LSU", "ULS", "PLS")
+    acc = {k: np.zeros_like(oc.sys[k]) for k in keys}
+    rhs = {k: np.zeros_like(oc.sys[k]) for k in ("rhsu", "rhsp", "rhsls")}
+    for e in range(E):
+        me = M.Mesh(m.xg, np.asfortranarray(m.ien[e:e + 1]), m.elm_id[e:e + 1].copy(), m.faces, m.dims, m.lengths)
+        ce = M.Case(case.name, me, case.params, case.state, case.ibc, case.kernel)
+        oe = oracle.OracleCase(ce)
+        oe.assemble_quenching(F.OVS_TENSOR_MAT | F.OVS_TENSOR_VEC, 3)
+        re_of = np.repeat(np.arange(N), np.diff(oe.col))
+        for ke, (r, c) in enumerate(zip(re_of, oe.row)):
+            k = slot[(int(r), int(c) - 1)]
+            for name in keys:
+                acc[name][k] += oe.sys[name][ke]
+        for name in rhs:
+            rhs[name] += oe.sys[name]
+    for name in keys:
+        scale = max(np.abs(oc.sys[name]).max(), 1e-300)
+        np.testing.assert_allclose(acc[name], oc.sys[name], rtol=0, atol=1e-13 * scale, err_msg=name)
+    for name in rhs:
+        scale = max(np.abs(oc.sys[name]).max(), 1e-300)
+        np.testing.assert_allclose(rhs[name], oc.sys[name], rtol=0, atol=1e-13 * scale, err_msg=name)
