@@ -1527,3 +1527,44 @@ def test_scatter_is_the_sum_of_element_assemblies(oracle):
     for name in rhs:
         scale = max(np.abs(oc.sys[name]).max(), 1e-300)
         np.testing.assert_allclose(rhs[name], oc.sys[name], rtol=0, atol=1e-13 * scale, err_msg=name)
+
+
+def test_spmv_block_structure(oracle):
+    """SparseProd_NS_conv / SparseProdUP_3D / SparseProd_LS (src/SparseProd.f90:
+    4-60, 128-242) against a dense product built here from the CSR blocks:
+    u rows take K11 (row component i, column component j at (i-1)*3+j), ULS
+    and G; p rows take D1, PLS and M; phi rows take LSU and LS and no
+    pressure; the (u, p) product drops the phi blocks; the scalar product
+    uses the temperature values."""
+    case = M.random_case(nx=3, ny=2, nz=2, seed=29)
+    oc = oracle.OracleCase(case)
+    N, K = oc.N, oc.icnt
+    rng = np.random.default_rng(8)
+    blocks = {"K11": rng.standard_normal((K, 9)), "G": rng.standard_normal((K, 3)), "D1": rng.standard_normal((K, 3)),
+              "M": rng.standard_normal(K), "LS": rng.standard_normal(K), "LSU": rng.standard_normal((K, 3)),
+              "ULS": rng.standard_normal((K, 3)), "PLS": rng.standard_normal(K)}
+    oc.load_system("nsvof", {**blocks, "rhs": np.zeros((N, 5))})
+    oc.load_system("tem", {"TEM": rng.standard_normal(K), "rhs": np.zeros((N, 1))})
+    r_of = np.repeat(np.arange(N), np.diff(oc.col))
+    c_of = oc.row - 1
+    A = np.zeros((5 * N, 5 * N))          # field-major unknowns: u1, u2, u3, p, phi
+    for k in range(K):
+        r, c = r_of[k], c_of[k]
+        for i in range(3):
+            for j in range(3):
+                A[i * N + r, j * N + c] += blocks["K11"][k, 3 * i + j]
+            A[i * N + r, 3 * N + c] += blocks["G"][k, i]
+            A[i * N + r, 4 * N + c] += blocks["ULS"][k, i]
+            A[3 * N + r, i * N + c] += blocks["D1"][k, i]
+            A[4 * N + r, i * N + c] += blocks["LSU"][k, i]
+        A[3 * N + r, 3 * N + c] += blocks["M"][k]
+        A[3 * N + r, 4 * N + c] += blocks["PLS"][k]
+        A[4 * N + r, 4 * N + c] += blocks["LS"][k]
+    x = rng.standard_normal((N, 5))
+    want = (A @ x.T.reshape(-1)).reshape(5, N).T
+    np.testing.assert_allclose(oc.spmv("nsvof", x), want, rtol=0, atol=1e-12 * np.abs(want).max())
+    want_up = (A[:4 * N, :4 * N] @ x[:, :4].T.reshape(-1)).reshape(4, N).T
+    np.testing.assert_allclose(oc.spmv("ns", x[:, :4]), want_up, rtol=0, atol=1e-12 * np.abs(want_up).max())
+    T = np.zeros((N, N))
+    np.add.at(T, (r_of, c_of), oc.sys["TEM"])
+    np.testing.assert_allclose(oc.spmv("tem", x[:, :1])[:, 0], T @ x[:, 0], rtol=0, atol=1e-12 * np.abs(T).max() * 10)
