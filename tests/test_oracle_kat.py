@@ -1568,3 +1568,49 @@ def test_spmv_block_structure(oracle):
     T = np.zeros((N, N))
     np.add.at(T, (r_of, c_of), oc.sys["TEM"])
     np.testing.assert_allclose(oc.spmv("tem", x[:, :1])[:, 0], T @ x[:, 0], rtol=0, atol=1e-12 * np.abs(T).max() * 10)
+
+
+@pytest.mark.parametrize("kind", ["ns", "nsvof", "tem"])
+def test_gmres_preconditioner_rules(oracle, kind):
+    """The block-diagonal preconditioners of SparseGMRES_up (src/
+    SparseGMRES_NS.f90:74-121), SparseGMRES_ns_conv (src/SparseGMRES_NS_conv.f:
+    54-139) and SparseGMRES_tem (src/SparseGMRES_tem.f90:52-58), through the
+    cycle's first norm unorm = |P^-1 b|: the exact inverse of each 3x3
+    velocity block, 1/M with 1 where M = 0, 1/LS with 0 where LS = 0, and
+    1/diag with 1 where the temperature diagonal is 0; some diagonals are
+    planted at 0."""
+    case = M.random_case(nx=3, ny=2, nz=2, seed=31)
+    oc = oracle.OracleCase(case)
+    N, K = oc.N, oc.icnt
+    rng = np.random.default_rng(9)
+    r_of = np.repeat(np.arange(N), np.diff(oc.col))
+    dslot = np.array([k for k in range(K) if oc.row[k] - 1 == r_of[k]])
+    K11 = rng.standard_normal((K, 9))
+    K11[dslot] += 4.0 * np.array([1, 0, 0, 0, 1, 0, 0, 0, 1])   # regular velocity blocks
+    Mv, LS, TEM = rng.standard_normal(K), rng.standard_normal(K), rng.standard_normal(K)
+    zero = rng.permutation(N)[:5]
+    Mv[dslot[zero]] = 0.0
+    LS[dslot[zero[:3]]] = 0.0
+    TEM[dslot[zero[2:]]] = 0.0
+    b = rng.standard_normal((N, 5))
+    blocks = {"K11": K11, "G": rng.standard_normal((K, 3)), "D1": rng.standard_normal((K, 3)), "M": Mv, "LS": LS,
+              "LSU": rng.standard_normal((K, 3)), "ULS": rng.standard_normal((K, 3)), "PLS": rng.standard_normal(K)}
+    if kind == "tem":
+        oc.load_system("tem", {"TEM": TEM, "rhs": b[:, :1]})
+        t = TEM[dslot]
+        pb = np.where(t == 0.0, 1.0, 1.0 / np.where(t == 0.0, 1.0, t)) * b[:, 0]
+    else:
+        nf = 5 if kind == "nsvof" else 4
+        oc.load_system(kind, {**{k: v for k, v in blocks.items() if kind == "nsvof" or k in ("K11", "G", "D1", "M")},
+                              "rhs": b[:, :nf]})
+        pb = np.zeros((N, nf))
+        for i in range(N):
+            B = K11[dslot[i]].reshape(3, 3)
+            pb[i, :3] = np.linalg.solve(B, b[i, :3])
+            m = Mv[dslot[i]]
+            pb[i, 3] = b[i, 3] / m if m != 0.0 else b[i, 3]
+            if kind == "nsvof":
+                ls = LS[dslot[i]]
+                pb[i, 4] = b[i, 4] / ls if ls != 0.0 else 0.0
+    _, _, _, r0 = oc.gmres(kind, 1e-3, 1, 1)
+    assert abs(r0 - np.linalg.norm(pb)) <= 1e-12 * np.linalg.norm(pb)
