@@ -1614,3 +1614,22 @@ def test_gmres_preconditioner_rules(oracle, kind):
                 pb[i, 4] = b[i, 4] / ls if ls != 0.0 else 0.0
     _, _, _, r0 = oc.gmres(kind, 1e-3, 1, 1)
     assert abs(r0 - np.linalg.norm(pb)) <= 1e-12 * np.linalg.norm(pb)
+
+
+def test_gmres_exit_rule_and_single_cycle(oracle):
+    """The cycle's exit (src/SparseGMRES_NS.f90:327; SparseGMRES_tem.f90:219):
+    stop when |e(k+1)| <= tol |P^-1 b| AND k >= Kspace_mn -- a loose
+    tolerance still runs Kspace_mn iterations -- and no restart: a space too
+    small for the tolerance returns after Kspace iterations with its partial
+    solution, |e| above the target."""
+    case = M.quench_case(M.box_tet(4, 3, 5, 1.0, 1.0, 1.25), "exit")
+    oc = oracle.OracleCase(case)
+    oc.assemble_quenching(6, 3)
+    _, it_loose, er, r0 = oc.gmres("nsvof", 0.9, 50, 1)
+    assert it_loose >= 1 and er <= 0.9 * r0
+    _, it_min, er_min, _ = oc.gmres("nsvof", 0.9, 50, 7)
+    assert it_min == max(7, it_loose)
+    s_short, it_short, er_short, r0s = oc.gmres("nsvof", 1e-12, 3, 1)
+    assert it_short == 3 and er_short > 1e-12 * r0s and np.abs(s_short).max() > 0.0
+    _, it_long, er_long, _ = oc.gmres("nsvof", 1e-12, 300, 1)
+    assert it_long > 3 and er_long < er_short
