@@ -1633,3 +1633,20 @@ def test_gmres_exit_rule_and_single_cycle(oracle):
     assert it_short == 3 and er_short > 1e-12 * r0s and np.abs(s_short).max() > 0.0
     _, it_long, er_long, _ = oc.gmres("nsvof", 1e-12, 300, 1)
     assert it_long > 3 and er_long < er_short
+
+
+@pytest.mark.parametrize("dims, hexa, N, E, nnz", [
+    ((16, 16, 16), False, 4913, 24576, 66961),                  # config 1
+    ((48, 48, 96), False, 232897, 1327104, 3398977),           # config 2
+    ((128, 128, 128), False, 2146689, 12582912, 31802497),     # config 3 (the bench workload)
+    ((96, 96, 96), True, 912673, 884736, 24137569),            # config 4
+    ((32, 32, 32), False, 35937, 196608, 513313),              # config 5
+])
+def test_config_sizes(dims, hexa, N, E, nnz):
+    """The sizes of the five workloads (nodes, elements, CSR entries) from
+    the closed forms the pattern tests pin (Kuhn split: nodes + both
+    directions of every edge; hexahedra: the 27-point stencil)."""
+    nx, ny, nz = dims
+    assert (nx + 1) * (ny + 1) * (nz + 1) == N
+    assert (1 if hexa else 6) * nx * ny * nz == E
+    assert (M.expected_nnz_hex if hexa else M.expected_nnz_kuhn)(nx, ny, nz) == nnz
