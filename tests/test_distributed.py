@@ -592,3 +592,39 @@ def test_partitioned_newton_mixed_mode(oracle):
         for r, p in enumerate(p3):
             np.testing.assert_allclose(oc3[r].state_arrays[name], g1[p.nodes], rtol=0, atol=1e-10 * scale,
                                        err_msg=name)
+
+
+class OracleStepBcPartition(OracleStepPartition):
+    def __init__(self, oc, owned, spec):
+        super().__init__(oc, owned)
+        self.spec = spec
+
+    def apply_bcs(self):
+        self.oc.set_bcs(self.spec, 3)
+
+
+def test_partitioned_time_loop_with_bc_producers(oracle):
+    """quench_time_steps(bcs=True) over steps 0-2: three parts, each with its
+    own part of the setBCs input, follow the one-part run (iterations,
+    Krylov counts, state and old values to 1e-10, IBC equal)."""
+    case = _stirred_case()
+    m = case.mesh
+    spec = M.box_bc_spec(m, u={b: (0.0, 0.0, 0.0) for b in range(1, 6)}, phi={6: 1.0}, T={5: 300.0})
+    runs = {}
+    for nparts in (1, 3):
+        parts = P.make_parts(m, nparts)
+        plan = D.halo_plan(parts)
+        ocs = {r: oracle.OracleCase(P.local_case(case, p)) for r, p in enumerate(parts)}
+        sp = {r: OracleStepBcPartition(ocs[r], plan.owned[r], P.local_bc_spec(spec, parts[r])) for r in ocs}
+        with np.errstate(divide="ignore", invalid="ignore"):
+            last, kt = D.quench_time_steps(D.LocalComm(plan), sp, 0, 3, bcs=True, **NEWTON)
+        runs[nparts] = (last, kt, ocs, parts)
+    (l1, k1, o1, _), (l3, k3, o3, p3) = runs[1], runs[3]
+    assert k1 == k3 and l1["iterations"] == l3["iterations"] and np.isfinite(l1["residual"]).all()
+    g = o1[0].state_arrays
+    for r, p in enumerate(p3):
+        np.testing.assert_array_equal(o3[r].ibc, o1[0].ibc[p.nodes])
+        for name in ("ug", "acg", "pg", "phig", "tg", "ugold", "acgold"):
+            scale = max(np.abs(g[name]).max(), 1e-300)
+            np.testing.assert_allclose(o3[r].state_arrays[name], g[name][p.nodes], rtol=0, atol=1e-10 * scale,
+                                       err_msg=name)
