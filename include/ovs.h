@@ -219,6 +219,12 @@ int ovs_set_option(ovs_ctx* ctx, int option, int value);
  * active (face terms are not differentiated). */
 int ovs_set_faces(ovs_ctx* ctx, int nface, const int* f2e, const int* face_or,
                   const int* flags, const double* hconv, const double* tinf);
+/* The checks ovs_set_faces makes, without a context or a device, for a tet
+ * mesh of nelem elements: OVS_OK, or OVS_ERR_ARG for an owning element
+ * outside 1..nelem, a FACE_OR outside 1..4, an unknown flag bit, or a
+ * convective face without the hconv / tinf tables. */
+int ovs_check_faces(int nelem, int nface, const int* f2e, const int* face_or, const int* flags,
+                    const double* hconv, const double* tinf);
 
 /* Boundary data of setBCs_NSVOF / setBCs_Tem (src/setBCs.f90:172-278) as the
  * reference holds it: the node sets of the boundaries and the tables read by

@@ -540,3 +540,14 @@ def check_bc_spec(spec, nnode: int) -> int:
     OVS_ERR_ARG)."""
     keep, cs = spec.to_c()
     return int(F.load().ovs_check_bc_spec(C.byref(cs), int(nnode)))
+
+
+def check_faces(bf, nelem: int) -> int:
+    """ovs_check_faces: the checks of Context.set_faces for a face set
+    (mesh.BoundaryFaces) on a tet mesh of nelem elements, without a device.
+    Returns the status (OVS_OK or OVS_ERR_ARG)."""
+    f2e, fo, fl = (np.ascontiguousarray(a, dtype=np.int32) for a in (bf.f2e, bf.face_or, bf.flags))
+    hc, ti = (np.ascontiguousarray(a, dtype=np.float64) for a in (bf.hconv, bf.tinf))
+    n = int(f2e.size)
+    return int(F.load().ovs_check_faces(int(nelem), n, _iptr(f2e), _iptr(fo), _iptr(fl),
+                                        _dptr(hc) if hc.size else None, _dptr(ti) if ti.size else None))

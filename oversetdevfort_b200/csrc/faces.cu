@@ -410,21 +410,41 @@ void free_faces(ovs_ctx* c) {
 
 void ovs_faces_free(ovs_ctx* c) { free_faces(c); }
 
+namespace {
+// The per-face checks of a face set on a tet mesh of nelem elements: owning
+// elements in 1..nelem, FACE_OR in 1..4, known flag bits, and the convective
+// tables present when a face carries the convective term.
+int validate_faces(int nelem, int nface, const int* f2e, const int* face_or, const int* flags, const double* hconv,
+                   const double* tinf) {
+  if (nface > (1 << 28)) return OVS_ERR_ARG;
+  int all = 0;
+  for (int f = 0; f < nface; ++f) {
+    if (f2e[f] < 1 || f2e[f] > nelem || face_or[f] < 1 || face_or[f] > 4) return OVS_ERR_ARG;
+    if (flags[f] & ~(OVS_FACE_WEAK | OVS_FACE_CONVH)) return OVS_ERR_ARG;
+    all |= flags[f];
+  }
+  if ((all & OVS_FACE_CONVH) && (!hconv || !tinf)) return OVS_ERR_ARG;
+  return OVS_OK;
+}
+}  // namespace
+
+int ovs_check_faces(int nelem, int nface, const int* f2e, const int* face_or, const int* flags, const double* hconv,
+                    const double* tinf) {
+  if (nelem <= 0 || nface < 0) return OVS_ERR_ARG;
+  if (nface > 0 && (!f2e || !face_or || !flags)) return OVS_ERR_ARG;
+  return validate_faces(nelem, nface, f2e, face_or, flags, hconv, tinf);
+}
+
 int ovs_faces_set_impl(ovs_ctx* c, int nface, const int* f2e, const int* face_or, const int* flags,
                        const double* hconv, const double* tinf) {
   if (nface < 0) return OVS_ERR_ARG;
   if (nface > 0 && (!f2e || !face_or || !flags)) return OVS_ERR_ARG;
   if (nface > 0 && c->nshl != 4) return OVS_ERR_ARG;   // face rules exist for tets (and prisms) only
   if (nface > 0 && !c->have_mesh) return OVS_ERR_STATE;
-  if (nface > (1 << 28)) return OVS_ERR_ARG;
-  int all = 0;
-  for (int f = 0; f < nface; ++f) {
-    if (f2e[f] < 1 || f2e[f] > c->E || face_or[f] < 1 || face_or[f] > 4) return OVS_ERR_ARG;
-    if (flags[f] & ~(OVS_FACE_WEAK | OVS_FACE_CONVH)) return OVS_ERR_ARG;
-    all |= flags[f];
-  }
-  if ((all & OVS_FACE_CONVH) && (!hconv || !tinf)) return OVS_ERR_ARG;
   int st;
+  if ((st = validate_faces(c->E, nface, f2e, face_or, flags, hconv, tinf))) return st;
+  int all = 0;   // the face kinds present, for the assembly dispatch
+  for (int f = 0; f < nface; ++f) all |= flags[f];
   if ((st = ovs_activate(c))) return st;
   cudaStream_t s = c->stream;
   OVS_CUDA_TRY(cudaStreamSynchronize(s));

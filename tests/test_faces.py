@@ -207,3 +207,24 @@ def test_convective_face_matrix_is_its_residual_jacobian(oracle):
     oc.newton_update(F.OVS_SYS_TEM, np.asfortranarray(d[:, None]))
     oc.assemble_quenching(2, 4)
     np.testing.assert_allclose(oc.sys["rhstem"] - r0, -kd, rtol=0, atol=1e-11 * np.abs(kd).max())
+
+
+def test_face_set_checks_without_a_device(lib):
+    """ovs_check_faces, the checks ovs_set_faces makes, on the host: the box
+    face set passes; an owning element beyond the mesh, a FACE_OR of 5, an
+    unknown flag bit and convective faces without their tables are
+    rejected; an empty set passes."""
+    from oversetdevfort_b200 import api
+    m = M.box_tet(3, 2, 2)
+    bf = M.face_set(m, weak=(1, 6), convective={6: (5.0, 300.0)})
+    assert api.check_faces(bf, m.nelem) == F.OVS_OK
+    assert api.check_faces(bf, int(bf.f2e.max()) - 1) == F.OVS_ERR_ARG
+    for field, bad in (("face_or", 5), ("flags", 8)):
+        b2 = M.BoundaryFaces(*(np.array(getattr(bf, k), copy=True) for k in ("f2e", "face_or", "flags", "hconv", "tinf")))
+        getattr(b2, field)[0] = bad
+        assert api.check_faces(b2, m.nelem) == F.OVS_ERR_ARG, field
+    b3 = M.BoundaryFaces(bf.f2e, bf.face_or, bf.flags, np.zeros(0), np.zeros(0))
+    assert api.check_faces(b3, m.nelem) == F.OVS_ERR_ARG                # convective faces, no tables
+    z = np.zeros(0, dtype=np.int32)
+    assert api.check_faces(M.BoundaryFaces(z, z, z, np.zeros(0), np.zeros(0)), m.nelem) == F.OVS_OK
+    assert lib.ovs_check_faces(0, 0, None, None, None, None, None) == F.OVS_ERR_ARG
