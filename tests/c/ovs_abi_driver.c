@@ -101,6 +101,29 @@ static int run_abi(void) {
   EXPECT(ovs_newton_update(NULL, OVS_SYS_NS) == OVS_ERR_ARG, "newton_update(NULL)");
   EXPECT(ovs_gen_spar_struc(4, 1, 4, NULL, NULL, NULL, &icnt) == OVS_ERR_ARG, "gen_spar_struc(NULL)");
 
+  /* the stateless input checks: one tet, its four faces, two boundaries */
+  {
+    const int f2e[4] = {1, 1, 1, 1}, face_or[4] = {1, 2, 3, 4};
+    int flags[4] = {OVS_FACE_WEAK, 0, OVS_FACE_CONVH, 0};
+    const double hconv[4] = {5.0, 0.0, 5.0, 0.0}, tinf[4] = {300.0, 0.0, 300.0, 0.0};
+    const int face_id[2] = {2, 1}, bnode_ptr[3] = {0, 3, 5}, bnodes[5] = {1, 2, 3, 3, 4};
+    const int ut[2 * 3] = {1, 0, 1, 1, 0, 1}, pt[2] = {0, 1}, tt[2] = {1, 0};
+    const double uv[2 * 3] = {0.0, 1.0, 0.0, 0.0, 0.0, 0.0}, pv[2] = {0.0, 1.0}, tv[2] = {300.0, 0.0};
+    ovs_bc_spec sp;
+    int bad_nodes[5] = {1, 2, 3, 3, 5};
+    EXPECT(ovs_check_faces(1, 4, f2e, face_or, flags, hconv, tinf) == OVS_OK, "check_faces");
+    EXPECT(ovs_check_faces(1, 4, f2e, face_or, flags, NULL, NULL) == OVS_ERR_ARG, "check_faces without tables");
+    flags[1] = 8;
+    EXPECT(ovs_check_faces(1, 4, f2e, face_or, flags, hconv, tinf) == OVS_ERR_ARG, "check_faces bad flag");
+    memset(&sp, 0, sizeof sp);
+    sp.nbound = 2; sp.ntype = 2; sp.face_id = face_id; sp.bnode_ptr = bnode_ptr; sp.bnodes = bnodes;
+    sp.bcug_type = ut; sp.bcug_valu = uv; sp.bcphig_type = pt; sp.bcphig_valu = pv;
+    sp.bctg_type = tt; sp.bctg_valu = tv;
+    EXPECT(ovs_check_bc_spec(&sp, 4) == OVS_OK, "check_bc_spec");
+    sp.bnodes = bad_nodes;
+    EXPECT(ovs_check_bc_spec(&sp, 4) == OVS_ERR_ARG, "check_bc_spec node out of range");
+  }
+
   dims.nnode = 4; dims.nelem = 1; dims.nshl = 4; dims.device = -1;
   st = ovs_create(&ctx, &dims);
   if (st == OVS_ERR_NODEVICE) {
