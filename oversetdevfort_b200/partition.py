@@ -37,6 +37,8 @@ def owner_ranges(nnode: int, nparts: int) -> np.ndarray:
 
 
 def make_parts(m: "M.Mesh", nparts: int) -> list[Part]:
+    if nparts < 1 or nparts > m.nnode:
+        raise ValueError(f"need 1 <= nparts <= nnode ({m.nnode}): every part owns at least one node")
     ien0 = np.asarray(m.ien, dtype=np.int64) - 1
     bounds = owner_ranges(m.nnode, nparts)
     owner_of_node = np.searchsorted(bounds, np.arange(m.nnode), side="right") - 1

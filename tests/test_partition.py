@@ -144,3 +144,17 @@ def test_two_gloo_ranks_rebuild_global_system(oracle):
         p.join(timeout=120)
         assert p.exitcode == 0
     assert ok
+
+
+def test_part_count_limits():
+    """Every part owns at least one node: 1..N parts, the owned ranges cover
+    the nodes once; more parts than nodes, or none, is an error."""
+    import pytest
+    m = M.box_tet(2, 2, 1)
+    for n in (1, 5, m.nnode):
+        parts = P.make_parts(m, n)
+        owned = np.concatenate([p.nodes[p.owned] for p in parts])
+        assert np.array_equal(np.sort(owned), np.arange(m.nnode)) and all(p.owned.size for p in parts)
+    for n in (0, m.nnode + 1):
+        with pytest.raises(ValueError):
+            P.make_parts(m, n)
