@@ -35,3 +35,27 @@ def test_reference_arm_counts_usable_cores():
     assert 1 <= n <= (os.cpu_count() or n)
     if hasattr(os, "sched_getaffinity"):
         assert n == len(os.sched_getaffinity(0))
+
+
+def test_reference_arm_json_line():
+    """bench.py --impl reference (CPU, a small cube): one JSON line with the
+    contract's keys, impl "reference", a cpu_baseline of kind "port" and an
+    e2e with no host-device traffic."""
+    import json
+    import subprocess
+    import sys
+    from pathlib import Path
+    root = Path(__file__).resolve().parent.parent
+    res = subprocess.run([sys.executable, str(root / "bench.py"), "--impl", "reference", "--steps", "2", "--warmup", "3",
+                          "--n", "16"], capture_output=True, text=True, timeout=600, cwd=root)
+    assert res.returncode == 0, res.stderr[-2000:]
+    lines = [ln for ln in res.stdout.splitlines() if ln.startswith("{")]
+    assert len(lines) == 1
+    d = json.loads(lines[0])
+    for k in ("metric", "value", "unit", "n_gpus", "steps", "warmup", "ms_per_step", "higher_is_better", "scaling",
+              "vs_baseline", "dtype", "data", "config", "cpu_baseline", "e2e"):
+        assert k in d, k
+    assert d["impl"] == "reference" and d["steps"] == 2 and d["warmup"] == 3 and d["value"] > 0
+    assert d["cpu_baseline"]["kind"] == "port" and d["cpu_baseline"]["cores"] >= 1
+    assert d["e2e"]["h2d_bytes_per_step"] == 0 and d["e2e"]["d2h_bytes_per_step"] == 0
+    assert "workload" in d["config"]
