@@ -59,3 +59,22 @@ def test_reference_arm_json_line():
     assert d["cpu_baseline"]["kind"] == "port" and d["cpu_baseline"]["cores"] >= 1
     assert d["e2e"]["h2d_bytes_per_step"] == 0 and d["e2e"]["d2h_bytes_per_step"] == 0
     assert "workload" in d["config"]
+
+
+def test_own_arm_fails_without_a_device():
+    """bench.py's own arm has no CPU path: without a CUDA device it exits
+    non-zero on ovs_create's OVS_ERR_NODEVICE and prints no bench line."""
+    import subprocess
+    import sys
+    from pathlib import Path
+    import pytest
+    import torch
+    if torch.cuda.is_available():
+        pytest.skip("a device is present")
+    root = Path(__file__).resolve().parent.parent
+    res = subprocess.run([sys.executable, str(root / "bench.py"), "--steps", "1", "--warmup", "3", "--n", "8",
+                          "--no-solve", "--no-adjoint", "--no-hex", "--no-cpu"], capture_output=True, text=True,
+                         timeout=600, cwd=root)
+    assert res.returncode != 0
+    assert "no CUDA device" in res.stderr
+    assert not [ln for ln in res.stdout.splitlines() if ln.startswith("{")]
