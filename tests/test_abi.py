@@ -110,3 +110,15 @@ def test_integration_guide_lists_every_entry_point():
     doc = (ROOT / "INTEGRATION.md").read_text()
     missing = [n for n in _declared() if n not in doc]
     assert not missing, missing
+
+
+def test_smoke_needs_the_device():
+    """__graft_entry__.smoke() runs the CUDA path only: without a device it
+    raises instead of passing on the oracle."""
+    import pytest
+    import torch
+    if torch.cuda.is_available():
+        pytest.skip("a device is present")
+    import __graft_entry__ as g
+    with pytest.raises(F.OvsError):
+        g.smoke()
