@@ -1134,6 +1134,7 @@ int profile_krylov_t(ovs_ctx* c, int what, int sys, int reps, double* ms) {
   if ((st = ensure_basis(c, prec, sizeof(TM) * ld * (kspace + 1)))) return st;
   TM* V = reinterpret_cast<TM*>(c->basis[prec]);
   fill_kernel<TM><<<1184, 256, 0, c->stream>>>(V, ld * (kspace + 1), 1.0);
+  ++c->launches;
   GmresDev* gm = c->gm;
   int km[2] = {kspace, 1};
   OVS_CUDA_TRY(cudaMemcpyAsync(&gm->kspace, km, sizeof(km), cudaMemcpyHostToDevice, c->stream));

@@ -49,24 +49,28 @@ __global__ void scan_add_kernel(int* __restrict__ out, const int* __restrict__ o
   if (i < n && blockIdx.x > 0) out[i] += offs[blockIdx.x];
 }
 
-// exclusive scan of n ints (n may be large); tmp needs >= 2*ceil(n/1024)+2 ints
-int exclusive_scan(const int* in, int* out, int n, int* tmp, cudaStream_t s) {
+// exclusive scan of n ints (n may be large); tmp needs >= 2*ceil(n/1024)+2 ints;
+// *launches counts the kernels it launches
+int exclusive_scan(const int* in, int* out, int n, int* tmp, cudaStream_t s, long long* launches) {
   int nb = (n + SCAN_T - 1) / SCAN_T;
   int* sums = tmp;
   int* sums_scan = tmp + nb + 1;
   scan_block_kernel<<<nb, SCAN_T, 0, s>>>(in, out, sums, n);
+  ++*launches;
   if (nb > 1) {
     int nb2 = (nb + SCAN_T - 1) / SCAN_T;
     if (nb2 > 1) {
       // second level recursion (n up to 2^30)
       int* tmp2 = sums_scan + nb + 1;
-      int st = exclusive_scan(sums, sums_scan, nb, tmp2, s);
+      int st = exclusive_scan(sums, sums_scan, nb, tmp2, s, launches);
       if (st) return st;
     } else {
       int* dummy = sums_scan + nb + 1;
       scan_block_kernel<<<1, SCAN_T, 0, s>>>(sums, sums_scan, dummy, nb);
+      ++*launches;
     }
     scan_add_kernel<<<nb, SCAN_T, 0, s>>>(out, sums_scan, n);
+    ++*launches;
   }
   return cudaGetLastError() == cudaSuccess ? 0 : OVS_ERR_CUDA;
 }
@@ -224,9 +228,11 @@ int ovs_pattern_to_host(ovs_ctx* c, int* col, int* row) {
   int* tmp = nullptr;
   OVS_CUDA_TRY(cudaMallocAsync(&tmp, sizeof(int) * (n1 > n2 ? n1 : n2), s));
   to_one_based_kernel<<<ovs_grid(n1, 256, 1 << 30), 256, 0, s>>>(c->rowptr, tmp, n1);
+  ++c->launches;
   OVS_CUDA_TRY(cudaMemcpyAsync(col, tmp, sizeof(int) * n1, cudaMemcpyDeviceToHost, s));
   if (row && n2) {
     to_one_based_kernel<<<ovs_grid(n2, 256, 1 << 30), 256, 0, s>>>(c->colidx, tmp, n2);
+    ++c->launches;
     OVS_CUDA_TRY(cudaMemcpyAsync(row, tmp, sizeof(int) * n2, cudaMemcpyDeviceToHost, s));
   }
   OVS_CUDA_TRY(cudaFreeAsync(tmp, s));
@@ -253,14 +259,16 @@ int ovs_pattern_build(ovs_ctx* c) {
   OVS_CUDA_TRY(cudaMemsetAsync(stats, 0, sizeof(int) * 8, s));
   // stats: [0] bad node ids, [1] row overflow, [2] max elements per node, [3] max degree
   count_n2e_kernel<<<ovs_grid(EN, 256, 1 << 30), 256, 0, s>>>(c->ien, E, nshl, N, cnt, stats + 0);
-  if ((st = exclusive_scan(cnt, c->n2e_ptr, N + 1, tmp, s))) return st;
+  ++c->launches;
+  if ((st = exclusive_scan(cnt, c->n2e_ptr, N + 1, tmp, s, &c->launches))) return st;
   OVS_CUDA_TRY(cudaMemcpyAsync(cnt, c->n2e_ptr, sizeof(int) * N, cudaMemcpyDeviceToDevice, s));
   fill_n2e_kernel<<<ovs_grid(EN, 256, 1 << 30), 256, 0, s>>>(c->ien, E, nshl, N, cnt, c->n2e);
   sort_n2e_kernel<<<ovs_grid(N, 128, 1 << 30), 128, 0, s>>>(c->n2e_ptr, c->n2e, N, stats + 2);
   row_len_kernel<<<ovs_grid(N, 128, 1 << 30), 128, 0, s>>>(c->ien, nshl, N, c->n2e_ptr, c->n2e,
                                                            cnt, stats + 1, stats + 3);
+  c->launches += 3;
   OVS_CUDA_TRY(cudaMemsetAsync(cnt + N, 0, sizeof(int), s));
-  if ((st = exclusive_scan(cnt, c->rowptr, N + 1, tmp, s))) return st;
+  if ((st = exclusive_scan(cnt, c->rowptr, N + 1, tmp, s, &c->launches))) return st;
   int h[8];
   OVS_CUDA_TRY(cudaMemcpyAsync(h, stats, sizeof(int) * 8, cudaMemcpyDeviceToHost, s));
   int nnz = 0;
@@ -275,15 +283,18 @@ int ovs_pattern_build(ovs_ctx* c) {
   if ((st = ovs_ensure((void**)&c->colidx, sizeof(int) * (size_t)(nnz > 0 ? nnz : 1)))) return st;
   row_fill_kernel<<<ovs_grid(N, 128, 1 << 30), 128, 0, s>>>(c->ien, nshl, N, c->n2e_ptr, c->n2e,
                                                             c->rowptr, c->colidx, c->diag);
+  ++c->launches;
   if (nshl == 8) {
     if ((st = ovs_ensure((void**)&c->n2s, 2 * sizeof(unsigned) * (size_t)(EN > 0 ? EN : 1)))) return st;
     slot_map8_kernel<<<ovs_grid(N, 128, 1 << 30), 128, 0, s>>>(c->ien, N, c->n2e_ptr, c->n2e, c->rowptr,
                                                                c->colidx, reinterpret_cast<uint2*>(c->n2s));
+    ++c->launches;
   }
   if (nshl == 4) {
     if ((st = ovs_ensure((void**)&c->n2s, sizeof(unsigned) * (size_t)(EN > 0 ? EN : 1)))) return st;
     slot_map_kernel<<<ovs_grid(N, 128, 1 << 30), 128, 0, s>>>(c->ien, N, c->n2e_ptr, c->n2e, c->rowptr,
                                                               c->colidx, c->n2s);
+    ++c->launches;
   }
   OVS_CUDA_TRY(cudaFreeAsync(cnt, s));
   OVS_CUDA_TRY(cudaFreeAsync(tmp, s));

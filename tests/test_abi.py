@@ -122,3 +122,19 @@ def test_smoke_needs_the_device():
     import __graft_entry__ as g
     with pytest.raises(F.OvsError):
         g.smoke()
+
+
+def test_every_kernel_launch_is_counted():
+    """ovs_launch_count (and bench.py's gpu_launches from it) covers every
+    kernel a context launches: each launch site in csrc/ is followed within
+    a few lines by an increment of the context's counter.  The one exception
+    is ovs_gmres_tem_noalloc, which has no context."""
+    csrc = ROOT / "oversetdevfort_b200" / "csrc"
+    missing = []
+    for f in sorted(csrc.glob("*.cu*")):
+        lines = f.read_text().splitlines()
+        for i, ln in enumerate(lines):
+            if "<<<" in ln and not ln.strip().startswith("//"):
+                if "launches" not in "\n".join(lines[i:i + 9]) and f.name != "noalloc.cu":
+                    missing.append(f"{f.name}:{i + 1}")
+    assert not missing, missing
