@@ -138,3 +138,35 @@ def test_every_kernel_launch_is_counted():
                 if "launches" not in "\n".join(lines[i:i + 9]) and f.name != "noalloc.cu":
                     missing.append(f"{f.name}:{i + 1}")
     assert not missing, missing
+
+
+def test_enum_values_match_the_python_constants():
+    """Every OVS_* constant the header defines (enums and #defines) has the
+    same value in oversetdevfort_b200._ffi when the binding names it."""
+    txt = re.sub(r"/\*.*?\*/", "", (ROOT / "include" / "ovs.h").read_text(), flags=re.S)
+    values = {}
+    for body in re.findall(r"enum\s*\{(.*?)\}", txt, flags=re.S):
+        nxt = 0
+        for item in body.split(","):
+            item = item.strip()
+            if not item:
+                continue
+            if "=" in item:
+                name, val = (t.strip() for t in item.split("=", 1))
+                nxt = int(val, 0)
+            else:
+                name = item
+            values[name] = nxt
+            nxt += 1
+    for name, val in re.findall(r"#define\s+(OVS_\w+)\s+(-?\d+)", txt):
+        values[name] = int(val)
+    assert len(values) > 40
+    checked = 0
+    for name, val in values.items():
+        if hasattr(F, name):
+            assert getattr(F, name) == val, (name, getattr(F, name), val)
+            checked += 1
+    assert checked >= 30, checked
+    # the nodal fields: OVS_F_<NAME> is FIELD_ID["<name>"] in the binding
+    fields = {n[6:].lower(): v for n, v in values.items() if n.startswith("OVS_F_") and n != "OVS_F_COUNT"}
+    assert fields == F.FIELD_ID and values["OVS_F_COUNT"] == len(F.FIELDS)
