@@ -170,3 +170,35 @@ def test_enum_values_match_the_python_constants():
     # the nodal fields: OVS_F_<NAME> is FIELD_ID["<name>"] in the binding
     fields = {n[6:].lower(): v for n, v in values.items() if n.startswith("OVS_F_") and n != "OVS_F_COUNT"}
     assert fields == F.FIELD_ID and values["OVS_F_COUNT"] == len(F.FIELDS)
+
+
+def test_struct_layouts_match_the_header(tmp_path):
+    """Every ctypes structure of the binding has the size and field offsets
+    of its C struct in include/ovs.h, as gcc lays it out (the program that
+    prints them is generated from the ctypes field lists)."""
+    import shutil
+    import subprocess
+    import pytest
+    if shutil.which("gcc") is None:
+        pytest.skip("gcc not available")
+    pairs = [(F.OvsDims, "ovs_dims"), (F.OvsParams, "ovs_params"), (F.OvsGmresInfo, "ovs_gmres_info"),
+             (F.OvsSolveInfo, "ovs_solve_info"), (F.OvsNewtonOpts, "ovs_newton_opts"),
+             (F.OvsNewtonInfo, "ovs_newton_info"), (F.OvsBcSpec, "ovs_bc_spec")]
+    body = []
+    for cls, cname in pairs:
+        body.append(f'  printf("{cname} size %zu\\n", sizeof({cname}));')
+        for fname, *_ in cls._fields_:
+            body.append(f'  printf("{cname} {fname} %zu\\n", offsetof({cname}, {fname}));')
+    src = tmp_path / "layout.c"
+    src.write_text('#include <stddef.h>\n#include <stdio.h>\n#include "ovs.h"\nint main(void) {\n' + "\n".join(body)
+                   + "\n  return 0;\n}\n")
+    exe = tmp_path / "layout"
+    res = subprocess.run(["gcc", "-std=c99", "-I", str(ROOT / "include"), str(src), "-o", str(exe)],
+                         capture_output=True, text=True)
+    assert res.returncode == 0, res.stderr
+    out = subprocess.run([str(exe)], capture_output=True, text=True, check=True).stdout.splitlines()
+    got = {tuple(ln.split()[:2]): int(ln.split()[2]) for ln in out}
+    for cls, cname in pairs:
+        assert got[(cname, "size")] == ctypes.sizeof(cls), cname
+        for fname, *_ in cls._fields_:
+            assert got[(cname, fname)] == getattr(cls, fname).offset, (cname, fname)
