@@ -202,3 +202,19 @@ def test_struct_layouts_match_the_header(tmp_path):
         assert got[(cname, "size")] == ctypes.sizeof(cls), cname
         for fname, *_ in cls._fields_:
             assert got[(cname, fname)] == getattr(cls, fname).offset, (cname, fname)
+
+
+def test_ctypes_signatures_match_the_prototypes(lib):
+    """Each entry point's ctypes argtypes has the parameter count of its
+    prototype in include/ovs.h, and its result is a C int (or a string for
+    ovs_status_string)."""
+    txt = re.sub(r"/\*.*?\*/", "", (ROOT / "include" / "ovs.h").read_text(), flags=re.S)
+    protos = dict(re.findall(r"\b(?:int|const char\*)\s+(ovs_\w+)\s*\(([^)]*)\)\s*;", txt))
+    assert len(protos) == len(F.EXPORTS)
+    for name, params in protos.items():
+        params = params.strip()
+        n = 0 if params in ("", "void") else params.count(",") + 1
+        fn = getattr(lib, name)
+        assert len(fn.argtypes) == n, (name, len(fn.argtypes), n)
+        want = ctypes.c_char_p if name == "ovs_status_string" else ctypes.c_int
+        assert fn.restype is want, name
