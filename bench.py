@@ -40,51 +40,6 @@ sys.path.insert(0, str(ROOT))
 METRIC = "assembly Melem/s & GMRES s/solve at 2.1M nodes, mixed vs FP64 to rel. resid 1e-8"
 
 
-def ncu_traffic_per_tet(name, tets=663552):
-    """DRAM bytes (read + write) per tet of one launch, from a committed ncu
-    summary of the kernel on a workload of `tets` tets; the bench scales it
-    by the tets of its own workload.  (None, reason) when absent."""
-    import re
-    path = os.path.join(os.path.dirname(os.path.abspath(__file__)), "profiles", name)
-    try:
-        txt = open(path).read()
-    except OSError:
-        return None, "no ncu summary"
-    def mb(metric):
-        m = re.search(r"`%s`\) \| ([0-9.]+) (Kbyte|Mbyte|Gbyte|byte)" % re.escape(metric), txt)
-        if not m:
-            return None
-        return float(m.group(1)) * {"byte": 1, "Kbyte": 1e3, "Mbyte": 1e6, "Gbyte": 1e9}[m.group(2)]
-    rd, wr = mb("dram__bytes_read.sum"), mb("dram__bytes_write.sum")
-    if rd is None or wr is None:
-        return None, "no DRAM counters in " + name
-    return (rd + wr) / float(tets), ("ncu dram__bytes_read.sum + dram__bytes_write.sum of one launch on a "
-                                     "%d-tet case (profiles/%s), per tet times the tets of this workload"
-                                     % (tets, name))
-
-
-def ncu_flops_per_tet(name, tets):
-    """Executed FP32 flops per tet of one launch (FFMA x 2 + FADD + FMUL
-    thread instructions) from a committed ncu summary of the kernel on a
-    workload of `tets` tets.  (None, reason) when absent."""
-    import re
-    path = os.path.join(os.path.dirname(os.path.abspath(__file__)), "profiles", name)
-    try:
-        txt = open(path).read()
-    except OSError:
-        return None, "no ncu summary"
-    def cnt(metric):
-        m = re.search(r"`%s` \| ([0-9.eE+]+)" % re.escape(metric), txt)
-        return float(m.group(1)) if m else None
-    ffma = cnt("smsp__sass_thread_inst_executed_op_ffma_pred_on.sum")
-    fadd = cnt("smsp__sass_thread_inst_executed_op_fadd_pred_on.sum")
-    fmul = cnt("smsp__sass_thread_inst_executed_op_fmul_pred_on.sum")
-    if None in (ffma, fadd, fmul):
-        return None, "no FP32 instruction counters in " + name
-    return (2 * ffma + fadd + fmul) / float(tets), ("ncu FFMA x 2 + FADD + FMUL thread instructions of one launch "
-                                                   "on a %d-tet case (profiles/%s), per tet" % (tets, name))
-
-
 def _peaks():
     try:
         return json.loads((ROOT / "MEASURED_PEAKS.json").read_text()), "measured"
@@ -202,6 +157,22 @@ def cpu_assembly_pass(case, reps: int = 1):
     return best, oc.E, oc.N
 
 
+def cpu_gmres_iteration(case, kspace: int = 50):
+    """Seconds per Arnoldi iteration of the oracle's FP64 coupled GMRES cycle
+    (SparseGMRES_ns_conv restated: preconditioned SpMV + modified
+    Gram-Schmidt + Givens) on `case`'s NS+VOF system: one full cycle of
+    `kspace` iterations (a tolerance no cycle meets), so the average
+    Gram-Schmidt depth is that of a kspace cycle.  Returns (s/iteration,
+    iterations, nodes)."""
+    from oracle import pyoracle as O
+    oc = O.OracleCase(case)
+    oc.assemble_quenching(6, 3)
+    t0 = time.perf_counter()
+    _, it, _, _ = oc.gmres("nsvof", 1e-300, kspace, kspace)
+    t = time.perf_counter() - t0
+    return t / max(it, 1), it, oc.N
+
+
 def _cpu_worker(args):
     n, k0, nl, steps, warmup = args
     case = config3_slab(n, k0, nl)
@@ -227,22 +198,39 @@ def _host_cores() -> int:
         return os.cpu_count() or 1
 
 
+def slab_layers(n: int, parts: int):
+    """Split the n cell layers of the cube into `parts` contiguous slabs
+    (sizes differ by at most one layer); together they cover every layer
+    exactly once.  Returns [(k0, nl), ...] for the non-empty slabs."""
+    parts = max(1, min(parts, n))
+    base, extra = divmod(n, parts)
+    out, k0 = [], 0
+    for i in range(parts):
+        nl = base + (1 if i < extra else 0)
+        out.append((k0, nl))
+        k0 += nl
+    return out
+
+
 def run_reference(args, world, rank):
     """--impl reference: the reference's CPU algorithm (the oracle port; the
-    Fortran reference cannot be compiled here) on all host cores, one
-    process per core on its own slab of the workload, like the reference's
-    MPI ranks."""
+    Fortran reference cannot be compiled here) on all host cores it may use,
+    one process per core like the reference's MPI ranks.  Together the
+    processes assemble the WHOLE workload: the n^3 cube is cut into one slab
+    of cell layers per process, every layer in exactly one slab, and a step is
+    done when the slowest process is (the same elements, fields and physics
+    as the GPU arm's step)."""
     if rank != 0:
         return
     import multiprocessing as mp
     cores = _host_cores()
-    n, nl = args.n, 2
-    nslab = max(1, n // nl)
-    jobs = [(n, (i * nl) % (n - nl + 1), nl, args.steps, args.warmup) for i in range(cores)]
+    n = args.n
+    slabs = slab_layers(n, cores)
+    jobs = [(n, k0, nl, args.steps, args.warmup) for k0, nl in slabs]
     from oracle import pyoracle as O
     O.build()
     t0 = time.time()
-    with mp.get_context("spawn").Pool(cores) as pool:
+    with mp.get_context("spawn").Pool(len(jobs)) as pool:
         res = pool.map(_cpu_worker, jobs)
     wall = time.time() - t0
     E_tot = sum(e for e, _ in res)
@@ -254,12 +242,13 @@ def run_reference(args, world, rank):
         "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
         "ms_per_step": statistics.mean(per_step) * 1e3, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-        "config": {"workload": f"config3 quench NS+VOF+T assembly, {n}^3 cells x6 tets; each of "
-                               f"{cores} processes assembles a {n}x{n}x{nl}-cell slab of it",
-                   "cache": "per-process slab", "parallelism": f"{cores} processes (MPI-rank analogue)"},
-        "cpu_baseline": {"value": value, "unit": "Melem/s", "cores": cores, "kind": "port",
-                         "sample": f"{cores} slabs of {E_tot // cores} tets, alpha stage + NS+VOF + T "
-                                   f"element loops MAT+VEC, {args.steps} timed passes"},
+        "config": {"workload": f"config3: NS+VOF+T quench assembly pass, {n}^3 cells x6 Kuhn tets "
+                               f"({E_tot} tets), FP64, all {n} cell layers split over {len(jobs)} processes",
+                   "cache": "per-process slab", "parallelism": f"{len(jobs)} processes (MPI-rank analogue)"},
+        "cpu_baseline": {"value": value, "unit": "Melem/s", "cores": len(jobs), "kind": "port",
+                         "sample": f"the whole {E_tot}-tet workload, {len(jobs)} slabs of "
+                                   f"{min(nl for _, nl in slabs)}-{max(nl for _, nl in slabs)} cell layers: "
+                                   f"alpha stage + NS+VOF + T element loops MAT+VEC, {args.steps} timed passes"},
         "e2e": {"value": value, "unit": "Melem/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
         "wall_s": wall,
     }
@@ -381,6 +370,74 @@ def run_hex(local_rank, args):
 
 
 # --------------------------------------------------------------- GPU arm
+def assembly_pass_bytes(E: int, N: int, nnz: int, s: int) -> int:
+    """Algorithmic bytes of one NS+VOF assembly pass (MAT+VEC): IEN 16 E,
+    the unique nodal inputs 23 N s (x, d, u, a, um, am, p, phi, phidot, T,
+    alpha-stage old values folded in), IBC 6 N, the CSR values written
+    24 nnz s and the RHS 5 N s.  Intermediates of this design (node records,
+    element summaries, slot map) are not counted."""
+    return 16 * E + 23 * N * s + 6 * N + 24 * nnz * s + 5 * N * s
+
+
+def spmv_bytes(N: int, nnz: int, s: int) -> int:
+    """Algorithmic bytes of the preconditioned NS+VOF SpMV: values 24 nnz s,
+    colidx 4 nnz, rowptr 4 (N + 1), x and y 5 N s each, block-diagonal
+    preconditioner 11 N s."""
+    return 24 * nnz * s + 4 * nnz + 4 * (N + 1) + 5 * N * s + 5 * N * s + 11 * N * s
+
+
+def ncu_dram_per_tet(name: str, tets: int):
+    """DRAM bytes (read + write) per tet of the kernels in a committed ncu
+    summary (every `dram__bytes_read.sum` / `dram__bytes_write.sum` row of
+    the file is added: one row pair per kernel of the pass) taken on a
+    `tets`-tet case.  (None, reason) when the summary is absent."""
+    import re
+    path = ROOT / "profiles" / name
+    try:
+        txt = path.read_text()
+    except OSError:
+        return None, "no ncu summary " + name
+    unit = {"byte": 1, "Kbyte": 1e3, "Mbyte": 1e6, "Gbyte": 1e9}
+    tot, found = 0.0, 0
+    for m in re.finditer(r"`dram__bytes_(read|write)\.sum`\)? \| ([0-9.]+) (Kbyte|Mbyte|Gbyte|byte)", txt):
+        tot += float(m.group(2)) * unit[m.group(3)]
+        found += 1
+    if found == 0:
+        return None, "no DRAM counters in " + name
+    return tot / float(tets), ("ncu dram__bytes_read.sum + dram__bytes_write.sum of every kernel of the pass on "
+                               "a %d-tet case (profiles/%s), per tet, times the tets of this workload" % (tets, name))
+
+
+def run_config2(local_rank, args):
+    """Config 2: one coupled quench time step (solveNavStoVOFTem form) on the
+    1x1x2 box of 48x48x96 cells x6 tets (1,327,104 tets, 232,897 nodes): the
+    device Newton loop (ovs_quench_newton) with 3 Newton iterations, the
+    reference's GMRES cycle (Krylov space 50, tolerance 1e-6) in FP64, and
+    the same step with every solve by the mixed refinement to 1e-6 on the
+    FP64 systems.  Wall time per step and iteration counts."""
+    from oversetdevfort_b200 import _ffi as F
+    from oversetdevfort_b200 import mesh as M
+    from oversetdevfort_b200.api import Context
+
+    case = M.config2()
+    out = {"workload": f"config2: {case.mesh.nelem} tets, {case.mesh.nnode} nodes (48x48x96 cells x6), "
+                       f"3 Newton iterations, GMRES Krylov space 50 to 1e-6"}
+    for mode, name in ((F.OVS_FP64, "fp64"), (F.OVS_MIXED, "mixed")):
+        ctx = Context.from_case(case, device=local_rank)
+        kw = dict(newton_max=3, solve_tem=True, kspace=50, kspace_min=1, max_cycles=50, tol_ns=1e-6, tol_tem=1e-6,
+                  utol=(1e-30,) * 4, atol=(1e-30,) * 4)
+        ctx.quench_newton(mode, **kw)            # warm-up: allocations, module load
+        ctx.close()
+        ctx = Context.from_case(case, device=local_rank)
+        info = ctx.quench_newton(mode, **kw)
+        out[name] = {"s_per_step": info.seconds, "newton_iterations": info.iterations,
+                     "krylov_iterations_ns": info.krylov_iterations_ns,
+                     "krylov_iterations_tem": info.krylov_iterations_tem,
+                     "residual0": list(info.residual0), "residual": list(info.residual)}
+        ctx.close()
+    return out
+
+
 def run_ours(args, world, rank, local_rank, dist):
     import numpy as np
     from oversetdevfort_b200 import _ffi as F
@@ -420,129 +477,125 @@ def run_ours(args, world, rank, local_rank, dist):
         t, Es, Ns = cpu_assembly_pass(slab, reps=1)
         cpu = {"value": Es / t / 1e6, "unit": "Melem/s", "cores": 1, "kind": "port",
                "sample": f"{Es} tets ({n}x{n}x{nl}-cell slab of the workload across the interface): "
-                         f"alpha stage + NS+VOF + T element loops MAT+VEC, one pass, {t:.1f} s"}
+                         f"alpha stage + NS+VOF + T element loops MAT+VEC in FP64, one pass, {t:.1f} s"}
+        if not args.no_solve:
+            spi, its, Nsl = cpu_gmres_iteration(slab, args.kspace)
+            cpu["gmres"] = {"s_per_iteration_sample": spi, "iterations_timed": its, "nodes_sample": Nsl,
+                            "s_per_iteration_workload": spi * N / Nsl, "cores": 1,
+                            "sample": f"one FP64 SparseGMRES_ns_conv cycle of {its} iterations on the slab's "
+                                      f"NS+VOF system ({Nsl} nodes), scaled to {N} nodes by the node count"}
 
     clocks = ClockSampler(local_rank)
     clocks.start()
     launches0 = ctx.launch_count()
     # ------------------------------------------------- timed assembly
     res = {}
-    for prec, name in ((F.OVS_FP32, "fp32"), (F.OVS_FP64, "fp64")):
+    nlaunch = {}
+    for prec, name in ((F.OVS_FP64, "fp64"), (F.OVS_FP32, "fp32")):
         for _ in range(args.warmup):
             assembly_pass(prec)
         barrier_()
         ctx.synchronize()
+        l0 = ctx.launch_count()
         t0 = time.time()
         ms = [assembly_pass(prec) for _ in range(args.steps)]
         ctx.synchronize()
         wall = time.time() - t0
+        nlaunch[name] = ctx.launch_count() - l0
         barrier_()
         res[name] = {"ms": maxr(statistics.mean(ms)), "wall_s": wall}
-    launches_step = (ctx.launch_count() - launches0) / (2 * (args.warmup + args.steps))
-    ms_step = res["fp32"]["ms"]
+    ms_step = res["fp64"]["ms"]
     value = replica_throughput(world, E, ms_step)
 
     # --------------------------------------------- kernel roofline
     prof = {}
-    prof["asm_nsvof_fp32_ms"] = ctx.profile(F.OVS_PROF_ASSEMBLE, F.OVS_ASM_NSVOF, F.OVS_FP32, 5)
-    prof["asm_tem_fp32_ms"] = ctx.profile(F.OVS_PROF_ASSEMBLE, F.OVS_ASM_TEM, F.OVS_FP32, 5)
-    prof["asm_nsvof_fp64_ms"] = ctx.profile(F.OVS_PROF_ASSEMBLE, F.OVS_ASM_NSVOF, F.OVS_FP64, 3)
-    ctx.assemble(F.OVS_ASM_TEM, 6, F.OVS_FP32)
-    prof["asm_tem_fp32_elements_ms"] = ctx.profile(F.OVS_PROF_ASSEMBLE_ELEMENTS, F.OVS_ASM_TEM, F.OVS_FP32, 5)
-    prof["asm_tem_fp32_rows_ms"] = ctx.profile(F.OVS_PROF_ASSEMBLE_ROWS, F.OVS_ASM_TEM, F.OVS_FP32, 5)
+    for prec, nm in ((F.OVS_FP64, "fp64"), (F.OVS_FP32, "fp32")):
+        for kern, kn in ((F.OVS_ASM_NSVOF, "nsvof"), (F.OVS_ASM_TEM, "tem")):
+            ctx.assemble(kern, 6, prec)
+            prof[f"asm_{kn}_{nm}_ms"] = ctx.profile(F.OVS_PROF_ASSEMBLE, kern, prec, 5)
+            prof[f"asm_{kn}_{nm}_elements_ms"] = ctx.profile(F.OVS_PROF_ASSEMBLE_ELEMENTS, kern, prec, 5)
+            prof[f"asm_{kn}_{nm}_rows_ms"] = ctx.profile(F.OVS_PROF_ASSEMBLE_ROWS, kern, prec, 5)
     ctx.assemble(F.OVS_ASM_NSVOF, 6, F.OVS_FP32)
-    prof["asm_nsvof_fp32_elements_ms"] = ctx.profile(F.OVS_PROF_ASSEMBLE_ELEMENTS, F.OVS_ASM_NSVOF, F.OVS_FP32, 5)
-    prof["asm_nsvof_fp32_rows_ms"] = ctx.profile(F.OVS_PROF_ASSEMBLE_ROWS, F.OVS_ASM_NSVOF, F.OVS_FP32, 5)
-    ctx.assemble(F.OVS_ASM_NSVOF, 6, F.OVS_FP32)
+    ctx.assemble(F.OVS_ASM_NSVOF, 6, F.OVS_FP64)
     prof["spmv_nsvof_fp32_ms"] = ctx.profile(F.OVS_PROF_SPMV, F.OVS_SYS_NSVOF, F.OVS_FP32, 20)
     prof["spmv_nsvof_fp64_ms"] = ctx.profile(F.OVS_PROF_SPMV, F.OVS_SYS_NSVOF, F.OVS_FP64, 10)
     prof["arnoldi_k25_nsvof_fp32_ms"] = ctx.profile(F.OVS_PROF_ARNOLDI, F.OVS_SYS_NSVOF, F.OVS_FP32, 10)
     prof["arnoldi_k25_nsvof_fp64_ms"] = ctx.profile(F.OVS_PROF_ARNOLDI, F.OVS_SYS_NSVOF, F.OVS_FP64, 10)
-    prof["arnoldi_fused_k25_nsvof_fp32_ms"] = ctx.profile(F.OVS_PROF_ARNOLDI_FUSED, F.OVS_SYS_NSVOF, F.OVS_FP32, 10)
-    prof["arnoldi_fused_k25_nsvof_fp64_ms"] = ctx.profile(F.OVS_PROF_ARNOLDI_FUSED, F.OVS_SYS_NSVOF, F.OVS_FP64, 10)
-
-    def spmv_bytes(s):  # values, colidx, rowptr, x gather (once), y, preconditioner
-        return 24 * nnz * s + 4 * nnz + 4 * (N + 1) + 5 * N * s + 5 * N * s + 11 * N * s
-
-    def rows_bytes(s):
-        # row pass, NS+VOF: element summaries read once (88 values per tet),
-        # ien 16E, node-to-element map 16E + 4(N+1), pattern 4 nnz + 4(N+1),
-        # IBC N, CSR values written 24 nnz s, RHS 5 N s
-        return 88 * E * s + 16 * E + 16 * E + 4 * (N + 1) + 4 * nnz + 4 * (N + 1) + N \
-            + 24 * nnz * s + 5 * N * s
-
-    def pass_bytes(s):
-        # whole NS+VOF assembly pass (element + row kernels), intermediates
-        # excluded: ien 16E, unique nodal inputs 23 N s, IBC 6N (one byte
-        # here: N), CSR values 24 nnz s, RHS 5 N s
-        return 16 * E + 23 * N * s + N + 24 * nnz * s + 5 * N * s
 
     hbm = float(peaks["hbm_gbs"])
-    sp_ach = spmv_bytes(4) / (prof["spmv_nsvof_fp32_ms"] * 1e-3) / 1e9
-    as_ach = rows_bytes(4) / (prof["asm_nsvof_fp32_rows_ms"] * 1e-3) / 1e9
-    pa_ach = pass_bytes(4) / (prof["asm_nsvof_fp32_ms"] * 1e-3) / 1e9
-    traffic, traffic_src = ncu_traffic_per_tet("assemble_rows_kernel_quench128_dram.md", 12582912)
-    roof_asm = {"kernel": "assemble_rows_kernel<float,NSVOF> (row-owner element assembly)",
-                "bound": "hbm", "achieved": as_ach, "peak": hbm, "unit": "GB/s",
-                "frac": as_ach / hbm, "traffic": traffic * E if traffic else None,
-                "traffic_source": traffic_src, "peak_kind": peak_kind,
-                "algorithmic_bytes": rows_bytes(4), "avg_ms": prof["asm_nsvof_fp32_rows_ms"]}
-    # compute side: executed FP32 flops of the row kernel (ncu counters) against
-    # the FMA throughput measured now on this device
+    pass64 = assembly_pass_bytes(E, N, nnz, 8)
+    pa_ach = pass64 / (prof["asm_nsvof_fp64_ms"] * 1e-3) / 1e9
+    row_ach = pass64 / (prof["asm_nsvof_fp64_rows_ms"] * 1e-3) / 1e9
+    dpt, dpt_src = ncu_dram_per_tet("assembly_nsvof_fp64_quench48_dram.md", 663552)
+    roof_asm = {"kernel": "element_summary_kernel + assemble_rows_kernel <double, NSVOF>: one NS+VOF assembly "
+                          "pass (MAT+VEC), the dominant work of the step",
+                "bound": "hbm", "achieved": pa_ach, "peak": hbm, "unit": "GB/s", "frac": pa_ach / hbm,
+                "traffic": dpt * E if dpt else None, "traffic_source": dpt_src, "peak_kind": peak_kind,
+                "algorithmic_bytes": pass64,
+                "algorithmic_bytes_formula": "16 E + 23 N s + 6 N + 24 nnz s + 5 N s, s = 8",
+                "avg_ms": prof["asm_nsvof_fp64_ms"],
+                "rows_kernel_only": {"avg_ms": prof["asm_nsvof_fp64_rows_ms"], "achieved": row_ach,
+                                     "frac": row_ach / hbm,
+                                     "note": "the pass's algorithmic bytes over the row kernel's time alone"}}
+    fp64_peak = ctx.measure_fp64_peak()
     fp32_peak = ctx.measure_fp32_peak()
-    fpt, fpt_src = ncu_flops_per_tet("assemble_rows_kernel_quench48_flops.md", 663552)
-    if fpt:
-        fl = fpt * E
-        t_hbm, t_fp = rows_bytes(4) / (hbm * 1e9), fl / (fp32_peak * 1e12)
-        roof_asm["compute"] = {"bound": "fp32", "unit": "TFLOP/s", "peak": fp32_peak, "peak_kind": "measured now",
-                               "executed_flops": fl,
-                               "achieved": fl / (prof["asm_nsvof_fp32_rows_ms"] * 1e-3) / 1e12,
-                               "frac": fl / (prof["asm_nsvof_fp32_rows_ms"] * 1e-3) / 1e12 / fp32_peak,
-                               "source": fpt_src,
-                               "bound_ms": 1e3 * max(t_hbm, t_fp),
-                               "frac_of_bound": 1e3 * max(t_hbm, t_fp) / prof["asm_nsvof_fp32_rows_ms"]}
-    else:
-        roof_asm["compute"] = {"bound": "fp32", "peak": fp32_peak, "unit": "TFLOP/s", "executed_flops": None,
-                               "source": fpt_src}
-    roof_pass = {"kernels": "element_summary_kernel + assemble_rows_kernel <float,NSVOF>", "bound": "hbm",
-                 "achieved": pa_ach, "peak": hbm, "unit": "GB/s", "frac": pa_ach / hbm,
-                 "algorithmic_bytes": pass_bytes(4), "avg_ms": prof["asm_nsvof_fp32_ms"],
-                 "peak_kind": peak_kind}
+    roof_asm["compute_peaks_measured_tflops"] = {"fp64_fma": fp64_peak, "fp32_fma": fp32_peak}
+    pass32 = assembly_pass_bytes(E, N, nnz, 4)
+    roof_asm32 = {"kernels": "element_summary_kernel + assemble_rows_kernel <float, NSVOF>", "bound": "hbm",
+                  "achieved": pass32 / (prof["asm_nsvof_fp32_ms"] * 1e-3) / 1e9, "peak": hbm, "unit": "GB/s",
+                  "algorithmic_bytes": pass32, "avg_ms": prof["asm_nsvof_fp32_ms"], "peak_kind": peak_kind}
+    roof_asm32["frac"] = roof_asm32["achieved"] / hbm
+    sp_ach = spmv_bytes(N, nnz, 4) / (prof["spmv_nsvof_fp32_ms"] * 1e-3) / 1e9
+    sp64_ach = spmv_bytes(N, nnz, 8) / (prof["spmv_nsvof_fp64_ms"] * 1e-3) / 1e9
     roof_spmv = {"kernel": "spmv_block_kernel<6,float> (P^-1 A x, NS+VOF)", "bound": "hbm",
                  "achieved": sp_ach, "peak": hbm, "unit": "GB/s", "frac": sp_ach / hbm, "traffic": None,
-                 "peak_kind": peak_kind, "algorithmic_bytes": spmv_bytes(4),
-                 "avg_ms": prof["spmv_nsvof_fp32_ms"]}
+                 "peak_kind": peak_kind, "algorithmic_bytes": spmv_bytes(N, nnz, 4),
+                 "avg_ms": prof["spmv_nsvof_fp32_ms"],
+                 "fp64": {"achieved": sp64_ach, "frac": sp64_ach / hbm, "avg_ms": prof["spmv_nsvof_fp64_ms"],
+                          "algorithmic_bytes": spmv_bytes(N, nnz, 8)}}
 
     # ------------------------------------------------------- solves
     gm = {}
     if not args.no_solve:
         sols = {}
-        for mode, name in ((F.OVS_FP32, "mixed"), (F.OVS_FP64, "fp64")):
-            rec = {}
-            for sysid, kern, key in ((F.OVS_SYS_NSVOF, F.OVS_ASM_NSVOF, "nsvof"),
-                                     (F.OVS_SYS_TEM, F.OVS_ASM_TEM, "tem")):
-                ctx.assemble(kern, 6, mode)
+        true_res = {}
+        for sysid, kern, key in ((F.OVS_SYS_NSVOF, F.OVS_ASM_NSVOF, "nsvof"), (F.OVS_SYS_TEM, F.OVS_ASM_TEM, "tem")):
+            ctx.assemble(kern, 6, F.OVS_FP64)     # one FP64 system, solved both ways
+            b = ctx.get_rhs(sysid, F.OVS_FP64)
+            for mode, name in ((F.OVS_MIXED, "mixed"), (F.OVS_FP64, "fp64")):
                 barrier_()
                 sol, info = ctx.solve(sysid, mode, args.rtol, kspace=args.kspace, max_cycles=args.max_cycles)
                 barrier_()
-                rec[key] = {"s": maxr(info.seconds), "iterations": info.iterations, "cycles": info.cycles,
-                            "rel_residual": info.rel_residual, "converged": bool(info.converged)}
+                r = b - ctx.spmv(sysid, F.OVS_FP64, sol)
+                true_res[(name, key)] = float(np.linalg.norm(r) / max(np.linalg.norm(b), 1e-300))
+                gm.setdefault(name, {})[key] = {
+                    "s": maxr(info.seconds), "iterations": info.iterations, "cycles": info.cycles,
+                    "rel_residual_device": info.rel_residual, "converged": bool(info.converged),
+                    "true_rel_residual_fp64_system": true_res[(name, key)]}
                 sols[(name, key)] = sol
-            rec["s_per_solve"] = rec["nsvof"]["s"] + rec["tem"]["s"]
-            gm[name] = rec
+        for name in ("mixed", "fp64"):
+            gm[name]["s_per_solve"] = gm[name]["nsvof"]["s"] + gm[name]["tem"]["s"]
         gm["speedup_mixed_vs_fp64"] = gm["fp64"]["s_per_solve"] / gm["mixed"]["s_per_solve"]
         err = {}
         for key, names in (("nsvof", ["u", "v", "w", "p", "phi"]), ("tem", ["T"])):
-            a, b = sols[("mixed", key)], sols[("fp64", key)]
+            a, bb = sols[("mixed", key)], sols[("fp64", key)]
             for f, nm in enumerate(names):
-                err[nm] = float(np.abs(a[:, f] - b[:, f]).max() / max(np.abs(b[:, f]).max(), 1e-300))
+                err[nm] = float(np.abs(a[:, f] - bb[:, f]).max() / max(np.abs(bb[:, f]).max(), 1e-300))
         gm["max_rel_err_mixed_vs_fp64"] = err
         gm["rtol"] = args.rtol
         gm["kspace"] = args.kspace
+        gm["note"] = ("both modes solve the same FP64-assembled systems; the mixed time includes the FP32 "
+                      "rounding of the matrix and its preconditioner set-up; true residuals recomputed on the "
+                      "host from an FP64 SpMV of the returned solution")
+        if cpu is not None and "gmres" in cpu:
+            it64 = gm["fp64"]["nsvof"]["iterations"]
+            cpu["gmres"]["s_per_solve_extrapolated"] = cpu["gmres"]["s_per_iteration_workload"] * it64
+            cpu["gmres"]["extrapolation"] = (f"s/iteration at {N} nodes x the FP64 GPU solve's {it64} NS+VOF "
+                                             f"iterations (restarted GMRES({args.kspace}) to {args.rtol})")
 
     # ------------------------------------------------------------ e2e
     # public API with host buffers: upload the state the assembly reads from
-    # page-locked host memory, assemble all fields (FP32), read the residual back
+    # page-locked host memory, assemble all fields (FP64), read the residual back
     fields = ["dg", "dgold", "ug", "ugold", "acg", "acgold", "ugm", "ugmold", "pg", "phig", "phigold",
               "rphig", "rphigold", "tg", "tgold", "rtg", "rtgold"]
     host = {}
@@ -556,14 +609,15 @@ def run_ours(args, world, rank, local_rank, dist):
     d2h = out_ns.array.nbytes + out_t.array.nbytes
     import ctypes as C
     dp = C.POINTER(C.c_double)
+    P = F.OVS_FP64
 
     def e2e_step():
         for f in fields:
             F.check(ctx.lib.ovs_set_field(ctx.h, F.FIELD_ID[f], host[f].array.ctypes.data_as(dp)), f)
-        ctx.assemble(F.OVS_ASM_NSVOF, 6, F.OVS_FP32)
-        ctx.assemble(F.OVS_ASM_TEM, 6, F.OVS_FP32)
-        F.check(ctx.lib.ovs_get_rhs(ctx.h, F.OVS_SYS_NSVOF, F.OVS_FP32, out_ns.array.ctypes.data_as(dp)), "rhs")
-        F.check(ctx.lib.ovs_get_rhs(ctx.h, F.OVS_SYS_TEM, F.OVS_FP32, out_t.array.ctypes.data_as(dp)), "rhs")
+        ctx.assemble(F.OVS_ASM_NSVOF, 6, P)
+        ctx.assemble(F.OVS_ASM_TEM, 6, P)
+        F.check(ctx.lib.ovs_get_rhs(ctx.h, F.OVS_SYS_NSVOF, P, out_ns.array.ctypes.data_as(dp)), "rhs")
+        F.check(ctx.lib.ovs_get_rhs(ctx.h, F.OVS_SYS_TEM, P, out_t.array.ctypes.data_as(dp)), "rhs")
 
     def e2e_streamed(nsteps):
         # the same copies per step, overlapped with the assembly: step i+1's
@@ -574,10 +628,10 @@ def run_ours(args, world, rank, local_rank, dist):
             ctx.commit_staged()
             if i + 1 < nsteps:
                 ctx.stage_fields({f: host[f].array for f in fields})
-            ctx.assemble(F.OVS_ASM_NSVOF, 6, F.OVS_FP32)
-            ctx.assemble(F.OVS_ASM_TEM, 6, F.OVS_FP32)
-            ctx.get_rhs_async(F.OVS_SYS_NSVOF, F.OVS_FP32, out_ns.array)
-            ctx.get_rhs_async(F.OVS_SYS_TEM, F.OVS_FP32, out_t.array)
+            ctx.assemble(F.OVS_ASM_NSVOF, 6, P)
+            ctx.assemble(F.OVS_ASM_TEM, 6, P)
+            ctx.get_rhs_async(F.OVS_SYS_NSVOF, P, out_ns.array)
+            ctx.get_rhs_async(F.OVS_SYS_TEM, P, out_t.array)
         ctx.sync_copies()
 
     for _ in range(args.warmup):
@@ -596,34 +650,40 @@ def run_ours(args, world, rank, local_rank, dist):
     barrier_()
     clk = clocks.stop()
     total_launches = ctx.launch_count() - launches0
+    for pa in list(host.values()) + [out_ns, out_t]:
+        pa.free()
+    ctx.close()
+    cfg2 = None if (args.no_solve or args.no_config2) else run_config2(local_rank, args)
     adj = None if args.no_adjoint else run_adjoint(local_rank)
     hexr = None if args.no_hex else run_hex(local_rank, args)
 
     line = {
         "metric": METRIC, "value": value, "unit": "Melem/s", "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": ms_step, "higher_is_better": True, "scaling": "weak",
-        "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+        "vs_baseline": None, "dtype": "f64", "data": "synthetic",
         "config": {"workload": f"config3: NS+VOF+T quench assembly pass, {n}^3 cells x6 Kuhn tets "
-                               f"({E} tets, {N} nodes, {nnz} CSR slots), FP32 mixed path",
-                   "cache": f"inputs larger than L2 (FP32 CSR values alone {24 * nnz * 4 / 1e9:.2f} GB); no flush",
+                               f"({E} tets, {N} nodes, {nnz} CSR slots), FP64 (the reference's arithmetic)",
+                   "cache": f"inputs larger than L2 (FP64 CSR values alone {24 * nnz * 8 / 1e9:.2f} GB); no flush",
                    "parallelism": f"replicas x{world}" if world > 1 else "1 GPU"},
         "e2e": {"value": world * E / e2e_s / 1e6, "unit": "Melem/s", "h2d_bytes_per_step": h2d,
                 "d2h_bytes_per_step": d2h,
-                "mode": "streamed: every step's 17 fields copied from pinned host memory and its residual "
-                        "read back, overlapped with the neighbouring steps' assembly (ovs_stage_fields, "
+                "mode": "streamed: every step's 17 FP64 fields copied from pinned host memory and its FP64 "
+                        "residual read back, overlapped with the neighbouring steps' assembly (ovs_stage_fields, "
                         "ovs_commit_staged, ovs_get_rhs_async, ovs_sync_copies); all copies inside the timed "
                         "region",
                 "serial_value": world * E / e2e_serial_s / 1e6,
                 "serial_mode": "ovs_set_field x17, assemble, ovs_get_rhs x2, one after another"},
-        "gpu_launches": int(launches_step * args.steps),
+        "gpu_launches": int(nlaunch["fp64"]),
         "clocks": clk,
         "roofline": roof_asm,
+        "roofline_fp32_pass": roof_asm32,
         "roofline_spmv": roof_spmv,
-        "roofline_assembly_pass": roof_pass,
-        "assembly_melem_s": {"fp32": world * E / (res["fp32"]["ms"] * 1e-3) / 1e6,
-                             "fp64": world * E / (res["fp64"]["ms"] * 1e-3) / 1e6,
-                             "ms_fp32": res["fp32"]["ms"], "ms_fp64": res["fp64"]["ms"]},
+        "assembly_melem_s": {"fp64": world * E / (res["fp64"]["ms"] * 1e-3) / 1e6,
+                             "fp32": world * E / (res["fp32"]["ms"] * 1e-3) / 1e6,
+                             "ms_fp64": res["fp64"]["ms"], "ms_fp32": res["fp32"]["ms"],
+                             "launches_per_step": {k: v / args.steps for k, v in nlaunch.items()}},
         "gmres": gm,
+        "config2": cfg2,
         "adjoint": adj,
         "hex": hexr,
         "kernel_ms": prof,
@@ -634,9 +694,6 @@ def run_ours(args, world, rank, local_rank, dist):
         line["cpu_baseline"] = cpu
     if rank == 0:
         print(json.dumps(line), flush=True)
-    for pa in list(host.values()) + [out_ns, out_t]:
-        pa.free()
-    ctx.close()
 
 
 def main():
@@ -652,6 +709,7 @@ def main():
     ap.add_argument("--no-solve", action="store_true")
     ap.add_argument("--no-adjoint", action="store_true")
     ap.add_argument("--no-hex", action="store_true")
+    ap.add_argument("--no-config2", action="store_true")
     ap.add_argument("--hex-n", type=int, default=96, help="hex cells per side (config 4: 96)")
     ap.add_argument("--no-cpu", action="store_true")
     args = ap.parse_args()

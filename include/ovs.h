@@ -49,7 +49,10 @@ enum {
 };
 
 /* ------------------------------------------------------------- selectors */
-enum { OVS_FP64 = 0, OVS_FP32 = 1 };
+/* Storage precisions of the assembled systems (and of an assembly pass).
+ * OVS_MIXED is a solve mode only (ovs_solve, ovs_newton_opts.mode): the FP64
+ * system solved with an FP32 inner Krylov method, see ovs_solve. */
+enum { OVS_FP64 = 0, OVS_FP32 = 1, OVS_MIXED = 2 };
 
 /* assembly kernels (the reference element routines they replace) */
 enum {
@@ -190,6 +193,13 @@ int ovs_upload_mesh(ovs_ctx* ctx, const double* xg, const int* ien,
 int ovs_build_pattern(ovs_ctx* ctx, int* icnt);
 /* copy the pattern out (1-based, reference layout), col(N+1), row(icnt) */
 int ovs_get_pattern(ovs_ctx* ctx, int* col, int* row);
+/* The element-slot -> CSR-slot map the assembly scatters through: lmap is
+ * (NELEM, nshl, nshl) column-major, lmap(e,a,b) = the 1-based slot k that
+ * FillSparseMat_3D adds element entry (a, b) of element e to,
+ * k = SparseMatLoc_3D(row(c:c+n-1), n, IEN(e,b)) + c - 1 with
+ * c = col(IEN(e,a)), n = col(IEN(e,a)+1) - c (src/FillSparseMat.f90:4-28,
+ * 47-57).  Computed once by ovs_build_pattern. */
+int ovs_get_slot_map(ovs_ctx* ctx, int* lmap);
 
 int ovs_set_params(ovs_ctx* ctx, const ovs_params* p);
 /* IBC(N,nibc) column-major, entries 0/1 (src/setBCs.f90:183-187: columns
@@ -351,10 +361,21 @@ int ovs_gmres(ovs_ctx* ctx, int system, double tol, int kspace,
 
 /* Solve A x = b to ||b - A x||_2 <= rtol ||b||_2 (true residual, FP64).
  * mode OVS_FP64: restarted FP64 GMRES(kspace) on the FP64 system.
- * mode OVS_FP32: mixed precision - FP32 system and FP32 Krylov basis inside,
- * FP64 Gram-Schmidt dots / Givens / back-substitution, FP64 iterative
- * refinement residual r = b - A x.  The solution stays on the device
- * (ovs_newton_update applies it); sol (host, may be NULL) receives a copy. */
+ * mode OVS_MIXED: the FP64 system (needs an FP64 assembly of `system`) by
+ *   iterative refinement: the refinement residual r = b - A x is formed with
+ *   the FP64 matrix and right-hand side, and each correction is a GMRES cycle
+ *   on the FP32 rounding of that matrix (FP32 values, preconditioner, SpMV
+ *   and Krylov basis; FP64 Gram-Schmidt dots, Givens rotations and
+ *   back-substitution).  The rounding is written into the FP32 matrix of
+ *   `system` (overwriting an FP32 assembly) inside the timed solve.  The
+ *   solution converges to the FP64 system's, not to an FP32-assembled one.
+ * mode OVS_FP32: the same scheme on the FP32-assembled system alone (matrix
+ *   and right-hand side assembled in FP32; the refinement residual in FP64
+ *   arithmetic on those FP32 values): it converges to the solution of the
+ *   FP32-assembled system, which differs from the FP64 system's by the
+ *   FP32 assembly's rounding times the condition number.
+ * The solution stays on the device (ovs_newton_update applies it); sol
+ * (host, may be NULL) receives a copy. */
 int ovs_solve(ovs_ctx* ctx, int system, int mode, double rtol, int kspace,
               int max_cycles, double* sol, ovs_solve_info* info);
 
@@ -384,8 +405,10 @@ int ovs_residual_norms(ovs_ctx* ctx, int precision, double r[4]);
  * of all fields and stop when every field passes check_convergence (:190-215:
  * residual < utol * residual0 or residual < atol, sums of squares as
  * calculate_residual).  mode OVS_FP64: FP64 assembly and the reference GMRES
- * cycle (tol, kspace, kspace_min, zero start); OVS_FP32: FP32 assembly and
- * the mixed-precision refined solve to relative residual tol (max_cycles).
+ * cycle (tol, kspace, kspace_min, zero start); OVS_MIXED: FP64 assembly and
+ * residuals, every solve by ovs_solve's OVS_MIXED refinement to relative
+ * residual tol (max_cycles); OVS_FP32: FP32 assembly and residuals, every
+ * solve by ovs_solve's OVS_FP32 refinement.
  * The predictor of driver.f90:83-85 and the BC producers stay with the
  * caller (set the fields and IBC before the call).  Only the 4 residual
  * norms per iteration travel to the host. */
@@ -430,6 +453,9 @@ int ovs_commit_old(ovs_ctx* ctx, int update_vof_tem_old);
  * compute-side roofline denominator of the CUDA-core assembly kernels);
  * no reference counterpart (a measurement helper). */
 int ovs_measure_fp32_peak(ovs_ctx* ctx, double* tflops);
+/* The same for FP64 FMAs (the FP64 assembly kernels' compute-side
+ * denominator); no reference counterpart (a measurement helper). */
+int ovs_measure_fp64_peak(ovs_ctx* ctx, double* tflops);
 
 enum { OVS_PROF_SPMV = 1, OVS_PROF_ASSEMBLE = 2, OVS_PROF_ARNOLDI = 3, OVS_PROF_ARNOLDI_FUSED = 4,
        OVS_PROF_ASSEMBLE_ELEMENTS = 5, OVS_PROF_ASSEMBLE_ROWS = 6 };

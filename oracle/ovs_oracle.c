@@ -90,6 +90,22 @@ int orc_sparse_mat_loc(const int* list, int n, int goal) {
   return lo;
 }
 
+/* The global slots FillSparseMat_3D scatters element entry (a, b) to
+ * (src/FillSparseMat.f90:47-57): i = IEN(e,a), c = col(i), n = col(i+1) - c,
+ * locn = SparseMatLoc_3D(row(c:c+n-1), n, IEN(e,b)), k = locn + c - 1.
+ * lmap is (nelem, nshl, nshl) column-major, 1-based k. */
+void orc_slot_map(int nelem, int nshl, const int* ien, const int* col, const int* row, int* lmap) {
+  for (int e = 0; e < nelem; ++e)
+    for (int a = 0; a < nshl; ++a) {
+      const int i = ien[cm(e, nelem, a)];
+      const int c = col[i - 1], n = col[i] - c;
+      for (int b = 0; b < nshl; ++b) {
+        const int locn = orc_sparse_mat_loc(row + (c - 1), n, ien[cm(e, nelem, b)]);
+        lmap[(size_t)e + (size_t)nelem * ((size_t)a + (size_t)nshl * b)] = locn + c - 1;
+      }
+    }
+}
+
 /* ----------------------------------------------------------------------
  * Quadrature: genGPandGWtetpri src/genGP_GW.f90:317-431 (tet 4-pt, hex 8-pt)
  * -------------------------------------------------------------------- */

@@ -60,6 +60,9 @@ typedef struct orc_system {
 int orc_gen_spar_struc(int nnode, int nelem, int nshl, const int* ien,
                        int* col, int* row, int* icnt);
 int orc_sparse_mat_loc(const int* list, int n, int goal);
+/* k(e,a,b) of FillSparseMat_3D for every element entry: (nelem,nshl,nshl)
+ * column-major, 1-based global CSR slots */
+void orc_slot_map(int nelem, int nshl, const int* ien, const int* col, const int* row, int* lmap);
 
 /* full assembly drivers (alpha stage + zeroing + element loop) */
 double orc_assemble_navsto(const orc_mesh* m, const ovs_params* p,

@@ -71,6 +71,8 @@ def load():
     lib.orc_eval_shape.argtypes = [C.c_int, C.c_int, _dp, _dp, _dp, _dp, _dp, _dp]
     lib.orc_eval_shape.restype = C.c_double
     lib.orc_sparse_mat_loc.argtypes = [_ip, C.c_int, C.c_int]
+    lib.orc_slot_map.argtypes = [C.c_int, C.c_int, _ip, _ip, _ip, _ip]
+    lib.orc_slot_map.restype = None
     for fn in ("orc_assemble_navsto",):
         getattr(lib, fn).argtypes = [C.POINTER(OrcMesh), pp, C.POINTER(OrcState), C.POINTER(OrcSystem), C.c_int]
         getattr(lib, fn).restype = C.c_double
@@ -120,6 +122,19 @@ def gen_spar_struc(ien: np.ndarray, nnode: int):
     st = lib.orc_gen_spar_struc(nnode, E, nshl, _i(ien), _i(col), _i(row), C.byref(icnt))
     assert st == 0, st
     return col, row[: icnt.value]
+
+
+def slot_map(ien: np.ndarray, col: np.ndarray, row: np.ndarray) -> np.ndarray:
+    """k(e, a, b) of FillSparseMat_3D (src/FillSparseMat.f90:47-57) for
+    every element entry: (E, nshl, nshl) Fortran-order int32, 1-based."""
+    lib = load()
+    ien = np.asfortranarray(ien, dtype=np.int32)
+    E, nshl = ien.shape
+    col = np.ascontiguousarray(col, dtype=np.int32)
+    row = np.ascontiguousarray(row, dtype=np.int32)
+    out = np.zeros((E, nshl, nshl), dtype=np.int32, order="F")
+    lib.orc_slot_map(E, nshl, _i(ien), _i(col), _i(row), _i(out))
+    return out
 
 
 def eval_shape(nshl: int, igp: int, xl: np.ndarray, dl: np.ndarray | None = None):

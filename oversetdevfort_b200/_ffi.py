@@ -24,7 +24,7 @@ OVS_ERR_PATTERN = -6
 OVS_ERR_NODEVICE = -7
 OVS_ERR_TIMEOUT = -8
 
-OVS_FP64, OVS_FP32 = 0, 1
+OVS_FP64, OVS_FP32, OVS_MIXED = 0, 1, 2
 OVS_ASM_NS, OVS_ASM_NSVOF, OVS_ASM_TEM = 1, 2, 3
 OVS_SYS_NS, OVS_SYS_NSVOF, OVS_SYS_TEM = 1, 2, 3
 OVS_TENSOR_VEC, OVS_TENSOR_MAT = 2, 4
@@ -49,13 +49,13 @@ FIELD_WIDTH = {n: (3 if i <= FIELD_ID["acgmold"] else 1) for n, i in FIELD_ID.it
 EXPORTS = [
     "ovs_params_genalpha", "ovs_version", "ovs_status_string", "ovs_gen_spar_struc",
     "ovs_create", "ovs_destroy", "ovs_synchronize", "ovs_get_stream", "ovs_upload_mesh",
-    "ovs_build_pattern", "ovs_get_pattern", "ovs_set_params", "ovs_set_ibc", "ovs_set_field",
+    "ovs_build_pattern", "ovs_get_pattern", "ovs_get_slot_map", "ovs_set_params", "ovs_set_ibc", "ovs_set_field",
     "ovs_get_field", "ovs_assemble", "ovs_get_rhs", "ovs_set_rhs", "ovs_get_lhs_block",
     "ovs_set_lhs_block", "ovs_spmv", "ovs_gmres", "ovs_solve", "ovs_newton_update", "ovs_set_solution", "ovs_predictor", "ovs_commit_old",
     "ovs_residual_norms", "ovs_profile", "ovs_launch_count", "ovs_last_device_ms",
     "ovs_host_alloc", "ovs_host_free", "ovs_residual_vjp", "ovs_gmres_transposed", "ovs_quench_newton",
     "ovs_quench_time_steps", "ovs_stage_fields", "ovs_commit_staged", "ovs_get_rhs_async", "ovs_sync_copies",
-    "ovs_build_precond", "ovs_spmv_device", "ovs_precond_device", "ovs_measure_fp32_peak", "ovs_set_option", "ovs_set_faces", "ovs_check_faces", "ovs_set_bc_spec", "ovs_check_bc_spec", "ovs_assemble_async", "ovs_assemble_wait", "ovs_apply_bcs", "ovs_get_ibc",
+    "ovs_build_precond", "ovs_spmv_device", "ovs_precond_device", "ovs_measure_fp32_peak", "ovs_measure_fp64_peak", "ovs_set_option", "ovs_set_faces", "ovs_check_faces", "ovs_set_bc_spec", "ovs_check_bc_spec", "ovs_assemble_async", "ovs_assemble_wait", "ovs_apply_bcs", "ovs_get_ibc",
     "ovs_gmres_tem_noalloc",
 ]
 
@@ -131,6 +131,7 @@ def load(path: str | os.PathLike | None = None) -> C.CDLL:
         "ovs_upload_mesh": ([vp, dp, ip, ip], C.c_int),
         "ovs_build_pattern": ([vp, ip], C.c_int),
         "ovs_get_pattern": ([vp, ip, ip], C.c_int),
+        "ovs_get_slot_map": ([vp, ip], C.c_int),
         "ovs_set_params": ([vp, C.POINTER(OvsParams)], C.c_int),
         "ovs_set_ibc": ([vp, ip, C.c_int], C.c_int),
         "ovs_set_faces": ([vp, C.c_int, ip, ip, ip, dp, dp], C.c_int),
@@ -144,6 +145,7 @@ def load(path: str | os.PathLike | None = None) -> C.CDLL:
         "ovs_spmv_device": ([vp, C.c_int, C.c_int, C.c_int, vp, vp], C.c_int),
         "ovs_precond_device": ([vp, C.c_int, C.c_int, vp, vp], C.c_int),
         "ovs_measure_fp32_peak": ([vp, dp], C.c_int),
+        "ovs_measure_fp64_peak": ([vp, dp], C.c_int),
         "ovs_set_bc_spec": ([vp, C.POINTER(OvsBcSpec)], C.c_int),
         "ovs_check_bc_spec": ([C.POINTER(OvsBcSpec), C.c_int], C.c_int),
         "ovs_apply_bcs": ([vp, C.c_int], C.c_int),

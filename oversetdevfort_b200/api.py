@@ -127,6 +127,13 @@ class Context:
         F.check(self.lib.ovs_get_pattern(self.h, _iptr(col), _iptr(row)), "ovs_get_pattern")
         return col, row[: self.icnt]
 
+    def get_slot_map(self) -> np.ndarray:
+        """k(e, a, b) of FillSparseMat_3D for every element entry: (E, nshl,
+        nshl) Fortran-order int32, 1-based CSR slots (ovs_get_slot_map)."""
+        out = np.zeros((self.E, self.nshl, self.nshl), dtype=np.int32, order="F")
+        F.check(self.lib.ovs_get_slot_map(self.h, _iptr(out)), "ovs_get_slot_map")
+        return out
+
     # ---------------------------------------------------------- parameters
     def set_params(self, p: dict):
         self.params = dict(p)
@@ -283,6 +290,10 @@ class Context:
 
     def solve(self, system: int, mode: int, rtol: float, kspace: int = 50, max_cycles: int = 100,
               want_solution: bool = True):
+        """ovs_solve: drive ||b - A x|| / ||b|| to rtol.  mode OVS_FP64
+        (restarted FP64 GMRES), OVS_MIXED (the FP64 system refined with FP32
+        inner cycles on the rounded FP64 matrix) or OVS_FP32 (the
+        FP32-assembled system).  Returns (solution or None, OvsSolveInfo)."""
         info = F.OvsSolveInfo()
         s = np.zeros((self.N, NF[system]), order="F") if want_solution else None
         F.check(self.lib.ovs_solve(self.h, system, mode, rtol, kspace, max_cycles,
@@ -387,6 +398,12 @@ class Context:
         """Measured FP32 FMA throughput of the device, TFLOP/s."""
         t = C.c_double(0.0)
         F.check(self.lib.ovs_measure_fp32_peak(self.h, C.byref(t)), "ovs_measure_fp32_peak")
+        return t.value
+
+    def measure_fp64_peak(self) -> float:
+        """Measured FP64 FMA throughput of the device, TFLOP/s."""
+        t = C.c_double(0.0)
+        F.check(self.lib.ovs_measure_fp64_peak(self.h, C.byref(t)), "ovs_measure_fp64_peak")
         return t.value
 
     def launch_count(self) -> int:

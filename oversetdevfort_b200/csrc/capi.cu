@@ -343,6 +343,14 @@ int ovs_get_pattern(ovs_ctx* c, int* col, int* row) {
   return ovs_pattern_to_host(c, col, row);
 }
 
+int ovs_get_slot_map(ovs_ctx* c, int* lmap) {
+  if (!c || !lmap) return OVS_ERR_ARG;
+  if (!c->have_pattern || !c->n2s) return OVS_ERR_STATE;
+  int st;
+  if ((st = ovs_activate(c))) return st;
+  return ovs_slot_map_to_host(c, lmap);
+}
+
 int ovs_gen_spar_struc(int nnode, int nelem, int nshl, const int* ien, int* col, int* row, int* icnt) {
   if (!ien || !col || !icnt) return OVS_ERR_ARG;
   ovs_dims d = {nnode, nelem, nshl, 0};
@@ -678,6 +686,7 @@ int ovs_gmres(ovs_ctx* c, int sys, double tol, int kspace, int kspace_min, doubl
 
 int ovs_solve(ovs_ctx* c, int sys, int mode, double rtol, int kspace, int max_cycles, double* sol,
               ovs_solve_info* info) {
+  if (mode != OVS_FP64 && mode != OVS_FP32 && mode != OVS_MIXED) return OVS_ERR_ARG;
   if (!sys_ok(c, sys, mode == OVS_FP32 ? OVS_FP32 : OVS_FP64)) return OVS_ERR_ARG;
   if (kspace < 1 || kspace > OVS_MAX_KSPACE || max_cycles < 1 || !(rtol > 0.0)) return OVS_ERR_ARG;
   int st;
@@ -771,35 +780,38 @@ int ovs_profile(ovs_ctx* c, int what, int system, int precision, int reps, doubl
   return ovs_profile_krylov(c, what, system, precision, reps, avg_ms);
 }
 
-// FP32 FMA throughput of the device: 8 independent chains per thread,
-// 4 blocks of 256 threads per SM; the compute-side roofline denominator of
-// the assembly kernels (their work is FP32 arithmetic on the CUDA cores).
-__global__ void __launch_bounds__(256) fma_peak_kernel(float* out, int iters, float seed) {
-  float a[8];
+// FMA throughput of the device in T (float or double): 8 independent chains
+// per thread, 4 blocks of 256 threads per SM; the compute-side roofline
+// denominators of the assembly kernels (their work is FP32 or FP64
+// arithmetic on the CUDA cores).
+extern "C++" {
+template <typename T>
+__global__ void __launch_bounds__(256) fma_peak_kernel(T* out, int iters, T seed) {
+  T a[8];
 #pragma unroll
-  for (int k = 0; k < 8; ++k) a[k] = seed + 1e-7f * (float)threadIdx.x + (float)k;
-  const float m = 1.0000001f, b = 1e-7f;
+  for (int k = 0; k < 8; ++k) a[k] = seed + (T)1e-7 * (T)threadIdx.x + (T)k;
+  const T m = (T)1.0000001, b = (T)1e-7;
   for (int i = 0; i < iters; ++i) {
 #pragma unroll
-    for (int k = 0; k < 8; ++k) a[k] = fmaf(a[k], m, b);
+    for (int k = 0; k < 8; ++k) a[k] = fma(a[k], m, b);
   }
-  float s = 0.f;
+  T s = 0;
 #pragma unroll
   for (int k = 0; k < 8; ++k) s += a[k];
   if (threadIdx.x == 0) out[blockIdx.x] = s;
 }
 
-int ovs_measure_fp32_peak(ovs_ctx* c, double* tflops) {
-  if (!c || !tflops) return OVS_ERR_ARG;
+template <typename T>
+static int measure_fma_peak(ovs_ctx* c, int iters, double* tflops) {
   int st;
   if ((st = ovs_activate(c))) return st;
-  const int blocks = 4 * c->num_sms, iters = 1 << 14;
-  float* out = nullptr;
-  OVS_CUDA_TRY(cudaMallocAsync(&out, sizeof(float) * blocks, c->stream));
-  for (int w = 0; w < 3; ++w) fma_peak_kernel<<<blocks, 256, 0, c->stream>>>(out, iters, 1.0f);
+  const int blocks = 4 * c->num_sms;
+  T* out = nullptr;
+  OVS_CUDA_TRY(cudaMallocAsync(&out, sizeof(T) * blocks, c->stream));
+  for (int w = 0; w < 3; ++w) fma_peak_kernel<T><<<blocks, 256, 0, c->stream>>>(out, iters, (T)1);
   OVS_CUDA_TRY(cudaEventRecord(c->ev0, c->stream));
   const int reps = 10;
-  for (int r = 0; r < reps; ++r) fma_peak_kernel<<<blocks, 256, 0, c->stream>>>(out, iters, 1.0f);
+  for (int r = 0; r < reps; ++r) fma_peak_kernel<T><<<blocks, 256, 0, c->stream>>>(out, iters, (T)1);
   OVS_CUDA_TRY(cudaEventRecord(c->ev1, c->stream));
   c->launches += 3 + reps;
   OVS_CUDA_TRY(cudaGetLastError());
@@ -811,6 +823,17 @@ int ovs_measure_fp32_peak(ovs_ctx* c, double* tflops) {
   const double flops = 2.0 * 8.0 * iters * 256.0 * blocks * reps;
   *tflops = flops / (ms * 1e-3) / 1e12;
   return OVS_OK;
+}
+}  // extern "C++"
+
+int ovs_measure_fp32_peak(ovs_ctx* c, double* tflops) {
+  if (!c || !tflops) return OVS_ERR_ARG;
+  return measure_fma_peak<float>(c, 1 << 14, tflops);
+}
+
+int ovs_measure_fp64_peak(ovs_ctx* c, double* tflops) {
+  if (!c || !tflops) return OVS_ERR_ARG;
+  return measure_fma_peak<double>(c, 1 << 13, tflops);
 }
 
 int ovs_launch_count(ovs_ctx* c, long long* n) {
@@ -881,12 +904,13 @@ int ovs_gmres_transposed(ovs_ctx* c, int sys, const double* rhs, double tol, int
 
 // solmultiphasethermofluid_stag (src/solveFlow.f90:4-164) on the context
 int ovs_quench_newton(ovs_ctx* c, const ovs_newton_opts* o, ovs_newton_info* info) {
-  if (!c || !o || (o->mode != OVS_FP64 && o->mode != OVS_FP32) || o->newton_max < 0) return OVS_ERR_ARG;
+  if (!c || !o || (o->mode != OVS_FP64 && o->mode != OVS_FP32 && o->mode != OVS_MIXED) || o->newton_max < 0)
+    return OVS_ERR_ARG;
   if (o->kspace < 1 || o->kspace > OVS_MAX_KSPACE || o->max_cycles < 1) return OVS_ERR_ARG;
   int st;
   if ((st = ovs_activate(c))) return st;
   const auto t0 = std::chrono::steady_clock::now();
-  const int prec = o->mode;
+  const int prec = o->mode == OVS_FP32 ? OVS_FP32 : OVS_FP64;   // assembly and residual precision
   ovs_newton_info ni;
   memset(&ni, 0, sizeof(ni));
   auto check = [&](const double* r) {   // check_convergence, all three field groups
@@ -900,7 +924,7 @@ int ovs_quench_newton(ovs_ctx* c, const ovs_newton_opts* o, ovs_newton_info* inf
   auto solve = [&](int sys, double tol, int* its) -> int {
     const size_t n = (size_t)c->N * ovs_sys_nf(sys);
     int s2;
-    if (prec == OVS_FP64) {
+    if (o->mode == OVS_FP64) {
       if ((s2 = ovs_ensure((void**)&c->sol[sys], sizeof(double) * 5 * (size_t)c->N))) return s2;
       OVS_CUDA_TRY(cudaMemsetAsync(c->sol[sys], 0, sizeof(double) * n, c->stream));
       ovs_gmres_info gi;
@@ -910,7 +934,7 @@ int ovs_quench_newton(ovs_ctx* c, const ovs_newton_opts* o, ovs_newton_info* inf
     } else {
       ovs_solve_info si;
       memset(&si, 0, sizeof(si));
-      if ((s2 = ovs_solve_impl(c, sys, OVS_FP32, tol, o->kspace, o->max_cycles, &si))) return s2;
+      if ((s2 = ovs_solve_impl(c, sys, o->mode, tol, o->kspace, o->max_cycles, &si))) return s2;
       *its += si.iterations;
     }
     return ovs_newton_update(c, sys);

@@ -1268,10 +1268,17 @@ int ovs_gmres_ref_impl(ovs_ctx* c, int sys, double tol, int kspace, int kmin, do
 }
 
 // Restarted / iteratively refined solve to a true FP64 relative residual.
+// `outer` is the system whose residual b - A x is driven to rtol (matrix and
+// right-hand side of that precision, FP64 arithmetic), `inner` the matrix
+// precision of the GMRES cycles that compute the corrections:
+//   OVS_FP64  outer FP64, inner FP64 (restarted GMRES);
+//   OVS_MIXED outer FP64, inner FP32 = the rounding of the FP64 matrix;
+//   OVS_FP32  outer FP32, inner FP32 (the FP32-assembled system).
 int ovs_solve_impl(ovs_ctx* c, int sys, int mode, double rtol, int kspace, int max_cycles,
                    ovs_solve_info* info) {
-  const int prec = mode == OVS_FP32 ? OVS_FP32 : OVS_FP64;
-  SysStore& S = c->sys[sys][prec];
+  const int outer = mode == OVS_FP32 ? OVS_FP32 : OVS_FP64;
+  const int prec = mode == OVS_FP64 ? OVS_FP64 : OVS_FP32;   // inner
+  SysStore& S = c->sys[sys][outer];
   if (!S.vals || !S.rhs) return OVS_ERR_STATE;
   const int N = c->N, nf = ovs_sys_nf(sys);
   const size_t n = (size_t)N * nf;
@@ -1283,8 +1290,19 @@ int ovs_solve_impl(ovs_ctx* c, int sys, int mode, double rtol, int kspace, int m
   double* b = c->work64;
   double* r = c->work64 + 5 * (size_t)N;
   OVS_CUDA_TRY(cudaEventRecord(c->ev0, s));
+  if (mode == OVS_MIXED) {
+    // the inner operator: FP32 rounding of the FP64 matrix values
+    SysStore& S32 = c->sys[sys][OVS_FP32];
+    const size_t nv = (size_t)c->nnz * ovs_sys_nv(sys);
+    if ((st = ovs_ensure(&S32.vals, sizeof(float) * nv))) return st;
+    convert_kernel<double, float><<<ovs_grid(nv, 256, 16 * c->num_sms), 256, 0, s>>>(
+        as<double>(S.vals), reinterpret_cast<float*>(S32.vals), nv);
+    ++c->launches;
+    OVS_CUDA_TRY(cudaGetLastError());
+    S32.have_mat = true;
+  }
   if ((st = ovs_precond_setup(c, sys, prec))) return st;
-  if (prec == OVS_FP64) {
+  if (outer == OVS_FP64) {
     OVS_CUDA_TRY(cudaMemcpyAsync(b, S.rhs, sizeof(double) * n, cudaMemcpyDeviceToDevice, s));
   } else {
     convert_kernel<float, double><<<ovs_grid(n, 256, 4096), 256, 0, s>>>(as<float>(S.rhs), b, n);
@@ -1308,8 +1326,8 @@ int ovs_solve_impl(ovs_ctx* c, int sys, int mode, double rtol, int kspace, int m
     if (st) return st;
     iters += gi.iterations;
     ++cycles;
-    // r = b - A x in FP64 arithmetic
-    if (prec == OVS_FP64) st = launch_spmv<double, double, double, 2>(c, sys, as<double>(S.vals), x, r, nullptr, b, nullptr);
+    // r = b - A x in FP64 arithmetic, with the outer system's matrix
+    if (outer == OVS_FP64) st = launch_spmv<double, double, double, 2>(c, sys, as<double>(S.vals), x, r, nullptr, b, nullptr);
     else st = launch_spmv<float, double, double, 2>(c, sys, as<float>(S.vals), x, r, nullptr, b, nullptr);
     if (st) return st;
     double rr;

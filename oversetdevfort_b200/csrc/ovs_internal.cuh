@@ -167,6 +167,7 @@ int ovs_activate(ovs_ctx* c);
 // pattern.cu
 int ovs_pattern_build(ovs_ctx* c);
 int ovs_pattern_to_host(ovs_ctx* c, int* col, int* row);
+int ovs_slot_map_to_host(ovs_ctx* c, int* lmap);
 
 // assemble.cu
 int ovs_assemble_impl(ovs_ctx* c, int kernel, int tensor_flag, int prec,

@@ -215,6 +215,28 @@ __global__ void slot_map8_kernel(const int* __restrict__ ien, int N, const int* 
   }
 }
 
+// Global 1-based CSR slot k(e, a, b) of every element entry, from the slot
+// map: the n2e entry (e, a) of row A = IEN(e, a) holds the in-row offsets of
+// the element's nodes, so k = rowptr[A] + offset_b + 1.  Every (e, a) occurs
+// exactly once in the node-to-element lists.  lmap is (E, nshl, nshl)
+// column-major, the index order of FillSparseMat_3D's (a, b) loops.
+__global__ void slot_export_kernel(int N, int E, int nshl, const int* __restrict__ n2e_ptr,
+                                   const int* __restrict__ n2e, const unsigned* __restrict__ n2s,
+                                   const int* __restrict__ rowptr, int* __restrict__ lmap) {
+  const int A = blockIdx.x * blockDim.x + threadIdx.x;
+  if (A >= N) return;
+  const int rp1 = rowptr[A] + 1;
+  const int words = nshl == 8 ? 2 : 1;
+  for (int k = n2e_ptr[A]; k < n2e_ptr[A + 1]; ++k) {
+    const int e = n2e[k] >> 3, a = n2e[k] & 7;
+    for (int b = 0; b < nshl; ++b) {
+      const unsigned w = n2s[(size_t)k * words + (b >> 2)];
+      const int off = (int)((w >> (8 * (b & 3))) & 0xffu);
+      lmap[(size_t)e + (size_t)E * ((size_t)a + (size_t)nshl * b)] = rp1 + off;
+    }
+  }
+}
+
 __global__ void to_one_based_kernel(const int* __restrict__ in, int* __restrict__ out, size_t n) {
   size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x;
   if (i < n) out[i] = in[i] + 1;
@@ -235,6 +257,21 @@ int ovs_pattern_to_host(ovs_ctx* c, int* col, int* row) {
     ++c->launches;
     OVS_CUDA_TRY(cudaMemcpyAsync(row, tmp, sizeof(int) * n2, cudaMemcpyDeviceToHost, s));
   }
+  OVS_CUDA_TRY(cudaFreeAsync(tmp, s));
+  OVS_CUDA_TRY(cudaStreamSynchronize(s));
+  return OVS_OK;
+}
+
+int ovs_slot_map_to_host(ovs_ctx* c, int* lmap) {
+  cudaStream_t s = c->stream;
+  const size_t n = (size_t)c->E * c->nshl * c->nshl;
+  int* tmp = nullptr;
+  OVS_CUDA_TRY(cudaMallocAsync(&tmp, sizeof(int) * (n > 0 ? n : 1), s));
+  slot_export_kernel<<<ovs_grid(c->N, 128, 1 << 30), 128, 0, s>>>(c->N, c->E, c->nshl, c->n2e_ptr, c->n2e,
+                                                                 c->n2s, c->rowptr, tmp);
+  ++c->launches;
+  OVS_CUDA_TRY(cudaGetLastError());
+  if (n) OVS_CUDA_TRY(cudaMemcpyAsync(lmap, tmp, sizeof(int) * n, cudaMemcpyDeviceToHost, s));
   OVS_CUDA_TRY(cudaFreeAsync(tmp, s));
   OVS_CUDA_TRY(cudaStreamSynchronize(s));
   return OVS_OK;

@@ -1,7 +1,8 @@
-"""The bench's readers of the committed ncu summaries (CPU): the DRAM
-traffic and the executed FP32 flops per tet that bench.py puts into its
-roofline entries come out of profiles/ with the expected values, and a
-missing summary is reported rather than guessed."""
+"""bench.py's helpers (CPU): the reader of the committed ncu summaries (the
+DRAM traffic per tet of its roofline entry, every kernel of a pass added;
+a missing summary reported rather than guessed), the algorithmic bytes of
+the scope table, the reference arm's slabs (every cell layer of the
+workload exactly once) and its JSON line."""
 import os
 import sys
 
@@ -12,20 +13,43 @@ import bench  # noqa: E402
 
 
 def test_dram_traffic_per_tet_from_profile():
-    per_tet, src = bench.ncu_traffic_per_tet("assemble_rows_kernel_quench128_dram.md", 12582912)
-    assert per_tet is not None and "profiles/assemble_rows_kernel_quench128_dram.md" in src
-    # 8.28 GB per launch of the 128^3 case
-    assert abs(per_tet * 12582912 / 1e9 - 8.28) < 0.01
+    # assemble_rows_kernel_quench48.md: one kernel, 397.439488 MB read and
+    # 146.457856 MB written on the 663,552-tet case
+    per_tet, src = bench.ncu_dram_per_tet("assemble_rows_kernel_quench48.md", 663552)
+    assert per_tet is not None and "profiles/assemble_rows_kernel_quench48.md" in src
+    assert abs(per_tet * 663552 - (397.439488e6 + 146.457856e6)) < 1.0
 
 
-def test_fp32_flops_per_tet_from_profile():
-    per_tet, src = bench.ncu_flops_per_tet("assemble_rows_kernel_quench48_flops.md", 663552)
-    assert per_tet == 4948.0 and "FFMA" in src
+def test_dram_traffic_adds_every_kernel_of_a_summary(tmp_path, monkeypatch):
+    prof = tmp_path / "profiles"
+    prof.mkdir()
+    (prof / "two.md").write_text("| `dram__bytes_read.sum` | 1.5 Mbyte |\n| `dram__bytes_write.sum` | 500 Kbyte |\n"
+                                 "| `dram__bytes_read.sum` | 2 Gbyte |\n| `dram__bytes_write.sum` | 10 byte |\n")
+    monkeypatch.setattr(bench, "ROOT", tmp_path)
+    per_tet, _ = bench.ncu_dram_per_tet("two.md", 10)
+    assert abs(per_tet * 10 - (1.5e6 + 5e5 + 2e9 + 10)) < 1e-3
 
 
 def test_missing_summaries_are_reported():
-    assert bench.ncu_traffic_per_tet("no_such_summary.md", 1) == (None, "no ncu summary")
-    assert bench.ncu_flops_per_tet("no_such_summary.md", 1) == (None, "no ncu summary")
+    per_tet, why = bench.ncu_dram_per_tet("no_such_summary.md", 1)
+    assert per_tet is None and "no ncu summary" in why
+
+
+def test_algorithmic_bytes_of_the_scope_table():
+    """The pass and SpMV bytes at config 3 (128^3 x6 tets): NS+VOF assembly
+    6.80 GB in FP64 and 3.51 GB in FP32; preconditioned SpMV 3.37 GB FP32."""
+    E, N, nnz = 12582912, 2146689, 31802497
+    assert abs(bench.assembly_pass_bytes(E, N, nnz, 8) / 1e9 - 6.80) < 0.005
+    assert abs(bench.assembly_pass_bytes(E, N, nnz, 4) / 1e9 - 3.507) < 0.001
+    assert abs(bench.spmv_bytes(N, nnz, 4) / 1e9 - 3.37) < 0.01
+
+
+def test_reference_slabs_cover_the_workload():
+    for n, parts in ((128, 16), (128, 12), (16, 32), (7, 3), (1, 1)):
+        sl = bench.slab_layers(n, parts)
+        assert sum(nl for _, nl in sl) == n and sl[0][0] == 0
+        assert all(k0 + nl == sl[i + 1][0] for i, (k0, nl) in enumerate(sl[:-1]))
+        assert max(nl for _, nl in sl) - min(nl for _, nl in sl) <= 1 and min(nl for _, nl in sl) >= 1
 
 
 def test_reference_arm_counts_usable_cores():

@@ -85,3 +85,76 @@ def test_device_time_steps_match_host_driver():
     assert kt > 0
     a.close()
     b.close()
+
+
+def _stirred_case(name):
+    """A quench box with a seeded random velocity off the walls, so every
+    Newton iteration has convective and stabilisation work to do."""
+    case = M.quench_case(M.box_tet(6, 6, 8, 1.0, 1.0, 1.25), name)
+    rng = np.random.default_rng(3)
+    free = np.asarray(case.ibc)[:, 0] == 0
+    for f in ("ug", "ugold"):
+        case.state[f][free] = 0.05 * rng.standard_normal((int(free.sum()), 3))
+    return case
+
+
+NEWTON = dict(newton_max=3, solve_tem=True, kspace=150, kspace_min=1, tol_ns=1e-8, tol_tem=1e-8,
+              utol=(1e-6,) * 4, atol=(1e-30,) * 4)
+
+
+def _close(gpu, ref, tol, what):
+    scale = max(np.abs(ref).max(), 1e-300)
+    err = np.abs(np.asarray(gpu) - np.asarray(ref)).max()
+    assert err <= tol * scale, f"{what}: {err:.3e} vs scale {scale:.3e}"
+
+
+def test_device_newton_matches_oracle(oracle):
+    """ovs_quench_newton (FP64) against the oracle's Newton loop of
+    solmultiphasethermofluid_stag: the same Newton and Krylov iteration
+    counts, the same convergence verdict, every state field to 1e-10."""
+    case = _stirred_case("newton_oracle")
+    ctx = Context.from_case(case)
+    info = ctx.quench_newton(F.OVS_FP64, **NEWTON)
+    oc = oracle.OracleCase(case)
+    ref = oc.quench_newton(NEWTON["newton_max"], True, NEWTON["kspace"], 1, NEWTON["tol_ns"], NEWTON["tol_tem"],
+                           NEWTON["utol"], NEWTON["atol"])
+    assert info.iterations == ref["iterations"] and bool(info.converged) == bool(ref["converged"])
+    assert info.krylov_iterations_ns == ref["krylov_ns"] and info.krylov_iterations_tem == ref["krylov_tem"]
+    for f in FIELDS:
+        _close(ctx.get_field(f), oc.state_arrays[f], 1e-10, f)
+    _close(np.array(info.residual0), ref["residual0"], 1e-10, "residual0")
+    ctx.close()
+
+
+def test_device_time_steps_match_oracle(oracle):
+    """ovs_quench_time_steps over steps 0-2 (driver.f90:70-100: predictor,
+    Newton loop with the istep rules, old values) against the oracle's
+    driver loop: the last step's iteration counts and every state field and
+    old value to 1e-10."""
+    case = _stirred_case("steps_oracle")
+    ctx = Context.from_case(case)
+    info, _ = ctx.quench_time_steps(0, 3, mode=F.OVS_FP64, max_cycles=1, **NEWTON)
+    oc = oracle.OracleCase(case)
+    ref = oc.quench_time_steps(0, 3, NEWTON["newton_max"], True, NEWTON["kspace"], 1, NEWTON["tol_ns"],
+                               NEWTON["tol_tem"], NEWTON["utol"], NEWTON["atol"])
+    assert info.iterations == ref["iterations"]
+    assert info.krylov_iterations_ns == ref["krylov_ns"] and info.krylov_iterations_tem == ref["krylov_tem"]
+    for f in FIELDS + ("ugold", "acgold"):
+        _close(ctx.get_field(f), oc.state_arrays[f], 1e-10, f)
+    ctx.close()
+
+
+def test_device_newton_mixed_follows_fp64():
+    """The OVS_MIXED Newton loop (FP64 assembly and residuals, solves by the
+    mixed refinement to the FP64 systems) takes the FP64 loop's Newton
+    iterations and ends within 1e-6 of its state."""
+    case = _stirred_case("newton_mixed")
+    a = Context.from_case(case)
+    i64 = a.quench_newton(F.OVS_FP64, **NEWTON)
+    b = Context.from_case(case)
+    imx = b.quench_newton(F.OVS_MIXED, max_cycles=100, **NEWTON)
+    assert imx.iterations == i64.iterations and bool(imx.converged) == bool(i64.converged)
+    for f in FIELDS:
+        _close(b.get_field(f), a.get_field(f), 1e-6, f)
+    a.close()
+    b.close()

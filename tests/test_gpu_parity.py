@@ -223,6 +223,25 @@ def test_gmres_tem_zero_rhs_returns_zero(oracle):
     assert np.all(s == 0.0)   # SparseGMRES_tem.f90:68-71 zeroes sol
 
 
+@pytest.mark.parametrize("mk", [lambda: M.config1().mesh, lambda: M.box_hex(6, 5, 4),
+                                lambda: M.box_tet(48, 48, 96, 1.0, 1.0, 2.0)],
+                         ids=["config1", "hex", "config2_mesh"])
+def test_slot_map_bit_exact(oracle, mk):
+    """The element-slot -> CSR-slot map the assembly scatters through equals
+    FillSparseMat_3D's k = SparseMatLoc_3D(...) + col(IEN(e,a)) - 1 for every
+    (element, a, b), on config 1, a hexahedral box and the config-2 mesh
+    (1,327,104 tets)."""
+    m = mk()
+    ctx = Context(m.nnode, m.nelem, m.ien.shape[1])
+    ctx.upload_mesh(m)
+    ctx.build_pattern()
+    col, row = ctx.get_pattern()
+    lmap = ctx.get_slot_map()
+    ctx.close()
+    ref = oracle.slot_map(m.ien, col, row)
+    np.testing.assert_array_equal(lmap, ref)
+
+
 def test_config1_newton_step(oracle):
     """Config 1 end to end: NS assembly, reference GMRES(50, 1e-6), Newton
     update - GPU vs oracle."""
@@ -247,11 +266,14 @@ def test_config1_newton_step(oracle):
     assert r_g[0] > 0
 
 
-@pytest.mark.parametrize("mode", [F.OVS_FP64, F.OVS_FP32])
+@pytest.mark.parametrize("mode", [F.OVS_FP64, F.OVS_FP32, F.OVS_MIXED])
 def test_refined_solve_reaches_true_residual(oracle, mode):
+    """The refined solve's own residual claim, rechecked with the oracle's
+    SpMV on the system it refines against: the FP64 system for OVS_FP64 and
+    OVS_MIXED, the FP32-assembled one for OVS_FP32."""
     case = M.quench_case(M.box_tet(8, 8, 8), "q8")
     ctx = _ctx(case)
-    prec = F.OVS_FP64 if mode == F.OVS_FP64 else F.OVS_FP32
+    prec = F.OVS_FP32 if mode == F.OVS_FP32 else F.OVS_FP64
     ctx.assemble(F.OVS_ASM_NSVOF, 6, prec)
     sol, info = ctx.solve(F.OVS_SYS_NSVOF, mode, 1e-8, kspace=50, max_cycles=200)
     assert info.converged and info.rel_residual <= 1e-8
@@ -263,17 +285,47 @@ def test_refined_solve_reaches_true_residual(oracle, mode):
     assert np.linalg.norm(r) <= 1.05e-8 * np.linalg.norm(sysblocks["rhs"])
 
 
+@pytest.mark.parametrize("sysid,kern,nf", [(F.OVS_SYS_NSVOF, F.OVS_ASM_NSVOF, 5), (F.OVS_SYS_TEM, F.OVS_ASM_TEM, 1)])
+def test_mixed_reaches_fp64_solution(oracle, sysid, kern, nf):
+    """OVS_MIXED solves the FP64 system: every field of its solution is
+    within 1e-5 (relative to the field's largest value) of the restarted
+    FP64 GMRES solution, and of the oracle's dense solve of the FP64 system,
+    and its true FP64 residual meets rtol.  The FP32-assembled system's
+    solution (OVS_FP32) is further away; that difference is the FP32
+    assembly's rounding, which OVS_MIXED does not inherit."""
+    case = M.quench_case(M.box_tet(8, 8, 8), "q8")
+    ctx = _ctx(case)
+    ctx.assemble(kern, 6, F.OVS_FP64)
+    s64, i64 = ctx.solve(sysid, F.OVS_FP64, 1e-10, 50, 300)
+    smx, imx = ctx.solve(sysid, F.OVS_MIXED, 1e-10, 50, 300)
+    assert i64.converged and imx.converged and imx.rel_residual <= 1e-10
+    oc = oracle.OracleCase(case)
+    sysblocks = ctx.get_system(sysid, F.OVS_FP64)
+    oc.load_system(KIND[sysid], sysblocks)
+    r = sysblocks["rhs"] - oc.spmv(KIND[sysid], smx)
+    assert np.linalg.norm(r) <= 1.05e-10 * np.linalg.norm(sysblocks["rhs"])
+    for f in range(nf):
+        scale = max(np.abs(s64[:, f]).max(), 1e-300)
+        assert np.abs(smx[:, f] - s64[:, f]).max() <= 1e-5 * scale, f
+    # the FP32 rounding of the matrix is what the inner cycles used
+    for b in SYS_BLOCKS[sysid]:
+        a32 = ctx.get_lhs(sysid, F.OVS_FP32, b)
+        np.testing.assert_array_equal(a32, sysblocks[BLOCK_NAME[b]].astype(np.float32).astype(np.float64))
+
+
 def test_mixed_vs_fp64_solution_error():
     case = M.quench_case(M.box_tet(8, 8, 8), "q8")
     ctx = _ctx(case)
     ctx.assemble(F.OVS_ASM_NSVOF, 6, F.OVS_FP64)
-    ctx.assemble(F.OVS_ASM_NSVOF, 6, F.OVS_FP32)
     s64, i64 = ctx.solve(F.OVS_SYS_NSVOF, F.OVS_FP64, 1e-10, 50, 300)
+    smx, imx = ctx.solve(F.OVS_SYS_NSVOF, F.OVS_MIXED, 1e-10, 50, 300)
+    ctx.assemble(F.OVS_ASM_NSVOF, 6, F.OVS_FP32)
     s32, i32 = ctx.solve(F.OVS_SYS_NSVOF, F.OVS_FP32, 1e-10, 50, 300)
-    assert i64.converged and i32.converged
+    assert i64.converged and imx.converged and i32.converged
     for f in range(5):
-        err = np.abs(s32[:, f] - s64[:, f]).max() / max(np.abs(s64[:, f]).max(), 1e-300)
-        assert err < 1e-3, (f, err)   # FP32 assembly: O(kappa * 1e-7)
+        scale = max(np.abs(s64[:, f]).max(), 1e-300)
+        assert np.abs(smx[:, f] - s64[:, f]).max() <= 1e-5 * scale, f
+        assert np.abs(s32[:, f] - s64[:, f]).max() <= 1e-3 * scale, f   # FP32 assembly: O(kappa * 1e-7)
 
 
 # ------------------------------------------------------------ error paths

@@ -71,6 +71,26 @@ def test_sparse_mat_loc_semantics(oracle):
     assert lib.orc_sparse_mat_loc(p, 4, 11) == 4
 
 
+@pytest.mark.parametrize("mk", [lambda: M.box_tet(4, 3, 3), lambda: M.box_hex(3, 2, 2)])
+def test_slot_map_points_at_the_column(oracle, mk):
+    """FillSparseMat_3D's slot k(e,a,b) lies in row IEN(e,a) and holds
+    column IEN(e,b) (rows are sorted and contain every element neighbour, so
+    the search finds the goal itself); on a random permutation of the
+    element order the map follows the elements."""
+    m = mk()
+    col, row = oracle.gen_spar_struc(m.ien, m.nnode)
+    lmap = oracle.slot_map(m.ien, col, row)
+    E, nshl = m.ien.shape
+    for a in range(nshl):
+        i = m.ien[:, a]
+        for b in range(nshl):
+            k = lmap[:, a, b]
+            assert np.all((k >= col[i - 1]) & (k < col[i]))
+            np.testing.assert_array_equal(row[k - 1], m.ien[:, b])
+    perm = np.random.default_rng(0).permutation(E)
+    np.testing.assert_array_equal(oracle.slot_map(m.ien[perm], col, row), lmap[perm])
+
+
 def test_mesh_orientation():
     for m in (M.box_tet(3, 2, 2, 1.0, 0.5, 2.0), M.box_hex(2, 2, 3)):
         x = m.xg[m.ien - 1]  # (E, nshl, 3)
