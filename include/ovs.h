@@ -527,10 +527,20 @@ int ovs_gmres_transposed(ovs_ctx* ctx, int system, const double* rhs, double tol
  * OVS_NOALLOC_SCRATCH_BYTES inside the library (held by every GPU that loads
  * the library until the process exits).  Limits: n <= OVS_NOALLOC_MAX_N and
  * kspace <= OVS_NOALLOC_MAX_KSPACE; larger requests return OVS_ERR_ARG.
- * The first call on a device looks up the device address of that array, so
- * make it before any stream capture.  All calls share the array: calls that
- * overlap on the GPU (other streams, other host threads) race.  `stream` is
- * a cudaStream_t (NULL: default stream); the call returns after the solve. */
+ * Set-up on first use: the first call on a device looks up the device
+ * address of that array (cudaGetSymbolAddress), and under CUDA's default
+ * lazy module loading it is also the call that loads the library's module
+ * onto the device, which is when the array itself is allocated.  Make that
+ * first call (a warm-up call will do) before any stream capture and before
+ * any phase in which nothing may be allocated; later calls allocate nothing.
+ * All calls share the array, which keeps the last call's contents: serialize
+ * them (one stream, one host thread at a time); calls that overlap on the
+ * GPU (other streams, other host threads) race, their info read-back
+ * included.  `stream` is a cudaStream_t (NULL: default stream); the call is
+ * synchronous and returns after the solve.  Results follow SparseGMRES_tem's
+ * arithmetic (reciprocal scaling of the Krylov vectors and rotations); a
+ * zero Hessenberg column, where the reference's rotation is 0/0, ends the
+ * cycle with the previous columns' solution and breakdown = 1. */
 #define OVS_NOALLOC_MAX_N 16384
 #define OVS_NOALLOC_MAX_KSPACE 40
 #define OVS_NOALLOC_SCRATCH_BYTES 5537792

@@ -445,6 +445,17 @@ __device__ void givens_step(GmresDev* gm, int k) {
   }
   const double a = Hk[k - 1], b = Hk[k];
   const double tmp = sqrt(a * a + b * b);
+  if (tmp == 0.0) {
+    // column k of H is zero (P^-1 A v_k has no component outside
+    // v_1..v_{k-1}): the rotation would be 0/0 and the reference carries NaN
+    // on; the cycle ends with the solution of the first k-1 columns
+    gm->iks = k - 1;
+    gm->ercheck = fabs(gm->e[k - 1]);
+    gm->done = 1;
+    gm->converged = gm->ercheck <= gm->epsnrm;
+    gm->breakdown = 1;
+    return;
+  }
   gm->cs[k - 1] = a / tmp;
   gm->sn[k - 1] = b / tmp;
   Hk[k - 1] = tmp;

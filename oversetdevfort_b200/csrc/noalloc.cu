@@ -108,7 +108,8 @@ gmres_tem_single_cta(int n, const int* __restrict__ rowptr, const int* __restric
   un = sqrt(na_block_sum(un, sh));
   const double epsnrm = tol * un;
   if (t == 0) e[0] = un;
-  for (int i = t; i < n; i += NA_THREADS) V[i] = V[i] / un;
+  const double uninv = 1.0 / un;                   // unorm = 1/unorm; u = u*unorm
+  for (int i = t; i < n; i += NA_THREADS) V[i] = V[i] * uninv;
   __syncthreads();
   int iks = 0;
   double ercheck = un;
@@ -136,8 +137,10 @@ gmres_tem_single_cta(int n, const int* __restrict__ rowptr, const int* __restric
       if (t == 0) H[(size_t)(k - 1) * NA_LDH + (j - 1)] = beta;
     }
     const double unorm = sqrt(beta);
-    if (unorm != 0.0)
-      for (int i = t; i < n; i += NA_THREADS) w[i] = w[i] / unorm;
+    if (unorm != 0.0) {
+      const double uinv = 1.0 / unorm;
+      for (int i = t; i < n; i += NA_THREADS) w[i] = w[i] * uinv;
+    }
     if (t == 0) {                                  // Givens update and exit test
       double* Hk = H + (size_t)(k - 1) * NA_LDH;
       Hk[k] = unorm;
@@ -148,18 +151,28 @@ gmres_tem_single_cta(int n, const int* __restrict__ rowptr, const int* __restric
       }
       const double a = Hk[k - 1], b = Hk[k];
       const double tmp = sqrt(a * a + b * b);
-      cs[k - 1] = a / tmp;
-      sn[k - 1] = b / tmp;
-      Hk[k - 1] = tmp;
-      Hk[k] = 0.0;
-      const double t2 = cs[k - 1] * e[k - 1] + sn[k - 1] * e[k];
-      e[k] = -sn[k - 1] * e[k - 1] + cs[k - 1] * e[k];
-      e[k - 1] = t2;
-      const double er = fabs(e[k]);
-      S[NA_SCAL] = er;
-      if ((er <= epsnrm && k >= kmin) || unorm == 0.0) s_done = (unorm == 0.0) ? 2 : 1;
+      if (tmp == 0.0) {
+        // column k of H is zero: P^-1 A v_k lies in the span of v_1..v_{k-1}
+        // with no component of its own, the rotation is 0/0 (the reference
+        // would carry NaN on).  The cycle ends with the solution of the
+        // first k-1 columns.
+        s_done = 3;
+      } else {
+        const double tmp1 = 1.0 / tmp;
+        cs[k - 1] = a * tmp1;
+        sn[k - 1] = b * tmp1;
+        Hk[k - 1] = tmp;
+        Hk[k] = 0.0;
+        const double t2 = cs[k - 1] * e[k - 1] + sn[k - 1] * e[k];
+        e[k] = -sn[k - 1] * e[k - 1] + cs[k - 1] * e[k];
+        e[k - 1] = t2;
+        const double er = fabs(e[k]);
+        S[NA_SCAL] = er;
+        if ((er <= epsnrm && k >= kmin) || unorm == 0.0) s_done = (unorm == 0.0) ? 2 : 1;
+      }
     }
     __syncthreads();
+    if (s_done == 3) { breakdown = 1; break; }
     iks = k;
     ercheck = S[NA_SCAL];
     if (s_done) { breakdown = s_done == 2; break; }
@@ -215,6 +228,9 @@ extern "C" int ovs_gmres_tem_noalloc(int n, const int* rowptr, const int* colidx
   cudaStream_t s = static_cast<cudaStream_t>(stream);
   int* info_i = reinterpret_cast<int*>(S + NA_SCAL + 2);
   double* info_d = S + NA_SCAL + 4;
+  // an error left pending by an earlier call of the caller's is not this
+  // launch's: clear it so the check below sees this launch alone
+  (void)cudaGetLastError();
   gmres_tem_single_cta<<<1, NA_THREADS, 0, s>>>(n, rowptr, colidx, vals, rhs, sol, tol, kspace, kspace_min, S,
                                                 info_i, info_d);
   OVS_CUDA_TRY(cudaGetLastError());
