@@ -515,6 +515,17 @@ def run_ours(args, world, rank, local_rank, dist):
             prof[f"asm_{kn}_{nm}_ms"] = ctx.profile(F.OVS_PROF_ASSEMBLE, kern, prec, 5)
             prof[f"asm_{kn}_{nm}_elements_ms"] = ctx.profile(F.OVS_PROF_ASSEMBLE_ELEMENTS, kern, prec, 5)
             prof[f"asm_{kn}_{nm}_rows_ms"] = ctx.profile(F.OVS_PROF_ASSEMBLE_ROWS, kern, prec, 5)
+    # the row pass with its element summaries staged through shared memory
+    # (default) against lane-by-lane global reads, same box, same data
+    rows_ab = {}
+    for staged in (1, 0):       # ends on the library default
+        ctx.set_option(F.OVS_OPT_ROWS_STAGED, staged)
+        for prec, nm in ((F.OVS_FP64, "fp64"), (F.OVS_FP32, "fp32")):
+            for kern, kn in ((F.OVS_ASM_NSVOF, "nsvof"), (F.OVS_ASM_TEM, "tem")):
+                ctx.assemble(kern, 6, prec)
+                rows_ab[f"{kn}_{nm}_{'staged' if staged else 'global'}_ms"] = \
+                    ctx.profile(F.OVS_PROF_ASSEMBLE_ROWS, kern, prec, 5)
+    prof["rows_variants"] = rows_ab
     ctx.assemble(F.OVS_ASM_NSVOF, 6, F.OVS_FP32)
     ctx.assemble(F.OVS_ASM_NSVOF, 6, F.OVS_FP64)
     prof["spmv_nsvof_fp32_ms"] = ctx.profile(F.OVS_PROF_SPMV, F.OVS_SYS_NSVOF, F.OVS_FP32, 20)

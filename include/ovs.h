@@ -105,7 +105,10 @@ enum {
   OVS_OPT_HEX_TC = 1,          /* 1: FP32 NS+VOF hexahedra take the tcgen05 element-matrix pass (3xTF32);
                                   0 (default, the faster one measured; env OVS_HEX_TC=1 sets 1): the
                                   CUDA-core row expansion */
-  OVS_OPT_ARNOLDI_FUSED = 2    /* 1: one-launch Arnoldi variant (default 0; env OVS_ARNOLDI_FUSED=1) */
+  OVS_OPT_ARNOLDI_FUSED = 2,   /* 1: one-launch Arnoldi variant (default 0; env OVS_ARNOLDI_FUSED=1) */
+  OVS_OPT_ROWS_STAGED = 3      /* tet row pass: 1 (env OVS_ROWS_STAGED=1) stages each chunk's element
+                                  summaries in shared memory with asynchronous copies; 0 (default) reads them
+                                  from global memory lane by lane */
 };
 
 /* boundary-face flags (ovs_set_faces) */

@@ -159,8 +159,8 @@ __device__ __forceinline__ void load_rec(const double* rec, int node, double r[1
     double2 v = __ldg(p + k);
     r[2 * k] = v.x; r[2 * k + 1] = v.y;
   }
-  double2 v0 = __ldg(p + 8), v1 = __ldg(p + 9);
-  lo[0] = v0.x; lo[1] = v0.y; lo[2] = v1.x; lo[3] = v1.y;
+  // FP64 records round nothing: their remainders (slots 16-19) are exactly 0
+  lo[0] = lo[1] = lo[2] = lo[3] = 0.0;
 }
 
 // Geometry of a linear tet on the current configuration x+d
@@ -612,13 +612,16 @@ __device__ void summarize_tem(const SumArgs& a, const T r[4][16], const T lo[4][
 // (fact1 Nb + fact2 cb + fact2 Nb src), E_b = sum eps Na Nb,
 // U_b = sum ufac Nb, PL_b = -sum plfac Na Nb, V_b = sum fact2 w (Na +
 // tauLS ca) Nb, W = sum ufac Na, where c_n = uadv . grad N_n.
-template <typename T>
+// 4 consecutive values: read-only global loads (SMEM = false) or loads from
+// the warp's shared-memory stage (SMEM = true)
+template <typename T, bool SMEM = false>
 __device__ __forceinline__ void ldv4(const T* p, T* d) {
   if constexpr (sizeof(T) == 4) {
-    const float4 v = __ldg(reinterpret_cast<const float4*>(p));
+    const float4 v = SMEM ? *reinterpret_cast<const float4*>(p) : __ldg(reinterpret_cast<const float4*>(p));
     d[0] = v.x; d[1] = v.y; d[2] = v.z; d[3] = v.w;
   } else {
-    const double2 a = __ldg(reinterpret_cast<const double2*>(p)), b = __ldg(reinterpret_cast<const double2*>(p) + 1);
+    const double2 a = SMEM ? reinterpret_cast<const double2*>(p)[0] : __ldg(reinterpret_cast<const double2*>(p));
+    const double2 b = SMEM ? reinterpret_cast<const double2*>(p)[1] : __ldg(reinterpret_cast<const double2*>(p) + 1);
     d[0] = a.x; d[1] = a.y; d[2] = b.x; d[3] = b.y;
   }
 }
@@ -626,13 +629,13 @@ __device__ __forceinline__ void ldv4(const T* p, T* d) {
 // Blocks (row node la, column nodes b0 + k*BS, k < NC) of an element from
 // its summary, by the sums above, in one Gauss-point loop.  The 4 lanes of an
 // NS/NS+VOF element take one column each (NC = 1); a T lane takes all four.
-template <typename T, int KIND, int NC>
+template <typename T, int KIND, int NC, bool SMEM = false>
 __device__ __forceinline__ void expand_block(const ovs_params& p, const T* sm, int la, int b0, int BS,
                                              T (&o)[NC][Lay<KIND>::NV < 4 ? 1 : Lay<KIND>::NV], T* rv) {
   using L = Lay<KIND>;
   T hd[16];
 #pragma unroll
-  for (int k = 0; k < 16; k += 4) ldv4(sm + k, hd + k);
+  for (int k = 0; k < 16; k += 4) ldv4<T, SMEM>(sm + k, hd + k);
   T g[4][3];
 #pragma unroll
   for (int n = 0; n < 4; ++n)
@@ -662,7 +665,7 @@ __device__ __forceinline__ void expand_block(const ovs_params& p, const T* sm, i
       tet_shape<T>(gp, N);
       T q[L::GPW];
 #pragma unroll
-      for (int k = 0; k < L::GPW; k += 4) ldv4(sm + L::GP0 + gp * L::GPW + k, q + k);
+      for (int k = 0; k < L::GPW; k += 4) ldv4<T, SMEM>(sm + L::GP0 + gp * L::GPW + k, q + k);
       const T uadv[3] = {q[0], q[1], q[2]}, rcp = q[3], dSe = q[4], trc = q[5];
       const T ca = ga[0] * uadv[0] + ga[1] * uadv[1] + ga[2] * uadv[2];
       const T aw = w * (pick4<T>(N, la) + trc * ca);
@@ -684,7 +687,7 @@ __device__ __forceinline__ void expand_block(const ovs_params& p, const T* sm, i
     T KDP = 0, dphi[3] = {0, 0, 0};
     if constexpr (vof) {
       T t4[4];
-      ldv4(sm + 16, t4);
+      ldv4<T, SMEM>(sm + 16, t4);
       KDP = t4[0]; dphi[0] = t4[1]; dphi[1] = t4[2]; dphi[2] = t4[3];
     }
     T Q = 0, R = 0, W = 0;
@@ -697,7 +700,7 @@ __device__ __forceinline__ void expand_block(const ovs_params& p, const T* sm, i
       tet_shape<T>(gp, N);
       T q[L::GPW];
 #pragma unroll
-      for (int k = 0; k < L::GPW; k += 4) ldv4(sm + L::GP0 + gp * L::GPW + k, q + k);
+      for (int k = 0; k < L::GPW; k += 4) ldv4<T, SMEM>(sm + L::GP0 + gp * L::GPW + k, q + k);
       T uadv[3], rho, rt;
       if constexpr (vof) {
         uadv[0] = q[0]; uadv[1] = q[1]; uadv[2] = q[2]; rho = q[3]; rt = q[4];
@@ -789,13 +792,33 @@ template <typename T, int KIND> struct Smem {
   static constexpr int NVP = (NV < 4) ? 1 : NV;
   static constexpr int BSTR = (NV < 4) ? 1 : NV + 16 / (int)sizeof(T);
   static constexpr int RSTR = NF + 1;
-  __host__ __device__ static size_t bytes(int max_deg) {
+  // the stage buffer of the staged row pass: the chunk's CH element
+  // summaries, copied in with one round of asynchronous 16-byte copies
+  static constexpr int SW = Lay<KIND>::SW;
+  __host__ __device__ static size_t bytes(int max_deg, bool staged = false) {
     size_t b = sizeof(T) * ((size_t)4 * CH * BSTR + (size_t)CH * RSTR + (size_t)max_deg * NVP);
     b = (b + 15) & ~(size_t)15;
     b += sizeof(int) * ((size_t)4 * CH + max_deg);
-    return (b + 15) & ~(size_t)15;
+    b = (b + 15) & ~(size_t)15;
+    if (staged) b += sizeof(T) * (size_t)CH * SW;
+    return b;
   }
+  __host__ __device__ static size_t stage_offset(int max_deg) { return bytes(max_deg, false); }
 };
+
+// 16-byte asynchronous global -> shared copy (cp.async, no register
+// staging) and 4-byte variant; completion by cp_async_wait_all
+__device__ __forceinline__ void cp_async16(void* dst, const void* src) {
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"((unsigned)__cvta_generic_to_shared(dst)),
+               "l"(src) : "memory");
+}
+__device__ __forceinline__ void cp_async4(void* dst, const void* src) {
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 4;" ::"r"((unsigned)__cvta_generic_to_shared(dst)),
+               "l"(src) : "memory");
+}
+__device__ __forceinline__ void cp_async_wait_all() {
+  asm volatile("cp.async.commit_group;\n\tcp.async.wait_group 0;" ::: "memory");
+}
 
 // ---------------------------------------------------------- pass 1 kernel
 // blocks per SM the element pass is compiled for: the FP32 NS+VOF pass at 3
@@ -852,7 +875,12 @@ __device__ __forceinline__ unsigned mask_of(int v) {
   return (unsigned)c_rowbits[v] | ((unsigned)c_colbits[v] << 8) | ((unsigned)c_diagbit[v] << 16);
 }
 
-template <typename T, int KIND, int WARPS>
+// STAGED: the warp first copies the chunk's element summaries into its
+// shared-memory stage with one round of asynchronous 16-byte copies (all in
+// flight together, no registers held), with the element ids of the next
+// chunk already loaded; the block expansion then reads shared memory.
+// Otherwise every lane reads its element's summary from global memory.
+template <typename T, int KIND, int WARPS, bool STAGED>
 __global__ void __launch_bounds__(WARPS * 32)
 assemble_rows_kernel(const AsmArgs a) {
   using S = Smem<T, KIND>;
@@ -863,7 +891,8 @@ assemble_rows_kernel(const AsmArgs a) {
   if (threadIdx.x < 24) masks[threadIdx.x] = (KIND == OVS_ASM_TEM) ? (TB | (TB << 8) | (TB << 16)) : mask_of(threadIdx.x);
   __syncthreads();
   const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
-  unsigned char* base = smem_raw + (size_t)wid * S::bytes(a.max_deg);
+  unsigned char* base = smem_raw + (size_t)wid * S::bytes(a.max_deg, STAGED);
+  T* stage = reinterpret_cast<T*>(base + S::stage_offset(a.max_deg));   // [CH][SW] (STAGED)
   T* blk = reinterpret_cast<T*>(base);                 // [CH][4][BSTR]
   T* rvs = blk + 4 * CH * BSTR;                        // [CH][RSTR]
   T* acc = rvs + CH * RSTR;                            // [max_deg][NVP]
@@ -878,22 +907,70 @@ assemble_rows_kernel(const AsmArgs a) {
   // with one lane per element (T) a lane takes all 4 columns
   constexpr int LPE = S::LPE, CPL = 4 / LPE;
   const int jl = lane / LPE, bl0 = lane % LPE;
+  constexpr int U16 = L::SW * (int)sizeof(T) / 16;          // 16-byte units per summary
+  static_assert(L::SW * sizeof(T) % 16 == 0, "summaries must be whole 16-byte units");
   for (int A = blockIdx.x * WARPS + wid; A < a.N; A += nwarps_total) {
     const int rp = a.rowptr[A], deg = a.rowptr[A + 1] - rp;
     const int ep = a.n2e_ptr[A], ne = a.n2e_ptr[A + 1] - ep;
-    for (int s = lane; s < deg; s += 32) cols[s] = a.colidx[rp + s];
+    if constexpr (STAGED) {
+      for (int s = lane; s < deg; s += 32) cp_async4(cols + s, a.colidx + rp + s);
+    } else {
+      for (int s = lane; s < deg; s += 32) cols[s] = a.colidx[rp + s];
+    }
     for (int q = lane; q < deg * NVP; q += 32) acc[q] = (T)0;
     T racc = (T)0;
+    // element ids and slots of the row's first chunk (lanes j < nc hold entry j)
+    int pk_n = 0;
+    unsigned s4_n = 0;
+    if (STAGED && lane < min(CH, ne)) {
+      pk_n = __ldg(a.n2e + ep + lane);
+      s4_n = __ldg(a.n2s + ep + lane);
+    }
     __syncwarp();
     for (int c0 = 0; c0 < ne; c0 += CH) {
       const int nc = min(CH, ne - c0);
+      int pk_c = 0;
+      unsigned s4_c = 0;
+      if constexpr (STAGED) {
+        pk_c = pk_n;
+        s4_c = s4_n;
+        // the next chunk's ids travel while this one is copied and expanded
+        if (c0 + CH < ne && lane < min(CH, ne - c0 - CH)) {
+          pk_n = __ldg(a.n2e + ep + c0 + CH + lane);
+          s4_n = __ldg(a.n2s + ep + c0 + CH + lane);
+        }
+        // every lane runs the same trip count: the shuffle needs the full warp
+        for (int it = 0; it < (CH * U16 + 31) / 32; ++it) {
+          const int u = lane + 32 * it;
+          const int j = min(u / U16, CH - 1);
+          const int e = __shfl_sync(0xffffffffu, pk_c, j) >> 3;
+          if (u < nc * U16) {
+            const int k = u - j * U16;
+            cp_async16(reinterpret_cast<unsigned char*>(stage + (size_t)j * L::SW) + 16 * k,
+                       reinterpret_cast<const unsigned char*>(sum + (size_t)e * L::SW) + 16 * k);
+          }
+        }
+        cp_async_wait_all();
+        __syncwarp();
+      }
       // ---------------- phase 1: block (A's row, column bl) of element jl
+      int packed;
+      unsigned slots4;
+      if constexpr (STAGED) {
+        packed = __shfl_sync(0xffffffffu, pk_c, min(jl, CH - 1));
+        slots4 = __shfl_sync(0xffffffffu, s4_c, min(jl, CH - 1));
+      }
       if (jl < nc) {
-        const int packed = __ldg(a.n2e + ep + c0 + jl);
-        const unsigned slots4 = __ldg(a.n2s + ep + c0 + jl);
+        if constexpr (!STAGED) {
+          packed = __ldg(a.n2e + ep + c0 + jl);
+          slots4 = __ldg(a.n2s + ep + c0 + jl);
+        }
         const int e = packed >> 3, la = packed & 7;
         T o[CPL][NVP], rv[NF];
-        expand_block<T, KIND, CPL>(a.p, sum + (size_t)e * L::SW, la, bl0, LPE, o, rv);
+        if constexpr (STAGED)
+          expand_block<T, KIND, CPL, true>(a.p, stage + (size_t)jl * L::SW, la, bl0, LPE, o, rv);
+        else
+          expand_block<T, KIND, CPL>(a.p, sum + (size_t)e * L::SW, la, bl0, LPE, o, rv);
 #pragma unroll
         for (int k = 0; k < CPL; ++k) {
           const int bl = bl0 + k * LPE;
@@ -934,6 +1011,10 @@ assemble_rows_kernel(const AsmArgs a) {
       }
       if (lane < NF)
         for (int j = 0; j < nc; ++j) racc += rvs[j * RSTR + lane];
+      __syncwarp();
+    }
+    if constexpr (STAGED) {   // the row's column copies (a node without elements skips the chunk loop)
+      cp_async_wait_all();
       __syncwarp();
     }
     // ---------------- row write with the Dirichlet treatment
@@ -1033,21 +1114,11 @@ __global__ void alpha_records_kernel(const AlphaArgs a) {
   for (int k = 0; k < REC; ++k) o[k] = r[k];
 }
 
-// parts: bit 0 the element pass, bit 1 the row pass
-template <typename T, int KIND>
-int launch_assemble(ovs_ctx* c, const AsmArgs& a, const SumArgs& sa, int parts = 3) {
-  // pass 1: element summaries
-  if (parts & 1) {
-    element_summary_kernel<T, KIND><<<(sa.E + 127) / 128, 128, 0, c->stream>>>(sa);
-    ++c->launches;
-    OVS_CUDA_TRY(cudaGetLastError());
-  }
-  if (!(parts & 2)) return OVS_OK;
-  // pass 2: rows
-  constexpr int WARPS = 4;
+template <typename T, int KIND, int WARPS, bool STAGED>
+int launch_rows(ovs_ctx* c, const AsmArgs& a) {
   using S = Smem<T, KIND>;
-  const size_t smem = S::bytes(a.max_deg) * WARPS;
-  auto kern = assemble_rows_kernel<T, KIND, WARPS>;
+  const size_t smem = S::bytes(a.max_deg, STAGED) * WARPS;
+  auto kern = assemble_rows_kernel<T, KIND, WARPS, STAGED>;
   OVS_CUDA_TRY(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
   int per_sm = 0;
   OVS_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, WARPS * 32, smem));
@@ -1060,6 +1131,21 @@ int launch_assemble(ovs_ctx* c, const AsmArgs& a, const SumArgs& sa, int parts =
   ++c->launches;
   OVS_CUDA_TRY(cudaGetLastError());
   return OVS_OK;
+}
+
+// parts: bit 0 the element pass, bit 1 the row pass
+template <typename T, int KIND>
+int launch_assemble(ovs_ctx* c, const AsmArgs& a, const SumArgs& sa, int parts = 3) {
+  // pass 1: element summaries
+  if (parts & 1) {
+    element_summary_kernel<T, KIND><<<(sa.E + 127) / 128, 128, 0, c->stream>>>(sa);
+    ++c->launches;
+    OVS_CUDA_TRY(cudaGetLastError());
+  }
+  if (!(parts & 2)) return OVS_OK;
+  // pass 2: rows
+  if (c->rows_staged) return launch_rows<T, KIND, 4, true>(c, a);
+  return launch_rows<T, KIND, 4, false>(c, a);
 }
 
 

@@ -196,6 +196,8 @@ int create_resources(ovs_ctx* c, const ovs_dims* dims) {
     c->arnoldi_fused = e && e[0] == '1';
     const char* h = getenv("OVS_HEX_TC");
     c->hex_tc = h && h[0] == '1';
+    const char* rs = getenv("OVS_ROWS_STAGED");
+    if (rs) c->rows_staged = rs[0] != '0';
   }
   c->N = dims->nnode;
   c->E = dims->nelem;
@@ -397,6 +399,7 @@ int ovs_set_option(ovs_ctx* c, int option, int value) {
   if (!c) return OVS_ERR_ARG;
   switch (option) {
     case OVS_OPT_HEX_TC: c->hex_tc = value != 0; return OVS_OK;
+    case OVS_OPT_ROWS_STAGED: c->rows_staged = value != 0; return OVS_OK;
     case OVS_OPT_ARNOLDI_FUSED: c->arnoldi_fused = value != 0; return OVS_OK;
     default: return OVS_ERR_ARG;
   }

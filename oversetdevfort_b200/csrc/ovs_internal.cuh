@@ -116,6 +116,9 @@ struct ovs_ctx {
               ev_rhs_out = nullptr;
   // hex tensor-core pass (FP32 NS+VOF): off unless OVS_HEX_TC=1 or OVS_OPT_HEX_TC
   int hex_tc = 0;
+  // tet row pass: element summaries staged through shared memory by
+  // asynchronous copies (1, default) or read by every lane from global memory
+  int rows_staged = 0;
   void* hex_kbuf = nullptr;              // E x 64 x 24 block values
   float* hex_w = nullptr;                // W hi + lo, canonical layout
   // boundary-condition producers (ovs_set_bc_spec)
