@@ -114,6 +114,14 @@ class LocalComm:
             s = s + v
         return s
 
+    def allreduce_t(self, vals):
+        """Sum of 0-dim tensors (one per part) as a tensor on the first
+        part's device, in part order, without a host round trip."""
+        s = vals[0]
+        for v in vals[1:]:
+            s = s + v.to(s.device)
+        return s
+
     def halo(self, vecs: dict):
         pl = self.plan
         for r in vecs:
@@ -157,6 +165,15 @@ class TorchComm:
         t = torch.as_tensor(np.asarray(vals[0], dtype=np.float64), device=self.device).clone()
         dist.all_reduce(t)
         return t.cpu().numpy()
+
+    def allreduce_t(self, vals):
+        """The global sum of this rank's 0-dim tensor, left on the device:
+        with NCCL the all-reduce is queued on the current stream and nothing
+        waits on the host."""
+        import torch.distributed as dist
+        t = vals[0].to(self.device).reshape(1).clone()
+        dist.all_reduce(t)
+        return t[0]
 
     def halo(self, vecs: dict):
         import torch
@@ -257,14 +274,23 @@ def gmres_cycle(comm, ops: dict, rhs: dict, tol: float, kspace: int, kspace_min:
             ops[r].matvec(U[ik - 1][r], w[r])
         U.append(w)
         if orthog == "mgs":
-            beta = 0.0
+            # the k + 1 dots of the reference order stay on the device: each
+            # projection uses the previous dot as a device scalar, the
+            # all-reduces queue one after another, and the column of H comes
+            # to the host once per step
+            col = []
+            beta_t = None
             for jk in range(1, ik + 2):
                 if jk > 1:
                     for r in P:
-                        w[r] = w[r] - beta * U[jk - 2][r]
+                        w[r] = w[r] - beta_t.to(w[r].device) * U[jk - 2][r]
                     U[ik] = w
-                beta = gdot(w, U[jk - 1] if jk - 1 < ik else w)
-                H[jk - 1, ik - 1] = beta
+                other = U[jk - 1] if jk - 1 < ik else w
+                beta_t = comm.allreduce_t([(w[r][:, ow[r]] * other[r][:, ow[r]]).sum() for r in P])
+                col.append(beta_t)
+            hcol = torch.stack([c.to(col[0].device) for c in col]).cpu().numpy()
+            H[:ik + 1, ik - 1] = hcol
+            beta = float(hcol[-1])
         else:
             for _ in range(2):
                 loc = [np.array([float((U[j][r][:, ow[r]] * w[r][:, ow[r]]).sum()) for j in range(ik)]) for r in P]

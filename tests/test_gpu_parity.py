@@ -382,3 +382,24 @@ def test_kdc_integer_dummy_quirk(oracle):
     ob = oracle.OracleCase(base)
     ob.assemble_quenching(6, 3)
     assert np.abs(ob.sys["K11"] - oc.sys["K11"]).max() > 0   # k_dc is active
+
+
+@pytest.mark.parametrize("kind", ["nsvof", "tem", "ns"])
+@pytest.mark.parametrize("prec", [F.OVS_FP64, F.OVS_FP32])
+def test_row_pass_variants_bit_identical(kind, prec):
+    """The row pass with the element summaries staged through shared memory
+    (OVS_OPT_ROWS_STAGED = 1) and read lane by lane from global memory (0)
+    runs the same arithmetic in the same order: the assembled systems are
+    bit-identical, matrix and right-hand side."""
+    kernel = {"nsvof": F.OVS_ASM_NSVOF, "tem": F.OVS_ASM_TEM, "ns": F.OVS_ASM_NS}[kind]
+    sysid = {"nsvof": F.OVS_SYS_NSVOF, "tem": F.OVS_SYS_TEM, "ns": F.OVS_SYS_NS}[kind]
+    case = M.random_case(nx=6, ny=5, nz=4, seed=21, kernel=kernel)
+    out = []
+    for staged in (0, 1):
+        ctx = _ctx(case)
+        ctx.set_option(F.OVS_OPT_ROWS_STAGED, staged)
+        ctx.assemble(kernel, 6, prec)
+        out.append(ctx.get_system(sysid, prec))
+        ctx.close()
+    for k in out[0]:
+        np.testing.assert_array_equal(out[0][k], out[1][k], err_msg=k)
