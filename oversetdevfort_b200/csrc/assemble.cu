@@ -47,6 +47,7 @@ struct AsmArgs {
   const int* n2e_ptr;
   const int* n2e;
   const unsigned* n2s;    // slots of each entry's element nodes in the row
+  const int* row_order;   // processing order of the rows (a permutation), or null
   void* vals;             // nnz*NV
   void* rhs;              // NF*N field-major
   const void* kbuf;       // hex tensor-core block values (E x 64 x 24), or null
@@ -98,8 +99,8 @@ template <> struct Wide<Dual> { using type = Dual; };
 
 // VOF field at tet Gauss point g in FP64 from the record value (slot k)
 // plus its rounding remainder (lo[.][3]): sum_a N_a phi_a, in node order
-template <typename T>
-__device__ __forceinline__ typename Wide<T>::type gp_phi(const T r[4][16], const T lo[4][4], int k, int g) {
+template <typename T, typename RA, typename LA>
+__device__ __forceinline__ typename Wide<T>::type gp_phi(const RA& r, const LA& lo, int k, int g) {
   using W = typename Wide<T>::type;
   const double a = 0.5854101966249685, b = 0.1381966011250105;
   const double xi = (g == 0) ? a : b, eta = (g == 1) ? a : b, ze = (g == 2) ? a : b;
@@ -128,6 +129,17 @@ __device__ __forceinline__ void store_row(double* dst, const double* v) {
 #pragma unroll
   for (int k = 0; k < NV; k += 2)
     *reinterpret_cast<double2*>(dst + k) = make_double2(v[k], v[k + 1]);
+}
+
+// 4 values to global memory with the streaming cache hint (st.global.cs):
+// the CSR values are written once and not read again by the pass, so they
+// should not evict the element summaries the pass still reads from L2
+__device__ __forceinline__ void store4_cs(float* dst, const float* v) {
+  __stcs(reinterpret_cast<float4*>(dst), make_float4(v[0], v[1], v[2], v[3]));
+}
+__device__ __forceinline__ void store4_cs(double* dst, const double* v) {
+  __stcs(reinterpret_cast<double2*>(dst), make_double2(v[0], v[1]));
+  __stcs(reinterpret_cast<double2*>(dst) + 1, make_double2(v[2], v[3]));
 }
 
 template <typename T>
@@ -167,8 +179,8 @@ __device__ __forceinline__ void load_rec(const double* rec, int node, double r[1
 // (eval_shape_fem, src/eval_shape_FEM.f90:4-61, with get_inverse_3x3,
 // src/eval_shape.f90:85-112).  xd[a][i] = x+d of node a.  The Jacobian of a
 // linear tet is the same at every Gauss point, so it is evaluated once.
-template <typename T>
-__device__ __forceinline__ T tet_geometry(const T xd[4][3], const T lo[4][4], T g[4][3], T G[3][3]) {
+template <typename T, typename LA>
+__device__ __forceinline__ T tet_geometry(const T xd[4][3], const LA& lo, T g[4][3], T G[3][3]) {
   T A[3][3], Ai[3][3];
 #pragma unroll
   for (int i = 0; i < 3; ++i)
@@ -228,7 +240,9 @@ __device__ __forceinline__ void cfl_max(unsigned long long* bits, double v) {
 //   NS   : g(12) w KA KB MM | GP x4: uadv(3) rt        | residual 4x4 = 48
 //   NSVOF: g(12) w KA KB MM KDP dphi(3) | GP x4: uadv(3) rho rt tauLS src
 //          eps ufac plfac pad(2)                       | residual 4x5 = 88
-//   TEM  : g(12) w HK pad(2) | GP x4: uadv(3) rcp dSe trc pad(2) | residual 4 = 52
+//   TEM  : the 4x4 element matrix itself, row-major (a, b) | residual 4 = 20
+//          (a scalar system: its element matrix is smaller than the
+//          Gauss-point records it would be expanded from)
 // (Gauss-point records padded to 16-byte groups for vector loads)
 // with rt = rho tauM, trc = tauT rho cp and the factors of the block sums
 // below (src, eps, ufac, plfac of the phase-change terms).
@@ -240,7 +254,7 @@ template <> struct Lay<OVS_ASM_NSVOF> {
   static constexpr int SW = 88, GP0 = 20, GPW = 12, RHS0 = 68, NF = 5, NV = 24;
 };
 template <> struct Lay<OVS_ASM_TEM> {
-  static constexpr int SW = 52, GP0 = 16, GPW = 8, RHS0 = 48, NF = 1, NV = 1;
+  static constexpr int SW = 20, RHS0 = 16, NF = 1, NV = 1;
 };
 
 struct SumArgs {
@@ -254,8 +268,8 @@ struct SumArgs {
   ovs_params p;
 };
 
-template <typename T>
-__device__ __forceinline__ void element_geometry(const T r[4][16], const T lo[4][4], T g[4][3], T G[3][3],
+template <typename T, typename RA, typename LA>
+__device__ __forceinline__ void element_geometry(const RA& r, const LA& lo, T g[4][3], T G[3][3],
                                                  T& detj, T& GG, T& trG) {
   T xd[4][3];
 #pragma unroll
@@ -273,8 +287,8 @@ __device__ __forceinline__ void element_geometry(const T r[4][16], const T lo[4]
 
 // pass 1, NS-only: IntElmAss_NS_overset's Gauss loop with e3LHS_3D_fluid_Old /
 // e3Rhs_3D_fluid (quirks: uprime = 0, kap_dc = NS_kdc_a, tauBar = 0)
-template <typename T>
-__device__ void summarize_ns(const SumArgs& a, const T r[4][16], const T lo[4][4], bool target, T* o,
+template <typename T, typename RA, typename LA>
+__device__ void summarize_ns(const SumArgs& a, const RA& r, const LA& lo, bool target, T* o,
                              double& cfl, T& detj_out) {
   const ovs_params& p = a.p;
   T g[4][3], G[3][3], detj, GG, trG;
@@ -353,8 +367,8 @@ __device__ void summarize_ns(const SumArgs& a, const T r[4][16], const T lo[4][4
 // pass 1, NS+VOF quench (src/solveQuenching.f90:295-523); the viscous RHS
 // broadcast (:508-510) is kept: the three scalars sum_j gN_a,j (du(j,k) +
 // du(k,j)), k = 1..3, are subtracted from every momentum component
-template <typename T>
-__device__ void summarize_nsvof(const SumArgs& a, const T r[4][16], const T lo[4][4], bool fluid, T* o,
+template <typename T, typename RA, typename LA>
+__device__ void summarize_nsvof(const SumArgs& a, const RA& r, const LA& lo, bool fluid, T* o,
                                 double& cfl, T& detj_out) {
   using W = typename Wide<T>::type;
   const ovs_params& p = a.p;
@@ -394,7 +408,7 @@ __device__ void summarize_nsvof(const SumArgs& a, const T r[4][16], const T lo[4
   T ru[4][3], rp[4], rf[4];
 #pragma unroll
   for (int n = 0; n < 4; ++n) { ru[n][0] = ru[n][1] = ru[n][2] = 0; rp[n] = 0; rf[n] = 0; }
-#pragma unroll
+#pragma unroll (sizeof(T) == 8 ? 1 : 4)
   for (int gp = 0; gp < 4; ++gp) {
     T N[4];
     tet_shape<T>(gp, N);
@@ -501,10 +515,15 @@ __device__ void summarize_nsvof(const SumArgs& a, const T r[4][16], const T lo[4
 }
 
 // pass 1, temperature (src/solveQuenching.f90:712-856).  Record layout of
-// this pass: xd(0:2) u(3:5) um(6:8) phi(9) T(10) rT(11).  Solid elements store
-// uadv = dSe = trc = 0, which turns the fluid block formula into the solid one.
-template <typename T>
-__device__ void summarize_tem(const SumArgs& a, const T r[4][16], const T lo[4][4], bool fluid, T* o,
+// this pass: xd(0:2) u(3:5) um(6:8) phi(9) T(10) rT(11).  The element matrix
+// (:814-839) is formed here, per Gauss point
+//   K(a,b) += w (Na + trc ca) (rcp (fact1 Nb + fact2 cb) - fact2 dSe Nb)
+// with trc = tauT rho cp, c_n = uadv . grad N_n, then K(a,b) += HK gab; solid
+// elements take uadv = dSe = trc = 0, which turns the fluid block formula
+// into the solid one.  The adjoint instantiation (dual numbers) needs the
+// residual only and skips the matrix.
+template <typename T, typename RA, typename LA>
+__device__ void summarize_tem(const SumArgs& a, const RA& r, const LA& lo, bool fluid, T* o,
                               double& cfl, T& detj_out) {
   using W = typename Wide<T>::type;
   const ovs_params& p = a.p;
@@ -521,6 +540,12 @@ __device__ void summarize_tem(const SumArgs& a, const T r[4][16], const T lo[4][
 #pragma unroll
   for (int n = 0; n < 4; ++n) gdT[n] = g[n][0] * dT[0] + g[n][1] * dT[1] + g[n][2] * dT[2];
   T HK = 0, rt[4] = {0, 0, 0, 0};
+  const T fact1 = (T)p.almi;
+  T K[4][4];
+#pragma unroll
+  for (int ia = 0; ia < 4; ++ia)
+#pragma unroll
+    for (int ib = 0; ib < 4; ++ib) K[ia][ib] = (T)0;
   const bool kdc_on = fabs(p.tem_kdc) > 0.0;
 #pragma unroll
   for (int gp = 0; gp < 4; ++gp) {
@@ -570,12 +595,20 @@ __device__ void summarize_tem(const SumArgs& a, const T r[4][16], const T lo[4][
     T kdcT = 0;
     if (kdc_on && fluid) kdcT = (T)p.tem_kdc * fabs(res) / sqrt(GG) / (T)p.tref;
     const T dSe = (cpw - cpa) * mdot + ((cpw - cpa) * (Ti - ts) - lh) * dmdT;
-    T* og = o + Lay<OVS_ASM_TEM>::GP0 + gp * Lay<OVS_ASM_TEM>::GPW;
-    og[3] = rcp;
-    og[6] = 0; og[7] = 0;
+    if constexpr (!std::is_same<T, Dual>::value) {
+      const T uq[3] = {fluid ? uadv[0] : (T)0, fluid ? uadv[1] : (T)0, fluid ? uadv[2] : (T)0};
+      const T dSq = fluid ? dSe : (T)0, trq = fluid ? tauT * rcp : (T)0;
+      T cq[4];
+#pragma unroll
+      for (int n = 0; n < 4; ++n) cq[n] = g[n][0] * uq[0] + g[n][1] * uq[1] + g[n][2] * uq[2];
+#pragma unroll
+      for (int ia = 0; ia < 4; ++ia) {
+        const T aw = w * (N[ia] + trq * cq[ia]);
+#pragma unroll
+        for (int ib = 0; ib < 4; ++ib) K[ia][ib] += aw * (rcp * (fact1 * N[ib] + fact2 * cq[ib]) - fact2 * dSq * N[ib]);
+      }
+    }
     if (fluid) {
-      og[0] = uadv[0]; og[1] = uadv[1]; og[2] = uadv[2];
-      og[4] = dSe; og[5] = tauT * rcp;
       HK += fact2 * (hk + kdcT) * w;
 #pragma unroll
       for (int n = 0; n < 4; ++n) {
@@ -583,17 +616,18 @@ __device__ void summarize_tem(const SumArgs& a, const T r[4][16], const T lo[4][
         rt[n] += w * (-N[n] * rcp * (rTi + udT) + N[n] * Se - rcp * tauT * cn * res - (hk + kdcT) * gdT[n]);
       }
     } else {
-      og[0] = og[1] = og[2] = 0; og[4] = 0; og[5] = 0;
       HK += fact2 * hk * w;
 #pragma unroll
       for (int n = 0; n < 4; ++n) rt[n] += w * (-N[n] * rcp * rTi - hk * gdT[n]);
     }
   }
+  if constexpr (!std::is_same<T, Dual>::value) {
 #pragma unroll
-  for (int n = 0; n < 4; ++n)
+    for (int ia = 0; ia < 4; ++ia)
 #pragma unroll
-    for (int d = 0; d < 3; ++d) o[3 * n + d] = g[n][d];
-  o[12] = w; o[13] = HK; o[14] = 0; o[15] = 0;
+      for (int ib = 0; ib < 4; ++ib)
+        o[4 * ia + ib] = K[ia][ib] + HK * (g[ia][0] * g[ib][0] + g[ia][1] * g[ib][1] + g[ia][2] * g[ib][2]);
+  }
 #pragma unroll
   for (int n = 0; n < 4; ++n) o[Lay<OVS_ASM_TEM>::RHS0 + n] = rt[n];
 }
@@ -633,6 +667,12 @@ template <typename T, int KIND, int NC, bool SMEM = false>
 __device__ __forceinline__ void expand_block(const ovs_params& p, const T* sm, int la, int b0, int BS,
                                              T (&o)[NC][Lay<KIND>::NV < 4 ? 1 : Lay<KIND>::NV], T* rv) {
   using L = Lay<KIND>;
+  if constexpr (KIND == OVS_ASM_TEM) {
+    // the element pass stored the element matrix: row la, columns b
+#pragma unroll
+    for (int k = 0; k < NC; ++k) o[k][0] = sm[4 * la + b0 + k * BS];
+    rv[0] = sm[L::RHS0 + la];
+  } else {
   T hd[16];
 #pragma unroll
   for (int k = 0; k < 16; k += 4) ldv4<T, SMEM>(sm + k, hd + k);
@@ -653,33 +693,7 @@ __device__ __forceinline__ void expand_block(const ovs_params& p, const T* sm, i
   T gab[NC];
 #pragma unroll
   for (int k = 0; k < NC; ++k) gab[k] = ga[0] * gb[k][0] + ga[1] * gb[k][1] + ga[2] * gb[k][2];
-  if constexpr (KIND == OVS_ASM_TEM) {
-    const T fact1 = (T)p.almi, fact2 = (T)(p.alfi * p.gami * p.delt);
-    const T HK = hd[13];
-    T X[NC];
-#pragma unroll
-    for (int k = 0; k < NC; ++k) X[k] = 0;
-#pragma unroll
-    for (int gp = 0; gp < 4; ++gp) {
-      T N[4];
-      tet_shape<T>(gp, N);
-      T q[L::GPW];
-#pragma unroll
-      for (int k = 0; k < L::GPW; k += 4) ldv4<T, SMEM>(sm + L::GP0 + gp * L::GPW + k, q + k);
-      const T uadv[3] = {q[0], q[1], q[2]}, rcp = q[3], dSe = q[4], trc = q[5];
-      const T ca = ga[0] * uadv[0] + ga[1] * uadv[1] + ga[2] * uadv[2];
-      const T aw = w * (pick4<T>(N, la) + trc * ca);
-#pragma unroll
-      for (int k = 0; k < NC; ++k) {
-        const T cb = gb[k][0] * uadv[0] + gb[k][1] * uadv[1] + gb[k][2] * uadv[2];
-        const T Nb = pick4<T>(N, b0 + k * BS);
-        X[k] += aw * (rcp * (fact1 * Nb + fact2 * cb) - fact2 * dSe * Nb);
-      }
-    }
-#pragma unroll
-    for (int k = 0; k < NC; ++k) o[k][0] = X[k] + HK * gab[k];
-    rv[0] = sm[L::RHS0 + la];
-  } else {
+  {
     constexpr bool vof = KIND == OVS_ASM_NSVOF;
     const T fact1 = (T)p.almi;
     const T fact2 = vof ? (T)(p.alfi * p.delt * p.gami) : (T)(p.alfi * p.gami * p.delt);
@@ -760,6 +774,7 @@ __device__ __forceinline__ void expand_block(const ovs_params& p, const T* sm, i
 #pragma unroll
     for (int f = 0; f < L::NF; ++f) rv[f] = sm[L::RHS0 + L::NF * la + f];
   }
+  }
 }
 
 template <typename T> struct Vec4 {};
@@ -826,6 +841,27 @@ __device__ __forceinline__ void cp_async_wait_all() {
 // the compiler chooses (tighter bounds spill)
 template <typename T, int KIND> struct SumMinBlocks { static constexpr int v = 1; };
 template <> struct SumMinBlocks<float, OVS_ASM_NSVOF> { static constexpr int v = 3; };
+template <> struct SumMinBlocks<double, OVS_ASM_NSVOF> { static constexpr int v = 3; };
+template <> struct SumMinBlocks<double, OVS_ASM_TEM> { static constexpr int v = 3; };
+
+// FP64 node records held in shared memory instead of registers (64 values
+// per element, transposed so a warp's accesses hit 32 consecutive banks),
+// and zero rounding remainders: the FP64 element routines otherwise need
+// more registers than a thread has.
+template <typename T> struct SmemRecRow {
+  const volatile T* p;   // volatile: read where used, not hoisted into registers
+  __device__ __forceinline__ T operator[](int k) const { return p[(size_t)k * 128]; }
+};
+template <typename T> struct SmemRecs {
+  const T* p;   // this thread's column of a [64][128] block array
+  __device__ __forceinline__ SmemRecRow<T> operator[](int n) const { return SmemRecRow<T>{p + (size_t)n * 16 * 128}; }
+};
+template <typename T> struct ZeroRow {
+  __device__ __forceinline__ T operator[](int) const { return (T)0; }
+};
+template <typename T> struct ZeroRecs {
+  __device__ __forceinline__ ZeroRow<T> operator[](int) const { return ZeroRow<T>{}; }
+};
 
 template <typename T, int KIND>
 __global__ void __launch_bounds__(128, SumMinBlocks<T, KIND>::v)
@@ -837,24 +873,45 @@ element_summary_kernel(const SumArgs a) {
   if (e < a.E) {
     const int4 nd = __ldg(reinterpret_cast<const int4*>(a.ien) + e);
     const int nodes[4] = {nd.x, nd.y, nd.z, nd.w};
-    T r[4][16], lo[4][4];
     const T* rec = reinterpret_cast<const T*>(a.rec);
-#pragma unroll
-    for (int n = 0; n < 4; ++n) load_rec(rec, nodes[n], r[n], lo[n]);
     const int eid = __ldg(a.elm_id + e);
-    T o[L::SW];
     T detj;
-    if constexpr (KIND == OVS_ASM_NS) {
-      const bool target = ((a.p.subdomain_flag & 1) && eid == a.p.elm_id_set[0]) ||
-                          ((a.p.subdomain_flag & 2) && eid == a.p.elm_id_set[1]);
-      summarize_ns<T>(a, r, lo, target, o, cfl, detj);
-    } else if constexpr (KIND == OVS_ASM_NSVOF) {
-      summarize_nsvof<T>(a, r, lo, eid == a.p.fluid_elm_id, o, cfl, detj);
+    auto run = [&](const auto& r, const auto& lo, T* o) {
+      if constexpr (KIND == OVS_ASM_NS) {
+        const bool target = ((a.p.subdomain_flag & 1) && eid == a.p.elm_id_set[0]) ||
+                            ((a.p.subdomain_flag & 2) && eid == a.p.elm_id_set[1]);
+        summarize_ns<T>(a, r, lo, target, o, cfl, detj);
+      } else if constexpr (KIND == OVS_ASM_NSVOF) {
+        summarize_nsvof<T>(a, r, lo, eid == a.p.fluid_elm_id, o, cfl, detj);
+      } else {
+        summarize_tem<T>(a, r, lo, eid == a.p.fluid_elm_id, o, cfl, detj);
+      }
+    };
+    if constexpr (sizeof(T) == 8) {
+      // records through shared memory; the summary written straight to
+      // global memory as its values are produced
+      extern __shared__ __align__(16) unsigned char sm_elem[];
+      T* col = reinterpret_cast<T*>(sm_elem) + threadIdx.x;
+#pragma unroll
+      for (int n = 0; n < 4; ++n) {
+        const double2* q = reinterpret_cast<const double2*>(rec) + (size_t)nodes[n] * (REC / 2);
+#pragma unroll
+        for (int k = 0; k < 8; ++k) {
+          const double2 v = __ldg(q + k);
+          col[(size_t)(n * 16 + 2 * k) * 128] = v.x;
+          col[(size_t)(n * 16 + 2 * k + 1) * 128] = v.y;
+        }
+      }
+      run(SmemRecs<T>{col}, ZeroRecs<T>{}, reinterpret_cast<T*>(a.sum) + (size_t)e * L::SW);
     } else {
-      summarize_tem<T>(a, r, lo, eid == a.p.fluid_elm_id, o, cfl, detj);
+      T r[4][16], lo[4][4];
+#pragma unroll
+      for (int n = 0; n < 4; ++n) load_rec(rec, nodes[n], r[n], lo[n]);
+      T o[L::SW];
+      run(r, lo, o);
+      store_row<L::SW>(reinterpret_cast<T*>(a.sum) + (size_t)e * L::SW, o);
     }
     if (!(detj > (T)0)) nbad = 1;
-    store_row<L::SW>(reinterpret_cast<T*>(a.sum) + (size_t)e * L::SW, o);
   }
 #pragma unroll
   for (int off = 16; off > 0; off >>= 1) {
@@ -909,7 +966,11 @@ assemble_rows_kernel(const AsmArgs a) {
   const int jl = lane / LPE, bl0 = lane % LPE;
   constexpr int U16 = L::SW * (int)sizeof(T) / 16;          // 16-byte units per summary
   static_assert(L::SW * sizeof(T) % 16 == 0, "summaries must be whole 16-byte units");
-  for (int A = blockIdx.x * WARPS + wid; A < a.N; A += nwarps_total) {
+  for (int t = blockIdx.x * WARPS + wid; t < a.N; t += nwarps_total) {
+    // rows in the spatial order of the nodes (when given), so that the rows
+    // sharing an element are in flight together and its summary is read
+    // from L2 rather than DRAM
+    const int A = a.row_order ? __ldg(a.row_order + t) : t;
     const int rp = a.rowptr[A], deg = a.rowptr[A + 1] - rp;
     const int ep = a.n2e_ptr[A], ne = a.n2e_ptr[A + 1] - ep;
     if constexpr (STAGED) {
@@ -1039,7 +1100,7 @@ assemble_rows_kernel(const AsmArgs a) {
             if (dg && ((ibA << 16) & m & 0xff0000u)) val = cnt;
             v4[t] = val;
           }
-          store_row<4>(out + (size_t)s * NV + 4 * gidx, v4);
+          store4_cs(out + (size_t)s * NV + 4 * gidx, v4);
         }
       } else {
         for (int q = lane; q < deg; q += 32) {
@@ -1048,7 +1109,7 @@ assemble_rows_kernel(const AsmArgs a) {
           T val = acc[q];
           if ((ibA & TB) || (ibB & TB)) val = (T)0;
           if (B == A && (ibA & TB)) val = cnt;
-          out[q] = val;
+          __stcs(out + q, val);
         }
       }
     }
@@ -1058,7 +1119,7 @@ assemble_rows_kernel(const AsmArgs a) {
       else bit = (lane < 3) ? (1u << lane) : (lane == 3 ? PB : FB);
       T v = (ibA & bit) ? (T)0 : racc;
       if (!isfinite((double)v)) atomicOr(a.flags + 1, 1);
-      reinterpret_cast<T*>(a.rhs)[(size_t)lane * a.N + A] = v;
+      __stcs(reinterpret_cast<T*>(a.rhs) + (size_t)lane * a.N + A, v);
     }
     __syncwarp();
   }
@@ -1138,13 +1199,19 @@ template <typename T, int KIND>
 int launch_assemble(ovs_ctx* c, const AsmArgs& a, const SumArgs& sa, int parts = 3) {
   // pass 1: element summaries
   if (parts & 1) {
-    element_summary_kernel<T, KIND><<<(sa.E + 127) / 128, 128, 0, c->stream>>>(sa);
+    // FP64: the node records of the block's 128 elements in shared memory
+    const size_t esm = sizeof(T) == 8 ? sizeof(T) * 64 * 128 : 0;
+    if (esm) OVS_CUDA_TRY(cudaFuncSetAttribute(element_summary_kernel<T, KIND>,
+                                               cudaFuncAttributeMaxDynamicSharedMemorySize, (int)esm));
+    element_summary_kernel<T, KIND><<<(sa.E + 127) / 128, 128, esm, c->stream>>>(sa);
     ++c->launches;
     OVS_CUDA_TRY(cudaGetLastError());
   }
   if (!(parts & 2)) return OVS_OK;
   // pass 2: rows
-  if (c->rows_staged) return launch_rows<T, KIND, 4, true>(c, a);
+  // the temperature summaries (20 values, one lane per element) gain
+  // nothing from staging: measured slower, so it reads them directly
+  if (c->rows_staged && KIND != OVS_ASM_TEM) return launch_rows<T, KIND, 4, true>(c, a);
   return launch_rows<T, KIND, 4, false>(c, a);
 }
 
@@ -1356,6 +1423,7 @@ static void fill_args(ovs_ctx* c, int prec, SysStore& S, int tensor_flag, AsmArg
   a.mat = (tensor_flag & OVS_TENSOR_MAT) != 0;
   a.vec = (tensor_flag & OVS_TENSOR_VEC) != 0;
   a.n2s = c->n2s;
+  a.row_order = c->row_order;
   a.max_deg = c->max_deg;
   a.p = c->params;
   a.kbuf = nullptr;

@@ -256,7 +256,7 @@ int ovs_destroy(ovs_ctx* c) {
   ovs_streaming_free(c);
   if (c->hex_kbuf) cudaFree(c->hex_kbuf);
   if (c->hex_w) cudaFree(c->hex_w);
-  void* ptrs[] = {c->ien, c->elm_id, c->ibc, c->rowptr, c->colidx, c->diag, c->n2e_ptr, c->n2e, c->n2s, c->tmap, c->vals_t, c->vjp_cot, c->vjp_ge, c->vjp_grad,
+  void* ptrs[] = {c->ien, c->elm_id, c->ibc, c->rowptr, c->colidx, c->diag, c->n2e_ptr, c->n2e, c->n2s, c->row_order, c->tmap, c->vals_t, c->vjp_cot, c->vjp_ge, c->vjp_grad,
                   c->rec[0], c->rec[1], c->esum[0], c->esum[1], c->gm, c->basis[0], c->basis[1], c->work64, c->work32, c->wvec, c->coop_part,
                   c->flags, c->cfl_bits};
   for (void* p : ptrs) if (p) cudaFree(p);

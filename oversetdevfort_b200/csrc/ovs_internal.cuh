@@ -94,6 +94,7 @@ struct ovs_ctx {
   double* vjp_cot = nullptr; // residual VJP work: cotangent, element terms, nodal result
   double* vjp_ge = nullptr;
   double* vjp_grad = nullptr;
+  int* row_order = nullptr;  // N: rows in Morton order of the node coordinates (the row pass's order)
   unsigned* n2s = nullptr;   // nshl*E entries: slots of the element's nodes in the row, one byte each
                              // (one word per entry for tets, two for hexahedra)
   int nnz = 0;
@@ -118,7 +119,7 @@ struct ovs_ctx {
   int hex_tc = 0;
   // tet row pass: element summaries staged through shared memory by
   // asynchronous copies (1, default) or read by every lane from global memory
-  int rows_staged = 0;
+  int rows_staged = 1;
   void* hex_kbuf = nullptr;              // E x 64 x 24 block values
   float* hex_w = nullptr;                // W hi + lo, canonical layout
   // boundary-condition producers (ovs_set_bc_spec)

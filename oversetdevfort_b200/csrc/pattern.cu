@@ -10,7 +10,59 @@
 // the output layout identical to the reference's col/row arrays.
 #include "ovs_internal.cuh"
 
+#include <cub/device/device_radix_sort.cuh>
+
+#include <vector>
+
+#include <math.h>
+
 namespace {
+
+// ------------------------------------------------ spatial order of the rows
+// Per block: min and max of each coordinate (N x 3 column-major xg).
+__global__ void bbox_kernel(const double* __restrict__ xg, int N, double* __restrict__ out) {
+  __shared__ double sh[6][256];
+  double lo[3] = {INFINITY, INFINITY, INFINITY}, hi[3] = {-INFINITY, -INFINITY, -INFINITY};
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < N; i += gridDim.x * blockDim.x)
+    for (int d = 0; d < 3; ++d) {
+      const double v = xg[(size_t)d * N + i];
+      lo[d] = fmin(lo[d], v);
+      hi[d] = fmax(hi[d], v);
+    }
+  for (int d = 0; d < 3; ++d) { sh[d][threadIdx.x] = lo[d]; sh[3 + d][threadIdx.x] = hi[d]; }
+  __syncthreads();
+  for (int o = blockDim.x / 2; o > 0; o >>= 1) {
+    if (threadIdx.x < o)
+      for (int d = 0; d < 3; ++d) {
+        sh[d][threadIdx.x] = fmin(sh[d][threadIdx.x], sh[d][threadIdx.x + o]);
+        sh[3 + d][threadIdx.x] = fmax(sh[3 + d][threadIdx.x], sh[3 + d][threadIdx.x + o]);
+      }
+    __syncthreads();
+  }
+  if (threadIdx.x < 6) out[(size_t)blockIdx.x * 6 + threadIdx.x] = sh[threadIdx.x][0];
+}
+
+// 21 bits of each quantized coordinate interleaved into a 63-bit Morton key
+__device__ __forceinline__ unsigned long long spread21(unsigned v) {
+  unsigned long long x = v & 0x1fffffULL;
+  x = (x | (x << 32)) & 0x1f00000000ffffULL;
+  x = (x | (x << 16)) & 0x1f0000ff0000ffULL;
+  x = (x | (x << 8)) & 0x100f00f00f00f00fULL;
+  x = (x | (x << 4)) & 0x10c30c30c30c30c3ULL;
+  x = (x | (x << 2)) & 0x1249249249249249ULL;
+  return x;
+}
+
+__global__ void morton_kernel(const double* __restrict__ xg, int N, double x0, double y0, double z0, double sx,
+                              double sy, double sz, unsigned long long* __restrict__ key, int* __restrict__ id) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= N) return;
+  const double q[3] = {(xg[i] - x0) * sx, (xg[(size_t)N + i] - y0) * sy, (xg[2 * (size_t)N + i] - z0) * sz};
+  unsigned u[3];
+  for (int d = 0; d < 3; ++d) u[d] = (unsigned)fmin(fmax(q[d], 0.0), 2097151.0);
+  key[i] = spread21(u[0]) | (spread21(u[1]) << 1) | (spread21(u[2]) << 2);
+  id[i] = i;
+}
 
 constexpr int SCAN_T = 1024;
 
@@ -277,6 +329,55 @@ int ovs_slot_map_to_host(ovs_ctx* c, int* lmap) {
   return OVS_OK;
 }
 
+// c->row_order: the nodes sorted by the Morton key of their coordinates,
+// the order in which the assembly's row pass visits the rows (each row's
+// result does not depend on the order).  Rows that share an element then
+// run close together in time and the element's summary is reused from L2.
+static int build_row_order(ovs_ctx* c) {
+  cudaStream_t s = c->stream;
+  const int N = c->N;
+  const double* xg = c->field[OVS_F_XG];
+  if (!xg || N < 2) return OVS_OK;
+  int st;
+  if ((st = ovs_ensure((void**)&c->row_order, sizeof(int) * N))) return st;
+  const int nb = ovs_grid(N, 256, 4 * c->num_sms);
+  double* part = nullptr;
+  OVS_CUDA_TRY(cudaMallocAsync(&part, sizeof(double) * 6 * nb, s));
+  bbox_kernel<<<nb, 256, 0, s>>>(xg, N, part);
+  ++c->launches;
+  std::vector<double> h((size_t)6 * nb);
+  OVS_CUDA_TRY(cudaMemcpyAsync(h.data(), part, sizeof(double) * 6 * nb, cudaMemcpyDeviceToHost, s));
+  OVS_CUDA_TRY(cudaStreamSynchronize(s));
+  OVS_CUDA_TRY(cudaFreeAsync(part, s));
+  double lo[3] = {INFINITY, INFINITY, INFINITY}, hi[3] = {-INFINITY, -INFINITY, -INFINITY};
+  for (int b = 0; b < nb; ++b)
+    for (int d = 0; d < 3; ++d) {
+      lo[d] = fmin(lo[d], h[(size_t)b * 6 + d]);
+      hi[d] = fmax(hi[d], h[(size_t)b * 6 + 3 + d]);
+    }
+  double sc[3];
+  for (int d = 0; d < 3; ++d) sc[d] = hi[d] > lo[d] ? 2097151.0 / (hi[d] - lo[d]) : 0.0;
+  unsigned long long *k0 = nullptr, *k1 = nullptr;
+  int* id0 = nullptr;
+  OVS_CUDA_TRY(cudaMallocAsync(&k0, sizeof(unsigned long long) * N, s));
+  OVS_CUDA_TRY(cudaMallocAsync(&k1, sizeof(unsigned long long) * N, s));
+  OVS_CUDA_TRY(cudaMallocAsync(&id0, sizeof(int) * N, s));
+  morton_kernel<<<ovs_grid(N, 256, 1 << 30), 256, 0, s>>>(xg, N, lo[0], lo[1], lo[2], sc[0], sc[1], sc[2], k0, id0);
+  ++c->launches;
+  size_t tbytes = 0;
+  OVS_CUDA_TRY(cub::DeviceRadixSort::SortPairs(nullptr, tbytes, k0, k1, id0, c->row_order, N, 0, 63, s));
+  void* tmp = nullptr;
+  OVS_CUDA_TRY(cudaMallocAsync(&tmp, tbytes > 0 ? tbytes : 16, s));
+  OVS_CUDA_TRY(cub::DeviceRadixSort::SortPairs(tmp, tbytes, k0, k1, id0, c->row_order, N, 0, 63, s));
+  c->launches += 4;   // the radix sort's passes (counted approximately)
+  OVS_CUDA_TRY(cudaFreeAsync(tmp, s));
+  OVS_CUDA_TRY(cudaFreeAsync(k0, s));
+  OVS_CUDA_TRY(cudaFreeAsync(k1, s));
+  OVS_CUDA_TRY(cudaFreeAsync(id0, s));
+  OVS_CUDA_TRY(cudaGetLastError());
+  return OVS_OK;
+}
+
 int ovs_pattern_build(ovs_ctx* c) {
   cudaStream_t s = c->stream;
   const int N = c->N, E = c->E, nshl = c->nshl;
@@ -336,6 +437,7 @@ int ovs_pattern_build(ovs_ctx* c) {
   OVS_CUDA_TRY(cudaFreeAsync(cnt, s));
   OVS_CUDA_TRY(cudaFreeAsync(tmp, s));
   OVS_CUDA_TRY(cudaFreeAsync(stats, s));
+  if ((st = build_row_order(c))) return st;
   OVS_CUDA_TRY(cudaStreamSynchronize(s));
   OVS_CUDA_TRY(cudaGetLastError());
   c->have_pattern = true;

@@ -1,13 +1,11 @@
-"""GPU checks of the pieces that have not run on a B200 yet; the file name
-keeps pytest from collecting it until they have passed once (then it moves
-to tests/test_gpu_*.py).  The partitioned Newton loop on GPU contexts
-(distributed.ContextPartition: ovs_set_solution, ovs_predictor,
-ovs_commit_old) against ovs_quench_newton / ovs_quench_time_steps on one
-context, FP64 and mixed; ovs_set_solution + ovs_newton_update against the
-update of an ovs_gmres solution; ovs_predictor / ovs_commit_old against host
-arithmetic; ovs_assemble_async / ovs_assemble_wait against ovs_assemble; the
-C driver's cavity mode.  Run with
-    python -m pytest tests/pending_gpu_checks.py -m gpu -x -q"""
+"""GPU checks of the partitioned Newton loop on device contexts and of the
+context calls it is built from: distributed.ContextPartition
+(ovs_set_solution, ovs_predictor, ovs_commit_old) against
+ovs_quench_newton / ovs_quench_time_steps on one context, FP64 and mixed;
+ovs_set_solution + ovs_newton_update against the update of an ovs_gmres
+solution; ovs_predictor / ovs_commit_old against host arithmetic;
+ovs_assemble_async / ovs_assemble_wait against ovs_assemble; the C driver's
+cavity mode (one config-1 Newton step through the C ABI from plain C)."""
 import numpy as np
 import pytest
 import torch

@@ -287,45 +287,58 @@ def test_refined_solve_reaches_true_residual(oracle, mode):
 
 @pytest.mark.parametrize("sysid,kern,nf", [(F.OVS_SYS_NSVOF, F.OVS_ASM_NSVOF, 5), (F.OVS_SYS_TEM, F.OVS_ASM_TEM, 1)])
 def test_mixed_reaches_fp64_solution(oracle, sysid, kern, nf):
-    """OVS_MIXED solves the FP64 system: every field of its solution is
-    within 1e-5 (relative to the field's largest value) of the restarted
-    FP64 GMRES solution, and of the oracle's dense solve of the FP64 system,
-    and its true FP64 residual meets rtol.  The FP32-assembled system's
-    solution (OVS_FP32) is further away; that difference is the FP32
-    assembly's rounding, which OVS_MIXED does not inherit."""
+    """OVS_MIXED solves the FP64 system: its true residual on the FP64
+    system (rechecked with the oracle's SpMV) meets rtol, and every field of
+    its solution is within 1e-5 (relative to the field's largest value) of
+    the restarted FP64 GMRES solution.  Both run to rtol 1e-12: on this box a
+    relative residual of 1e-10 leaves up to 8e-4 of uncertainty in the VOF
+    field of ANY solution (the pressure correction is ~1e7 and dominates the
+    residual norm), so field-by-field agreement is only meaningful when both
+    solves are tight.  The FP32 rounding of the matrix is what the inner
+    cycles used."""
     case = M.quench_case(M.box_tet(8, 8, 8), "q8")
     ctx = _ctx(case)
     ctx.assemble(kern, 6, F.OVS_FP64)
-    s64, i64 = ctx.solve(sysid, F.OVS_FP64, 1e-10, 50, 300)
-    smx, imx = ctx.solve(sysid, F.OVS_MIXED, 1e-10, 50, 300)
-    assert i64.converged and imx.converged and imx.rel_residual <= 1e-10
+    s64, i64 = ctx.solve(sysid, F.OVS_FP64, 1e-12, 50, 600)
+    smx, imx = ctx.solve(sysid, F.OVS_MIXED, 1e-12, 50, 600)
+    assert i64.converged and imx.converged and imx.rel_residual <= 1e-12
     oc = oracle.OracleCase(case)
     sysblocks = ctx.get_system(sysid, F.OVS_FP64)
     oc.load_system(KIND[sysid], sysblocks)
     r = sysblocks["rhs"] - oc.spmv(KIND[sysid], smx)
-    assert np.linalg.norm(r) <= 1.05e-10 * np.linalg.norm(sysblocks["rhs"])
+    assert np.linalg.norm(r) <= 2e-12 * np.linalg.norm(sysblocks["rhs"])
     for f in range(nf):
         scale = max(np.abs(s64[:, f]).max(), 1e-300)
         assert np.abs(smx[:, f] - s64[:, f]).max() <= 1e-5 * scale, f
-    # the FP32 rounding of the matrix is what the inner cycles used
     for b in SYS_BLOCKS[sysid]:
         a32 = ctx.get_lhs(sysid, F.OVS_FP32, b)
         np.testing.assert_array_equal(a32, sysblocks[BLOCK_NAME[b]].astype(np.float32).astype(np.float64))
 
 
-def test_mixed_vs_fp64_solution_error():
+def test_mixed_vs_fp64_solution_error(oracle):
+    """The FP32-assembled system (OVS_FP32) is a different system: its
+    solution has an FP64 residual far above what OVS_MIXED reaches on the
+    same FP64 system, and stays within the FP32 assembly's rounding times the
+    condition number of the FP64 solution."""
     case = M.quench_case(M.box_tet(8, 8, 8), "q8")
     ctx = _ctx(case)
     ctx.assemble(F.OVS_ASM_NSVOF, 6, F.OVS_FP64)
-    s64, i64 = ctx.solve(F.OVS_SYS_NSVOF, F.OVS_FP64, 1e-10, 50, 300)
-    smx, imx = ctx.solve(F.OVS_SYS_NSVOF, F.OVS_MIXED, 1e-10, 50, 300)
+    s64, i64 = ctx.solve(F.OVS_SYS_NSVOF, F.OVS_FP64, 1e-12, 50, 600)
+    smx, imx = ctx.solve(F.OVS_SYS_NSVOF, F.OVS_MIXED, 1e-12, 50, 600)
+    sys64 = ctx.get_system(F.OVS_SYS_NSVOF, F.OVS_FP64)
     ctx.assemble(F.OVS_ASM_NSVOF, 6, F.OVS_FP32)
-    s32, i32 = ctx.solve(F.OVS_SYS_NSVOF, F.OVS_FP32, 1e-10, 50, 300)
+    s32, i32 = ctx.solve(F.OVS_SYS_NSVOF, F.OVS_FP32, 1e-12, 50, 600)
     assert i64.converged and imx.converged and i32.converged
+    oc = oracle.OracleCase(case)
+    oc.load_system("nsvof", sys64)
+    bn = np.linalg.norm(sys64["rhs"])
+    res_mx = np.linalg.norm(sys64["rhs"] - oc.spmv("nsvof", smx)) / bn
+    res_32 = np.linalg.norm(sys64["rhs"] - oc.spmv("nsvof", s32)) / bn
+    assert res_mx <= 2e-12 and res_32 > 1e3 * res_mx, (res_mx, res_32)
     for f in range(5):
         scale = max(np.abs(s64[:, f]).max(), 1e-300)
         assert np.abs(smx[:, f] - s64[:, f]).max() <= 1e-5 * scale, f
-        assert np.abs(s32[:, f] - s64[:, f]).max() <= 1e-3 * scale, f   # FP32 assembly: O(kappa * 1e-7)
+        assert np.abs(s32[:, f] - s64[:, f]).max() <= 1e-2 * scale, f   # FP32 assembly: O(kappa * 1e-7)
 
 
 # ------------------------------------------------------------ error paths
