@@ -530,6 +530,16 @@ def run_ours(args, world, rank, local_rank, dist):
                 rows_ab[f"{kn}_{nm}_{'staged' if staged else 'global'}_ms"] = \
                     ctx.profile(F.OVS_PROF_ASSEMBLE_ROWS, kern, prec, 5)
     prof["rows_variants"] = rows_ab
+    # the FP64 element pass with the node records in shared memory (default)
+    # against registers
+    elem_ab = {}
+    for sm in (0, 1):           # ends on the library default
+        ctx.set_option(F.OVS_OPT_ELEM_SMEM, sm)
+        for kern, kn in ((F.OVS_ASM_NSVOF, "nsvof"), (F.OVS_ASM_TEM, "tem")):
+            ctx.assemble(kern, 6, F.OVS_FP64)
+            elem_ab[f"{kn}_fp64_{'smem' if sm else 'registers'}_ms"] = \
+                ctx.profile(F.OVS_PROF_ASSEMBLE_ELEMENTS, kern, F.OVS_FP64, 5)
+    prof["element_variants"] = elem_ab
     ctx.assemble(F.OVS_ASM_NSVOF, 6, F.OVS_FP32)
     ctx.assemble(F.OVS_ASM_NSVOF, 6, F.OVS_FP64)
     prof["spmv_nsvof_fp32_ms"] = ctx.profile(F.OVS_PROF_SPMV, F.OVS_SYS_NSVOF, F.OVS_FP32, 20)

@@ -106,9 +106,11 @@ enum {
                                   0 (default, the faster one measured; env OVS_HEX_TC=1 sets 1): the
                                   CUDA-core row expansion */
   OVS_OPT_ARNOLDI_FUSED = 2,   /* 1: one-launch Arnoldi variant (default 0; env OVS_ARNOLDI_FUSED=1) */
-  OVS_OPT_ROWS_STAGED = 3      /* tet row pass: 1 (env OVS_ROWS_STAGED=1) stages each chunk's element
-                                  summaries in shared memory with asynchronous copies; 0 (default) reads them
-                                  from global memory lane by lane */
+  OVS_OPT_ROWS_STAGED = 3,     /* tet row pass, NS and NS+VOF kernels: 1 (default) stages each chunk's element
+                                  summaries in shared memory with asynchronous copies; 0 (env OVS_ROWS_STAGED=0)
+                                  reads them from global memory lane by lane */
+  OVS_OPT_ELEM_SMEM = 4        /* FP64 tet element pass: 1 (default) holds the node records in shared memory;
+                                  0 (env OVS_ELEM_SMEM=0) in registers */
 };
 
 /* boundary-face flags (ovs_set_faces) */

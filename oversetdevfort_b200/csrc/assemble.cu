@@ -841,8 +841,6 @@ __device__ __forceinline__ void cp_async_wait_all() {
 // the compiler chooses (tighter bounds spill)
 template <typename T, int KIND> struct SumMinBlocks { static constexpr int v = 1; };
 template <> struct SumMinBlocks<float, OVS_ASM_NSVOF> { static constexpr int v = 3; };
-template <> struct SumMinBlocks<double, OVS_ASM_NSVOF> { static constexpr int v = 3; };
-template <> struct SumMinBlocks<double, OVS_ASM_TEM> { static constexpr int v = 3; };
 
 // FP64 node records held in shared memory instead of registers (64 values
 // per element, transposed so a warp's accesses hit 32 consecutive banks),
@@ -863,8 +861,13 @@ template <typename T> struct ZeroRecs {
   __device__ __forceinline__ ZeroRow<T> operator[](int) const { return ZeroRow<T>{}; }
 };
 
-template <typename T, int KIND>
-__global__ void __launch_bounds__(128, SumMinBlocks<T, KIND>::v)
+// SMEMREC (FP64 only): the node records through shared memory (a 3-block
+// register bound) instead of registers (255 registers, 2 blocks)
+template <typename T, int KIND, bool SMEMREC> struct SumBlocks { static constexpr int v = SumMinBlocks<T, KIND>::v; };
+template <int KIND> struct SumBlocks<double, KIND, true> { static constexpr int v = 3; };
+
+template <typename T, int KIND, bool SMEMREC>
+__global__ void __launch_bounds__(128, (SumBlocks<T, KIND, SMEMREC>::v))
 element_summary_kernel(const SumArgs a) {
   using L = Lay<KIND>;
   const int e = blockIdx.x * blockDim.x + threadIdx.x;
@@ -887,7 +890,7 @@ element_summary_kernel(const SumArgs a) {
         summarize_tem<T>(a, r, lo, eid == a.p.fluid_elm_id, o, cfl, detj);
       }
     };
-    if constexpr (sizeof(T) == 8) {
+    if constexpr (SMEMREC && sizeof(T) == 8) {
       // records through shared memory; the summary written straight to
       // global memory as its values are produced
       extern __shared__ __align__(16) unsigned char sm_elem[];
@@ -1199,11 +1202,15 @@ template <typename T, int KIND>
 int launch_assemble(ovs_ctx* c, const AsmArgs& a, const SumArgs& sa, int parts = 3) {
   // pass 1: element summaries
   if (parts & 1) {
-    // FP64: the node records of the block's 128 elements in shared memory
-    const size_t esm = sizeof(T) == 8 ? sizeof(T) * 64 * 128 : 0;
-    if (esm) OVS_CUDA_TRY(cudaFuncSetAttribute(element_summary_kernel<T, KIND>,
-                                               cudaFuncAttributeMaxDynamicSharedMemorySize, (int)esm));
-    element_summary_kernel<T, KIND><<<(sa.E + 127) / 128, 128, esm, c->stream>>>(sa);
+    if (sizeof(T) == 8 && c->elem_smem) {
+      // the node records of the block's 128 elements in shared memory
+      const size_t esm = sizeof(T) * 64 * 128;
+      OVS_CUDA_TRY(cudaFuncSetAttribute(element_summary_kernel<T, KIND, true>,
+                                        cudaFuncAttributeMaxDynamicSharedMemorySize, (int)esm));
+      element_summary_kernel<T, KIND, true><<<(sa.E + 127) / 128, 128, esm, c->stream>>>(sa);
+    } else {
+      element_summary_kernel<T, KIND, false><<<(sa.E + 127) / 128, 128, 0, c->stream>>>(sa);
+    }
     ++c->launches;
     OVS_CUDA_TRY(cudaGetLastError());
   }

@@ -198,6 +198,8 @@ int create_resources(ovs_ctx* c, const ovs_dims* dims) {
     c->hex_tc = h && h[0] == '1';
     const char* rs = getenv("OVS_ROWS_STAGED");
     if (rs) c->rows_staged = rs[0] != '0';
+    const char* es = getenv("OVS_ELEM_SMEM");
+    if (es) c->elem_smem = es[0] != '0';
   }
   c->N = dims->nnode;
   c->E = dims->nelem;
@@ -400,6 +402,7 @@ int ovs_set_option(ovs_ctx* c, int option, int value) {
   switch (option) {
     case OVS_OPT_HEX_TC: c->hex_tc = value != 0; return OVS_OK;
     case OVS_OPT_ROWS_STAGED: c->rows_staged = value != 0; return OVS_OK;
+    case OVS_OPT_ELEM_SMEM: c->elem_smem = value != 0; return OVS_OK;
     case OVS_OPT_ARNOLDI_FUSED: c->arnoldi_fused = value != 0; return OVS_OK;
     default: return OVS_ERR_ARG;
   }
