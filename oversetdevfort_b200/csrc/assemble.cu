@@ -92,6 +92,27 @@ __device__ __forceinline__ void tet_shape(int g, T N[4]) {
   N[3] = (T)1.0 - xi - eta - ze;
 }
 
+// FP64 node records held in shared memory instead of registers (64 values
+// per element, transposed so a warp's accesses hit 32 consecutive banks),
+// and zero rounding remainders: the FP64 element routines otherwise need
+// more registers than a thread has.
+template <typename T> struct SmemRecRow {
+  const volatile T* p;   // volatile: read where used, not hoisted into registers
+  __device__ __forceinline__ T operator[](int k) const { return p[(size_t)k * 128]; }
+};
+template <typename T> struct SmemRecs {
+  const T* p;   // this thread's column of a [64][128] block array
+  __device__ __forceinline__ SmemRecRow<T> operator[](int n) const { return SmemRecRow<T>{p + (size_t)n * 16 * 128}; }
+};
+template <typename T> struct ZeroRow {
+  __device__ __forceinline__ T operator[](int) const { return (T)0; }
+};
+template <typename T> struct ZeroRecs {
+  __device__ __forceinline__ ZeroRow<T> operator[](int) const { return ZeroRow<T>{}; }
+};
+
+// SMEMREC (FP64 only): the node records through shared memory (a 3-block
+// register bound) instead of registers (255 registers, 2 blocks)
 // Type of the VOF value and of the property blend: FP64 for the FP32 and
 // FP64 routines, the dual number itself for the adjoint.
 template <typename T> struct Wide { using type = double; };
@@ -408,7 +429,7 @@ __device__ void summarize_nsvof(const SumArgs& a, const RA& r, const LA& lo, boo
   T ru[4][3], rp[4], rf[4];
 #pragma unroll
   for (int n = 0; n < 4; ++n) { ru[n][0] = ru[n][1] = ru[n][2] = 0; rp[n] = 0; rf[n] = 0; }
-#pragma unroll (sizeof(T) == 8 ? 1 : 4)
+#pragma unroll (std::is_same<RA, SmemRecs<T>>::value ? 1 : 4)
   for (int gp = 0; gp < 4; ++gp) {
     T N[4];
     tet_shape<T>(gp, N);
@@ -842,27 +863,6 @@ __device__ __forceinline__ void cp_async_wait_all() {
 template <typename T, int KIND> struct SumMinBlocks { static constexpr int v = 1; };
 template <> struct SumMinBlocks<float, OVS_ASM_NSVOF> { static constexpr int v = 3; };
 
-// FP64 node records held in shared memory instead of registers (64 values
-// per element, transposed so a warp's accesses hit 32 consecutive banks),
-// and zero rounding remainders: the FP64 element routines otherwise need
-// more registers than a thread has.
-template <typename T> struct SmemRecRow {
-  const volatile T* p;   // volatile: read where used, not hoisted into registers
-  __device__ __forceinline__ T operator[](int k) const { return p[(size_t)k * 128]; }
-};
-template <typename T> struct SmemRecs {
-  const T* p;   // this thread's column of a [64][128] block array
-  __device__ __forceinline__ SmemRecRow<T> operator[](int n) const { return SmemRecRow<T>{p + (size_t)n * 16 * 128}; }
-};
-template <typename T> struct ZeroRow {
-  __device__ __forceinline__ T operator[](int) const { return (T)0; }
-};
-template <typename T> struct ZeroRecs {
-  __device__ __forceinline__ ZeroRow<T> operator[](int) const { return ZeroRow<T>{}; }
-};
-
-// SMEMREC (FP64 only): the node records through shared memory (a 3-block
-// register bound) instead of registers (255 registers, 2 blocks)
 template <typename T, int KIND, bool SMEMREC> struct SumBlocks { static constexpr int v = SumMinBlocks<T, KIND>::v; };
 template <int KIND> struct SumBlocks<double, KIND, true> { static constexpr int v = 3; };
 
