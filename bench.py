@@ -530,10 +530,10 @@ def run_ours(args, world, rank, local_rank, dist):
                 rows_ab[f"{kn}_{nm}_{'staged' if staged else 'global'}_ms"] = \
                     ctx.profile(F.OVS_PROF_ASSEMBLE_ROWS, kern, prec, 5)
     prof["rows_variants"] = rows_ab
-    # the FP64 element pass with the node records in shared memory (default)
-    # against registers
+    # the FP64 element pass with the node records in registers (default)
+    # against shared memory
     elem_ab = {}
-    for sm in (0, 1):           # ends on the library default
+    for sm in (1, 0):           # ends on the library default
         ctx.set_option(F.OVS_OPT_ELEM_SMEM, sm)
         for kern, kn in ((F.OVS_ASM_NSVOF, "nsvof"), (F.OVS_ASM_TEM, "tem")):
             ctx.assemble(kern, 6, F.OVS_FP64)

@@ -834,7 +834,7 @@ template <typename T, int KIND> struct Smem {
   __host__ __device__ static size_t bytes(int max_deg, bool staged = false) {
     size_t b = sizeof(T) * ((size_t)4 * CH * BSTR + (size_t)CH * RSTR + (size_t)max_deg * NVP);
     b = (b + 15) & ~(size_t)15;
-    b += sizeof(int) * ((size_t)4 * CH + 2 * (size_t)max_deg);
+    b += sizeof(int) * ((size_t)4 * CH + max_deg);
     b = (b + 15) & ~(size_t)15;
     if (staged) b += sizeof(T) * (size_t)CH * SW;
     return b;
@@ -960,7 +960,6 @@ assemble_rows_kernel(const AsmArgs a) {
   off = (off + 15) & ~(size_t)15;
   int* slot = reinterpret_cast<int*>(base + off);      // [CH][4]
   int* cols = slot + 4 * CH;                           // [max_deg]
-  int* colib = cols + a.max_deg;                       // [max_deg] IBC of the row's columns (STAGED)
 
   const T* sum = reinterpret_cast<const T*>(a.rec);
   const int nwarps_total = gridDim.x * WARPS;
@@ -970,47 +969,13 @@ assemble_rows_kernel(const AsmArgs a) {
   const int jl = lane / LPE, bl0 = lane % LPE;
   constexpr int U16 = L::SW * (int)sizeof(T) / 16;          // 16-byte units per summary
   static_assert(L::SW * sizeof(T) % 16 == 0, "summaries must be whole 16-byte units");
-  // rows in the spatial order of the nodes (when given), so that the rows
-  // sharing an element are in flight together and its summary is read from
-  // L2 rather than DRAM
-  auto order = [&](int tt) { return a.row_order ? __ldg(a.row_order + tt) : tt; };
-  // STAGED: a software pipeline over the warp's rows.  The next row's
-  // pointers load while this row starts, the id of the row after it one row
-  // earlier still, and the next row's first-chunk element ids once this
-  // row's first chunk has been copied; each row then starts without a
-  // dependent round trip to global memory.
-  int t = blockIdx.x * WARPS + wid;
-  int hA = 0, hrp = 0, hrp1 = 0, hep = 0, hep1 = 0;   // header of the row at t
-  int nA = 0;                                         // row id at t + stride
-  int pk_n = 0;
-  unsigned s4_n = 0;
-  if (STAGED && t < a.N) {
-    hA = order(t);
-    hrp = a.rowptr[hA]; hrp1 = a.rowptr[hA + 1];
-    hep = a.n2e_ptr[hA]; hep1 = a.n2e_ptr[hA + 1];
-    if (lane < min(CH, hep1 - hep)) {
-      pk_n = __ldg(a.n2e + hep + lane);
-      s4_n = __ldg(a.n2s + hep + lane);
-    }
-    if (t + nwarps_total < a.N) nA = order(t + nwarps_total);
-  }
-  for (; t < a.N; t += nwarps_total) {
-    int A, rp, deg, ep, ne;
-    int xrp = 0, xrp1 = 0, xep = 0, xep1 = 0, xA = 0;   // next row's header, in flight
-    const bool has_next = t + nwarps_total < a.N;
-    if constexpr (STAGED) {
-      A = hA; rp = hrp; deg = hrp1 - hrp; ep = hep; ne = hep1 - hep;
-      if (has_next) {
-        xrp = a.rowptr[nA]; xrp1 = a.rowptr[nA + 1];
-        xep = a.n2e_ptr[nA]; xep1 = a.n2e_ptr[nA + 1];
-        if (t + 2 * nwarps_total < a.N) xA = order(t + 2 * nwarps_total);
-      }
-    } else {
-      A = order(t);
-      rp = a.rowptr[A]; deg = a.rowptr[A + 1] - rp;
-      ep = a.n2e_ptr[A]; ne = a.n2e_ptr[A + 1] - ep;
-    }
-    const unsigned ibA = __ldg(a.ibc + A);   // needed at the row write; issued now
+  for (int t = blockIdx.x * WARPS + wid; t < a.N; t += nwarps_total) {
+    // rows in the spatial order of the nodes (when given), so that the rows
+    // sharing an element are in flight together and its summary is read
+    // from L2 rather than DRAM
+    const int A = a.row_order ? __ldg(a.row_order + t) : t;
+    const int rp = a.rowptr[A], deg = a.rowptr[A + 1] - rp;
+    const int ep = a.n2e_ptr[A], ne = a.n2e_ptr[A + 1] - ep;
     if constexpr (STAGED) {
       for (int s = lane; s < deg; s += 32) cp_async4(cols + s, a.colidx + rp + s);
     } else {
@@ -1018,8 +983,13 @@ assemble_rows_kernel(const AsmArgs a) {
     }
     for (int q = lane; q < deg * NVP; q += 32) acc[q] = (T)0;
     T racc = (T)0;
-    int pk_f = 0, ibq = 0;           // next row's first-chunk ids; IBC of column `lane`
-    unsigned s4_f = 0;
+    // element ids and slots of the row's first chunk (lanes j < nc hold entry j)
+    int pk_n = 0;
+    unsigned s4_n = 0;
+    if (STAGED && lane < min(CH, ne)) {
+      pk_n = __ldg(a.n2e + ep + lane);
+      s4_n = __ldg(a.n2s + ep + lane);
+    }
     __syncwarp();
     for (int c0 = 0; c0 < ne; c0 += CH) {
       const int nc = min(CH, ne - c0);
@@ -1046,15 +1016,6 @@ assemble_rows_kernel(const AsmArgs a) {
         }
         cp_async_wait_all();
         __syncwarp();
-        if (c0 == 0) {
-          // the columns have landed: their IBC bytes, and the next row's
-          // first-chunk ids, travel while the row is expanded
-          if (lane < deg) ibq = __ldg(a.ibc + cols[lane]);
-          if (has_next && lane < min(CH, xep1 - xep)) {
-            pk_f = __ldg(a.n2e + xep + lane);
-            s4_f = __ldg(a.n2s + xep + lane);
-          }
-        }
       }
       // ---------------- phase 1: block (A's row, column bl) of element jl
       int packed;
@@ -1119,18 +1080,9 @@ assemble_rows_kernel(const AsmArgs a) {
     if constexpr (STAGED) {   // the row's column copies (a node without elements skips the chunk loop)
       cp_async_wait_all();
       __syncwarp();
-      if (ne == 0) {
-        if (lane < deg) ibq = __ldg(a.ibc + cols[lane]);
-        if (has_next && lane < min(CH, xep1 - xep)) {
-          pk_f = __ldg(a.n2e + xep + lane);
-          s4_f = __ldg(a.n2s + xep + lane);
-        }
-      }
-      if (lane < deg) colib[lane] = ibq;
-      for (int q = 32 + lane; q < deg; q += 32) colib[q] = __ldg(a.ibc + cols[q]);
-      __syncwarp();
     }
     // ---------------- row write with the Dirichlet treatment
+    const unsigned ibA = a.ibc[A];
     if (a.mat) {
       T* out = reinterpret_cast<T*>(a.vals) + (size_t)rp * NV;
       const T cnt = (T)ne;
@@ -1140,7 +1092,7 @@ assemble_rows_kernel(const AsmArgs a) {
         for (int q = lane; q < deg * NG; q += 32) {
           const int s = q / NG, gidx = q - s * NG;
           const int B = cols[s];
-          const unsigned ibB = STAGED ? (unsigned)colib[s] : (unsigned)__ldg(a.ibc + B);
+          const unsigned ibB = __ldg(a.ibc + B);
           const bool dg = B == A;
           T v4[4];
 #pragma unroll
@@ -1173,12 +1125,6 @@ assemble_rows_kernel(const AsmArgs a) {
       __stcs(reinterpret_cast<T*>(a.rhs) + (size_t)lane * a.N + A, v);
     }
     __syncwarp();
-    if constexpr (STAGED) {   // the pipeline moves one row on
-      hA = nA; hrp = xrp; hrp1 = xrp1; hep = xep; hep1 = xep1;
-      nA = xA;
-      pk_n = pk_f;
-      s4_n = s4_f;
-    }
   }
 }
 

@@ -120,8 +120,8 @@ struct ovs_ctx {
   // tet row pass: element summaries staged through shared memory by
   // asynchronous copies (1, default) or read by every lane from global memory
   int rows_staged = 1;
-  // FP64 element pass: node records in shared memory (1) or registers (0)
-  int elem_smem = 1;
+  // FP64 element pass: node records in registers (0, measured faster) or shared memory (1)
+  int elem_smem = 0;
   void* hex_kbuf = nullptr;              // E x 64 x 24 block values
   float* hex_w = nullptr;                // W hi + lo, canonical layout
   // boundary-condition producers (ovs_set_bc_spec)
