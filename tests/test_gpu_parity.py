@@ -437,3 +437,49 @@ def test_element_pass_variants_bit_identical(kind):
         ctx.close()
     for k in out[0]:
         close(out[1][k], out[0][k], 1e-14, k)
+
+
+def _relabel(case, seed):
+    """The same case with its nodes numbered by a random permutation (an
+    unstructured numbering: rows far apart in memory share elements)."""
+    import copy
+    rng = np.random.default_rng(seed)
+    m = case.mesh
+    N = m.nnode
+    new_of_old = rng.permutation(N)               # old node i -> new node new_of_old[i]
+    old_of_new = np.argsort(new_of_old)
+    ien = np.asfortranarray((new_of_old[np.asarray(m.ien) - 1] + 1).astype(np.int32))
+    xg = np.asfortranarray(m.xg[old_of_new])
+    faces = [np.sort(new_of_old[f]) for f in m.faces]
+    mesh = M.Mesh(xg, ien, m.elm_id.copy(), faces, m.dims, m.lengths)
+    state = {k: np.asfortranarray(np.asarray(v)[old_of_new]) for k, v in case.state.items()}
+    ibc = np.asfortranarray(np.asarray(case.ibc)[old_of_new])
+    c = copy.copy(case)
+    c.mesh, c.state, c.ibc = mesh, state, ibc
+    return c, old_of_new
+
+
+@pytest.mark.parametrize("kind", ["nsvof", "tem"])
+@pytest.mark.parametrize("prec,tol", [(F.OVS_FP64, 1e-12), (F.OVS_FP32, 1e-5)])
+def test_assembly_on_a_permuted_numbering(oracle, kind, prec, tol):
+    """A random node numbering (rows that share an element far apart, the
+    spatial row order a true permutation) assembles to the oracle's system
+    on the same numbering, and its residual is the structured numbering's,
+    permuted."""
+    kernel = F.OVS_ASM_NSVOF if kind == "nsvof" else F.OVS_ASM_TEM
+    base = M.random_case(nx=6, ny=5, nz=4, seed=40, kernel=kernel)
+    case, old_of_new = _relabel(base, 7)
+    oc, ctx, sysid, k, cfl_o, cfl_g = _assemble_both(oracle, case, kernel, 6, prec)
+    _compare_system(oc, ctx, sysid, k, 6, prec, tol)
+    col, row = ctx.get_pattern()
+    col_o, row_o = oracle.gen_spar_struc(case.mesh.ien, case.mesh.nnode)
+    np.testing.assert_array_equal(col, col_o)
+    np.testing.assert_array_equal(row, row_o)
+    np.testing.assert_array_equal(ctx.get_slot_map(), oracle.slot_map(case.mesh.ien, col, row))
+    r_perm = ctx.get_rhs(sysid, prec)
+    ctx.close()
+    ctx2 = _ctx(base)
+    ctx2.assemble(kernel, 6, prec)
+    r_base = ctx2.get_rhs(sysid, prec)
+    ctx2.close()
+    close(r_perm, r_base[old_of_new], tol, "permuted residual")
