@@ -983,7 +983,6 @@ assemble_rows_kernel(const AsmArgs a) {
     }
     for (int q = lane; q < deg * NVP; q += 32) acc[q] = (T)0;
     T racc = (T)0;
-    T racc_s = (T)0;   // scalar rows with at most 32 slots: slot `lane`'s sum
     // element ids and slots of the row's first chunk (lanes j < nc hold entry j)
     int pk_n = 0;
     unsigned s4_n = 0;
@@ -1068,13 +1067,6 @@ assemble_rows_kernel(const AsmArgs a) {
           }
           __syncwarp();
         }
-      } else if (deg <= 32) {
-        // scalar rows: lane s owns slot s in a register and adds the
-        // chunk's entries for it in element order (an element's 4 entries
-        // go to distinct slots), the same order as the serial loop below,
-        // without a warp barrier per element
-        for (int q = 0; q < 4 * nc; ++q)
-          if (slot[q] == lane) racc_s += blk[q];
       } else {
         for (int j = 0; j < nc; ++j) {
           if (lane < 4) acc[slot[j * 4 + lane]] += blk[j * 4 + lane];
@@ -1117,7 +1109,7 @@ assemble_rows_kernel(const AsmArgs a) {
         for (int q = lane; q < deg; q += 32) {
           const int B = cols[q];
           const unsigned ibB = __ldg(a.ibc + B);
-          T val = deg <= 32 ? racc_s : acc[q];
+          T val = acc[q];
           if ((ibA & TB) || (ibB & TB)) val = (T)0;
           if (B == A && (ibA & TB)) val = cnt;
           __stcs(out + q, val);
