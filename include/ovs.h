@@ -384,6 +384,13 @@ int ovs_gmres(ovs_ctx* ctx, int system, double tol, int kspace,
 int ovs_solve(ovs_ctx* ctx, int system, int mode, double rtol, int kspace,
               int max_cycles, double* sol, ovs_solve_info* info);
 
+/* The FP32 matrix of `system` := the FP32 rounding of its FP64 matrix (needs
+ * an FP64 assembly of `system`): the inner operator of the OVS_MIXED
+ * refinement, for a solve driven from outside (the partitioned Newton loop);
+ * ovs_solve(OVS_MIXED) does the same itself.  No reference counterpart (a
+ * part of the mixed-precision extension). */
+int ovs_round_matrix(ovs_ctx* ctx, int system);
+
 /* Newton update with the last solution of `system` (src/solveFlow.f90:99-104,
  * 139-140; src/solveOverset.f90:76-78):
  *   NS/NSVOF: acg += du; ug += gami*Delt*du; pg += alfi*gami*Delt*dp;

@@ -51,7 +51,7 @@ EXPORTS = [
     "ovs_create", "ovs_destroy", "ovs_synchronize", "ovs_get_stream", "ovs_upload_mesh",
     "ovs_build_pattern", "ovs_get_pattern", "ovs_get_slot_map", "ovs_set_params", "ovs_set_ibc", "ovs_set_field",
     "ovs_get_field", "ovs_assemble", "ovs_get_rhs", "ovs_set_rhs", "ovs_get_lhs_block",
-    "ovs_set_lhs_block", "ovs_spmv", "ovs_gmres", "ovs_solve", "ovs_newton_update", "ovs_set_solution", "ovs_predictor", "ovs_commit_old",
+    "ovs_set_lhs_block", "ovs_spmv", "ovs_gmres", "ovs_solve", "ovs_round_matrix", "ovs_newton_update", "ovs_set_solution", "ovs_predictor", "ovs_commit_old",
     "ovs_residual_norms", "ovs_profile", "ovs_launch_count", "ovs_last_device_ms",
     "ovs_host_alloc", "ovs_host_free", "ovs_residual_vjp", "ovs_gmres_transposed", "ovs_quench_newton",
     "ovs_quench_time_steps", "ovs_stage_fields", "ovs_commit_staged", "ovs_get_rhs_async", "ovs_sync_copies",
@@ -163,6 +163,7 @@ def load(path: str | os.PathLike | None = None) -> C.CDLL:
         "ovs_gmres": ([vp, C.c_int, C.c_double, C.c_int, C.c_int, dp, C.POINTER(OvsGmresInfo)], C.c_int),
         "ovs_solve": ([vp, C.c_int, C.c_int, C.c_double, C.c_int, C.c_int, dp,
                        C.POINTER(OvsSolveInfo)], C.c_int),
+        "ovs_round_matrix": ([vp, C.c_int], C.c_int),
         "ovs_newton_update": ([vp, C.c_int], C.c_int),
         "ovs_set_solution": ([vp, C.c_int, vp], C.c_int),
         "ovs_predictor": ([vp], C.c_int),

@@ -347,6 +347,11 @@ class Context:
                                                C.byref(info), C.byref(kt)), "ovs_quench_time_steps")
         return info, kt.value
 
+    def round_matrix(self, system: int):
+        """ovs_round_matrix: the FP32 matrix of `system` := the FP32 rounding
+        of its FP64 matrix (the inner operator of the OVS_MIXED refinement)."""
+        F.check(self.lib.ovs_round_matrix(self.h, system), "ovs_round_matrix")
+
     def newton_update(self, system: int):
         F.check(self.lib.ovs_newton_update(self.h, system), "ovs_newton_update")
 

@@ -710,6 +710,14 @@ int ovs_solve(ovs_ctx* c, int sys, int mode, double rtol, int kspace, int max_cy
   return OVS_OK;
 }
 
+int ovs_round_matrix(ovs_ctx* c, int sys) {
+  if (!sys_ok(c, sys, OVS_FP64)) return OVS_ERR_ARG;
+  int st;
+  if ((st = ovs_activate(c)) || (st = ovs_round_impl(c, sys))) return st;
+  OVS_CUDA_TRY(cudaStreamSynchronize(c->stream));
+  return OVS_OK;
+}
+
 int ovs_newton_update(ovs_ctx* c, int sys) {
   if (!sys_ok(c, sys, OVS_FP64)) return OVS_ERR_ARG;
   if (!c->sol[sys] || !c->have_params) return OVS_ERR_STATE;

@@ -1278,6 +1278,23 @@ int ovs_gmres_ref_impl(ovs_ctx* c, int sys, double tol, int kspace, int kmin, do
   return OVS_OK;
 }
 
+// The FP32 matrix of `sys` := the FP32 rounding of its FP64 matrix (queued
+// on the context stream).
+int ovs_round_impl(ovs_ctx* c, int sys) {
+  SysStore& S = c->sys[sys][OVS_FP64];
+  if (!S.vals) return OVS_ERR_STATE;
+  SysStore& S32 = c->sys[sys][OVS_FP32];
+  const size_t nv = (size_t)c->nnz * ovs_sys_nv(sys);
+  int st;
+  if ((st = ovs_ensure(&S32.vals, sizeof(float) * nv))) return st;
+  convert_kernel<double, float><<<ovs_grid(nv, 256, 16 * c->num_sms), 256, 0, c->stream>>>(
+      as<double>(S.vals), reinterpret_cast<float*>(S32.vals), nv);
+  ++c->launches;
+  OVS_CUDA_TRY(cudaGetLastError());
+  S32.have_mat = true;
+  return OVS_OK;
+}
+
 // Restarted / iteratively refined solve to a true FP64 relative residual.
 // `outer` is the system whose residual b - A x is driven to rtol (matrix and
 // right-hand side of that precision, FP64 arithmetic), `inner` the matrix
@@ -1301,17 +1318,8 @@ int ovs_solve_impl(ovs_ctx* c, int sys, int mode, double rtol, int kspace, int m
   double* b = c->work64;
   double* r = c->work64 + 5 * (size_t)N;
   OVS_CUDA_TRY(cudaEventRecord(c->ev0, s));
-  if (mode == OVS_MIXED) {
-    // the inner operator: FP32 rounding of the FP64 matrix values
-    SysStore& S32 = c->sys[sys][OVS_FP32];
-    const size_t nv = (size_t)c->nnz * ovs_sys_nv(sys);
-    if ((st = ovs_ensure(&S32.vals, sizeof(float) * nv))) return st;
-    convert_kernel<double, float><<<ovs_grid(nv, 256, 16 * c->num_sms), 256, 0, s>>>(
-        as<double>(S.vals), reinterpret_cast<float*>(S32.vals), nv);
-    ++c->launches;
-    OVS_CUDA_TRY(cudaGetLastError());
-    S32.have_mat = true;
-  }
+  // the inner operator of OVS_MIXED: FP32 rounding of the FP64 matrix values
+  if (mode == OVS_MIXED && (st = ovs_round_impl(c, sys))) return st;
   if ((st = ovs_precond_setup(c, sys, prec))) return st;
   if (outer == OVS_FP64) {
     OVS_CUDA_TRY(cudaMemcpyAsync(b, S.rhs, sizeof(double) * n, cudaMemcpyDeviceToDevice, s));

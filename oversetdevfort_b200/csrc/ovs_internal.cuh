@@ -205,6 +205,7 @@ int ovs_gmres_ref_impl(ovs_ctx* c, int sys, double tol, int kspace, int kmin,
                        double* dsol, ovs_gmres_info* info);
 int ovs_solve_impl(ovs_ctx* c, int sys, int mode, double rtol, int kspace,
                    int max_cycles, ovs_solve_info* info);
+int ovs_round_impl(ovs_ctx* c, int sys);
 int ovs_update_impl(ovs_ctx* c, int sys);
 int ovs_resnorm_impl(ovs_ctx* c, int prec, double r[4]);
 int ovs_dot_impl(ovs_ctx* c, const double* a, const double* b, size_t n,

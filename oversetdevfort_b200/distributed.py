@@ -423,6 +423,11 @@ class ContextPartition:
     def operator(self, kind: str, precision: int = F.OVS_FP64):
         return DeviceOperator(self.ctx, _KIND_SYS[kind], precision)
 
+    def round(self, kind: str):
+        """The FP32 rounding of the part's FP64 matrix of `kind` (the inner
+        operator of the OVS_MIXED refinement)."""
+        self.ctx.round_matrix(_KIND_SYS[kind])
+
     def update(self, kind: str, sol):
         self.ctx.set_solution(_KIND_SYS[kind], sol.contiguous())
         self.ctx.newton_update(_KIND_SYS[kind])
@@ -461,15 +466,18 @@ def quench_newton(comm, parts: dict, newton_max: int = 3, solve_tem: bool = True
     converged, field_converged, residual0, residual and the Krylov
     iterations of both systems.
 
-    mode OVS_FP32 is ovs_quench_newton's mixed mode over the partitions:
+    mode OVS_FP32 is ovs_quench_newton's OVS_FP32 mode over the partitions:
     FP32 assembly, residuals from the FP32 right-hand sides, and each solve
     by `solve_refined` on the FP32 operators to the relative residual tol_ns
-    / tol_tem (max_cycles refinement cycles) instead of one FP64 cycle.  The
+    / tol_tem (max_cycles refinement cycles) instead of one FP64 cycle.
+    mode OVS_MIXED is its OVS_MIXED mode: FP64 assembly and residuals, and
+    each solve by `solve_refined` with the FP64 operators outside and, inside,
+    the FP32 rounding of each part's FP64 matrix (the parts' `round`).  The
     parts then take a precision argument in assemble, residual_sq, rhs and
     operator, and their operators provide `apply`."""
     P = comm.parts()
-    mixed = mode == F.OVS_FP32
-    prec = F.OVS_FP32 if mixed else F.OVS_FP64
+    mixed = mode in (F.OVS_FP32, F.OVS_MIXED)
+    prec = F.OVS_FP32 if mode == F.OVS_FP32 else F.OVS_FP64
     pk = {"precision": prec} if mixed else {}
 
     def residual():
@@ -483,7 +491,13 @@ def quench_newton(comm, parts: dict, newton_max: int = 3, solve_tem: bool = True
     def solve(kind, tol):
         rhs = {r: parts[r].rhs(kind, **pk) for r in P}
         ops = {r: parts[r].operator(kind, **pk) for r in P}
-        if mixed:
+        if mode == F.OVS_MIXED:
+            for r in P:
+                parts[r].round(kind)
+            inner = {r: parts[r].operator(kind, precision=F.OVS_FP32) for r in P}
+            sol, info = solve_refined(comm, inner, ops, rhs, tol, kspace, max_cycles, tem=kind == "tem",
+                                      orthog=orthog)
+        elif mixed:
             sol, info = solve_refined(comm, ops, ops, rhs, tol, kspace, max_cycles, tem=kind == "tem", orthog=orthog)
         else:
             sol, info = gmres_cycle(comm, ops, rhs, tol, kspace, kspace_min, tem=kind == "tem", orthog=orthog)

@@ -152,3 +152,43 @@ def test_partitioned_newton_mixed_on_contexts():
             np.testing.assert_allclose(c.get_field(n), a[p.nodes], rtol=0, atol=1e-6 * max(np.abs(a).max(), 1e-300))
     for c in ctxs:
         c.close()
+
+
+def test_partitioned_newton_mixed_fp64_system_on_contexts():
+    """The OVS_MIXED loop over three contexts (ContextPartition.round:
+    ovs_round_matrix of each part's FP64 matrix as the inner operator,
+    refinement against the FP64 parts) against ovs_quench_newton OVS_MIXED
+    on one context: converged, the same Newton iterations within one, the
+    state within 1e-6."""
+    case = _case()
+    g = Context.from_case(case)
+    info = g.quench_newton(mode=F.OVS_MIXED, max_cycles=40, **OPTS)
+    ref = {n: g.get_field(n) for n in ("ug", "pg", "phig", "tg")}
+    g.close()
+    parts = P.make_parts(case.mesh, 3)
+    plan = D.halo_plan(parts)
+    ctxs = [Context.from_case(P.local_case(case, p)) for p in parts]
+    sp = {r: D.ContextPartition(c, plan.owned[r], device="cuda:0") for r, c in enumerate(ctxs)}
+    out = D.quench_newton(D.LocalComm(plan), sp, mode=F.OVS_MIXED, max_cycles=40, **OPTS)
+    assert out["converged"] and abs(out["iterations"] - info.iterations) <= 1
+    for n, a in ref.items():
+        for c, p in zip(ctxs, parts):
+            np.testing.assert_allclose(c.get_field(n), a[p.nodes], rtol=0, atol=1e-6 * max(np.abs(a).max(), 1e-300))
+    for c in ctxs:
+        c.close()
+
+
+def test_round_matrix_is_the_fp32_rounding():
+    """ovs_round_matrix writes the FP32 rounding of every FP64 matrix block
+    into the FP32 store, and refuses a system without an FP64 matrix."""
+    case = _case()
+    c = Context.from_case(case)
+    with pytest.raises(F.OvsError):
+        c.round_matrix(F.OVS_SYS_NSVOF)
+    c.assemble(F.OVS_ASM_NSVOF, 6, F.OVS_FP64)
+    c.round_matrix(F.OVS_SYS_NSVOF)
+    from oversetdevfort_b200.api import SYS_BLOCKS
+    for b in SYS_BLOCKS[F.OVS_SYS_NSVOF]:
+        a64 = c.get_lhs(F.OVS_SYS_NSVOF, F.OVS_FP64, b)
+        np.testing.assert_array_equal(c.get_lhs(F.OVS_SYS_NSVOF, F.OVS_FP32, b), a64.astype(np.float32).astype(np.float64))
+    c.close()
