@@ -106,11 +106,15 @@ enum {
                                   0 (default, the faster one measured; env OVS_HEX_TC=1 sets 1): the
                                   CUDA-core row expansion */
   OVS_OPT_ARNOLDI_FUSED = 2,   /* 1: one-launch Arnoldi variant (default 0; env OVS_ARNOLDI_FUSED=1) */
-  OVS_OPT_ROWS_STAGED = 3,     /* tet row pass, NS and NS+VOF kernels: 1 (default) stages each chunk's element
-                                  summaries in shared memory with asynchronous copies; 0 (env OVS_ROWS_STAGED=0)
-                                  reads them from global memory lane by lane */
-  OVS_OPT_ELEM_SMEM = 4        /* FP64 tet element pass: 0 (default, the faster one measured) holds the node
+  OVS_OPT_ROWS_STAGED = 3,     /* chunked tet row pass (OVS_OPT_ROWS_GATHER = 0), NS and NS+VOF kernels: 1
+                                  (default) stages each chunk's element summaries in shared memory with
+                                  asynchronous copies; 0 (env OVS_ROWS_STAGED=0) reads them from global memory
+                                  lane by lane */
+  OVS_OPT_ELEM_SMEM = 4,       /* FP64 tet element pass: 0 (default, the faster one measured) holds the node
                                   records in registers; 1 (env OVS_ELEM_SMEM=1) in shared memory */
+  OVS_OPT_ROWS_GATHER = 5      /* tet row pass: 1 (default) every lane gathers whole blocks of the row by the
+                                  contribution lists built with the pattern; 0 (env OVS_ROWS_GATHER=0) the
+                                  chunked pass, element blocks reduced through shared memory */
 };
 
 /* boundary-face flags (ovs_set_faces) */

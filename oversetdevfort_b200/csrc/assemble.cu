@@ -47,7 +47,9 @@ struct AsmArgs {
   const int* n2e_ptr;
   const int* n2e;
   const unsigned* n2s;    // slots of each entry's element nodes in the row
-  const int* row_order;   // processing order of the rows (a permutation), or null
+  const int4* row_rec;    // per row in processing order: {A, rowptr[A], n2e_ptr[A], deg | sd << 8 | ne << 16}
+  const int* cptr;        // off-diagonal contribution lists (tets): offsets per CSR entry
+  const int* clist;       //   entries (e << 4) | (la << 2) | b
   void* vals;             // nnz*NV
   void* rhs;              // NF*N field-major
   const void* kbuf;       // hex tensor-core block values (E x 64 x 24), or null
@@ -256,27 +258,115 @@ __device__ __forceinline__ void cfl_max(unsigned long long* bits, double v) {
 // needs from its Gauss points, once, plus the element's residual rows, and
 // stores it as a compact summary of SW values.  Pass 2 (one warp per CSR
 // row) expands A's row of each element matrix from the summaries.  Inactive
-// elements (solid on the NS+VOF pass, non-target on the NS pass) store w = 0
-// and zero residuals, which makes every expanded block exactly zero.
-//   NS   : g(12) w KA KB MM | GP x4: uadv(3) rt        | residual 4x4 = 48
-//   NSVOF: g(12) w KA KB MM KDP dphi(3) | GP x4: uadv(3) rho rt tauLS src
-//          eps ufac plfac pad(2)                       | residual 4x5 = 88
+// elements (solid on the NS+VOF pass, non-target on the NS pass) store zero
+// sums and zero residuals, which makes every expanded block exactly zero.
+// NS / NS+VOF: the Gauss-point sums of the block formulas (see
+// expand_block), which pass 1 forms once per element:
+//   [0, ND0)     per (row node a, column node b), PW values at PW (4a + b):
+//                NS+VOF {S_ab, L1_ab + E_ab, PL_ab, V_ab}, NS {S_ab}
+//   [ND0, C0)    per node n, 8 values: grad N_n (3), PR_n, T_n, U_n, Q_n, 0
+//   [C0, RHS0)   KA KB MM, then NS+VOF: KDP dphi (3) 0; NS: 0
+//   [RHS0, SW)   the residual, NF values per node
+// (PR_n is both P_b and R_a of the block formulas, U_n both U_b and W_a)
 //   TEM  : the 4x4 element matrix itself, row-major (a, b) | residual 4 = 20
 //          (a scalar system: its element matrix is smaller than the
 //          Gauss-point records it would be expanded from)
-// (Gauss-point records padded to 16-byte groups for vector loads)
-// with rt = rho tauM, trc = tauT rho cp and the factors of the block sums
-// below (src, eps, ufac, plfac of the phase-change terms).
+// GQ: the values pass 1 keeps per Gauss point for the sums: uadv (3) and
+// rt = rho tauM; NS+VOF: uadv (3) rho rt tauLS src eps ufac plfac (the
+// factors of the phase-change terms).
 template <int KIND> struct Lay;
 template <> struct Lay<OVS_ASM_NS> {
-  static constexpr int SW = 48, GP0 = 16, GPW = 4, RHS0 = 32, NF = 4, NV = 16;
+  static constexpr int PW = 1, ND0 = 16, C0 = 48, RHS0 = 52, SW = 68, NF = 4, NV = 16, GQ = 4;
 };
 template <> struct Lay<OVS_ASM_NSVOF> {
-  static constexpr int SW = 88, GP0 = 20, GPW = 12, RHS0 = 68, NF = 5, NV = 24;
+  static constexpr int PW = 4, ND0 = 64, C0 = 96, RHS0 = 104, SW = 124, NF = 5, NV = 24, GQ = 10;
 };
 template <> struct Lay<OVS_ASM_TEM> {
   static constexpr int SW = 20, RHS0 = 16, NF = 1, NV = 1;
 };
+
+// 4 values to 16-byte aligned memory (vector stores for the summaries)
+template <typename T>
+__device__ __forceinline__ void put4(T* d, T a, T b, T c, T e) {
+  d[0] = a; d[1] = b; d[2] = c; d[3] = e;
+}
+__device__ __forceinline__ void put4(float* d, float a, float b, float c, float e) {
+  *reinterpret_cast<float4*>(d) = make_float4(a, b, c, e);
+}
+__device__ __forceinline__ void put4(double* d, double a, double b, double c, double e) {
+  reinterpret_cast<double2*>(d)[0] = make_double2(a, b);
+  reinterpret_cast<double2*>(d)[1] = make_double2(c, e);
+}
+
+// The Gauss-point sums of the NS / NS+VOF block formulas (expand_block)
+// from the per-point values q (layout GQ above), the shape gradients g and
+// the weight w, written to the summary o: with c_n = uadv . grad N_n,
+//   S_ab  = sum w rho (Na + rt ca)(fact1 Nb + fact2 cb)
+//   L1_ab = sum w (Na + tauLS ca)(fact1 Nb + fact2 cb + fact2 Nb src)
+//   E_ab  = sum eps Na Nb      PL_ab = -sum plfac Na Nb
+//   V_ab  = sum fact2 w (Na + tauLS ca) Nb
+//   PR_n  = sum fact2 w Nn     T_n = sum w rt (fact1 Nn + fact2 cn)
+//   U_n   = sum ufac Nn        Q_n = sum fact2 w rt cn
+// (rho = rho_ns on the NS pass).  Each sum is formed once per element here
+// instead of once per block in the row pass.
+template <typename T, int KIND>
+__device__ __forceinline__ void block_sums(const T (&q)[4][Lay<KIND>::GQ], const T (&g)[4][3], T w, T fact1,
+                                           T fact2, T rho_ns, T* o) {
+  using L = Lay<KIND>;
+  constexpr bool vof = KIND == OVS_ASM_NSVOF;
+  T c[4][4];
+#pragma unroll
+  for (int gp = 0; gp < 4; ++gp)
+#pragma unroll
+    for (int n = 0; n < 4; ++n) c[gp][n] = q[gp][0] * g[n][0] + q[gp][1] * g[n][1] + q[gp][2] * g[n][2];
+#pragma unroll
+  for (int a = 0; a < 4; ++a) {
+    T S[4], L1[4], PL[4], V[4];
+#pragma unroll
+    for (int b = 0; b < 4; ++b) S[b] = L1[b] = PL[b] = V[b] = 0;
+#pragma unroll
+    for (int gp = 0; gp < 4; ++gp) {
+      T N[4];
+      tet_shape<T>(gp, N);
+      const T rho = vof ? q[gp][3] : rho_ns;
+      const T rt = vof ? q[gp][4] : q[gp][3];
+      const T alpha = w * rho * (N[a] + rt * c[gp][a]);
+#pragma unroll
+      for (int b = 0; b < 4; ++b) {
+        const T beta = fact1 * N[b] + fact2 * c[gp][b];
+        S[b] += alpha * beta;
+        if constexpr (vof) {
+          const T gam = w * (N[a] + q[gp][5] * c[gp][a]);
+          L1[b] += gam * (beta + fact2 * N[b] * q[gp][6]) + q[gp][7] * N[a] * N[b];
+          PL[b] -= q[gp][9] * N[a] * N[b];
+          V[b] += fact2 * gam * N[b];
+        }
+      }
+    }
+    if constexpr (vof) {
+#pragma unroll
+      for (int b = 0; b < 4; ++b) put4(o + L::PW * (4 * a + b), S[b], L1[b], PL[b], V[b]);
+    } else {
+      put4(o + L::PW * 4 * a, S[0], S[1], S[2], S[3]);
+    }
+  }
+#pragma unroll
+  for (int n = 0; n < 4; ++n) {
+    T PR = 0, Tn = 0, U = 0, Q = 0;
+#pragma unroll
+    for (int gp = 0; gp < 4; ++gp) {
+      T N[4];
+      tet_shape<T>(gp, N);
+      const T rt = vof ? q[gp][4] : q[gp][3];
+      PR += fact2 * w * N[n];
+      Tn += w * rt * (fact1 * N[n] + fact2 * c[gp][n]);
+      Q += fact2 * w * rt * c[gp][n];
+      if constexpr (vof) U += q[gp][8] * N[n];
+    }
+    put4(o + L::ND0 + 8 * n, g[n][0], g[n][1], g[n][2], PR);
+    put4(o + L::ND0 + 8 * n + 4, Tn, U, Q, (T)0);
+  }
+}
 
 struct SumArgs {
   const void* rec;
@@ -327,7 +417,7 @@ __device__ void summarize_ns(const SumArgs& a, const RA& r, const LA& lo, bool t
   const T fact2 = (T)(p.alfi * p.gami * p.delt);
   const T taut = (T)(4.0 / (p.delt * p.delt));
   T KA = 0, KB = 0, MM = 0;
-  T ru[4][3], rp[4];
+  T ru[4][3], rp[4], q[4][Lay<OVS_ASM_NS>::GQ];
 #pragma unroll
   for (int n = 0; n < 4; ++n) { ru[n][0] = ru[n][1] = ru[n][2] = 0; rp[n] = 0; }
 #pragma unroll
@@ -352,8 +442,7 @@ __device__ void summarize_ns(const SumArgs& a, const RA& r, const LA& lo, bool t
       const double c = (double)p.delt * sqrt((double)taua);
       if (c > cfl) cfl = c;
     }
-    T* og = o + Lay<OVS_ASM_NS>::GP0 + gp * Lay<OVS_ASM_NS>::GPW;
-    og[0] = uadv[0]; og[1] = uadv[1]; og[2] = uadv[2]; og[3] = rho * tauM;
+    q[gp][0] = uadv[0]; q[gp][1] = uadv[1]; q[gp][2] = uadv[2]; q[gp][3] = rho * tauM;
     if (target) {
       KA += fact2 * mupkdc * w;
       KB += fact2 * tauC * w;
@@ -373,16 +462,12 @@ __device__ void summarize_ns(const SumArgs& a, const RA& r, const LA& lo, bool t
       for (int n = 0; n < 4; ++n) rp[n] -= (N[n] * divu) * w;
     }
   }
+  using L = Lay<OVS_ASM_NS>;
 #pragma unroll
-  for (int n = 0; n < 4; ++n)
-#pragma unroll
-    for (int d = 0; d < 3; ++d) o[3 * n + d] = g[n][d];
-  o[12] = target ? w : (T)0; o[13] = KA; o[14] = KB; o[15] = MM;
-#pragma unroll
-  for (int n = 0; n < 4; ++n) {
-    T* orh = o + Lay<OVS_ASM_NS>::RHS0 + 4 * n;
-    orh[0] = ru[n][0]; orh[1] = ru[n][1]; orh[2] = ru[n][2]; orh[3] = rp[n];
-  }
+  for (int n = 0; n < 4; ++n) put4(o + L::RHS0 + 4 * n, ru[n][0], ru[n][1], ru[n][2], rp[n]);
+  put4(o + L::C0, KA, KB, MM, (T)0);
+  if constexpr (!std::is_same<T, Dual>::value)
+    block_sums<T, OVS_ASM_NS>(q, g, target ? w : (T)0, (T)p.almi, fact2, rho, o);
 }
 
 // pass 1, NS+VOF quench (src/solveQuenching.f90:295-523); the viscous RHS
@@ -426,7 +511,7 @@ __device__ void summarize_nsvof(const SumArgs& a, const RA& r, const LA& lo, boo
     gdphi[n] = g[n][0] * dphi[0] + g[n][1] * dphi[1] + g[n][2] * dphi[2];
   }
   T KA = 0, KB = 0, MM = 0, KDP = 0;
-  T ru[4][3], rp[4], rf[4];
+  T ru[4][3], rp[4], rf[4], q[4][Lay<OVS_ASM_NSVOF>::GQ];
 #pragma unroll
   for (int n = 0; n < 4; ++n) { ru[n][0] = ru[n][1] = ru[n][2] = 0; rp[n] = 0; rf[n] = 0; }
 #pragma unroll (std::is_same<RA, SmemRecs<T>>::value ? 1 : 4)
@@ -494,15 +579,13 @@ __device__ void summarize_nsvof(const SumArgs& a, const RA& r, const LA& lo, boo
     if (kdcphi_on) kdphi = (T)p.lsc_kdc * fabs(res_phi) / sqrt(GG);
     const T mupk = mu + kdc;
     const T dmdi = dmd * ira;
-    T* og = o + Lay<OVS_ASM_NSVOF>::GP0 + gp * Lay<OVS_ASM_NSVOF>::GPW;
-    og[0] = uadv[0]; og[1] = uadv[1]; og[2] = uadv[2];
-    og[3] = rho; og[4] = rho * tauM; og[5] = tauLS;
-    og[6] = vdot + phii * ira * dmd - dmd / rhoa;
+    q[gp][0] = uadv[0]; q[gp][1] = uadv[1]; q[gp][2] = uadv[2];
+    q[gp][3] = rho; q[gp][4] = rho * tauM; q[gp][5] = tauLS;
+    q[gp][6] = vdot + phii * ira * dmd - dmd / rhoa;
     const T wf = fluid ? w : (T)0;   // solid elements contribute nothing
-    og[7] = fact2 * wf * tauC * dmdi * dmdi;
-    og[8] = fact2 * tauC * dmdi * wf;
-    og[9] = fact2 * dmdi * wf;
-    og[10] = 0; og[11] = 0;
+    q[gp][7] = fact2 * wf * tauC * dmdi * dmdi;
+    q[gp][8] = fact2 * tauC * dmdi * wf;
+    q[gp][9] = fact2 * dmdi * wf;
     if (!fluid) continue;
     KA += fact2 * mupk * w;
     KB += fact2 * (tauC + lambda) * w;
@@ -522,17 +605,21 @@ __device__ void summarize_nsvof(const SumArgs& a, const RA& r, const LA& lo, boo
       rf[n] += w * (-(N[n] + tauLS * c[n]) * res_phi - kdphi * gdphi[n] + N[n] * dmdi * tauC * (divu - vdot));
     }
   }
+  using L = Lay<OVS_ASM_NSVOF>;
+  {
+    T rh[20];
 #pragma unroll
-  for (int n = 0; n < 4; ++n)
+    for (int n = 0; n < 4; ++n) {
+      rh[5 * n] = ru[n][0]; rh[5 * n + 1] = ru[n][1]; rh[5 * n + 2] = ru[n][2];
+      rh[5 * n + 3] = rp[n]; rh[5 * n + 4] = rf[n];
+    }
 #pragma unroll
-    for (int d = 0; d < 3; ++d) o[3 * n + d] = g[n][d];
-  o[12] = fluid ? w : (T)0; o[13] = KA; o[14] = KB; o[15] = MM; o[16] = KDP;
-  o[17] = dphi[0]; o[18] = dphi[1]; o[19] = dphi[2];
-#pragma unroll
-  for (int n = 0; n < 4; ++n) {
-    T* orh = o + Lay<OVS_ASM_NSVOF>::RHS0 + 5 * n;
-    orh[0] = ru[n][0]; orh[1] = ru[n][1]; orh[2] = ru[n][2]; orh[3] = rp[n]; orh[4] = rf[n];
+    for (int k = 0; k < 20; k += 4) put4(o + L::RHS0 + k, rh[k], rh[k + 1], rh[k + 2], rh[k + 3]);
   }
+  put4(o + L::C0, KA, KB, MM, KDP);
+  put4(o + L::C0 + 4, dphi[0], dphi[1], dphi[2], (T)0);
+  if constexpr (!std::is_same<T, Dual>::value)
+    block_sums<T, OVS_ASM_NSVOF>(q, g, fluid ? w : (T)0, (T)p.almi, fact2, (T)0, o);
 }
 
 // pass 1, temperature (src/solveQuenching.f90:712-856).  Record layout of
@@ -655,18 +742,12 @@ __device__ void summarize_tem(const SumArgs& a, const RA& r, const LA& lo, bool 
 
 // -------------------------------------------------- pass 2: block expansion
 // Blocks of row A (local node la) of one element from its summary, for a
-// column node b (formulas factored from the reference's per Gauss
-// point sums; see the notes at each kind):
-//   K(i,j) = KA ga_j gb_i + KB ga_i gb_j + delta_ij (KA gab + S_b)
-//   G(i) = -ga_i P_b + gb_i Q        D(i) = gb_i R + ga_i T_b     M = MM gab
-//   LS = L1_b + KDP gab + E_b   ULS(i) = ga_i U_b   PLS = PL_b
-//   LSU(i) = dphi_i V_b - gb_i W
-// with the Gauss-point sums S_b = sum w rho (Na + rt ca)(fact1 Nb + fact2 cb),
-// P_b = sum fact2 w Nb, Q = sum fact2 w rt ca, R = sum fact2 w Na,
-// T_b = sum w rt (fact1 Nb + fact2 cb), L1_b = sum w (Na + tauLS ca)
-// (fact1 Nb + fact2 cb + fact2 Nb src), E_b = sum eps Na Nb,
-// U_b = sum ufac Nb, PL_b = -sum plfac Na Nb, V_b = sum fact2 w (Na +
-// tauLS ca) Nb, W = sum ufac Na, where c_n = uadv . grad N_n.
+// column node b (formulas factored from the reference's per Gauss point
+// sums, with the sums of block_sums):
+//   K(i,j) = KA ga_j gb_i + KB ga_i gb_j + delta_ij (KA gab + S_ab)
+//   G(i) = -ga_i PR_b + gb_i Q_a      D(i) = gb_i PR_a + ga_i T_b
+//   M = MM gab    LS = L1_ab + E_ab + KDP gab    ULS(i) = ga_i U_b
+//   PLS = PL_ab   LSU(i) = dphi_i V_ab - gb_i U_a
 // 4 consecutive values: read-only global loads (SMEM = false) or loads from
 // the warp's shared-memory stage (SMEM = true)
 template <typename T, bool SMEM = false>
@@ -680,121 +761,66 @@ __device__ __forceinline__ void ldv4(const T* p, T* d) {
     d[0] = a.x; d[1] = a.y; d[2] = b.x; d[3] = b.y;
   }
 }
+template <typename T, bool SMEM = false>
+__device__ __forceinline__ T ld1(const T* p) {
+  if constexpr (SMEM) return *p;
+  else return __ldg(p);
+}
 
 // Blocks (row node la, column nodes b0 + k*BS, k < NC) of an element from
-// its summary, by the sums above, in one Gauss-point loop.  The 4 lanes of an
-// NS/NS+VOF element take one column each (NC = 1); a T lane takes all four.
+// its summary.  The 4 lanes of an NS/NS+VOF element take one column each
+// (NC = 1); a T lane takes all four.  sm: the element's summary (global
+// memory, or its matrix part staged in shared memory with SMEM); the
+// residual rows behind it are read by the caller from global memory
 template <typename T, int KIND, int NC, bool SMEM = false>
-__device__ __forceinline__ void expand_block(const ovs_params& p, const T* sm, int la, int b0, int BS,
-                                             T (&o)[NC][Lay<KIND>::NV < 4 ? 1 : Lay<KIND>::NV], T* rv) {
+__device__ __forceinline__ void expand_block(const T* sm, int la, int b0, int BS,
+                                             T (&o)[NC][Lay<KIND>::NV < 4 ? 1 : Lay<KIND>::NV]) {
   using L = Lay<KIND>;
   if constexpr (KIND == OVS_ASM_TEM) {
     // the element pass stored the element matrix: row la, columns b
 #pragma unroll
     for (int k = 0; k < NC; ++k) o[k][0] = sm[4 * la + b0 + k * BS];
-    rv[0] = sm[L::RHS0 + la];
   } else {
-  T hd[16];
-#pragma unroll
-  for (int k = 0; k < 16; k += 4) ldv4<T, SMEM>(sm + k, hd + k);
-  T g[4][3];
-#pragma unroll
-  for (int n = 0; n < 4; ++n)
-#pragma unroll
-    for (int d = 0; d < 3; ++d) g[n][d] = hd[3 * n + d];
-  const T w = hd[12];
-  T ga[3], gb[NC][3];
-#pragma unroll
-  for (int d = 0; d < 3; ++d) {
-    const T col[4] = {g[0][d], g[1][d], g[2][d], g[3][d]};
-    ga[d] = pick4<T>(col, la);
-#pragma unroll
-    for (int k = 0; k < NC; ++k) gb[k][d] = pick4<T>(col, b0 + k * BS);
-  }
-  T gab[NC];
-#pragma unroll
-  for (int k = 0; k < NC; ++k) gab[k] = ga[0] * gb[k][0] + ga[1] * gb[k][1] + ga[2] * gb[k][2];
-  {
     constexpr bool vof = KIND == OVS_ASM_NSVOF;
-    const T fact1 = (T)p.almi;
-    const T fact2 = vof ? (T)(p.alfi * p.delt * p.gami) : (T)(p.alfi * p.gami * p.delt);
-    const T KA = hd[13], KB = hd[14], MM = hd[15];
-    T KDP = 0, dphi[3] = {0, 0, 0};
-    if constexpr (vof) {
-      T t4[4];
-      ldv4<T, SMEM>(sm + 16, t4);
-      KDP = t4[0]; dphi[0] = t4[1]; dphi[1] = t4[2]; dphi[2] = t4[3];
-    }
-    T Q = 0, R = 0, W = 0;
-    T S[NC], P[NC], Tt[NC], L1[NC], E[NC], U[NC], PL[NC], Vv[NC];
-#pragma unroll
-    for (int k = 0; k < NC; ++k) S[k] = P[k] = Tt[k] = L1[k] = E[k] = U[k] = PL[k] = Vv[k] = 0;
-#pragma unroll
-    for (int gp = 0; gp < 4; ++gp) {
-      T N[4];
-      tet_shape<T>(gp, N);
-      T q[L::GPW];
-#pragma unroll
-      for (int k = 0; k < L::GPW; k += 4) ldv4<T, SMEM>(sm + L::GP0 + gp * L::GPW + k, q + k);
-      T uadv[3], rho, rt;
-      if constexpr (vof) {
-        uadv[0] = q[0]; uadv[1] = q[1]; uadv[2] = q[2]; rho = q[3]; rt = q[4];
-      } else {
-        uadv[0] = q[0]; uadv[1] = q[1]; uadv[2] = q[2]; rho = (T)p.rhoa; rt = q[3];
-      }
-      const T ca = uadv[0] * ga[0] + uadv[1] * ga[1] + uadv[2] * ga[2];
-      const T Na = pick4<T>(N, la);
-      const T alpha = w * rho * (Na + rt * ca);
-      Q += fact2 * w * rt * ca;
-      R += fact2 * w * Na;
-      T gam = 0, tls = 0, src = 0, eps = 0, ufac = 0, plfac = 0;
-      if constexpr (vof) {
-        tls = q[5]; src = q[6]; eps = q[7]; ufac = q[8]; plfac = q[9];
-        gam = w * (Na + tls * ca);
-        W += ufac * Na;
-      }
-#pragma unroll
-      for (int k = 0; k < NC; ++k) {
-        const T cb = uadv[0] * gb[k][0] + uadv[1] * gb[k][1] + uadv[2] * gb[k][2];
-        const T Nb = pick4<T>(N, b0 + k * BS);
-        const T beta = fact1 * Nb + fact2 * cb;
-        S[k] += alpha * beta;
-        P[k] += fact2 * w * Nb;
-        Tt[k] += w * rt * beta;
-        if constexpr (vof) {
-          L1[k] += gam * (beta + fact2 * Nb * src);
-          E[k] += eps * Na * Nb;
-          U[k] += ufac * Nb;
-          PL[k] -= plfac * Na * Nb;
-          Vv[k] += fact2 * gam * Nb;
-        }
-      }
-    }
+    T na[8], cs[8];
+    ldv4<T, SMEM>(sm + L::ND0 + 8 * la, na);
+    ldv4<T, SMEM>(sm + L::ND0 + 8 * la + 4, na + 4);
+    ldv4<T, SMEM>(sm + L::C0, cs);
+    if constexpr (vof) ldv4<T, SMEM>(sm + L::C0 + 4, cs + 4);
+    const T ga[3] = {na[0], na[1], na[2]};
+    const T Ra = na[3], Wa = na[5], Qa = na[6];
+    const T KA = cs[0], KB = cs[1], MM = cs[2];
 #pragma unroll
     for (int k = 0; k < NC; ++k) {
-      const T* gk = gb[k];
-      const T dg = KA * gab[k] + S[k];
+      const int b = b0 + k * BS;
+      T nb[8], pr[4];
+      ldv4<T, SMEM>(sm + L::ND0 + 8 * b, nb);
+      ldv4<T, SMEM>(sm + L::ND0 + 8 * b + 4, nb + 4);
+      if constexpr (vof) ldv4<T, SMEM>(sm + L::PW * (4 * la + b), pr);
+      else pr[0] = ld1<T, SMEM>(sm + L::PW * (4 * la + b));
+      const T gk[3] = {nb[0], nb[1], nb[2]};
+      const T Pb = nb[3], Tb = nb[4], Ub = nb[5];
+      const T gab = ga[0] * gk[0] + ga[1] * gk[1] + ga[2] * gk[2];
+      const T dg = KA * gab + pr[0];
 #pragma unroll
       for (int i = 0; i < 3; ++i) {
 #pragma unroll
         for (int j = 0; j < 3; ++j) o[k][4 * i + j] = KA * ga[j] * gk[i] + KB * ga[i] * gk[j] + (i == j ? dg : (T)0);
-        o[k][4 * i + 3] = -ga[i] * P[k] + gk[i] * Q;
+        o[k][4 * i + 3] = -ga[i] * Pb + gk[i] * Qa;
       }
 #pragma unroll
-      for (int d = 0; d < 3; ++d) o[k][12 + d] = gk[d] * R + ga[d] * Tt[k];
-      o[k][15] = MM * gab[k];
+      for (int d = 0; d < 3; ++d) o[k][12 + d] = gk[d] * Ra + ga[d] * Tb;
+      o[k][15] = MM * gab;
       if constexpr (vof) {
+        const T KDP = cs[3];
 #pragma unroll
-        for (int d = 0; d < 3; ++d) o[k][16 + d] = dphi[d] * Vv[k] - gk[d] * W;
-        o[k][19] = L1[k] + KDP * gab[k] + E[k];
+        for (int d = 0; d < 3; ++d) o[k][16 + d] = cs[4 + d] * pr[3] - gk[d] * Wa;
+        o[k][19] = pr[1] + KDP * gab;
 #pragma unroll
-        for (int d = 0; d < 3; ++d) o[k][20 + d] = ga[d] * U[k];
-        o[k][23] = PL[k];
+        for (int d = 0; d < 3; ++d) o[k][20 + d] = ga[d] * Ub;
+        o[k][23] = pr[2];
       }
     }
-#pragma unroll
-    for (int f = 0; f < L::NF; ++f) rv[f] = sm[L::RHS0 + L::NF * la + f];
-  }
   }
 }
 
@@ -819,8 +845,9 @@ template <> struct Vec4<double> {
 
 // shared-memory layout per warp: the blocks of the chunk's elements
 // [CH elements][4 columns][BSTR] (stride padded so the 16-byte stores of a
-// quarter warp hit distinct banks), their RHS rows [8][RSTR], the row
-// accumulator [max_deg][NVP], then the slots [8][4] and the columns
+// quarter warp hit distinct banks), their RHS rows [CH][RSTR], the row
+// accumulator [max_deg][NVP], then the slot words of the chunk's elements
+// [CH], the columns [max_deg] and their Dirichlet masks [max_deg]
 template <typename T, int KIND> struct Smem {
   static constexpr int NV = Lay<KIND>::NV, NF = Lay<KIND>::NF;
   static constexpr int LPE = (NV < 4) ? 1 : 4;       // lanes per element
@@ -831,12 +858,17 @@ template <typename T, int KIND> struct Smem {
   // the stage buffer of the staged row pass: the chunk's CH element
   // summaries, copied in with one round of asynchronous 16-byte copies
   static constexpr int SW = Lay<KIND>::SW;
+  // values staged per element: the matrix part of the summary (the residual
+  // rows behind it are read from global memory by the lanes that need them)
+  static constexpr int SWS = (KIND == OVS_ASM_TEM) ? SW : Lay<KIND>::RHS0;
+  __host__ __device__ static size_t ints_offset(int max_deg) {
+    const size_t b = sizeof(T) * ((size_t)4 * CH * BSTR + (size_t)CH * RSTR + (size_t)max_deg * NVP);
+    return (b + 15) & ~(size_t)15;
+  }
   __host__ __device__ static size_t bytes(int max_deg, bool staged = false) {
-    size_t b = sizeof(T) * ((size_t)4 * CH * BSTR + (size_t)CH * RSTR + (size_t)max_deg * NVP);
+    size_t b = ints_offset(max_deg) + sizeof(int) * ((size_t)CH + 2 * (size_t)max_deg);
     b = (b + 15) & ~(size_t)15;
-    b += sizeof(int) * ((size_t)4 * CH + max_deg);
-    b = (b + 15) & ~(size_t)15;
-    if (staged) b += sizeof(T) * (size_t)CH * SW;
+    if (staged) b += sizeof(T) * (size_t)CH * SWS;
     return b;
   }
   __host__ __device__ static size_t stage_offset(int max_deg) { return bytes(max_deg, false); }
@@ -910,9 +942,15 @@ element_summary_kernel(const SumArgs a) {
       T r[4][16], lo[4][4];
 #pragma unroll
       for (int n = 0; n < 4; ++n) load_rec(rec, nodes[n], r[n], lo[n]);
-      T o[L::SW];
-      run(r, lo, o);
-      store_row<L::SW>(reinterpret_cast<T*>(a.sum) + (size_t)e * L::SW, o);
+      if constexpr (KIND == OVS_ASM_TEM) {
+        T o[L::SW];
+        run(r, lo, o);
+        store_row<L::SW>(reinterpret_cast<T*>(a.sum) + (size_t)e * L::SW, o);
+      } else {
+        // NS / NS+VOF write their summary with vector stores as its parts
+        // are formed
+        run(r, lo, reinterpret_cast<T*>(a.sum) + (size_t)e * L::SW);
+      }
     }
     if (!(detj > (T)0)) nbad = 1;
   }
@@ -935,74 +973,83 @@ __device__ __forceinline__ unsigned mask_of(int v) {
   return (unsigned)c_rowbits[v] | ((unsigned)c_colbits[v] << 8) | ((unsigned)c_diagbit[v] << 16);
 }
 
+// One warp per CSR row, the rows in the order of the row records (Morton
+// order of the nodes, so that the rows sharing an element run close
+// together in time and its summary comes from L2).  Per chunk of CH of the
+// row's elements: phase 1 expands block (A's row, column b) of each element
+// into shared memory (lane = element, column), phase 2 adds them into the
+// row accumulator, each lane owning value groups of whole slots and adding
+// the chunk's blocks that fall in its slot in ascending element order (so
+// every entry is summed in the same order on every run).  The next row's
+// record and its first element ids are loaded while the current row runs,
+// and the Dirichlet masks of the row's columns while its first chunk runs.
 // STAGED: the warp first copies the chunk's element summaries into its
 // shared-memory stage with one round of asynchronous 16-byte copies (all in
-// flight together, no registers held), with the element ids of the next
-// chunk already loaded; the block expansion then reads shared memory.
-// Otherwise every lane reads its element's summary from global memory.
+// flight together, no registers held); the block expansion then reads
+// shared memory.  Otherwise every lane reads its element's summary from
+// global memory.
 template <typename T, int KIND, int WARPS, bool STAGED>
 __global__ void __launch_bounds__(WARPS * 32)
 assemble_rows_kernel(const AsmArgs a) {
   using S = Smem<T, KIND>;
   using L = Lay<KIND>;
   constexpr int NV = S::NV, NF = S::NF, NVP = S::NVP, BSTR = S::BSTR, RSTR = S::RSTR, CH = S::CH;
+  constexpr int NG = (NV >= 4) ? NV / 4 : 1;   // value groups per slot: 4 values (T: the value)
   extern __shared__ __align__(16) unsigned char smem_raw[];
   __shared__ unsigned masks[24];
   if (threadIdx.x < 24) masks[threadIdx.x] = (KIND == OVS_ASM_TEM) ? (TB | (TB << 8) | (TB << 16)) : mask_of(threadIdx.x);
   __syncthreads();
   const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
   unsigned char* base = smem_raw + (size_t)wid * S::bytes(a.max_deg, STAGED);
-  T* stage = reinterpret_cast<T*>(base + S::stage_offset(a.max_deg));   // [CH][SW] (STAGED)
+  T* stage = reinterpret_cast<T*>(base + S::stage_offset(a.max_deg));   // [CH][SWS] (STAGED)
   T* blk = reinterpret_cast<T*>(base);                 // [CH][4][BSTR]
   T* rvs = blk + 4 * CH * BSTR;                        // [CH][RSTR]
   T* acc = rvs + CH * RSTR;                            // [max_deg][NVP]
-  size_t off = sizeof(T) * ((size_t)4 * CH * BSTR + (size_t)CH * RSTR + (size_t)a.max_deg * NVP);
-  off = (off + 15) & ~(size_t)15;
-  int* slot = reinterpret_cast<int*>(base + off);      // [CH][4]
-  int* cols = slot + 4 * CH;                           // [max_deg]
+  unsigned* sl4 = reinterpret_cast<unsigned*>(base + S::ints_offset(a.max_deg));   // [CH]
+  int* cols = reinterpret_cast<int*>(sl4 + CH);        // [max_deg]
+  unsigned* cib = reinterpret_cast<unsigned*>(cols + a.max_deg);                 // [max_deg]
 
   const T* sum = reinterpret_cast<const T*>(a.rec);
-  const int nwarps_total = gridDim.x * WARPS;
+  const int W = gridDim.x * WARPS;
   // lane = (element jl of the chunk, first column node bl0 of that element);
   // with one lane per element (T) a lane takes all 4 columns
   constexpr int LPE = S::LPE, CPL = 4 / LPE;
   const int jl = lane / LPE, bl0 = lane % LPE;
-  constexpr int U16 = L::SW * (int)sizeof(T) / 16;          // 16-byte units per summary
+  constexpr int SWS = S::SWS;
+  constexpr int U16 = SWS * (int)sizeof(T) / 16;            // 16-byte units staged per summary
+  static_assert(SWS * sizeof(T) % 16 == 0, "staged summaries must be whole 16-byte units");
   static_assert(L::SW * sizeof(T) % 16 == 0, "summaries must be whole 16-byte units");
-  for (int t = blockIdx.x * WARPS + wid; t < a.N; t += nwarps_total) {
-    // rows in the spatial order of the nodes (when given), so that the rows
-    // sharing an element are in flight together and its summary is read
-    // from L2 rather than DRAM
-    const int A = a.row_order ? __ldg(a.row_order + t) : t;
-    const int rp = a.rowptr[A], deg = a.rowptr[A + 1] - rp;
-    const int ep = a.n2e_ptr[A], ne = a.n2e_ptr[A + 1] - ep;
-    if constexpr (STAGED) {
-      for (int s = lane; s < deg; s += 32) cp_async4(cols + s, a.colidx + rp + s);
-    } else {
-      for (int s = lane; s < deg; s += 32) cols[s] = a.colidx[rp + s];
-    }
+  int t = blockIdx.x * WARPS + wid;
+  // row record {A, rowptr[A], n2e_ptr[A], deg | sd << 8 | ne << 16} and the element
+  // ids of the first chunk (lanes j < nc hold entry j)
+  int4 rr = make_int4(0, 0, 0, 0);
+  if (t < a.N) rr = __ldg(a.row_rec + t);
+  int pk_n = 0;
+  unsigned s4_n = 0;
+  if (t < a.N && lane < min(CH, rr.w >> 16)) {
+    pk_n = __ldg(a.n2e + rr.z + lane);
+    s4_n = __ldg(a.n2s + rr.z + lane);
+  }
+  for (; t < a.N; t += W) {
+    const int A = rr.x, rp = rr.y, ep = rr.z, deg = rr.w & 0xff, ne = rr.w >> 16;
+    int4 rn = make_int4(0, 0, 0, 0);
+    if (t + W < a.N) rn = __ldg(a.row_rec + t + W);
+    const unsigned ibA = __ldg(a.ibc + A);
+    for (int s = lane; s < deg; s += 32) cp_async4(cols + s, a.colidx + rp + s);
     for (int q = lane; q < deg * NVP; q += 32) acc[q] = (T)0;
     T racc = (T)0;
-    // element ids and slots of the row's first chunk (lanes j < nc hold entry j)
-    int pk_n = 0;
-    unsigned s4_n = 0;
-    if (STAGED && lane < min(CH, ne)) {
-      pk_n = __ldg(a.n2e + ep + lane);
-      s4_n = __ldg(a.n2s + ep + lane);
-    }
+    unsigned ib0 = 0, ib1 = 0;   // masks of columns lane and lane + 32
     __syncwarp();
     for (int c0 = 0; c0 < ne; c0 += CH) {
       const int nc = min(CH, ne - c0);
-      int pk_c = 0;
-      unsigned s4_c = 0;
+      const int pk_c = pk_n;
+      const unsigned s4_c = s4_n;
+      // the next chunk's ids travel while this one is expanded
+      if (c0 + CH < ne && lane < min(CH, ne - c0 - CH)) {
+        pk_n = __ldg(a.n2e + ep + c0 + CH + lane);
+        s4_n = __ldg(a.n2s + ep + c0 + CH + lane);
+      }
       if constexpr (STAGED) {
-        pk_c = pk_n;
-        s4_c = s4_n;
-        // the next chunk's ids travel while this one is copied and expanded
-        if (c0 + CH < ne && lane < min(CH, ne - c0 - CH)) {
-          pk_n = __ldg(a.n2e + ep + c0 + CH + lane);
-          s4_n = __ldg(a.n2s + ep + c0 + CH + lane);
-        }
         // every lane runs the same trip count: the shuffle needs the full warp
         for (int it = 0; it < (CH * U16 + 31) / 32; ++it) {
           const int u = lane + 32 * it;
@@ -1010,7 +1057,7 @@ assemble_rows_kernel(const AsmArgs a) {
           const int e = __shfl_sync(0xffffffffu, pk_c, j) >> 3;
           if (u < nc * U16) {
             const int k = u - j * U16;
-            cp_async16(reinterpret_cast<unsigned char*>(stage + (size_t)j * L::SW) + 16 * k,
+            cp_async16(reinterpret_cast<unsigned char*>(stage + (size_t)j * SWS) + 16 * k,
                        reinterpret_cast<const unsigned char*>(sum + (size_t)e * L::SW) + 16 * k);
           }
         }
@@ -1018,97 +1065,115 @@ assemble_rows_kernel(const AsmArgs a) {
         __syncwarp();
       }
       // ---------------- phase 1: block (A's row, column bl) of element jl
-      int packed;
-      unsigned slots4;
-      if constexpr (STAGED) {
-        packed = __shfl_sync(0xffffffffu, pk_c, min(jl, CH - 1));
-        slots4 = __shfl_sync(0xffffffffu, s4_c, min(jl, CH - 1));
-      }
+      const int packed = __shfl_sync(0xffffffffu, pk_c, min(jl, CH - 1));
+      const unsigned slots4 = __shfl_sync(0xffffffffu, s4_c, min(jl, CH - 1));
       if (jl < nc) {
-        if constexpr (!STAGED) {
-          packed = __ldg(a.n2e + ep + c0 + jl);
-          slots4 = __ldg(a.n2s + ep + c0 + jl);
-        }
         const int e = packed >> 3, la = packed & 7;
-        T o[CPL][NVP], rv[NF];
+        T o[CPL][NVP];
         if constexpr (STAGED)
-          expand_block<T, KIND, CPL, true>(a.p, stage + (size_t)jl * L::SW, la, bl0, LPE, o, rv);
+          expand_block<T, KIND, CPL, true>(stage + (size_t)jl * SWS, la, bl0, LPE, o);
         else
-          expand_block<T, KIND, CPL>(a.p, sum + (size_t)e * L::SW, la, bl0, LPE, o, rv);
+          expand_block<T, KIND, CPL>(sum + (size_t)e * L::SW, la, bl0, LPE, o);
 #pragma unroll
         for (int k = 0; k < CPL; ++k) {
-          const int bl = bl0 + k * LPE;
-          T* dst = blk + (jl * 4 + bl) * BSTR;
+          T* dst = blk + (jl * 4 + bl0 + k * LPE) * BSTR;
           if constexpr (NV >= 4) {
 #pragma unroll
             for (int v = 0; v < NV; v += 4) store_row<4>(dst + v, o[k] + v);
           } else {
             dst[0] = o[k][0];
           }
-          slot[jl * 4 + bl] = (int)((slots4 >> (8 * bl)) & 0xffu);
         }
-        if (bl0 == 0) {
+        if (bl0 == 0) {   // the element's slot word and residual rows of node la
+          sl4[jl] = slots4;
+          const T* r = sum + (size_t)e * L::SW + L::RHS0 + NF * la;
 #pragma unroll
-          for (int f = 0; f < NF; ++f) rvs[jl * RSTR + f] = rv[f];
+          for (int f = 0; f < NF; ++f) rvs[jl * RSTR + f] = r[f];
         }
       }
+      if (c0 == 0) {
+        // the columns have arrived (their copies were issued at the row's
+        // start); their masks travel while the row is assembled
+        if constexpr (!STAGED) cp_async_wait_all();
+        __syncwarp();
+        if (lane < deg) ib0 = __ldg(a.ibc + cols[lane]);
+        if (lane + 32 < deg) ib1 = __ldg(a.ibc + cols[lane + 32]);
+      }
       __syncwarp();
-      // ---------------- phase 2: ordered segmented reduction into acc
-      // elements are added one after another in ascending element id; the
-      // 4 blocks of one element go to distinct slots (elements with a
-      // repeated node are rejected at upload)
-      if constexpr (NV >= 4) {
-        constexpr int NG = NV / 4;
-        for (int j = 0; j < nc; ++j) {
-          if (lane < 4 * NG) {
-            const int b = lane / NG, gidx = lane - b * NG;
-            const int s = slot[j * 4 + b];
-            Vec4<T>::add(acc + s * NVP + gidx * 4, blk + (j * 4 + b) * BSTR + gidx * 4);
+      // ---------------- phase 2: ordered reduction into acc
+      // task q = (slot s, value group g); the 4 blocks of one element go to
+      // distinct slots (elements with a repeated node are rejected at upload)
+      for (int q = lane; q < deg * NG; q += 32) {
+        const int s = q / NG, g = q - s * NG;
+        const unsigned key = (unsigned)s * 0x01010101u;
+        if constexpr (NV >= 4) {
+          T v[4];
+          ldv4<T, true>(acc + s * NVP + 4 * g, v);
+          for (int j = 0; j < nc; ++j) {
+            const unsigned m = __vcmpeq4(sl4[j], key);
+            if (m) {
+              const int b = (__ffs(m) - 1) >> 3;
+              T x[4];
+              ldv4<T, true>(blk + (j * 4 + b) * BSTR + 4 * g, x);
+              v[0] += x[0]; v[1] += x[1]; v[2] += x[2]; v[3] += x[3];
+            }
           }
-          __syncwarp();
-        }
-      } else {
-        for (int j = 0; j < nc; ++j) {
-          if (lane < 4) acc[slot[j * 4 + lane]] += blk[j * 4 + lane];
-          __syncwarp();
+          store_row<4>(acc + s * NVP + 4 * g, v);
+        } else {
+          T v = acc[s];
+          for (int j = 0; j < nc; ++j) {
+            const unsigned m = __vcmpeq4(sl4[j], key);
+            if (m) v += blk[j * 4 + ((__ffs(m) - 1) >> 3)];
+          }
+          acc[s] = v;
         }
       }
       if (lane < NF)
         for (int j = 0; j < nc; ++j) racc += rvs[j * RSTR + lane];
       __syncwarp();
     }
-    if constexpr (STAGED) {   // the row's column copies (a node without elements skips the chunk loop)
+    if (ne == 0) {   // a node without elements: only the Dirichlet rows
       cp_async_wait_all();
       __syncwarp();
+      if (lane < deg) ib0 = __ldg(a.ibc + cols[lane]);
+      if (lane + 32 < deg) ib1 = __ldg(a.ibc + cols[lane + 32]);
+    }
+    // the next row's first element ids travel while this row is written
+    pk_n = 0;
+    s4_n = 0;
+    if (t + W < a.N && lane < min(CH, rn.w >> 16)) {
+      pk_n = __ldg(a.n2e + rn.z + lane);
+      s4_n = __ldg(a.n2s + rn.z + lane);
     }
     // ---------------- row write with the Dirichlet treatment
-    const unsigned ibA = a.ibc[A];
     if (a.mat) {
+      if (lane < deg) cib[lane] = ib0;
+      if (lane + 32 < deg) cib[lane + 32] = ib1;
+      for (int s = lane + 64; s < deg; s += 32) cib[s] = __ldg(a.ibc + cols[s]);
+      __syncwarp();
       T* out = reinterpret_cast<T*>(a.vals) + (size_t)rp * NV;
       const T cnt = (T)ne;
       if constexpr (NV >= 4) {
         // one 4-value group per lane and step, 16-byte aligned (NV % 4 == 0)
-        constexpr int NG = NV / 4;
         for (int q = lane; q < deg * NG; q += 32) {
           const int s = q / NG, gidx = q - s * NG;
-          const int B = cols[s];
-          const unsigned ibB = __ldg(a.ibc + B);
-          const bool dg = B == A;
+          const unsigned ibB = cib[s];
+          const bool dg = cols[s] == A;
           T v4[4];
 #pragma unroll
-          for (int t = 0; t < 4; ++t) {
-            const unsigned m = masks[4 * gidx + t];
-            T val = acc[s * NVP + 4 * gidx + t];
+          for (int u = 0; u < 4; ++u) {
+            const unsigned m = masks[4 * gidx + u];
+            T val = acc[s * NVP + 4 * gidx + u];
             if ((ibA & m & 0xffu) || ((ibB << 8) & m & 0xff00u)) val = (T)0;
             if (dg && ((ibA << 16) & m & 0xff0000u)) val = cnt;
-            v4[t] = val;
+            v4[u] = val;
           }
           store4_cs(out + (size_t)s * NV + 4 * gidx, v4);
         }
       } else {
         for (int q = lane; q < deg; q += 32) {
           const int B = cols[q];
-          const unsigned ibB = __ldg(a.ibc + B);
+          const unsigned ibB = cib[q];
           T val = acc[q];
           if ((ibA & TB) || (ibB & TB)) val = (T)0;
           if (B == A && (ibA & TB)) val = cnt;
@@ -1124,7 +1189,167 @@ assemble_rows_kernel(const AsmArgs a) {
       if (!isfinite((double)v)) atomicOr(a.flags + 1, 1);
       __stcs(reinterpret_cast<T*>(a.rhs) + (size_t)lane * a.N + A, v);
     }
+    rr = rn;
     __syncwarp();
+  }
+}
+
+// A block of NV values to its CSR slot with the Dirichlet treatment of the
+// row (ibA) and column (ibB) masks; dg: the diagonal entry (cnt, the row's
+// element count, on constrained diagonal positions)
+template <typename T, int NV>
+__device__ __forceinline__ void write_block(T* dst, const T* v, const unsigned* masks, unsigned ibA, unsigned ibB,
+                                            bool dg, T cnt) {
+  const bool plain = (ibA | ibB) == 0u;
+  if constexpr (NV >= 4) {
+#pragma unroll
+    for (int g = 0; g < NV; g += 4) {
+      T v4[4];
+#pragma unroll
+      for (int u = 0; u < 4; ++u) {
+        T val = v[g + u];
+        if (!plain) {
+          const unsigned m = masks[g + u];
+          if ((ibA & m & 0xffu) || ((ibB << 8) & m & 0xff00u)) val = (T)0;
+          if (dg && ((ibA << 16) & m & 0xff0000u)) val = cnt;
+        }
+        v4[u] = val;
+      }
+      store4_cs(dst + g, v4);
+    }
+  } else {
+    T val = v[0];
+    if ((ibA & TB) || (ibB & TB)) val = (T)0;
+    if (dg && (ibA & TB)) val = cnt;
+    __stcs(dst, val);
+  }
+}
+
+// Gather row pass (tets, the default): one warp per CSR row, every lane
+// owning whole blocks of the row, so that no block passes through shared
+// memory and only the diagonal is summed across lanes.  Lanes 0..GD-1 take
+// the off-diagonal entries (lane l the l-th, counting past the diagonal
+// slot; a row with more than GD of them takes further passes) and add the
+// blocks of the entry's contribution list, one per round, in ascending
+// element order, in registers.  Lanes GD..31 share the diagonal block and
+// the residual rows: lane GD + i takes the row's elements i, i + ND, ...
+// in ascending order, and the ND partial sums are then added in lane
+// order.  Every entry is thus summed in an order fixed by the mesh, the
+// same on every run.  Each round loads the next entry of the lane's list
+// while the current block is expanded.
+template <typename T, int KIND>
+__global__ void __launch_bounds__(128) gather_rows_kernel(const AsmArgs a) {
+  using L = Lay<KIND>;
+  constexpr int NV = L::NV, NF = L::NF;
+  constexpr int NVP = NV < 4 ? 1 : NV;
+  constexpr int ND = 8, GD = 32 - ND;
+  constexpr int PSTR = ((NVP + NF) * (int)sizeof(T) + 15) / 16 * 16 / (int)sizeof(T);
+  __shared__ unsigned masks[24];
+  __shared__ __align__(16) T part[4][ND][PSTR];   // the diagonal lanes' partial sums, per warp
+  if (threadIdx.x < 24) masks[threadIdx.x] = (KIND == OVS_ASM_TEM) ? (TB | (TB << 8) | (TB << 16)) : mask_of(threadIdx.x);
+  __syncthreads();
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+  const T* sum = reinterpret_cast<const T*>(a.rec);
+  const int W = gridDim.x * 4;
+  T(*pw)[PSTR] = part[wid];
+  const bool diagl = lane >= GD;
+  const int di = lane - GD;   // the diagonal lane's index
+  for (int t = blockIdx.x * 4 + wid; t < a.N; t += W) {
+    const int4 rr = __ldg(a.row_rec + t);
+    const int A = rr.x, rp = rr.y, ep = rr.z, deg = rr.w & 0xff, sd = (rr.w >> 8) & 0xff, ne = rr.w >> 16;
+    const unsigned ibA = __ldg(a.ibc + A);
+    const int nod = deg > 0 ? deg - 1 : 0;
+    T* out = reinterpret_cast<T*>(a.vals) + (size_t)rp * NV;
+    const T cnt = (T)ne;
+    for (int o0 = 0; o0 == 0 || o0 < nod; o0 += GD) {
+      const int o = o0 + lane;   // off-diagonal ordinal of the lane
+      const bool offl = !diagl && o < nod;
+      const int s = o < sd ? o : o + 1;
+      int c0 = 0, len = 0;
+      unsigned ibB = 0;
+      if (offl) {
+        c0 = __ldg(a.cptr + rp + s);
+        len = __ldg(a.cptr + rp + s + 1) - c0;
+        ibB = __ldg(a.ibc + __ldg(a.colidx + rp + s));
+      } else if (diagl && o0 == 0) {
+        len = ne > di ? (ne - di + ND - 1) / ND : 0;
+      }
+      const int rounds = __reduce_max_sync(0xffffffffu, (unsigned)len);
+      T acc[NVP], racc[NF];
+#pragma unroll
+      for (int v = 0; v < NVP; ++v) acc[v] = (T)0;
+#pragma unroll
+      for (int f = 0; f < NF; ++f) racc[f] = (T)0;
+      int ent = 0;
+      if (len > 0) ent = offl ? __ldg(a.clist + c0) : __ldg(a.n2e + ep + di);
+      for (int k = 0; k < rounds; ++k) {
+        const int cur = ent;
+        if (k + 1 < len) ent = offl ? __ldg(a.clist + c0 + k + 1) : __ldg(a.n2e + ep + di + (k + 1) * ND);
+        if (k < len) {
+          int e, la, b;
+          if (offl) {
+            e = cur >> 4; la = (cur >> 2) & 3; b = cur & 3;
+          } else {
+            e = cur >> 3; la = cur & 7; b = la;
+          }
+          const T* se = sum + (size_t)e * L::SW;
+          T ob[1][NVP];
+          expand_block<T, KIND, 1>(se, la, b, 0, ob);
+#pragma unroll
+          for (int v = 0; v < NVP; ++v) acc[v] += ob[0][v];
+          if (diagl) {
+#pragma unroll
+            for (int f = 0; f < NF; ++f) racc[f] += __ldg(se + L::RHS0 + NF * la + f);
+          }
+        }
+      }
+      if (offl && a.mat) write_block<T, NV>(out + (size_t)s * NV, acc, masks, ibA, ibB, false, cnt);
+      if (o0 == 0) {
+        if (diagl) {
+#pragma unroll
+          for (int v = 0; v < NVP; ++v) pw[di][v] = acc[v];
+#pragma unroll
+          for (int f = 0; f < NF; ++f) pw[di][NVP + f] = racc[f];
+        }
+        __syncwarp();
+        constexpr int NG = NV >= 4 ? NV / 4 : 1;
+        if (a.mat && deg > 0 && lane < NG) {
+          constexpr int GW = NV >= 4 ? 4 : 1;
+          T v4[GW];
+#pragma unroll
+          for (int u = 0; u < GW; ++u) v4[u] = pw[0][GW * lane + u];
+          for (int i = 1; i < ND; ++i)
+#pragma unroll
+            for (int u = 0; u < GW; ++u) v4[u] += pw[i][GW * lane + u];
+          if constexpr (NV >= 4) {
+#pragma unroll
+            for (int u = 0; u < 4; ++u) {
+              const unsigned m = masks[4 * lane + u];
+              if (ibA & m & 0xffu) v4[u] = (T)0;
+              if ((ibA << 8) & m & 0xff00u) v4[u] = (T)0;
+              if ((ibA << 16) & m & 0xff0000u) v4[u] = cnt;
+            }
+            store4_cs(out + (size_t)sd * NV + 4 * lane, v4);
+          } else {
+            T val = v4[0];
+            if (ibA & TB) val = cnt;
+            __stcs(out + sd, val);
+          }
+        }
+        if (a.vec && lane >= 32 - NF) {
+          const int f = lane - (32 - NF);
+          T v = pw[0][NVP + f];
+          for (int i = 1; i < ND; ++i) v += pw[i][NVP + f];
+          unsigned bit;
+          if (KIND == OVS_ASM_TEM) bit = TB;
+          else bit = (f < 3) ? (1u << f) : (f == 3 ? PB : FB);
+          if (ibA & bit) v = (T)0;
+          if (!isfinite((double)v)) atomicOr(a.flags + 1, 1);
+          __stcs(reinterpret_cast<T*>(a.rhs) + (size_t)f * a.N + A, v);
+        }
+        __syncwarp();
+      }
+    }
   }
 }
 
@@ -1197,6 +1422,22 @@ int launch_rows(ovs_ctx* c, const AsmArgs& a) {
   return OVS_OK;
 }
 
+template <typename T, int KIND>
+int launch_gather(ovs_ctx* c, const AsmArgs& a) {
+  auto kern = gather_rows_kernel<T, KIND>;
+  int per_sm = 0;
+  OVS_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, 128, 0));
+  if (per_sm < 1) return OVS_ERR_ARG;
+  long need = ((long)c->N + 3) / 4;
+  long grid = (long)per_sm * c->num_sms * 4;
+  if (grid > need) grid = need;
+  if (grid < 1) grid = 1;
+  kern<<<(int)grid, 128, 0, c->stream>>>(a);
+  ++c->launches;
+  OVS_CUDA_TRY(cudaGetLastError());
+  return OVS_OK;
+}
+
 // parts: bit 0 the element pass, bit 1 the row pass
 template <typename T, int KIND>
 int launch_assemble(ovs_ctx* c, const AsmArgs& a, const SumArgs& sa, int parts = 3) {
@@ -1218,6 +1459,7 @@ int launch_assemble(ovs_ctx* c, const AsmArgs& a, const SumArgs& sa, int parts =
   // pass 2: rows
   // the temperature summaries (20 values, one lane per element) gain
   // nothing from staging: measured slower, so it reads them directly
+  if (c->rows_gather && c->cptr) return launch_gather<T, KIND>(c, a);
   if (c->rows_staged && KIND != OVS_ASM_TEM) return launch_rows<T, KIND, 4, true>(c, a);
   return launch_rows<T, KIND, 4, false>(c, a);
 }
@@ -1430,7 +1672,9 @@ static void fill_args(ovs_ctx* c, int prec, SysStore& S, int tensor_flag, AsmArg
   a.mat = (tensor_flag & OVS_TENSOR_MAT) != 0;
   a.vec = (tensor_flag & OVS_TENSOR_VEC) != 0;
   a.n2s = c->n2s;
-  a.row_order = c->row_order;
+  a.row_rec = c->row_rec;
+  a.cptr = c->cptr;
+  a.clist = c->clist;
   a.max_deg = c->max_deg;
   a.p = c->params;
   a.kbuf = nullptr;

@@ -200,6 +200,8 @@ int create_resources(ovs_ctx* c, const ovs_dims* dims) {
     if (rs) c->rows_staged = rs[0] != '0';
     const char* es = getenv("OVS_ELEM_SMEM");
     if (es) c->elem_smem = es[0] != '0';
+    const char* rg = getenv("OVS_ROWS_GATHER");
+    if (rg) c->rows_gather = rg[0] != '0';
   }
   c->N = dims->nnode;
   c->E = dims->nelem;
@@ -258,7 +260,7 @@ int ovs_destroy(ovs_ctx* c) {
   ovs_streaming_free(c);
   if (c->hex_kbuf) cudaFree(c->hex_kbuf);
   if (c->hex_w) cudaFree(c->hex_w);
-  void* ptrs[] = {c->ien, c->elm_id, c->ibc, c->rowptr, c->colidx, c->diag, c->n2e_ptr, c->n2e, c->n2s, c->row_order, c->tmap, c->vals_t, c->vjp_cot, c->vjp_ge, c->vjp_grad,
+  void* ptrs[] = {c->ien, c->elm_id, c->ibc, c->rowptr, c->colidx, c->diag, c->n2e_ptr, c->n2e, c->n2s, c->row_order, c->row_rec, c->cptr, c->clist, c->tmap, c->vals_t, c->vjp_cot, c->vjp_ge, c->vjp_grad,
                   c->rec[0], c->rec[1], c->esum[0], c->esum[1], c->gm, c->basis[0], c->basis[1], c->work64, c->work32, c->wvec, c->coop_part,
                   c->flags, c->cfl_bits};
   for (void* p : ptrs) if (p) cudaFree(p);
@@ -403,6 +405,7 @@ int ovs_set_option(ovs_ctx* c, int option, int value) {
     case OVS_OPT_HEX_TC: c->hex_tc = value != 0; return OVS_OK;
     case OVS_OPT_ROWS_STAGED: c->rows_staged = value != 0; return OVS_OK;
     case OVS_OPT_ELEM_SMEM: c->elem_smem = value != 0; return OVS_OK;
+    case OVS_OPT_ROWS_GATHER: c->rows_gather = value != 0; return OVS_OK;
     case OVS_OPT_ARNOLDI_FUSED: c->arnoldi_fused = value != 0; return OVS_OK;
     default: return OVS_ERR_ARG;
   }

@@ -95,6 +95,9 @@ struct ovs_ctx {
   double* vjp_ge = nullptr;
   double* vjp_grad = nullptr;
   int* row_order = nullptr;  // N: rows in Morton order of the node coordinates (the row pass's order)
+  int4* row_rec = nullptr;   // N: per row in that order {A, rowptr[A], n2e_ptr[A], deg | sd << 8 | ne << 16}
+  int* cptr = nullptr;       // nnz + 1: off-diagonal contribution lists (tets), offsets into clist
+  int* clist = nullptr;      // 12 E entries (e << 4) | (la << 2) | b, ascending element per entry
   unsigned* n2s = nullptr;   // nshl*E entries: slots of the element's nodes in the row, one byte each
                              // (one word per entry for tets, two for hexahedra)
   int nnz = 0;
@@ -122,6 +125,9 @@ struct ovs_ctx {
   int rows_staged = 1;
   // FP64 element pass: node records in registers (0, measured faster) or shared memory (1)
   int elem_smem = 0;
+  // tet row pass: lanes gather whole blocks by the contribution lists (1,
+  // default) or the chunked pass reduces element blocks in shared memory (0)
+  int rows_gather = 1;
   void* hex_kbuf = nullptr;              // E x 64 x 24 block values
   float* hex_w = nullptr;                // W hi + lo, canonical layout
   // boundary-condition producers (ovs_set_bc_spec)

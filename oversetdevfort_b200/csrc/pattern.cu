@@ -378,6 +378,95 @@ static int build_row_order(ovs_ctx* c) {
   return OVS_OK;
 }
 
+// the row pass's row records, in its processing order (row_order[t], or t):
+// {A, rowptr[A], n2e_ptr[A], deg | sd << 8 | ne << 16} with sd the slot of
+// the diagonal entry in the row, one 16-byte load per row
+__global__ void row_rec_kernel(const int* order, const int* rowptr, const int* n2e_ptr, const int* diag, int N,
+                               int4* rec) {
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= N) return;
+  const int A = order ? order[t] : t;
+  const int rp = rowptr[A], ep = n2e_ptr[A], deg = rowptr[A + 1] - rp;
+  const int sd = diag[A] >= rp ? diag[A] - rp : 0;
+  rec[t] = make_int4(A, rp, ep, deg | (sd << 8) | ((n2e_ptr[A + 1] - ep) << 16));
+}
+
+static int build_row_rec(ovs_ctx* c) {
+  const int N = c->N;
+  if (N < 1) return OVS_OK;
+  // the record packs the degree and the diagonal slot in 8 bits each
+  // (OVS_MAX_DEG <= 255) and the element count in 15
+  if (c->max_deg > 0xff || c->max_elem > 0x7fff) return OVS_ERR_PATTERN;
+  int st;
+  if ((st = ovs_ensure((void**)&c->row_rec, sizeof(int4) * (size_t)N))) return st;
+  row_rec_kernel<<<ovs_grid(N, 256, 1 << 30), 256, 0, c->stream>>>(c->row_order, c->rowptr, c->n2e_ptr, c->diag,
+                                                                   N, c->row_rec);
+  ++c->launches;
+  OVS_CUDA_TRY(cudaGetLastError());
+  return OVS_OK;
+}
+
+// Contribution lists of the off-diagonal entries (tets), the gather row
+// pass's input: for entry (A, B), B != A, the elements holding both nodes in
+// ascending element order, each as (e << 4) | (la << 2) | b with
+// A = ien[e][la], B = ien[e][b]; cptr[k]..cptr[k+1] delimits entry k's list
+// (diagonal entries have none: every element of the row adds to them).
+// One thread per row, the row's entries counted / filled in n2e order.
+__global__ void contrib_count_kernel(int N, const int* __restrict__ rowptr, const int* __restrict__ n2e_ptr,
+                                     const int* __restrict__ n2e, const unsigned* __restrict__ n2s,
+                                     int* __restrict__ cnt) {
+  const int A = blockIdx.x * blockDim.x + threadIdx.x;
+  if (A >= N) return;
+  const int rp = rowptr[A];
+  for (int k = n2e_ptr[A]; k < n2e_ptr[A + 1]; ++k) {
+    const int la = n2e[k] & 7;
+    const unsigned w = n2s[k];
+    for (int b = 0; b < 4; ++b)
+      if (b != la) ++cnt[rp + ((w >> (8 * b)) & 0xffu)];
+  }
+}
+
+__global__ void contrib_fill_kernel(int N, const int* __restrict__ rowptr, const int* __restrict__ n2e_ptr,
+                                    const int* __restrict__ n2e, const unsigned* __restrict__ n2s,
+                                    int* __restrict__ cursor, int* __restrict__ list) {
+  const int A = blockIdx.x * blockDim.x + threadIdx.x;
+  if (A >= N) return;
+  const int rp = rowptr[A];
+  for (int k = n2e_ptr[A]; k < n2e_ptr[A + 1]; ++k) {
+    const int e = n2e[k] >> 3, la = n2e[k] & 7;
+    const unsigned w = n2s[k];
+    for (int b = 0; b < 4; ++b)
+      if (b != la) list[cursor[rp + ((w >> (8 * b)) & 0xffu)]++] = (e << 4) | (la << 2) | b;
+  }
+}
+
+static int build_contrib(ovs_ctx* c) {
+  cudaStream_t s = c->stream;
+  const int N = c->N, nnz = c->nnz;
+  if (c->nshl != 4 || N < 1 || nnz < 1) return OVS_OK;
+  if (c->E >= (1 << 27)) return OVS_OK;   // (e << 4) must fit an int: the chunked row pass serves
+  const size_t ents = (size_t)12 * c->E;  // 3 off-diagonal blocks per element row
+  int st;
+  if ((st = ovs_ensure((void**)&c->cptr, sizeof(int) * ((size_t)nnz + 1)))) return st;
+  if ((st = ovs_ensure((void**)&c->clist, sizeof(int) * (ents > 0 ? ents : 1)))) return st;
+  int *cnt = nullptr, *tmp = nullptr;
+  const int nb = (nnz + 1 + SCAN_T - 1) / SCAN_T;
+  OVS_CUDA_TRY(cudaMallocAsync(&cnt, sizeof(int) * ((size_t)nnz + 1), s));
+  OVS_CUDA_TRY(cudaMallocAsync(&tmp, sizeof(int) * (4 * (size_t)nb + 64), s));
+  OVS_CUDA_TRY(cudaMemsetAsync(cnt, 0, sizeof(int) * ((size_t)nnz + 1), s));
+  contrib_count_kernel<<<ovs_grid(N, 128, 1 << 30), 128, 0, s>>>(N, c->rowptr, c->n2e_ptr, c->n2e, c->n2s, cnt);
+  ++c->launches;
+  if ((st = exclusive_scan(cnt, c->cptr, nnz + 1, tmp, s, &c->launches))) return st;
+  OVS_CUDA_TRY(cudaMemcpyAsync(cnt, c->cptr, sizeof(int) * (size_t)nnz, cudaMemcpyDeviceToDevice, s));
+  contrib_fill_kernel<<<ovs_grid(N, 128, 1 << 30), 128, 0, s>>>(N, c->rowptr, c->n2e_ptr, c->n2e, c->n2s, cnt,
+                                                                c->clist);
+  ++c->launches;
+  OVS_CUDA_TRY(cudaFreeAsync(cnt, s));
+  OVS_CUDA_TRY(cudaFreeAsync(tmp, s));
+  OVS_CUDA_TRY(cudaGetLastError());
+  return OVS_OK;
+}
+
 int ovs_pattern_build(ovs_ctx* c) {
   cudaStream_t s = c->stream;
   const int N = c->N, E = c->E, nshl = c->nshl;
@@ -438,6 +527,8 @@ int ovs_pattern_build(ovs_ctx* c) {
   OVS_CUDA_TRY(cudaFreeAsync(tmp, s));
   OVS_CUDA_TRY(cudaFreeAsync(stats, s));
   if ((st = build_row_order(c))) return st;
+  if ((st = build_row_rec(c))) return st;
+  if ((st = build_contrib(c))) return st;
   OVS_CUDA_TRY(cudaStreamSynchronize(s));
   OVS_CUDA_TRY(cudaGetLastError());
   c->have_pattern = true;

@@ -400,22 +400,90 @@ def test_kdc_integer_dummy_quirk(oracle):
 @pytest.mark.parametrize("kind", ["nsvof", "tem", "ns"])
 @pytest.mark.parametrize("prec", [F.OVS_FP64, F.OVS_FP32])
 def test_row_pass_variants_bit_identical(kind, prec):
-    """The row pass with the element summaries staged through shared memory
-    (OVS_OPT_ROWS_STAGED = 1) and read lane by lane from global memory (0)
-    runs the same arithmetic in the same order: the assembled systems are
-    bit-identical, matrix and right-hand side."""
+    """The chunked row pass (OVS_OPT_ROWS_GATHER = 0) with the element
+    summaries staged through shared memory (OVS_OPT_ROWS_STAGED = 1) and
+    read lane by lane from global memory (0) runs the same arithmetic in the
+    same order: the assembled systems are bit-identical, matrix and
+    right-hand side."""
     kernel = {"nsvof": F.OVS_ASM_NSVOF, "tem": F.OVS_ASM_TEM, "ns": F.OVS_ASM_NS}[kind]
     sysid = {"nsvof": F.OVS_SYS_NSVOF, "tem": F.OVS_SYS_TEM, "ns": F.OVS_SYS_NS}[kind]
     case = M.random_case(nx=6, ny=5, nz=4, seed=21, kernel=kernel)
     out = []
     for staged in (0, 1):
         ctx = _ctx(case)
+        ctx.set_option(F.OVS_OPT_ROWS_GATHER, 0)
         ctx.set_option(F.OVS_OPT_ROWS_STAGED, staged)
         ctx.assemble(kernel, 6, prec)
         out.append(ctx.get_system(sysid, prec))
         ctx.close()
     for k in out[0]:
         np.testing.assert_array_equal(out[0][k], out[1][k], err_msg=k)
+
+
+@pytest.mark.parametrize("kind", ["nsvof", "tem", "ns"])
+@pytest.mark.parametrize("prec,tol", [(F.OVS_FP64, 1e-14), (F.OVS_FP32, 1e-6)])
+def test_gather_and_chunked_row_passes_agree(kind, prec, tol):
+    """The gather row pass (default) adds the diagonal blocks and the
+    residual rows in eight interleaved partial sums, the chunked pass
+    (OVS_OPT_ROWS_GATHER = 0) in one ascending sweep; the off-diagonal
+    blocks are added in the same ascending element order by both.  The
+    systems agree to rounding, normwise per block, and the gather pass gives
+    the same bits on a second run."""
+    kernel = {"nsvof": F.OVS_ASM_NSVOF, "tem": F.OVS_ASM_TEM, "ns": F.OVS_ASM_NS}[kind]
+    sysid = {"nsvof": F.OVS_SYS_NSVOF, "tem": F.OVS_SYS_TEM, "ns": F.OVS_SYS_NS}[kind]
+    case = M.random_case(nx=6, ny=5, nz=4, seed=23, kernel=kernel)
+    out = []
+    for gather in (1, 0, 1):
+        ctx = _ctx(case)
+        ctx.set_option(F.OVS_OPT_ROWS_GATHER, gather)
+        ctx.assemble(kernel, 6, prec)
+        out.append(ctx.get_system(sysid, prec))
+        ctx.close()
+    for k in out[0]:
+        close(out[0][k], out[1][k], tol, k)
+        np.testing.assert_array_equal(out[0][k], out[2][k], err_msg=k)
+
+
+def _fan_case(kernel, m=40, seed=31):
+    """A fan of m tets around the axis from node 0 to node 1 (ring nodes 2..):
+    the two axis rows have degree m + 2 and m elements, more off-diagonal
+    entries than the gather row pass has lanes for in one pass, and the
+    entry (0, 1) lists all m elements."""
+    base = M.random_case(nx=3, ny=3, nz=3, seed=seed, kernel=kernel)
+    rng = np.random.default_rng(seed)
+    ang = np.linspace(0.0, 2 * np.pi, m, endpoint=False) + rng.uniform(0.0, 0.02, m)
+    ring = np.stack([np.cos(ang), np.sin(ang), 0.5 + 0.05 * rng.uniform(-1, 1, m)], axis=1)
+    xg = np.asfortranarray(np.vstack([[0.0, 0.0, 0.0], [0.0, 0.0, 1.0], ring]))
+    ien = np.array([[0, 2 + i, 2 + (i + 1) % m, 1] for i in range(m)], dtype=np.int64)
+    for t in ien:   # positive DetJ = det[x1 - x4, x2 - x4, x3 - x4]
+        x = xg[t]
+        if np.linalg.det(np.stack([x[0] - x[3], x[1] - x[3], x[2] - x[3]])) < 0:
+            t[0], t[1] = t[1], t[0]
+    N = xg.shape[0]
+    elm = np.where(rng.random(m) < 0.15, 101, 102).astype(np.int32)
+    mesh = M.Mesh(xg, np.asfortranarray(ien.astype(np.int32) + 1), elm, [np.zeros(0, np.int64)] * 6,
+                  (m, 1, 1), (1.0, 1.0, 1.0))
+    st = {}
+    for k, v in base.state.items():
+        lo, hi = float(np.min(v)), float(np.max(v))
+        st[k] = np.asfortranarray(rng.uniform(lo, hi, size=(N,) + v.shape[1:]).astype(v.dtype))
+    ibc = np.asfortranarray((rng.random((N, 8)) < 0.2).astype(np.int32))
+    return M.Case(f"fan{m}", mesh, base.params, st, ibc, kernel, kspace=30, gmres_tol=1e-8)
+
+
+@pytest.mark.parametrize("kind", ["nsvof", "tem", "ns"])
+def test_assembly_high_degree_rows(oracle, kind):
+    """Rows of degree 42 (two passes of the gather row pass's off-diagonal
+    lanes, a 40-element contribution list) against the oracle, FP64 1e-12,
+    FP32 1e-5."""
+    kernel = {"nsvof": F.OVS_ASM_NSVOF, "tem": F.OVS_ASM_TEM, "ns": F.OVS_ASM_NS}[kind]
+    case = _fan_case(kernel)
+    oc, ctx, sysid, k, cfl_o, cfl_g = _assemble_both(oracle, case, kernel, 6, F.OVS_FP64)
+    ptr, cols = ctx.get_pattern()
+    assert np.diff(ptr).max() == 42
+    _compare_system(oc, ctx, sysid, k, 6, F.OVS_FP64, 1e-12)
+    ctx.assemble(kernel, 6, F.OVS_FP32)
+    _compare_system(oc, ctx, sysid, k, 6, F.OVS_FP32, 1e-5)
 
 
 @pytest.mark.parametrize("kind", ["nsvof", "tem", "ns"])
