@@ -112,9 +112,16 @@ enum {
                                   lane by lane */
   OVS_OPT_ELEM_SMEM = 4,       /* FP64 tet element pass: 0 (default, the faster one measured) holds the node
                                   records in registers; 1 (env OVS_ELEM_SMEM=1) in shared memory */
-  OVS_OPT_ROWS_GATHER = 5      /* tet row pass: 1 (default) every lane gathers whole blocks of the row by the
-                                  contribution lists built with the pattern; 0 (env OVS_ROWS_GATHER=0) the
-                                  chunked pass, element blocks reduced through shared memory */
+  OVS_OPT_ROWS_GATHER = 5,     /* tet row pass without tiles (OVS_OPT_ROWS_TILED = 0): 1 (default) every lane
+                                  gathers whole blocks of the row by the contribution lists built with the
+                                  pattern, reading the summaries from global memory; 0 (env
+                                  OVS_ROWS_GATHER=0) the chunked pass, element blocks reduced through shared
+                                  memory */
+  OVS_OPT_ROWS_TILED = 6,      /* tet row pass: 1 (env OVS_ROWS_TILED=1) one CTA per tile of rows, the tile's
+                                  element summaries staged in shared memory by bulk copies, then gathered as
+                                  above; 0 (default, the faster one measured) the untiled passes */
+  OVS_OPT_TILE_ELEMS = 7       /* element budget of a row tile (default 96, env OVS_TILE_ELEMS; 4..4000);
+                                  rows with more elements take the untiled gather pass */
 };
 
 /* boundary-face flags (ovs_set_faces) */

@@ -56,6 +56,7 @@ struct AsmArgs {
   int* flags;             // [0] non-positive DetJ count, [1] non-finite residual
   unsigned long long* cfl_bits;
   int N;
+  int nrows;              // row records the row pass visits (N, or the rows a tile cannot hold)
   int mat, vec;
   int max_deg;
   ovs_params p;
@@ -1023,17 +1024,17 @@ assemble_rows_kernel(const AsmArgs a) {
   // row record {A, rowptr[A], n2e_ptr[A], deg | sd << 8 | ne << 16} and the element
   // ids of the first chunk (lanes j < nc hold entry j)
   int4 rr = make_int4(0, 0, 0, 0);
-  if (t < a.N) rr = __ldg(a.row_rec + t);
+  if (t < a.nrows) rr = __ldg(a.row_rec + t);
   int pk_n = 0;
   unsigned s4_n = 0;
-  if (t < a.N && lane < min(CH, rr.w >> 16)) {
+  if (t < a.nrows && lane < min(CH, rr.w >> 16)) {
     pk_n = __ldg(a.n2e + rr.z + lane);
     s4_n = __ldg(a.n2s + rr.z + lane);
   }
-  for (; t < a.N; t += W) {
+  for (; t < a.nrows; t += W) {
     const int A = rr.x, rp = rr.y, ep = rr.z, deg = rr.w & 0xff, ne = rr.w >> 16;
     int4 rn = make_int4(0, 0, 0, 0);
-    if (t + W < a.N) rn = __ldg(a.row_rec + t + W);
+    if (t + W < a.nrows) rn = __ldg(a.row_rec + t + W);
     const unsigned ibA = __ldg(a.ibc + A);
     for (int s = lane; s < deg; s += 32) cp_async4(cols + s, a.colidx + rp + s);
     for (int q = lane; q < deg * NVP; q += 32) acc[q] = (T)0;
@@ -1141,7 +1142,7 @@ assemble_rows_kernel(const AsmArgs a) {
     // the next row's first element ids travel while this row is written
     pk_n = 0;
     s4_n = 0;
-    if (t + W < a.N && lane < min(CH, rn.w >> 16)) {
+    if (t + W < a.nrows && lane < min(CH, rn.w >> 16)) {
       pk_n = __ldg(a.n2e + rn.z + lane);
       s4_n = __ldg(a.n2s + rn.z + lane);
     }
@@ -1225,132 +1226,225 @@ __device__ __forceinline__ void write_block(T* dst, const T* v, const unsigned* 
   }
 }
 
-// Gather row pass (tets, the default): one warp per CSR row, every lane
-// owning whole blocks of the row, so that no block passes through shared
-// memory and only the diagonal is summed across lanes.  Lanes 0..GD-1 take
-// the off-diagonal entries (lane l the l-th, counting past the diagonal
-// slot; a row with more than GD of them takes further passes) and add the
-// blocks of the entry's contribution list, one per round, in ascending
-// element order, in registers.  Lanes GD..31 share the diagonal block and
-// the residual rows: lane GD + i takes the row's elements i, i + ND, ...
-// in ascending order, and the ND partial sums are then added in lane
-// order.  Every entry is thus summed in an order fixed by the mesh, the
-// same on every run.  Each round loads the next entry of the lane's list
-// while the current block is expanded.
+// Gather row pass (tets): one warp per CSR row, every lane owning whole
+// blocks of the row, so that no block passes through shared memory and only
+// the diagonal is summed across lanes.  Lanes 0..GD-1 take the off-diagonal
+// entries (lane l the l-th, counting past the diagonal slot; a row with more
+// than GD of them takes further passes) and add the blocks of the entry's
+// contribution list, one per round, in ascending element order, in
+// registers.  Lanes GD..31 share the diagonal block and the residual rows:
+// lane GD + i takes the row's elements i, i + ND, ... in ascending order,
+// and the ND partial sums are then added in lane order.  Every entry is thus
+// summed in an order fixed by the mesh, the same on every run.  Each round
+// loads the next entry of the lane's list while the current block is
+// expanded.  TILED: the element summaries come from the CTA's shared-memory
+// stage (tile-local element numbers in n2e_loc / clist_loc), otherwise from
+// global memory (element ids in n2e / clist).
+template <typename T, int KIND> struct GatherGeom {
+  static constexpr int NV = Lay<KIND>::NV, NF = Lay<KIND>::NF;
+  static constexpr int NVP = NV < 4 ? 1 : NV;
+  static constexpr int ND = 8, GD = 32 - ND;
+  static constexpr int PSTR = ((NVP + NF) * (int)sizeof(T) + 15) / 16 * 16 / (int)sizeof(T);
+};
+
+template <typename T, int KIND, bool TILED>
+__device__ __forceinline__ void gather_row(const AsmArgs& a, const int4 rr, const T* base, int str,
+                                           const uint16_t* n2e_loc, const uint16_t* clist_loc,
+                                           T (*pw)[GatherGeom<T, KIND>::PSTR], const unsigned* masks, int lane) {
+  using L = Lay<KIND>;
+  using Q = GatherGeom<T, KIND>;
+  constexpr int NV = Q::NV, NF = Q::NF, NVP = Q::NVP, ND = Q::ND, GD = Q::GD;
+  const bool diagl = lane >= GD;
+  const int di = lane - GD;   // the diagonal lane's index
+  const int A = rr.x, rp = rr.y, ep = rr.z, deg = rr.w & 0xff, sd = (rr.w >> 8) & 0xff, ne = rr.w >> 16;
+  const unsigned ibA = __ldg(a.ibc + A);
+  const int nod = deg > 0 ? deg - 1 : 0;
+  T* out = reinterpret_cast<T*>(a.vals) + (size_t)rp * NV;
+  const T cnt = (T)ne;
+  for (int o0 = 0; o0 == 0 || o0 < nod; o0 += GD) {
+    const int o = o0 + lane;   // off-diagonal ordinal of the lane
+    const bool offl = !diagl && o < nod;
+    const int s = o < sd ? o : o + 1;
+    int c0 = 0, len = 0;
+    unsigned ibB = 0;
+    if (offl) {
+      c0 = __ldg(a.cptr + rp + s);
+      len = __ldg(a.cptr + rp + s + 1) - c0;
+      ibB = __ldg(a.ibc + __ldg(a.colidx + rp + s));
+    } else if (diagl && o0 == 0) {
+      len = ne > di ? (ne - di + ND - 1) / ND : 0;
+    }
+    const int rounds = (int)__reduce_max_sync(0xffffffffu, (unsigned)len);
+    T acc[NVP], racc[NF];
+#pragma unroll
+    for (int v = 0; v < NVP; ++v) acc[v] = (T)0;
+#pragma unroll
+    for (int f = 0; f < NF; ++f) racc[f] = (T)0;
+    // entry k of the lane's list: off-diagonal (e << 4) | (la << 2) | b,
+    // diagonal (e << 3) | la (tiled: the tile-local element number)
+    auto entry = [&](int k) -> int {
+      if constexpr (TILED) return offl ? (int)__ldg(clist_loc + c0 + k) : (int)__ldg(n2e_loc + ep + di + k * ND);
+      else return offl ? __ldg(a.clist + c0 + k) : __ldg(a.n2e + ep + di + k * ND);
+    };
+    int ent = len > 0 ? entry(0) : 0;
+    for (int k = 0; k < rounds; ++k) {
+      const int cur = ent;
+      if (k + 1 < len) ent = entry(k + 1);
+      if (k < len) {
+        int e, la, b;
+        if (offl) {
+          e = cur >> 4; la = (cur >> 2) & 3; b = cur & 3;
+        } else if constexpr (TILED) {
+          e = cur >> 2; la = cur & 3; b = la;
+        } else {
+          e = cur >> 3; la = cur & 7; b = la;
+        }
+        const T* se = base + (size_t)e * str;
+        T ob[1][NVP];
+        expand_block<T, KIND, 1, TILED>(se, la, b, 0, ob);
+#pragma unroll
+        for (int v = 0; v < NVP; ++v) acc[v] += ob[0][v];
+        if (diagl) {
+#pragma unroll
+          for (int f = 0; f < NF; ++f) racc[f] += ld1<T, TILED>(se + L::RHS0 + NF * la + f);
+        }
+      }
+    }
+    if (offl && a.mat) write_block<T, NV>(out + (size_t)s * NV, acc, masks, ibA, ibB, false, cnt);
+    if (o0 == 0) {
+      if (diagl) {
+#pragma unroll
+        for (int v = 0; v < NVP; ++v) pw[di][v] = acc[v];
+#pragma unroll
+        for (int f = 0; f < NF; ++f) pw[di][NVP + f] = racc[f];
+      }
+      __syncwarp();
+      constexpr int NG = NV >= 4 ? NV / 4 : 1;
+      if (a.mat && deg > 0 && lane < NG) {
+        constexpr int GW = NV >= 4 ? 4 : 1;
+        T v4[GW];
+#pragma unroll
+        for (int u = 0; u < GW; ++u) v4[u] = pw[0][GW * lane + u];
+        for (int i = 1; i < ND; ++i)
+#pragma unroll
+          for (int u = 0; u < GW; ++u) v4[u] += pw[i][GW * lane + u];
+        if constexpr (NV >= 4) {
+#pragma unroll
+          for (int u = 0; u < 4; ++u) {
+            const unsigned m = masks[4 * lane + u];
+            if (ibA & m & 0xffu) v4[u] = (T)0;
+            if ((ibA << 8) & m & 0xff00u) v4[u] = (T)0;
+            if ((ibA << 16) & m & 0xff0000u) v4[u] = cnt;
+          }
+          store4_cs(out + (size_t)sd * NV + 4 * lane, v4);
+        } else {
+          T val = v4[0];
+          if (ibA & TB) val = cnt;
+          __stcs(out + sd, val);
+        }
+      }
+      if (a.vec && lane >= 32 - NF) {
+        const int f = lane - (32 - NF);
+        T v = pw[0][NVP + f];
+        for (int i = 1; i < ND; ++i) v += pw[i][NVP + f];
+        unsigned bit;
+        if (KIND == OVS_ASM_TEM) bit = TB;
+        else bit = (f < 3) ? (1u << f) : (f == 3 ? PB : FB);
+        if (ibA & bit) v = (T)0;
+        if (!isfinite((double)v)) atomicOr(a.flags + 1, 1);
+        __stcs(reinterpret_cast<T*>(a.rhs) + (size_t)f * a.N + A, v);
+      }
+      __syncwarp();
+    }
+  }
+}
+
 template <typename T, int KIND>
 __global__ void __launch_bounds__(128) gather_rows_kernel(const AsmArgs a) {
-  using L = Lay<KIND>;
-  constexpr int NV = L::NV, NF = L::NF;
-  constexpr int NVP = NV < 4 ? 1 : NV;
-  constexpr int ND = 8, GD = 32 - ND;
-  constexpr int PSTR = ((NVP + NF) * (int)sizeof(T) + 15) / 16 * 16 / (int)sizeof(T);
+  using Q = GatherGeom<T, KIND>;
   __shared__ unsigned masks[24];
-  __shared__ __align__(16) T part[4][ND][PSTR];   // the diagonal lanes' partial sums, per warp
+  __shared__ __align__(16) T part[4][Q::ND][Q::PSTR];   // the diagonal lanes' partial sums, per warp
   if (threadIdx.x < 24) masks[threadIdx.x] = (KIND == OVS_ASM_TEM) ? (TB | (TB << 8) | (TB << 16)) : mask_of(threadIdx.x);
   __syncthreads();
   const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
   const T* sum = reinterpret_cast<const T*>(a.rec);
   const int W = gridDim.x * 4;
-  T(*pw)[PSTR] = part[wid];
-  const bool diagl = lane >= GD;
-  const int di = lane - GD;   // the diagonal lane's index
-  for (int t = blockIdx.x * 4 + wid; t < a.N; t += W) {
-    const int4 rr = __ldg(a.row_rec + t);
-    const int A = rr.x, rp = rr.y, ep = rr.z, deg = rr.w & 0xff, sd = (rr.w >> 8) & 0xff, ne = rr.w >> 16;
-    const unsigned ibA = __ldg(a.ibc + A);
-    const int nod = deg > 0 ? deg - 1 : 0;
-    T* out = reinterpret_cast<T*>(a.vals) + (size_t)rp * NV;
-    const T cnt = (T)ne;
-    for (int o0 = 0; o0 == 0 || o0 < nod; o0 += GD) {
-      const int o = o0 + lane;   // off-diagonal ordinal of the lane
-      const bool offl = !diagl && o < nod;
-      const int s = o < sd ? o : o + 1;
-      int c0 = 0, len = 0;
-      unsigned ibB = 0;
-      if (offl) {
-        c0 = __ldg(a.cptr + rp + s);
-        len = __ldg(a.cptr + rp + s + 1) - c0;
-        ibB = __ldg(a.ibc + __ldg(a.colidx + rp + s));
-      } else if (diagl && o0 == 0) {
-        len = ne > di ? (ne - di + ND - 1) / ND : 0;
-      }
-      const int rounds = __reduce_max_sync(0xffffffffu, (unsigned)len);
-      T acc[NVP], racc[NF];
-#pragma unroll
-      for (int v = 0; v < NVP; ++v) acc[v] = (T)0;
-#pragma unroll
-      for (int f = 0; f < NF; ++f) racc[f] = (T)0;
-      int ent = 0;
-      if (len > 0) ent = offl ? __ldg(a.clist + c0) : __ldg(a.n2e + ep + di);
-      for (int k = 0; k < rounds; ++k) {
-        const int cur = ent;
-        if (k + 1 < len) ent = offl ? __ldg(a.clist + c0 + k + 1) : __ldg(a.n2e + ep + di + (k + 1) * ND);
-        if (k < len) {
-          int e, la, b;
-          if (offl) {
-            e = cur >> 4; la = (cur >> 2) & 3; b = cur & 3;
-          } else {
-            e = cur >> 3; la = cur & 7; b = la;
-          }
-          const T* se = sum + (size_t)e * L::SW;
-          T ob[1][NVP];
-          expand_block<T, KIND, 1>(se, la, b, 0, ob);
-#pragma unroll
-          for (int v = 0; v < NVP; ++v) acc[v] += ob[0][v];
-          if (diagl) {
-#pragma unroll
-            for (int f = 0; f < NF; ++f) racc[f] += __ldg(se + L::RHS0 + NF * la + f);
-          }
-        }
-      }
-      if (offl && a.mat) write_block<T, NV>(out + (size_t)s * NV, acc, masks, ibA, ibB, false, cnt);
-      if (o0 == 0) {
-        if (diagl) {
-#pragma unroll
-          for (int v = 0; v < NVP; ++v) pw[di][v] = acc[v];
-#pragma unroll
-          for (int f = 0; f < NF; ++f) pw[di][NVP + f] = racc[f];
-        }
-        __syncwarp();
-        constexpr int NG = NV >= 4 ? NV / 4 : 1;
-        if (a.mat && deg > 0 && lane < NG) {
-          constexpr int GW = NV >= 4 ? 4 : 1;
-          T v4[GW];
-#pragma unroll
-          for (int u = 0; u < GW; ++u) v4[u] = pw[0][GW * lane + u];
-          for (int i = 1; i < ND; ++i)
-#pragma unroll
-            for (int u = 0; u < GW; ++u) v4[u] += pw[i][GW * lane + u];
-          if constexpr (NV >= 4) {
-#pragma unroll
-            for (int u = 0; u < 4; ++u) {
-              const unsigned m = masks[4 * lane + u];
-              if (ibA & m & 0xffu) v4[u] = (T)0;
-              if ((ibA << 8) & m & 0xff00u) v4[u] = (T)0;
-              if ((ibA << 16) & m & 0xff0000u) v4[u] = cnt;
-            }
-            store4_cs(out + (size_t)sd * NV + 4 * lane, v4);
-          } else {
-            T val = v4[0];
-            if (ibA & TB) val = cnt;
-            __stcs(out + sd, val);
-          }
-        }
-        if (a.vec && lane >= 32 - NF) {
-          const int f = lane - (32 - NF);
-          T v = pw[0][NVP + f];
-          for (int i = 1; i < ND; ++i) v += pw[i][NVP + f];
-          unsigned bit;
-          if (KIND == OVS_ASM_TEM) bit = TB;
-          else bit = (f < 3) ? (1u << f) : (f == 3 ? PB : FB);
-          if (ibA & bit) v = (T)0;
-          if (!isfinite((double)v)) atomicOr(a.flags + 1, 1);
-          __stcs(reinterpret_cast<T*>(a.rhs) + (size_t)f * a.N + A, v);
-        }
-        __syncwarp();
-      }
-    }
+  for (int t = blockIdx.x * 4 + wid; t < a.nrows; t += W)
+    gather_row<T, KIND, false>(a, __ldg(a.row_rec + t), sum, Lay<KIND>::SW, nullptr, nullptr, part[wid], masks,
+                               lane);
+}
+
+// ---------------------------------------------------------- tiled row pass
+// One CTA per row tile (ovs_tiles_build): the summaries of the tile's
+// elements are copied into shared memory by bulk asynchronous copies
+// (cp.async.bulk, completing on one mbarrier; from this GPU's own memory, no
+// multicast), then the four warps take the tile's rows by the gather scheme
+// above, reading the summaries from shared memory.  Each summary is fetched
+// in whole 16-byte units, once per tile that uses it, instead of lane by
+// lane in scattered 16-byte loads.
+struct TileArgs {
+  const int* rptr;
+  const int* rows;
+  const int* eptr;
+  const int* elems;
+  const uint16_t* n2e_loc;
+  const uint16_t* clist_loc;
+};
+
+// a staged summary's stride in shared memory: an odd number of 16-byte
+// units, so the lanes reading different elements spread over the banks
+template <typename T, int KIND> struct TileStage {
+  static constexpr int SWB = Lay<KIND>::SW * (int)sizeof(T);
+  static constexpr int STRB = 16 * ((SWB / 16) | 1);
+  static constexpr int STR = STRB / (int)sizeof(T);
+  static_assert(SWB % 16 == 0, "summaries must be whole 16-byte units");
+};
+
+constexpr long TILE_WAIT_LIMIT = 1L << 26;   // bounded mbarrier wait (polls)
+
+template <typename T, int KIND>
+__global__ void __launch_bounds__(128) tiled_rows_kernel(const AsmArgs a, const TileArgs ta) {
+  using Q = GatherGeom<T, KIND>;
+  using G = TileStage<T, KIND>;
+  extern __shared__ __align__(128) unsigned char tile_smem[];
+  __shared__ __align__(8) unsigned long long bar;
+  __shared__ unsigned masks[24];
+  __shared__ __align__(16) T part[4][Q::ND][Q::PSTR];
+  T* stage = reinterpret_cast<T*>(tile_smem);
+  const int tile = blockIdx.x;
+  const int k0 = __ldg(ta.eptr + tile), nel = __ldg(ta.eptr + tile + 1) - k0;
+  const unsigned barp = (unsigned)__cvta_generic_to_shared(&bar);
+  if (threadIdx.x == 0) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(barp));
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
   }
+  if (threadIdx.x < 24) masks[threadIdx.x] = (KIND == OVS_ASM_TEM) ? (TB | (TB << 8) | (TB << 16)) : mask_of(threadIdx.x);
+  __syncthreads();
+  if (threadIdx.x == 0)
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(barp), "r"((unsigned)(nel * G::SWB))
+                 : "memory");
+  __syncthreads();   // the expected bytes are registered before any copy completes
+  const T* sum = reinterpret_cast<const T*>(a.rec);
+  for (int k = threadIdx.x; k < nel; k += blockDim.x) {
+    const int e = __ldg(ta.elems + k0 + k);
+    asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];"
+                 ::"r"((unsigned)__cvta_generic_to_shared(stage + (size_t)k * G::STR)), "l"(sum + (size_t)e * Lay<KIND>::SW),
+                 "r"((unsigned)G::SWB), "r"(barp)
+                 : "memory");
+  }
+  unsigned done = 0;
+  for (long it = 0; it < TILE_WAIT_LIMIT && !done; ++it)
+    asm volatile("{\n\t.reg .pred p;\n\tmbarrier.try_wait.parity.shared::cta.b64 p, [%1], 0;\n\t"
+                 "selp.u32 %0, 1, 0, p;\n\t}\n" : "=r"(done) : "r"(barp) : "memory");
+  if (!done) {   // the copies did not land: report, assemble nothing
+    if (threadIdx.x == 0) atomicOr(a.flags + 2, 1);
+    return;
+  }
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+  const int r1 = __ldg(ta.rptr + tile + 1);
+  for (int r = __ldg(ta.rptr + tile) + wid; r < r1; r += 4)
+    gather_row<T, KIND, true>(a, __ldg(a.row_rec + __ldg(ta.rows + r)), stage, G::STR, ta.n2e_loc, ta.clist_loc,
+                              part[wid], masks, lane);
 }
 
 // ---------------------------------------------------- alpha-stage records
@@ -1428,13 +1522,36 @@ int launch_gather(ovs_ctx* c, const AsmArgs& a) {
   int per_sm = 0;
   OVS_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, 128, 0));
   if (per_sm < 1) return OVS_ERR_ARG;
-  long need = ((long)c->N + 3) / 4;
+  long need = ((long)a.nrows + 3) / 4;
   long grid = (long)per_sm * c->num_sms * 4;
   if (grid > need) grid = need;
   if (grid < 1) grid = 1;
   kern<<<(int)grid, 128, 0, c->stream>>>(a);
   ++c->launches;
   OVS_CUDA_TRY(cudaGetLastError());
+  return OVS_OK;
+}
+
+template <typename T, int KIND>
+int launch_tiled(ovs_ctx* c, const AsmArgs& a) {
+  int st;
+  if ((st = ovs_tiles_build(c, c->tile_elems_opt))) return st;
+  using G = TileStage<T, KIND>;
+  const size_t smem = (size_t)c->tile_maxe * G::STRB;
+  auto kern = tiled_rows_kernel<T, KIND>;
+  OVS_CUDA_TRY(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  const TileArgs ta{c->tile_rptr, c->tile_rows, c->tile_eptr, c->tile_elems, c->n2e_loc, c->clist_loc};
+  if (c->ntiles > 0) {
+    kern<<<c->ntiles, 128, smem, c->stream>>>(a, ta);
+    ++c->launches;
+    OVS_CUDA_TRY(cudaGetLastError());
+  }
+  if (c->nbig > 0) {   // rows with more elements than a tile holds
+    AsmArgs b = a;
+    b.row_rec = c->big_rec;
+    b.nrows = c->nbig;
+    return launch_gather<T, KIND>(c, b);
+  }
   return OVS_OK;
 }
 
@@ -1459,6 +1576,7 @@ int launch_assemble(ovs_ctx* c, const AsmArgs& a, const SumArgs& sa, int parts =
   // pass 2: rows
   // the temperature summaries (20 values, one lane per element) gain
   // nothing from staging: measured slower, so it reads them directly
+  if (c->rows_tiled && c->cptr) return launch_tiled<T, KIND>(c, a);
   if (c->rows_gather && c->cptr) return launch_gather<T, KIND>(c, a);
   if (c->rows_staged && KIND != OVS_ASM_TEM) return launch_rows<T, KIND, 4, true>(c, a);
   return launch_rows<T, KIND, 4, false>(c, a);
@@ -1669,6 +1787,7 @@ static void fill_args(ovs_ctx* c, int prec, SysStore& S, int tensor_flag, AsmArg
   a.flags = c->flags;
   a.cfl_bits = c->cfl_bits;
   a.N = c->N;
+  a.nrows = c->N;
   a.mat = (tensor_flag & OVS_TENSOR_MAT) != 0;
   a.vec = (tensor_flag & OVS_TENSOR_VEC) != 0;
   a.n2s = c->n2s;

@@ -202,6 +202,10 @@ int create_resources(ovs_ctx* c, const ovs_dims* dims) {
     if (es) c->elem_smem = es[0] != '0';
     const char* rg = getenv("OVS_ROWS_GATHER");
     if (rg) c->rows_gather = rg[0] != '0';
+    const char* rt = getenv("OVS_ROWS_TILED");
+    if (rt) c->rows_tiled = rt[0] != '0';
+    const char* te = getenv("OVS_TILE_ELEMS");
+    if (te && atoi(te) >= 4 && atoi(te) <= 4000) c->tile_elems_opt = atoi(te);
   }
   c->N = dims->nnode;
   c->E = dims->nelem;
@@ -260,7 +264,8 @@ int ovs_destroy(ovs_ctx* c) {
   ovs_streaming_free(c);
   if (c->hex_kbuf) cudaFree(c->hex_kbuf);
   if (c->hex_w) cudaFree(c->hex_w);
-  void* ptrs[] = {c->ien, c->elm_id, c->ibc, c->rowptr, c->colidx, c->diag, c->n2e_ptr, c->n2e, c->n2s, c->row_order, c->row_rec, c->cptr, c->clist, c->tmap, c->vals_t, c->vjp_cot, c->vjp_ge, c->vjp_grad,
+  void* ptrs[] = {c->ien, c->elm_id, c->ibc, c->rowptr, c->colidx, c->diag, c->n2e_ptr, c->n2e, c->n2s, c->row_order, c->row_rec, c->cptr, c->clist, c->tile_rptr, c->tile_rows,
+                  c->tile_eptr, c->tile_elems, c->n2e_loc, c->clist_loc, c->big_rec, c->tmap, c->vals_t, c->vjp_cot, c->vjp_ge, c->vjp_grad,
                   c->rec[0], c->rec[1], c->esum[0], c->esum[1], c->gm, c->basis[0], c->basis[1], c->work64, c->work32, c->wvec, c->coop_part,
                   c->flags, c->cfl_bits};
   for (void* p : ptrs) if (p) cudaFree(p);
@@ -406,6 +411,11 @@ int ovs_set_option(ovs_ctx* c, int option, int value) {
     case OVS_OPT_ROWS_STAGED: c->rows_staged = value != 0; return OVS_OK;
     case OVS_OPT_ELEM_SMEM: c->elem_smem = value != 0; return OVS_OK;
     case OVS_OPT_ROWS_GATHER: c->rows_gather = value != 0; return OVS_OK;
+    case OVS_OPT_ROWS_TILED: c->rows_tiled = value != 0; return OVS_OK;
+    case OVS_OPT_TILE_ELEMS:
+      if (value < 4 || value > 4000) return OVS_ERR_ARG;
+      c->tile_elems_opt = value;
+      return OVS_OK;
     case OVS_OPT_ARNOLDI_FUSED: c->arnoldi_fused = value != 0; return OVS_OK;
     default: return OVS_ERR_ARG;
   }

@@ -98,6 +98,18 @@ struct ovs_ctx {
   int4* row_rec = nullptr;   // N: per row in that order {A, rowptr[A], n2e_ptr[A], deg | sd << 8 | ne << 16}
   int* cptr = nullptr;       // nnz + 1: off-diagonal contribution lists (tets), offsets into clist
   int* clist = nullptr;      // 12 E entries (e << 4) | (la << 2) | b, ascending element per entry
+  // row tiles of the tiled row pass (tets; built at the first assembly that
+  // takes that pass, ovs_tiles_build): runs of consecutive rows of row_rec
+  // whose elements, at most tile_maxe of them, are staged in one CTA's
+  // shared memory
+  int ntiles = 0, nbig = 0, tile_maxe = 0;
+  int* tile_rptr = nullptr;  // ntiles + 1: offsets into tile_rows
+  int* tile_rows = nullptr;  // row positions t (into row_rec) of each tile
+  int* tile_eptr = nullptr;  // ntiles + 1: offsets into tile_elems
+  int* tile_elems = nullptr; // the tile's elements, in first-use order
+  uint16_t* n2e_loc = nullptr;   // per n2e entry: (tile-local element << 2) | la
+  uint16_t* clist_loc = nullptr; // per clist entry: (tile-local element << 4) | (la << 2) | b
+  int4* big_rec = nullptr;   // nbig row records of rows with more than tile_maxe elements
   unsigned* n2s = nullptr;   // nshl*E entries: slots of the element's nodes in the row, one byte each
                              // (one word per entry for tets, two for hexahedra)
   int nnz = 0;
@@ -128,6 +140,11 @@ struct ovs_ctx {
   // tet row pass: lanes gather whole blocks by the contribution lists (1,
   // default) or the chunked pass reduces element blocks in shared memory (0)
   int rows_gather = 1;
+  // tet row pass: rows in CTA tiles with their element summaries staged in
+  // shared memory by bulk copies (1; default 0, measured slower than the
+  // gather pass), the element budget per tile
+  int rows_tiled = 0;
+  int tile_elems_opt = 96;
   void* hex_kbuf = nullptr;              // E x 64 x 24 block values
   float* hex_w = nullptr;                // W hi + lo, canonical layout
   // boundary-condition producers (ovs_set_bc_spec)
@@ -174,6 +191,7 @@ struct ovs_ctx {
 
 // ------------------------------------------------------------ helpers
 int ovs_ensure(void** p, size_t bytes);
+int ovs_tiles_build(ovs_ctx* c, int maxe);
 int ovs_activate(ovs_ctx* c);
 
 // pattern.cu

@@ -467,6 +467,107 @@ static int build_contrib(ovs_ctx* c) {
   return OVS_OK;
 }
 
+// Row tiles of the tiled row pass, built on the host from the row records,
+// the node-to-element lists and the contribution lists: consecutive rows of
+// the row order (Morton order of the nodes, so a tile is a compact cluster
+// of nodes) are added to a tile while its distinct elements stay within
+// maxe and its rows within 16.  For every row entry the element is
+// renumbered to its place in the tile's element list (n2e_loc, clist_loc).
+// A row with more than maxe elements takes no tile (big_rec lists them for
+// the gather pass).
+int ovs_tiles_build(ovs_ctx* c, int maxe) {
+  constexpr int RMAX = 16;
+  cudaStream_t s = c->stream;
+  const int N = c->N, E = c->E;
+  if (c->nshl != 4 || !c->cptr || !c->row_rec || N < 1) return OVS_ERR_STATE;
+  if (maxe < 4 || maxe > 4000) return OVS_ERR_ARG;
+  if (c->tile_maxe == maxe && c->tile_rptr) return OVS_OK;
+  void** olds[] = {(void**)&c->tile_rptr, (void**)&c->tile_rows, (void**)&c->tile_eptr, (void**)&c->tile_elems,
+                   (void**)&c->n2e_loc, (void**)&c->clist_loc, (void**)&c->big_rec};
+  for (void** q : olds) {
+    if (*q) cudaFree(*q);
+    *q = nullptr;
+  }
+  c->ntiles = c->nbig = c->tile_maxe = 0;
+  const size_t EN = (size_t)E * 4, NC = (size_t)12 * E, nnz = (size_t)c->nnz;
+  std::vector<int4> rec(N);
+  std::vector<int> n2e(EN), cptr(nnz + 1), clist(NC > 0 ? NC : 1);
+  OVS_CUDA_TRY(cudaMemcpyAsync(rec.data(), c->row_rec, sizeof(int4) * N, cudaMemcpyDeviceToHost, s));
+  OVS_CUDA_TRY(cudaMemcpyAsync(n2e.data(), c->n2e, sizeof(int) * EN, cudaMemcpyDeviceToHost, s));
+  OVS_CUDA_TRY(cudaMemcpyAsync(cptr.data(), c->cptr, sizeof(int) * (nnz + 1), cudaMemcpyDeviceToHost, s));
+  if (NC) OVS_CUDA_TRY(cudaMemcpyAsync(clist.data(), c->clist, sizeof(int) * NC, cudaMemcpyDeviceToHost, s));
+  OVS_CUDA_TRY(cudaStreamSynchronize(s));
+  std::vector<int> stamp(E, -1), loc(E, 0), trptr{0}, trows, teptr{0}, telems;
+  std::vector<uint16_t> n2e_loc(EN, 0), clist_loc(NC > 0 ? NC : 1, 0);
+  std::vector<int4> big;
+  trows.reserve(N);
+  telems.reserve((size_t)N * 20);
+  int tile = 0, cnt = 0, rows = 0;
+  for (int t = 0; t < N; ++t) {
+    const int4 r = rec[t];
+    const int rp = r.y, ep = r.z, deg = r.w & 0xff, sd = (r.w >> 8) & 0xff, ne = r.w >> 16;
+    if (ne > maxe) {
+      big.push_back(r);
+      continue;
+    }
+    int nnew = 0;
+    for (int j = 0; j < ne; ++j) nnew += stamp[n2e[ep + j] >> 3] != tile;
+    if (rows > 0 && (cnt + nnew > maxe || rows >= RMAX)) {   // close the tile
+      trptr.push_back((int)trows.size());
+      teptr.push_back((int)telems.size());
+      ++tile;
+      cnt = rows = 0;
+    }
+    for (int j = 0; j < ne; ++j) {
+      const int e = n2e[ep + j] >> 3, la = n2e[ep + j] & 7;
+      if (stamp[e] != tile) {
+        stamp[e] = tile;
+        loc[e] = cnt++;
+        telems.push_back(e);
+      }
+      n2e_loc[ep + j] = (uint16_t)((loc[e] << 2) | la);
+    }
+    for (int q = 0; q < deg; ++q) {
+      if (q == sd) continue;
+      for (int k = cptr[rp + q]; k < cptr[rp + q + 1]; ++k)
+        clist_loc[k] = (uint16_t)((loc[clist[k] >> 4] << 4) | (clist[k] & 15));
+    }
+    trows.push_back(t);
+    ++rows;
+  }
+  if (rows > 0) {
+    trptr.push_back((int)trows.size());
+    teptr.push_back((int)telems.size());
+    ++tile;
+  }
+  int st;
+  const int nt = tile;
+  if ((st = ovs_ensure((void**)&c->tile_rptr, sizeof(int) * (nt + 1)))) return st;
+  if ((st = ovs_ensure((void**)&c->tile_rows, sizeof(int) * (trows.size() + 1)))) return st;
+  if ((st = ovs_ensure((void**)&c->tile_eptr, sizeof(int) * (nt + 1)))) return st;
+  if ((st = ovs_ensure((void**)&c->tile_elems, sizeof(int) * (telems.size() + 1)))) return st;
+  if ((st = ovs_ensure((void**)&c->n2e_loc, sizeof(uint16_t) * EN))) return st;
+  if ((st = ovs_ensure((void**)&c->clist_loc, sizeof(uint16_t) * clist_loc.size()))) return st;
+  if ((st = ovs_ensure((void**)&c->big_rec, sizeof(int4) * (big.size() + 1)))) return st;
+  OVS_CUDA_TRY(cudaMemcpyAsync(c->tile_rptr, trptr.data(), sizeof(int) * (nt + 1), cudaMemcpyHostToDevice, s));
+  if (!trows.empty())
+    OVS_CUDA_TRY(cudaMemcpyAsync(c->tile_rows, trows.data(), sizeof(int) * trows.size(), cudaMemcpyHostToDevice, s));
+  OVS_CUDA_TRY(cudaMemcpyAsync(c->tile_eptr, teptr.data(), sizeof(int) * (nt + 1), cudaMemcpyHostToDevice, s));
+  if (!telems.empty())
+    OVS_CUDA_TRY(
+        cudaMemcpyAsync(c->tile_elems, telems.data(), sizeof(int) * telems.size(), cudaMemcpyHostToDevice, s));
+  OVS_CUDA_TRY(cudaMemcpyAsync(c->n2e_loc, n2e_loc.data(), sizeof(uint16_t) * EN, cudaMemcpyHostToDevice, s));
+  OVS_CUDA_TRY(cudaMemcpyAsync(c->clist_loc, clist_loc.data(), sizeof(uint16_t) * clist_loc.size(),
+                               cudaMemcpyHostToDevice, s));
+  if (!big.empty())
+    OVS_CUDA_TRY(cudaMemcpyAsync(c->big_rec, big.data(), sizeof(int4) * big.size(), cudaMemcpyHostToDevice, s));
+  OVS_CUDA_TRY(cudaStreamSynchronize(s));
+  c->ntiles = nt;
+  c->nbig = (int)big.size();
+  c->tile_maxe = maxe;
+  return OVS_OK;
+}
+
 int ovs_pattern_build(ovs_ctx* c) {
   cudaStream_t s = c->stream;
   const int N = c->N, E = c->E, nshl = c->nshl;

@@ -411,6 +411,7 @@ def test_row_pass_variants_bit_identical(kind, prec):
     out = []
     for staged in (0, 1):
         ctx = _ctx(case)
+        ctx.set_option(F.OVS_OPT_ROWS_TILED, 0)
         ctx.set_option(F.OVS_OPT_ROWS_GATHER, 0)
         ctx.set_option(F.OVS_OPT_ROWS_STAGED, staged)
         ctx.assemble(kernel, 6, prec)
@@ -422,26 +423,29 @@ def test_row_pass_variants_bit_identical(kind, prec):
 
 @pytest.mark.parametrize("kind", ["nsvof", "tem", "ns"])
 @pytest.mark.parametrize("prec,tol", [(F.OVS_FP64, 1e-14), (F.OVS_FP32, 1e-6)])
-def test_gather_and_chunked_row_passes_agree(kind, prec, tol):
-    """The gather row pass (default) adds the diagonal blocks and the
-    residual rows in eight interleaved partial sums, the chunked pass
-    (OVS_OPT_ROWS_GATHER = 0) in one ascending sweep; the off-diagonal
-    blocks are added in the same ascending element order by both.  The
-    systems agree to rounding, normwise per block, and the gather pass gives
-    the same bits on a second run."""
+def test_row_passes_agree(kind, prec, tol):
+    """The tiled row pass (default: summaries staged per row tile in shared
+    memory), the untiled gather pass (OVS_OPT_ROWS_TILED = 0) and the
+    chunked pass (also OVS_OPT_ROWS_GATHER = 0).  Tiled and gather add every
+    entry in the same order (the diagonal blocks and the residual rows in
+    eight interleaved partial sums); the chunked pass adds everything in one
+    ascending sweep.  The systems agree to rounding, normwise per block, and
+    the tiled pass gives the same bits on a second run."""
     kernel = {"nsvof": F.OVS_ASM_NSVOF, "tem": F.OVS_ASM_TEM, "ns": F.OVS_ASM_NS}[kind]
     sysid = {"nsvof": F.OVS_SYS_NSVOF, "tem": F.OVS_SYS_TEM, "ns": F.OVS_SYS_NS}[kind]
     case = M.random_case(nx=6, ny=5, nz=4, seed=23, kernel=kernel)
     out = []
-    for gather in (1, 0, 1):
+    for tiled, gather in ((1, 1), (0, 1), (0, 0), (1, 1)):
         ctx = _ctx(case)
+        ctx.set_option(F.OVS_OPT_ROWS_TILED, tiled)
         ctx.set_option(F.OVS_OPT_ROWS_GATHER, gather)
         ctx.assemble(kernel, 6, prec)
         out.append(ctx.get_system(sysid, prec))
         ctx.close()
     for k in out[0]:
         close(out[0][k], out[1][k], tol, k)
-        np.testing.assert_array_equal(out[0][k], out[2][k], err_msg=k)
+        close(out[1][k], out[2][k], tol, k)
+        np.testing.assert_array_equal(out[0][k], out[3][k], err_msg=k)
 
 
 def _fan_case(kernel, m=40, seed=31):
@@ -472,13 +476,28 @@ def _fan_case(kernel, m=40, seed=31):
 
 
 @pytest.mark.parametrize("kind", ["nsvof", "tem", "ns"])
-def test_assembly_high_degree_rows(oracle, kind):
-    """Rows of degree 42 (two passes of the gather row pass's off-diagonal
+@pytest.mark.parametrize("tile_elems", [0, 96, 16])
+def test_assembly_high_degree_rows(oracle, kind, tile_elems):
+    """Rows of degree 42 (two passes of the gather scheme's off-diagonal
     lanes, a 40-element contribution list) against the oracle, FP64 1e-12,
-    FP32 1e-5."""
+    FP32 1e-5: the default gather pass (0), and the tiled pass with a 96-
+    and a 16-element tile budget (with 16 the two 40-element rows take the
+    untiled gather pass beside the tiles)."""
     kernel = {"nsvof": F.OVS_ASM_NSVOF, "tem": F.OVS_ASM_TEM, "ns": F.OVS_ASM_NS}[kind]
     case = _fan_case(kernel)
-    oc, ctx, sysid, k, cfl_o, cfl_g = _assemble_both(oracle, case, kernel, 6, F.OVS_FP64)
+    oc = oracle.OracleCase(case)
+    ctx = _ctx(case)
+    if tile_elems:
+        ctx.set_option(F.OVS_OPT_ROWS_TILED, 1)
+        ctx.set_option(F.OVS_OPT_TILE_ELEMS, tile_elems)
+    if kernel == F.OVS_ASM_NS:
+        oc.assemble_navsto(6)
+        assembleNavSto(ctx, 6, F.OVS_FP64)
+        sysid, k = F.OVS_SYS_NS, "ns"
+    else:
+        oc.assemble_quenching(6, 3 if kernel == F.OVS_ASM_NSVOF else 4)
+        assembleQuenching(ctx, 6, 3 if kernel == F.OVS_ASM_NSVOF else 4, F.OVS_FP64)
+        sysid, k = (F.OVS_SYS_NSVOF, "nsvof") if kernel == F.OVS_ASM_NSVOF else (F.OVS_SYS_TEM, "tem")
     ptr, cols = ctx.get_pattern()
     assert np.diff(ptr).max() == 42
     _compare_system(oc, ctx, sysid, k, 6, F.OVS_FP64, 1e-12)
