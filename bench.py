@@ -519,16 +519,20 @@ def run_ours(args, world, rank, local_rank, dist):
             prof[f"asm_{kn}_{nm}_ms"] = ctx.profile(F.OVS_PROF_ASSEMBLE, kern, prec, 5)
             prof[f"asm_{kn}_{nm}_elements_ms"] = ctx.profile(F.OVS_PROF_ASSEMBLE_ELEMENTS, kern, prec, 5)
             prof[f"asm_{kn}_{nm}_rows_ms"] = ctx.profile(F.OVS_PROF_ASSEMBLE_ROWS, kern, prec, 5)
-    # the row pass with its element summaries staged through shared memory
-    # (default) against lane-by-lane global reads, same box, same data
+    # the row-pass variants, same box, same data: the chunked pass (element
+    # blocks reduced through shared memory, summaries staged by cp.async),
+    # the tiled pass (summaries staged per row tile by bulk copies) and the
+    # gather pass (the default, last)
     rows_ab = {}
-    for staged in (0, 1):       # ends on the library default (staged)
-        ctx.set_option(F.OVS_OPT_ROWS_STAGED, staged)
+    for vn, opts in (("chunked", ((F.OVS_OPT_ROWS_TILED, 0), (F.OVS_OPT_ROWS_GATHER, 0))),
+                     ("tiled", ((F.OVS_OPT_ROWS_TILED, 1), (F.OVS_OPT_ROWS_GATHER, 1))),
+                     ("gather", ((F.OVS_OPT_ROWS_TILED, 0), (F.OVS_OPT_ROWS_GATHER, 1)))):
+        for o, v in opts:
+            ctx.set_option(o, v)
         for prec, nm in ((F.OVS_FP64, "fp64"), (F.OVS_FP32, "fp32")):
             for kern, kn in ((F.OVS_ASM_NSVOF, "nsvof"), (F.OVS_ASM_TEM, "tem")):
                 ctx.assemble(kern, 6, prec)
-                rows_ab[f"{kn}_{nm}_{'staged' if staged else 'global'}_ms"] = \
-                    ctx.profile(F.OVS_PROF_ASSEMBLE_ROWS, kern, prec, 5)
+                rows_ab[f"{kn}_{nm}_{vn}_ms"] = ctx.profile(F.OVS_PROF_ASSEMBLE_ROWS, kern, prec, 5)
     prof["rows_variants"] = rows_ab
     # the FP64 element pass with the node records in registers (default)
     # against shared memory
@@ -552,7 +556,7 @@ def run_ours(args, world, rank, local_rank, dist):
     pa_ach = pass64 / (prof["asm_nsvof_fp64_ms"] * 1e-3) / 1e9
     row_ach = pass64 / (prof["asm_nsvof_fp64_rows_ms"] * 1e-3) / 1e9
     dpt, dpt_src = ncu_dram_per_tet("assembly_nsvof_fp64_quench48_dram.md", 663552)
-    roof_asm = {"kernel": "element_summary_kernel + assemble_rows_kernel <double, NSVOF>: one NS+VOF assembly "
+    roof_asm = {"kernel": "element_summary_kernel + gather_rows_kernel <double, NSVOF>: one NS+VOF assembly "
                           "pass (MAT+VEC), the dominant work of the step",
                 "bound": "hbm", "achieved": pa_ach, "peak": hbm, "unit": "GB/s", "frac": pa_ach / hbm,
                 "traffic": dpt * E if dpt else None, "traffic_source": dpt_src, "peak_kind": peak_kind,
@@ -566,7 +570,7 @@ def run_ours(args, world, rank, local_rank, dist):
     fp32_peak = ctx.measure_fp32_peak()
     roof_asm["compute_peaks_measured_tflops"] = {"fp64_fma": fp64_peak, "fp32_fma": fp32_peak}
     pass32 = assembly_pass_bytes(E, N, nnz, 4)
-    roof_asm32 = {"kernels": "element_summary_kernel + assemble_rows_kernel <float, NSVOF>", "bound": "hbm",
+    roof_asm32 = {"kernels": "element_summary_kernel + gather_rows_kernel <float, NSVOF>", "bound": "hbm",
                   "achieved": pass32 / (prof["asm_nsvof_fp32_ms"] * 1e-3) / 1e9, "peak": hbm, "unit": "GB/s",
                   "algorithmic_bytes": pass32, "avg_ms": prof["asm_nsvof_fp32_ms"], "peak_kind": peak_kind}
     roof_asm32["frac"] = roof_asm32["achieved"] / hbm

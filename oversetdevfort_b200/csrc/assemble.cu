@@ -1226,34 +1226,211 @@ __device__ __forceinline__ void write_block(T* dst, const T* v, const unsigned* 
   }
 }
 
-// Gather row pass (tets): one warp per CSR row, every lane owning whole
-// blocks of the row, so that no block passes through shared memory and only
-// the diagonal is summed across lanes.  Lanes 0..GD-1 take the off-diagonal
-// entries (lane l the l-th, counting past the diagonal slot; a row with more
-// than GD of them takes further passes) and add the blocks of the entry's
-// contribution list, one per round, in ascending element order, in
-// registers.  Lanes GD..31 share the diagonal block and the residual rows:
-// lane GD + i takes the row's elements i, i + ND, ... in ascending order,
-// and the ND partial sums are then added in lane order.  Every entry is thus
-// summed in an order fixed by the mesh, the same on every run.  Each round
-// loads the next entry of the lane's list while the current block is
-// expanded.  TILED: the element summaries come from the CTA's shared-memory
-// stage (tile-local element numbers in n2e_loc / clist_loc), otherwise from
-// global memory (element ids in n2e / clist).
+// Gather row pass (tets): one warp per CSR row, every lane summing whole
+// blocks of the row in registers, so that no element block passes through
+// shared memory.  The work of a row is its off-diagonal entries'
+// contribution lists (the elements holding both nodes, ascending) and the
+// diagonal entry's list (all the row's elements, ascending, with the
+// residual rows).  Each list is cut into pieces of at most R consecutive
+// entries, R the fewest rounds for which the pieces fit the 32 lanes (an
+// interior Kuhn-mesh row: 96 entries, lists of 4, 6 and 24, R = 4); a lane
+// adds its piece one entry per round, loading the next entry while the
+// current block is expanded.  The pieces' sums then meet in the warp's
+// shared memory, and each output task (entry, 4-value group) adds its
+// entry's pieces in order and writes the group, consecutive lanes writing
+// consecutive groups.  Every entry is summed in an order fixed by the mesh,
+// the same on every run.  A row with more than 31 off-diagonal entries
+// takes further passes.  TILED: the element summaries come from the CTA's
+// shared-memory stage (tile-local element numbers in n2e_loc / clist_loc),
+// otherwise from global memory (element ids in n2e / clist).
 template <typename T, int KIND> struct GatherGeom {
   static constexpr int NV = Lay<KIND>::NV, NF = Lay<KIND>::NF;
   static constexpr int NVP = NV < 4 ? 1 : NV;
-  static constexpr int ND = 8, GD = 32 - ND;
   static constexpr int PSTR = ((NVP + NF) * (int)sizeof(T) + 15) / 16 * 16 / (int)sizeof(T);
 };
+// per warp: the lanes' piece sums and the pass's entry table (slot, first
+// lane, lanes, column mask; the diagonal last)
+template <typename T, int KIND> struct GatherSmem {
+  T part[32][GatherGeom<T, KIND>::PSTR];
+  int slot[33], first[33], nl[33];
+  unsigned ib[33];
+};
+
+__device__ __forceinline__ int warp_excl_scan(int v, int lane) {
+  int x = v;
+#pragma unroll
+  for (int d = 1; d < 32; d <<= 1) {
+    const int y = __shfl_up_sync(0xffffffffu, x, d);
+    if (lane >= d) x += y;
+  }
+  return x - v;
+}
 
 template <typename T, int KIND, bool TILED>
 __device__ __forceinline__ void gather_row(const AsmArgs& a, const int4 rr, const T* base, int str,
                                            const uint16_t* n2e_loc, const uint16_t* clist_loc,
-                                           T (*pw)[GatherGeom<T, KIND>::PSTR], const unsigned* masks, int lane) {
+                                           GatherSmem<T, KIND>& w, const unsigned* masks, int lane) {
   using L = Lay<KIND>;
   using Q = GatherGeom<T, KIND>;
-  constexpr int NV = Q::NV, NF = Q::NF, NVP = Q::NVP, ND = Q::ND, GD = Q::GD;
+  constexpr int NV = Q::NV, NF = Q::NF, NVP = Q::NVP;
+  constexpr int NG = NV >= 4 ? NV / 4 : 1, GW = NV >= 4 ? 4 : 1;
+  constexpr unsigned FULL = 0xffffffffu;
+  const int A = rr.x, rp = rr.y, ep = rr.z, deg = rr.w & 0xff, sd = (rr.w >> 8) & 0xff, ne = rr.w >> 16;
+  const unsigned ibA = __ldg(a.ibc + A);
+  const int nod = deg > 0 ? deg - 1 : 0;
+  T* out = reinterpret_cast<T*>(a.vals) + (size_t)rp * NV;
+  const T cnt = (T)ne;
+  for (int o0 = 0; o0 == 0 || o0 < nod;) {
+    const bool wd = o0 == 0;                        // this pass also takes the diagonal and the residual
+    const int nsl = min(nod - o0, wd ? 31 : 32);    // the pass's off-diagonal entries
+    int s = 0, c0 = 0, len = 0;                     // lane j < nsl: entry j
+    unsigned ibB = 0;
+    if (lane < nsl) {
+      const int o = o0 + lane;
+      s = o < sd ? o : o + 1;
+      c0 = __ldg(a.cptr + rp + s);
+      len = __ldg(a.cptr + rp + s + 1) - c0;
+      ibB = __ldg(a.ibc + __ldg(a.colidx + rp + s));
+    }
+    const int nd = wd ? ne : 0;
+    int R = max(1, (__reduce_add_sync(FULL, len) + nd + 31) / 32);
+    while (__reduce_add_sync(FULL, (len + R - 1) / R) + (nd + R - 1) / R > 32) ++R;
+    const int P = (len + R - 1) / R;                // lanes of entry j
+    const int F = warp_excl_scan(P, lane);          // its first lane
+    const int Fd = __reduce_add_sync(FULL, P);      // the diagonal's first lane
+    const int PD = (nd + R - 1) / R;
+    if (lane < nsl) {
+      w.slot[lane] = s; w.first[lane] = F; w.nl[lane] = P; w.ib[lane] = ibB;
+    }
+    if (wd && lane == 0) {
+      w.slot[nsl] = sd; w.first[nsl] = Fd; w.nl[nsl] = PD; w.ib[nsl] = ibA;
+    }
+    // this lane's piece: of entry k (the last with first lane <= lane), or
+    // of the diagonal list
+    int k = 0;
+#pragma unroll
+    for (int step = 16; step > 0; step >>= 1) {
+      const int j = k + step;
+      const int Fj = __shfl_sync(FULL, F, j & 31);
+      if (j < nsl && Fj <= lane) k = j;
+    }
+    const int Fk = __shfl_sync(FULL, F, k), c0k = __shfl_sync(FULL, c0, k), lenk = __shfl_sync(FULL, len, k);
+    const bool dl = lane >= Fd && lane < Fd + PD;  // a diagonal piece
+    int pc0 = 0, plen = 0;
+    if (lane < Fd) {
+      pc0 = c0k + (lane - Fk) * R;
+      plen = min(R, lenk - (lane - Fk) * R);
+    } else if (dl) {
+      pc0 = ep + (lane - Fd) * R;
+      plen = min(R, ne - (lane - Fd) * R);
+    }
+    T acc[NVP], racc[NF];
+#pragma unroll
+    for (int v = 0; v < NVP; ++v) acc[v] = (T)0;
+#pragma unroll
+    for (int f = 0; f < NF; ++f) racc[f] = (T)0;
+    // entry i of the piece: off-diagonal (e << 4) | (la << 2) | b, diagonal
+    // (e << 3) | la (tiled: (tile-local element << 2) | la)
+    auto entry = [&](int i) -> int {
+      if constexpr (TILED) return dl ? (int)__ldg(n2e_loc + pc0 + i) : (int)__ldg(clist_loc + pc0 + i);
+      else return dl ? __ldg(a.n2e + pc0 + i) : __ldg(a.clist + pc0 + i);
+    };
+    int ent = plen > 0 ? entry(0) : 0;
+    for (int r = 0; r < R; ++r) {
+      const int cur = ent;
+      if (r + 1 < plen) ent = entry(r + 1);
+      if (r < plen) {
+        int e, la, b;
+        if (!dl) {
+          e = cur >> 4; la = (cur >> 2) & 3; b = cur & 3;
+        } else if constexpr (TILED) {
+          e = cur >> 2; la = cur & 3; b = la;
+        } else {
+          e = cur >> 3; la = cur & 7; b = la;
+        }
+        const T* se = base + (size_t)e * str;
+        T ob[1][NVP];
+        expand_block<T, KIND, 1, TILED>(se, la, b, 0, ob);
+#pragma unroll
+        for (int v = 0; v < NVP; ++v) acc[v] += ob[0][v];
+        if (dl) {
+#pragma unroll
+          for (int f = 0; f < NF; ++f) racc[f] += ld1<T, TILED>(se + L::RHS0 + NF * la + f);
+        }
+      }
+    }
+    if (plen > 0) {
+#pragma unroll
+      for (int v = 0; v < NVP; ++v) w.part[lane][v] = acc[v];
+      if (dl) {
+#pragma unroll
+        for (int f = 0; f < NF; ++f) w.part[lane][NVP + f] = racc[f];
+      }
+    }
+    __syncwarp();
+    // output tasks (entry j, group g): the entry's pieces added in order
+    if (a.mat && deg > 0) {
+      const int nt = (nsl + (wd ? 1 : 0)) * NG;
+      for (int q = lane; q < nt; q += 32) {
+        const int j = q / NG, g = q - j * NG;
+        const int f0 = w.first[j], n = w.nl[j];
+        const unsigned ib = w.ib[j];
+        const bool dg = wd && j == nsl;
+        T v[GW];
+#pragma unroll
+        for (int u = 0; u < GW; ++u) v[u] = (T)0;
+        for (int pp = 0; pp < n; ++pp)
+#pragma unroll
+          for (int u = 0; u < GW; ++u) v[u] += w.part[f0 + pp][GW * g + u];
+        T* dst = out + (size_t)w.slot[j] * NV + GW * g;
+        if constexpr (NV >= 4) {
+          if ((ibA | ib) != 0u) {
+#pragma unroll
+            for (int u = 0; u < 4; ++u) {
+              const unsigned m = masks[4 * g + u];
+              if ((ibA & m & 0xffu) || ((ib << 8) & m & 0xff00u)) v[u] = (T)0;
+              if (dg && ((ibA << 16) & m & 0xff0000u)) v[u] = cnt;
+            }
+          }
+          store4_cs(dst, v);
+        } else {
+          if ((ibA & TB) || (ib & TB)) v[0] = (T)0;
+          if (dg && (ibA & TB)) v[0] = cnt;
+          __stcs(dst, v[0]);
+        }
+      }
+    }
+    if (wd && a.vec && lane < NF) {
+      T v = (T)0;
+      for (int pp = 0; pp < PD; ++pp) v += w.part[Fd + pp][NVP + lane];
+      unsigned bit;
+      if (KIND == OVS_ASM_TEM) bit = TB;
+      else bit = (lane < 3) ? (1u << lane) : (lane == 3 ? PB : FB);
+      if (ibA & bit) v = (T)0;
+      if (!isfinite((double)v)) atomicOr(a.flags + 1, 1);
+      __stcs(reinterpret_cast<T*>(a.rhs) + (size_t)lane * a.N + A, v);
+    }
+    __syncwarp();
+    o0 += nsl;
+  }
+}
+
+// Interleaved form of the gather scheme (the temperature rows, whose
+// blocks are single values: the piece bookkeeping above costs more than it
+// saves there).  Lanes 0..GD-1 take the off-diagonal entries (lane l the
+// l-th, counting past the diagonal slot; a row with more than GD of them
+// takes further passes) and add each entry's whole list, one block per
+// round; lanes GD..31 share the diagonal block and the residual rows, lane
+// GD + i taking the row's elements i, i + ND, ... in ascending order, the ND
+// partial sums then added in lane order.
+template <typename T, int KIND, bool TILED>
+__device__ __forceinline__ void gather_row_il(const AsmArgs& a, const int4 rr, const T* base, int str,
+                                              const uint16_t* n2e_loc, const uint16_t* clist_loc,
+                                              GatherSmem<T, KIND>& w, const unsigned* masks, int lane) {
+  using L = Lay<KIND>;
+  using Q = GatherGeom<T, KIND>;
+  constexpr int NV = Q::NV, NF = Q::NF, NVP = Q::NVP, ND = 8, GD = 32 - ND;
+  T(*pw)[Q::PSTR] = w.part;
   const bool diagl = lane >= GD;
   const int di = lane - GD;   // the diagonal lane's index
   const int A = rr.x, rp = rr.y, ep = rr.z, deg = rr.w & 0xff, sd = (rr.w >> 8) & 0xff, ne = rr.w >> 16;
@@ -1361,17 +1538,19 @@ __device__ __forceinline__ void gather_row(const AsmArgs& a, const int4 rr, cons
 
 template <typename T, int KIND>
 __global__ void __launch_bounds__(128) gather_rows_kernel(const AsmArgs a) {
-  using Q = GatherGeom<T, KIND>;
   __shared__ unsigned masks[24];
-  __shared__ __align__(16) T part[4][Q::ND][Q::PSTR];   // the diagonal lanes' partial sums, per warp
+  __shared__ __align__(16) GatherSmem<T, KIND> gw[4];
   if (threadIdx.x < 24) masks[threadIdx.x] = (KIND == OVS_ASM_TEM) ? (TB | (TB << 8) | (TB << 16)) : mask_of(threadIdx.x);
   __syncthreads();
   const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
   const T* sum = reinterpret_cast<const T*>(a.rec);
   const int W = gridDim.x * 4;
   for (int t = blockIdx.x * 4 + wid; t < a.nrows; t += W)
-    gather_row<T, KIND, false>(a, __ldg(a.row_rec + t), sum, Lay<KIND>::SW, nullptr, nullptr, part[wid], masks,
-                               lane);
+    if constexpr (KIND == OVS_ASM_TEM)
+      gather_row_il<T, KIND, false>(a, __ldg(a.row_rec + t), sum, Lay<KIND>::SW, nullptr, nullptr, gw[wid], masks,
+                                    lane);
+    else
+      gather_row<T, KIND, false>(a, __ldg(a.row_rec + t), sum, Lay<KIND>::SW, nullptr, nullptr, gw[wid], masks, lane);
 }
 
 // ---------------------------------------------------------- tiled row pass
@@ -1404,12 +1583,11 @@ constexpr long TILE_WAIT_LIMIT = 1L << 26;   // bounded mbarrier wait (polls)
 
 template <typename T, int KIND>
 __global__ void __launch_bounds__(128) tiled_rows_kernel(const AsmArgs a, const TileArgs ta) {
-  using Q = GatherGeom<T, KIND>;
   using G = TileStage<T, KIND>;
   extern __shared__ __align__(128) unsigned char tile_smem[];
   __shared__ __align__(8) unsigned long long bar;
   __shared__ unsigned masks[24];
-  __shared__ __align__(16) T part[4][Q::ND][Q::PSTR];
+  __shared__ __align__(16) GatherSmem<T, KIND> gw[4];
   T* stage = reinterpret_cast<T*>(tile_smem);
   const int tile = blockIdx.x;
   const int k0 = __ldg(ta.eptr + tile), nel = __ldg(ta.eptr + tile + 1) - k0;
@@ -1442,9 +1620,13 @@ __global__ void __launch_bounds__(128) tiled_rows_kernel(const AsmArgs a, const 
   }
   const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
   const int r1 = __ldg(ta.rptr + tile + 1);
-  for (int r = __ldg(ta.rptr + tile) + wid; r < r1; r += 4)
-    gather_row<T, KIND, true>(a, __ldg(a.row_rec + __ldg(ta.rows + r)), stage, G::STR, ta.n2e_loc, ta.clist_loc,
-                              part[wid], masks, lane);
+  for (int r = __ldg(ta.rptr + tile) + wid; r < r1; r += 4) {
+    const int4 rr = __ldg(a.row_rec + __ldg(ta.rows + r));
+    if constexpr (KIND == OVS_ASM_TEM)
+      gather_row_il<T, KIND, true>(a, rr, stage, G::STR, ta.n2e_loc, ta.clist_loc, gw[wid], masks, lane);
+    else
+      gather_row<T, KIND, true>(a, rr, stage, G::STR, ta.n2e_loc, ta.clist_loc, gw[wid], masks, lane);
+  }
 }
 
 // ---------------------------------------------------- alpha-stage records

@@ -427,10 +427,10 @@ def test_row_passes_agree(kind, prec, tol):
     """The tiled row pass (default: summaries staged per row tile in shared
     memory), the untiled gather pass (OVS_OPT_ROWS_TILED = 0) and the
     chunked pass (also OVS_OPT_ROWS_GATHER = 0).  Tiled and gather add every
-    entry in the same order (the diagonal blocks and the residual rows in
-    eight interleaved partial sums); the chunked pass adds everything in one
-    ascending sweep.  The systems agree to rounding, normwise per block, and
-    the tiled pass gives the same bits on a second run."""
+    entry in the same order (each entry's list in pieces of consecutive
+    elements, the pieces added in order); the chunked pass adds every entry
+    in one ascending sweep.  The systems agree to rounding, normwise per
+    block, and the tiled pass gives the same bits on a second run."""
     kernel = {"nsvof": F.OVS_ASM_NSVOF, "tem": F.OVS_ASM_TEM, "ns": F.OVS_ASM_NS}[kind]
     sysid = {"nsvof": F.OVS_SYS_NSVOF, "tem": F.OVS_SYS_TEM, "ns": F.OVS_SYS_NS}[kind]
     case = M.random_case(nx=6, ny=5, nz=4, seed=23, kernel=kernel)
@@ -478,8 +478,8 @@ def _fan_case(kernel, m=40, seed=31):
 @pytest.mark.parametrize("kind", ["nsvof", "tem", "ns"])
 @pytest.mark.parametrize("tile_elems", [0, 96, 16])
 def test_assembly_high_degree_rows(oracle, kind, tile_elems):
-    """Rows of degree 42 (two passes of the gather scheme's off-diagonal
-    lanes, a 40-element contribution list) against the oracle, FP64 1e-12,
+    """Rows of degree 42 (two passes of the gather scheme's lanes, a
+    40-element contribution list) against the oracle, FP64 1e-12,
     FP32 1e-5: the default gather pass (0), and the tiled pass with a 96-
     and a 16-element tile budget (with 16 the two 40-element rows take the
     untiled gather pass beside the tiles)."""
