@@ -534,15 +534,17 @@ def run_ours(args, world, rank, local_rank, dist):
                 ctx.assemble(kern, 6, prec)
                 rows_ab[f"{kn}_{nm}_{vn}_ms"] = ctx.profile(F.OVS_PROF_ASSEMBLE_ROWS, kern, prec, 5)
     prof["rows_variants"] = rows_ab
-    # the FP64 element pass with the node records in registers (default)
-    # against shared memory
+    # the FP64 element pass with the node records in registers against
+    # shared memory (the default takes shared memory for NS+VOF, registers
+    # for T)
     elem_ab = {}
-    for sm in (1, 0):           # ends on the library default
+    for sm in (1, 0):
         ctx.set_option(F.OVS_OPT_ELEM_SMEM, sm)
         for kern, kn in ((F.OVS_ASM_NSVOF, "nsvof"), (F.OVS_ASM_TEM, "tem")):
             ctx.assemble(kern, 6, F.OVS_FP64)
             elem_ab[f"{kn}_fp64_{'smem' if sm else 'registers'}_ms"] = \
                 ctx.profile(F.OVS_PROF_ASSEMBLE_ELEMENTS, kern, F.OVS_FP64, 5)
+    ctx.set_option(F.OVS_OPT_ELEM_SMEM, -1)   # back to the library default
     prof["element_variants"] = elem_ab
     ctx.assemble(F.OVS_ASM_NSVOF, 6, F.OVS_FP32)
     ctx.assemble(F.OVS_ASM_NSVOF, 6, F.OVS_FP64)

@@ -110,8 +110,10 @@ enum {
                                   (default) stages each chunk's element summaries in shared memory with
                                   asynchronous copies; 0 (env OVS_ROWS_STAGED=0) reads them from global memory
                                   lane by lane */
-  OVS_OPT_ELEM_SMEM = 4,       /* FP64 tet element pass: 0 (default, the faster one measured) holds the node
-                                  records in registers; 1 (env OVS_ELEM_SMEM=1) in shared memory */
+  OVS_OPT_ELEM_SMEM = 4,       /* FP64 tet element pass: 0 (env OVS_ELEM_SMEM=0) holds the node records in
+                                  registers, 1 (env OVS_ELEM_SMEM=1) in shared memory; -1 (default) shared
+                                  memory for NS+VOF and registers for NS and T, the faster of the two
+                                  measured for each */
   OVS_OPT_ROWS_GATHER = 5,     /* tet row pass without tiles (OVS_OPT_ROWS_TILED = 0): 1 (default) every lane
                                   gathers whole blocks of the row by the contribution lists built with the
                                   pattern, reading the summaries from global memory; 0 (env

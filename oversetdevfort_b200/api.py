@@ -145,7 +145,9 @@ class Context:
         F.check(self.lib.ovs_set_ibc(self.h, _iptr(a), a.shape[1]), "ovs_set_ibc")
 
     def set_option(self, option: int, value: int):
-        """OVS_OPT_HEX_TC / OVS_OPT_ARNOLDI_FUSED for this context."""
+        """A kernel-variant option of this context (OVS_OPT_*: HEX_TC,
+        ARNOLDI_FUSED, ROWS_STAGED, ELEM_SMEM, ROWS_GATHER, ROWS_TILED,
+        TILE_ELEMS); see include/ovs.h for the values."""
         F.check(self.lib.ovs_set_option(self.h, option, int(value)), "ovs_set_option")
 
     def set_faces(self, bf):

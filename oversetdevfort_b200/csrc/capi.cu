@@ -409,7 +409,7 @@ int ovs_set_option(ovs_ctx* c, int option, int value) {
   switch (option) {
     case OVS_OPT_HEX_TC: c->hex_tc = value != 0; return OVS_OK;
     case OVS_OPT_ROWS_STAGED: c->rows_staged = value != 0; return OVS_OK;
-    case OVS_OPT_ELEM_SMEM: c->elem_smem = value != 0; return OVS_OK;
+    case OVS_OPT_ELEM_SMEM: c->elem_smem = value < 0 ? -1 : (value != 0); return OVS_OK;
     case OVS_OPT_ROWS_GATHER: c->rows_gather = value != 0; return OVS_OK;
     case OVS_OPT_ROWS_TILED: c->rows_tiled = value != 0; return OVS_OK;
     case OVS_OPT_TILE_ELEMS:

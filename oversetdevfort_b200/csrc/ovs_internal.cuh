@@ -135,8 +135,10 @@ struct ovs_ctx {
   // tet row pass: element summaries staged through shared memory by
   // asynchronous copies (1, default) or read by every lane from global memory
   int rows_staged = 1;
-  // FP64 element pass: node records in registers (0, measured faster) or shared memory (1)
-  int elem_smem = 0;
+  // FP64 element pass: node records in registers (0) or shared memory (1);
+  // -1 (default): shared memory for NS+VOF, registers for the others, the
+  // faster of the two measured for each
+  int elem_smem = -1;
   // tet row pass: lanes gather whole blocks by the contribution lists (1,
   // default) or the chunked pass reduces element blocks in shared memory (0)
   int rows_gather = 1;
