@@ -122,8 +122,12 @@ enum {
   OVS_OPT_ROWS_TILED = 6,      /* tet row pass: 1 (env OVS_ROWS_TILED=1) one CTA per tile of rows, the tile's
                                   element summaries staged in shared memory by bulk copies, then gathered as
                                   above; 0 (default, the faster one measured) the untiled passes */
-  OVS_OPT_TILE_ELEMS = 7       /* element budget of a row tile (default 96, env OVS_TILE_ELEMS; 4..4000);
+  OVS_OPT_TILE_ELEMS = 7,      /* element budget of a row tile (default 96, env OVS_TILE_ELEMS; 4..4000);
                                   rows with more elements take the untiled gather pass */
+  OVS_OPT_MIXED_OUTER = 8      /* OVS_MIXED solves: m > 0 (default 30, env OVS_MIXED_OUTER; up to 200) a
+                                  flexible GMRES(m) outer in FP64 whose directions are preconditioned by one
+                                  FP32 GMRES cycle each; 0 the restarted refinement (one FP32 cycle on the
+                                  true FP64 residual per step) */
 };
 
 /* boundary-face flags (ovs_set_faces) */

@@ -36,7 +36,7 @@ OVS_VJP_ACG, OVS_VJP_RPHIG, OVS_VJP_RTG, OVS_VJP_COUNT = 9, 12, 13, 14
 OVS_NOALLOC_MAX_N, OVS_NOALLOC_MAX_KSPACE = 16384, 40
 OVS_FACE_WEAK, OVS_FACE_CONVH = 1, 2
 OVS_OPT_HEX_TC, OVS_OPT_ARNOLDI_FUSED, OVS_OPT_ROWS_STAGED, OVS_OPT_ELEM_SMEM = 1, 2, 3, 4
-OVS_OPT_ROWS_GATHER, OVS_OPT_ROWS_TILED, OVS_OPT_TILE_ELEMS = 5, 6, 7
+OVS_OPT_ROWS_GATHER, OVS_OPT_ROWS_TILED, OVS_OPT_TILE_ELEMS, OVS_OPT_MIXED_OUTER = 5, 6, 7, 8
 OVS_SPMV_PRECOND = 1
 (OVS_BLK_K11, OVS_BLK_G, OVS_BLK_D1, OVS_BLK_M, OVS_BLK_LS, OVS_BLK_LSU,
  OVS_BLK_ULS, OVS_BLK_PLS, OVS_BLK_TEM) = range(9)

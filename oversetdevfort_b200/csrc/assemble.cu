@@ -949,10 +949,13 @@ __device__ __forceinline__ void cp_async_wait_all() {
 
 // ---------------------------------------------------------- pass 1 kernel
 // blocks per SM the element pass is compiled for: the FP32 NS+VOF pass at 3
-// (168 registers, measured faster than the unbounded 178), the others as
-// the compiler chooses (tighter bounds spill)
+// (168 registers, measured faster than the unbounded 178 and than 2 or 4),
+// the FP32 temperature pass at 4 (1.25 against 1.45 ms at 160 registers),
+// the others as the compiler chooses (the FP64 temperature pass measured
+// slower at 3)
 template <typename T, int KIND> struct SumMinBlocks { static constexpr int v = 1; };
 template <> struct SumMinBlocks<float, OVS_ASM_NSVOF> { static constexpr int v = 3; };
+template <> struct SumMinBlocks<float, OVS_ASM_TEM> { static constexpr int v = 4; };
 
 template <typename T, int KIND, bool SMEMREC> struct SumBlocks { static constexpr int v = SumMinBlocks<T, KIND>::v; };
 template <int KIND> struct SumBlocks<double, KIND, true> { static constexpr int v = 3; };

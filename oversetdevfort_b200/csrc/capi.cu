@@ -202,6 +202,8 @@ int create_resources(ovs_ctx* c, const ovs_dims* dims) {
     if (es) c->elem_smem = es[0] != '0';
     const char* rg = getenv("OVS_ROWS_GATHER");
     if (rg) c->rows_gather = rg[0] != '0';
+    const char* mo = getenv("OVS_MIXED_OUTER");
+    if (mo && atoi(mo) >= 0 && atoi(mo) <= 200) c->mixed_outer = atoi(mo);
     const char* rt = getenv("OVS_ROWS_TILED");
     if (rt) c->rows_tiled = rt[0] != '0';
     const char* te = getenv("OVS_TILE_ELEMS");
@@ -265,7 +267,7 @@ int ovs_destroy(ovs_ctx* c) {
   if (c->hex_kbuf) cudaFree(c->hex_kbuf);
   if (c->hex_w) cudaFree(c->hex_w);
   void* ptrs[] = {c->ien, c->elm_id, c->ibc, c->rowptr, c->colidx, c->diag, c->n2e_ptr, c->n2e, c->n2s, c->row_order, c->row_rec, c->cptr, c->clist, c->tile_rptr, c->tile_rows,
-                  c->tile_eptr, c->tile_elems, c->n2e_loc, c->clist_loc, c->big_rec, c->tmap, c->vals_t, c->vjp_cot, c->vjp_ge, c->vjp_grad,
+                  c->tile_eptr, c->tile_elems, c->n2e_loc, c->clist_loc, c->big_rec, c->fg_buf, c->tmap, c->vals_t, c->vjp_cot, c->vjp_ge, c->vjp_grad,
                   c->rec[0], c->rec[1], c->esum[0], c->esum[1], c->gm, c->basis[0], c->basis[1], c->work64, c->work32, c->wvec, c->coop_part,
                   c->flags, c->cfl_bits};
   for (void* p : ptrs) if (p) cudaFree(p);
@@ -412,6 +414,10 @@ int ovs_set_option(ovs_ctx* c, int option, int value) {
     case OVS_OPT_ELEM_SMEM: c->elem_smem = value < 0 ? -1 : (value != 0); return OVS_OK;
     case OVS_OPT_ROWS_GATHER: c->rows_gather = value != 0; return OVS_OK;
     case OVS_OPT_ROWS_TILED: c->rows_tiled = value != 0; return OVS_OK;
+    case OVS_OPT_MIXED_OUTER:
+      if (value < 0 || value > 200) return OVS_ERR_ARG;
+      c->mixed_outer = value;
+      return OVS_OK;
     case OVS_OPT_TILE_ELEMS:
       if (value < 4 || value > 4000) return OVS_ERR_ARG;
       c->tile_elems_opt = value;

@@ -22,6 +22,9 @@
 // per batch of iterations.
 #include "ovs_internal.cuh"
 
+#include <algorithm>
+#include <vector>
+
 #include <cooperative_groups.h>
 #include <math.h>
 #include <string.h>
@@ -347,12 +350,18 @@ dot_kernel(const TA* __restrict__ a, const TB* __restrict__ b, size_t n, GmresDe
 template <typename TM, typename TV = double>
 __global__ void __launch_bounds__(OVS_RED_THREADS)
 gm_start_kernel(int N, int nf, int sys, const double* __restrict__ rhs, const TM* __restrict__ pre,
-                TV* __restrict__ v0, double tol, GmresDev* gm) {  // v0: FP64 work vector
+                TV* __restrict__ v0, double tol, GmresDev* gm, int raw) {  // v0: FP64 work vector
   __shared__ double sh[32];
   double s = 0.0;
   for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < (size_t)N;
        i += (size_t)gridDim.x * blockDim.x) {
-    if (sys == OVS_SYS_TEM) {
+    if (raw) {   // rhs is already preconditioned
+      for (int f = 0; f < nf; ++f) {
+        const double z = rhs[(size_t)f * N + i];
+        v0[(size_t)f * N + i] = (TV)z;
+        s += z * z;
+      }
+    } else if (sys == OVS_SYS_TEM) {
       const double z = (double)pre[i] * rhs[i];
       v0[i] = (TV)z;
       s += z * z;
@@ -1050,9 +1059,11 @@ int launch_arnoldi(ovs_ctx* c, int sys, const ArnoldiPlan& pl, const TM* vals, c
 
 // One GMRES cycle on system `sys` with matrix/preconditioner precision TM
 // and basis precision TV.  rhs and sol are FP64 device vectors (nf*N).
+// rhs_pre: rhs is P^-1 times the right-hand side already (the cycle then
+// solves P^-1 A x = rhs)
 template <typename TM, typename TV, bool ACC64 = true>
 int gmres_cycle(ovs_ctx* c, int sys, const double* rhs, double* sol, double tol, int kspace,
-                int kmin, ovs_gmres_info* info) {
+                int kmin, ovs_gmres_info* info, bool rhs_pre = false) {
   const int N = c->N, nf = ovs_sys_nf(sys);
   const size_t n = (size_t)N * nf;
   const int prec = sizeof(TM) == 8 ? OVS_FP64 : OVS_FP32;
@@ -1077,7 +1088,8 @@ int gmres_cycle(ovs_ctx* c, int sys, const double* rhs, double* sol, double tol,
   OVS_CUDA_TRY(cudaMemcpyAsync(&gm->kspace, km, sizeof(km), cudaMemcpyHostToDevice, s));
   OVS_CUDA_TRY(cudaMemsetAsync(gm->H, 0, sizeof(double) * (size_t)(kspace + 1) * kspace, s));
   OVS_CUDA_TRY(cudaMemsetAsync(gm->e, 0, sizeof(double) * (size_t)(kspace + 1), s));
-  gm_start_kernel<TM, double><<<OVS_RED_BLOCKS, OVS_RED_THREADS, 0, s>>>(N, nf, sys, rhs, pre, wd, tol, gm);
+  gm_start_kernel<TM, double><<<OVS_RED_BLOCKS, OVS_RED_THREADS, 0, s>>>(N, nf, sys, rhs, pre, wd, tol, gm,
+                                                                         rhs_pre ? 1 : 0);
   gm_normalize_kernel<TV, double><<<OVS_RED_BLOCKS, OVS_RED_THREADS, 0, s>>>(wd, V, n, gm, 1);
   c->launches += 2;
   OVS_CUDA_TRY(cudaGetLastError());
@@ -1295,6 +1307,145 @@ int ovs_round_impl(ovs_ctx* c, int sys) {
   return OVS_OK;
 }
 
+// y = y + a x and y = a x over n values (y FP64)
+template <typename TX>
+__global__ void axpy64_kernel(double* __restrict__ y, const TX* __restrict__ x, double a, size_t n) {
+  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x)
+    y[i] += a * (double)x[i];
+}
+__global__ void scale64_kernel(double* __restrict__ y, const double* __restrict__ x, double a, size_t n) {
+  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x)
+    y[i] = a * x[i];
+}
+
+// OVS_MIXED with a flexible Krylov outer (FGMRES(m), Saad 1993): the outer
+// iteration runs in FP64 on the FP64 system, and each of its directions is
+// preconditioned by one FP32 GMRES cycle on the FP32 rounding of the matrix
+// (z_j ~ A^-1 v_j), so the corrections of successive inner cycles are
+// combined by a least-squares fit instead of added one after another.  The
+// outer basis V (m + 1 vectors) and the preconditioned directions Z (m) are
+// FP64; the outer Gram-Schmidt is modified Gram-Schmidt with FP64 dots.
+// After m directions, or when the outer residual estimate reaches rtol, x
+// is updated and the true residual b - A x recomputed with the FP64 matrix.
+// x, r, b: FP64 device vectors (r = b - A x on entry); cycles counts inner
+// cycles (max_cycles bounds them), iters inner iterations.
+static int solve_flexible(ovs_ctx* c, int sys, double rtol, int kspace, int max_cycles, int m, double* x,
+                          double* r, const double* b, double bnorm, int& cycles, int& iters, double& rel) {
+  const size_t n = (size_t)c->N * ovs_sys_nf(sys);
+  cudaStream_t s = c->stream;
+  SysStore& S = c->sys[sys][OVS_FP64];
+  const int gr = ovs_grid(n, 256, 8 * c->num_sms);
+  // V (m + 1 FP64 vectors) and Z (m FP32 vectors: a direction rounded to
+  // FP32 before its product is taken is as good a direction, and A z_j is
+  // formed from the rounded z_j), kept by the context between solves
+  const size_t need = sizeof(double) * n * ((size_t)m + 1) + sizeof(float) * n * (size_t)m;
+  if (c->fg_bytes < need) {
+    if (c->fg_buf) cudaFree(c->fg_buf);
+    c->fg_buf = nullptr;
+    c->fg_bytes = 0;
+    if (cudaMalloc(&c->fg_buf, need) != cudaSuccess) {
+      cudaGetLastError();
+      c->fg_buf = nullptr;
+      return OVS_ERR_NOMEM;
+    }
+    c->fg_bytes = need;
+  }
+  double* V = reinterpret_cast<double*>(c->fg_buf);
+  float* Z = reinterpret_cast<float*>(V + n * ((size_t)m + 1));
+  double* zw = r;   // the inner cycle's FP64 correction, in the residual's storage until the update
+  std::vector<double> H((size_t)(m + 1) * m), g(m + 1), cs(m), sn(m), y(m);
+  int st = OVS_OK;
+  if ((st = ovs_precond_setup(c, sys, OVS_FP64))) return st;
+  while (rel > rtol && cycles < max_cycles) {
+    // the outer iteration minimizes the preconditioned residual P^-1 (b - A x)
+    // (the block-Jacobi scaling balances the fields, whose raw residuals
+    // differ by orders of magnitude); v_1 = P^-1 r / |P^-1 r|
+    if ((st = ovs_precond_apply_impl(c, sys, OVS_FP64, r, V))) break;
+    double vv;
+    if ((st = dot64(c, V, V, n, &vv))) break;
+    const double beta = sqrt(vv);
+    if (!(beta > 0.0)) break;
+    scale64_kernel<<<gr, 256, 0, s>>>(V, V, 1.0 / beta, n);
+    ++c->launches;
+    const double target = 0.5 * beta * rtol / rel;   // the reduction the true residual still needs
+    std::fill(H.begin(), H.end(), 0.0);
+    std::fill(g.begin(), g.end(), 0.0);
+    g[0] = beta;
+    int j = 0;
+    bool stop = false;
+    for (; j < m && !stop && cycles < max_cycles; ++j) {
+      double* vj = V + n * (size_t)j;
+      float* zj = Z + n * (size_t)j;
+      double* w = V + n * (size_t)(j + 1);
+      OVS_CUDA_TRY(cudaMemsetAsync(zw, 0, sizeof(double) * n, s));
+      double tin = target / fabs(g[j]);
+      if (tin < 1e-6) tin = 1e-6;
+      if (tin > 0.5) tin = 0.5;
+      ovs_gmres_info gi;
+      if ((st = gmres_cycle<float, float, false>(c, sys, vj, zw, tin, kspace, 1, &gi, true))) break;
+      iters += gi.iterations;
+      ++cycles;
+      convert_kernel<double, float><<<gr, 256, 0, s>>>(zw, zj, n);
+      ++c->launches;
+      if ((st = launch_spmv<double, float, double, 1>(c, sys, as<double>(S.vals), zj, w, as<double>(S.binv),
+                                                        nullptr, nullptr)))
+        break;
+      for (int i = 0; i <= j; ++i) {
+        double h;
+        if ((st = dot64(c, w, V + n * (size_t)i, n, &h))) break;
+        H[(size_t)j * (m + 1) + i] = h;
+        axpy64_kernel<<<gr, 256, 0, s>>>(w, V + n * (size_t)i, -h, n);
+        ++c->launches;
+      }
+      if (st) break;
+      double ww;
+      if ((st = dot64(c, w, w, n, &ww))) break;
+      const double hn = sqrt(ww);
+      H[(size_t)j * (m + 1) + j + 1] = hn;
+      if (hn > 0.0) {
+        scale64_kernel<<<gr, 256, 0, s>>>(w, w, 1.0 / hn, n);
+        ++c->launches;
+      }
+      // Givens rotations of column j
+      double* hc = &H[(size_t)j * (m + 1)];
+      for (int i = 0; i < j; ++i) {
+        const double t = cs[i] * hc[i] + sn[i] * hc[i + 1];
+        hc[i + 1] = -sn[i] * hc[i] + cs[i] * hc[i + 1];
+        hc[i] = t;
+      }
+      const double den = sqrt(hc[j] * hc[j] + hc[j + 1] * hc[j + 1]);
+      if (den == 0.0) { stop = true; break; }   // a zero column: the directions so far span the solution
+      cs[j] = hc[j] / den;
+      sn[j] = hc[j + 1] / den;
+      hc[j] = den;
+      hc[j + 1] = 0.0;
+      g[j + 1] = -sn[j] * g[j];
+      g[j] = cs[j] * g[j];
+      if (!(hn > 0.0) || fabs(g[j + 1]) <= target) stop = true;
+    }
+    if (st) break;
+    // x += Z y with H y = g (upper triangular, j x j)
+    for (int i = j - 1; i >= 0; --i) {
+      double t = g[i];
+      for (int k = i + 1; k < j; ++k) t -= H[(size_t)k * (m + 1) + i] * y[k];
+      y[i] = H[(size_t)i * (m + 1) + i] != 0.0 ? t / H[(size_t)i * (m + 1) + i] : 0.0;
+    }
+    for (int i = 0; i < j; ++i) {
+      axpy64_kernel<<<gr, 256, 0, s>>>(x, Z + n * (size_t)i, y[i], n);
+      ++c->launches;
+    }
+    // (zw, the residual's storage, is rewritten with the true residual next)
+    // the true residual with the FP64 matrix
+    if ((st = launch_spmv<double, double, double, 2>(c, sys, as<double>(S.vals), x, r, nullptr, b, nullptr))) break;
+    double rr;
+    if ((st = dot64(c, r, r, n, &rr))) break;
+    rel = sqrt(rr) / bnorm;
+    if (!(rel == rel) || j == 0) break;
+  }
+  OVS_CUDA_TRY(cudaGetLastError());
+  return st;
+}
+
 // Restarted / iteratively refined solve to a true FP64 relative residual.
 // `outer` is the system whose residual b - A x is driven to rtol (matrix and
 // right-hand side of that precision, FP64 arithmetic), `inner` the matrix
@@ -1335,6 +1486,10 @@ int ovs_solve_impl(ovs_ctx* c, int sys, int mode, double rtol, int kspace, int m
   double rel = bnorm > 0.0 ? 1.0 : 0.0;
   int cycles = 0, iters = 0;
   const double floor_tol = prec == OVS_FP32 ? 1e-6 : 1e-14;
+  if (mode == OVS_MIXED && c->mixed_outer > 0 && rel > rtol) {
+    if ((st = solve_flexible(c, sys, rtol, kspace, max_cycles, c->mixed_outer, x, r, b, bnorm, cycles, iters, rel)))
+      return st;
+  }
   while (rel > rtol && cycles < max_cycles) {
     double tin = rtol / rel;
     if (tin < floor_tol) tin = floor_tol;

@@ -139,6 +139,11 @@ struct ovs_ctx {
   // -1 (default): shared memory for NS+VOF, registers for the others, the
   // faster of the two measured for each
   int elem_smem = -1;
+  // OVS_MIXED: FGMRES(m) outer over FP32 inner cycles (m = mixed_outer > 0,
+  // default 30) or the restarted refinement (0)
+  int mixed_outer = 30;
+  void* fg_buf = nullptr;    // the flexible outer's basis and directions
+  size_t fg_bytes = 0;
   // tet row pass: lanes gather whole blocks by the contribution lists (1,
   // default) or the chunked pass reduces element blocks in shared memory (0)
   int rows_gather = 1;

@@ -158,10 +158,12 @@ def test_partitioned_newton_mixed_fp64_system_on_contexts():
     """The OVS_MIXED loop over three contexts (ContextPartition.round:
     ovs_round_matrix of each part's FP64 matrix as the inner operator,
     refinement against the FP64 parts) against ovs_quench_newton OVS_MIXED
-    on one context: converged, the same Newton iterations within one, the
-    state within 1e-6."""
+    on one context with the same restarted refinement
+    (OVS_OPT_MIXED_OUTER = 0): converged, the same Newton iterations within
+    one, the state within 1e-6."""
     case = _case()
     g = Context.from_case(case)
+    g.set_option(F.OVS_OPT_MIXED_OUTER, 0)
     info = g.quench_newton(mode=F.OVS_MIXED, max_cycles=40, **OPTS)
     ref = {n: g.get_field(n) for n in ("ug", "pg", "phig", "tg")}
     g.close()

@@ -286,18 +286,21 @@ def test_refined_solve_reaches_true_residual(oracle, mode):
 
 
 @pytest.mark.parametrize("sysid,kern,nf", [(F.OVS_SYS_NSVOF, F.OVS_ASM_NSVOF, 5), (F.OVS_SYS_TEM, F.OVS_ASM_TEM, 1)])
-def test_mixed_reaches_fp64_solution(oracle, sysid, kern, nf):
-    """OVS_MIXED solves the FP64 system: its true residual on the FP64
-    system (rechecked with the oracle's SpMV) meets rtol, and every field of
-    its solution is within 1e-5 (relative to the field's largest value) of
-    the restarted FP64 GMRES solution.  Both run to rtol 1e-12: on this box a
-    relative residual of 1e-10 leaves up to 8e-4 of uncertainty in the VOF
-    field of ANY solution (the pressure correction is ~1e7 and dominates the
-    residual norm), so field-by-field agreement is only meaningful when both
-    solves are tight.  The FP32 rounding of the matrix is what the inner
-    cycles used."""
+@pytest.mark.parametrize("outer", [30, 0])
+def test_mixed_reaches_fp64_solution(oracle, sysid, kern, nf, outer):
+    """OVS_MIXED solves the FP64 system, with the flexible FGMRES(30) outer
+    (default) and with the restarted refinement (OVS_OPT_MIXED_OUTER = 0):
+    its true residual on the FP64 system (rechecked with the oracle's SpMV)
+    meets rtol, and every field of its solution is within 1e-5 (relative to
+    the field's largest value) of the restarted FP64 GMRES solution.  Both
+    run to rtol 1e-12: on this box a relative residual of 1e-10 leaves up to
+    8e-4 of uncertainty in the VOF field of ANY solution (the pressure
+    correction is ~1e7 and dominates the residual norm), so field-by-field
+    agreement is only meaningful when both solves are tight.  The FP32
+    rounding of the matrix is what the inner cycles used."""
     case = M.quench_case(M.box_tet(8, 8, 8), "q8")
     ctx = _ctx(case)
+    ctx.set_option(F.OVS_OPT_MIXED_OUTER, outer)
     ctx.assemble(kern, 6, F.OVS_FP64)
     s64, i64 = ctx.solve(sysid, F.OVS_FP64, 1e-12, 50, 600)
     smx, imx = ctx.solve(sysid, F.OVS_MIXED, 1e-12, 50, 600)
