@@ -383,14 +383,19 @@ int ovs_gmres(ovs_ctx* ctx, int system, double tol, int kspace,
 
 /* Solve A x = b to ||b - A x||_2 <= rtol ||b||_2 (true residual, FP64).
  * mode OVS_FP64: restarted FP64 GMRES(kspace) on the FP64 system.
- * mode OVS_MIXED: the FP64 system (needs an FP64 assembly of `system`) by
- *   iterative refinement: the refinement residual r = b - A x is formed with
- *   the FP64 matrix and right-hand side, and each correction is a GMRES cycle
- *   on the FP32 rounding of that matrix (FP32 values, preconditioner, SpMV
- *   and Krylov basis; FP64 Gram-Schmidt dots, Givens rotations and
- *   back-substitution).  The rounding is written into the FP32 matrix of
- *   `system` (overwriting an FP32 assembly) inside the timed solve.  The
- *   solution converges to the FP64 system's, not to an FP32-assembled one.
+ * mode OVS_MIXED: the FP64 system (needs an FP64 assembly of `system`).
+ *   Default (OVS_OPT_MIXED_OUTER = m > 0): a flexible GMRES(m) outer in FP64
+ *   arithmetic on the FP64 matrix, minimizing the block-Jacobi-preconditioned
+ *   residual, each of whose directions is one GMRES(kspace) cycle on the FP32
+ *   rounding of that matrix (FP32 values, preconditioner, SpMV and Krylov
+ *   basis; FP64 Gram-Schmidt dots, Givens rotations and back-substitution);
+ *   after m directions, or when the outer estimate is reached, the true
+ *   residual b - A x is formed with the FP64 matrix and the outer restarts
+ *   from it.  OVS_OPT_MIXED_OUTER = 0: iterative refinement, one FP32 cycle
+ *   on the true FP64 residual per step.  max_cycles bounds the FP32 cycles.
+ *   The rounding is written into the FP32 matrix of `system` (overwriting an
+ *   FP32 assembly) inside the timed solve.  The solution converges to the
+ *   FP64 system's, not to an FP32-assembled one.
  * mode OVS_FP32: the same scheme on the FP32-assembled system alone (matrix
  *   and right-hand side assembled in FP32; the refinement residual in FP64
  *   arithmetic on those FP32 values): it converges to the solution of the
