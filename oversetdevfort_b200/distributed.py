@@ -229,7 +229,7 @@ class DeviceOperator:
 
 
 def gmres_cycle(comm, ops: dict, rhs: dict, tol: float, kspace: int, kspace_min: int = 1, tem: bool = False,
-                orthog: str = "mgs"):
+                orthog: str = "mgs", rhs_pre: bool = False):
     """One GMRES(kspace) cycle from a zero start on the partitions of `comm`
     (SparseGMRES_ns_conv / _up / _tem semantics): `ops[r]` the operator of
     part r, `rhs[r]` its right-hand side (nf, N_local) with the owned rows
@@ -237,7 +237,9 @@ def gmres_cycle(comm, ops: dict, rhs: dict, tol: float, kspace: int, kspace_min:
     sum per dot, k + 1 at step k); "cgs2" orthogonalizes with classical
     Gram-Schmidt twice (two vector sums and one norm per step, whatever k),
     for ranks where the latency of a collective outweighs its size.
-    Returns (solution per part with ghosts filled, info dict)."""
+    rhs_pre: rhs is already P^-1 times the right-hand side (the cycle then
+    solves P^-1 A x = rhs).  Returns (solution per part with ghosts filled,
+    info dict)."""
     if orthog not in ("mgs", "cgs2"):
         raise ValueError("orthog must be 'mgs' or 'cgs2'")
     import torch
@@ -255,7 +257,10 @@ def gmres_cycle(comm, ops: dict, rhs: dict, tol: float, kspace: int, kspace_min:
         return sol, info
     U = [{r: torch.empty_like(rhs[r]) for r in P}]
     for r in P:
-        ops[r].precond(rhs[r], U[0][r])
+        if rhs_pre:
+            U[0][r].copy_(rhs[r])
+        else:
+            ops[r].precond(rhs[r], U[0][r])
     unorm = math.sqrt(gdot(U[0], U[0]))
     info["res0"] = unorm
     epsnrm = tol * unorm
@@ -380,6 +385,103 @@ def solve_refined(comm, inner: dict, outer: dict, rhs: dict, rtol: float, kspace
     return x, {"cycles": cycles, "iterations": iters, "converged": bool(rel <= rtol), "rel_residual": rel}
 
 
+def solve_flexible(comm, inner: dict, outer: dict, rhs: dict, rtol: float, kspace: int = 50,
+                   max_cycles: int = 100, m: int = 30, tem: bool = False, orthog: str = "mgs",
+                   floor_tol: float = 1e-6):
+    """A x = b to a true relative residual ||b - A x||_2 <= rtol ||b||_2 over
+    the partitions: `ovs_solve`'s OVS_MIXED flexible outer on distributed
+    vectors.  FGMRES(m) in FP64 on the `outer` operators (P^-1 A and P^-1 of
+    the FP64 system) minimizes the preconditioned residual; each direction
+    z_j is one GMRES cycle on the `inner` operators (the FP32 system) with
+    the right-hand side v_j taken as preconditioned, rounded to FP32 before
+    P^-1 A z_j is formed.  After m directions, or when the outer estimate
+    reaches the reduction still needed, x is updated and r = b - A x formed
+    with the outer operators' plain product (`apply`) after a halo update of
+    x.  Dots are global sums over owned rows.  Returns (x per part with
+    ghosts filled, info: cycles (inner cycles), iterations, converged,
+    rel_residual)."""
+    import torch
+    P = comm.parts()
+    pl = comm.plan
+    ow = {r: torch.as_tensor(pl.owned[r], dtype=torch.long, device=rhs[r].device) for r in P}
+
+    def gdot(a, b):
+        return comm.allreduce([float((a[r][:, ow[r]] * b[r][:, ow[r]]).sum()) for r in P])
+
+    x = {r: torch.zeros_like(rhs[r]) for r in P}
+    res = {r: rhs[r].clone() for r in P}
+    bnorm = math.sqrt(gdot(rhs, rhs))
+    rel = 1.0 if bnorm > 0.0 else 0.0
+    cycles = iters = 0
+    while rel > rtol and cycles < max_cycles:
+        v0 = {r: torch.empty_like(rhs[r]) for r in P}
+        for r in P:
+            outer[r].precond(res[r], v0[r])
+        beta = math.sqrt(gdot(v0, v0))
+        if not beta > 0.0:
+            break
+        V = [{r: v0[r] / beta for r in P}]
+        Z = []
+        target = 0.5 * beta * rtol / rel
+        H = np.zeros((m + 1, m))
+        g = np.zeros(m + 1)
+        cs, sn = np.zeros(m), np.zeros(m)
+        g[0] = beta
+        j = 0
+        while j < m and cycles < max_cycles:
+            tin = min(max(target / abs(g[j]), floor_tol), 0.5)
+            z, info = gmres_cycle(comm, inner, V[j], tin, kspace, 1, tem=tem, orthog=orthog, rhs_pre=True)
+            iters += info["iterations"]
+            cycles += 1
+            z = {r: z[r].float().double() for r in P}   # the stored direction, FP32
+            w = {r: torch.empty_like(rhs[r]) for r in P}
+            for r in P:
+                outer[r].matvec(z[r], w[r])
+            for i in range(j + 1):
+                h = gdot(w, V[i])
+                H[i, j] = h
+                for r in P:
+                    w[r] = w[r] - h * V[i][r]
+            hn = math.sqrt(gdot(w, w))
+            H[j + 1, j] = hn
+            if hn > 0.0:
+                for r in P:
+                    w[r] = w[r] / hn
+            V.append(w)
+            Z.append(z)
+            for i in range(j):
+                t = cs[i] * H[i, j] + sn[i] * H[i + 1, j]
+                H[i + 1, j] = -sn[i] * H[i, j] + cs[i] * H[i + 1, j]
+                H[i, j] = t
+            den = math.hypot(H[j, j], H[j + 1, j])
+            if den == 0.0:   # a zero column: the directions so far span the solution
+                Z.pop()
+                break
+            cs[j], sn[j] = H[j, j] / den, H[j + 1, j] / den
+            H[j, j], H[j + 1, j] = den, 0.0
+            g[j + 1] = -sn[j] * g[j]
+            g[j] = cs[j] * g[j]
+            j += 1
+            if not hn > 0.0 or abs(g[j]) <= target:
+                break
+        k = len(Z)
+        y = np.zeros(k)
+        for i in range(k - 1, -1, -1):
+            y[i] = (g[i] - H[i, i + 1:k] @ y[i + 1:k]) / H[i, i] if H[i, i] != 0.0 else 0.0
+        for i in range(k):
+            for r in P:
+                x[r] = x[r] + float(y[i]) * Z[i][r]
+        comm.halo(x)
+        for r in P:
+            ax = torch.empty_like(x[r])
+            outer[r].apply(x[r], ax)
+            res[r] = rhs[r] - ax
+        rel = math.sqrt(gdot(res, res)) / bnorm
+        if rel != rel or k == 0:
+            break
+    return x, {"cycles": cycles, "iterations": iters, "converged": bool(rel <= rtol), "rel_residual": rel}
+
+
 # assembleQuenching field flags (commonpars, src/modules.f90:218-222)
 FIELD_NS, FIELD_VOF, FIELD_TEM = 1, 2, 4
 _KIND_SYS = {"nsvof": F.OVS_SYS_NSVOF, "tem": F.OVS_SYS_TEM}
@@ -442,7 +544,7 @@ class ContextPartition:
 def quench_newton(comm, parts: dict, newton_max: int = 3, solve_tem: bool = True, kspace: int = 50,
                   kspace_min: int = 1, tol_ns: float = 1e-6, tol_tem: float = 1e-6, utol=(1e-3,) * 4,
                   atol=(1e-15,) * 4, orthog: str = "mgs", bcs: bool = False, mode: int = F.OVS_FP64,
-                  max_cycles: int = 100) -> dict:
+                  max_cycles: int = 100, mixed_outer: int = 30) -> dict:
     """The Newton loop of one quench time step over owner-computes partitions:
     solmultiphasethermofluid_stag (src/solveFlow.f90:4-164) as the reference
     runs it on several ranks.  `parts[r]` is part r's local system
@@ -471,10 +573,12 @@ def quench_newton(comm, parts: dict, newton_max: int = 3, solve_tem: bool = True
     by `solve_refined` on the FP32 operators to the relative residual tol_ns
     / tol_tem (max_cycles refinement cycles) instead of one FP64 cycle.
     mode OVS_MIXED is its OVS_MIXED mode: FP64 assembly and residuals, and
-    each solve by `solve_refined` with the FP64 operators outside and, inside,
-    the FP32 rounding of each part's FP64 matrix (the parts' `round`).  The
-    parts then take a precision argument in assemble, residual_sq, rhs and
-    operator, and their operators provide `apply`."""
+    each solve with the FP64 operators outside and, inside, the FP32
+    rounding of each part's FP64 matrix (the parts' `round`): by
+    `solve_flexible` with an FGMRES(mixed_outer) outer (the default, as
+    OVS_OPT_MIXED_OUTER = 30), or by `solve_refined` with mixed_outer = 0.
+    The parts then take a precision argument in assemble, residual_sq, rhs
+    and operator, and their operators provide `apply`."""
     P = comm.parts()
     mixed = mode in (F.OVS_FP32, F.OVS_MIXED)
     prec = F.OVS_FP32 if mode == F.OVS_FP32 else F.OVS_FP64
@@ -495,8 +599,12 @@ def quench_newton(comm, parts: dict, newton_max: int = 3, solve_tem: bool = True
             for r in P:
                 parts[r].round(kind)
             inner = {r: parts[r].operator(kind, precision=F.OVS_FP32) for r in P}
-            sol, info = solve_refined(comm, inner, ops, rhs, tol, kspace, max_cycles, tem=kind == "tem",
-                                      orthog=orthog)
+            if mixed_outer > 0:
+                sol, info = solve_flexible(comm, inner, ops, rhs, tol, kspace, max_cycles, mixed_outer,
+                                           tem=kind == "tem", orthog=orthog)
+            else:
+                sol, info = solve_refined(comm, inner, ops, rhs, tol, kspace, max_cycles, tem=kind == "tem",
+                                          orthog=orthog)
         elif mixed:
             sol, info = solve_refined(comm, ops, ops, rhs, tol, kspace, max_cycles, tem=kind == "tem", orthog=orthog)
         else:

@@ -154,16 +154,17 @@ def test_partitioned_newton_mixed_on_contexts():
         c.close()
 
 
-def test_partitioned_newton_mixed_fp64_system_on_contexts():
+@pytest.mark.parametrize("outer", [30, 0])
+def test_partitioned_newton_mixed_fp64_system_on_contexts(outer):
     """The OVS_MIXED loop over three contexts (ContextPartition.round:
-    ovs_round_matrix of each part's FP64 matrix as the inner operator,
-    refinement against the FP64 parts) against ovs_quench_newton OVS_MIXED
-    on one context with the same restarted refinement
-    (OVS_OPT_MIXED_OUTER = 0): converged, the same Newton iterations within
-    one, the state within 1e-6."""
+    ovs_round_matrix of each part's FP64 matrix as the inner operator, the
+    FP64 parts outside) against ovs_quench_newton OVS_MIXED on one context,
+    both with the flexible outer (30) and both with the restarted refinement
+    (0): converged, the same Newton iterations within one, the state within
+    1e-6."""
     case = _case()
     g = Context.from_case(case)
-    g.set_option(F.OVS_OPT_MIXED_OUTER, 0)
+    g.set_option(F.OVS_OPT_MIXED_OUTER, outer)
     info = g.quench_newton(mode=F.OVS_MIXED, max_cycles=40, **OPTS)
     ref = {n: g.get_field(n) for n in ("ug", "pg", "phig", "tg")}
     g.close()
@@ -171,7 +172,7 @@ def test_partitioned_newton_mixed_fp64_system_on_contexts():
     plan = D.halo_plan(parts)
     ctxs = [Context.from_case(P.local_case(case, p)) for p in parts]
     sp = {r: D.ContextPartition(c, plan.owned[r], device="cuda:0") for r, c in enumerate(ctxs)}
-    out = D.quench_newton(D.LocalComm(plan), sp, mode=F.OVS_MIXED, max_cycles=40, **OPTS)
+    out = D.quench_newton(D.LocalComm(plan), sp, mode=F.OVS_MIXED, max_cycles=40, mixed_outer=outer, **OPTS)
     assert out["converged"] and abs(out["iterations"] - info.iterations) <= 1
     for n, a in ref.items():
         for c, p in zip(ctxs, parts):
