@@ -58,7 +58,10 @@ enum { OVS_FP64 = 0, OVS_FP32 = 1, OVS_MIXED = 2 };
 enum {
   OVS_ASM_NS = 1,     /* IntElmAss_NS_overset, src/assembleNavSto.f90:76-336 */
   OVS_ASM_NSVOF = 2,  /* IntElmAss_NSVOF_Quenching_STAB, src/solveQuenching.f90:122-573 */
-  OVS_ASM_TEM = 3     /* IntElmAss_Tem_Quenching_STAB, src/solveQuenching.f90:579-882 */
+  OVS_ASM_TEM = 3,    /* IntElmAss_Tem_Quenching_STAB, src/solveQuenching.f90:579-882 */
+  OVS_ASM_QUENCH = 4  /* both quench passes, NS+VOF then T: assembleQuenching with ASSEMBLE_FIELD_NS, _VOF
+                         and _TEM (src/solveQuenching.f90:4-117), one status (cfl: the larger of the two
+                         passes', which evaluate the same advection speed) */
 };
 
 /* linear systems (dofs per node) */
@@ -301,10 +304,11 @@ int ovs_get_field(ovs_ctx* ctx, int field, double* host);
 
 /* Assembly.  Replaces assembleNavSto (kernel OVS_ASM_NS,
  * src/assembleNavSto.f90:4-72) and assembleQuenching with
- * ASSEMBLE_FIELD_NS+VOF (OVS_ASM_NSVOF) or ASSEMBLE_FIELD_TEM (OVS_ASM_TEM)
- * (src/solveQuenching.f90:4-117): alpha-stage blend, zeroing, element loop,
- * element Dirichlet BCs and the scatter into CSR/RHS, in `precision`.
- * cfl (may be NULL) receives the largest element CFL number. */
+ * ASSEMBLE_FIELD_NS+VOF (OVS_ASM_NSVOF), ASSEMBLE_FIELD_TEM (OVS_ASM_TEM) or
+ * all three (OVS_ASM_QUENCH) (src/solveQuenching.f90:4-117): alpha-stage
+ * blend, zeroing, element loop, element Dirichlet BCs and the scatter into
+ * CSR/RHS, in `precision`.  cfl (may be NULL) receives the largest element
+ * CFL number. */
 int ovs_assemble(ovs_ctx* ctx, int kernel, int tensor_flag, int precision,
                  double* cfl);
 /* ovs_assemble without the wait: the pass is queued on the context stream

@@ -25,7 +25,7 @@ OVS_ERR_NODEVICE = -7
 OVS_ERR_TIMEOUT = -8
 
 OVS_FP64, OVS_FP32, OVS_MIXED = 0, 1, 2
-OVS_ASM_NS, OVS_ASM_NSVOF, OVS_ASM_TEM = 1, 2, 3
+OVS_ASM_NS, OVS_ASM_NSVOF, OVS_ASM_TEM, OVS_ASM_QUENCH = 1, 2, 3, 4
 OVS_SYS_NS, OVS_SYS_NSVOF, OVS_SYS_TEM = 1, 2, 3
 OVS_TENSOR_VEC, OVS_TENSOR_MAT = 2, 4
 OVS_PROF_SPMV, OVS_PROF_ASSEMBLE, OVS_PROF_ARNOLDI, OVS_PROF_ARNOLDI_FUSED = 1, 2, 3, 4

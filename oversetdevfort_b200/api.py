@@ -476,8 +476,12 @@ def assembleNavSto(ctx: Context, assemble_tensor_flag: int, precision: int = F.O
 def assembleQuenching(ctx: Context, assemble_tensor_flag: int, assemble_field_flag: int,
                       precision: int = F.OVS_FP64) -> float:
     """src/solveQuenching.f90:4-117: NS+VOF when NS or VOF is flagged, then
-    the temperature pass when TEM is flagged."""
+    the temperature pass when TEM is flagged (both flagged: one
+    OVS_ASM_QUENCH call; its CFL number is the larger of the two passes',
+    which evaluate the same advection speed)."""
     cfl = 0.0
+    if assemble_field_flag & ASSEMBLE_FIELD_TEM and assemble_field_flag & (ASSEMBLE_FIELD_NS | ASSEMBLE_FIELD_VOF):
+        return ctx.assemble(F.OVS_ASM_QUENCH, assemble_tensor_flag, precision)
     if assemble_field_flag & (ASSEMBLE_FIELD_NS | ASSEMBLE_FIELD_VOF):
         cfl = ctx.assemble(F.OVS_ASM_NSVOF, assemble_tensor_flag, precision)
     if assemble_field_flag & ASSEMBLE_FIELD_TEM:

@@ -2119,44 +2119,10 @@ int ovs_profile_assemble(ovs_ctx* c, int kernel, int prec, int reps, double* ms,
   return OVS_OK;
 }
 
-int ovs_assemble_impl(ovs_ctx* c, int kernel, int tensor_flag, int prec, double* cfl) {
-  if (!c->have_pattern || !c->have_params) return OVS_ERR_STATE;
-  if (c->nshl != 4 && c->nshl != 8) return OVS_ERR_ARG;
-  if (c->nshl == 8 && kernel == OVS_ASM_NS) return OVS_ERR_ARG;
-  if (kernel != OVS_ASM_NS && kernel != OVS_ASM_NSVOF && kernel != OVS_ASM_TEM) return OVS_ERR_ARG;
-  if (prec != OVS_FP64 && prec != OVS_FP32) return OVS_ERR_ARG;
-  const int sys = kernel == OVS_ASM_NS ? OVS_SYS_NS : (kernel == OVS_ASM_NSVOF ? OVS_SYS_NSVOF : OVS_SYS_TEM);
-  const size_t ts = prec == OVS_FP64 ? 8 : 4;
-  const int nv = ovs_sys_nv(sys), nf = ovs_sys_nf(sys);
-  SysStore& S = c->sys[sys][prec];
-  int st;
-  if ((st = ovs_ensure(&S.vals, ts * (size_t)c->nnz * nv))) return st;
-  if ((st = ovs_ensure(&S.rhs, ts * (size_t)c->N * nf))) return st;
-  if ((st = ovs_ensure(&c->rec[prec], ts * (size_t)c->N * REC))) return st;
-  const size_t sw = c->nshl == 8 ? (size_t)HexLay<OVS_ASM_NSVOF>::SW : (size_t)Lay<OVS_ASM_NSVOF>::SW;
-  if ((st = ovs_ensure(&c->esum[prec], ts * (size_t)c->E * sw))) return st;
+// the assembly status of the pass (flags and CFL number) to the host, or to
+// the page-locked slots of ovs_assemble_async
+static int finish_status(ovs_ctx* c, double* cfl) {
   cudaStream_t s = c->stream;
-  OVS_CUDA_TRY(cudaMemsetAsync(c->flags, 0, sizeof(int) * 4, s));
-  OVS_CUDA_TRY(cudaMemsetAsync(c->cfl_bits, 0, sizeof(unsigned long long), s));
-  AlphaArgs aa;
-  for (int f = 0; f < OVS_F_COUNT; ++f) aa.f[f] = c->field[f];
-  aa.xg = c->field[OVS_F_XG];
-  aa.rec = c->rec[prec];
-  aa.N = c->N;
-  aa.tem = kernel == OVS_ASM_TEM;
-  aa.almi = c->params.almi;
-  aa.alfi = c->params.alfi;
-  if (prec == OVS_FP64) alpha_records_kernel<double><<<ovs_grid(c->N, 256, 1 << 30), 256, 0, s>>>(aa);
-  else alpha_records_kernel<float><<<ovs_grid(c->N, 256, 1 << 30), 256, 0, s>>>(aa);
-  ++c->launches;
-  OVS_CUDA_TRY(cudaGetLastError());
-  AsmArgs a;
-  SumArgs sa;
-  fill_args(c, prec, S, tensor_flag, a, sa);
-  if ((st = dispatch_assemble(c, kernel, prec, a, sa))) return st;
-  if ((st = ovs_faces_assemble(c, kernel, prec, a.mat, a.vec))) return st;
-  if (a.mat) S.have_mat = true;
-  if (a.vec) S.have_rhs = true;
   if (c->defer_status) {   // ovs_assemble_async: the status travels to a page-locked slot, read at the wait
     const int k = c->async_n++;
     OVS_CUDA_TRY(cudaMemcpyAsync(c->h_async_flags + 4 * k, c->flags, sizeof(int) * 4, cudaMemcpyDeviceToHost, s));
@@ -2179,6 +2145,69 @@ int ovs_assemble_impl(ovs_ctx* c, int kernel, int tensor_flag, int prec, double*
   if (hflags[1]) return OVS_ERR_NONFINITE;
   if (hflags[0]) return OVS_WARN_NEG_DETJ;
   return OVS_OK;
+}
+
+// alpha-stage records of a pass (the record layout of the NS+VOF or the
+// temperature routine)
+static int alpha_stage(ovs_ctx* c, int prec, bool tem) {
+  AlphaArgs aa;
+  for (int f = 0; f < OVS_F_COUNT; ++f) aa.f[f] = c->field[f];
+  aa.xg = c->field[OVS_F_XG];
+  aa.rec = c->rec[prec];
+  aa.N = c->N;
+  aa.tem = tem;
+  aa.almi = c->params.almi;
+  aa.alfi = c->params.alfi;
+  if (prec == OVS_FP64) alpha_records_kernel<double><<<ovs_grid(c->N, 256, 1 << 30), 256, 0, c->stream>>>(aa);
+  else alpha_records_kernel<float><<<ovs_grid(c->N, 256, 1 << 30), 256, 0, c->stream>>>(aa);
+  ++c->launches;
+  OVS_CUDA_TRY(cudaGetLastError());
+  return OVS_OK;
+}
+
+// one pass of `kernel` (alpha stage, element pass, row pass, faces) with its
+// flags and CFL number accumulated on the device (cleared by the caller)
+static int assemble_pass(ovs_ctx* c, int kernel, int tensor_flag, int prec) {
+  const int sys = kernel == OVS_ASM_NS ? OVS_SYS_NS : (kernel == OVS_ASM_NSVOF ? OVS_SYS_NSVOF : OVS_SYS_TEM);
+  const size_t ts = prec == OVS_FP64 ? 8 : 4;
+  SysStore& S = c->sys[sys][prec];
+  int st;
+  if ((st = ovs_ensure(&S.vals, ts * (size_t)c->nnz * ovs_sys_nv(sys)))) return st;
+  if ((st = ovs_ensure(&S.rhs, ts * (size_t)c->N * ovs_sys_nf(sys)))) return st;
+  if ((st = ovs_ensure(&c->rec[prec], ts * (size_t)c->N * REC))) return st;
+  const size_t sw = c->nshl == 8 ? (size_t)HexLay<OVS_ASM_NSVOF>::SW : (size_t)Lay<OVS_ASM_NSVOF>::SW;
+  if ((st = ovs_ensure(&c->esum[prec], ts * (size_t)c->E * sw))) return st;
+  if ((st = alpha_stage(c, prec, kernel == OVS_ASM_TEM))) return st;
+  AsmArgs a;
+  SumArgs sa;
+  fill_args(c, prec, S, tensor_flag, a, sa);
+  if ((st = dispatch_assemble(c, kernel, prec, a, sa))) return st;
+  if ((st = ovs_faces_assemble(c, kernel, prec, a.mat, a.vec))) return st;
+  if (a.mat) S.have_mat = true;
+  if (a.vec) S.have_rhs = true;
+  return OVS_OK;
+}
+
+int ovs_assemble_impl(ovs_ctx* c, int kernel, int tensor_flag, int prec, double* cfl) {
+  if (!c->have_pattern || !c->have_params) return OVS_ERR_STATE;
+  if (c->nshl != 4 && c->nshl != 8) return OVS_ERR_ARG;
+  if (kernel == OVS_ASM_QUENCH) {   // the NS+VOF pass, then the temperature pass; one status
+    if (prec != OVS_FP64 && prec != OVS_FP32) return OVS_ERR_ARG;
+    int st;
+    OVS_CUDA_TRY(cudaMemsetAsync(c->flags, 0, sizeof(int) * 4, c->stream));
+    OVS_CUDA_TRY(cudaMemsetAsync(c->cfl_bits, 0, sizeof(unsigned long long), c->stream));
+    if ((st = assemble_pass(c, OVS_ASM_NSVOF, tensor_flag, prec))) return st;
+    if ((st = assemble_pass(c, OVS_ASM_TEM, tensor_flag, prec))) return st;
+    return finish_status(c, cfl);
+  }
+  if (c->nshl == 8 && kernel == OVS_ASM_NS) return OVS_ERR_ARG;
+  if (kernel != OVS_ASM_NS && kernel != OVS_ASM_NSVOF && kernel != OVS_ASM_TEM) return OVS_ERR_ARG;
+  if (prec != OVS_FP64 && prec != OVS_FP32) return OVS_ERR_ARG;
+  int st;
+  OVS_CUDA_TRY(cudaMemsetAsync(c->flags, 0, sizeof(int) * 4, c->stream));
+  OVS_CUDA_TRY(cudaMemsetAsync(c->cfl_bits, 0, sizeof(unsigned long long), c->stream));
+  if ((st = assemble_pass(c, kernel, tensor_flag, prec))) return st;
+  return finish_status(c, cfl);
 }
 
 int ovs_residual_vjp_impl(ovs_ctx* c, int kernel, const double* cot_host, double* grad_host) {

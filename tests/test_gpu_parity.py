@@ -451,6 +451,42 @@ def test_row_passes_agree(kind, prec, tol):
         np.testing.assert_array_equal(out[0][k], out[3][k], err_msg=k)
 
 
+@pytest.mark.parametrize("prec", [F.OVS_FP64, F.OVS_FP32])
+@pytest.mark.parametrize("seed", [24, 25])
+def test_quench_assembly_call_matches_two_passes(oracle, prec, seed):
+    """OVS_ASM_QUENCH (assembleQuenching with NS, VOF and TEM flagged: the
+    NS+VOF pass then the temperature pass under one status) against the two
+    passes called apart: the same systems and CFL number, bit for bit on a
+    second run, and the FP64 systems within 1e-12 of the oracle's."""
+    case = M.random_case(nx=6, ny=5, nz=4, seed=seed, kernel=F.OVS_ASM_NSVOF)
+    runs = []
+    for fused in (True, False, True):
+        ctx = _ctx(case)
+        if fused:
+            cfl = ctx.assemble(F.OVS_ASM_QUENCH, 6, prec)
+        else:
+            cfl = ctx.assemble(F.OVS_ASM_NSVOF, 6, prec)
+            ctx.assemble(F.OVS_ASM_TEM, 6, prec)
+        runs.append((cfl, ctx.get_system(F.OVS_SYS_NSVOF, prec), ctx.get_system(F.OVS_SYS_TEM, prec)))
+        ctx.close()
+    (c0, n0, t0), (c1, n1, t1), (c2, n2, t2) = runs
+    assert c0 == c1 == c2
+    for k in n0:
+        np.testing.assert_array_equal(n0[k], n1[k], err_msg="nsvof." + k)
+        np.testing.assert_array_equal(n0[k], n2[k], err_msg="nsvof." + k)
+    for k in t0:
+        np.testing.assert_array_equal(t0[k], t1[k], err_msg="tem." + k)
+        np.testing.assert_array_equal(t0[k], t2[k], err_msg="tem." + k)
+    if prec == F.OVS_FP64:
+        oc = oracle.OracleCase(case)
+        oc.assemble_quenching(6, 7)
+        ctx = _ctx(case)
+        ctx.assemble(F.OVS_ASM_QUENCH, 6, prec)
+        _compare_system(oc, ctx, F.OVS_SYS_NSVOF, "nsvof", 6, prec, 1e-12)
+        _compare_system(oc, ctx, F.OVS_SYS_TEM, "tem", 6, prec, 1e-12)
+        ctx.close()
+
+
 def _fan_case(kernel, m=40, seed=31):
     """A fan of m tets around the axis from node 0 to node 1 (ring nodes 2..):
     the two axis rows have degree m + 2 and m elements, more off-diagonal
