@@ -370,7 +370,8 @@ int ovs_precond_device(ovs_ctx* ctx, int system, int precision,
  *   last commit); OVS_ERR_STATE when nothing is staged.
  * ovs_get_rhs_async: the right-hand side of `system` as FP64 into `host`
  *   through a download stream, after the work issued so far; `host` is valid
- *   after ovs_sync_copies.
+ *   after ovs_sync_copies.  Each system has its own read-back buffer: a
+ *   read-back waits only for the previous read-back of the same system.
  * ovs_sync_copies: waits for both copy streams. */
 int ovs_stage_fields(ovs_ctx* ctx, int nfields, const int* ids, const double* const* host);
 int ovs_commit_staged(ovs_ctx* ctx);

@@ -286,7 +286,14 @@ template <> struct Lay<OVS_ASM_TEM> {
   static constexpr int SW = 20, RHS0 = 16, NF = 1, NV = 1;
 };
 
-// 4 values to 16-byte aligned memory (vector stores for the summaries)
+// 4 values of an element summary (global memory; 16-byte aligned in FP32,
+// 32-byte aligned in FP64, where every 4-value group of a summary sits on
+// a 32-byte boundary) with one vector store.  FP64 uses the 256-bit global
+// store of sm_100: one instruction instead of two 128-bit stores, measured
+// 5.9 against 7.1 ms for the FP64 NS+VOF element pass at 128^3 (the pass
+// writes 31 such groups per tet).  The asm carries no memory clobber: the
+// element pass never reads a summary it writes, and the row pass that
+// reads it is a later launch
 template <typename T>
 __device__ __forceinline__ void put4(T* d, T a, T b, T c, T e) {
   d[0] = a; d[1] = b; d[2] = c; d[3] = e;
@@ -295,8 +302,7 @@ __device__ __forceinline__ void put4(float* d, float a, float b, float c, float 
   *reinterpret_cast<float4*>(d) = make_float4(a, b, c, e);
 }
 __device__ __forceinline__ void put4(double* d, double a, double b, double c, double e) {
-  reinterpret_cast<double2*>(d)[0] = make_double2(a, b);
-  reinterpret_cast<double2*>(d)[1] = make_double2(c, e);
+  asm volatile("st.global.v4.f64 [%0], {%1, %2, %3, %4};" ::"l"(d), "d"(a), "d"(b), "d"(c), "d"(e));
 }
 
 // The Gauss-point sums of the NS / NS+VOF block formulas (expand_block)
@@ -1010,7 +1016,15 @@ element_summary_kernel(const SumArgs a) {
       if constexpr (KIND == OVS_ASM_TEM) {
         T o[L::SW];
         run(r, lo, o);
-        store_row<L::SW>(reinterpret_cast<T*>(a.sum) + (size_t)e * L::SW, o);
+        // 20 values per tet: 5 groups of 4 (256-bit stores in FP64, the
+        // summary 32-byte aligned; 2.45 against 2.52 ms at 128^3)
+        T* dst = reinterpret_cast<T*>(a.sum) + (size_t)e * L::SW;
+        if constexpr (sizeof(T) == 8) {
+#pragma unroll
+          for (int k = 0; k < L::SW; k += 4) put4(dst + k, o[k], o[k + 1], o[k + 2], o[k + 3]);
+        } else {
+          store_row<L::SW>(dst, o);
+        }
       } else {
         // NS / NS+VOF write their summary with vector stores as its parts
         // are formed

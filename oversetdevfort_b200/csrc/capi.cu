@@ -526,7 +526,7 @@ int ovs_get_rhs(ovs_ctx* c, int sys, int prec, double* rhs) {
     // through the context's FP64 read-back buffer of this system (no
     // allocation per call), after any asynchronous read-back still using it
     if ((st = ovs_ensure((void**)&c->rhs_out[sys], sizeof(double) * n))) return st;
-    if (c->ev_rhs_out) OVS_CUDA_TRY(cudaStreamWaitEvent(c->stream, c->ev_rhs_out, 0));
+    if (c->ev_rhs_out[sys]) OVS_CUDA_TRY(cudaStreamWaitEvent(c->stream, c->ev_rhs_out[sys], 0));
     double* tmp = c->rhs_out[sys];
     copy_convert_kernel<float, double><<<ovs_grid(n, 256, 1 << 30), 256, 0, c->stream>>>((const float*)S.rhs, tmp, n);
     ++c->launches;

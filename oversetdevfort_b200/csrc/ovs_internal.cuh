@@ -128,8 +128,8 @@ struct ovs_ctx {
   unsigned staged_mask = 0;
   double* rhs_out[4] = {};                // FP64 read-back buffer per system
   cudaStream_t up_stream = nullptr, up_stream2 = nullptr, down_stream = nullptr;
-  cudaEvent_t ev_staged = nullptr, ev_staged2 = nullptr, ev_commit = nullptr, ev_rhs_ready = nullptr,
-              ev_rhs_out = nullptr;
+  cudaEvent_t ev_staged = nullptr, ev_staged2 = nullptr, ev_commit = nullptr, ev_rhs_ready = nullptr;
+  cudaEvent_t ev_rhs_out[4] = {};         // the last read-back of rhs_out[sys] done
   // hex tensor-core pass (FP32 NS+VOF): off unless OVS_HEX_TC=1 or OVS_OPT_HEX_TC
   int hex_tc = 0;
   // tet row pass: element summaries staged through shared memory by

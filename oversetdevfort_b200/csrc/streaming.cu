@@ -27,10 +27,10 @@ int ensure_copy_streams(ovs_ctx* c) {
     OVS_CUDA_TRY(cudaEventCreateWithFlags(&c->ev_staged, cudaEventDisableTiming));
     OVS_CUDA_TRY(cudaEventCreateWithFlags(&c->ev_commit, cudaEventDisableTiming));
     OVS_CUDA_TRY(cudaEventCreateWithFlags(&c->ev_rhs_ready, cudaEventDisableTiming));
-    OVS_CUDA_TRY(cudaEventCreateWithFlags(&c->ev_rhs_out, cudaEventDisableTiming));
+    for (int s = 0; s < 4; ++s) OVS_CUDA_TRY(cudaEventCreateWithFlags(&c->ev_rhs_out[s], cudaEventDisableTiming));
     // nothing has used the staging buffers yet
     OVS_CUDA_TRY(cudaEventRecord(c->ev_commit, c->stream));
-    OVS_CUDA_TRY(cudaEventRecord(c->ev_rhs_out, c->down_stream));
+    for (int s = 0; s < 4; ++s) OVS_CUDA_TRY(cudaEventRecord(c->ev_rhs_out[s], c->down_stream));
   }
   return OVS_OK;
 }
@@ -45,10 +45,12 @@ void ovs_streaming_free(ovs_ctx* c) {
   if (c->up_stream) cudaStreamDestroy(c->up_stream);
   if (c->up_stream2) cudaStreamDestroy(c->up_stream2);
   if (c->down_stream) cudaStreamDestroy(c->down_stream);
-  cudaEvent_t evs[] = {c->ev_staged, c->ev_staged2, c->ev_commit, c->ev_rhs_ready, c->ev_rhs_out};
+  cudaEvent_t evs[] = {c->ev_staged, c->ev_staged2, c->ev_commit, c->ev_rhs_ready,
+                       c->ev_rhs_out[0], c->ev_rhs_out[1], c->ev_rhs_out[2], c->ev_rhs_out[3]};
   for (cudaEvent_t e : evs) if (e) cudaEventDestroy(e);
   c->up_stream = c->up_stream2 = c->down_stream = nullptr;
-  c->ev_staged = c->ev_staged2 = c->ev_commit = c->ev_rhs_ready = c->ev_rhs_out = nullptr;
+  c->ev_staged = c->ev_staged2 = c->ev_commit = c->ev_rhs_ready = nullptr;
+  for (int s = 0; s < 4; ++s) c->ev_rhs_out[s] = nullptr;
   c->staged_mask = 0;
 }
 
@@ -106,8 +108,10 @@ int ovs_get_rhs_async(ovs_ctx* c, int sys, int prec, double* host) {
   if ((st = ensure_copy_streams(c))) return st;
   const size_t n = (size_t)c->N * ovs_sys_nf(sys);
   if ((st = ovs_ensure((void**)&c->rhs_out[sys], sizeof(double) * n))) return st;
-  // the previous read-back of this buffer must be done before it is rewritten
-  OVS_CUDA_TRY(cudaStreamWaitEvent(c->stream, c->ev_rhs_out, 0));
+  // the previous read-back of this system's buffer must be done before it
+  // is rewritten (each system has its own buffer and event: the read-back
+  // of one system does not hold up the conversion of another)
+  OVS_CUDA_TRY(cudaStreamWaitEvent(c->stream, c->ev_rhs_out[sys], 0));
   if (prec == OVS_FP64)
     convert_kernel<double, double><<<ovs_grid(n, 256, 4 * c->num_sms * 8), 256, 0, c->stream>>>(
         reinterpret_cast<const double*>(S.rhs), c->rhs_out[sys], n);
@@ -119,7 +123,7 @@ int ovs_get_rhs_async(ovs_ctx* c, int sys, int prec, double* host) {
   OVS_CUDA_TRY(cudaEventRecord(c->ev_rhs_ready, c->stream));
   OVS_CUDA_TRY(cudaStreamWaitEvent(c->down_stream, c->ev_rhs_ready, 0));
   OVS_CUDA_TRY(cudaMemcpyAsync(host, c->rhs_out[sys], sizeof(double) * n, cudaMemcpyDeviceToHost, c->down_stream));
-  OVS_CUDA_TRY(cudaEventRecord(c->ev_rhs_out, c->down_stream));
+  OVS_CUDA_TRY(cudaEventRecord(c->ev_rhs_out[sys], c->down_stream));
   return OVS_OK;
 }
 

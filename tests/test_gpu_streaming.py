@@ -80,3 +80,45 @@ def test_partial_staging_and_empty_commit():
     np.testing.assert_array_equal(ctx.get_field("ug"), ug2.array)
     ctx.sync_copies()
     ctx.close()
+
+
+@pytest.mark.parametrize("prec", [F.OVS_FP32, F.OVS_FP64])
+def test_streamed_async_quench_steady_state_matches_synchronous(prec):
+    """The steady-state loop of a time loop: one OVS_ASM_QUENCH pass per step
+    queued with ovs_assemble_async, every step staging the next step's
+    fields (the last one the fields of a step after the loop), both
+    residuals read back on the download stream per step into their own
+    host buffers (the read-backs of the two systems do not wait for each
+    other), the status read once per step."""
+    case = M.quench_case(M.box_tet(10, 10, 12, 1.0, 1.0, 1.25), "stream3")
+    N = case.mesh.nnode
+    states = _states(case, 4)
+    sync = Context.from_case(case)
+    ref = []
+    for st in states[:3]:
+        for f in FIELDS:
+            sync.set_field(f, st[f].array)
+        sync.assemble(F.OVS_ASM_NSVOF, 6, prec)
+        sync.assemble(F.OVS_ASM_TEM, 6, prec)
+        ref.append((sync.get_rhs(F.OVS_SYS_NSVOF, prec), sync.get_rhs(F.OVS_SYS_TEM, prec)))
+    sync.close()
+    ctx = Context.from_case(case)
+    outs = [(PinnedArray((N, 5)), PinnedArray((N, 1))) for _ in range(3)]
+    ctx.stage_fields({f: states[0][f].array for f in FIELDS})
+    ctx.sync_copies()
+    for i in range(3):
+        ctx.commit_staged()
+        ctx.stage_fields({f: states[i + 1][f].array for f in FIELDS})
+        ctx.assemble_async(F.OVS_ASM_QUENCH, 6, prec)
+        ctx.get_rhs_async(F.OVS_SYS_NSVOF, prec, outs[i][0].array)
+        ctx.get_rhs_async(F.OVS_SYS_TEM, prec, outs[i][1].array)
+        ctx.assemble_wait()
+    ctx.sync_copies()
+    for (a, b), (ra, rb) in zip(outs, ref):
+        np.testing.assert_array_equal(a.array, ra)
+        np.testing.assert_array_equal(b.array, rb)
+    # the fields staged by the last step are the fourth state's
+    ctx.commit_staged()
+    np.testing.assert_array_equal(ctx.get_field("ug"), states[3]["ug"].array)
+    np.testing.assert_array_equal(ctx.get_field("tg"), states[3]["tg"].array)
+    ctx.close()
