@@ -1344,9 +1344,6 @@ __device__ __forceinline__ int warp_excl_scan(int v, int lane) {
   return x - v;
 }
 
-// gather rows: the loads of the next round in flight while a block is
-// formed (FP64, measured 2% faster; FP32 measured faster with one buffer)
-template <typename T> struct GatherPipe { static constexpr bool v = sizeof(T) == 8; };
 
 template <typename T, int KIND, bool TILED>
 __device__ __forceinline__ void gather_row(const AsmArgs& a, const int4 rr, const T* base, int str,
@@ -1417,77 +1414,30 @@ __device__ __forceinline__ void gather_row(const AsmArgs& a, const int4 rr, cons
       if constexpr (TILED) return dl ? (int)__ldg(n2e_loc + pc0 + i) : (int)__ldg(clist_loc + pc0 + i);
       else return dl ? __ldg(a.n2e + pc0 + i) : __ldg(a.clist + pc0 + i);
     };
-    // the summary values of an entry's block (and, on a diagonal lane, its
-    // residual rows)
-    auto fetch = [&](int cur, BlockIn<T>& in, T (&rv)[NF]) {
-      int e, la, b;
-      if (!dl) {
-        e = cur >> 4; la = (cur >> 2) & 3; b = cur & 3;
-      } else if constexpr (TILED) {
-        e = cur >> 2; la = cur & 3; b = la;
-      } else {
-        e = cur >> 3; la = cur & 7; b = la;
-      }
-      const T* se = base + (size_t)e * str;
-      load_block<T, KIND, TILED>(se, la, b, in);
-      if (dl) {   // only the diagonal lanes read residual rows
-#pragma unroll
-        for (int f = 0; f < NF; ++f) rv[f] = ld1<T, TILED>(se + L::RHS0 + NF * la + f);
-      } else {
-#pragma unroll
-        for (int f = 0; f < NF; ++f) rv[f] = (T)0;
-      }
-    };
-    auto add = [&](const BlockIn<T>& in, const T (&rv)[NF]) {
-      T ob[NVP];
-      form_block<T, KIND>(in, ob);
-#pragma unroll
-      for (int v = 0; v < NVP; ++v) acc[v] += ob[v];
-#pragma unroll
-      for (int f = 0; f < NF; ++f) racc[f] += rv[f];
-    };
-    if constexpr (GatherPipe<T>::v) {
-      // the loads of round r + 1 are issued before round r's block is
-      // formed (two buffers, the entries two rounds ahead)
-      BlockIn<T> b0, b1;
-      T v0[NF], v1[NF];
-      int ent = 0;
-      if (plen > 0) fetch(entry(0), b0, v0);
-      if (plen > 1) ent = entry(1);
-      auto step = [&](int r, BlockIn<T>& cur, T (&cv)[NF], BlockIn<T>& nxt, T (&nv)[NF]) {
-        if (r + 1 < plen) {
-          fetch(ent, nxt, nv);
-          if (r + 2 < plen) ent = entry(r + 2);
+    // one entry per round, the next round's entry loaded ahead (a second
+    // buffer of summary loads in flight measured slower in FP64, 13.3 vs
+    // 12.7 ms at 128^3: 235 registers and 8 warps per SM against 128 and 16)
+    int ent = plen > 0 ? entry(0) : 0;
+    for (int r = 0; r < R; ++r) {
+      const int cur = ent;
+      if (r + 1 < plen) ent = entry(r + 1);
+      if (r < plen) {
+        int e, la, b;
+        if (!dl) {
+          e = cur >> 4; la = (cur >> 2) & 3; b = cur & 3;
+        } else if constexpr (TILED) {
+          e = cur >> 2; la = cur & 3; b = la;
+        } else {
+          e = cur >> 3; la = cur & 7; b = la;
         }
-        if (r < plen) add(cur, cv);
-      };
-      for (int r = 0; r < R; r += 2) {
-        step(r, b0, v0, b1, v1);
-        if (r + 1 < R) step(r + 1, b1, v1, b0, v0);
-      }
-    } else {
-      int ent = plen > 0 ? entry(0) : 0;
-      for (int r = 0; r < R; ++r) {
-        const int cur = ent;
-        if (r + 1 < plen) ent = entry(r + 1);
-        if (r < plen) {
-          int e, la, b;
-          if (!dl) {
-            e = cur >> 4; la = (cur >> 2) & 3; b = cur & 3;
-          } else if constexpr (TILED) {
-            e = cur >> 2; la = cur & 3; b = la;
-          } else {
-            e = cur >> 3; la = cur & 7; b = la;
-          }
-          const T* se = base + (size_t)e * str;
-          T ob[1][NVP];
-          expand_block<T, KIND, 1, TILED>(se, la, b, 0, ob);
+        const T* se = base + (size_t)e * str;
+        T ob[1][NVP];
+        expand_block<T, KIND, 1, TILED>(se, la, b, 0, ob);
 #pragma unroll
-          for (int v = 0; v < NVP; ++v) acc[v] += ob[0][v];
-          if (dl) {
+        for (int v = 0; v < NVP; ++v) acc[v] += ob[0][v];
+        if (dl) {
 #pragma unroll
-            for (int f = 0; f < NF; ++f) racc[f] += ld1<T, TILED>(se + L::RHS0 + NF * la + f);
-          }
+          for (int f = 0; f < NF; ++f) racc[f] += ld1<T, TILED>(se + L::RHS0 + NF * la + f);
         }
       }
     }
