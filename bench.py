@@ -414,6 +414,23 @@ def ncu_dram_per_tet(name: str, tets: int):
                                "a %d-tet case (profiles/%s), per tet, times the tets of this workload" % (tets, name))
 
 
+def ncu_flops_per_tet(name: str):
+    """Executed FP64 flops per tet of the kernels in a committed ncu summary
+    (every `fp64_flops_per_tet` entry of the file is added: one per kernel
+    of the pass).  (None, reason) when absent."""
+    import re
+    path = ROOT / "profiles" / name
+    try:
+        txt = path.read_text()
+    except OSError:
+        return None, "no ncu summary " + name
+    vals = [float(m.group(1)) for m in re.finditer(r"`fp64_flops_per_tet` ([0-9.]+)", txt)]
+    if not vals:
+        return None, "no FP64 flop counts in " + name
+    return sum(vals), ("ncu DFMA x 2 + DMUL + DADD thread instructions of every kernel of the pass on the "
+                       "663552-tet case (profiles/%s), per tet, times the tets of this workload" % name)
+
+
 def run_config2(local_rank, args):
     """Config 2: one coupled quench time step (solveNavStoVOFTem form) on the
     1x1x2 box of 48x48x96 cells x6 tets (1,327,104 tets, 232,897 nodes): the
@@ -573,6 +590,14 @@ def run_ours(args, world, rank, local_rank, dist):
     fp64_peak = ctx.measure_fp64_peak()
     fp32_peak = ctx.measure_fp32_peak()
     roof_asm["compute_peaks_measured_tflops"] = {"fp64_fma": fp64_peak, "fp32_fma": fp32_peak}
+    fpt, fpt_src = ncu_flops_per_tet("assemble_nsvof_fp64_quench48.md")
+    if fpt:
+        fl = fpt * E
+        ach = fl / (prof["asm_nsvof_fp64_ms"] * 1e-3) / 1e12
+        roof_asm["compute_fp64"] = {"flops_per_tet": fpt, "flops_per_pass": fl, "achieved_tflops": ach,
+                                    "peak_tflops": fp64_peak, "frac": ach / fp64_peak,
+                                    "peak_kind": "measured live (ovs_measure_fp64_peak, FP64 FMA)",
+                                    "source": fpt_src}
     pass32 = assembly_pass_bytes(E, N, nnz, 4)
     roof_asm32 = {"kernels": "element_summary_kernel + gather_rows_kernel <float, NSVOF>", "bound": "hbm",
                   "achieved": pass32 / (prof["asm_nsvof_fp32_ms"] * 1e-3) / 1e9, "peak": hbm, "unit": "GB/s",

@@ -1,6 +1,7 @@
 """bench.py's helpers (CPU): the reader of the committed ncu summaries (the
 DRAM traffic per tet of its roofline entry, every kernel of a pass added;
-a missing summary reported rather than guessed), the algorithmic bytes of
+a missing summary reported rather than guessed; the executed FP64 flops per
+tet of the compute figure), the algorithmic bytes of
 the scope table, the reference arm's slabs (every cell layer of the
 workload exactly once) and its JSON line."""
 import os
@@ -33,6 +34,21 @@ def test_dram_traffic_adds_every_kernel_of_a_summary(tmp_path, monkeypatch):
 def test_missing_summaries_are_reported():
     per_tet, why = bench.ncu_dram_per_tet("no_such_summary.md", 1)
     assert per_tet is None and "no ncu summary" in why
+    fl, why = bench.ncu_flops_per_tet("no_such_summary.md")
+    assert fl is None and "no ncu summary" in why
+
+
+def test_fp64_flops_per_tet_add_every_kernel(tmp_path, monkeypatch):
+    prof = tmp_path / "profiles"
+    prof.mkdir()
+    (prof / "f.md").write_text("| element pass | 1 | 2 | 3 | 4 | `fp64_flops_per_tet` 4612 |\n"
+                               "| row pass | 1 | 2 | 3 | 4 | `fp64_flops_per_tet` 1839 |\n")
+    monkeypatch.setattr(bench, "ROOT", tmp_path)
+    fl, src = bench.ncu_flops_per_tet("f.md")
+    assert fl == 4612 + 1839 and "profiles/f.md" in src
+    (prof / "g.md").write_text("no counts here\n")
+    fl, why = bench.ncu_flops_per_tet("g.md")
+    assert fl is None and "no FP64 flop counts" in why
 
 
 def test_algorithmic_bytes_of_the_scope_table():
