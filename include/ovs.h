@@ -354,6 +354,15 @@ int ovs_spmv_device(ovs_ctx* ctx, int system, int precision, int flags,
                     const double* dx, double* dy);
 int ovs_precond_device(ovs_ctx* ctx, int system, int precision,
                        const double* dx, double* dy);
+/* ovs_spmv_device_rows: ovs_spmv_device on the rows drows[0..nrows) only
+ * (drows: a device int array of 0-based local rows, each in [0, N); an
+ * index outside that range is skipped); the other rows of dy are left as
+ * they are, and every listed row equals the full product's bit for bit.
+ * A partition computes the rows that read no ghost entry of dx while the
+ * halo exchange is in flight, then the others (src/SparseGMRES_NS_conv.f
+ * :169-176 exchanges before the whole product).  nrows = 0 does nothing. */
+int ovs_spmv_device_rows(ovs_ctx* ctx, int system, int precision, int flags,
+                         const double* dx, double* dy, const int* drows, int nrows);
 
 /* Streaming time steps (the Newton drivers push the state and read the
  * residual back every iteration, src/solveFlow.f90:39-40, 71-72, 116-117,

@@ -56,7 +56,7 @@ EXPORTS = [
     "ovs_residual_norms", "ovs_profile", "ovs_launch_count", "ovs_last_device_ms",
     "ovs_host_alloc", "ovs_host_free", "ovs_residual_vjp", "ovs_gmres_transposed", "ovs_quench_newton",
     "ovs_quench_time_steps", "ovs_stage_fields", "ovs_commit_staged", "ovs_get_rhs_async", "ovs_sync_copies",
-    "ovs_build_precond", "ovs_spmv_device", "ovs_precond_device", "ovs_measure_fp32_peak", "ovs_measure_fp64_peak", "ovs_set_option", "ovs_set_faces", "ovs_check_faces", "ovs_set_bc_spec", "ovs_check_bc_spec", "ovs_assemble_async", "ovs_assemble_wait", "ovs_apply_bcs", "ovs_get_ibc",
+    "ovs_build_precond", "ovs_spmv_device", "ovs_spmv_device_rows", "ovs_precond_device", "ovs_measure_fp32_peak", "ovs_measure_fp64_peak", "ovs_set_option", "ovs_set_faces", "ovs_check_faces", "ovs_set_bc_spec", "ovs_check_bc_spec", "ovs_assemble_async", "ovs_assemble_wait", "ovs_apply_bcs", "ovs_get_ibc",
     "ovs_gmres_tem_noalloc",
 ]
 
@@ -145,6 +145,7 @@ def load(path: str | os.PathLike | None = None) -> C.CDLL:
         "ovs_build_precond": ([vp, C.c_int, C.c_int], C.c_int),
         "ovs_spmv_device": ([vp, C.c_int, C.c_int, C.c_int, vp, vp], C.c_int),
         "ovs_precond_device": ([vp, C.c_int, C.c_int, vp, vp], C.c_int),
+        "ovs_spmv_device_rows": ([vp, C.c_int, C.c_int, C.c_int, vp, vp, vp, C.c_int], C.c_int),
         "ovs_measure_fp32_peak": ([vp, dp], C.c_int),
         "ovs_measure_fp64_peak": ([vp, dp], C.c_int),
         "ovs_set_bc_spec": ([vp, C.POINTER(OvsBcSpec)], C.c_int),

@@ -674,6 +674,17 @@ int ovs_spmv_device(ovs_ctx* c, int sys, int prec, int flags, const double* dx, 
   return OVS_OK;
 }
 
+int ovs_spmv_device_rows(ovs_ctx* c, int sys, int prec, int flags, const double* dx, double* dy,
+                         const int* drows, int nrows) {
+  if (!sys_ok(c, sys, prec) || !dx || !dy || (flags & ~OVS_SPMV_PRECOND) || nrows < 0 || (nrows > 0 && !drows))
+    return OVS_ERR_ARG;
+  int st;
+  if ((st = ovs_activate(c))) return st;
+  if ((st = ovs_spmv_rows_impl(c, sys, prec, (flags & OVS_SPMV_PRECOND) != 0, dx, dy, drows, nrows))) return st;
+  OVS_CUDA_TRY(cudaStreamSynchronize(c->stream));
+  return OVS_OK;
+}
+
 int ovs_precond_device(ovs_ctx* c, int sys, int prec, const double* dx, double* dy) {
   if (!sys_ok(c, sys, prec) || !dx || !dy) return OVS_ERR_ARG;
   int st;

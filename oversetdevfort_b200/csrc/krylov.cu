@@ -62,11 +62,15 @@ template <> struct AccT<float, float, false> { using type = float; };
 //   NSVOF(NG=6): + row phi over (u1,u2,u3,phi), + column phi into (u1,u2,u3,p)
 // The RPW = 32/NG rows of warp chunk `wglob` (all 32 lanes take part in
 // the shuffles).
-template <int NG, typename TM, typename TX, typename TY, int MODE, bool ACC64>
+// LIST: the warp chunks run over the row list rows[0, nrows) (local row
+// indices; an index outside [0, N) is skipped) instead of rows 0..N-1;
+// each listed row is computed exactly as in the full product.
+template <int NG, typename TM, typename TX, typename TY, int MODE, bool ACC64, bool LIST = false>
 __device__ __forceinline__ void spmv_block_warp(long wglob, int N, const int* __restrict__ rowptr,
                                                 const int* __restrict__ colidx, const TM* __restrict__ vals,
                                                 const TX* __restrict__ x, TY* __restrict__ y,
-                                                const TM* __restrict__ pre, const double* __restrict__ b) {
+                                                const TM* __restrict__ pre, const double* __restrict__ b,
+                                                const int* __restrict__ rows = nullptr, long nrows = 0) {
   using AT = typename AccT<TM, TX, ACC64>::type;
   constexpr int NV = 4 * NG;
   constexpr int RPW = 32 / NG;  // rows per warp
@@ -74,8 +78,16 @@ __device__ __forceinline__ void spmv_block_warp(long wglob, int N, const int* __
   const int sub = lane / NG;
   const int g = lane - sub * NG;
   const long rowl = wglob * RPW + sub;
-  const bool active = sub < RPW && rowl < N;
-  const int row = active ? (int)rowl : 0;
+  bool active;
+  int row;
+  if constexpr (LIST) {
+    const int rl = (sub < RPW && rowl < nrows) ? __ldg(rows + rowl) : -1;
+    active = rl >= 0 && rl < N;
+    row = active ? rl : 0;
+  } else {
+    active = sub < RPW && rowl < N;
+    row = active ? (int)rowl : 0;
+  }
   // column fields read by this lane's 4 values
   int cf0, cf1, cf2, cf3;
   if (NG == 6 && g == 5) { cf0 = cf1 = cf2 = cf3 = 4; }
@@ -178,18 +190,39 @@ spmv_block_kernel(int N, const int* __restrict__ rowptr, const int* __restrict__
   spmv_block_warp<NG, TM, TX, TY, MODE, ACC64>(wglob, N, rowptr, colidx, vals, x, y, pre, b);
 }
 
+// the same product over a list of rows (a partition's interior or boundary
+// rows, ovs_spmv_device_rows)
+template <int NG, typename TM, typename TX, typename TY, int MODE>
+__global__ void __launch_bounds__(SPMV_THREADS)
+spmv_block_rows_kernel(int N, const int* __restrict__ rowptr, const int* __restrict__ colidx,
+                       const TM* __restrict__ vals, const TX* __restrict__ x, TY* __restrict__ y,
+                       const TM* __restrict__ pre, const int* __restrict__ rows, int nrows) {
+  const long wglob = ((long)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  spmv_block_warp<NG, TM, TX, TY, MODE, true, true>(wglob, N, rowptr, colidx, vals, x, y, pre, nullptr, rows,
+                                                     nrows);
+}
+
 // scalar CSR (temperature): 8 lanes per row
-template <typename TM, typename TX, typename TY, int MODE, bool ACC64>
+template <typename TM, typename TX, typename TY, int MODE, bool ACC64, bool LIST = false>
 __device__ __forceinline__ void spmv_scalar_warp(long wglob, int N, const int* __restrict__ rowptr,
                                                  const int* __restrict__ colidx, const TM* __restrict__ vals,
                                                  const TX* __restrict__ x, TY* __restrict__ y,
-                                                 const TM* __restrict__ pre, const double* __restrict__ b) {
+                                                 const TM* __restrict__ pre, const double* __restrict__ b,
+                                                 const int* __restrict__ rows = nullptr, long nrows = 0) {
   using AT = typename AccT<TM, TX, ACC64>::type;
   const int lane = threadIdx.x & 31;
   const int sub = lane >> 3, k = lane & 7;
   const long rowl = wglob * 4 + sub;
-  const bool active = rowl < N;
-  const int row = active ? (int)rowl : 0;
+  bool active;
+  int row;
+  if constexpr (LIST) {
+    const int rl = rowl < nrows ? __ldg(rows + rowl) : -1;
+    active = rl >= 0 && rl < N;
+    row = active ? rl : 0;
+  } else {
+    active = rowl < N;
+    row = active ? (int)rowl : 0;
+  }
   AT a = 0;
   if (active) {
     const int s0 = __ldg(rowptr + row), s1 = __ldg(rowptr + row + 1);
@@ -214,6 +247,39 @@ spmv_scalar_kernel(int N, const int* __restrict__ rowptr, const int* __restrict_
   if (done && *done) return;
   const long wglob = ((long)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   spmv_scalar_warp<TM, TX, TY, MODE, ACC64>(wglob, N, rowptr, colidx, vals, x, y, pre, b);
+}
+
+template <typename TM, typename TX, typename TY, int MODE>
+__global__ void __launch_bounds__(SPMV_THREADS)
+spmv_scalar_rows_kernel(int N, const int* __restrict__ rowptr, const int* __restrict__ colidx,
+                        const TM* __restrict__ vals, const TX* __restrict__ x, TY* __restrict__ y,
+                        const TM* __restrict__ pre, const int* __restrict__ rows, int nrows) {
+  const long wglob = ((long)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  spmv_scalar_warp<TM, TX, TY, MODE, true, true>(wglob, N, rowptr, colidx, vals, x, y, pre, nullptr, rows, nrows);
+}
+
+// y = A x or P^-1 A x (MODE 0 / 1) on the listed rows only (FP64 vectors,
+// FP64 accumulation as in the full FP64-vector product)
+template <typename TM, int MODE>
+int launch_spmv_rows(ovs_ctx* c, int sys, const TM* vals, const double* x, double* y, const TM* pre,
+                     const int* rows, int nrows) {
+  if (nrows <= 0) return OVS_OK;
+  const int N = c->N;
+  int rpw = sys == OVS_SYS_NS ? 8 : (sys == OVS_SYS_NSVOF ? 5 : 4);
+  long warps = ((long)nrows + rpw - 1) / rpw;
+  long blocks = (warps * 32 + SPMV_THREADS - 1) / SPMV_THREADS;
+  if (sys == OVS_SYS_NS)
+    spmv_block_rows_kernel<4, TM, double, double, MODE><<<(int)blocks, SPMV_THREADS, 0, c->stream>>>(
+        N, c->rowptr, c->colidx, vals, x, y, pre, rows, nrows);
+  else if (sys == OVS_SYS_NSVOF)
+    spmv_block_rows_kernel<6, TM, double, double, MODE><<<(int)blocks, SPMV_THREADS, 0, c->stream>>>(
+        N, c->rowptr, c->colidx, vals, x, y, pre, rows, nrows);
+  else
+    spmv_scalar_rows_kernel<TM, double, double, MODE><<<(int)blocks, SPMV_THREADS, 0, c->stream>>>(
+        N, c->rowptr, c->colidx, vals, x, y, pre, rows, nrows);
+  ++c->launches;
+  OVS_CUDA_TRY(cudaGetLastError());
+  return OVS_OK;
 }
 
 template <typename TM, typename TX, typename TY, int MODE, bool ACC64 = true>
@@ -1255,6 +1321,19 @@ int ovs_spmv_pre_impl(ovs_ctx* c, int sys, int prec, const double* dx, double* d
   if (prec == OVS_FP64)
     return launch_spmv<double, double, double, 1>(c, sys, as<double>(S.vals), dx, dy, as<double>(S.binv), nullptr, nullptr);
   return launch_spmv<float, double, double, 1>(c, sys, as<float>(S.vals), dx, dy, as<float>(S.binv), nullptr, nullptr);
+}
+
+// the same products on a list of rows (device int array, local indices)
+int ovs_spmv_rows_impl(ovs_ctx* c, int sys, int prec, bool precond, const double* dx, double* dy, const int* rows,
+                       int nrows) {
+  SysStore& S = c->sys[sys][prec];
+  if (!S.vals || (precond && !S.binv)) return OVS_ERR_STATE;
+  if (prec == OVS_FP64) {
+    if (precond) return launch_spmv_rows<double, 1>(c, sys, as<double>(S.vals), dx, dy, as<double>(S.binv), rows, nrows);
+    return launch_spmv_rows<double, 0>(c, sys, as<double>(S.vals), dx, dy, nullptr, rows, nrows);
+  }
+  if (precond) return launch_spmv_rows<float, 1>(c, sys, as<float>(S.vals), dx, dy, as<float>(S.binv), rows, nrows);
+  return launch_spmv_rows<float, 0>(c, sys, as<float>(S.vals), dx, dy, nullptr, rows, nrows);
 }
 
 // y = A x (dx, dy FP64 device vectors), plain product

@@ -231,6 +231,8 @@ int ovs_precond_setup(ovs_ctx* c, int sys, int prec);
 int ovs_spmv_impl(ovs_ctx* c, int sys, int prec, const double* dx,
                   double* dy);
 int ovs_spmv_pre_impl(ovs_ctx* c, int sys, int prec, const double* dx, double* dy);
+int ovs_spmv_rows_impl(ovs_ctx* c, int sys, int prec, bool precond, const double* dx, double* dy, const int* rows,
+                       int nrows);
 int ovs_precond_apply_impl(ovs_ctx* c, int sys, int prec, const double* dx, double* dy);
 int ovs_gmres_ref_impl(ovs_ctx* c, int sys, double tol, int kspace, int kmin,
                        double* dsol, ovs_gmres_info* info);

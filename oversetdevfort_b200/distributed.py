@@ -28,7 +28,10 @@ point-to-point halo messages and one all-reduce per dot product (or, with
 orthog="cgs2", two vector all-reduces and one norm per Arnoldi step).  The local
 products are this package's CUDA kernels (`DeviceOperator`, through
 `ovs_spmv_device` / `ovs_precond_device`); the exchanges and the small
-Hessenberg algebra run on the host side of each rank.
+Hessenberg algebra run on the host side of each rank.  Each product is
+split around its halo exchange: the rows that read no ghost entry run
+while the messages are in flight, the others after the ghosts land
+(`split_rows`, `ovs_spmv_device_rows`).
 """
 from __future__ import annotations
 
@@ -76,6 +79,23 @@ def halo_plan(parts) -> HaloPlan:
                     [int(p.nodes.size) for p in parts])
 
 
+def split_rows(col, row, owned, nlocal: int):
+    """The owned rows of a partition's local CSR pattern (col: row pointer,
+    row: column indices, both 1-based, as ovs_get_pattern gives them) split
+    into interior rows, whose columns are all owned nodes, and boundary rows,
+    which read at least one ghost; each ascending.  The interior part of a
+    product needs no halo values, so it can run while the halo exchange is
+    in flight."""
+    col = np.asarray(col, dtype=np.int64) - 1
+    row = np.asarray(row, dtype=np.int64) - 1
+    ghost = np.ones(nlocal, dtype=bool)
+    ghost[np.asarray(owned, dtype=np.int64)] = False
+    rid = np.repeat(np.arange(nlocal), np.diff(col))
+    reads_ghost = np.bincount(rid, weights=ghost[row].astype(np.float64), minlength=nlocal) > 0
+    own = np.sort(np.asarray(owned, dtype=np.int64))
+    return own[~reads_ghost[own]], own[reads_ghost[own]]
+
+
 class _Index:
     """Index tensors of a plan on a device, made once."""
 
@@ -121,6 +141,13 @@ class LocalComm:
         for v in vals[1:]:
             s = s + v.to(s.device)
         return s
+
+    def halo_start(self, vecs: dict):
+        """In one process the halo copies are done at once."""
+        self.halo(vecs)
+
+    def halo_finish(self, handle):
+        pass
 
     def halo(self, vecs: dict):
         pl = self.plan
@@ -176,6 +203,13 @@ class TorchComm:
         return t[0]
 
     def halo(self, vecs: dict):
+        self.halo_finish(self.halo_start(vecs))
+
+    def halo_start(self, vecs: dict):
+        """Posts this rank's halo messages (the owned values its neighbours
+        hold as ghosts out, its ghosts' values in) and returns at once; the
+        ghosts are written by halo_finish.  Between the two, work that reads
+        no ghost entry can run."""
         import torch
         import torch.distributed as dist
         r, pl = self.rank, self.plan
@@ -191,9 +225,14 @@ class TorchComm:
                 rb = torch.empty((x.shape[0], pl.recv[r][s].size), dtype=x.dtype, device=x.device)
                 ops.append(dist.P2POp(dist.irecv, rb, s))
                 bufs.append((s, rb))
-        if ops:
-            for q in dist.batch_isend_irecv(ops):
-                q.wait()
+        reqs = dist.batch_isend_irecv(ops) if ops else []
+        return reqs, bufs, x
+
+    def halo_finish(self, handle):
+        reqs, bufs, x = handle
+        r, pl = self.rank, self.plan
+        for q in reqs:
+            q.wait()
         for s, rb in bufs:
             x[:, self.idx.get(("r", r, s), pl.recv[r][s], x.device)] = rb
 
@@ -204,7 +243,30 @@ class DeviceOperator:
 
     def __init__(self, ctx, system: int, precision: int = F.OVS_FP64):
         self.ctx, self.system, self.precision = ctx, system, precision
+        self._parts = None
         F.check(ctx.lib.ovs_build_precond(ctx.h, system, precision), "ovs_build_precond")
+
+    def split(self, owned):
+        """Interior and boundary owned rows of this partition (split_rows on
+        the context's pattern), for matvec_part; made once."""
+        if self._parts is None:
+            col, row = self.ctx.get_pattern()
+            inner, bnd = split_rows(col, row, owned, self.ctx.N)
+            self._parts = {"interior": inner.astype(np.int32), "boundary": bnd.astype(np.int32)}
+            self._dev = {}
+
+    def matvec_part(self, x, y, part: str):
+        """P^-1 A x on the interior or the boundary rows only
+        (ovs_spmv_device_rows); the other rows of y are left as they are."""
+        import torch
+        key = (part, str(x.device))
+        if key not in self._dev:
+            self._dev[key] = torch.as_tensor(self._parts[part], device=x.device)
+        rows = self._dev[key]
+        self._sync()
+        F.check(self.ctx.lib.ovs_spmv_device_rows(self.ctx.h, self.system, self.precision, F.OVS_SPMV_PRECOND,
+                                                  x.data_ptr(), y.data_ptr(), rows.data_ptr(), int(rows.numel())),
+                "ovs_spmv_device_rows")
 
     @staticmethod
     def _sync():
@@ -229,7 +291,7 @@ class DeviceOperator:
 
 
 def gmres_cycle(comm, ops: dict, rhs: dict, tol: float, kspace: int, kspace_min: int = 1, tem: bool = False,
-                orthog: str = "mgs", rhs_pre: bool = False):
+                orthog: str = "mgs", rhs_pre: bool = False, overlap: bool = True):
     """One GMRES(kspace) cycle from a zero start on the partitions of `comm`
     (SparseGMRES_ns_conv / _up / _tem semantics): `ops[r]` the operator of
     part r, `rhs[r]` its right-hand side (nf, N_local) with the owned rows
@@ -238,8 +300,11 @@ def gmres_cycle(comm, ops: dict, rhs: dict, tol: float, kspace: int, kspace_min:
     Gram-Schmidt twice (two vector sums and one norm per step, whatever k),
     for ranks where the latency of a collective outweighs its size.
     rhs_pre: rhs is already P^-1 times the right-hand side (the cycle then
-    solves P^-1 A x = rhs).  Returns (solution per part with ghosts filled,
-    info dict)."""
+    solves P^-1 A x = rhs).  overlap: where every operator has split /
+    matvec_part, each product runs its interior rows while the halo
+    exchange is in flight and its boundary rows after it (the owned rows
+    are the same bit for bit, so is the cycle).  Returns (solution per part
+    with ghosts filled, info dict)."""
     if orthog not in ("mgs", "cgs2"):
         raise ValueError("orthog must be 'mgs' or 'cgs2'")
     import torch
@@ -252,6 +317,10 @@ def gmres_cycle(comm, ops: dict, rhs: dict, tol: float, kspace: int, kspace_min:
 
     sol = {r: torch.zeros_like(rhs[r]) for r in P}
     info = {"iterations": 0, "converged": False, "ercheck": 0.0, "res0": 0.0}
+    split = overlap and all(hasattr(ops[r], "matvec_part") and hasattr(ops[r], "split") for r in P)
+    if split:
+        for r in P:
+            ops[r].split(pl.owned[r])
     if tem and gdot(rhs, rhs) == 0.0:   # SparseGMRES_tem.f90:68-71
         info["converged"] = True
         return sol, info
@@ -273,10 +342,21 @@ def gmres_cycle(comm, ops: dict, rhs: dict, tol: float, kspace: int, kspace_min:
     iks, ercheck = 0, 0.0
     for ik in range(1, kspace + 1):
         iks = ik
-        comm.halo(U[ik - 1])
-        w = {r: torch.empty_like(rhs[r]) for r in P}
-        for r in P:
-            ops[r].matvec(U[ik - 1][r], w[r])
+        if split:
+            # ghost rows of w stay 0: no dot reads them, and the next halo
+            # exchange overwrites them before any product does
+            w = {r: torch.zeros_like(rhs[r]) for r in P}
+            h = comm.halo_start(U[ik - 1])
+            for r in P:
+                ops[r].matvec_part(U[ik - 1][r], w[r], "interior")
+            comm.halo_finish(h)
+            for r in P:
+                ops[r].matvec_part(U[ik - 1][r], w[r], "boundary")
+        else:
+            comm.halo(U[ik - 1])
+            w = {r: torch.empty_like(rhs[r]) for r in P}
+            for r in P:
+                ops[r].matvec(U[ik - 1][r], w[r])
         U.append(w)
         if orthog == "mgs":
             # the k + 1 dots of the reference order stay on the device: each

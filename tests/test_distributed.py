@@ -4,7 +4,9 @@ partitions -- three in one process (LocalComm) and two gloo ranks
 (TorchComm) -- against the oracle's single-domain GMRES of the same system:
 the same iteration count and the same solution to 1e-10, ghosts included.
 The local products here use the oracle's local system (test stand-in for
-the GPU operator, which tests/test_gpu_distributed.py covers)."""
+the GPU operator, which tests/test_gpu_distributed.py covers), with the
+interior / boundary split of the overlapped product: on the gloo ranks the
+interior rows are computed while the halo messages are in flight."""
 import os
 import socket
 
@@ -76,6 +78,18 @@ class OracleOperator:
         with np.errstate(invalid="ignore"):
             y.copy_(torch.from_numpy(self._pre(np.ascontiguousarray(ax.T))))
 
+    def split(self, owned):
+        inner, bnd = D.split_rows(self.oc.col, self.oc.row, owned, self.oc.N)
+        self.parts = {"interior": torch.as_tensor(inner), "boundary": torch.as_tensor(bnd)}
+
+    def matvec_part(self, x, y, part):
+        # the product from x as it is now (its ghosts may still be stale),
+        # only the part's rows written
+        full = torch.empty_like(y)
+        self.matvec(x, full)
+        idx = self.parts[part]
+        y[:, idx] = full[:, idx]
+
 
 def _case(kind):
     # a quench box: every node in fluid elements, so every diagonal block is
@@ -138,6 +152,53 @@ def test_local_comm_gmres_matches_single_domain(oracle, kind):
     scale = np.abs(sg).max()
     for r, p in enumerate(parts):
         np.testing.assert_allclose(sol[r].numpy().T, sg[p.nodes], atol=1e-10 * scale, rtol=0)
+
+
+def test_split_rows_interior_and_boundary(oracle):
+    """Owned rows with every column owned are interior, the others
+    boundary; ghost rows are in neither; each list ascending."""
+    # 5 local nodes, 0-2 owned, 3-4 ghosts; rows (0-based columns):
+    # 0: {0,1}  1: {0,1,3}  2: {2}  3: {1,3}  4: {4,2}
+    rows = [[0, 1], [0, 1, 3], [2], [1, 3], [2, 4]]
+    col = np.cumsum([0] + [len(r) for r in rows]) + 1
+    row = np.concatenate([np.asarray(r) for r in rows]) + 1
+    inner, bnd = D.split_rows(col, row, [2, 0, 1], 5)
+    np.testing.assert_array_equal(inner, [0, 2])
+    np.testing.assert_array_equal(bnd, [1])
+    case = _case("nsvof")
+    parts = P.make_parts(case.mesh, 3)
+    for p in parts:
+        oc = oracle.OracleCase(P.local_case(case, p))
+        inner, bnd = D.split_rows(oc.col, oc.row, p.owned, p.nodes.size)
+        assert inner.size + bnd.size == np.asarray(p.owned).size and inner.size > 0 and bnd.size > 0
+        ghost = np.ones(p.nodes.size, bool)
+        ghost[p.owned] = False
+        c0, r0 = oc.col.astype(np.int64) - 1, oc.row.astype(np.int64) - 1
+        for i in inner:
+            assert not ghost[r0[c0[i]:c0[i + 1]]].any()
+        for i in bnd:
+            assert ghost[r0[c0[i]:c0[i + 1]]].any()
+
+
+@pytest.mark.parametrize("kind", ["nsvof", "tem"])
+def test_overlapped_products_give_the_same_cycle(oracle, kind):
+    """Interior rows while the halo is in flight, boundary rows after it:
+    the same iterations and the same solution bit for bit as the product
+    taken whole after the halo exchange."""
+    case = _case(kind)
+    parts = P.make_parts(case.mesh, 3)
+    plan = D.halo_plan(parts)
+    ops, rhs = {}, {}
+    for r, p in enumerate(parts):
+        oc = _local(oracle, case, p, kind)
+        ops[r] = OracleOperator(oc, kind)
+        rhs[r] = torch.from_numpy(np.ascontiguousarray(oc.system(kind)["rhs"].T))
+    out = [D.gmres_cycle(D.LocalComm(plan), ops, rhs, 1e-8, 200, 1, tem=kind == "tem", overlap=ov)
+           for ov in (True, False)]
+    (s1, i1), (s2, i2) = out
+    assert i1["iterations"] == i2["iterations"] and i1["converged"]
+    for r in s1:
+        np.testing.assert_array_equal(s1[r].numpy(), s2[r].numpy())
 
 
 def test_cgs2_orthogonalization_converges_to_the_same_solution(oracle):
