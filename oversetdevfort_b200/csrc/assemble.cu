@@ -496,6 +496,27 @@ __device__ void summarize_ns(const SumArgs& a, const RA& r, const LA& lo, bool t
 // the three scalars sum_j gN_a,j (du(j,k) + du(k,j)), k = 1..3, are
 // subtracted from every momentum component.  ui, umi, aci, pri, phid (FP64),
 // rphii, Ti: the fields at the point; N: its shape values.
+// Reciprocals taken once per element for the Gauss-point routines: of the
+// launch constants ts, rhoa, rhow, tref and of the element's trG, GG and
+// sqrt(GG).  The point formulas multiply by them where the reference
+// divides (a quotient and the product with the reciprocal differ by
+// rounding only); each FP64 division is a reciprocal sequence of its own.
+template <typename T> struct PointInv {
+  T ts, rhoa, rhow, tref, trG, GG, sGG;
+};
+template <typename T>
+__device__ __forceinline__ PointInv<T> point_inv(const ovs_params& p, T trG, T GG) {
+  PointInv<T> iv;
+  iv.ts = (T)(1.0 / p.ts);
+  iv.rhoa = (T)(1.0 / p.rhoa);
+  iv.rhow = (T)(1.0 / p.rhow);
+  iv.tref = (T)(1.0 / p.tref);
+  iv.trG = (T)1.0 / trG;
+  iv.GG = (T)1.0 / GG;
+  iv.sGG = (T)1.0 / sqrt(GG);
+  return iv;
+}
+
 template <typename T>
 __device__ __forceinline__ void nsvof_point(const ovs_params& p, bool fluid, const T (&N)[4], const T (&g)[4][3],
                                             const T (&G)[3][3], T GG, T trG, T w, const T (&du)[3][3],
@@ -503,12 +524,12 @@ __device__ __forceinline__ void nsvof_point(const ovs_params& p, bool fluid, con
                                             const T (&gdphi)[4], const T (&ui)[3], const T (&umi)[3],
                                             const T (&aci)[3], T pri, typename Wide<T>::type phid, T rphii, T Ti,
                                             T* q, T& KA, T& KB, T& MM, T& KDP, T (&ru)[4][3], T (&rp)[4],
-                                            T (&rf)[4], double& cfl) {
+                                            T (&rf)[4], double& cfl, const PointInv<T>& iv) {
   using W = typename Wide<T>::type;
   const T fact2 = (T)(p.alfi * p.delt * p.gami);
   const T taut = (T)(4.0 / (p.delt * p.delt));
   const T rhoa = (T)p.rhoa, rhow = (T)p.rhow, ts = (T)p.ts;
-  const T ira = (T)1.0 / rhoa - (T)1.0 / rhow;
+  const T ira = iv.rhoa - iv.rhow;
   const bool kdc_on = fabs(p.ns_kdc_w) + fabs(p.ns_kdc_a) > 0.0;
   const bool kdcphi_on = fabs(p.lsc_kdc) > 0.0;
   const T phii = (T)phid;
@@ -516,13 +537,13 @@ __device__ __forceinline__ void nsvof_point(const ovs_params& p, bool fluid, con
   const T phic = (T)phicd;
   T mdot, dmd;
   if (Ti > ts) {
-    mdot = (T)p.c_evap * (T)(1.0 - phicd) * rhow * (Ti - ts) / ts;
-    dmd = -(T)p.c_evap * rhow * (Ti - ts) / ts * (T)p.c_dmdot;
+    mdot = (T)p.c_evap * (T)(1.0 - phicd) * rhow * (Ti - ts) * iv.ts;
+    dmd = -(T)p.c_evap * rhow * (Ti - ts) * iv.ts * (T)p.c_dmdot;
   } else {
-    mdot = (T)p.c_cond * phic * rhoa * (Ti - ts) / ts;
-    dmd = (T)p.c_cond * rhoa * (Ti - ts) / ts * (T)p.c_dmdot;
+    mdot = (T)p.c_cond * phic * rhoa * (Ti - ts) * iv.ts;
+    dmd = (T)p.c_cond * rhoa * (Ti - ts) * iv.ts * (T)p.c_dmdot;
   }
-  const T vdot = mdot / rhoa - mdot / rhow;
+  const T vdot = mdot * iv.rhoa - mdot * iv.rhow;
   T rho, mu;
   if (fluid) {
     rho = (T)(p.rhow * (1.0 - phicd) + p.rhoa * phicd);
@@ -540,13 +561,13 @@ __device__ __forceinline__ void nsvof_point(const ovs_params& p, bool fluid, con
     tmp1[i] = rho * aci[i] + rho * conv - (T)p.gravvec[i] * rho;
     rL[i] = tmp1[i] + dp[i];
   }
-  const T res_phi = rphii + (uadv[0] * dphi[0] + uadv[1] * dphi[1] + uadv[2] * dphi[2]) + phii * vdot - mdot / rhoa;
+  const T res_phi = rphii + (uadv[0] * dphi[0] + uadv[1] * dphi[1] + uadv[2] * dphi[2]) + phii * vdot - mdot * iv.rhoa;
   const T taua = quad_uGu<T>(uadv, G);
   const T nu = mu / rho;
   const T taud = nu * nu * (T)12.0 * GG;
   const T tauM = (T)1.0 / (rho * sqrt(taut + taua + taud));
   const T tauLS = (T)1.0 / sqrt(taut + taua);
-  const T tauC = rho * sqrt(taua + taud) / trG;
+  const T tauC = rho * sqrt(taua + taud) * iv.trG;
   {
     const double cf = (double)p.delt * sqrt((double)taua);
     if (cf > cfl) cfl = cf;
@@ -555,15 +576,15 @@ __device__ __forceinline__ void nsvof_point(const ovs_params& p, bool fluid, con
   if (kdc_on) {
     const double nk = (double)(p.ns_kdc_w * (1.0 - phicd) + p.ns_kdc_a * phicd);
     const T rr = rL[0] * rL[0] + rL[1] * rL[1] + rL[2] * rL[2];
-    kdc = (T)low_word(nk) * sqrt(rr / GG);
+    kdc = (T)low_word(nk) * sqrt(rr * iv.GG);
   }
   T kdphi = 0;
-  if (kdcphi_on) kdphi = (T)p.lsc_kdc * fabs(res_phi) / sqrt(GG);
+  if (kdcphi_on) kdphi = (T)p.lsc_kdc * fabs(res_phi) * iv.sGG;
   const T mupk = mu + kdc;
   const T dmdi = dmd * ira;
   q[0] = uadv[0]; q[1] = uadv[1]; q[2] = uadv[2];
   q[3] = rho; q[4] = rho * tauM; q[5] = tauLS;
-  q[6] = vdot + phii * ira * dmd - dmd / rhoa;
+  q[6] = vdot + phii * ira * dmd - dmd * iv.rhoa;
   const T wf = fluid ? w : (T)0;   // solid elements contribute nothing
   q[7] = fact2 * wf * tauC * dmdi * dmdi;
   q[8] = fact2 * tauC * dmdi * wf;
@@ -630,6 +651,7 @@ __device__ void summarize_nsvof(const SumArgs& a, const RA& r, const LA& lo, boo
   const T divu = du[0][0] + du[1][1] + du[2][2];
   T svis[4], gdphi[4];
   nsvof_node_terms<T>(g, du, dphi, svis, gdphi);
+  const PointInv<T> iv = point_inv<T>(p, trG, GG);
   T KA = 0, KB = 0, MM = 0, KDP = 0;
   T ru[4][3], rp[4], rf[4], q[4][Lay<OVS_ASM_NSVOF>::GQ];
 #pragma unroll
@@ -650,7 +672,7 @@ __device__ void summarize_nsvof(const SumArgs& a, const RA& r, const LA& lo, boo
     const T rphii = r[0][14] * N[0] + r[1][14] * N[1] + r[2][14] * N[2] + r[3][14] * N[3];
     const T Ti = r[0][15] * N[0] + r[1][15] * N[1] + r[2][15] * N[2] + r[3][15] * N[3];
     nsvof_point<T>(p, fluid, N, g, G, GG, trG, w, du, dp, dphi, divu, svis, gdphi, ui, umi, aci, pri, phid, rphii, Ti,
-                   q[gp], KA, KB, MM, KDP, ru, rp, rf, cfl);
+                   q[gp], KA, KB, MM, KDP, ru, rp, rf, cfl, iv);
   }
   using L = Lay<OVS_ASM_NSVOF>;
   {
@@ -686,6 +708,7 @@ __device__ void summarize_tem(const SumArgs& a, const RA& r, const LA& lo, bool 
   element_geometry<T>(r, lo, g, G, detj, GG, trG);
   detj_out = detj;
   const T w = detj * (T)(0.25 / 6.0);
+  const PointInv<T> iv = point_inv<T>(p, trG, GG);
   T dT[3];
 #pragma unroll
   for (int j = 0; j < 3; ++j) dT[j] = r[0][10] * g[0][j] + r[1][10] * g[1][j] + r[2][10] * g[2][j] + r[3][10] * g[3][j];
@@ -719,11 +742,11 @@ __device__ void summarize_tem(const SumArgs& a, const RA& r, const LA& lo, bool 
     const T phic = (T)phicd;
     T mdot, dmdT;
     if (Ti > ts) {
-      mdot = (T)p.c_evap * (T)(1.0 - phicd) * (T)p.rhow * (Ti - ts) / ts;
-      dmdT = (T)p.c_evap * (T)(1.0 - phicd) * (T)p.rhow / ts * (T)p.c_dmdot;
+      mdot = (T)p.c_evap * (T)(1.0 - phicd) * (T)p.rhow * (Ti - ts) * iv.ts;
+      dmdT = (T)p.c_evap * (T)(1.0 - phicd) * (T)p.rhow * iv.ts * (T)p.c_dmdot;
     } else {
-      mdot = (T)p.c_cond * phic * (T)p.rhoa * (Ti - ts) / ts;
-      dmdT = (T)p.c_cond * phic * (T)p.rhoa / ts * (T)p.c_dmdot;
+      mdot = (T)p.c_cond * phic * (T)p.rhoa * (Ti - ts) * iv.ts;
+      dmdT = (T)p.c_cond * phic * (T)p.rhoa * iv.ts * (T)p.c_dmdot;
     }
     T rho, cp, hk, rcp;
     if (fluid) {
@@ -748,7 +771,7 @@ __device__ void summarize_tem(const SumArgs& a, const RA& r, const LA& lo, bool 
       if (cf > cfl) cfl = cf;
     }
     T kdcT = 0;
-    if (kdc_on && fluid) kdcT = (T)p.tem_kdc * fabs(res) / sqrt(GG) / (T)p.tref;
+    if (kdc_on && fluid) kdcT = (T)p.tem_kdc * fabs(res) * iv.sGG * iv.tref;
     const T dSe = (cpw - cpa) * mdot + ((cpw - cpa) * (Ti - ts) - lh) * dmdT;
     if constexpr (!std::is_same<T, Dual>::value) {
       const T uq[3] = {fluid ? uadv[0] : (T)0, fluid ? uadv[1] : (T)0, fluid ? uadv[2] : (T)0};
