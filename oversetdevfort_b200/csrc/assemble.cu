@@ -387,6 +387,12 @@ __device__ __forceinline__ void block_sums(const T (&q)[4][Lay<KIND>::GQ], const
   for (int a = 0; a < 4; ++a) block_sums_row<T, KIND>(q, g, w, fact1, fact2, rho_ns, a, o);
 }
 
+// 1 / sqrt(x): the reciprocal square root (FP64, FP32), and for the dual
+// numbers of the adjoint the quotient
+__device__ __forceinline__ double inv_sqrt(double x) { return rsqrt(x); }
+__device__ __forceinline__ float inv_sqrt(float x) { return rsqrtf(x); }
+__device__ __forceinline__ Dual inv_sqrt(const Dual& x) { return 1.0 / sqrt(x); }
+
 struct SumArgs {
   const void* rec;
   const int* ien;
@@ -435,6 +441,10 @@ __device__ void summarize_ns(const SumArgs& a, const RA& r, const LA& lo, bool t
   const T rho = (T)p.rhoa, mu = (T)p.mua, mupkdc = mu + (T)p.ns_kdc_a;
   const T fact2 = (T)(p.alfi * p.gami * p.delt);
   const T taut = (T)(4.0 / (p.delt * p.delt));
+  // the element's constants as reciprocals (rho, mu and trG are fixed over
+  // its points): products instead of per-point divisions
+  const T irho = (T)1.0 / rho, itrG = (T)1.0 / trG;
+  const T nu = mu * irho;
   T KA = 0, KB = 0, MM = 0;
   T ru[4][3], rp[4], q[4][Lay<OVS_ASM_NS>::GQ];
 #pragma unroll
@@ -453,10 +463,9 @@ __device__ void summarize_ns(const SumArgs& a, const RA& r, const LA& lo, bool t
     const T pri = r[0][12] * N[0] + r[1][12] * N[1] + r[2][12] * N[2] + r[3][12] * N[3];
     const T uadv[3] = {ui[0] - umi[0], ui[1] - umi[1], ui[2] - umi[2]};
     const T taua = quad_uGu<T>(uadv, G);
-    const T nu = mu / rho;
     const T taud = nu * nu * (T)12.0 * GG;
-    const T tauM = (T)1.0 / (rho * sqrt(taut + taua + taud));
-    const T tauC = rho * sqrt(taua + taud) / trG;
+    const T tauM = irho * inv_sqrt(taut + taua + taud);
+    const T tauC = rho * sqrt(taua + taud) * itrG;
     {
       const double c = (double)p.delt * sqrt((double)taua);
       if (c > cfl) cfl = c;
@@ -501,12 +510,18 @@ __device__ void summarize_ns(const SumArgs& a, const RA& r, const LA& lo, bool t
 // sqrt(GG).  The point formulas multiply by them where the reference
 // divides (a quotient and the product with the reciprocal differ by
 // rounding only); each FP64 division is a reciprocal sequence of its own.
+// At a point, one reciprocal of rho (rho cp for the temperature) serves
+// nu, tauM (kk, tauT), and 1/sqrt is the reciprocal square root
+// (inv_sqrt).  Measured for the FP64 element passes at 128^3: NS+VOF 5.9
+// -> 4.35 ms with the per-element reciprocals -> 4.24 ms with the point
+// ones, T 2.45 -> 1.74 -> 1.62 ms (FP32: 3.83 -> 2.78 and 1.25 -> 0.91).
 template <typename T> struct PointInv {
-  T ts, rhoa, rhow, tref, trG, GG, sGG;
+  T ts, rhoa, rhow, tref, trG, GG, sGG, taut;   // taut = 4 / delt^2 itself
 };
 template <typename T>
 __device__ __forceinline__ PointInv<T> point_inv(const ovs_params& p, T trG, T GG) {
   PointInv<T> iv;
+  iv.taut = (T)(4.0 / (p.delt * p.delt));
   iv.ts = (T)(1.0 / p.ts);
   iv.rhoa = (T)(1.0 / p.rhoa);
   iv.rhow = (T)(1.0 / p.rhow);
@@ -527,7 +542,7 @@ __device__ __forceinline__ void nsvof_point(const ovs_params& p, bool fluid, con
                                             T (&rf)[4], double& cfl, const PointInv<T>& iv) {
   using W = typename Wide<T>::type;
   const T fact2 = (T)(p.alfi * p.delt * p.gami);
-  const T taut = (T)(4.0 / (p.delt * p.delt));
+  const T taut = iv.taut;
   const T rhoa = (T)p.rhoa, rhow = (T)p.rhow, ts = (T)p.ts;
   const T ira = iv.rhoa - iv.rhow;
   const bool kdc_on = fabs(p.ns_kdc_w) + fabs(p.ns_kdc_a) > 0.0;
@@ -563,10 +578,11 @@ __device__ __forceinline__ void nsvof_point(const ovs_params& p, bool fluid, con
   }
   const T res_phi = rphii + (uadv[0] * dphi[0] + uadv[1] * dphi[1] + uadv[2] * dphi[2]) + phii * vdot - mdot * iv.rhoa;
   const T taua = quad_uGu<T>(uadv, G);
-  const T nu = mu / rho;
+  const T irho = (T)1.0 / rho;
+  const T nu = mu * irho;
   const T taud = nu * nu * (T)12.0 * GG;
-  const T tauM = (T)1.0 / (rho * sqrt(taut + taua + taud));
-  const T tauLS = (T)1.0 / sqrt(taut + taua);
+  const T tauM = irho * inv_sqrt(taut + taua + taud);
+  const T tauLS = inv_sqrt(taut + taua);
   const T tauC = rho * sqrt(taua + taud) * iv.trG;
   {
     const double cf = (double)p.delt * sqrt((double)taua);
@@ -762,10 +778,11 @@ __device__ void summarize_tem(const SumArgs& a, const RA& r, const LA& lo, bool 
     const T udT = uadv[0] * dT[0] + uadv[1] * dT[1] + uadv[2] * dT[2];
     const T res = rcp * (rTi + udT) - Se;
     const T taua = quad_uGu<T>(uadv, G);
-    T tt = taua + (T)(4.0 / (p.delt * p.delt));
-    const T kk = hk / (rho * cp);
+    T tt = taua + iv.taut;
+    const T ircp = (T)1.0 / (rho * cp);
+    const T kk = hk * ircp;
     tt = tt + kk * kk * (T)12.0 * GG;
-    const T tauT = (T)1.0 / (rho * cp * sqrt(tt));
+    const T tauT = ircp * inv_sqrt(tt);
     {
       const double cf = (double)p.delt * sqrt((double)taua);
       if (cf > cfl) cfl = cf;
