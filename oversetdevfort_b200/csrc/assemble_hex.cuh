@@ -121,7 +121,10 @@ __device__ void hex_summarize_nsvof(const ovs_params& p, const T r[8][16], const
   const T fact2 = (T)(p.alfi * p.delt * p.gami);
   const T taut = (T)(4.0 / (p.delt * p.delt));
   const T rhoa = (T)p.rhoa, rhow = (T)p.rhow, ts = (T)p.ts;
-  const T ira = (T)1.0 / rhoa - (T)1.0 / rhow;
+  // reciprocals of the launch constants, taken once: the point formulas
+  // multiply by them where the reference divides (as the tet routines)
+  const T its = (T)(1.0 / p.ts), irhoa = (T)(1.0 / p.rhoa), irhow = (T)(1.0 / p.rhow);
+  const T ira = irhoa - irhow;
   const bool kdc_on = fabs(p.ns_kdc_w) + fabs(p.ns_kdc_a) > 0.0;
   const bool kdcphi_on = fabs(p.lsc_kdc) > 0.0;
   T ru[8][3], rp[8], rf[8];
@@ -173,13 +176,13 @@ __device__ void hex_summarize_nsvof(const ovs_params& p, const T r[8][16], const
     const T phic = (T)phicd;
     T mdot, dmd;
     if (Ti > ts) {
-      mdot = (T)p.c_evap * (T)(1.0 - phicd) * rhow * (Ti - ts) / ts;
-      dmd = -(T)p.c_evap * rhow * (Ti - ts) / ts * (T)p.c_dmdot;
+      mdot = (T)p.c_evap * (T)(1.0 - phicd) * rhow * (Ti - ts) * its;
+      dmd = -(T)p.c_evap * rhow * (Ti - ts) * its * (T)p.c_dmdot;
     } else {
-      mdot = (T)p.c_cond * phic * rhoa * (Ti - ts) / ts;
-      dmd = (T)p.c_cond * rhoa * (Ti - ts) / ts * (T)p.c_dmdot;
+      mdot = (T)p.c_cond * phic * rhoa * (Ti - ts) * its;
+      dmd = (T)p.c_cond * rhoa * (Ti - ts) * its * (T)p.c_dmdot;
     }
-    const T vdot = mdot / rhoa - mdot / rhow;
+    const T vdot = mdot * irhoa - mdot * irhow;
     T rho, mu;
     if (fluid) {
       rho = (T)(p.rhow * (1.0 - phicd) + p.rhoa * phicd);
@@ -197,12 +200,13 @@ __device__ void hex_summarize_nsvof(const ovs_params& p, const T r[8][16], const
       tmp1[i] = rho * aci[i] + rho * conv - (T)p.gravvec[i] * rho;
       rL[i] = tmp1[i] + dp[i];
     }
-    const T res_phi = rphii + (uadv[0] * dphi[0] + uadv[1] * dphi[1] + uadv[2] * dphi[2]) + phii * vdot - mdot / rhoa;
+    const T res_phi = rphii + (uadv[0] * dphi[0] + uadv[1] * dphi[1] + uadv[2] * dphi[2]) + phii * vdot - mdot * irhoa;
     const T taua = quad_uGu<T>(uadv, G);
-    const T nu = mu / rho;
+    const T irho = (T)1.0 / rho;
+    const T nu = mu * irho;
     const T taud = nu * nu * (T)12.0 * GG;
-    const T tauM = (T)1.0 / (rho * sqrt(taut + taua + taud));
-    const T tauLS = (T)1.0 / sqrt(taut + taua);
+    const T tauM = irho * inv_sqrt(taut + taua + taud);
+    const T tauLS = inv_sqrt(taut + taua);
     const T tauC = rho * sqrt(taua + taud) / trG;
     {
       const double cf = (double)p.delt * sqrt((double)taua);
@@ -234,7 +238,7 @@ __device__ void hex_summarize_nsvof(const ovs_params& p, const T r[8][16], const
 #pragma unroll
       for (int k = 0; k < 3; ++k) rec[17 + k] = Ai[k][0] * uadv[0] + Ai[k][1] * uadv[1] + Ai[k][2] * uadv[2];
       rec[20] = rho; rec[21] = rho * tauM; rec[22] = tauLS;
-      rec[23] = vdot + phii * ira * dmd - dmd / rhoa;
+      rec[23] = vdot + phii * ira * dmd - dmd * irhoa;
       rec[24] = fact2 * wf * tauC * dmdi * dmdi;
       rec[25] = fact2 * tauC * dmdi * wf;
       rec[26] = fact2 * dmdi * wf;
@@ -254,7 +258,7 @@ __device__ void hex_summarize_nsvof(const ovs_params& p, const T r[8][16], const
       rec[29] = dphi[0]; rec[30] = dphi[1]; rec[31] = dphi[2];
       rec[32] = uadv[0]; rec[33] = uadv[1]; rec[34] = uadv[2];
       rec[35] = rho; rec[36] = rho * tauM; rec[37] = tauLS;
-      rec[38] = vdot + phii * ira * dmd - dmd / rhoa;
+      rec[38] = vdot + phii * ira * dmd - dmd * irhoa;
       rec[39] = fact2 * wf * tauC * dmdi * dmdi;
       rec[40] = fact2 * tauC * dmdi * wf;
       rec[41] = fact2 * dmdi * wf;
@@ -300,6 +304,7 @@ __device__ void hex_summarize_tem(const ovs_params& p, const T r[8][16], const T
   using L = HexLay<OVS_ASM_TEM>;
   const T fact2 = (T)(p.alfi * p.gami * p.delt);
   const T ts = (T)p.ts, cpw = (T)p.cpw, cpa = (T)p.cpa, lh = (T)p.lh;
+  const T its = (T)(1.0 / p.ts), itref = (T)(1.0 / p.tref), taut = (T)(4.0 / (p.delt * p.delt));
   const bool kdc_on = fabs(p.tem_kdc) > 0.0;
   T rt[8];
 #pragma unroll
@@ -338,11 +343,11 @@ __device__ void hex_summarize_tem(const ovs_params& p, const T r[8][16], const T
     const T phic = (T)phicd;
     T mdot, dmdT;
     if (Ti > ts) {
-      mdot = (T)p.c_evap * (T)(1.0 - phicd) * (T)p.rhow * (Ti - ts) / ts;
-      dmdT = (T)p.c_evap * (T)(1.0 - phicd) * (T)p.rhow / ts * (T)p.c_dmdot;
+      mdot = (T)p.c_evap * (T)(1.0 - phicd) * (T)p.rhow * (Ti - ts) * its;
+      dmdT = (T)p.c_evap * (T)(1.0 - phicd) * (T)p.rhow * its * (T)p.c_dmdot;
     } else {
-      mdot = (T)p.c_cond * phic * (T)p.rhoa * (Ti - ts) / ts;
-      dmdT = (T)p.c_cond * phic * (T)p.rhoa / ts * (T)p.c_dmdot;
+      mdot = (T)p.c_cond * phic * (T)p.rhoa * (Ti - ts) * its;
+      dmdT = (T)p.c_cond * phic * (T)p.rhoa * its * (T)p.c_dmdot;
     }
     T rho, cp, hk, rcp;
     if (fluid) {
@@ -358,16 +363,17 @@ __device__ void hex_summarize_tem(const ovs_params& p, const T r[8][16], const T
     const T udT = uadv[0] * dT[0] + uadv[1] * dT[1] + uadv[2] * dT[2];
     const T res = rcp * (rTi + udT) - Se;
     const T taua = quad_uGu<T>(uadv, G);
-    T tt = taua + (T)(4.0 / (p.delt * p.delt));
-    const T kk = hk / (rho * cp);
+    T tt = taua + taut;
+    const T ircp = (T)1.0 / (rho * cp);
+    const T kk = hk * ircp;
     tt = tt + kk * kk * (T)12.0 * GG;
-    const T tauT = (T)1.0 / (rho * cp * sqrt(tt));
+    const T tauT = ircp * inv_sqrt(tt);
     {
       const double cf = (double)p.delt * sqrt((double)taua);
       if (cf > cfl) cfl = cf;
     }
     T kdcT = 0;
-    if (kdc_on && fluid) kdcT = (T)p.tem_kdc * fabs(res) / sqrt(GG) / (T)p.tref;
+    if (kdc_on && fluid) kdcT = (T)p.tem_kdc * fabs(res) * inv_sqrt(GG) * itref;
     const T dSe = (cpw - cpa) * mdot + ((cpw - cpa) * (Ti - ts) - lh) * dmdT;
     T rec[L::GPW];
 #pragma unroll
