@@ -114,7 +114,7 @@ __device__ __forceinline__ void store_n(T* dst, const T* v, int n) {
 // TC: write the compact records of the tensor-core matrix pass instead
 template <typename T, bool TC = false>
 __device__ void hex_summarize_nsvof(const ovs_params& p, const T r[8][16], const T lo[8][4], bool fluid,
-                                    T* out, double& cfl, int& nbad) {
+                                    T* out, double& tamax, int& nbad) {
   using W = typename Wide<T>::type;
   using L = HexLay<OVS_ASM_NSVOF>;
   constexpr int RHS0 = TC ? HexTcLay::RHS0 : L::RHS0;
@@ -208,10 +208,7 @@ __device__ void hex_summarize_nsvof(const ovs_params& p, const T r[8][16], const
     const T tauM = irho * inv_sqrt(taut + taua + taud);
     const T tauLS = inv_sqrt(taut + taua);
     const T tauC = rho * sqrt(taua + taud) / trG;
-    {
-      const double cf = (double)p.delt * sqrt((double)taua);
-      if (cf > cfl) cfl = cf;
-    }
+    if ((double)taua > tamax) tamax = (double)taua;   // CFL number: delt sqrt(max taua), in the kernel
     T kdc = 0;
     if (kdc_on) {
       const double nk = (double)(p.ns_kdc_w * (1.0 - phicd) + p.ns_kdc_a * phicd);
@@ -299,7 +296,7 @@ __device__ void hex_summarize_nsvof(const ovs_params& p, const T r[8][16], const
 // record layout of this pass: xd(0:2) u(3:5) um(6:8) phi(9) T(10) rT(11)
 template <typename T>
 __device__ void hex_summarize_tem(const ovs_params& p, const T r[8][16], const T lo[8][4], bool fluid, T* out,
-                                  double& cfl, int& nbad) {
+                                  double& tamax, int& nbad) {
   using W = typename Wide<T>::type;
   using L = HexLay<OVS_ASM_TEM>;
   const T fact2 = (T)(p.alfi * p.gami * p.delt);
@@ -368,10 +365,7 @@ __device__ void hex_summarize_tem(const ovs_params& p, const T r[8][16], const T
     const T kk = hk * ircp;
     tt = tt + kk * kk * (T)12.0 * GG;
     const T tauT = ircp * inv_sqrt(tt);
-    {
-      const double cf = (double)p.delt * sqrt((double)taua);
-      if (cf > cfl) cfl = cf;
-    }
+    if ((double)taua > tamax) tamax = (double)taua;   // CFL number: delt sqrt(max taua), in the kernel
     T kdcT = 0;
     if (kdc_on && fluid) kdcT = (T)p.tem_kdc * fabs(res) * inv_sqrt(GG) * itref;
     const T dSe = (cpw - cpa) * mdot + ((cpw - cpa) * (Ti - ts) - lh) * dmdT;
@@ -408,7 +402,7 @@ __global__ void __launch_bounds__(64) hex_element_kernel(const SumArgs a) {
   using L = HexLay<KIND>;
   constexpr int SW = TC ? HexTcLay::SW : L::SW;
   const int e = blockIdx.x * blockDim.x + threadIdx.x;
-  double cfl = 0.0;
+  double tamax = 0.0;   // the element's largest taua over its points
   int nbad = 0;
   if (e < a.E) {
     T r[8][16], lo[8][4];
@@ -417,9 +411,10 @@ __global__ void __launch_bounds__(64) hex_element_kernel(const SumArgs a) {
     for (int n = 0; n < 8; ++n) load_rec(rec, a.ien[8 * (size_t)e + n], r[n], lo[n]);
     const bool fluid = __ldg(a.elm_id + e) == a.p.fluid_elm_id;
     T* out = reinterpret_cast<T*>(a.sum) + (size_t)e * SW;
-    if constexpr (KIND == OVS_ASM_NSVOF) hex_summarize_nsvof<T, TC>(a.p, r, lo, fluid, out, cfl, nbad);
-    else hex_summarize_tem<T>(a.p, r, lo, fluid, out, cfl, nbad);
+    if constexpr (KIND == OVS_ASM_NSVOF) hex_summarize_nsvof<T, TC>(a.p, r, lo, fluid, out, tamax, nbad);
+    else hex_summarize_tem<T>(a.p, r, lo, fluid, out, tamax, nbad);
   }
+  double cfl = (double)a.p.delt * sqrt(tamax);   // as the tet element pass
 #pragma unroll
   for (int off = 16; off > 0; off >>= 1) {
     cfl = fmax(cfl, __shfl_xor_sync(0xffffffffu, cfl, off));
