@@ -301,9 +301,10 @@ def gmres_cycle(comm, ops: dict, rhs: dict, tol: float, kspace: int, kspace_min:
     for ranks where the latency of a collective outweighs its size.
     rhs_pre: rhs is already P^-1 times the right-hand side (the cycle then
     solves P^-1 A x = rhs).  overlap: where every operator has split /
-    matvec_part, each product runs its interior rows while the halo
-    exchange is in flight and its boundary rows after it (the owned rows
-    are the same bit for bit, so is the cycle).  Returns (solution per part
+    matvec_part and comm has halo_start / halo_finish, each product runs
+    its interior rows while the halo exchange is in flight and its boundary
+    rows after it (the owned rows are the same bit for bit, so is the
+    cycle); otherwise the product is taken whole after the exchange.  Returns (solution per part
     with ghosts filled, info dict)."""
     if orthog not in ("mgs", "cgs2"):
         raise ValueError("orthog must be 'mgs' or 'cgs2'")
@@ -317,7 +318,8 @@ def gmres_cycle(comm, ops: dict, rhs: dict, tol: float, kspace: int, kspace_min:
 
     sol = {r: torch.zeros_like(rhs[r]) for r in P}
     info = {"iterations": 0, "converged": False, "ercheck": 0.0, "res0": 0.0}
-    split = overlap and all(hasattr(ops[r], "matvec_part") and hasattr(ops[r], "split") for r in P)
+    split = (overlap and hasattr(comm, "halo_start") and hasattr(comm, "halo_finish")
+             and all(hasattr(ops[r], "matvec_part") and hasattr(ops[r], "split") for r in P))
     if split:
         for r in P:
             ops[r].split(pl.owned[r])

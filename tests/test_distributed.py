@@ -200,6 +200,23 @@ def test_overlapped_products_give_the_same_cycle(oracle, kind):
     for r in s1:
         np.testing.assert_array_equal(s1[r].numpy(), s2[r].numpy())
 
+    class WholeHaloComm:
+        """A comm with the whole-vector exchange only (no halo_start):
+        the cycle takes each product whole after it."""
+
+        def __init__(self, plan):
+            self.plan, self._c = plan, D.LocalComm(plan)
+
+        def __getattr__(self, name):
+            if name in ("halo_start", "halo_finish"):
+                raise AttributeError(name)
+            return getattr(self._c, name)
+
+    s3, i3 = D.gmres_cycle(WholeHaloComm(plan), ops, rhs, 1e-8, 200, 1, tem=kind == "tem")
+    assert i3["iterations"] == i1["iterations"]
+    for r in s1:
+        np.testing.assert_array_equal(s3[r].numpy(), s1[r].numpy())
+
 
 def test_cgs2_orthogonalization_converges_to_the_same_solution(oracle):
     """The batched (classical, twice) Gram-Schmidt variant: two vector sums
