@@ -165,6 +165,12 @@ def test_split_rows_interior_and_boundary(oracle):
     inner, bnd = D.split_rows(col, row, [2, 0, 1], 5)
     np.testing.assert_array_equal(inner, [0, 2])
     np.testing.assert_array_equal(bnd, [1])
+    # one part owning every node: all rows interior; no owned node: nothing
+    inner, bnd = D.split_rows(col, row, np.arange(5), 5)
+    np.testing.assert_array_equal(inner, np.arange(5))
+    assert bnd.size == 0
+    inner, bnd = D.split_rows(col, row, np.zeros(0, dtype=np.int64), 5)
+    assert inner.size == 0 and bnd.size == 0
     case = _case("nsvof")
     parts = P.make_parts(case.mesh, 3)
     for p in parts:
