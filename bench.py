@@ -461,6 +461,32 @@ def run_config2(local_rank, args):
     return out
 
 
+def streamed_steps(ctx, F, fields: dict, out_ns, out_t, nsteps: int, primed: bool) -> None:
+    """nsteps end-to-end FP64 quench steps with their copies overlapped:
+    step i+1's fields go up on the upload streams while step i assembles,
+    step i's residuals come back on the download stream while step i+1 runs;
+    the pass is queued without waiting (ovs_assemble_async) and the step's
+    status is read once (ovs_assemble_wait).  primed: the first step's
+    fields were staged by the step before (a running time loop), and every
+    step stages the next step's fields, the last one those of the step
+    after the loop; unprimed: the first step's upload is staged here and
+    waited for, and the last step stages nothing.  Either way the loop
+    holds nsteps uploads of every field, nsteps passes and nsteps read-backs
+    of both residuals, all finished when it returns (ovs_sync_copies)."""
+    P = F.OVS_FP64
+    if not primed:
+        ctx.stage_fields(fields)
+    for i in range(nsteps):
+        ctx.commit_staged()
+        if primed or i + 1 < nsteps:
+            ctx.stage_fields(fields)
+        ctx.assemble_async(F.OVS_ASM_QUENCH, 6, P)
+        ctx.get_rhs_async(F.OVS_SYS_NSVOF, P, out_ns)
+        ctx.get_rhs_async(F.OVS_SYS_TEM, P, out_t)
+        ctx.assemble_wait()
+    ctx.sync_copies()
+
+
 def run_ours(args, world, rank, local_rank, dist):
     import numpy as np
     from oversetdevfort_b200 import _ffi as F
@@ -696,27 +722,7 @@ def run_ours(args, world, rank, local_rank, dist):
         F.check(ctx.lib.ovs_get_rhs(ctx.h, F.OVS_SYS_TEM, P, out_t.array.ctypes.data_as(dp)), "rhs")
 
     def e2e_streamed(nsteps, primed):
-        # the same copies per step, overlapped with the assembly: step i+1's
-        # fields go up on the upload streams while step i assembles, step i's
-        # residual comes back on the download stream while step i+1 runs; the
-        # pass is queued without waiting (ovs_assemble_async) and the
-        # step's status is read once (ovs_assemble_wait).  primed: the first
-        # step's fields were staged by the step before (a running time
-        # loop); every step stages the next step's fields, so nsteps steps
-        # still copy nsteps x 17 fields up and nsteps residuals down.
-        # Unprimed: the first step's upload is staged here and waited for,
-        # the last step stages nothing
-        if not primed:
-            ctx.stage_fields({f: host[f].array for f in fields})
-        for i in range(nsteps):
-            ctx.commit_staged()
-            if primed or i + 1 < nsteps:
-                ctx.stage_fields({f: host[f].array for f in fields})
-            ctx.assemble_async(F.OVS_ASM_QUENCH, 6, P)
-            ctx.get_rhs_async(F.OVS_SYS_NSVOF, P, out_ns.array)
-            ctx.get_rhs_async(F.OVS_SYS_TEM, P, out_t.array)
-            ctx.assemble_wait()
-        ctx.sync_copies()
+        streamed_steps(ctx, F, {f: host[f].array for f in fields}, out_ns.array, out_t.array, nsteps, primed)
 
     for _ in range(args.warmup):
         e2e_step()

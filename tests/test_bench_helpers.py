@@ -118,3 +118,47 @@ def test_own_arm_fails_without_a_device():
     assert res.returncode != 0
     assert "no CUDA device" in res.stderr
     assert not [ln for ln in res.stdout.splitlines() if ln.startswith("{")]
+
+
+class _RecordingContext:
+    """Stands in for api.Context in the streamed end-to-end loop: records
+    the calls in order."""
+
+    def __init__(self):
+        self.calls = []
+
+    def __getattr__(self, name):
+        if name.startswith("_"):
+            raise AttributeError(name)
+        return lambda *a, **k: self.calls.append(name)
+
+
+def _count(calls, name):
+    return sum(c == name for c in calls)
+
+
+def test_streamed_steps_hold_every_steps_copies():
+    """bench.streamed_steps: K steps hold K uploads of the fields, K passes
+    and K read-backs of both residuals, primed (the steady state of a time
+    loop) or not; every step commits its fields before its pass, stages
+    the next step's only after that commit, and the loop ends with the
+    copies synchronized."""
+    from oversetdevfort_b200 import _ffi as F
+    for primed in (False, True):
+        for K in (1, 3, 5):
+            ctx = _RecordingContext()
+            bench.streamed_steps(ctx, F, {"ug": None}, None, None, K, primed)
+            c = ctx.calls
+            assert _count(c, "stage_fields") == K
+            assert _count(c, "commit_staged") == K
+            assert _count(c, "assemble_async") == K and _count(c, "assemble_wait") == K
+            assert _count(c, "get_rhs_async") == 2 * K
+            assert c[-1] == "sync_copies" and _count(c, "sync_copies") == 1
+            commits = [i for i, n in enumerate(c) if n == "commit_staged"]
+            passes = [i for i, n in enumerate(c) if n == "assemble_async"]
+            assert all(cm < ps for cm, ps in zip(commits, passes))
+            stages = [i for i, n in enumerate(c) if n == "stage_fields"]
+            inside = [s for s in stages if s > commits[0]]
+            # primed: each step stages after its own commit; unprimed: the
+            # first upload comes before the loop, the last step stages nothing
+            assert len(inside) == (K if primed else K - 1)
